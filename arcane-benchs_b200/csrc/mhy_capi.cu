@@ -1,0 +1,496 @@
+// mhy_capi.cu -- the C ABI of include/mhy.h: context, device memory, init,
+// per-entry-point calls, CUDA-graph replay of whole cycles.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mhy_kernels.cuh"
+
+using namespace mhy;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define MHY_CUDA(call)                                                                        \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(e_ == cudaErrorMemoryAllocation ? MHY_ERR_OOM : MHY_ERR_CUDA,               \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+  } while (0)
+
+constexpr int kThreads = 256;
+inline unsigned blocks(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+enum Phase {
+  PH_SAVE = 0, PH_VELOCITY, PH_BC, PH_POSITION, PH_GEOMETRY, PH_DENSITY, PH_VISCOSITY, PH_ENERGY,
+  PH_REMAP, PH_DELTA_T
+};
+
+}  // namespace
+
+struct mhy_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Dims dm{};
+  Phys ph{};
+  BCTable bct{};
+  mhy_options opt{};
+  std::vector<double> h_coords;
+  std::vector<void*> allocs;
+  // nodes
+  double *x0 = nullptr, *xl = nullptr, *v = nullptr, *vh = nullptr, *nm = nullptr, *ud = nullptr;
+  double *phid[2] = {nullptr, nullptr}, *Gd = nullptr;
+  uint16_t* bcmask = nullptr;
+  // cells
+  double *rho = nullptr, *e = nullptr, *q = nullptr, *p = nullptr, *cs = nullptr, *mass = nullptr;
+  double *L = nullptr, *Ve = nullptr, *xc = nullptr, *U = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr;
+  double *Gc = nullptr;
+  // faces
+  double *n0 = nullptr, *A = nullptr, *uf = nullptr, *xf = nullptr, *dxf = nullptr, *gf = nullptr, *phif = nullptr;
+  Scalars* S = nullptr;
+  int sens = 0;
+  int phase = PH_SAVE;
+  bool state_set = false, initialized = false;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  int kernels_per_cycle = 0;
+
+  template <class T>
+  int alloc(T** ptr, size_t count) {
+    void* p_ = nullptr;
+    cudaError_t err = cudaMalloc(&p_, count * sizeof(T) + 16);
+    if (err != cudaSuccess) return fail(MHY_ERR_OOM, "cudaMalloc failed: " + std::string(cudaGetErrorString(err)));
+    allocs.push_back(p_);
+    *ptr = static_cast<T*>(p_);
+    return MHY_OK;
+  }
+};
+
+extern "C" {
+
+const char* mhy_last_error(void) { return g_last_error.c_str(); }
+
+void mhy_options_default(mhy_options* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->cfl = 0.3;
+  o->threshold = 1.e-10;
+  o->deltat_init = 1.e-5;
+  o->deltat_min = 1.e-8;
+  o->deltat_max = 0.01;
+  o->final_time = 0.2;
+  o->longueur_caracteristique = 0;
+  o->pseudo_centree = 0;
+  o->ordre_projection = 2;
+  o->projection_limiteur_id = 0;
+  o->nb_bc = 6;
+  const int surf[6] = {MHY_XMIN, MHY_XMAX, MHY_YMIN, MHY_YMAX, MHY_ZMIN, MHY_ZMAX};
+  const int typ[6] = {MHY_VX, MHY_VX, MHY_VY, MHY_VY, MHY_VZ, MHY_VZ};
+  for (int b = 0; b < 6; ++b) { o->bc[b].surface = surf[b]; o->bc[b].type = typ[b]; o->bc[b].value = 0.; }
+  o->nb_env = 1;
+  o->adiabatic_cst[0] = 1.4;
+  o->precision = 0;
+}
+
+int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mhy_ctx** out) {
+  if (!mesh || !opt || !out || !mesh->node_coords) return fail(MHY_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (mesh->nx < 2 || mesh->ny < 2 || mesh->nz < 2) return fail(MHY_ERR_ARG, "need at least 2 cells per direction");
+  if (opt->nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "only one environment is implemented on the device");
+  if (opt->ordre_projection < 1 || opt->ordre_projection > 2)
+    return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
+  if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
+    return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0 (minmod), 1 (superBee) or 2 (vanLeer)");
+  if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
+  if (opt->precision != 0) return fail(MHY_ERR_UNSUPPORTED, "precision mode not implemented");
+  for (int b = 0; b < opt->nb_bc; ++b)
+    if (opt->bc[b].surface < 0 || opt->bc[b].surface > 5 || opt->bc[b].type < 0 || opt->bc[b].type > 2)
+      return fail(MHY_ERR_ARG, "bad boundary condition");
+
+  mhy_ctx* c = new mhy_ctx();
+  c->opt = *opt;
+  if (device >= 0) {
+    cudaError_t err = cudaSetDevice(device);
+    if (err != cudaSuccess) { delete c; return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  }
+  cudaGetDevice(&c->device);
+  Dims& dm = c->dm;
+  dm.nx = mesh->nx; dm.ny = mesh->ny; dm.nz = mesh->nz;
+  dm.C = (long long)dm.nx * dm.ny * dm.nz;
+  dm.N = (long long)(dm.nx + 1) * (dm.ny + 1) * (dm.nz + 1);
+  dm.Fx = (long long)(dm.nx + 1) * dm.ny * dm.nz;
+  dm.Fy = (long long)dm.nx * (dm.ny + 1) * dm.nz;
+  dm.F = dm.Fx + dm.Fy + (long long)dm.nx * dm.ny * (dm.nz + 1);
+  Phys& ph = c->ph;
+  ph.gamma = opt->adiabatic_cst[0]; ph.threshold = opt->threshold; ph.cfl = opt->cfl;
+  ph.deltat_min = opt->deltat_min; ph.deltat_max = opt->deltat_max; ph.final_time = opt->final_time;
+  ph.lc_mode = opt->longueur_caracteristique; ph.pseudo_centree = opt->pseudo_centree;
+  ph.ordre_projection = opt->ordre_projection; ph.limiteur_id = opt->projection_limiteur_id;
+  c->bct.nb = opt->nb_bc;
+  for (int b = 0; b < opt->nb_bc; ++b) { c->bct.type[b] = opt->bc[b].type; c->bct.value[b] = opt->bc[b].value; }
+  c->h_coords.assign(mesh->node_coords, mesh->node_coords + 3 * dm.N);
+
+  int rc = MHY_OK;
+  auto A_ = [&](double** pp, long long n) { if (rc == MHY_OK) rc = c->alloc(pp, (size_t)n); };
+  const long long C = dm.C, N = dm.N, F = dm.F;
+  A_(&c->x0, 3 * N); A_(&c->xl, 3 * N); A_(&c->v, 3 * N); A_(&c->vh, 3 * N); A_(&c->nm, N); A_(&c->ud, 5 * N);
+  A_(&c->phid[0], 4 * N); A_(&c->phid[1], 4 * N); A_(&c->Gd, 3 * N);
+  A_(&c->rho, C); A_(&c->e, C); A_(&c->q, C); A_(&c->p, C); A_(&c->cs, C); A_(&c->mass, C); A_(&c->L, C);
+  A_(&c->Ve, C); A_(&c->xc, 3 * C); A_(&c->U, 4 * C); A_(&c->dpf, C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C);
+  A_(&c->Gc, 4 * C);
+  A_(&c->n0, 3 * F); A_(&c->A, F); A_(&c->uf, F); A_(&c->xf, 3 * F); A_(&c->dxf, F); A_(&c->gf, 4 * F);
+  A_(&c->phif, 4 * F);
+  if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
+  if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
+  if (rc != MHY_OK) { mhy_destroy(c); return rc; }
+  cudaError_t err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+
+  // node coordinates xyz-interleaved -> SoA
+  {
+    std::vector<double> soa(3 * N);
+    for (long long n = 0; n < N; ++n)
+      for (int a = 0; a < 3; ++a) soa[a * N + n] = c->h_coords[3 * n + a];
+    err = cudaMemcpy(c->x0, soa.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  }
+  // arrays whose untouched entries must read 0 (boundary-face gradients and
+  // face values, dual gradients of nodes never inner so far)
+  cudaMemset(c->gf, 0, 4 * F * sizeof(double));
+  cudaMemset(c->phif, 0, 4 * F * sizeof(double));
+  cudaMemset(c->Gd, 0, 3 * N * sizeof(double));
+  cudaMemset(c->dxf, 0, F * sizeof(double));
+
+  // Boundary node groups by coordinate threshold, PrepareFaceGroup
+  // (MahycoAnnexe.cc:183-251); bit b of bcmask[n] set when BC entry b applies.
+  {
+    const int nx = dm.nx, ny = dm.ny, nz = dm.nz;
+    const double* X = c->h_coords.data();
+    double mx[3] = {-1., -1., -1.};
+    for (long long n = 0; n < N; ++n)
+      for (int a = 0; a < 3; ++a) mx[a] = (mx[a] < X[3 * n + a]) ? X[3 * n + a] : mx[a];
+    std::vector<uint8_t> grp(N, 0);
+    const double thr = opt->threshold;
+    auto nid = [&](int i, int j, int k) { return (long long)i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k); };
+    auto face = [&](long long f0, long long f1, long long f2, long long f3) {
+      long long fn[4] = {f0, f1, f2, f3};
+      uint8_t fl = 0x3f;
+      for (int a = 0; a < 4; ++a) {
+        const double* x = X + 3 * fn[a];
+        if (x[0] > thr) fl &= ~(1u << MHY_XMIN);
+        if (x[1] > thr) fl &= ~(1u << MHY_YMIN);
+        if (x[2] > thr) fl &= ~(1u << MHY_ZMIN);
+        if (std::fabs(x[0] - mx[0]) > thr) fl &= ~(1u << MHY_XMAX);
+        if (std::fabs(x[1] - mx[1]) > thr) fl &= ~(1u << MHY_YMAX);
+        if (std::fabs(x[2] - mx[2]) > thr) fl &= ~(1u << MHY_ZMAX);
+      }
+      if (fl) for (int a = 0; a < 4; ++a) grp[fn[a]] |= fl;
+    };
+    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i <= nx; ++i)
+      face(nid(i, j, k), nid(i, j + 1, k), nid(i, j + 1, k + 1), nid(i, j, k + 1));
+    for (int k = 0; k < nz; ++k) for (int j = 0; j <= ny; ++j) for (int i = 0; i < nx; ++i)
+      face(nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j, k + 1), nid(i, j, k + 1));
+    for (int k = 0; k <= nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i)
+      face(nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k));
+    std::vector<uint16_t> mask(N, 0);
+    for (long long n = 0; n < N; ++n)
+      for (int b = 0; b < opt->nb_bc; ++b)
+        if (grp[n] >> opt->bc[b].surface & 1u) mask[n] |= (uint16_t)(1u << b);
+    err = cudaMemcpy(c->bcmask, mask.data(), N * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  }
+  Scalars s0{};
+  s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.min_bits = 0x7fefffffffffffffull;
+  err = cudaMemcpy(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice);
+  if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  c->kernels_per_cycle = 2 + 1 + 3 * 6 + 2 + 2;
+  err = cudaDeviceSynchronize();  // the memsets above ran on the legacy stream
+  if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  *out = c;
+  return MHY_OK;
+}
+
+int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
+  if (!c || !st || !st->fracvol || !st->density || !st->pressure || !st->velocity) return fail(MHY_ERR_ARG, "null argument");
+  const long long C = c->dm.C, N = c->dm.N;
+  for (long long i = 0; i < C; ++i)
+    if (!(st->fracvol[i] > 0.)) return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
+  MHY_CUDA(cudaMemcpy(c->rho, st->density, C * sizeof(double), cudaMemcpyHostToDevice));
+  MHY_CUDA(cudaMemcpy(c->p, st->pressure, C * sizeof(double), cudaMemcpyHostToDevice));
+  std::vector<double> soa(3 * N);
+  for (long long n = 0; n < N; ++n)
+    for (int a = 0; a < 3; ++a) soa[a * N + n] = st->velocity[3 * n + a];
+  MHY_CUDA(cudaMemcpy(c->v, soa.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice));
+  c->state_set = true;
+  return MHY_OK;
+}
+
+int mhy_hydro_start_init(mhy_ctx* c) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  if (!c->state_set) return fail(MHY_ERR_STATE, "mhy_set_state must come first");
+  const Dims& dm = c->dm;
+  cudaStream_t s = c->stream;
+  // temporaries: initial cell and face centres
+  double *xc0 = nullptr, *xf0 = nullptr;
+  MHY_CUDA(cudaMalloc(&xc0, 3 * dm.C * sizeof(double)));
+  MHY_CUDA(cudaMalloc(&xf0, 3 * dm.F * sizeof(double)));
+  k_init_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, xc0, c->cqs, c->Ve, c->L, c->ph.lc_mode);
+  k_init_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->x0, c->n0, xf0);
+  k_init_outer_normals<<<blocks(dm.C), kThreads, 0, s>>>(dm, xc0, xf0, c->ofn);
+  k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph.gamma, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
+  k_node_mass<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->mass, c->nm);
+  MHY_CUDA(cudaGetLastError());
+  MHY_CUDA(cudaStreamSynchronize(s));
+  cudaFree(xc0);
+  cudaFree(xf0);
+  c->initialized = true;
+  c->phase = PH_SAVE;
+  return MHY_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int launch_velocity(mhy_ctx* c) {
+  const Dims& dm = c->dm;
+  k_lagrange_nodes<<<blocks(dm.N), kThreads, 0, c->stream>>>(dm, c->S, c->p, c->q, c->cqs, c->nm, c->v, c->x0,
+                                                             c->bcmask, c->bct, c->vh, c->xl, c->ud, c->phid[0]);
+  return MHY_OK;
+}
+
+int launch_geometry(mhy_ctx* c) {
+  const Dims& dm = c->dm;
+  k_lagrange_cells<<<blocks(dm.C), kThreads, 0, c->stream>>>(dm, c->S, c->ph, c->xl, c->rho, c->e, c->q, c->p,
+                                                             c->cs, c->mass, c->cqs, c->xc, c->L, c->U);
+  return MHY_OK;
+}
+
+int launch_remap(mhy_ctx* c, int sens) {
+  const Dims& dm = c->dm;
+  cudaStream_t s = c->stream;
+  const double order2 = (double)(c->ph.ordre_projection - 1);
+  const int lim = c->ph.ordre_projection > 1 ? c->ph.limiteur_id : -1;
+  k_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->xl, c->vh, c->n0, c->A, c->uf, c->xf);
+  int cur = 0;
+  for (int i = 0; i < 3; ++i) {
+    const int d = (i + sens) % 3;
+    long long nf = d == 0 ? dm.Fx : (d == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
+    k_sweep_face_grad<<<blocks(nf), kThreads, 0, s>>>(dm, d, c->xc, c->n0, c->U, c->dxf, c->gf);
+    k_sweep_cell_grad<<<blocks(dm.C), kThreads, 0, s>>>(dm, d, lim, c->gf, c->Gc);
+    k_sweep_face_phi<<<blocks(nf), kThreads, 0, s>>>(dm, d, order2, c->xc, c->n0, c->xf, c->uf, c->dxf, c->U,
+                                                    c->Gc, c->phif);
+    k_sweep_cell_update<<<blocks(dm.C), kThreads, 0, s>>>(dm, d, c->S, c->n0, c->uf, c->A, c->ofn, c->phif, c->U,
+                                                         c->dpf);
+    if (c->ph.ordre_projection > 1)
+      k_sweep_dual_grad<<<blocks(dm.N), kThreads, 0, s>>>(dm, d, lim, c->xl, c->phid[cur], c->Gd);
+    k_sweep_dual_update<<<blocks(dm.N), kThreads, 0, s>>>(dm, d, c->S, order2, c->xl, c->dpf, c->Gd, c->phid[cur],
+                                                         c->ud, c->phid[1 - cur]);
+    cur = 1 - cur;
+  }
+  k_finalize_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph, c->S, c->U, c->Ve, c->rho, c->e, c->q, c->p, c->cs,
+                                                     c->mass);
+  k_finalize_nodes<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->ud, c->vh, c->mass, c->v, c->nm);
+  return MHY_OK;
+}
+
+int launch_delta_t(mhy_ctx* c) {
+  const Dims& dm = c->dm;
+  k_dt_min<<<blocks(dm.C), kThreads, 0, c->stream>>>(dm, c->S, c->L, c->cs, c->v);
+  k_dt_finish<<<1, 1, 0, c->stream>>>(c->S, c->ph);
+  return MHY_OK;
+}
+
+int launch_cycle(mhy_ctx* c, int sens) {
+  launch_velocity(c);
+  launch_geometry(c);
+  launch_remap(c, sens);
+  launch_delta_t(c);
+  return MHY_OK;
+}
+
+int check_phase(mhy_ctx* c, int expected) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
+  if (c->phase != expected) return fail(MHY_ERR_ORDER, "entry point called out of the time-loop order");
+  return MHY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhy_save_values_at_n(mhy_ctx* c) {
+  int rc = check_phase(c, PH_SAVE); if (rc) return rc;
+  c->phase = PH_VELOCITY; return MHY_OK;
+}
+int mhy_update_velocity(mhy_ctx* c) {
+  int rc = check_phase(c, PH_VELOCITY); if (rc) return rc;
+  launch_velocity(c); MHY_CUDA(cudaGetLastError());
+  c->phase = PH_BC; return MHY_OK;
+}
+int mhy_apply_boundary_condition(mhy_ctx* c) {
+  int rc = check_phase(c, PH_BC); if (rc) return rc;
+  c->phase = PH_POSITION; return MHY_OK;
+}
+int mhy_update_position(mhy_ctx* c) {
+  int rc = check_phase(c, PH_POSITION); if (rc) return rc;
+  c->phase = PH_GEOMETRY; return MHY_OK;
+}
+int mhy_compute_geometric_values(mhy_ctx* c) {
+  int rc = check_phase(c, PH_GEOMETRY); if (rc) return rc;
+  launch_geometry(c); MHY_CUDA(cudaGetLastError());
+  c->phase = PH_DENSITY; return MHY_OK;
+}
+int mhy_update_density(mhy_ctx* c) {
+  int rc = check_phase(c, PH_DENSITY); if (rc) return rc;
+  c->phase = PH_VISCOSITY; return MHY_OK;
+}
+int mhy_compute_artificial_viscosity(mhy_ctx* c) {
+  int rc = check_phase(c, PH_VISCOSITY); if (rc) return rc;
+  c->phase = PH_ENERGY; return MHY_OK;
+}
+int mhy_update_energy_and_pressure(mhy_ctx* c) {
+  int rc = check_phase(c, PH_ENERGY); if (rc) return rc;
+  c->phase = PH_REMAP; return MHY_OK;
+}
+int mhy_remap(mhy_ctx* c) {
+  int rc = check_phase(c, PH_REMAP); if (rc) return rc;
+  launch_remap(c, c->sens); MHY_CUDA(cudaGetLastError());
+  c->sens = (c->sens + 1) % 3;
+  c->phase = PH_DELTA_T; return MHY_OK;
+}
+int mhy_compute_delta_t(mhy_ctx* c) {
+  int rc = check_phase(c, PH_DELTA_T); if (rc) return rc;
+  launch_delta_t(c); MHY_CUDA(cudaGetLastError());
+  c->phase = PH_SAVE; return MHY_OK;
+}
+
+int mhy_step(mhy_ctx* c, int ncycles) {
+  int rc = check_phase(c, PH_SAVE); if (rc) return rc;
+  if (ncycles < 0) return fail(MHY_ERR_ARG, "ncycles < 0");
+  for (int it = 0; it < ncycles; ++it) {
+    const int s = c->sens;
+    if (!c->graph[s]) {
+      cudaGraph_t g = nullptr;
+      MHY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      launch_cycle(c, s);
+      cudaError_t le = cudaGetLastError();
+      cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+      if (le != cudaSuccess || ee != cudaSuccess)
+        return fail(MHY_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
+      cudaError_t ie = cudaGraphInstantiate(&c->graph[s], g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) { c->graph[s] = nullptr; return fail(MHY_ERR_CUDA, cudaGetErrorString(ie)); }
+    }
+    MHY_CUDA(cudaGraphLaunch(c->graph[s], c->stream));
+    c->sens = (s + 1) % 3;
+  }
+  return MHY_OK;
+}
+
+int mhy_synchronize(mhy_ctx* c) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  Scalars h{};
+  MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h.status & MHY_STATUS_DT_MIN) return fail(MHY_ERR_DT_MIN, "dt fell below deltat-min");
+  if (h.status & (MHY_STATUS_NAN_DT | MHY_STATUS_ZERO_MASS)) return fail(MHY_ERR_NUMERIC, "numeric status raised on the device");
+  return MHY_OK;
+}
+
+int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
+  if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  const long long C = c->dm.C, N = c->dm.N;
+  const double* src = nullptr;
+  bool vec = false;
+  long long n = C;
+  switch (field) {
+    case MHY_FIELD_DENSITY: src = c->rho; break;
+    case MHY_FIELD_INTERNAL_ENERGY: src = c->e; break;
+    case MHY_FIELD_PRESSURE: src = c->p; break;
+    case MHY_FIELD_SOUND_SPEED: src = c->cs; break;
+    case MHY_FIELD_PSEUDO_VISCOSITY: src = c->q; break;
+    case MHY_FIELD_CELL_VOLUME: src = c->Ve; break;
+    case MHY_FIELD_CELL_MASS: src = c->mass; break;
+    case MHY_FIELD_CARACTERISTIC_LENGTH: src = c->L; break;
+    case MHY_FIELD_VELOCITY: src = c->v; vec = true; n = N; break;
+    case MHY_FIELD_NODE_MASS: src = c->nm; n = N; break;
+    case MHY_FIELD_NODE_COORD: src = c->xl; vec = true; n = N; break;
+    default: return fail(MHY_ERR_ARG, "unknown field");
+  }
+  const size_t need = (size_t)n * (vec ? 3 : 1) * sizeof(double);
+  if (bytes < need) return fail(MHY_ERR_ARG, "destination too small");
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  if (!vec) {
+    MHY_CUDA(cudaMemcpy(dst, src, need, cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<double> soa(3 * n);
+    MHY_CUDA(cudaMemcpy(soa.data(), src, need, cudaMemcpyDeviceToHost));
+    double* o = static_cast<double*>(dst);
+    for (long long i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) o[3 * i + a] = soa[a * n + i];
+  }
+  return MHY_OK;
+}
+
+int mhy_get_dt(mhy_ctx* c, double* dt, double* dt_old) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  Scalars h{};
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
+  if (dt) *dt = h.dt;
+  if (dt_old) *dt_old = h.old_dt;
+  return MHY_OK;
+}
+
+int mhy_get_time(mhy_ctx* c, double* time, int64_t* iteration) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  Scalars h{};
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
+  if (time) *time = h.time;
+  if (iteration) *iteration = h.iteration;
+  return MHY_OK;
+}
+
+int mhy_get_status(mhy_ctx* c, uint32_t* flags) {
+  if (!c || !flags) return fail(MHY_ERR_ARG, "null argument");
+  Scalars h{};
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
+  *flags = h.status;
+  return MHY_OK;
+}
+
+int mhy_get_sizes(mhy_ctx* c, int64_t* ncells, int64_t* nnodes, int64_t* nfaces) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  if (ncells) *ncells = c->dm.C;
+  if (nnodes) *nnodes = c->dm.N;
+  if (nfaces) *nfaces = c->dm.F;
+  return MHY_OK;
+}
+
+void* mhy_get_stream(mhy_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int mhy_kernels_per_cycle(mhy_ctx* c) { return c ? c->kernels_per_cycle : 0; }
+
+void mhy_destroy(mhy_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int s = 0; s < 3; ++s) if (c->graph[s]) cudaGraphExecDestroy(c->graph[s]);
+  for (void* p_ : c->allocs) cudaFree(p_);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // extern "C"

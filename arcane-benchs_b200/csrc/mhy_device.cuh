@@ -1,0 +1,142 @@
+// mhy_device.cuh -- device helpers shared by the kernels: exact-order vector
+// arithmetic, limiters, the energy update, structured indexing.
+//
+// Every helper evaluates its expression in the same order, with the same
+// roundings, as the reference's Arcane Real3 code (sums left to right,
+// dot = x*x'+y*y'+z*z', cross as math::vecMul), so that with --fmad=false the
+// device produces the same bits as the CPU oracle.
+#pragma once
+
+#include <cstdint>
+#include "mhy_pow_third.h"
+
+namespace mhy {
+
+struct D3 { double x, y, z; };
+__device__ __forceinline__ D3 d3(double x, double y, double z) { return D3{x, y, z}; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(double s, D3 v) { return D3{v.x * s, v.y * s, v.z * s}; }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 u, D3 v) {
+  return D3{u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+}
+__device__ __forceinline__ double norm2(D3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ double comp(D3 a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
+// Arcane math::min / math::max and std::min / std::max, as the reference writes them
+__device__ __forceinline__ double amin(double a, double b) { return (a < b) ? a : b; }
+__device__ __forceinline__ double amax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+// Flux limiters, mahyco/src/Remap/RemapADIService.h:260-286
+__device__ __forceinline__ double limiter(int id, double r) {
+  switch (id) {
+    case 0: return smax(0.0, smin(1.0, r));
+    case 1: return smax(0.0, smax(smin(2.0 * r, 1.0), smin(r, 2.0)));
+    case 2: return (r <= 0.0 ? 0.0 : 2.0 * r / (1.0 + r));
+    default: return 0.0;
+  }
+}
+
+// compute_eint, mahyco/src/MahycoModule.cc:1630-1654
+__device__ __forceinline__ double compute_eint(bool pc, double g, double qn, double q, double rn,
+                                               double r, double p, double en) {
+  double pseudo = 0.;
+  if (pc && ((qn + q) * (1.0 / r - 1.0 / rn) < 0.)) pseudo = 0.5 * (q + qn);
+  if (!pc && (q * (1.0 / r - 1.0 / rn) < 0.)) pseudo = q;
+  double denom = 1 + 0.5 * (g - 1.0) * r * (1.0 / r - 1.0 / rn);
+  double numer = en - (0.5 * p + pseudo) * (1.0 / r - 1.0 / rn);
+  return numer / denom;
+}
+
+// Corner vectors (CQS) of a hexahedron, mahyco/src/MahycoModule.cc:2195-2258,
+// face centres from :1080-1087.  Node order SN_trigo.
+__device__ __forceinline__ void face_centres(const D3 x[8], D3 fc[6]) {
+  fc[0] = 0.25 * (x[0] + x[3] + x[2] + x[1]);
+  fc[1] = 0.25 * (x[0] + x[4] + x[7] + x[3]);
+  fc[2] = 0.25 * (x[0] + x[1] + x[5] + x[4]);
+  fc[3] = 0.25 * (x[4] + x[5] + x[6] + x[7]);
+  fc[4] = 0.25 * (x[1] + x[2] + x[6] + x[5]);
+  fc[5] = 0.25 * (x[2] + x[3] + x[7] + x[6]);
+}
+
+__device__ __forceinline__ void compute_cqs(const D3 x[8], const D3 fc[6], D3 out[8]) {
+  const D3 c0 = fc[0], c1 = fc[1], c2 = fc[2], c3 = fc[3], c4 = fc[4], c5 = fc[5];
+  const D3 n1a04 = 0.5 * cross(x[0] - c0, x[3] - c0);
+  const D3 n1a03 = 0.5 * cross(x[3] - c0, x[2] - c0);
+  const D3 n1a02 = 0.5 * cross(x[2] - c0, x[1] - c0);
+  const D3 n1a01 = 0.5 * cross(x[1] - c0, x[0] - c0);
+  const D3 n2a05 = 0.5 * cross(x[0] - c1, x[4] - c1);
+  const D3 n2a12 = 0.5 * cross(x[4] - c1, x[7] - c1);
+  const D3 n2a08 = 0.5 * cross(x[7] - c1, x[3] - c1);
+  const D3 n2a04 = 0.5 * cross(x[3] - c1, x[0] - c1);
+  const D3 n3a01 = 0.5 * cross(x[0] - c2, x[1] - c2);
+  const D3 n3a06 = 0.5 * cross(x[1] - c2, x[5] - c2);
+  const D3 n3a09 = 0.5 * cross(x[5] - c2, x[4] - c2);
+  const D3 n3a05 = 0.5 * cross(x[4] - c2, x[0] - c2);
+  const D3 n4a09 = 0.5 * cross(x[4] - c3, x[5] - c3);
+  const D3 n4a10 = 0.5 * cross(x[5] - c3, x[6] - c3);
+  const D3 n4a11 = 0.5 * cross(x[6] - c3, x[7] - c3);
+  const D3 n4a12 = 0.5 * cross(x[7] - c3, x[4] - c3);
+  const D3 n5a02 = 0.5 * cross(x[1] - c4, x[2] - c4);
+  const D3 n5a07 = 0.5 * cross(x[2] - c4, x[6] - c4);
+  const D3 n5a10 = 0.5 * cross(x[6] - c4, x[5] - c4);
+  const D3 n5a06 = 0.5 * cross(x[5] - c4, x[1] - c4);
+  const D3 n6a03 = 0.5 * cross(x[2] - c5, x[3] - c5);
+  const D3 n6a08 = 0.5 * cross(x[3] - c5, x[7] - c5);
+  const D3 n6a11 = 0.5 * cross(x[7] - c5, x[6] - c5);
+  const D3 n6a07 = 0.5 * cross(x[6] - c5, x[2] - c5);
+  const double t = 1. / 12.;
+  out[0] = t * (5. * (n1a01 + n1a04 + n2a04 + n2a05 + n3a05 + n3a01) + (n1a02 + n1a03 + n2a08 + n2a12 + n3a06 + n3a09));
+  out[1] = t * (5. * (n1a01 + n1a02 + n3a01 + n3a06 + n5a06 + n5a02) + (n1a04 + n1a03 + n3a09 + n3a05 + n5a10 + n5a07));
+  out[2] = t * (5. * (n1a02 + n1a03 + n5a07 + n5a02 + n6a07 + n6a03) + (n1a01 + n1a04 + n5a06 + n5a10 + n6a11 + n6a08));
+  out[3] = t * (5. * (n1a03 + n1a04 + n2a08 + n2a04 + n6a08 + n6a03) + (n1a01 + n1a02 + n2a05 + n2a12 + n6a07 + n6a11));
+  out[4] = t * (5. * (n2a05 + n2a12 + n3a05 + n3a09 + n4a09 + n4a12) + (n2a08 + n2a04 + n3a01 + n3a06 + n4a10 + n4a11));
+  out[5] = t * (5. * (n3a06 + n3a09 + n4a09 + n4a10 + n5a10 + n5a06) + (n3a01 + n3a05 + n4a12 + n4a11 + n5a07 + n5a02));
+  out[6] = t * (5. * (n4a11 + n4a10 + n5a10 + n5a07 + n6a07 + n6a11) + (n4a12 + n4a09 + n5a06 + n5a02 + n6a03 + n6a08));
+  out[7] = t * (5. * (n2a08 + n2a12 + n4a12 + n4a11 + n6a11 + n6a08) + (n2a04 + n2a05 + n4a09 + n4a10 + n6a07 + n6a03));
+}
+
+// Structured mesh dimensions and index maps.
+struct Dims {
+  int nx, ny, nz;          // cells per direction
+  long long C, N, F, Fx, Fy;
+  __device__ __forceinline__ long long cid(int i, int j, int k) const { return i + (long long)nx * (j + (long long)ny * k); }
+  __device__ __forceinline__ long long nid(int i, int j, int k) const { return i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k); }
+  __device__ __forceinline__ int ncd(int d) const { return d == 0 ? nx : (d == 1 ? ny : nz); }
+  // face of direction d whose lowest node is (i,j,k)
+  __device__ __forceinline__ long long fid(int d, int i, int j, int k) const {
+    if (d == 0) return i + (long long)(nx + 1) * (j + (long long)ny * k);
+    if (d == 1) return Fx + i + (long long)nx * (j + (long long)(ny + 1) * k);
+    return Fx + Fy + i + (long long)nx * (j + (long long)ny * k);
+  }
+  __device__ __forceinline__ void cijk(long long c, int& i, int& j, int& k) const {
+    i = (int)(c % nx); long long t = c / nx; j = (int)(t % ny); k = (int)(t / ny);
+  }
+  __device__ __forceinline__ void nijk(long long n, int& i, int& j, int& k) const {
+    i = (int)(n % (nx + 1)); long long t = n / (nx + 1); j = (int)(t % (ny + 1)); k = (int)(t / (ny + 1));
+  }
+  // number of faces of direction d, and (i,j,k) of its t-th face
+  __device__ __forceinline__ long long nfd(int d) const {
+    return d == 0 ? Fx : (d == 1 ? Fy : F - Fx - Fy);
+  }
+  __device__ __forceinline__ void fdijk(int d, long long t, int& i, int& j, int& k) const {
+    int ex = nx + (d == 0), ey = ny + (d == 1);
+    i = (int)(t % ex); long long u = t / ex; j = (int)(u % ey); k = (int)(u / ey);
+  }
+};
+
+// SN_trigo node offsets of a cell, cartesian/CartConnectivityCellNode.h:83-94
+__device__ __constant__ const int kCellNodeOff[8][3] = {{0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1}};
+
+// Face node order: X (0,0,0),(0,1,0),(0,1,1),(0,0,1); Y (0,0,0),(1,0,0),(1,0,1),(0,0,1);
+// Z (0,0,0),(1,0,0),(1,1,0),(0,1,0).  With the reference normal formula (whose
+// y component is the negated cross-product component) every normal points to +axis.
+__device__ __forceinline__ void face_node_ids(const Dims& dm, int d, int i, int j, int k, long long out[4]) {
+  if (d == 0) { out[0] = dm.nid(i, j, k); out[1] = dm.nid(i, j + 1, k); out[2] = dm.nid(i, j + 1, k + 1); out[3] = dm.nid(i, j, k + 1); }
+  else if (d == 1) { out[0] = dm.nid(i, j, k); out[1] = dm.nid(i + 1, j, k); out[2] = dm.nid(i + 1, j, k + 1); out[3] = dm.nid(i, j, k + 1); }
+  else { out[0] = dm.nid(i, j, k); out[1] = dm.nid(i + 1, j, k); out[2] = dm.nid(i + 1, j + 1, k); out[3] = dm.nid(i, j + 1, k); }
+}
+
+}  // namespace mhy

@@ -1,0 +1,213 @@
+"""ctypes binding of the C ABI in include/mhy.h (libmhy_b200.so, sm_100a).
+
+There is no CPU fallback: loading fails with an exception when the CUDA
+library has not been built or no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+from . import gen  # noqa: F401  (re-export)
+
+_PKG = pathlib.Path(__file__).resolve().parent.parent
+LIB_PATH = _PKG / "lib" / "libmhy_b200.so"
+
+MHY_MAX_BC = 16
+MHY_MAX_ENV = 8
+
+FIELDS = {"density": 0, "internal_energy": 1, "pressure": 2, "sound_speed": 3, "pseudo_viscosity": 4,
+          "cell_volume": 5, "cell_mass": 6, "caracteristic_length": 7, "velocity": 10, "node_mass": 11,
+          "node_coord": 12}
+STATUS_DT_MIN, STATUS_FINAL_TIME, STATUS_NAN_DT, STATUS_ZERO_MASS = 1, 2, 4, 8
+ERRORS = {-1: "MHY_ERR_ARG", -2: "MHY_ERR_CUDA", -3: "MHY_ERR_OOM", -4: "MHY_ERR_UNSUPPORTED",
+          -5: "MHY_ERR_ORDER", -6: "MHY_ERR_DT_MIN", -7: "MHY_ERR_NUMERIC", -8: "MHY_ERR_STATE"}
+
+# every symbol include/mhy.h declares
+EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_start_init",
+            "mhy_save_values_at_n", "mhy_update_velocity", "mhy_apply_boundary_condition",
+            "mhy_update_position", "mhy_compute_geometric_values", "mhy_update_density",
+            "mhy_compute_artificial_viscosity", "mhy_update_energy_and_pressure", "mhy_remap",
+            "mhy_compute_delta_t", "mhy_step", "mhy_synchronize", "mhy_get_field", "mhy_get_dt",
+            "mhy_get_time", "mhy_get_status", "mhy_get_sizes", "mhy_get_stream", "mhy_kernels_per_cycle",
+            "mhy_last_error", "mhy_destroy"]
+
+
+class MhyError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class BC(ctypes.Structure):
+    _fields_ = [("surface", ctypes.c_int32), ("type", ctypes.c_int32), ("value", ctypes.c_double)]
+
+
+class COptions(ctypes.Structure):
+    _fields_ = [("cfl", ctypes.c_double), ("threshold", ctypes.c_double), ("deltat_init", ctypes.c_double),
+                ("deltat_min", ctypes.c_double), ("deltat_max", ctypes.c_double), ("final_time", ctypes.c_double),
+                ("longueur_caracteristique", ctypes.c_int32), ("pseudo_centree", ctypes.c_int32),
+                ("ordre_projection", ctypes.c_int32), ("projection_limiteur_id", ctypes.c_int32),
+                ("nb_bc", ctypes.c_int32), ("bc", BC * MHY_MAX_BC), ("nb_env", ctypes.c_int32),
+                ("adiabatic_cst", ctypes.c_double * MHY_MAX_ENV), ("precision", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
+
+
+class CMesh(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("node_coords", ctypes.POINTER(ctypes.c_double))]
+
+
+class CState(ctypes.Structure):
+    _fields_ = [("fracvol", ctypes.POINTER(ctypes.c_double)), ("density", ctypes.POINTER(ctypes.c_double)),
+                ("pressure", ctypes.POINTER(ctypes.c_double)), ("velocity", ctypes.POINTER(ctypes.c_double))]
+
+
+_lib = None
+
+
+def load(path: pathlib.Path | str | None = None):
+    """Load the shared library (no GPU call is made)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with arcane-benchs_b200/build.py (no CPU fallback exists)")
+    L = ctypes.CDLL(str(p))
+    vp = ctypes.c_void_p
+    L.mhy_options_default.argtypes = [ctypes.POINTER(COptions)]
+    L.mhy_options_default.restype = None
+    L.mhy_create.argtypes = [ctypes.POINTER(CMesh), ctypes.POINTER(COptions), ctypes.c_int, ctypes.POINTER(vp)]
+    L.mhy_set_state.argtypes = [vp, ctypes.POINTER(CState)]
+    for name in ["mhy_hydro_start_init", "mhy_save_values_at_n", "mhy_update_velocity",
+                 "mhy_apply_boundary_condition", "mhy_update_position", "mhy_compute_geometric_values",
+                 "mhy_update_density", "mhy_compute_artificial_viscosity", "mhy_update_energy_and_pressure",
+                 "mhy_remap", "mhy_compute_delta_t", "mhy_synchronize", "mhy_kernels_per_cycle"]:
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = ctypes.c_int
+    L.mhy_step.argtypes = [vp, ctypes.c_int]
+    L.mhy_get_field.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
+    L.mhy_get_dt.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.mhy_get_time.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.mhy_get_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
+    L.mhy_get_sizes.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int64)] * 3
+    L.mhy_get_stream.argtypes = [vp]
+    L.mhy_get_stream.restype = vp
+    L.mhy_last_error.restype = ctypes.c_char_p
+    L.mhy_destroy.argtypes = [vp]
+    L.mhy_destroy.restype = None
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise MhyError(rc, load().mhy_last_error().decode())
+    return rc
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_options(opts, gammas) -> COptions:
+    o = COptions()
+    load().mhy_options_default(ctypes.byref(o))
+    o.cfl, o.threshold = opts.cfl, opts.threshold
+    o.deltat_init, o.deltat_min, o.deltat_max = opts.deltat_init, opts.deltat_min, opts.deltat_max
+    o.final_time = opts.final_time
+    o.longueur_caracteristique = opts.longueur_caracteristique
+    o.pseudo_centree = opts.pseudo_centree
+    o.ordre_projection = opts.ordre_projection
+    o.projection_limiteur_id = opts.projection_limiteur_id
+    o.nb_bc = len(opts.boundary_conditions)
+    for b, (s, t, v) in enumerate(opts.boundary_conditions):
+        o.bc[b] = BC(s, t, v)
+    o.nb_env = len(gammas)
+    for k, g in enumerate(gammas):
+        o.adiabatic_cst[k] = float(g)
+    return o
+
+
+class Context:
+    """One mesh instance on one GPU (mhy_ctx)."""
+
+    def __init__(self, case, device: int = -1, init: bool = True):
+        L = load()
+        self.case = case
+        self._coords = np.ascontiguousarray(case.coords, dtype=np.float64)
+        mesh = CMesh(case.nx, case.ny, case.nz, _dp(self._coords))
+        opt = make_options(case.options, case.gamma)
+        h = ctypes.c_void_p()
+        _check(L.mhy_create(ctypes.byref(mesh), ctypes.byref(opt), device, ctypes.byref(h)))
+        self.h = h
+        fv = np.ascontiguousarray(case.fracvol, dtype=np.float64)
+        de = np.ascontiguousarray(case.density, dtype=np.float64)
+        pr = np.ascontiguousarray(case.pressure, dtype=np.float64)
+        ve = np.ascontiguousarray(case.velocity, dtype=np.float64)
+        st = CState(_dp(fv), _dp(de), _dp(pr), _dp(ve))
+        _check(L.mhy_set_state(self.h, ctypes.byref(st)))
+        if init:
+            _check(L.mhy_hydro_start_init(self.h))
+
+    # the compute-loop entry points in the reference order
+    def cycle_by_entry_points(self):
+        L = load()
+        for name in ["mhy_save_values_at_n", "mhy_update_velocity", "mhy_apply_boundary_condition",
+                     "mhy_update_position", "mhy_compute_geometric_values", "mhy_update_density",
+                     "mhy_compute_artificial_viscosity", "mhy_update_energy_and_pressure", "mhy_remap",
+                     "mhy_compute_delta_t"]:
+            _check(getattr(L, name)(self.h))
+
+    def step(self, ncycles: int = 1):
+        _check(load().mhy_step(self.h, int(ncycles)))
+
+    def synchronize(self):
+        _check(load().mhy_synchronize(self.h))
+
+    def dt(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(load().mhy_get_dt(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def time(self):
+        t, it = ctypes.c_double(), ctypes.c_int64()
+        _check(load().mhy_get_time(self.h, ctypes.byref(t), ctypes.byref(it)))
+        return t.value, it.value
+
+    def status(self) -> int:
+        f = ctypes.c_uint32()
+        _check(load().mhy_get_status(self.h, ctypes.byref(f)))
+        return f.value
+
+    def kernels_per_cycle(self) -> int:
+        return load().mhy_kernels_per_cycle(self.h)
+
+    def stream(self) -> int:
+        return load().mhy_get_stream(self.h) or 0
+
+    def field(self, name: str) -> np.ndarray:
+        c = self.case
+        fid = FIELDS[name]
+        if name in ("velocity", "node_coord"):
+            out = np.empty((c.nnodes, 3))
+        elif name == "node_mass":
+            out = np.empty(c.nnodes)
+        else:
+            out = np.empty(c.ncells)
+        _check(load().mhy_get_field(self.h, fid, out.ctypes.data_as(ctypes.c_void_p), out.nbytes))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().mhy_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,163 @@
+/* mhy.h -- C ABI of the B200 implementation of MaHyCo's Lagrange + ADI-remap step.
+ *
+ * Every entry point returns 0 (MHY_OK) or a negative MHY_ERR_* code; nothing
+ * throws across this boundary and nothing calls exit().  A context owns its
+ * device memory and one CUDA stream; all work is ordered on that stream.  One
+ * context per host thread.  The caller owns every host buffer it passes.
+ *
+ * Reference interfaces replaced (paths relative to the reference project root):
+ *   - the Arcane module entry points of mahyco/src/Mahyco.axl:150-168, called in
+ *     the order of mahyco/src/Mahyco.config:18-41 (MahycoModule.cc);
+ *   - the remap service interface IRemap, mahyco/src/Remap/IRemap.h:32-65
+ *     (appliRemap + remapVariables, called from mahyco/src/PrepareRemap.cc:462);
+ *   - the equation-of-state interface IEquationOfState,
+ *     mahyco/src/eos/IEquationOfState.h:32-65 (PerfectGas, applied after the remap,
+ *     mahyco/src/PrepareRemap.cc:553-558).
+ */
+#ifndef MHY_H
+#define MHY_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define MHY_OK                 0
+#define MHY_ERR_ARG           -1   /* bad argument or size */
+#define MHY_ERR_CUDA          -2   /* a CUDA call failed (message: mhy_last_error) */
+#define MHY_ERR_OOM           -3   /* device allocation failed */
+#define MHY_ERR_UNSUPPORTED   -4   /* option or configuration not implemented */
+#define MHY_ERR_ORDER         -5   /* entry point called out of the time-loop order */
+#define MHY_ERR_DT_MIN        -6   /* new dt < deltat-min (reference: exit(1), MahycoModule.cc:2152-2159) */
+#define MHY_ERR_NUMERIC       -7   /* NaN / non-positive volume detected on the device */
+#define MHY_ERR_STATE         -8   /* context not initialised / state missing */
+
+/* ---- device status bits (mhy_get_status) ---- */
+#define MHY_STATUS_DT_MIN       0x1u  /* dt fell below deltat-min */
+#define MHY_STATUS_FINAL_TIME   0x2u  /* time passed final-time (reference stopComputeLoop) */
+#define MHY_STATUS_NAN_DT       0x4u  /* a cell's dx/(c+|v|) was NaN or negative */
+#define MHY_STATUS_ZERO_MASS    0x8u  /* a cell's remapped mass was exactly 0 (unsupported) */
+
+/* ---- boundary conditions (TypesMahyco.h:9-18, MahycoAnnexe.cc:183-281) ---- */
+enum { MHY_XMIN = 0, MHY_XMAX, MHY_YMIN, MHY_YMAX, MHY_ZMIN, MHY_ZMAX };
+enum { MHY_VX = 0, MHY_VY = 1, MHY_VZ = 2 };
+
+typedef struct mhy_bc {
+  int32_t surface;   /* MHY_XMIN .. MHY_ZMAX: nodes of the faces lying on that plane */
+  int32_t type;      /* MHY_VX / MHY_VY / MHY_VZ: velocity component imposed */
+  double value;
+} mhy_bc;
+
+#define MHY_MAX_BC  16
+#define MHY_MAX_ENV 8
+
+/* Options, with the names of Mahyco.axl:170-340 and Remap/RemapADI.axl:139-177.
+ * mhy_options_default() gives the reference defaults plus the values of the
+ * decks in mahyco/data/Data.1.arc:59-104. */
+typedef struct mhy_options {
+  double cfl;                        /* 0.3 */
+  double threshold;                  /* 1e-10 */
+  double deltat_init;                /* 1e-5 */
+  double deltat_min;                 /* 1e-8 */
+  double deltat_max;                 /* 0.01 */
+  double final_time;                 /* 0.2 */
+  int32_t longueur_caracteristique;  /* 0 "racine-cubique-volume", 1 "faces-opposees" */
+  int32_t pseudo_centree;            /* 0 */
+  int32_t ordre_projection;          /* 2 (1 and 2 supported) */
+  int32_t projection_limiteur_id;    /* 0 minmod, 1 superBee, 2 vanLeer */
+  int32_t nb_bc;
+  mhy_bc bc[MHY_MAX_BC];             /* default: walls on the six planes */
+  int32_t nb_env;                    /* number of environments (one ideal gas each) */
+  double adiabatic_cst[MHY_MAX_ENV]; /* PerfectGas adiabatic-cst per environment */
+  int32_t precision;                 /* 0: plain FP64 */
+  int32_t reserved[7];
+} mhy_options;
+
+/* Structured hexahedral mesh: (nx+1)(ny+1)(nz+1) nodes, node (i,j,k) at
+ * index i + (nx+1)*(j + (ny+1)*k), coordinates xyz interleaved (copied). */
+typedef struct mhy_mesh_desc {
+  int32_t nx, ny, nz;
+  const double* node_coords;
+} mhy_mesh_desc;
+
+/* Initial state, the role of the test-case service initVar + the EOS initEOS
+ * (casTest/IInitialisations.h:32-50, eos/IEquationOfState.h): per environment
+ * volume fraction, density and pressure of every cell (nb_env x ncells,
+ * environment-major; a cell belongs to environment k when fracvol > 0), and
+ * the node velocity (nnodes x 3 interleaved). */
+typedef struct mhy_state {
+  const double* fracvol;
+  const double* density;
+  const double* pressure;
+  const double* velocity;
+} mhy_state;
+
+/* Fields readable with mhy_get_field (global cell values; velocity/coords as xyz) */
+typedef enum mhy_field {
+  MHY_FIELD_DENSITY = 0, MHY_FIELD_INTERNAL_ENERGY = 1, MHY_FIELD_PRESSURE = 2,
+  MHY_FIELD_SOUND_SPEED = 3, MHY_FIELD_PSEUDO_VISCOSITY = 4, MHY_FIELD_CELL_VOLUME = 5,
+  MHY_FIELD_CELL_MASS = 6, MHY_FIELD_CARACTERISTIC_LENGTH = 7,
+  MHY_FIELD_VELOCITY = 10, MHY_FIELD_NODE_MASS = 11, MHY_FIELD_NODE_COORD = 12
+} mhy_field;
+
+typedef struct mhy_ctx mhy_ctx;
+
+void mhy_options_default(mhy_options* opt);
+
+/* Mesh + options -> context (MahycoModule::accBuild, MahycoModule.cc:34-43, and
+ * the mesh/connectivity part of AccEnvDefaultService::initMesh,
+ * accenv/AccEnvDefaultService.cc:274-302). device < 0: current device. */
+int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mhy_ctx** out);
+
+/* Initial state (casModel()->initVar, MahycoModule.cc:104). */
+int mhy_set_state(mhy_ctx* ctx, const mhy_state* st);
+
+/* Init entry points of Mahyco.config:23-29 in one call: HydroStartInit
+ * (MahycoModule.cc:48-188), PrepareFaceGroup (MahycoAnnexe.cc:183-251),
+ * ComputeCellMass (MahycoModule.cc:199-225), ComputeNodeMass (:235-266). */
+int mhy_hydro_start_init(mhy_ctx* ctx);
+
+/* Compute-loop entry points, Mahyco.config:30-41, to be called in this order
+ * once per cycle.  The work is fused into fewer kernels, so a function may do
+ * the work of the next ones (e.g. mhy_update_velocity also applies the
+ * boundary conditions and moves the nodes); fields are only defined at cycle
+ * boundaries.  Out-of-order calls return MHY_ERR_ORDER. */
+int mhy_save_values_at_n(mhy_ctx* ctx);             /* MahycoModule.cc:308-450 */
+int mhy_update_velocity(mhy_ctx* ctx);              /* MahycoModule.cc:678-731 */
+int mhy_apply_boundary_condition(mhy_ctx* ctx);     /* MahycoModule.cc:936-1004 */
+int mhy_update_position(mhy_ctx* ctx);              /* MahycoModule.cc:870-931 */
+int mhy_compute_geometric_values(mhy_ctx* ctx);     /* MahycoModule.cc:1054-1299 */
+int mhy_update_density(mhy_ctx* ctx);               /* MahycoModule.cc:1331-1426 */
+int mhy_compute_artificial_viscosity(mhy_ctx* ctx); /* MahycoModule.cc:454-578 */
+int mhy_update_energy_and_pressure(mhy_ctx* ctx);   /* MahycoModule.cc:1439-1478 */
+int mhy_remap(mhy_ctx* ctx);                        /* PrepareRemap.cc:448-563 = IRemap::appliRemap
+                                                       + remapVariables + IEquationOfState::applyEOS */
+int mhy_compute_delta_t(mhy_ctx* ctx);              /* MahycoModule.cc:2076-2191 */
+
+/* ncycles complete cycles (all entry points above), replayed from a CUDA graph. */
+int mhy_step(mhy_ctx* ctx, int ncycles);
+
+/* Wait for the context's stream; returns MHY_ERR_DT_MIN / MHY_ERR_NUMERIC when
+ * the device raised the matching status bit. */
+int mhy_synchronize(mhy_ctx* ctx);
+
+int mhy_get_field(mhy_ctx* ctx, int field, void* dst, size_t bytes);
+/* dt of the next cycle (m_global_deltat), dt of the last cycle (m_old_deltat) */
+int mhy_get_dt(mhy_ctx* ctx, double* dt, double* dt_old);
+int mhy_get_time(mhy_ctx* ctx, double* time, int64_t* iteration);
+int mhy_get_status(mhy_ctx* ctx, uint32_t* flags);
+int mhy_get_sizes(mhy_ctx* ctx, int64_t* ncells, int64_t* nnodes, int64_t* nfaces);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own work after it. */
+void* mhy_get_stream(mhy_ctx* ctx);
+/* Number of kernels one cycle launches. */
+int mhy_kernels_per_cycle(mhy_ctx* ctx);
+const char* mhy_last_error(void);
+void mhy_destroy(mhy_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MHY_H */
