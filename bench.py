@@ -1,0 +1,277 @@
+"""Benchmark of the Lagrange + ADI-remap step (MaHyCo) on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: Sedov point blast, 128^3 hex mesh on [0,1.2]^3 with 1% seeded node
+jitter, one ideal gas (gamma 1.4), plain FP64.  A step is one cycle
+(Lagrange phase + three directional remap sweeps + finalisation + dt
+reduction) over the whole mesh.  Metric: cell-cycles/s (whole job).
+
+`value` is timed with CUDA events on the context stream around K graph-replayed
+cycles, state resident in HBM (working set ~2 GB > 126 MB L2, so no L2 flush is
+needed).  `e2e` is the same metric through the reference-facing C ABI: from host
+buffers (pinned), mhy_create + mhy_set_state + mhy_hydro_start_init, then K
+cycles driven entry point by entry point with dt read back to the host every
+cycle (the Arcane time loop reads it), then the final density, energy and
+velocity read back.  N > 1 GPUs run independent replicas (weak scaling; the
+path has no data exchange between independent meshes).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "arcane-benchs_b200"))
+
+METRIC = "cell-cycles/s"
+def workload_name(n):
+    return f"sedov-{n}^3-jitter1%-fp64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="mesh cells per direction")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-cycles", type=int, default=5)
+    return ap.parse_args()
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or f[0] != self.gpu:
+                continue
+            try:
+                sm.append(float(f[1])); smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() in ("active", "0x1", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(case, cycles):
+    """The oracle (CPU restatement of the reference algorithm) on this host, all cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import mhy_oracle
+    threads = os.cpu_count() or 1
+    o = mhy_oracle.Oracle(case, pow_mode="libm", threads=threads)
+    o.step(1)  # first cycle (page faults, thread start) not timed
+    t0 = time.perf_counter()
+    o.step(cycles)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": case.ncells * cycles / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"Sedov {case.nx}^3 (same mesh and state), cycles 2..{cycles + 1} after init, "
+                      f"OpenMP {threads} threads, oracle built -O3 -ffp-contract=off"}
+
+
+def run_reference(args):
+    """--impl reference: the reference algorithm on the host cores (the reference
+    itself needs the Arcane framework, absent here, so its CPU restatement runs)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from mhy_b200 import gen
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import mhy_oracle
+    case = gen.sedov(n=args.n)
+    threads = os.cpu_count() or 1
+    o = mhy_oracle.Oracle(case, pow_mode="libm", threads=threads)
+    t0 = time.perf_counter()
+    o.step(max(1, args.warmup))
+    per = (time.perf_counter() - t0) / max(1, args.warmup)
+    budget_s = 90.0
+    k = max(1, min(args.steps, int(budget_s / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(k)
+    el = time.perf_counter() - t0
+    val = case.ncells * k / el
+    sample = (f"Sedov {args.n}^3, {k} of {args.steps} requested cycles timed after {max(1, args.warmup)} warm-up "
+              f"(bounded to ~{budget_s:.0f} s), OpenMP {threads} threads")
+    line = {"metric": METRIC, "value": val, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+            "steps": k, "warmup": max(1, args.warmup), "ms_per_step": el / k * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(args.n), "cells": case.ncells, "nodes": case.nnodes},
+            "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import mhy_b200
+    from mhy_b200 import gen, bytes_model
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    case = gen.sedov(n=args.n)
+    ctx = mhy_b200.Context(case, device=local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+    kpc = ctx.kernels_per_cycle()
+
+    ctx.step(args.warmup)
+    ctx.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        ctx.step(args.steps)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = start.elapsed_time(stop)
+    ctx.synchronize()
+    status = ctx.status()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * case.ncells * args.steps / (ms / 1e3)
+    ctx.close()
+
+    # end to end through the per-entry-point C ABI, host buffers in pinned memory
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+        hcase = gen.Case(case.name, case.nx, case.ny, case.nz, pinned(case.coords), case.gamma,
+                         pinned(case.fracvol), pinned(case.density), pinned(case.pressure), pinned(case.velocity),
+                         case.options, case.cycles)
+        out_rho = pinned(np.zeros(case.ncells)); out_e = pinned(np.zeros(case.ncells))
+        out_v = pinned(np.zeros((case.nnodes, 3)))
+        L = mhy_b200.load()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c2 = mhy_b200.Context(hcase, device=local)
+        for _ in range(args.steps):
+            c2.cycle_by_entry_points()
+            c2.dt()                                   # D2H of the step's result (dt, 16 B) + sync
+        for name, arr in (("density", out_rho), ("internal_energy", out_e), ("velocity", out_v)):
+            mhy_b200._check(L.mhy_get_field(c2.h, mhy_b200.FIELDS[name], arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes))
+        el = time.perf_counter() - t0
+        c2.close()
+        if world > 1:
+            t = torch.tensor([el], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        h2d = (case.coords.nbytes + case.fracvol.nbytes + case.density.nbytes + case.pressure.nbytes
+               + case.velocity.nbytes) / args.steps
+        d2h = 16 + (out_rho.nbytes + out_e.nbytes + out_v.nbytes) / args.steps
+        e2e = {"value": world * case.ncells * args.steps / el, "unit": METRIC,
+               "h2d_bytes_per_step": round(h2d, 1), "d2h_bytes_per_step": round(d2h, 1),
+               "path": "mhy_create+mhy_set_state+mhy_hydro_start_init, per-cycle entry points + mhy_get_dt, "
+                       "mhy_get_field x3; wall clock, max over ranks"}
+
+    b_alg = bytes_model.bytes_per_cell_cycle(case.ncells, case.nnodes)
+    peak, peak_kind = measured_peak()
+    per_gpu_cells_per_s = case.ncells * args.steps / (ms / 1e3)
+    achieved = b_alg * per_gpu_cells_per_s / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "kernel": f"one cycle graph ({kpc} kernels), algorithmic bytes {b_alg:.1f} B/cell-cycle",
+                "peak_kind": peak_kind}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case, args.cpu_sample_cycles)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_name(args.n), "cells": case.ncells, "nodes": case.nnodes,
+                           "cells_per_gpu": case.ncells, "parallelism": f"replicas{world}",
+                           "l2": "working set ~2 GB > 126 MB L2 (no flush needed)"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
