@@ -32,7 +32,7 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_compute_artificial_viscosity", "mhy_update_energy_and_pressure", "mhy_remap",
             "mhy_compute_delta_t", "mhy_step", "mhy_synchronize", "mhy_get_field", "mhy_get_dt",
             "mhy_get_time", "mhy_get_status", "mhy_get_sizes", "mhy_get_stream", "mhy_kernels_per_cycle",
-            "mhy_last_error", "mhy_destroy"]
+            "mhy_last_error", "mhy_destroy", "mhy_compute_hydro_dt_noalloc"]
 
 
 class MhyError(RuntimeError):
@@ -99,6 +99,8 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_last_error.restype = ctypes.c_char_p
     L.mhy_destroy.argtypes = [vp]
     L.mhy_destroy.restype = None
+    L.mhy_compute_hydro_dt_noalloc.argtypes = [ctypes.c_int32] * 3 + [vp] * 3 + [ctypes.c_double] * 3 + [vp, vp]
+    L.mhy_compute_hydro_dt_noalloc.restype = ctypes.c_int
     _lib = L
     return L
 

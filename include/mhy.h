@@ -157,6 +157,24 @@ int mhy_kernels_per_cycle(mhy_ctx* ctx);
 const char* mhy_last_error(void);
 void mhy_destroy(mhy_ctx* ctx);
 
+/* CFL time step from device-resident fields, for callers that cannot allocate
+ * device memory (a host framework that owns all device allocations, or code
+ * recording into a stream capture).  No counterpart in the reference: it is the
+ * dt reduction of mhy_compute_delta_t with its scratch in a fixed 64 KiB
+ * __device__ array instead of context memory.  Inputs (device pointers):
+ * characteristic length L and sound speed cs per cell, node velocity v as
+ * three planes (x[N], y[N], z[N]).  Output (device pointer, 2 doubles):
+ * out[0] = min over cells of L/(cs + max |v| over the cell's nodes),
+ * out[1] = min(cfl*out[0], 1.05*dt_old, deltat_max).  Work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream); nothing is allocated.
+ * Meshes above 134217728 cells are rejected with MHY_ERR_ARG.  All calls on a
+ * device share the scratch: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device resolves the scratch
+ * address; make it before any stream capture. */
+int mhy_compute_hydro_dt_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* L, const double* cs,
+                                 const double* v, double cfl, double dt_old, double deltat_max,
+                                 double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
