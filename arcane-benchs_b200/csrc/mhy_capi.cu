@@ -49,15 +49,16 @@ struct mhy_ctx {
   std::vector<double> h_coords;
   std::vector<void*> allocs;
   // nodes
-  double *x0 = nullptr, *xl = nullptr, *v = nullptr, *vh = nullptr, *nm = nullptr, *ud = nullptr;
-  double *phid[2] = {nullptr, nullptr}, *Gd = nullptr;
+  double *x0 = nullptr, *v = nullptr, *vh = nullptr, *nm = nullptr, *Gd = nullptr;
+  double *ud[2] = {nullptr, nullptr};
   uint16_t* bcmask = nullptr;
   // cells
   double *rho = nullptr, *e = nullptr, *q = nullptr, *p = nullptr, *cs = nullptr, *mass = nullptr;
-  double *L = nullptr, *Ve = nullptr, *xc = nullptr, *U = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr;
-  double *Gc = nullptr;
+  double *L = nullptr, *Ve = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr, *xc = nullptr;
+  double *U[2] = {nullptr, nullptr};
   // faces
-  double *n0 = nullptr, *A = nullptr, *uf = nullptr, *xf = nullptr, *dxf = nullptr, *gf = nullptr, *phif = nullptr;
+  double* n0 = nullptr;
+  FaceData fd{};
   Scalars* S = nullptr;
   int sens = 0;
   int phase = PH_SAVE;
@@ -73,6 +74,17 @@ struct mhy_ctx {
     allocs.push_back(p_);
     *ptr = static_cast<T*>(p_);
     return MHY_OK;
+  }
+
+  CycleArgs args() const {
+    CycleArgs a{};
+    a.dm = dm; a.S = S; a.ph = ph; a.bct = bct; a.bcmask = bcmask;
+    a.x0 = x0; a.n0 = n0; a.ofn = ofn;
+    a.v = v; a.vh = vh; a.nm = nm; a.cqs = cqs; a.L = L; a.dpf = dpf; a.Gd = Gd; a.xc = xc;
+    a.U[0] = U[0]; a.U[1] = U[1]; a.ud[0] = ud[0]; a.ud[1] = ud[1];
+    a.fd = fd;
+    a.st.rho = rho; a.st.e = e; a.st.q = q; a.st.p = p; a.st.cs = cs; a.st.mass = mass; a.st.Ve = Ve;
+    return a;
   }
 };
 
@@ -142,13 +154,18 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   int rc = MHY_OK;
   auto A_ = [&](double** pp, long long n) { if (rc == MHY_OK) rc = c->alloc(pp, (size_t)n); };
   const long long C = dm.C, N = dm.N, F = dm.F;
-  A_(&c->x0, 3 * N); A_(&c->xl, 3 * N); A_(&c->v, 3 * N); A_(&c->vh, 3 * N); A_(&c->nm, N); A_(&c->ud, 5 * N);
-  A_(&c->phid[0], 4 * N); A_(&c->phid[1], 4 * N); A_(&c->Gd, 3 * N);
+  A_(&c->x0, 3 * N); A_(&c->v, 3 * N); A_(&c->vh, 3 * N); A_(&c->nm, N); A_(&c->Gd, 3 * N);
+  A_(&c->ud[0], 5 * N); A_(&c->ud[1], 5 * N);
   A_(&c->rho, C); A_(&c->e, C); A_(&c->q, C); A_(&c->p, C); A_(&c->cs, C); A_(&c->mass, C); A_(&c->L, C);
-  A_(&c->Ve, C); A_(&c->xc, 3 * C); A_(&c->U, 4 * C); A_(&c->dpf, C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C);
-  A_(&c->Gc, 4 * C);
-  A_(&c->n0, 3 * F); A_(&c->A, F); A_(&c->uf, F); A_(&c->xf, 3 * F); A_(&c->dxf, F); A_(&c->gf, 4 * F);
-  A_(&c->phif, 4 * F);
+  A_(&c->Ve, C); A_(&c->dpf, C); A_(&c->xc, 3 * C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C); A_(&c->U[0], 4 * C); A_(&c->U[1], 4 * C);
+  A_(&c->n0, 3 * F);
+  {
+    const long long nf[3] = {dm.Fx, dm.Fy, dm.F - dm.Fx - dm.Fy};
+    for (int d = 0; d < 3; ++d) {
+      A_(&c->fd.db[d], nf[d]); A_(&c->fd.df[d], nf[d]); A_(&c->fd.A[d], nf[d]);
+      A_(&c->fd.u[d], nf[d]);
+    }
+  }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
   if (rc != MHY_OK) { mhy_destroy(c); return rc; }
@@ -163,12 +180,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     err = cudaMemcpy(c->x0, soa.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   }
-  // arrays whose untouched entries must read 0 (boundary-face gradients and
-  // face values, dual gradients of nodes never inner so far)
-  cudaMemset(c->gf, 0, 4 * F * sizeof(double));
-  cudaMemset(c->phif, 0, 4 * F * sizeof(double));
+  // dual gradients of nodes never inner so far read 0 (the reference's
+  // variables start at zero)
   cudaMemset(c->Gd, 0, 3 * N * sizeof(double));
-  cudaMemset(c->dxf, 0, F * sizeof(double));
 
   // Boundary node groups by coordinate threshold, PrepareFaceGroup
   // (MahycoAnnexe.cc:183-251); bit b of bcmask[n] set when BC entry b applies.
@@ -212,7 +226,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.min_bits = 0x7fefffffffffffffull;
   err = cudaMemcpy(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  c->kernels_per_cycle = 2 + 1 + 3 * 6 + 2 + 2;
+  c->kernels_per_cycle = kKernelsPerCycle;
   err = cudaDeviceSynchronize();  // the memsets above ran on the legacy stream
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   *out = c;
@@ -261,60 +275,16 @@ int mhy_hydro_start_init(mhy_ctx* c) {
 
 namespace {
 
-int launch_velocity(mhy_ctx* c) {
-  const Dims& dm = c->dm;
-  k_lagrange_nodes<<<blocks(dm.N), kThreads, 0, c->stream>>>(dm, c->S, c->p, c->q, c->cqs, c->nm, c->v, c->x0,
-                                                             c->bcmask, c->bct, c->vh, c->xl, c->ud, c->phid[0]);
-  return MHY_OK;
-}
-
-int launch_geometry(mhy_ctx* c) {
-  const Dims& dm = c->dm;
-  k_lagrange_cells<<<blocks(dm.C), kThreads, 0, c->stream>>>(dm, c->S, c->ph, c->xl, c->rho, c->e, c->q, c->p,
-                                                             c->cs, c->mass, c->cqs, c->xc, c->L, c->U);
-  return MHY_OK;
-}
-
-int launch_remap(mhy_ctx* c, int sens) {
-  const Dims& dm = c->dm;
-  cudaStream_t s = c->stream;
-  const double order2 = (double)(c->ph.ordre_projection - 1);
-  const int lim = c->ph.ordre_projection > 1 ? c->ph.limiteur_id : -1;
-  k_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->xl, c->vh, c->n0, c->A, c->uf, c->xf);
-  int cur = 0;
-  for (int i = 0; i < 3; ++i) {
-    const int d = (i + sens) % 3;
-    long long nf = d == 0 ? dm.Fx : (d == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
-    k_sweep_face_grad<<<blocks(nf), kThreads, 0, s>>>(dm, d, c->xc, c->n0, c->U, c->dxf, c->gf);
-    k_sweep_cell_grad<<<blocks(dm.C), kThreads, 0, s>>>(dm, d, lim, c->gf, c->Gc);
-    k_sweep_face_phi<<<blocks(nf), kThreads, 0, s>>>(dm, d, order2, c->xc, c->n0, c->xf, c->uf, c->dxf, c->U,
-                                                    c->Gc, c->phif);
-    k_sweep_cell_update<<<blocks(dm.C), kThreads, 0, s>>>(dm, d, c->S, c->n0, c->uf, c->A, c->ofn, c->phif, c->U,
-                                                         c->dpf);
-    if (c->ph.ordre_projection > 1)
-      k_sweep_dual_grad<<<blocks(dm.N), kThreads, 0, s>>>(dm, d, lim, c->xl, c->phid[cur], c->Gd);
-    k_sweep_dual_update<<<blocks(dm.N), kThreads, 0, s>>>(dm, d, c->S, order2, c->xl, c->dpf, c->Gd, c->phid[cur],
-                                                         c->ud, c->phid[1 - cur]);
-    cur = 1 - cur;
-  }
-  k_finalize_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph, c->S, c->U, c->Ve, c->rho, c->e, c->q, c->p, c->cs,
-                                                     c->mass);
-  k_finalize_nodes<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->ud, c->vh, c->mass, c->v, c->nm);
-  return MHY_OK;
-}
-
-int launch_delta_t(mhy_ctx* c) {
-  const Dims& dm = c->dm;
-  k_dt_min<<<blocks(dm.C), kThreads, 0, c->stream>>>(dm, c->S, c->L, c->cs, c->v);
-  k_dt_finish<<<1, 1, 0, c->stream>>>(c->S, c->ph);
-  return MHY_OK;
-}
+int launch_velocity(mhy_ctx* c) { launch_lagrange_nodes(c->args(), c->stream); return MHY_OK; }
+int launch_geometry(mhy_ctx* c) { launch_lagrange_cells(c->args(), c->stream); return MHY_OK; }
+int launch_remap_(mhy_ctx* c, int sens) { launch_remap(c->args(), sens, c->stream); return MHY_OK; }
+int launch_delta_t_(mhy_ctx* c) { launch_delta_t(c->args(), c->stream); return MHY_OK; }
 
 int launch_cycle(mhy_ctx* c, int sens) {
   launch_velocity(c);
   launch_geometry(c);
-  launch_remap(c, sens);
-  launch_delta_t(c);
+  launch_remap_(c, sens);
+  launch_delta_t_(c);
   return MHY_OK;
 }
 
@@ -365,13 +335,13 @@ int mhy_update_energy_and_pressure(mhy_ctx* c) {
 }
 int mhy_remap(mhy_ctx* c) {
   int rc = check_phase(c, PH_REMAP); if (rc) return rc;
-  launch_remap(c, c->sens); MHY_CUDA(cudaGetLastError());
+  launch_remap_(c, c->sens); MHY_CUDA(cudaGetLastError());
   c->sens = (c->sens + 1) % 3;
   c->phase = PH_DELTA_T; return MHY_OK;
 }
 int mhy_compute_delta_t(mhy_ctx* c) {
   int rc = check_phase(c, PH_DELTA_T); if (rc) return rc;
-  launch_delta_t(c); MHY_CUDA(cudaGetLastError());
+  launch_delta_t_(c); MHY_CUDA(cudaGetLastError());
   c->phase = PH_SAVE; return MHY_OK;
 }
 
@@ -425,7 +395,21 @@ int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
     case MHY_FIELD_CARACTERISTIC_LENGTH: src = c->L; break;
     case MHY_FIELD_VELOCITY: src = c->v; vec = true; n = N; break;
     case MHY_FIELD_NODE_MASS: src = c->nm; n = N; break;
-    case MHY_FIELD_NODE_COORD: src = c->xl; vec = true; n = N; break;
+    case MHY_FIELD_NODE_COORD: {
+      // Lagrangian coordinates of the last cycle: x0 + dt * v_half (MahycoModule.cc:899-901)
+      if (bytes < (size_t)N * 3 * sizeof(double)) return fail(MHY_ERR_ARG, "destination too small");
+      MHY_CUDA(cudaStreamSynchronize(c->stream));
+      std::vector<double> x0h(3 * N), vhh(3 * N);
+      Scalars h{};
+      MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
+      MHY_CUDA(cudaMemcpy(x0h.data(), c->x0, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
+      MHY_CUDA(cudaMemcpy(vhh.data(), c->vh, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
+      double* o = static_cast<double*>(dst);
+      const double dtu = h.iteration > 0 ? h.old_dt : 0.0;
+      for (long long i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) o[3 * i + a] = h.iteration > 0 ? x0h[a * N + i] + vhh[a * N + i] * dtu : x0h[a * N + i];
+      return MHY_OK;
+    }
     default: return fail(MHY_ERR_ARG, "unknown field");
   }
   const size_t need = (size_t)n * (vec ? 3 : 1) * sizeof(double);

@@ -1,0 +1,979 @@
+// mhy_cycle.cu -- fused sm_100a kernels of one Lagrange + ADI-remap cycle
+// (single environment, plain FP64).
+//
+// Ten launches per cycle:
+//   k_cyc_lagrange_nodes      nodes: force from the previous corner vectors, velocity, BCs
+//   k_cyc_lagrange_cells      cells: corner vectors, volume, length, density, viscosity, energy,
+//                             remap variables U, and the geometry of each cell's low faces
+//   3 x sweep, cells         face gradients, limited cell gradients, upwind face values,
+//                             fluxes and U update (1D stencil along d); the last one also
+//                             finalises the cell state (remapVariables + EOS)
+//   3 x sweep, nodes         dual mass fluxes, limited nodal gradients, upwind momentum and
+//                             kinetic-energy update; the last one also gives the node
+//                             velocity and mass
+//   k_dt_min, k_dt_finish     CFL reduction and the new dt
+//
+// Every expression keeps the operation order of the reference (see the
+// citations), so with --fmad=false the results equal the CPU oracle bit for bit.
+#include "mhy_kernels.cuh"
+
+namespace mhy {
+
+// ------------------------------------------------------------------------
+// Lagrange phase, nodes: SaveValuesAtN (v_n = v, x = x0), UpdateVelocity,
+// ApplyBoundaryCondition (MahycoModule.cc:308-450, 589-665, 936-1004).
+__global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ cqs,
+    const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
+    double* __restrict__ vh) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i > dm.nx) return;
+  const long long n = dm.nid(i, j, k);
+  const double dtv = 0.5 * (S->old_dt + S->dt);
+  const int loc[2][2][2] = {{{0, 4}, {3, 7}}, {{1, 5}, {2, 6}}};
+  D3 F = d3(0, 0, 0);
+#pragma unroll
+  for (int dk = 1; dk >= 0; --dk)
+#pragma unroll
+    for (int dj = 1; dj >= 0; --dj)
+#pragma unroll
+      for (int di = 1; di >= 0; --di) {
+        const int ci = i - di, cj = j - dj, ck = k - dk;
+        if (ci < 0 || cj < 0 || ck < 0 || ci >= dm.nx || cj >= dm.ny || ck >= dm.nz) continue;
+        const long long c = dm.cid(ci, cj, ck);
+        const int l = loc[di][dj][dk];
+        const double pq = p[c] + q[c];
+        F = F + pq * d3(cqs[(l * 3 + 0) * dm.C + c], cqs[(l * 3 + 1) * dm.C + c], cqs[(l * 3 + 2) * dm.C + c]);
+      }
+  const double s = dtv / nm[n];
+  D3 u = d3(v[n], v[dm.N + n], v[2 * dm.N + n]) + s * F;
+  const unsigned mask = bcmask[n];
+  if (mask)
+    for (int b = 0; b < bct.nb; ++b)
+      if (mask >> b & 1u) {
+        if (bct.type[b] == 0) u.x = bct.value[b];
+        else if (bct.type[b] == 1) u.y = bct.value[b];
+        else u.z = bct.value[b];
+      }
+  vh[n] = u.x; vh[dm.N + n] = u.y; vh[2 * dm.N + n] = u.z;
+}
+
+// ------------------------------------------------------------------------
+// Lagrange phase, cells: UpdatePosition (cell centre), ComputeGeometricValues,
+// UpdateDensity, ComputeArtificialViscosity, UpdateEnergyAndPressure (GP),
+// computeVariablesForRemap_PBorn0 and computeFaceQuantitesForRemap for the
+// cell's low faces, with the face-only terms of computeGradPhiFace and the
+// upwind reconstruction precomputed (dx_f, (x_f - x_c).n0 for both cells).
+// (MahycoModule.cc:913-928, 1054-1262, 1331-1370, 517-528, 1715-1726;
+// PrepareRemap.cc:33-55, 93-117, 311-332; RemapADIService.cc:171-172, 710.)
+__device__ __forceinline__ D3 load_xl(const Dims& dm, const double* __restrict__ x0, const double* __restrict__ vh,
+                                      double dt, long long n) {
+  return d3(x0[n], x0[dm.N + n], x0[2 * dm.N + n]) + dt * d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
+}
+
+// Half cross product 0.5 * (a - c) x (b - c) (MahycoModule.cc:2206-2239).
+__device__ __forceinline__ D3 half_cross(D3 a, D3 b, D3 c) { return 0.5 * cross(a - c, b - c); }
+
+// Corner vectors accumulated face by face.  Each corner's two six-term sums
+// of MahycoModule.cc:2242-2257 take two consecutive terms from each of its
+// three faces, in increasing face order, so adding them as the faces are
+// visited keeps the reference's order; a corner is finished as soon as its
+// third face is done.
+struct CornerAcc { D3 s1, s2; };
+__device__ __forceinline__ void acc_start(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) { a.s1 = t1 + t2; a.s2 = u1 + u2; }
+__device__ __forceinline__ void acc_add(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) {
+  a.s1 = a.s1 + t1; a.s1 = a.s1 + t2; a.s2 = a.s2 + u1; a.s2 = a.s2 + u2;
+}
+
+__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Scalars* __restrict__ S, Phys ph,
+    const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
+    const double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
+    const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
+    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= dm.nx) return;
+  const long long c = dm.cid(i, j, k);
+  const long long C = dm.C;
+  const double dt = S->dt;
+  D3 x[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    x[a] = load_xl(dm, x0, vh, dt, dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]));
+  D3 sm = d3(0., 0., 0.);
+#pragma unroll
+  for (int a = 0; a < 8; ++a) sm = sm + x[a];
+  const D3 xc = .125 * sm;
+  xcs[c] = xc.x; xcs[C + c] = xc.y; xcs[2 * C + c] = xc.z;
+
+  // corner vectors, face by face (face centres as in MahycoModule.cc:1080-1087)
+  const double t12 = 1. / 12.;
+  double dv[8];
+  auto finish = [&](int a, const CornerAcc& ac) {
+    const D3 o = t12 * (5. * ac.s1 + ac.s2);
+    cqs[(a * 3 + 0) * C + c] = o.x; cqs[(a * 3 + 1) * C + c] = o.y; cqs[(a * 3 + 2) * C + c] = o.z;
+    dv[a] = dot(x[a], o);
+  };
+  CornerAcc k0, k1, k2, k3, k4, k5, k6, k7;
+  {
+    const D3 c0 = 0.25 * (x[0] + x[3] + x[2] + x[1]);
+    const D3 n04 = half_cross(x[0], x[3], c0), n03 = half_cross(x[3], x[2], c0);
+    const D3 n02 = half_cross(x[2], x[1], c0), n01 = half_cross(x[1], x[0], c0);
+    acc_start(k0, n01, n04, n02, n03);
+    acc_start(k1, n01, n02, n04, n03);
+    acc_start(k2, n02, n03, n01, n04);
+    acc_start(k3, n03, n04, n01, n02);
+  }
+  {
+    const D3 c1 = 0.25 * (x[0] + x[4] + x[7] + x[3]);
+    const D3 n05 = half_cross(x[0], x[4], c1), n12 = half_cross(x[4], x[7], c1);
+    const D3 n08 = half_cross(x[7], x[3], c1), n04 = half_cross(x[3], x[0], c1);
+    acc_add(k0, n04, n05, n08, n12);
+    acc_add(k3, n08, n04, n05, n12);
+    acc_start(k4, n05, n12, n08, n04);
+    acc_start(k7, n08, n12, n04, n05);
+  }
+  {
+    const D3 c2 = 0.25 * (x[0] + x[1] + x[5] + x[4]);
+    const D3 n01 = half_cross(x[0], x[1], c2), n06 = half_cross(x[1], x[5], c2);
+    const D3 n09 = half_cross(x[5], x[4], c2), n05 = half_cross(x[4], x[0], c2);
+    acc_add(k0, n05, n01, n06, n09);
+    finish(0, k0);
+    acc_add(k1, n01, n06, n09, n05);
+    acc_add(k4, n05, n09, n01, n06);
+    acc_start(k5, n06, n09, n01, n05);
+  }
+  {
+    const D3 c3 = 0.25 * (x[4] + x[5] + x[6] + x[7]);
+    const D3 n09 = half_cross(x[4], x[5], c3), n10 = half_cross(x[5], x[6], c3);
+    const D3 n11 = half_cross(x[6], x[7], c3), n12 = half_cross(x[7], x[4], c3);
+    acc_add(k4, n09, n12, n10, n11);
+    finish(4, k4);
+    acc_add(k5, n09, n10, n12, n11);
+    acc_start(k6, n11, n10, n12, n09);
+    acc_add(k7, n12, n11, n09, n10);
+  }
+  {
+    const D3 c4 = 0.25 * (x[1] + x[2] + x[6] + x[5]);
+    const D3 n02 = half_cross(x[1], x[2], c4), n07 = half_cross(x[2], x[6], c4);
+    const D3 n10 = half_cross(x[6], x[5], c4), n06 = half_cross(x[5], x[1], c4);
+    acc_add(k1, n06, n02, n10, n07);
+    finish(1, k1);
+    acc_add(k2, n07, n02, n06, n10);
+    acc_add(k5, n10, n06, n07, n02);
+    finish(5, k5);
+    acc_add(k6, n10, n07, n06, n02);
+  }
+  {
+    const D3 c5 = 0.25 * (x[2] + x[3] + x[7] + x[6]);
+    const D3 n03 = half_cross(x[2], x[3], c5), n08 = half_cross(x[3], x[7], c5);
+    const D3 n11 = half_cross(x[7], x[6], c5), n07 = half_cross(x[6], x[2], c5);
+    acc_add(k2, n07, n03, n11, n08);
+    finish(2, k2);
+    acc_add(k3, n08, n03, n07, n11);
+    finish(3, k3);
+    acc_add(k6, n07, n11, n03, n08);
+    finish(6, k6);
+    acc_add(k7, n11, n08, n07, n03);
+    finish(7, k7);
+  }
+  double V = 0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) V += dv[a];
+  V *= 1. / 3;
+  double Lc;
+  if (ph.lc_mode == 0) Lc = pow_third(V);
+  else {
+    D3 fc[6];
+    face_centres(x, fc);
+    const double d1 = norm2(fc[0] - fc[3]), d2 = norm2(fc[2] - fc[5]), d3_ = norm2(fc[1] - fc[4]);
+    Lc = (d1 * d2 * d3_) / (d1 * d2 + d1 * d3_ + d2 * d3_);
+  }
+  L[c] = Lc;
+  {
+    const double inv_deltat = 1.0 / dt;
+    const double rn = rho[c];
+    const double nd = mass[c] / V;
+    const double tau = 0.5 * (1.0 / rn + 1.0 / nd);
+    const double du = inv_deltat * (1.0 / nd - 1.0 / rn) / tau;
+    double qn = 0.;
+    const double g = ph.gamma;
+    if (du < 0.0) qn = 1. / tau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
+    const double en = compute_eint(ph.pseudo_centree != 0, g, q[c], qn, rn, nd, p[c], e[c]);
+    U[c] = V;
+    U[C + c] = V * nd;
+    U[2 * C + c] = V * nd * en;
+    U[3 * C + c] = V * qn;
+  }
+  // Remap face data from this cell's nodes (PrepareRemap.cc:41-55, 105-117;
+  // RemapADIService.cc:710): for the low face of each direction (an inner
+  // face) |A| along d, u_f and (x_f - x_c).n0 with this cell as the next cell;
+  // for the high face (an inner face) (x_f - x_c).n0 with this cell as the
+  // previous one.  Face node order: X (0,3,7,4), Y (0,1,5,4), Z (0,1,2,3) low;
+  // X (1,2,6,5), Y (3,2,6,7), Z (4,5,6,7) high, in SN_trigo cell-node numbers.
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int id = d == 0 ? i : (d == 1 ? j : k);
+    const int lo[3][4] = {{0, 3, 7, 4}, {0, 1, 5, 4}, {0, 1, 2, 3}};
+    const int hi[3][4] = {{1, 2, 6, 5}, {3, 2, 6, 7}, {4, 5, 6, 7}};
+    const long long off = d == 0 ? 0 : (d == 1 ? dm.Fx : dm.Fx + dm.Fy);
+    if (id > 0) {
+      const long long f = dm.fid(d, i, j, k);
+      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
+      const D3 a0 = x[lo[d][0]], a1 = x[lo[d][1]], a2 = x[lo[d][2]], a3 = x[lo[d][3]];
+      D3 xf = d3(0., 0., 0.);
+      xf = xf + .25 * a0; xf = xf + .25 * a1; xf = xf + .25 * a2; xf = xf + .25 * a3;
+      D3 vs = d3(0., 0., 0.);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int a = lo[d][b];
+        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+        vs = vs + d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]);
+      }
+      const D3 cr = 0.5 * cross(a2 - a0, a3 - a1);
+      double A = fabs(comp(cr, d));
+      if (!(fabs(comp(nrm, d)) >= 1.0E-10)) A = 0.;   // RemapADIService.cc:925 filter: no flux
+      const long long t = f - off;
+      fd.A[d][t] = A;
+      fd.u[d][t] = dot(.25 * vs, nrm);
+      fd.df[d][t] = dot(xf - xc, nrm);
+    }
+    if (id + 1 < dm.ncd(d)) {
+      const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
+      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
+      D3 xf = d3(0., 0., 0.);
+      xf = xf + .25 * x[hi[d][0]]; xf = xf + .25 * x[hi[d][1]]; xf = xf + .25 * x[hi[d][2]]; xf = xf + .25 * x[hi[d][3]];
+      fd.db[d][f - off] = dot(xf - xc, nrm);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Directional sweeps.  The stencil of the remap runs along one direction d,
+// so each line of cells (or nodes) along d is independent.  Two layouts, both
+// without shared memory or block barriers:
+//  * d = y, z ("march"): a lane owns one line (lanes = consecutive x, so every
+//    load is coalesced) and walks a segment of kMarchLen items along d with a
+//    sliding window in registers; every intermediate is computed once per
+//    segment, the first two items of a segment re-read their predecessors;
+//  * d = x ("warp row"): a warp holds 32 consecutive items of a row, one per
+//    lane, exchanges neighbours with shuffles and updates the 28 inner ones.
+
+constexpr int kMarchLen = 32;   // items per segment along d
+constexpr int kMarchWarps = 4;  // warps per block of the march kernels
+constexpr int kRowUpd = 28;     // items updated per warp by the row kernels
+constexpr int kRowWarps = 8;    // warps per block of the row kernels
+
+// remapVariables "moy" kernel for a single-environment cell and the PerfectGas
+// EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
+// PrepareRemap.cc:553-559).
+__device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, const CellState& st, long long c,
+                                              const double u[4]) {
+  const double thr = ph.threshold;
+  const double U0 = u[0], U1 = u[1], U2 = u[2], U3 = u[3];
+  const double vol = st.Ve[c];
+  const double volt = 0. + U0, masset = 0. + U1;
+  const double unsurvolt = 1. / volt;
+  const double unsurvol = 1. / vol;
+  double fvol = U0 * unsurvolt;
+  if (fvol < thr) fvol = 0.;
+  const double somme_frac = 0. + fvol;
+  const double unsursomme_frac = 1. / somme_frac;
+  fvol = fvol * unsursomme_frac;
+  double mf = 1.;
+  if (masset != 0.) {
+    const double unsurmasset = 1. / masset;
+    mf = U1 * unsurmasset;
+    if (fvol < thr) mf = 0.;
+    const double fmasset = 0. + mf;
+    if (fmasset != 0.) { const double unsurfmasset = 1. / fmasset; mf = mf * unsurfmasset; }
+  } else {
+    atomicOr(&const_cast<Scalars*>(S)->status, MHY_STATUS_ZERO_MASS);
+  }
+  double de = 0.;
+  if (fvol > thr) { const double vn = U0 * vol * unsurvolt; de = U1 / vn; }
+  const double density_nplus1 = 0. + fvol * de;
+  const double cm = vol * density_nplus1;
+  double ee = 0.;
+  if (fvol > thr && U1 != 0.) ee = U2 / U1;
+  double energie = 0. + mf * ee;
+  const double pv = U3 * unsurvol;
+  const double pseudo = 0. + fvol * pv;
+  double r = de;
+  if (r < 0. || energie < 0.) { energie = 0.; r = 0.; }
+  const double g = ph.gamma;
+  const double pr = (g - 1.) * r * energie;
+  st.rho[c] = r;
+  st.e[c] = energie;
+  st.q[c] = pseudo;
+  st.mass[c] = mf * cm;
+  st.p[c] = pr;
+  st.cs[c] = sqrt(g * pr / r);
+}
+
+// computeUremap_PBorn0 for one cell (RemapADIService.cc:909-987): fluxes
+// o*u*A*dt*Phi_f through the back and front faces along d, U -= sum, dual mass
+// flux sum 0.5*flux*o, clamping of mass and energy.  The boundary faces of d
+// carry Phi_f = 0 and contribute nothing.
+template <bool LAST>
+__device__ __forceinline__ void update_cell(const Phys& ph, const Scalars* S, const CellState& st, long long c,
+                                            double dt, bool inb, double ob, double ub, double Ab, const double Pfb[4],
+                                            bool inf, double of, double uf, double Af, const double Pff[4],
+                                            const double Uold[4], double* __restrict__ Uout, double* __restrict__ dpf,
+                                            long long C) {
+  const double cb = inb ? ob * ub * Ab * dt : 0.;
+  const double cf = inf ? of * uf * Af * dt : 0.;
+  double u[4], dpm = 0.;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double flux_face = 0., dp = 0.;
+    if (inb) { const double fl = cb * Pfb[v]; flux_face += fl; dp += 0.5 * fl * ob; }
+    if (inf) { const double fl = cf * Pff[v]; flux_face += fl; dp += 0.5 * fl * of; }
+    u[v] = Uold[v] - flux_face;
+    if (v == 1) dpm = dp;
+  }
+  if (u[1] < 0.) u[1] = 0.;
+  if (u[2] < 0.) u[2] = 0.;
+  dpf[c] = dpm;
+  if (!LAST) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Uout[v * C + c] = u[v];
+  } else {
+    finalize_cell(ph, S, st, c, u);
+  }
+}
+
+// Phi = U / sum of the environment volumes = U / U0 for one environment
+// (RemapADIService.cc:962-970, PrepareRemap.cc:394-398); Phi0 = U0/U0 = 1.
+__device__ __forceinline__ void phi_of(const double U[4], double P[4]) {
+  const double U0 = U[0];
+  P[0] = 1.0;
+  P[1] = U[1] / U0; P[2] = U[2] / U0; P[3] = U[3] / U0;
+}
+
+// Face gradients (R:174-177) of variables 1..3; variable 0 is zero.
+__device__ __forceinline__ void face_grad(bool inner, double dx, const double Pn[4], const double Pp[4], double g[4]) {
+  g[0] = 0.;
+#pragma unroll
+  for (int v = 1; v < 4; ++v) g[v] = inner ? (Pn[v] - Pp[v]) / dx : 0.;
+}
+
+// Limited cell gradient from the back and front face gradients (R:497-506):
+//   gc = 0; if (gb != 0) gc += 0.5*(phi(gf/gb)*gb); if (gf != 0) gc += 0.5*(phi(gb/gf)*gf).
+// For minmod, phi(r) = max(0, min(1, r)): with finite gb, gf of opposite signs or
+// a zero the two terms are signed zeros and gc = +0; with equal signs the ratio
+// whose numerator is the smaller magnitude is the only one below 1, the other
+// term is exactly 0.5*g.  So one division gives the reference's bits.
+__device__ __forceinline__ double limited_one(int lim, double gb, double gf) {
+  if (lim == 0) {
+    if (gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.))) return 0.;
+    const bool fsmall = fabs(gf) < fabs(gb);
+    const double r = fsmall ? gf / gb : gb / gf;
+    const double t1 = fsmall ? 0.5 * (r * gb) : 0.5 * (1.0 * gb);
+    const double t2 = fsmall ? 0.5 * (1.0 * gf) : 0.5 * (r * gf);
+    return (0. + t1) + t2;
+  }
+  double gc = 0.;
+  if (gb != 0.) gc += 0.5 * (limiter(lim, gf / gb) * gb);
+  if (gf != 0.) gc += 0.5 * (limiter(lim, gb / gf) * gf);
+  return gc;
+}
+
+// Variable 0 (the volume) has Phi = U0/U0 = 1 on every cell of a
+// single-environment mesh, so its face gradients are zero and its limited
+// gradient is +0; only variables 1..3 are computed.
+__device__ __forceinline__ void limited_grad(int lim, const double gb[4], const double gf[4], double G[4]) {
+  G[0] = 0.;
+#pragma unroll
+  for (int v = 1; v < 4; ++v) G[v] = limited_one(lim, gb[v], gf[v]);
+}
+
+// Upwind face value (R:707-714): from the previous cell when u_f dx_f > 0.
+__device__ __forceinline__ void face_value(double order2, double u, double dx, double db, double df,
+                                           const double Pp[4], const double Gp[4], const double Pn[4],
+                                           const double Gn[4], double Pf[4]) {
+  const bool back = u * dx > 0.0;
+  const double dot_xf = back ? db : df;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) Pf[v] = back ? (Pp[v] + order2 * dot_xf * Gp[v]) : (Pn[v] + order2 * dot_xf * Gn[v]);
+}
+
+// ---- cells, d = y or z: march --------------------------------------------
+template <int D, bool LAST>
+__global__ void __launch_bounds__(32 * kMarchWarps) k_cyc_sweep_cells_march(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
+  const int t2 = blockIdx.z;                          // k for d = y, j for d = z
+  const int nd = dm.ncd(D);
+  const int a = (blockIdx.y * kMarchWarps + warp) * kMarchLen;
+  if (i >= dm.nx || a >= nd) return;
+  const int b = min(a + kMarchLen, nd);
+  const long long C = dm.C;
+  const double* __restrict__ fdb = fd.db[D];
+  const double* __restrict__ fdf = fd.df[D];
+  const double* __restrict__ fA = fd.A[D];
+  const double* __restrict__ fu = fd.u[D];
+  const long long foff = D == 1 ? dm.Fx : dm.Fx + dm.Fy;
+  auto cid = [&](int s) -> long long {
+    return D == 1 ? i + (long long)dm.nx * (s + (long long)dm.ny * t2) : i + (long long)dm.nx * (t2 + (long long)dm.ny * s);
+  };
+  auto ftid = [&](int q) -> long long {   // low face of cell q, index within direction d
+    return D == 1 ? i + (long long)dm.nx * (q + (long long)(dm.ny + 1) * t2) : i + (long long)dm.nx * (t2 + (long long)dm.ny * q);
+  };
+  const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;
+  const double order2 = (double)(ph.ordre_projection - 1);
+  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  const double dt = S->dt;
+  auto inner = [&](int q) { return q >= 1 && q <= nd - 1; };
+  // raw data of item s: U and cell centre of cell s; n0, db, df, u, A of its low face
+  struct Raw { double U[4], xc[3], n[3], db, df, u, A; };
+  auto fetch = [&](int s, Raw& r) {
+    if (s >= 0 && s < nd) {
+      const long long c = cid(s);
+      r.U[0] = Uin[c]; r.U[1] = Uin[C + c]; r.U[2] = Uin[2 * C + c]; r.U[3] = Uin[3 * C + c];
+      r.xc[0] = xcs[c]; r.xc[1] = xcs[C + c]; r.xc[2] = xcs[2 * C + c];
+    } else {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) r.U[v] = 0.;
+      r.xc[0] = r.xc[1] = r.xc[2] = 0.;
+    }
+    if (inner(s)) {
+      const long long t = ftid(s), f = foff + t;
+      r.n[0] = n0[f]; r.n[1] = n0[dm.F + f]; r.n[2] = n0[2 * dm.F + f];
+      r.db = fdb[t]; r.df = fdf[t]; r.u = fu[t]; r.A = fA[t];
+    } else {
+      r.n[0] = r.n[1] = r.n[2] = 0.; r.db = r.df = r.u = r.A = 0.;
+    }
+  };
+  auto phis = [&](int s, const Raw& r, double P[4]) {
+    if (s >= 0 && s < nd) phi_of(r.U, P);
+    else {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) P[v] = 0.;
+    }
+  };
+  // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172)
+  auto dxf = [&](const Raw& next, const double xp[3]) {
+    return dot(d3(next.xc[0], next.xc[1], next.xc[2]) - d3(xp[0], xp[1], xp[2]), d3(next.n[0], next.n[1], next.n[2]));
+  };
+
+  // prologue: items a-2 .. a+1
+  Raw rm2, rm1, ra, rb;
+  fetch(a - 2, rm2); fetch(a - 1, rm1); fetch(a, ra); fetch(a + 1, rb);
+  double Pm2[4], Pm1[4], Pa[4], Pb[4], Ua[4], Ub[4];
+  phis(a - 2, rm2, Pm2); phis(a - 1, rm1, Pm1); phis(a, ra, Pa); phis(a + 1, rb, Pb);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) { Ua[v] = ra.U[v]; Ub[v] = rb.U[v]; }
+  const double dxm1 = inner(a - 1) ? dxf(rm1, rm2.xc) : 0.;
+  const double dxA = inner(a) ? dxf(ra, rm1.xc) : 0.;
+  double dxB = inner(a + 1) ? dxf(rb, ra.xc) : 0.;
+  double uA = ra.u, AA = ra.A, dbB = rb.db, dfB = rb.df, uB = rb.u, AB = rb.A;
+  double xB[3] = {rb.xc[0], rb.xc[1], rb.xc[2]};
+  double gm1[4], gA[4], gB[4];
+  face_grad(inner(a - 1), dxm1, Pm1, Pm2, gm1);
+  face_grad(inner(a), dxA, Pa, Pm1, gA);
+  face_grad(inner(a + 1), dxB, Pb, Pa, gB);
+  double Gm1[4], Ga[4], PfA[4];
+  limited_grad(lim, gm1, gA, Gm1);
+  limited_grad(lim, gA, gB, Ga);
+  if (inner(a)) face_value(order2, uA, dxA, ra.db, ra.df, Pm1, Gm1, Pa, Ga, PfA);
+  else {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) PfA[v] = 0.;
+  }
+
+  Raw nx;
+  double nob = 0., nof = 0.;
+  auto fetch_next = [&](int s) {   // item s+2 and the outer normals of cell s
+    fetch(s + 2, nx);
+    if (s < nd) { const long long c0 = cid(s); nob = ofn[lb * C + c0]; nof = ofn[lf * C + c0]; }
+  };
+  fetch_next(a);
+  for (int s = a; s < b; ++s) {
+    const Raw rc = nx;
+    const double ob = nob, of = nof;
+    if (s + 1 < b) fetch_next(s + 1);
+    const bool ic = inner(s + 2);
+    double Pc[4];
+    phis(s + 2, rc, Pc);
+    const double dxC = ic ? dxf(rc, xB) : 0.;
+    const long long c = cid(s);
+    double gC[4], Gb[4], PfB[4];
+    face_grad(ic, dxC, Pc, Pb, gC);
+    limited_grad(lim, gB, gC, Gb);
+    const bool ib = inner(s + 1);
+    if (ib) face_value(order2, uB, dxB, dbB, dfB, Pa, Ga, Pb, Gb, PfB);
+    else {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) PfB[v] = 0.;
+    }
+    update_cell<LAST>(ph, S, st, c, dt, inner(s), ob, uA, AA, PfA, ib, of, uB, AB, PfB, Ua, Uout, dpf, C);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      Ua[v] = Ub[v]; Ub[v] = rc.U[v]; Pa[v] = Pb[v]; Pb[v] = Pc[v]; Ga[v] = Gb[v]; gB[v] = gC[v]; PfA[v] = PfB[v];
+    }
+    uA = uB; AA = AB;
+    dxB = dxC; dbB = rc.db; dfB = rc.df; uB = rc.u; AB = rc.A;
+    xB[0] = rc.xc[0]; xB[1] = rc.xc[1]; xB[2] = rc.xc[2];
+  }
+}
+
+// ---- cells, d = x: warp row ----------------------------------------------
+template <bool LAST>
+__global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_cells_row(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st) {
+  const int lane = threadIdx.x & 31;
+  const int jr = blockIdx.y * kRowWarps + (threadIdx.x >> 5), kr = blockIdx.z;
+  if (jr >= dm.ny) return;                           // whole warp leaves together
+  const long long row = jr + (long long)dm.ny * kr;
+  const int s = blockIdx.x * kRowUpd - 2 + lane;     // x index of this lane's cell
+  const int nd = dm.nx;
+  const bool valid = s >= 0 && s < nd;
+  const bool inner = s >= 1 && s <= nd - 1;          // this lane's low face
+  const long long C = dm.C;
+  const long long c = row * dm.nx + s;               // cell id (row = j + ny k)
+  const long long t = row * (dm.nx + 1) + s;         // x-face id of the low face
+  const double order2 = (double)(ph.ordre_projection - 1);
+  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  double U[4] = {0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.};
+  if (valid) {
+    U[0] = Uin[c]; U[1] = Uin[C + c]; U[2] = Uin[2 * C + c]; U[3] = Uin[3 * C + c];
+    phi_of(U, P);
+  }
+  const unsigned full = 0xffffffffu;
+  double xc[3] = {0., 0., 0.};
+  if (valid) { xc[0] = xcs[c]; xc[1] = xcs[C + c]; xc[2] = xcs[2 * C + c]; }
+  const double xpx = __shfl_up_sync(full, xc[0], 1), xpy = __shfl_up_sync(full, xc[1], 1),
+               xpz = __shfl_up_sync(full, xc[2], 1);
+  double dx = 0., db = 0., df = 0., u = 0., A = 0.;
+  if (inner) {
+    db = fd.db[0][t]; df = fd.df[0][t]; u = fd.u[0][t]; A = fd.A[0][t];
+    dx = dot(d3(xc[0], xc[1], xc[2]) - d3(xpx, xpy, xpz), d3(n0[t], n0[dm.F + t], n0[2 * dm.F + t]));
+  }
+  double g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) Pp[v] = __shfl_up_sync(full, P[v], 1);
+  face_grad(inner, dx, P, Pp, g);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
+  limited_grad(lim, g, gr, G);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
+  if (inner) face_value(order2, u, dx, db, df, Pp, Gp, P, G, Pf);
+  else {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Pf[v] = 0.;
+  }
+  double Pfn[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
+  const double un = __shfl_down_sync(full, u, 1), An = __shfl_down_sync(full, A, 1);
+  if (lane < 2 || lane >= 2 + kRowUpd || !valid) return;
+  const bool infr = s + 1 <= nd - 1;
+  const double ob = ofn[1 * C + c], of = ofn[4 * C + c];
+  update_cell<LAST>(ph, S, st, c, S->dt, inner, ob, u, A, Pf, infr, of, un, An, Pfn, U, Uout, dpf, C);
+}
+
+// ---- nodes ---------------------------------------------------------------
+// Dual update of one inner node (DualPhaseRemap.cc:382-521).
+__device__ __forceinline__ void dual_update(int D, double order2, double dt, double bfm, double ffm,
+                                            const double Pm[4], const double Pn[4], const double Pp[4],
+                                            const double Gm[3], const double Gn[3], const double Gp[3],
+                                            double xm, double xn, double xp, double ud[5]) {
+  const double u3 = ud[3] + (bfm - ffm);
+  const double pnd = Pn[D];
+  const double ufront = 0.5 * (pnd + pnd);                     // DualPhaseRemap.cc:391
+  const double sfront = (ufront > 0) ? 1.0 : -1.0;
+  const double uback = 0.5 * (Pm[D] + pnd);
+  const double sback = (uback > 0) ? 1.0 : -1.0;
+  const bool fup = ffm < 0., bup = bfm > 0.;
+  const double tf = sfront * (xp - xn) - dt * ufront;
+  const double tb = sback * (xn - xm) - dt * uback;
+  double out[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double gfa = c < 3 ? (fup ? Gp[c] : Gn[c]) : 0.;    // index 4 never set (DualPhaseRemap.cc:771)
+    const double gba = c < 3 ? (bup ? Gm[c] : Gn[c]) : 0.;
+    const double FV = (fup ? Pp[c] : Pn[c]) + order2 * (0.5 * gfa * tf);
+    const double BV = (bup ? Pm[c] : Pn[c]) + order2 * (0.5 * gba * tb);
+    out[c] = ud[c < 3 ? c : 4] + (bfm * BV - ffm * FV);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) if (fabs(out[c]) < 1.e-300) out[c] = 0.;
+  ud[0] = out[0]; ud[1] = out[1]; ud[2] = out[2]; ud[3] = u3; ud[4] = out[3];
+}
+
+// Limited nodal gradient (DualPhaseRemap.cc:736-777); the terms are
+// (0.5*phi(r))*g here, and the same single-division reading of minmod applies.
+__device__ __forceinline__ void dual_grad(int lim, const double Pm[4], const double Pn[4], const double Pp[4],
+                                          double xm, double xn, double xp, double G[3]) {
+  const double hf = xp - xn, hb = xn - xm;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double gf = (Pp[c] - Pn[c]) / hf;
+    const double gb = (Pn[c] - Pm[c]) / hb;
+    double g = 0.;
+    if (lim == 0) {
+      if (!(gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.)))) {
+        const bool fsmall = fabs(gf) < fabs(gb);
+        const double r = fsmall ? gf / gb : gb / gf;
+        const double t1 = fsmall ? 0.5 * r * gb : 0.5 * 1.0 * gb;
+        const double t2 = fsmall ? 0.5 * 1.0 * gf : 0.5 * r * gf;
+        g = (0. + t1) + t2;
+      }
+    } else {
+      if (gb != 0.) g += 0.5 * limiter(lim, gf / gb) * gb;
+      if (gf != 0.) g += 0.5 * limiter(lim, gb / gf) * gf;
+    }
+    G[c] = g;
+  }
+}
+
+// Node velocity and node mass at the end of the remap (RemapADIFinal.cc:660-672, 697-719).
+__device__ __forceinline__ void finalize_node(const Dims& dm, long long n, int i, int j, int k, const double ud[5],
+                                              const double* __restrict__ vh, const double* __restrict__ mass,
+                                              double* __restrict__ vout, double* __restrict__ nm_out) {
+  const double m = ud[3];
+  if (m != 0.) {
+    vout[n] = ud[0] / m; vout[dm.N + n] = ud[1] / m; vout[2 * dm.N + n] = ud[2] / m;
+  } else {
+    vout[n] = vh[n]; vout[dm.N + n] = vh[dm.N + n]; vout[2 * dm.N + n] = vh[2 * dm.N + n];
+  }
+  double sm = 0.;
+#pragma unroll
+  for (int dk = 1; dk >= 0; --dk)
+#pragma unroll
+    for (int dj = 1; dj >= 0; --dj)
+#pragma unroll
+      for (int di = 1; di >= 0; --di) {
+        const int ci = i - di, cj = j - dj, ck = k - dk;
+        if (ci < 0 || cj < 0 || ck < 0 || ci >= dm.nx || cj >= dm.ny || ck >= dm.nz) continue;
+        sm += mass[dm.cid(ci, cj, ck)];
+      }
+  nm_out[n] = .125 * sm;
+}
+
+// Sum of 0.25*dual mass flux over the 4 cells whose index along d is cd and
+// whose transverse indices are idx[d1]+s1, idx[d2]+s2 (s1, s2 in {-1, 0}),
+// in the order of DualPhaseRemap.cc:299-340.
+template <int D>
+__device__ __forceinline__ double flux4(const Dims& dm, const double* __restrict__ dpf, int cd, const int idx[3]) {
+  constexpr int d1 = (D + 1) % 3, d2 = (D + 2) % 3;
+  double f = 0.;
+  if (cd < 0 || cd >= dm.ncd(D)) return f;
+#pragma unroll
+  for (int s1 = -1; s1 <= 0; ++s1)
+#pragma unroll
+    for (int s2 = -1; s2 <= 0; ++s2) {
+      int ci[3] = {idx[0], idx[1], idx[2]};
+      ci[D] = cd; ci[d1] += s1; ci[d2] += s2;
+      if (ci[d1] >= 0 && ci[d1] < dm.ncd(d1) && ci[d2] >= 0 && ci[d2] < dm.ncd(d2))
+        f += 0.25 * dpf[dm.cid(ci[0], ci[1], ci[2])];
+    }
+  return f;
+}
+
+// Node state at the start of a sweep: U_dual and Phi_dual (PrepareRemap.cc:411-433
+// on the first sweep or for nodes not yet updated this cycle, else U_dual / m).
+template <bool FIRST>
+__device__ __forceinline__ void load_node(const Dims& dm, long long n, bool updated, const double* __restrict__ nm,
+                                          const double* __restrict__ vh, const double* __restrict__ udin,
+                                          double ud[5], double P[4]) {
+  const D3 u = d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
+  if (FIRST) {
+    const double m = nm[n];
+    const double un = norm2(u);
+    ud[0] = m * u.x; ud[1] = m * u.y; ud[2] = m * u.z; ud[3] = m; ud[4] = 0.5 * m * un;
+    P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
+  } else {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) ud[c] = udin[c * dm.N + n];
+    if (updated) {
+      const double m = ud[3];
+      P[0] = ud[0] / m; P[1] = ud[1] / m; P[2] = ud[2] / m; P[3] = ud[4] / m;
+    } else {
+      P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
+    }
+  }
+}
+
+// ---- nodes, d = y or z: march --------------------------------------------
+template <int D, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(32 * kMarchWarps) k_cyc_sweep_nodes_march(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
+  const int t2 = blockIdx.z;                          // k for d = y, j for d = z
+  const int nn = dm.ncd(D) + 1;
+  const int a = (blockIdx.y * kMarchWarps + warp) * kMarchLen;
+  if (i > dm.nx || a >= nn) return;
+  const int b = min(a + kMarchLen, nn);
+  const long long N = dm.N;
+  auto nid = [&](int m) -> long long {
+    return D == 1 ? i + (long long)(dm.nx + 1) * (m + (long long)(dm.ny + 1) * t2)
+                  : i + (long long)(dm.nx + 1) * (t2 + (long long)(dm.ny + 1) * m);
+  };
+  auto ijk = [&](int m, int idx[3]) { idx[0] = i; idx[D] = m; idx[D == 1 ? 2 : 1] = t2; };
+  const int ot = D == 1 ? 2 : 1;                      // the other transverse direction
+  const bool on_plane_t = i == 0 || i == dm.nx || t2 == 0 || t2 == dm.ncd(ot);
+  bool updated = false;                               // inner along an earlier direction of this cycle
+  if ((prev_inner & 1) && i > 0 && i < dm.nx) updated = true;
+  if ((prev_inner >> ot & 1) && t2 > 0 && t2 < dm.ncd(ot)) updated = true;
+  const double dt = S->dt;
+  const double order2 = (double)(ph.ordre_projection - 1);
+  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  const bool grad_on = ph.ordre_projection > 1;
+  auto inner = [&](int m) { return m >= 1 && m <= nn - 2; };
+  // raw data of node m: velocity, coordinate along d, U_dual (or node mass on the first sweep)
+  struct NRaw { double v[3], x0d, ud[5]; };
+  auto fetch = [&](int m, NRaw& r) {
+    if (m >= 0 && m < nn) {
+      const long long n = nid(m);
+      r.v[0] = vh[n]; r.v[1] = vh[N + n]; r.v[2] = vh[2 * N + n];
+      r.x0d = x0[D * N + n];
+      if (FIRST) { r.ud[3] = nm_in[n]; }
+      else {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) r.ud[c] = udin[c * N + n];
+      }
+    } else {
+      r.v[0] = r.v[1] = r.v[2] = 0.; r.x0d = 0.;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) r.ud[c] = 0.;
+    }
+  };
+  // U_dual and Phi_dual of node m from its raw data (PrepareRemap.cc:411-433, DualPhaseRemap.cc:515-521)
+  auto expand = [&](int m, const NRaw& r, double ud[5], double P[4], double& x) {
+    if (m >= 0 && m < nn) {
+      const D3 u = d3(r.v[0], r.v[1], r.v[2]);
+      if (FIRST) {
+        const double mm = r.ud[3];
+        const double un = norm2(u);
+        ud[0] = mm * u.x; ud[1] = mm * u.y; ud[2] = mm * u.z; ud[3] = mm; ud[4] = 0.5 * mm * un;
+        P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
+      } else {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) ud[c] = r.ud[c];
+        if (updated) {
+          const double mm = ud[3];
+          P[0] = ud[0] / mm; P[1] = ud[1] / mm; P[2] = ud[2] / mm; P[3] = ud[4] / mm;
+        } else {
+          P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
+        }
+      }
+      x = r.x0d + r.v[D] * dt;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) ud[c] = 0.;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) P[c] = 0.;
+      x = 0.;
+    }
+  };
+  auto stored_grad = [&](int m, double G[3]) {
+    const long long n = nid(m);
+    G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n];
+  };
+  // prologue: nodes a-2 .. a+1
+  double udA[5], udB[5], tmp5[5], Pm2[4], Pm1[4], PA[4], PB[4], xm2, xm1, xA, xB;
+  {
+    NRaw r0, r1, r2, r3;
+    fetch(a - 2, r0); fetch(a - 1, r1); fetch(a, r2); fetch(a + 1, r3);
+    expand(a - 2, r0, tmp5, Pm2, xm2);
+    expand(a - 1, r1, tmp5, Pm1, xm1);
+    expand(a, r2, udA, PA, xA);
+    expand(a + 1, r3, udB, PB, xB);
+  }
+  double Gm1[3] = {0., 0., 0.}, GA[3] = {0., 0., 0.};
+  if (a - 1 >= 0) {
+    if (inner(a - 1) && grad_on) dual_grad(lim, Pm2, Pm1, PA, xm2, xm1, xA, Gm1); else stored_grad(a - 1, Gm1);
+  }
+  if (inner(a) && grad_on) dual_grad(lim, Pm1, PA, PB, xm1, xA, xB, GA); else stored_grad(a, GA);
+  int idx[3];
+  ijk(a, idx);
+  double bfm = flux4<D>(dm, dpf, a - 1, idx);         // back cells of node a = front cells of node a-1
+
+  NRaw nx;
+  fetch(a + 2, nx);
+  for (int m = a; m < b; ++m) {
+    const NRaw rc = nx;
+    if (m + 1 < b) fetch(m + 3, nx);
+    double udC[5], PC[4], xC;
+    expand(m + 2, rc, udC, PC, xC);
+    double GB[3] = {0., 0., 0.};
+    if (m + 1 < nn) {
+      if (inner(m + 1) && grad_on) dual_grad(lim, PA, PB, PC, xA, xB, xC, GB); else stored_grad(m + 1, GB);
+    }
+    ijk(m, idx);
+    const double ffm = flux4<D>(dm, dpf, m, idx);
+    const long long n = nid(m);
+    if (inner(m)) {
+      if (on_plane_t && grad_on) { Gd[n] = GA[0]; Gd[N + n] = GA[1]; Gd[2 * N + n] = GA[2]; }
+      dual_update(D, order2, dt, bfm, ffm, Pm1, PA, PB, Gm1, GA, GB, xm1, xA, xB, udA);
+    }
+    if (!LAST) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) udout[c * N + n] = udA[c];
+    } else {
+      finalize_node(dm, n, idx[0], idx[1], idx[2], udA, vh, mass, vout, nm_out);
+    }
+    bfm = ffm;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) { Pm1[c] = PA[c]; PA[c] = PB[c]; PB[c] = PC[c]; }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) { udA[c] = udB[c]; udB[c] = udC[c]; }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { Gm1[c] = GA[c]; GA[c] = GB[c]; }
+    xm1 = xA; xA = xB; xB = xC;
+  }
+}
+
+// ---- nodes, d = x: warp row ----------------------------------------------
+template <bool FIRST, bool LAST>
+__global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_nodes_row(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out) {
+  const int lane = threadIdx.x & 31;
+  const int nn = dm.nx + 1;
+  const int j = blockIdx.y * kRowWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  if (j > dm.ny) return;                             // whole warp leaves together
+  const long long row = j + (long long)(dm.ny + 1) * k;
+  const int m = blockIdx.x * kRowUpd - 2 + lane;     // x index of this lane's node
+  const bool valid = m >= 0 && m < nn;
+  const bool inner = m >= 1 && m <= nn - 2;
+  const long long N = dm.N;
+  const long long n = row * nn + m;
+  bool updated = false;
+  if ((prev_inner >> 1 & 1) && j > 0 && j < dm.ny) updated = true;
+  if ((prev_inner >> 2 & 1) && k > 0 && k < dm.nz) updated = true;
+  const double dt = S->dt;
+  const double order2 = (double)(ph.ordre_projection - 1);
+  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  const bool grad_on = ph.ordre_projection > 1;
+  double ud[5] = {0., 0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, x = 0.;
+  if (valid) {
+    load_node<FIRST>(dm, n, updated, nm_in, vh, udin, ud, P);
+    x = x0[n] + vh[n] * dt;
+  }
+  const unsigned full = 0xffffffffu;
+  double Pm[4], Pp[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) { Pm[c] = __shfl_up_sync(full, P[c], 1); Pp[c] = __shfl_down_sync(full, P[c], 1); }
+  const double xm = __shfl_up_sync(full, x, 1), xp = __shfl_down_sync(full, x, 1);
+  double G[3] = {0., 0., 0.};
+  if (valid) {
+    if (inner && grad_on) dual_grad(lim, Pm, P, Pp, xm, x, xp, G);
+    else { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
+  }
+  double Gm[3], Gp[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) { Gm[c] = __shfl_up_sync(full, G[c], 1); Gp[c] = __shfl_down_sync(full, G[c], 1); }
+  const int idx[3] = {m, j, k};
+  const double ffm = valid ? flux4<0>(dm, dpf, m, idx) : 0.;
+  const double bfm = __shfl_up_sync(full, ffm, 1);     // back cells of node m = front cells of node m-1
+  if (lane < 2 || lane >= 2 + kRowUpd || !valid) return;
+  if (inner) {
+    const bool on_plane_t = j == 0 || j == dm.ny || k == 0 || k == dm.nz;
+    if (on_plane_t && grad_on) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
+    dual_update(0, order2, dt, bfm, ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
+  }
+  if (!LAST) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) udout[c * N + n] = ud[c];
+  } else {
+    finalize_node(dm, n, m, j, k, ud, vh, mass, vout, nm_out);
+  }
+}
+
+// ------------------------------------------------------------------------
+// Host-side launchers.
+template <int D>
+static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, double* Uout, cudaStream_t s) {
+  const Dims& dm = a.dm;
+  if constexpr (D == 0) {
+    const dim3 nb((dm.nx + kRowUpd - 1) / kRowUpd, (dm.ny + kRowWarps - 1) / kRowWarps, dm.nz);
+    if (last) k_cyc_sweep_cells_row<true><<<nb, 32 * kRowWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    else k_cyc_sweep_cells_row<false><<<nb, 32 * kRowWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  } else {
+  const int nd = dm.ncd(D);
+  const int nseg = (nd + kMarchLen - 1) / kMarchLen;
+  dim3 g((dm.nx + 31) / 32, (nseg + kMarchWarps - 1) / kMarchWarps, D == 1 ? dm.nz : dm.ny);
+  if (last) k_cyc_sweep_cells_march<D, true><<<g, 32 * kMarchWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  else k_cyc_sweep_cells_march<D, false><<<g, 32 * kMarchWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  }
+}
+
+template <int D, bool FIRST, bool LAST>
+static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
+  const Dims& dm = a.dm;
+  if constexpr (D == 0) {
+    const dim3 nb((dm.nx + 1 + kRowUpd - 1) / kRowUpd, (dm.ny + 1 + kRowWarps - 1) / kRowWarps, dm.nz + 1);
+    k_cyc_sweep_nodes_row<FIRST, LAST><<<nb, 32 * kRowWarps, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout,
+                                                                     a.dpf, a.Gd, a.st.mass, a.v, a.nm);
+  } else {
+  const int nn = dm.ncd(D) + 1;
+  const int nseg = (nn + kMarchLen - 1) / kMarchLen;
+  dim3 g((dm.nx + 1 + 31) / 32, (nseg + kMarchWarps - 1) / kMarchWarps, D == 1 ? dm.nz + 1 : dm.ny + 1);
+  k_cyc_sweep_nodes_march<D, FIRST, LAST><<<g, 32 * kMarchWarps, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin,
+                                                                       udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm);
+  }
+}
+
+template <int D>
+static void sweep_nodes_d(const CycleArgs& a, bool first, bool last, int prev, const double* udin, double* udout,
+                          cudaStream_t s) {
+  if (first) sweep_nodes_launch<D, true, false>(a, prev, udin, udout, s);
+  else if (last) sweep_nodes_launch<D, false, true>(a, prev, udin, udout, s);
+  else sweep_nodes_launch<D, false, false>(a, prev, udin, udout, s);
+}
+
+void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
+  const dim3 nbn((a.dm.nx + 1 + 127) / 128, a.dm.ny + 1, a.dm.nz + 1);
+  k_cyc_lagrange_nodes<<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh);
+}
+
+void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
+  const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
+  k_cyc_lagrange_cells<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
+                                           a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd);
+}
+
+// Three sweeps d = (i + sens) % 3 (RemapADIService.cc:28-30).  U: Lagrange
+// writes U[0]; sweeps read U[0] -> U[1] -> U[0] and the last one finalises.
+// U_dual: the first sweep builds it from the Lagrange velocity and writes
+// ud[0]; then ud[0] -> ud[1]; the last one writes the node velocity and mass.
+void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
+  int prev = 0;
+  for (int it = 0; it < 3; ++it) {
+    const int d = (it + sens) % 3;
+    const bool first = it == 0, last = it == 2;
+    const double* uin = a.U[it & 1];
+    double* uout = a.U[(it + 1) & 1];
+    const double* udin = a.ud[(it + 1) & 1];
+    double* udout = a.ud[it & 1];
+    if (d == 0) sweep_cells_d<0>(a, last, uin, uout, s);
+    else if (d == 1) sweep_cells_d<1>(a, last, uin, uout, s);
+    else sweep_cells_d<2>(a, last, uin, uout, s);
+    if (d == 0) sweep_nodes_d<0>(a, first, last, prev, udin, udout, s);
+    else if (d == 1) sweep_nodes_d<1>(a, first, last, prev, udin, udout, s);
+    else sweep_nodes_d<2>(a, first, last, prev, udin, udout, s);
+    prev |= 1 << d;
+  }
+}
+
+void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
+  const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
+  k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.v);
+  k_dt_finish<<<1, 1, 0, s>>>(a.S, a.ph);
+}
+
+}  // namespace mhy

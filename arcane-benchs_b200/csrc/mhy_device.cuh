@@ -104,7 +104,7 @@ struct Dims {
   long long C, N, F, Fx, Fy;
   __device__ __forceinline__ long long cid(int i, int j, int k) const { return i + (long long)nx * (j + (long long)ny * k); }
   __device__ __forceinline__ long long nid(int i, int j, int k) const { return i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k); }
-  __device__ __forceinline__ int ncd(int d) const { return d == 0 ? nx : (d == 1 ? ny : nz); }
+  __host__ __device__ __forceinline__ int ncd(int d) const { return d == 0 ? nx : (d == 1 ? ny : nz); }
   // face of direction d whose lowest node is (i,j,k)
   __device__ __forceinline__ long long fid(int d, int i, int j, int k) const {
     if (d == 0) return i + (long long)(nx + 1) * (j + (long long)ny * k);

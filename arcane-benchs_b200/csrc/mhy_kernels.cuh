@@ -31,36 +31,48 @@ struct BCTable {
   double value[MHY_MAX_BC];
 };
 
+// Per-cycle data of the inner faces of each direction d (index = face index
+// within direction d): (x_f - x_c(prev)).n0, (x_f - x_c(next)).n0, |A_f|
+// along d, normal velocity u_f.
+struct FaceData {
+  double* db[3];
+  double* df[3];
+  double* A[3];
+  double* u[3];
+};
+
+// Persistent cell state (global values of a single-environment mesh).
+struct CellState {
+  double *rho, *e, *q, *p, *cs, *mass;
+  const double* Ve;
+};
+
+struct CycleArgs {
+  Dims dm;
+  Scalars* S;
+  Phys ph;
+  BCTable bct;
+  const uint16_t* bcmask;
+  const double *x0, *n0, *ofn;
+  double *v, *vh, *nm, *cqs, *L, *dpf, *Gd, *xc;
+  double* U[2];
+  double* ud[2];
+  FaceData fd;
+  CellState st;
+};
+
+void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s);
+void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s);
+void launch_remap(const CycleArgs& a, int sens, cudaStream_t s);
+void launch_delta_t(const CycleArgs& a, cudaStream_t s);
+constexpr int kKernelsPerCycle = 10;
+
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);
 __global__ void k_init_faces(Dims dm, const double* x0, double* n0, double* xf0);
 __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* xf0, double* ofn);
 __global__ void k_init_state(Dims dm, double gamma, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
-__global__ void k_lagrange_nodes(Dims dm, const Scalars* S, const double* p, const double* q, const double* cqs,
-                                 const double* nm, const double* v, const double* x0, const uint16_t* bcmask,
-                                 BCTable bct, double* vh, double* xl, double* ud, double* phid);
-__global__ void k_lagrange_cells(Dims dm, const Scalars* S, Phys ph, const double* xl, const double* rho,
-                                 const double* e, const double* q, const double* p, const double* cs,
-                                 const double* mass, double* cqs, double* xc, double* L, double* U);
-__global__ void k_faces(Dims dm, const double* xl, const double* vh, const double* n0, double* A, double* uf,
-                        double* xf);
-__global__ void k_sweep_face_grad(Dims dm, int d, const double* xc, const double* n0, const double* U, double* dxf,
-                                  double* gf);
-__global__ void k_sweep_cell_grad(Dims dm, int d, int lim, const double* gf, double* G);
-__global__ void k_sweep_face_phi(Dims dm, int d, double order2, const double* xc, const double* n0,
-                                 const double* xf, const double* uf, const double* dxf, const double* U,
-                                 const double* G, double* phif);
-__global__ void k_sweep_cell_update(Dims dm, int d, const Scalars* S, const double* n0, const double* uf,
-                                    const double* A, const double* ofn, const double* phif, double* U, double* dpf);
-__global__ void k_sweep_dual_grad(Dims dm, int d, int lim, const double* xl, const double* phid, double* G);
-__global__ void k_sweep_dual_update(Dims dm, int d, const Scalars* S, double order2, const double* xl,
-                                    const double* dpf, const double* G, const double* phid, double* ud,
-                                    double* phid_out);
-__global__ void k_finalize_cells(Dims dm, Phys ph, Scalars* S, const double* U, const double* Ve, double* rho,
-                                 double* e, double* q, double* p, double* cs, double* mass);
-__global__ void k_finalize_nodes(Dims dm, const double* ud, const double* vh, const double* mass, double* v,
-                                 double* nm);
 __global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* v);
 __global__ void k_dt_finish(Scalars* S, Phys ph);
 
