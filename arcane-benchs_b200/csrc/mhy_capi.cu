@@ -49,7 +49,7 @@ struct mhy_ctx {
   std::vector<double> h_coords;
   std::vector<void*> allocs;
   // nodes
-  double *x0 = nullptr, *v = nullptr, *vh = nullptr, *nm = nullptr, *Gd = nullptr;
+  double *x0 = nullptr, *v = nullptr, *vh = nullptr, *nm = nullptr, *Gd = nullptr, *vnorm = nullptr;
   double *ud[2] = {nullptr, nullptr};
   uint16_t* bcmask = nullptr;
   // cells
@@ -80,7 +80,7 @@ struct mhy_ctx {
     CycleArgs a{};
     a.dm = dm; a.S = S; a.ph = ph; a.bct = bct; a.bcmask = bcmask;
     a.x0 = x0; a.n0 = n0; a.ofn = ofn;
-    a.v = v; a.vh = vh; a.nm = nm; a.cqs = cqs; a.L = L; a.dpf = dpf; a.Gd = Gd; a.xc = xc;
+    a.v = v; a.vh = vh; a.nm = nm; a.cqs = cqs; a.L = L; a.dpf = dpf; a.Gd = Gd; a.xc = xc; a.vnorm = vnorm;
     a.U[0] = U[0]; a.U[1] = U[1]; a.ud[0] = ud[0]; a.ud[1] = ud[1];
     a.fd = fd;
     a.st.rho = rho; a.st.e = e; a.st.q = q; a.st.p = p; a.st.cs = cs; a.st.mass = mass; a.st.Ve = Ve;
@@ -154,7 +154,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   int rc = MHY_OK;
   auto A_ = [&](double** pp, long long n) { if (rc == MHY_OK) rc = c->alloc(pp, (size_t)n); };
   const long long C = dm.C, N = dm.N, F = dm.F;
-  A_(&c->x0, 3 * N); A_(&c->v, 3 * N); A_(&c->vh, 3 * N); A_(&c->nm, N); A_(&c->Gd, 3 * N);
+  A_(&c->x0, 3 * N); A_(&c->v, 3 * N); A_(&c->vh, 3 * N); A_(&c->nm, N); A_(&c->Gd, 3 * N); A_(&c->vnorm, N);
   A_(&c->ud[0], 5 * N); A_(&c->ud[1], 5 * N);
   A_(&c->rho, C); A_(&c->e, C); A_(&c->q, C); A_(&c->p, C); A_(&c->cs, C); A_(&c->mass, C); A_(&c->L, C);
   A_(&c->Ve, C); A_(&c->dpf, C); A_(&c->xc, 3 * C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C); A_(&c->U[0], 4 * C); A_(&c->U[1], 4 * C);
@@ -223,7 +223,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   }
   Scalars s0{};
-  s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.min_bits = 0x7fefffffffffffffull;
+  s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.inv_dt = 1.0 / opt->deltat_init; s0.min_bits = 0x7fefffffffffffffull;
   err = cudaMemcpy(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   c->kernels_per_cycle = kKernelsPerCycle;

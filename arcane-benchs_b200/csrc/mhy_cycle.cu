@@ -190,15 +190,17 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Sc
   }
   L[c] = Lc;
   {
-    const double inv_deltat = 1.0 / dt;
+    const double inv_deltat = S->inv_dt;                        // 1.0 / dt
     const double rn = rho[c];
     const double nd = mass[c] / V;
-    const double tau = 0.5 * (1.0 / rn + 1.0 / nd);
-    const double du = inv_deltat * (1.0 / nd - 1.0 / rn) / tau;
+    const double irn = 1.0 / rn, ind = 1.0 / nd;
+    const double tau = 0.5 * (irn + ind);
+    const double itau = 1. / tau;
+    const double du = qdiv(inv_deltat * (ind - irn), tau, itau);
     double qn = 0.;
     const double g = ph.gamma;
-    if (du < 0.0) qn = 1. / tau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-    const double en = compute_eint(ph.pseudo_centree != 0, g, q[c], qn, rn, nd, p[c], e[c]);
+    if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
+    const double en = compute_eint(ph.pseudo_centree != 0, g, q[c], qn, ind, irn, nd, p[c], e[c]);
     U[c] = V;
     U[C + c] = V * nd;
     U[2 * C + c] = V * nd * en;
@@ -249,19 +251,16 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Sc
 
 // ------------------------------------------------------------------------
 // Directional sweeps.  The stencil of the remap runs along one direction d,
-// so each line of cells (or nodes) along d is independent.  Two layouts, both
-// without shared memory or block barriers:
-//  * d = y, z ("march"): a lane owns one line (lanes = consecutive x, so every
-//    load is coalesced) and walks a segment of kMarchLen items along d with a
-//    sliding window in registers; every intermediate is computed once per
-//    segment, the first two items of a segment re-read their predecessors;
-//  * d = x ("warp row"): a warp holds 32 consecutive items of a row, one per
-//    lane, exchanges neighbours with shuffles and updates the 28 inner ones.
+// so each line of cells (or nodes) along d is independent.  A warp holds 32
+// consecutive items of one line, one per lane, exchanges neighbours with
+// shuffles (no shared memory, no block barrier) and updates the 28 inner ones.
+// For d = x the warps of a block are 8 neighbouring lines (rows) and every
+// load is coalesced; for d = y, z the warps of a block are the lines of 8
+// consecutive x, so the 8 warps together use each 64-byte span they touch
+// (through L1).
 
-constexpr int kMarchLen = 32;   // items per segment along d
-constexpr int kMarchWarps = 4;  // warps per block of the march kernels
-constexpr int kRowUpd = 28;     // items updated per warp by the row kernels
-constexpr int kRowWarps = 8;    // warps per block of the row kernels
+constexpr int kLineUpd = 28;    // items updated per warp (32 lanes, 2 halo lanes on each side)
+constexpr int kLineWarps = 8;   // warps (lines) per block
 
 // remapVariables "moy" kernel for a single-environment cell and the PerfectGas
 // EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
@@ -294,7 +293,7 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
   const double density_nplus1 = 0. + fvol * de;
   const double cm = vol * density_nplus1;
   double ee = 0.;
-  if (fvol > thr && U1 != 0.) ee = U2 / U1;
+  if (fvol > thr && U1 != 0.) ee = qdiv(U2, U1, 1. / masset);   // masset = 0 + U1 = U1
   double energie = 0. + mf * ee;
   const double pv = U3 * unsurvol;
   const double pseudo = 0. + fvol * pv;
@@ -345,16 +344,17 @@ __device__ __forceinline__ void update_cell(const Phys& ph, const Scalars* S, co
 // Phi = U / sum of the environment volumes = U / U0 for one environment
 // (RemapADIService.cc:962-970, PrepareRemap.cc:394-398); Phi0 = U0/U0 = 1.
 __device__ __forceinline__ void phi_of(const double U[4], double P[4]) {
-  const double U0 = U[0];
+  const double U0 = U[0], r = 1.0 / U0;
   P[0] = 1.0;
-  P[1] = U[1] / U0; P[2] = U[2] / U0; P[3] = U[3] / U0;
+  P[1] = qdiv(U[1], U0, r); P[2] = qdiv(U[2], U0, r); P[3] = qdiv(U[3], U0, r);
 }
 
 // Face gradients (R:174-177) of variables 1..3; variable 0 is zero.
 __device__ __forceinline__ void face_grad(bool inner, double dx, const double Pn[4], const double Pp[4], double g[4]) {
   g[0] = 0.;
+  const double r = inner ? 1.0 / dx : 0.;
 #pragma unroll
-  for (int v = 1; v < 4; ++v) g[v] = inner ? (Pn[v] - Pp[v]) / dx : 0.;
+  for (int v = 1; v < 4; ++v) g[v] = inner ? qdiv(Pn[v] - Pp[v], dx, r) : 0.;
 }
 
 // Limited cell gradient from the back and front face gradients (R:497-506):
@@ -397,163 +397,63 @@ __device__ __forceinline__ void face_value(double order2, double u, double dx, d
   for (int v = 0; v < 4; ++v) Pf[v] = back ? (Pp[v] + order2 * dot_xf * Gp[v]) : (Pn[v] + order2 * dot_xf * Gn[v]);
 }
 
-// ---- cells, d = y or z: march --------------------------------------------
+// Index map of a line of cells along D for the warp w of the block.
+template <int D>
+struct CellLine {
+  int i, j, k;          // coordinates of the line (the D one is replaced by the position)
+  bool ok;
+  __device__ CellLine(const Dims& dm, int w) {
+    if (D == 0) { i = 0; j = blockIdx.y * kLineWarps + w; k = blockIdx.z; ok = j < dm.ny; }
+    else if (D == 1) { i = blockIdx.x * kLineWarps + w; j = 0; k = blockIdx.z; ok = i < dm.nx; }
+    else { i = blockIdx.x * kLineWarps + w; j = blockIdx.z; k = 0; ok = i < dm.nx; }
+  }
+  __device__ long long cell(const Dims& dm, int s) const {
+    return D == 0 ? dm.cid(s, j, k) : (D == 1 ? dm.cid(i, s, k) : dm.cid(i, j, s));
+  }
+  // index of the low face of the cell at position s, within direction D
+  __device__ long long face(const Dims& dm, int s) const {
+    if (D == 0) return s + (long long)(dm.nx + 1) * (j + (long long)dm.ny * k);
+    if (D == 1) return i + (long long)dm.nx * (s + (long long)(dm.ny + 1) * k);
+    return i + (long long)dm.nx * (j + (long long)dm.ny * s);
+  }
+  __device__ static int seg0() { return (D == 0 ? blockIdx.x : blockIdx.y) * kLineUpd; }
+};
+
+// ---- cells ---------------------------------------------------------------
 template <int D, bool LAST>
-__global__ void __launch_bounds__(32 * kMarchWarps) k_cyc_sweep_cells_march(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
-    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
-    double* __restrict__ dpf, CellState st) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int i = blockIdx.x * 32 + lane;
-  const int t2 = blockIdx.z;                          // k for d = y, j for d = z
-  const int nd = dm.ncd(D);
-  const int a = (blockIdx.y * kMarchWarps + warp) * kMarchLen;
-  if (i >= dm.nx || a >= nd) return;
-  const int b = min(a + kMarchLen, nd);
-  const long long C = dm.C;
-  const double* __restrict__ fdb = fd.db[D];
-  const double* __restrict__ fdf = fd.df[D];
-  const double* __restrict__ fA = fd.A[D];
-  const double* __restrict__ fu = fd.u[D];
-  const long long foff = D == 1 ? dm.Fx : dm.Fx + dm.Fy;
-  auto cid = [&](int s) -> long long {
-    return D == 1 ? i + (long long)dm.nx * (s + (long long)dm.ny * t2) : i + (long long)dm.nx * (t2 + (long long)dm.ny * s);
-  };
-  auto ftid = [&](int q) -> long long {   // low face of cell q, index within direction d
-    return D == 1 ? i + (long long)dm.nx * (q + (long long)(dm.ny + 1) * t2) : i + (long long)dm.nx * (t2 + (long long)dm.ny * q);
-  };
-  const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;
-  const double order2 = (double)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  const double dt = S->dt;
-  auto inner = [&](int q) { return q >= 1 && q <= nd - 1; };
-  // raw data of item s: U and cell centre of cell s; n0, db, df, u, A of its low face
-  struct Raw { double U[4], xc[3], n[3], db, df, u, A; };
-  auto fetch = [&](int s, Raw& r) {
-    if (s >= 0 && s < nd) {
-      const long long c = cid(s);
-      r.U[0] = Uin[c]; r.U[1] = Uin[C + c]; r.U[2] = Uin[2 * C + c]; r.U[3] = Uin[3 * C + c];
-      r.xc[0] = xcs[c]; r.xc[1] = xcs[C + c]; r.xc[2] = xcs[2 * C + c];
-    } else {
-#pragma unroll
-      for (int v = 0; v < 4; ++v) r.U[v] = 0.;
-      r.xc[0] = r.xc[1] = r.xc[2] = 0.;
-    }
-    if (inner(s)) {
-      const long long t = ftid(s), f = foff + t;
-      r.n[0] = n0[f]; r.n[1] = n0[dm.F + f]; r.n[2] = n0[2 * dm.F + f];
-      r.db = fdb[t]; r.df = fdf[t]; r.u = fu[t]; r.A = fA[t];
-    } else {
-      r.n[0] = r.n[1] = r.n[2] = 0.; r.db = r.df = r.u = r.A = 0.;
-    }
-  };
-  auto phis = [&](int s, const Raw& r, double P[4]) {
-    if (s >= 0 && s < nd) phi_of(r.U, P);
-    else {
-#pragma unroll
-      for (int v = 0; v < 4; ++v) P[v] = 0.;
-    }
-  };
-  // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172)
-  auto dxf = [&](const Raw& next, const double xp[3]) {
-    return dot(d3(next.xc[0], next.xc[1], next.xc[2]) - d3(xp[0], xp[1], xp[2]), d3(next.n[0], next.n[1], next.n[2]));
-  };
-
-  // prologue: items a-2 .. a+1
-  Raw rm2, rm1, ra, rb;
-  fetch(a - 2, rm2); fetch(a - 1, rm1); fetch(a, ra); fetch(a + 1, rb);
-  double Pm2[4], Pm1[4], Pa[4], Pb[4], Ua[4], Ub[4];
-  phis(a - 2, rm2, Pm2); phis(a - 1, rm1, Pm1); phis(a, ra, Pa); phis(a + 1, rb, Pb);
-#pragma unroll
-  for (int v = 0; v < 4; ++v) { Ua[v] = ra.U[v]; Ub[v] = rb.U[v]; }
-  const double dxm1 = inner(a - 1) ? dxf(rm1, rm2.xc) : 0.;
-  const double dxA = inner(a) ? dxf(ra, rm1.xc) : 0.;
-  double dxB = inner(a + 1) ? dxf(rb, ra.xc) : 0.;
-  double uA = ra.u, AA = ra.A, dbB = rb.db, dfB = rb.df, uB = rb.u, AB = rb.A;
-  double xB[3] = {rb.xc[0], rb.xc[1], rb.xc[2]};
-  double gm1[4], gA[4], gB[4];
-  face_grad(inner(a - 1), dxm1, Pm1, Pm2, gm1);
-  face_grad(inner(a), dxA, Pa, Pm1, gA);
-  face_grad(inner(a + 1), dxB, Pb, Pa, gB);
-  double Gm1[4], Ga[4], PfA[4];
-  limited_grad(lim, gm1, gA, Gm1);
-  limited_grad(lim, gA, gB, Ga);
-  if (inner(a)) face_value(order2, uA, dxA, ra.db, ra.df, Pm1, Gm1, Pa, Ga, PfA);
-  else {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) PfA[v] = 0.;
-  }
-
-  Raw nx;
-  double nob = 0., nof = 0.;
-  auto fetch_next = [&](int s) {   // item s+2 and the outer normals of cell s
-    fetch(s + 2, nx);
-    if (s < nd) { const long long c0 = cid(s); nob = ofn[lb * C + c0]; nof = ofn[lf * C + c0]; }
-  };
-  fetch_next(a);
-  for (int s = a; s < b; ++s) {
-    const Raw rc = nx;
-    const double ob = nob, of = nof;
-    if (s + 1 < b) fetch_next(s + 1);
-    const bool ic = inner(s + 2);
-    double Pc[4];
-    phis(s + 2, rc, Pc);
-    const double dxC = ic ? dxf(rc, xB) : 0.;
-    const long long c = cid(s);
-    double gC[4], Gb[4], PfB[4];
-    face_grad(ic, dxC, Pc, Pb, gC);
-    limited_grad(lim, gB, gC, Gb);
-    const bool ib = inner(s + 1);
-    if (ib) face_value(order2, uB, dxB, dbB, dfB, Pa, Ga, Pb, Gb, PfB);
-    else {
-#pragma unroll
-      for (int v = 0; v < 4; ++v) PfB[v] = 0.;
-    }
-    update_cell<LAST>(ph, S, st, c, dt, inner(s), ob, uA, AA, PfA, ib, of, uB, AB, PfB, Ua, Uout, dpf, C);
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      Ua[v] = Ub[v]; Ub[v] = rc.U[v]; Pa[v] = Pb[v]; Pb[v] = Pc[v]; Ga[v] = Gb[v]; gB[v] = gC[v]; PfA[v] = PfB[v];
-    }
-    uA = uB; AA = AB;
-    dxB = dxC; dbB = rc.db; dfB = rc.df; uB = rc.u; AB = rc.A;
-    xB[0] = rc.xc[0]; xB[1] = rc.xc[1]; xB[2] = rc.xc[2];
-  }
-}
-
-// ---- cells, d = x: warp row ----------------------------------------------
-template <bool LAST>
-__global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_cells_row(Dims dm, const Scalars* __restrict__ S,
+__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
   const int lane = threadIdx.x & 31;
-  const int jr = blockIdx.y * kRowWarps + (threadIdx.x >> 5), kr = blockIdx.z;
-  if (jr >= dm.ny) return;                           // whole warp leaves together
-  const long long row = jr + (long long)dm.ny * kr;
-  const int s = blockIdx.x * kRowUpd - 2 + lane;     // x index of this lane's cell
-  const int nd = dm.nx;
+  const CellLine<D> ln(dm, threadIdx.x >> 5);
+  if (!ln.ok) return;                                  // whole warp leaves together
+  const int s = CellLine<D>::seg0() - 2 + lane;        // position of this lane's cell along D
+  const int nd = dm.ncd(D);
   const bool valid = s >= 0 && s < nd;
-  const bool inner = s >= 1 && s <= nd - 1;          // this lane's low face
+  const bool inner = s >= 1 && s <= nd - 1;            // this lane's low face is an inner face
   const long long C = dm.C;
-  const long long c = row * dm.nx + s;               // cell id (row = j + ny k)
-  const long long t = row * (dm.nx + 1) + s;         // x-face id of the low face
+  const long long c = valid ? ln.cell(dm, s) : 0;
+  const long long t = inner ? ln.face(dm, s) : 0;
+  const long long f = t + (D == 0 ? 0 : (D == 1 ? dm.Fx : dm.Fx + dm.Fy));
   const double order2 = (double)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  double U[4] = {0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.};
+  double U[4] = {0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, xc[3] = {0., 0., 0.};
+  double db = 0., df = 0., u = 0., A = 0., nx = 0., ny = 0., nz = 0.;
   if (valid) {
     U[0] = Uin[c]; U[1] = Uin[C + c]; U[2] = Uin[2 * C + c]; U[3] = Uin[3 * C + c];
-    phi_of(U, P);
+    xc[0] = xcs[c]; xc[1] = xcs[C + c]; xc[2] = xcs[2 * C + c];
   }
+  if (inner) {
+    db = fd.db[D][t]; df = fd.df[D][t]; u = fd.u[D][t]; A = fd.A[D][t];
+    nx = n0[f]; ny = n0[dm.F + f]; nz = n0[2 * dm.F + f];
+  }
+  if (valid) phi_of(U, P);
   const unsigned full = 0xffffffffu;
-  double xc[3] = {0., 0., 0.};
-  if (valid) { xc[0] = xcs[c]; xc[1] = xcs[C + c]; xc[2] = xcs[2 * C + c]; }
   const double xpx = __shfl_up_sync(full, xc[0], 1), xpy = __shfl_up_sync(full, xc[1], 1),
                xpz = __shfl_up_sync(full, xc[2], 1);
-  double dx = 0., db = 0., df = 0., u = 0., A = 0.;
-  if (inner) {
-    db = fd.db[0][t]; df = fd.df[0][t]; u = fd.u[0][t]; A = fd.A[0][t];
-    dx = dot(d3(xc[0], xc[1], xc[2]) - d3(xpx, xpy, xpz), d3(n0[t], n0[dm.F + t], n0[2 * dm.F + t]));
-  }
+  // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172)
+  const double dx = inner ? dot(d3(xc[0], xc[1], xc[2]) - d3(xpx, xpy, xpz), d3(nx, ny, nz)) : 0.;
   double g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pp[v] = __shfl_up_sync(full, P[v], 1);
@@ -572,9 +472,10 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_cells_row(Dims dm,
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
   const double un = __shfl_down_sync(full, u, 1), An = __shfl_down_sync(full, A, 1);
-  if (lane < 2 || lane >= 2 + kRowUpd || !valid) return;
+  if (lane < 2 || lane >= 2 + kLineUpd || !valid) return;
   const bool infr = s + 1 <= nd - 1;
-  const double ob = ofn[1 * C + c], of = ofn[4 * C + c];
+  const int lb = D == 0 ? 1 : (D == 1 ? 2 : 0), lf = D == 0 ? 4 : (D == 1 ? 5 : 3);
+  const double ob = ofn[lb * C + c], of = ofn[lf * C + c];
   update_cell<LAST>(ph, S, st, c, S->dt, inner, ob, u, A, Pf, infr, of, un, An, Pfn, U, Uout, dpf, C);
 }
 
@@ -612,10 +513,11 @@ __device__ __forceinline__ void dual_update(int D, double order2, double dt, dou
 __device__ __forceinline__ void dual_grad(int lim, const double Pm[4], const double Pn[4], const double Pp[4],
                                           double xm, double xn, double xp, double G[3]) {
   const double hf = xp - xn, hb = xn - xm;
+  const double rf = 1.0 / hf, rb = 1.0 / hb;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const double gf = (Pp[c] - Pn[c]) / hf;
-    const double gb = (Pn[c] - Pm[c]) / hb;
+    const double gf = qdiv(Pp[c] - Pn[c], hf, rf);
+    const double gb = qdiv(Pn[c] - Pm[c], hb, rb);
     double g = 0.;
     if (lim == 0) {
       if (!(gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.)))) {
@@ -634,15 +536,22 @@ __device__ __forceinline__ void dual_grad(int lim, const double Pm[4], const dou
 }
 
 // Node velocity and node mass at the end of the remap (RemapADIFinal.cc:660-672, 697-719).
+// |v| of every node is kept for the dt reduction (computed once instead of
+// once per adjacent cell, MahycoModule.cc:2053).
 __device__ __forceinline__ void finalize_node(const Dims& dm, long long n, int i, int j, int k, const double ud[5],
                                               const double* __restrict__ vh, const double* __restrict__ mass,
-                                              double* __restrict__ vout, double* __restrict__ nm_out) {
+                                              double* __restrict__ vout, double* __restrict__ nm_out,
+                                              double* __restrict__ vnorm) {
   const double m = ud[3];
+  D3 u;
   if (m != 0.) {
-    vout[n] = ud[0] / m; vout[dm.N + n] = ud[1] / m; vout[2 * dm.N + n] = ud[2] / m;
+    const double rm = 1.0 / m;
+    u = d3(qdiv(ud[0], m, rm), qdiv(ud[1], m, rm), qdiv(ud[2], m, rm));
   } else {
-    vout[n] = vh[n]; vout[dm.N + n] = vh[dm.N + n]; vout[2 * dm.N + n] = vh[2 * dm.N + n];
+    u = d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
   }
+  vout[n] = u.x; vout[dm.N + n] = u.y; vout[2 * dm.N + n] = u.z;
+  vnorm[n] = norm2(u);
   double sm = 0.;
 #pragma unroll
   for (int dk = 1; dk >= 0; --dk)
@@ -693,168 +602,53 @@ __device__ __forceinline__ void load_node(const Dims& dm, long long n, bool upda
 #pragma unroll
     for (int c = 0; c < 5; ++c) ud[c] = udin[c * dm.N + n];
     if (updated) {
-      const double m = ud[3];
-      P[0] = ud[0] / m; P[1] = ud[1] / m; P[2] = ud[2] / m; P[3] = ud[4] / m;
+      const double m = ud[3], rm = 1.0 / m;
+      P[0] = qdiv(ud[0], m, rm); P[1] = qdiv(ud[1], m, rm); P[2] = qdiv(ud[2], m, rm); P[3] = qdiv(ud[4], m, rm);
     } else {
       P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
     }
   }
 }
 
-// ---- nodes, d = y or z: march --------------------------------------------
+// Index map of a line of nodes along D for the warp w of the block.
+template <int D>
+struct NodeLine {
+  int i, j, k;
+  bool ok;
+  __device__ NodeLine(const Dims& dm, int w) {
+    if (D == 0) { i = 0; j = blockIdx.y * kLineWarps + w; k = blockIdx.z; ok = j <= dm.ny; }
+    else if (D == 1) { i = blockIdx.x * kLineWarps + w; j = 0; k = blockIdx.z; ok = i <= dm.nx; }
+    else { i = blockIdx.x * kLineWarps + w; j = blockIdx.z; k = 0; ok = i <= dm.nx; }
+  }
+  __device__ void ijk(int m, int idx[3]) const {
+    idx[0] = i; idx[1] = j; idx[2] = k; idx[D] = m;
+  }
+  __device__ static int seg0() { return (D == 0 ? blockIdx.x : blockIdx.y) * kLineUpd; }
+};
+
+// ---- nodes ---------------------------------------------------------------
 template <int D, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kMarchWarps) k_cyc_sweep_nodes_march(Dims dm, const Scalars* __restrict__ S,
+__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int i = blockIdx.x * 32 + lane;
-  const int t2 = blockIdx.z;                          // k for d = y, j for d = z
-  const int nn = dm.ncd(D) + 1;
-  const int a = (blockIdx.y * kMarchWarps + warp) * kMarchLen;
-  if (i > dm.nx || a >= nn) return;
-  const int b = min(a + kMarchLen, nn);
-  const long long N = dm.N;
-  auto nid = [&](int m) -> long long {
-    return D == 1 ? i + (long long)(dm.nx + 1) * (m + (long long)(dm.ny + 1) * t2)
-                  : i + (long long)(dm.nx + 1) * (t2 + (long long)(dm.ny + 1) * m);
-  };
-  auto ijk = [&](int m, int idx[3]) { idx[0] = i; idx[D] = m; idx[D == 1 ? 2 : 1] = t2; };
-  const int ot = D == 1 ? 2 : 1;                      // the other transverse direction
-  const bool on_plane_t = i == 0 || i == dm.nx || t2 == 0 || t2 == dm.ncd(ot);
-  bool updated = false;                               // inner along an earlier direction of this cycle
-  if ((prev_inner & 1) && i > 0 && i < dm.nx) updated = true;
-  if ((prev_inner >> ot & 1) && t2 > 0 && t2 < dm.ncd(ot)) updated = true;
-  const double dt = S->dt;
-  const double order2 = (double)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  const bool grad_on = ph.ordre_projection > 1;
-  auto inner = [&](int m) { return m >= 1 && m <= nn - 2; };
-  // raw data of node m: velocity, coordinate along d, U_dual (or node mass on the first sweep)
-  struct NRaw { double v[3], x0d, ud[5]; };
-  auto fetch = [&](int m, NRaw& r) {
-    if (m >= 0 && m < nn) {
-      const long long n = nid(m);
-      r.v[0] = vh[n]; r.v[1] = vh[N + n]; r.v[2] = vh[2 * N + n];
-      r.x0d = x0[D * N + n];
-      if (FIRST) { r.ud[3] = nm_in[n]; }
-      else {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) r.ud[c] = udin[c * N + n];
-      }
-    } else {
-      r.v[0] = r.v[1] = r.v[2] = 0.; r.x0d = 0.;
-#pragma unroll
-      for (int c = 0; c < 5; ++c) r.ud[c] = 0.;
-    }
-  };
-  // U_dual and Phi_dual of node m from its raw data (PrepareRemap.cc:411-433, DualPhaseRemap.cc:515-521)
-  auto expand = [&](int m, const NRaw& r, double ud[5], double P[4], double& x) {
-    if (m >= 0 && m < nn) {
-      const D3 u = d3(r.v[0], r.v[1], r.v[2]);
-      if (FIRST) {
-        const double mm = r.ud[3];
-        const double un = norm2(u);
-        ud[0] = mm * u.x; ud[1] = mm * u.y; ud[2] = mm * u.z; ud[3] = mm; ud[4] = 0.5 * mm * un;
-        P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
-      } else {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) ud[c] = r.ud[c];
-        if (updated) {
-          const double mm = ud[3];
-          P[0] = ud[0] / mm; P[1] = ud[1] / mm; P[2] = ud[2] / mm; P[3] = ud[4] / mm;
-        } else {
-          P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
-        }
-      }
-      x = r.x0d + r.v[D] * dt;
-    } else {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) ud[c] = 0.;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) P[c] = 0.;
-      x = 0.;
-    }
-  };
-  auto stored_grad = [&](int m, double G[3]) {
-    const long long n = nid(m);
-    G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n];
-  };
-  // prologue: nodes a-2 .. a+1
-  double udA[5], udB[5], tmp5[5], Pm2[4], Pm1[4], PA[4], PB[4], xm2, xm1, xA, xB;
-  {
-    NRaw r0, r1, r2, r3;
-    fetch(a - 2, r0); fetch(a - 1, r1); fetch(a, r2); fetch(a + 1, r3);
-    expand(a - 2, r0, tmp5, Pm2, xm2);
-    expand(a - 1, r1, tmp5, Pm1, xm1);
-    expand(a, r2, udA, PA, xA);
-    expand(a + 1, r3, udB, PB, xB);
-  }
-  double Gm1[3] = {0., 0., 0.}, GA[3] = {0., 0., 0.};
-  if (a - 1 >= 0) {
-    if (inner(a - 1) && grad_on) dual_grad(lim, Pm2, Pm1, PA, xm2, xm1, xA, Gm1); else stored_grad(a - 1, Gm1);
-  }
-  if (inner(a) && grad_on) dual_grad(lim, Pm1, PA, PB, xm1, xA, xB, GA); else stored_grad(a, GA);
-  int idx[3];
-  ijk(a, idx);
-  double bfm = flux4<D>(dm, dpf, a - 1, idx);         // back cells of node a = front cells of node a-1
-
-  NRaw nx;
-  fetch(a + 2, nx);
-  for (int m = a; m < b; ++m) {
-    const NRaw rc = nx;
-    if (m + 1 < b) fetch(m + 3, nx);
-    double udC[5], PC[4], xC;
-    expand(m + 2, rc, udC, PC, xC);
-    double GB[3] = {0., 0., 0.};
-    if (m + 1 < nn) {
-      if (inner(m + 1) && grad_on) dual_grad(lim, PA, PB, PC, xA, xB, xC, GB); else stored_grad(m + 1, GB);
-    }
-    ijk(m, idx);
-    const double ffm = flux4<D>(dm, dpf, m, idx);
-    const long long n = nid(m);
-    if (inner(m)) {
-      if (on_plane_t && grad_on) { Gd[n] = GA[0]; Gd[N + n] = GA[1]; Gd[2 * N + n] = GA[2]; }
-      dual_update(D, order2, dt, bfm, ffm, Pm1, PA, PB, Gm1, GA, GB, xm1, xA, xB, udA);
-    }
-    if (!LAST) {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) udout[c * N + n] = udA[c];
-    } else {
-      finalize_node(dm, n, idx[0], idx[1], idx[2], udA, vh, mass, vout, nm_out);
-    }
-    bfm = ffm;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) { Pm1[c] = PA[c]; PA[c] = PB[c]; PB[c] = PC[c]; }
-#pragma unroll
-    for (int c = 0; c < 5; ++c) { udA[c] = udB[c]; udB[c] = udC[c]; }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) { Gm1[c] = GA[c]; GA[c] = GB[c]; }
-    xm1 = xA; xA = xB; xB = xC;
-  }
-}
-
-// ---- nodes, d = x: warp row ----------------------------------------------
-template <bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_nodes_row(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
-    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
-    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out) {
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
   const int lane = threadIdx.x & 31;
-  const int nn = dm.nx + 1;
-  const int j = blockIdx.y * kRowWarps + (threadIdx.x >> 5), k = blockIdx.z;
-  if (j > dm.ny) return;                             // whole warp leaves together
-  const long long row = j + (long long)(dm.ny + 1) * k;
-  const int m = blockIdx.x * kRowUpd - 2 + lane;     // x index of this lane's node
+  const NodeLine<D> ln(dm, threadIdx.x >> 5);
+  if (!ln.ok) return;                                  // whole warp leaves together
+  const int nn = dm.ncd(D) + 1;
+  const int m = NodeLine<D>::seg0() - 2 + lane;        // position of this lane's node along D
   const bool valid = m >= 0 && m < nn;
   const bool inner = m >= 1 && m <= nn - 2;
+  int idx[3];
+  ln.ijk(valid ? m : 0, idx);
   const long long N = dm.N;
-  const long long n = row * nn + m;
+  const long long n = dm.nid(idx[0], idx[1], idx[2]);
+  // inner along an earlier direction of this cycle: Phi_dual = U_dual / m there
   bool updated = false;
-  if ((prev_inner >> 1 & 1) && j > 0 && j < dm.ny) updated = true;
-  if ((prev_inner >> 2 & 1) && k > 0 && k < dm.nz) updated = true;
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd)
+    if (dd != D && (prev_inner >> dd & 1) && idx[dd] > 0 && idx[dd] < dm.ncd(dd)) updated = true;
   const double dt = S->dt;
   const double order2 = (double)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
@@ -862,35 +656,35 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_nodes_row(Dims dm,
   double ud[5] = {0., 0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, x = 0.;
   if (valid) {
     load_node<FIRST>(dm, n, updated, nm_in, vh, udin, ud, P);
-    x = x0[n] + vh[n] * dt;
+    x = x0[D * N + n] + vh[D * N + n] * dt;
   }
+  const double ffm = valid ? flux4<D>(dm, dpf, m, idx) : 0.;
+  double Gs[3] = {0., 0., 0.};
+  const bool stale = valid && !(inner && grad_on);
+  if (stale) { Gs[0] = Gd[n]; Gs[1] = Gd[N + n]; Gs[2] = Gd[2 * N + n]; }
   const unsigned full = 0xffffffffu;
   double Pm[4], Pp[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) { Pm[c] = __shfl_up_sync(full, P[c], 1); Pp[c] = __shfl_down_sync(full, P[c], 1); }
   const double xm = __shfl_up_sync(full, x, 1), xp = __shfl_down_sync(full, x, 1);
-  double G[3] = {0., 0., 0.};
-  if (valid) {
-    if (inner && grad_on) dual_grad(lim, Pm, P, Pp, xm, x, xp, G);
-    else { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
-  }
+  double G[3] = {Gs[0], Gs[1], Gs[2]};
+  if (valid && inner && grad_on) dual_grad(lim, Pm, P, Pp, xm, x, xp, G);
   double Gm[3], Gp[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) { Gm[c] = __shfl_up_sync(full, G[c], 1); Gp[c] = __shfl_down_sync(full, G[c], 1); }
-  const int idx[3] = {m, j, k};
-  const double ffm = valid ? flux4<0>(dm, dpf, m, idx) : 0.;
   const double bfm = __shfl_up_sync(full, ffm, 1);     // back cells of node m = front cells of node m-1
-  if (lane < 2 || lane >= 2 + kRowUpd || !valid) return;
+  if (lane < 2 || lane >= 2 + kLineUpd || !valid) return;
   if (inner) {
-    const bool on_plane_t = j == 0 || j == dm.ny || k == 0 || k == dm.nz;
-    if (on_plane_t && grad_on) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
-    dual_update(0, order2, dt, bfm, ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
+    const bool on_plane = (D != 0 && (idx[0] == 0 || idx[0] == dm.nx)) || (D != 1 && (idx[1] == 0 || idx[1] == dm.ny)) ||
+                          (D != 2 && (idx[2] == 0 || idx[2] == dm.nz));
+    if (on_plane && grad_on) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
+    dual_update(D, order2, dt, bfm, ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
   }
   if (!LAST) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) udout[c * N + n] = ud[c];
   } else {
-    finalize_node(dm, n, m, j, k, ud, vh, mass, vout, nm_out);
+    finalize_node(dm, n, idx[0], idx[1], idx[2], ud, vh, mass, vout, nm_out, vnorm);
   }
 }
 
@@ -899,33 +693,25 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_cyc_sweep_nodes_row(Dims dm,
 template <int D>
 static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
-  if constexpr (D == 0) {
-    const dim3 nb((dm.nx + kRowUpd - 1) / kRowUpd, (dm.ny + kRowWarps - 1) / kRowWarps, dm.nz);
-    if (last) k_cyc_sweep_cells_row<true><<<nb, 32 * kRowWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-    else k_cyc_sweep_cells_row<false><<<nb, 32 * kRowWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-  } else {
-  const int nd = dm.ncd(D);
-  const int nseg = (nd + kMarchLen - 1) / kMarchLen;
-  dim3 g((dm.nx + 31) / 32, (nseg + kMarchWarps - 1) / kMarchWarps, D == 1 ? dm.nz : dm.ny);
-  if (last) k_cyc_sweep_cells_march<D, true><<<g, 32 * kMarchWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-  else k_cyc_sweep_cells_march<D, false><<<g, 32 * kMarchWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-  }
+  const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
+  dim3 g;
+  if (D == 0) g = dim3(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
+  else if (D == 1) g = dim3((dm.nx + kLineWarps - 1) / kLineWarps, nseg, dm.nz);
+  else g = dim3((dm.nx + kLineWarps - 1) / kLineWarps, nseg, dm.ny);
+  if (last) k_cyc_sweep_cells<D, true><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  else k_cyc_sweep_cells<D, false><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
 }
 
 template <int D, bool FIRST, bool LAST>
 static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
   const Dims& dm = a.dm;
-  if constexpr (D == 0) {
-    const dim3 nb((dm.nx + 1 + kRowUpd - 1) / kRowUpd, (dm.ny + 1 + kRowWarps - 1) / kRowWarps, dm.nz + 1);
-    k_cyc_sweep_nodes_row<FIRST, LAST><<<nb, 32 * kRowWarps, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout,
-                                                                     a.dpf, a.Gd, a.st.mass, a.v, a.nm);
-  } else {
-  const int nn = dm.ncd(D) + 1;
-  const int nseg = (nn + kMarchLen - 1) / kMarchLen;
-  dim3 g((dm.nx + 1 + 31) / 32, (nseg + kMarchWarps - 1) / kMarchWarps, D == 1 ? dm.nz + 1 : dm.ny + 1);
-  k_cyc_sweep_nodes_march<D, FIRST, LAST><<<g, 32 * kMarchWarps, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin,
-                                                                       udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm);
-  }
+  const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
+  dim3 g;
+  if (D == 0) g = dim3(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
+  else if (D == 1) g = dim3((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, dm.nz + 1);
+  else g = dim3((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, dm.ny + 1);
+  k_cyc_sweep_nodes<D, FIRST, LAST><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout,
+                                                                  a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
 }
 
 template <int D>
@@ -935,6 +721,7 @@ static void sweep_nodes_d(const CycleArgs& a, bool first, bool last, int prev, c
   else if (last) sweep_nodes_launch<D, false, true>(a, prev, udin, udout, s);
   else sweep_nodes_launch<D, false, false>(a, prev, udin, udout, s);
 }
+
 
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbn((a.dm.nx + 1 + 127) / 128, a.dm.ny + 1, a.dm.nz + 1);
@@ -972,7 +759,7 @@ void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
 
 void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
-  k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.v);
+  k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.vnorm);
   k_dt_finish<<<1, 1, 0, s>>>(a.S, a.ph);
 }
 

@@ -113,10 +113,11 @@ __global__ void k_node_mass(Dims dm, const double* __restrict__ mass, double* __
 }
 
 // computeHydroDeltaT (MahycoModule.cc:2047-2061): min over cells of
-// L / (c + max |v|), warp shuffle + block reduction, one atomicMin per block
-// on the bit pattern (non-negative doubles order like unsigned integers).
+// L / (c + max |v|) (|v| per node precomputed), warp shuffle + block
+// reduction, one atomicMin per block on the bit pattern (non-negative doubles
+// order like unsigned integers).
 __global__ void k_dt_min(Dims dm, Scalars* __restrict__ S, const double* __restrict__ L,
-                         const double* __restrict__ cs, const double* __restrict__ v) {
+                         const double* __restrict__ cs, const double* __restrict__ vnorm) {
   __shared__ unsigned long long wmin[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   unsigned long long best = 0x7fefffffffffffffull;  // DBL_MAX
@@ -125,7 +126,7 @@ __global__ void k_dt_min(Dims dm, Scalars* __restrict__ S, const double* __restr
     double vmax = 0.;
     for (int a = 0; a < 8; ++a) {
       long long n = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
-      vmax = amax(norm2(d3(v[n], v[dm.N + n], v[2 * dm.N + n])), vmax);
+      vmax = amax(vnorm[n], vmax);
     }
     double dx_sound = L[c] / (cs[c] + vmax);
     if (dx_sound >= 0.) best = (unsigned long long)__double_as_longlong(dx_sound);
@@ -158,6 +159,7 @@ __global__ void k_dt_finish(Scalars* S, Phys ph) {
   new_dt = amin(new_dt, ph.deltat_max);
   if (new_dt < ph.deltat_min) S->status |= MHY_STATUS_DT_MIN;
   S->dt = new_dt;
+  S->inv_dt = 1.0 / new_dt;
   if (S->time > ph.final_time) S->status |= MHY_STATUS_FINAL_TIME;
   S->min_bits = 0x7fefffffffffffffull;
   S->iteration += 1;

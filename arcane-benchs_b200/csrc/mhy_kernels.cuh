@@ -13,6 +13,7 @@ namespace mhy {
 struct Scalars {
   double dt;
   double old_dt;
+  double inv_dt;       // 1.0 / dt
   double time;
   unsigned long long min_bits;
   unsigned int status;
@@ -54,7 +55,7 @@ struct CycleArgs {
   BCTable bct;
   const uint16_t* bcmask;
   const double *x0, *n0, *ofn;
-  double *v, *vh, *nm, *cqs, *L, *dpf, *Gd, *xc;
+  double *v, *vh, *nm, *cqs, *L, *dpf, *Gd, *xc, *vnorm;
   double* U[2];
   double* ud[2];
   FaceData fd;
@@ -73,7 +74,7 @@ __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* x
 __global__ void k_init_state(Dims dm, double gamma, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
-__global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* v);
+__global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm);
 __global__ void k_dt_finish(Scalars* S, Phys ph);
 
 }  // namespace mhy

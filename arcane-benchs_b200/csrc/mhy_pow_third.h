@@ -10,9 +10,9 @@
 //   t = fl(1/3) = 1/3 - delta,  delta = 2^-54 / 3  (exact: fl(1/3) = 6004799503160661 * 2^-54)
 //   V^t = cbrt(V) * exp(-delta * ln V) = cbrt(V) * (1 - delta ln V) + O(delta^2 ln^2 V)
 //
-// cbrt(V) is obtained by Newton's method on y^3 = m (m the mantissa scaled into
-// [1,8)), then refined to a double-double y + ylo with an exact residual
-// m - y^3 built from error-free products (fma(a,b,-ab) is the exact rounding
+// cbrt(V) is obtained from Newton's iteration for the reciprocal cube root of
+// m (the mantissa scaled into [1,8)), which needs no division, then refined to
+// a double-double y + ylo with an exact residual m - y^3 built from error-free products (fma(a,b,-ab) is the exact rounding
 // error of a*b; Dekker 1971 / Ogita-Rump-Oishi 2005).  ln V is needed only to
 // ~1e-10 relative (the correction term is at most 1.4e-14 of the result) and is
 // taken from the atanh series ln m = 2 atanh((m-1)/(m+1)) on m in [sqrt(1/2), sqrt(2)).
@@ -85,11 +85,22 @@ MHY_POW_HD double pow_third(double v) {
   const int r = ex - 3 * q;
   const double mr = m * (double)(1 << r);               // [1,8), exact
 
-  // Newton on y^3 = mr from a linear start (max rel. error ~0.1 on [1,8)).
-  double y = 0.7 + 0.16 * mr;
-  for (int it = 0; it < 6; ++it) {
-    const double y2 = y * y;
-    y = y - (y2 * y - mr) / (3.0 * y2);
+  // Reciprocal cube root w ~ m^(-1/3) 2^(-r/3) by Newton's iteration
+  // w <- w + w (1 - mr w^3) / 3, which needs no division, from a quadratic
+  // start on [1,2) (max rel. error 3e-3) -> 3 iterations reach full precision.
+  double w = (0.09202394 * m - 0.47733264) * m + 1.38237822;
+  w = w * (r == 0 ? 1.0 : (r == 1 ? 0.7937005259840998 : 0.6299605249474366));
+  const double third = 1.0 / 3.0;
+  for (int it = 0; it < 3; ++it) {
+    const double w3 = (w * w) * w;
+    w = w + w * ((1.0 - mr * w3) * third);
+  }
+  const double w2 = w * w;
+  double y = mr * w2;                                   // cbrt(mr), within a few ulps
+  // one Newton step on y itself, using 1/(3 y^2) ~ w^2 / 3
+  {
+    const double yy = y * y;
+    y = y - (yy * y - mr) * (w2 * third);
   }
   // Exact-ish residual res = mr - y^3 with error-free transformations.
   const double y2 = y * y;
@@ -98,7 +109,7 @@ MHY_POW_HD double pow_third(double v) {
   const double e3 = pow3_fma(y2, y, -y3);               // y2*y = y3 + e3 exactly
   // y^3 = y3 + e3 + e2*y (+ e2*... terms below 2^-150 relative)
   const double res = ((mr - y3) - e3) - e2 * y;         // mr - y3 exact (Sterbenz)
-  const double ylo = res / (3.0 * y2);
+  const double ylo = res * (w2 * third);                // res / (3 y^2) to ~1e-15 relative
 
   // ln V = ex*ln2 + ln m with m folded into [sqrt(1/2), sqrt(2)).
   double mm = m;
