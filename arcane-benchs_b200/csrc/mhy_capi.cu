@@ -117,6 +117,16 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (!mesh || !opt || !out || !mesh->node_coords) return fail(MHY_ERR_ARG, "null argument");
   *out = nullptr;
   if (mesh->nx < 2 || mesh->ny < 2 || mesh->nz < 2) return fail(MHY_ERR_ARG, "need at least 2 cells per direction");
+  {
+    // The sweep kernels index elements with 32-bit offsets; the largest is
+    // 24 C (the corner vectors) or 3 F (the face normals).
+    const long long nx = mesh->nx, ny = mesh->ny, nz = mesh->nz;
+    const long long C = nx * ny * nz, N = (nx + 1) * (ny + 1) * (nz + 1);
+    const long long F = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1);
+    if (nx > 65535 || ny > 65535 || nz > 65535 || 24 * C >= (1LL << 31) || 5 * N >= (1LL << 31) ||
+        3 * F >= (1LL << 31))
+      return fail(MHY_ERR_ARG, "mesh too large for one context (at most 89 million cells)");
+  }
   if (opt->nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "only one environment is implemented on the device");
   if (opt->ordre_projection < 1 || opt->ordre_projection > 2)
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");

@@ -249,27 +249,39 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Sc
   }
 }
 
+
 // ------------------------------------------------------------------------
 // Directional sweeps.  The stencil of the remap runs along one direction d,
 // so each line of cells (or nodes) along d is independent.  A warp holds 32
 // consecutive items of one line, one per lane, exchanges neighbours with
-// shuffles (no shared memory, no block barrier) and updates the 28 inner ones.
-// For d = x the warps of a block are 8 neighbouring lines (rows) and every
-// load is coalesced; for d = y, z the warps of a block are the lines of 8
-// consecutive x, so the 8 warps together use each 64-byte span they touch
-// (through L1).
+// shuffles and updates the 28 inner ones; a block holds 8 lines.
+//   d = x: the 8 lines are neighbouring rows and a lane's loads and stores
+//          are coalesced along x as they are.
+//   d = y, z: the 8 lines are 8 consecutive x at one (z or y), and a warp's
+//          items are a stride apart in memory.  The block therefore stages
+//          its 8 x 32 tile of every input array in shared memory with loads
+//          that run along x (8 doubles = 64 contiguous bytes per row), each
+//          warp reads its line from there, writes its results back into its
+//          own rows, and the block stores them along x again.
+// All index arithmetic is 32-bit (mhy_create bounds the mesh so that every
+// element offset fits).
 
 constexpr int kLineUpd = 28;    // items updated per warp (32 lanes, 2 halo lanes on each side)
 constexpr int kLineWarps = 8;   // warps (lines) per block
+// Row length (doubles) of a staged tile [array][line][position].  Staging
+// stores by thread (x = tid % 8, p = tid / 8) hit address 36 x + p, whose
+// 8-byte bank pairs (4 x + p) mod 16 cover every pair exactly twice per warp,
+// and line reads run along p, so both are free of bank conflicts.
+constexpr int kTileLd = 36;
+constexpr int kTileArr = kLineWarps * kTileLd;   // doubles per staged array
 
 // remapVariables "moy" kernel for a single-environment cell and the PerfectGas
 // EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
-// PrepareRemap.cc:553-559).
-__device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, const CellState& st, long long c,
-                                              const double u[4]) {
+// PrepareRemap.cc:553-559).  out = rho, e, q, mass, p, c.
+__device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, double vol, const double u[4],
+                                              double out[6]) {
   const double thr = ph.threshold;
   const double U0 = u[0], U1 = u[1], U2 = u[2], U3 = u[3];
-  const double vol = st.Ve[c];
   const double volt = 0. + U0, masset = 0. + U1;
   const double unsurvolt = 1. / volt;
   const double unsurvol = 1. / vol;
@@ -301,44 +313,12 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
   if (r < 0. || energie < 0.) { energie = 0.; r = 0.; }
   const double g = ph.gamma;
   const double pr = (g - 1.) * r * energie;
-  st.rho[c] = r;
-  st.e[c] = energie;
-  st.q[c] = pseudo;
-  st.mass[c] = mf * cm;
-  st.p[c] = pr;
-  st.cs[c] = sqrt(g * pr / r);
-}
-
-// computeUremap_PBorn0 for one cell (RemapADIService.cc:909-987): fluxes
-// o*u*A*dt*Phi_f through the back and front faces along d, U -= sum, dual mass
-// flux sum 0.5*flux*o, clamping of mass and energy.  The boundary faces of d
-// carry Phi_f = 0 and contribute nothing.
-template <bool LAST>
-__device__ __forceinline__ void update_cell(const Phys& ph, const Scalars* S, const CellState& st, long long c,
-                                            double dt, bool inb, double ob, double ub, double Ab, const double Pfb[4],
-                                            bool inf, double of, double uf, double Af, const double Pff[4],
-                                            const double Uold[4], double* __restrict__ Uout, double* __restrict__ dpf,
-                                            long long C) {
-  const double cb = inb ? ob * ub * Ab * dt : 0.;
-  const double cf = inf ? of * uf * Af * dt : 0.;
-  double u[4], dpm = 0.;
-#pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    double flux_face = 0., dp = 0.;
-    if (inb) { const double fl = cb * Pfb[v]; flux_face += fl; dp += 0.5 * fl * ob; }
-    if (inf) { const double fl = cf * Pff[v]; flux_face += fl; dp += 0.5 * fl * of; }
-    u[v] = Uold[v] - flux_face;
-    if (v == 1) dpm = dp;
-  }
-  if (u[1] < 0.) u[1] = 0.;
-  if (u[2] < 0.) u[2] = 0.;
-  dpf[c] = dpm;
-  if (!LAST) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) Uout[v * C + c] = u[v];
-  } else {
-    finalize_cell(ph, S, st, c, u);
-  }
+  out[0] = r;
+  out[1] = energie;
+  out[2] = pseudo;
+  out[3] = mf * cm;
+  out[4] = pr;
+  out[5] = sqrt(g * pr / r);
 }
 
 // Phi = U / sum of the environment volumes = U / U0 for one environment
@@ -397,63 +377,35 @@ __device__ __forceinline__ void face_value(double order2, double u, double dx, d
   for (int v = 0; v < 4; ++v) Pf[v] = back ? (Pp[v] + order2 * dot_xf * Gp[v]) : (Pn[v] + order2 * dot_xf * Gn[v]);
 }
 
-// Index map of a line of cells along D for the warp w of the block.
-template <int D>
-struct CellLine {
-  int i, j, k;          // coordinates of the line (the D one is replaced by the position)
-  bool ok;
-  __device__ CellLine(const Dims& dm, int w) {
-    if (D == 0) { i = 0; j = blockIdx.y * kLineWarps + w; k = blockIdx.z; ok = j < dm.ny; }
-    else if (D == 1) { i = blockIdx.x * kLineWarps + w; j = 0; k = blockIdx.z; ok = i < dm.nx; }
-    else { i = blockIdx.x * kLineWarps + w; j = blockIdx.z; k = 0; ok = i < dm.nx; }
-  }
-  __device__ long long cell(const Dims& dm, int s) const {
-    return D == 0 ? dm.cid(s, j, k) : (D == 1 ? dm.cid(i, s, k) : dm.cid(i, j, s));
-  }
-  // index of the low face of the cell at position s, within direction D
-  __device__ long long face(const Dims& dm, int s) const {
-    if (D == 0) return s + (long long)(dm.nx + 1) * (j + (long long)dm.ny * k);
-    if (D == 1) return i + (long long)dm.nx * (s + (long long)(dm.ny + 1) * k);
-    return i + (long long)dm.nx * (j + (long long)dm.ny * s);
-  }
-  __device__ static int seg0() { return (D == 0 ? blockIdx.x : blockIdx.y) * kLineUpd; }
-};
-
 // ---- cells ---------------------------------------------------------------
-template <int D, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
-    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
-    double* __restrict__ dpf, CellState st) {
-  const int lane = threadIdx.x & 31;
-  const CellLine<D> ln(dm, threadIdx.x >> 5);
-  if (!ln.ok) return;                                  // whole warp leaves together
-  const int s = CellLine<D>::seg0() - 2 + lane;        // position of this lane's cell along D
-  const int nd = dm.ncd(D);
-  const bool valid = s >= 0 && s < nd;
-  const bool inner = s >= 1 && s <= nd - 1;            // this lane's low face is an inner face
-  const long long C = dm.C;
-  const long long c = valid ? ln.cell(dm, s) : 0;
-  const long long t = inner ? ln.face(dm, s) : 0;
-  const long long f = t + (D == 0 ? 0 : (D == 1 ? dm.Fx : dm.Fx + dm.Fy));
+// Inputs of one lane (one cell of a line along d).
+struct CellIn {
+  double U[4], xc[3];
+  double db, df, u, A, n[3];   // low face of the cell along d (inner faces only)
+  double ob, of;               // outward-normal component along d of the back and front faces
+  double vol;                  // initial cell volume (last sweep only)
+};
+constexpr int kCellOutLast = 7;   // rho, e, q, mass, p, c, dual mass flux
+constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
+
+// One line step of computeGradPhiFace, computeGradPhiCell, the upwind face
+// values and computeUremap_PBorn0 (RemapADIService.cc:91-271, 447-517, 658-720,
+// 909-987).  Every lane takes part in the shuffles; lanes with upd set get
+// their cell's results in out.  The boundary faces of d carry Phi_f = 0 and
+// contribute nothing.
+template <bool LAST>
+__device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
+                                          bool infr, bool upd, const CellIn& in, double* out) {
   const double order2 = (double)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  double U[4] = {0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, xc[3] = {0., 0., 0.};
-  double db = 0., df = 0., u = 0., A = 0., nx = 0., ny = 0., nz = 0.;
-  if (valid) {
-    U[0] = Uin[c]; U[1] = Uin[C + c]; U[2] = Uin[2 * C + c]; U[3] = Uin[3 * C + c];
-    xc[0] = xcs[c]; xc[1] = xcs[C + c]; xc[2] = xcs[2 * C + c];
-  }
-  if (inner) {
-    db = fd.db[D][t]; df = fd.df[D][t]; u = fd.u[D][t]; A = fd.A[D][t];
-    nx = n0[f]; ny = n0[dm.F + f]; nz = n0[2 * dm.F + f];
-  }
-  if (valid) phi_of(U, P);
+  double P[4] = {0., 0., 0., 0.};
+  if (valid) phi_of(in.U, P);
   const unsigned full = 0xffffffffu;
-  const double xpx = __shfl_up_sync(full, xc[0], 1), xpy = __shfl_up_sync(full, xc[1], 1),
-               xpz = __shfl_up_sync(full, xc[2], 1);
+  const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
+               xpz = __shfl_up_sync(full, in.xc[2], 1);
   // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172)
-  const double dx = inner ? dot(d3(xc[0], xc[1], xc[2]) - d3(xpx, xpy, xpz), d3(nx, ny, nz)) : 0.;
+  const double dx = inner ? dot(d3(in.xc[0], in.xc[1], in.xc[2]) - d3(xpx, xpy, xpz), d3(in.n[0], in.n[1], in.n[2]))
+                          : 0.;
   double g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pp[v] = __shfl_up_sync(full, P[v], 1);
@@ -463,7 +415,7 @@ __global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells(Dims dm, co
   limited_grad(lim, g, gr, G);
 #pragma unroll
   for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
-  if (inner) face_value(order2, u, dx, db, df, Pp, Gp, P, G, Pf);
+  if (inner) face_value(order2, in.u, dx, in.db, in.df, Pp, Gp, P, G, Pf);
   else {
 #pragma unroll
     for (int v = 0; v < 4; ++v) Pf[v] = 0.;
@@ -471,12 +423,153 @@ __global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells(Dims dm, co
   double Pfn[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
-  const double un = __shfl_down_sync(full, u, 1), An = __shfl_down_sync(full, A, 1);
-  if (lane < 2 || lane >= 2 + kLineUpd || !valid) return;
+  const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
+  if (!upd) return;
+  // fluxes o*u*A*dt*Phi_f through the back and front faces, U -= sum, dual
+  // mass flux sum 0.5*flux*o, clamping of mass and energy (R:909-987)
+  const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
+  const double cf = infr ? in.of * un * An * dt : 0.;
+  double u[4], dpm = 0.;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    double flux_face = 0., dp = 0.;
+    if (inner) { const double fl = cb * Pf[v]; flux_face += fl; dp += 0.5 * fl * in.ob; }
+    if (infr) { const double fl = cf * Pfn[v]; flux_face += fl; dp += 0.5 * fl * in.of; }
+    u[v] = in.U[v] - flux_face;
+    if (v == 1) dpm = dp;
+  }
+  if (u[1] < 0.) u[1] = 0.;
+  if (u[2] < 0.) u[2] = 0.;
+  if (!LAST) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) out[v] = u[v];
+    out[4] = dpm;
+  } else {
+    finalize_cell(ph, S, in.vol, u, out);
+    out[6] = dpm;
+  }
+}
+
+// Cell sweep along x: lanes run along the rows, loads and stores as they are.
+template <bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  if (j >= dm.ny) return;                              // whole warp leaves together
+  const int nd = dm.nx, C = (int)dm.C, F = (int)dm.F;
+  const int s = blockIdx.x * kLineUpd - 2 + lane;      // position of this lane's cell along x
+  const bool valid = s >= 0 && s < nd;
+  const bool inner = s >= 1 && s <= nd - 1;            // this lane's low face is an inner face
   const bool infr = s + 1 <= nd - 1;
-  const int lb = D == 0 ? 1 : (D == 1 ? 2 : 0), lf = D == 0 ? 4 : (D == 1 ? 5 : 3);
-  const double ob = ofn[lb * C + c], of = ofn[lf * C + c];
-  update_cell<LAST>(ph, S, st, c, S->dt, inner, ob, u, A, Pf, infr, of, un, An, Pfn, U, Uout, dpf, C);
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  const int c = valid ? s + dm.nx * (j + dm.ny * k) : 0;
+  const int t = inner ? s + (dm.nx + 1) * (j + dm.ny * k) : 0;   // x faces come first: t is also the face id
+  CellIn in;
+  in.U[0] = in.U[1] = in.U[2] = in.U[3] = 0.; in.xc[0] = in.xc[1] = in.xc[2] = 0.;
+  in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = in.vol = 0.;
+  if (valid) {
+    in.U[0] = Uin[c]; in.U[1] = Uin[C + c]; in.U[2] = Uin[2 * C + c]; in.U[3] = Uin[3 * C + c];
+    in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
+  }
+  if (inner) {
+    in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
+    in.n[0] = n0[t]; in.n[1] = n0[F + t]; in.n[2] = n0[2 * F + t];
+  }
+  if (upd) {
+    in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c];
+    if (LAST) in.vol = st.Ve[c];
+  }
+  double out[LAST ? kCellOutLast : kCellOutMid];
+  cell_line<LAST>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  if (!upd) return;
+  if (!LAST) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Uout[v * C + c] = out[v];
+    dpf[c] = out[4];
+  } else {
+    st.rho[c] = out[0]; st.e[c] = out[1]; st.q[c] = out[2]; st.mass[c] = out[3]; st.p[c] = out[4]; st.cs[c] = out[5];
+    dpf[c] = out[6];
+  }
+}
+
+// Cell sweep along y (D = 1) or z (D = 2), staged through shared memory.
+// Block (bx, by, bz): x = 8 bx .. 8 bx + 7, positions 28 by - 2 .. 28 by + 29
+// along D, and bz = the remaining coordinate (z for D = 1, y for D = 2).
+template <int D, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st) {
+  constexpr int NA = LAST ? 17 : 16;                  // staged input arrays
+  __shared__ double tile[NA * kTileArr];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int nd = dm.ncd(D), C = (int)dm.C, F = (int)dm.F;
+  const int foff = D == 1 ? (int)dm.Fx : (int)(dm.Fx + dm.Fy);
+  const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;   // back / front faces of d in cell-face order
+  // thread (x, p) of the staging layout; also used for the stores at the end
+  const int sx = tid & 7, sp = tid >> 3;
+  const int si = i0 + sx, ss = seg0 + sp;
+  const bool s_valid = si < dm.nx && ss >= 0 && ss < nd;
+  const int sc = D == 1 ? si + dm.nx * (ss + dm.ny * o) : si + dm.nx * (o + dm.ny * ss);
+  {
+    const bool s_inner = si < dm.nx && ss >= 1 && ss <= nd - 1;
+    const int st_ = D == 1 ? si + dm.nx * (ss + (dm.ny + 1) * o) : sc;   // face index within direction D
+    double v[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) v[a] = 0.;
+    if (s_valid) {
+      v[0] = Uin[sc]; v[1] = Uin[C + sc]; v[2] = Uin[2 * C + sc]; v[3] = Uin[3 * C + sc];
+      v[4] = xcs[sc]; v[5] = xcs[C + sc]; v[6] = xcs[2 * C + sc];
+      v[14] = ofn[lb * C + sc]; v[15] = ofn[lf * C + sc];
+      if (LAST) v[NA - 1] = st.Ve[sc];
+    }
+    if (s_inner) {
+      v[7] = fd.db[D][st_]; v[8] = fd.df[D][st_]; v[9] = fd.u[D][st_]; v[10] = fd.A[D][st_];
+      const int f = foff + st_;
+      v[11] = n0[f]; v[12] = n0[F + f]; v[13] = n0[2 * F + f];
+    }
+#pragma unroll
+    for (int a = 0; a < NA; ++a) tile[a * kTileArr + sx * kTileLd + sp] = v[a];
+  }
+  __syncthreads();
+  // line w, position lane
+  const int s = seg0 + lane;
+  const bool line_ok = i0 + w < dm.nx;
+  const bool valid = line_ok && s >= 0 && s < nd;
+  const bool inner = line_ok && s >= 1 && s <= nd - 1;
+  const bool infr = s + 1 <= nd - 1;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  double* row = tile + w * kTileLd + lane;
+  CellIn in;
+  in.U[0] = row[0]; in.U[1] = row[kTileArr]; in.U[2] = row[2 * kTileArr]; in.U[3] = row[3 * kTileArr];
+  in.xc[0] = row[4 * kTileArr]; in.xc[1] = row[5 * kTileArr]; in.xc[2] = row[6 * kTileArr];
+  in.db = row[7 * kTileArr]; in.df = row[8 * kTileArr]; in.u = row[9 * kTileArr]; in.A = row[10 * kTileArr];
+  in.n[0] = row[11 * kTileArr]; in.n[1] = row[12 * kTileArr]; in.n[2] = row[13 * kTileArr];
+  in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
+  in.vol = LAST ? row[(NA - 1) * kTileArr] : 0.;
+  constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
+  double out[NO];
+  cell_line<LAST>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  // each lane overwrites only the tile column it read itself
+  if (upd) {
+#pragma unroll
+    for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];
+  }
+  __syncthreads();
+  if (!(s_valid && sp >= 2 && sp < 2 + kLineUpd)) return;
+  const double* r = tile + sx * kTileLd + sp;
+  if (!LAST) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Uout[v * C + sc] = r[v * kTileArr];
+    dpf[sc] = r[4 * kTileArr];
+  } else {
+    st.rho[sc] = r[0]; st.e[sc] = r[kTileArr]; st.q[sc] = r[2 * kTileArr]; st.mass[sc] = r[3 * kTileArr];
+    st.p[sc] = r[4 * kTileArr]; st.cs[sc] = r[5 * kTileArr]; dpf[sc] = r[6 * kTileArr];
+  }
 }
 
 // ---- nodes ---------------------------------------------------------------
@@ -508,183 +601,314 @@ __device__ __forceinline__ void dual_update(int D, double order2, double dt, dou
   ud[0] = out[0]; ud[1] = out[1]; ud[2] = out[2]; ud[3] = u3; ud[4] = out[3];
 }
 
-// Limited nodal gradient (DualPhaseRemap.cc:736-777); the terms are
-// (0.5*phi(r))*g here, and the same single-division reading of minmod applies.
-__device__ __forceinline__ void dual_grad(int lim, const double Pm[4], const double Pn[4], const double Pp[4],
-                                          double xm, double xn, double xp, double G[3]) {
-  const double hf = xp - xn, hb = xn - xm;
-  const double rf = 1.0 / hf, rb = 1.0 / hb;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const double gf = qdiv(Pp[c] - Pn[c], hf, rf);
-    const double gb = qdiv(Pn[c] - Pm[c], hb, rb);
-    double g = 0.;
-    if (lim == 0) {
-      if (!(gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.)))) {
-        const bool fsmall = fabs(gf) < fabs(gb);
-        const double r = fsmall ? gf / gb : gb / gf;
-        const double t1 = fsmall ? 0.5 * r * gb : 0.5 * 1.0 * gb;
-        const double t2 = fsmall ? 0.5 * 1.0 * gf : 0.5 * r * gf;
-        g = (0. + t1) + t2;
-      }
-    } else {
-      if (gb != 0.) g += 0.5 * limiter(lim, gf / gb) * gb;
-      if (gf != 0.) g += 0.5 * limiter(lim, gb / gf) * gf;
+// One limited nodal gradient component (DualPhaseRemap.cc:736-777) from the
+// back and front differences; the terms are (0.5*phi(r))*g here, and the same
+// single-division reading of minmod applies.
+__device__ __forceinline__ double dual_limited(int lim, double gb, double gf) {
+  double g = 0.;
+  if (lim == 0) {
+    if (!(gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.)))) {
+      const bool fsmall = fabs(gf) < fabs(gb);
+      const double r = fsmall ? gf / gb : gb / gf;
+      const double t1 = fsmall ? 0.5 * r * gb : 0.5 * 1.0 * gb;
+      const double t2 = fsmall ? 0.5 * 1.0 * gf : 0.5 * r * gf;
+      g = (0. + t1) + t2;
     }
-    G[c] = g;
-  }
-}
-
-// Node velocity and node mass at the end of the remap (RemapADIFinal.cc:660-672, 697-719).
-// |v| of every node is kept for the dt reduction (computed once instead of
-// once per adjacent cell, MahycoModule.cc:2053).
-__device__ __forceinline__ void finalize_node(const Dims& dm, long long n, int i, int j, int k, const double ud[5],
-                                              const double* __restrict__ vh, const double* __restrict__ mass,
-                                              double* __restrict__ vout, double* __restrict__ nm_out,
-                                              double* __restrict__ vnorm) {
-  const double m = ud[3];
-  D3 u;
-  if (m != 0.) {
-    const double rm = 1.0 / m;
-    u = d3(qdiv(ud[0], m, rm), qdiv(ud[1], m, rm), qdiv(ud[2], m, rm));
   } else {
-    u = d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
+    if (gb != 0.) g += 0.5 * limiter(lim, gf / gb) * gb;
+    if (gf != 0.) g += 0.5 * limiter(lim, gb / gf) * gf;
   }
-  vout[n] = u.x; vout[dm.N + n] = u.y; vout[2 * dm.N + n] = u.z;
-  vnorm[n] = norm2(u);
-  double sm = 0.;
-#pragma unroll
-  for (int dk = 1; dk >= 0; --dk)
-#pragma unroll
-    for (int dj = 1; dj >= 0; --dj)
-#pragma unroll
-      for (int di = 1; di >= 0; --di) {
-        const int ci = i - di, cj = j - dj, ck = k - dk;
-        if (ci < 0 || cj < 0 || ck < 0 || ci >= dm.nx || cj >= dm.ny || ck >= dm.nz) continue;
-        sm += mass[dm.cid(ci, cj, ck)];
-      }
-  nm_out[n] = .125 * sm;
+  return g;
 }
 
-// Sum of 0.25*dual mass flux over the 4 cells whose index along d is cd and
-// whose transverse indices are idx[d1]+s1, idx[d2]+s2 (s1, s2 in {-1, 0}),
-// in the order of DualPhaseRemap.cc:299-340.
-template <int D>
-__device__ __forceinline__ double flux4(const Dims& dm, const double* __restrict__ dpf, int cd, const int idx[3]) {
-  constexpr int d1 = (D + 1) % 3, d2 = (D + 2) % 3;
-  double f = 0.;
-  if (cd < 0 || cd >= dm.ncd(D)) return f;
-#pragma unroll
-  for (int s1 = -1; s1 <= 0; ++s1)
-#pragma unroll
-    for (int s2 = -1; s2 <= 0; ++s2) {
-      int ci[3] = {idx[0], idx[1], idx[2]};
-      ci[D] = cd; ci[d1] += s1; ci[d2] += s2;
-      if (ci[d1] >= 0 && ci[d1] < dm.ncd(d1) && ci[d2] >= 0 && ci[d2] < dm.ncd(d2))
-        f += 0.25 * dpf[dm.cid(ci[0], ci[1], ci[2])];
-    }
-  return f;
-}
-
-// Node state at the start of a sweep: U_dual and Phi_dual (PrepareRemap.cc:411-433
-// on the first sweep or for nodes not yet updated this cycle, else U_dual / m).
-template <bool FIRST>
-__device__ __forceinline__ void load_node(const Dims& dm, long long n, bool updated, const double* __restrict__ nm,
-                                          const double* __restrict__ vh, const double* __restrict__ udin,
-                                          double ud[5], double P[4]) {
-  const D3 u = d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
-  if (FIRST) {
-    const double m = nm[n];
-    const double un = norm2(u);
-    ud[0] = m * u.x; ud[1] = m * u.y; ud[2] = m * u.z; ud[3] = m; ud[4] = 0.5 * m * un;
-    P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
-  } else {
-#pragma unroll
-    for (int c = 0; c < 5; ++c) ud[c] = udin[c * dm.N + n];
-    if (updated) {
-      const double m = ud[3], rm = 1.0 / m;
-      P[0] = qdiv(ud[0], m, rm); P[1] = qdiv(ud[1], m, rm); P[2] = qdiv(ud[2], m, rm); P[3] = qdiv(ud[4], m, rm);
-    } else {
-      P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
-    }
-  }
-}
-
-// Index map of a line of nodes along D for the warp w of the block.
-template <int D>
-struct NodeLine {
-  int i, j, k;
-  bool ok;
-  __device__ NodeLine(const Dims& dm, int w) {
-    if (D == 0) { i = 0; j = blockIdx.y * kLineWarps + w; k = blockIdx.z; ok = j <= dm.ny; }
-    else if (D == 1) { i = blockIdx.x * kLineWarps + w; j = 0; k = blockIdx.z; ok = i <= dm.nx; }
-    else { i = blockIdx.x * kLineWarps + w; j = blockIdx.z; k = 0; ok = i <= dm.nx; }
-  }
-  __device__ void ijk(int m, int idx[3]) const {
-    idx[0] = i; idx[1] = j; idx[2] = k; idx[D] = m;
-  }
-  __device__ static int seg0() { return (D == 0 ? blockIdx.x : blockIdx.y) * kLineUpd; }
+// Inputs of one lane (one node of a line along d).
+struct NodeIn {
+  double vh[3];    // Lagrange velocity
+  double x0d;      // initial coordinate along d
+  double nm;       // node mass (first sweep)
+  double ud[5];    // U_dual (later sweeps)
+  double ffm;      // sum of 0.25 * dual mass flux of the 4 cells in front (DualPhaseRemap.cc:299-340)
+  double msum;     // sum of the masses of the up to 8 cells around the node (last sweep)
 };
+constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| on the last sweep
 
-// ---- nodes ---------------------------------------------------------------
+// One line step of computeDualUremap and computeDualGradPhi_LimC
+// (DualPhaseRemap.cc:22-523, 700-778), then remapVariables for the node
+// velocity and mass on the last sweep (RemapADIFinal.cc:660-672, 697-719;
+// |v| is kept for the dt reduction, MahycoModule.cc:2053).  The state at the
+// start of a sweep is PrepareRemap.cc:411-433 on the first sweep or for nodes
+// not yet updated this cycle, else U_dual / m.  G holds the node's stale
+// gradient on entry and its gradient on return.
 template <int D, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
-    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
-    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  const int lane = threadIdx.x & 31;
-  const NodeLine<D> ln(dm, threadIdx.x >> 5);
-  if (!ln.ok) return;                                  // whole warp leaves together
-  const int nn = dm.ncd(D) + 1;
-  const int m = NodeLine<D>::seg0() - 2 + lane;        // position of this lane's node along D
-  const bool valid = m >= 0 && m < nn;
-  const bool inner = m >= 1 && m <= nn - 2;
-  int idx[3];
-  ln.ijk(valid ? m : 0, idx);
-  const long long N = dm.N;
-  const long long n = dm.nid(idx[0], idx[1], idx[2]);
-  // inner along an earlier direction of this cycle: Phi_dual = U_dual / m there
-  bool updated = false;
-#pragma unroll
-  for (int dd = 0; dd < 3; ++dd)
-    if (dd != D && (prev_inner >> dd & 1) && idx[dd] > 0 && idx[dd] < dm.ncd(dd)) updated = true;
-  const double dt = S->dt;
+__device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
+                                          bool upd, const NodeIn& in, double G[3], double* out) {
   const double order2 = (double)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
   const bool grad_on = ph.ordre_projection > 1;
   double ud[5] = {0., 0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, x = 0.;
   if (valid) {
-    load_node<FIRST>(dm, n, updated, nm_in, vh, udin, ud, P);
-    x = x0[D * N + n] + vh[D * N + n] * dt;
+    const D3 u = d3(in.vh[0], in.vh[1], in.vh[2]);
+    if (FIRST) {
+      const double m = in.nm;
+      const double un = norm2(u);
+      ud[0] = m * u.x; ud[1] = m * u.y; ud[2] = m * u.z; ud[3] = m; ud[4] = 0.5 * m * un;
+      P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) ud[c] = in.ud[c];
+      if (updated) {
+        const double m = ud[3], rm = 1.0 / m;
+        P[0] = qdiv(ud[0], m, rm); P[1] = qdiv(ud[1], m, rm); P[2] = qdiv(ud[2], m, rm); P[3] = qdiv(ud[4], m, rm);
+      } else {
+        P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
+      }
+    }
+    x = in.x0d + in.vh[D] * dt;
   }
-  const double ffm = valid ? flux4<D>(dm, dpf, m, idx) : 0.;
-  double Gs[3] = {0., 0., 0.};
-  const bool stale = valid && !(inner && grad_on);
-  if (stale) { Gs[0] = Gd[n]; Gs[1] = Gd[N + n]; Gs[2] = Gd[2 * N + n]; }
   const unsigned full = 0xffffffffu;
   double Pm[4], Pp[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) { Pm[c] = __shfl_up_sync(full, P[c], 1); Pp[c] = __shfl_down_sync(full, P[c], 1); }
   const double xm = __shfl_up_sync(full, x, 1), xp = __shfl_down_sync(full, x, 1);
-  double G[3] = {Gs[0], Gs[1], Gs[2]};
-  if (valid && inner && grad_on) dual_grad(lim, Pm, P, Pp, xm, x, xp, G);
+  if (grad_on) {
+    // front difference quotient of this node = back difference quotient of the next
+    const double hf = xp - x, rf = 1.0 / hf;
+    double gf[3], gb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gf[c] = qdiv(Pp[c] - P[c], hf, rf);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gb[c] = __shfl_up_sync(full, gf[c], 1);
+    if (valid && inner) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) G[c] = dual_limited(lim, gb[c], gf[c]);
+    }
+  }
   double Gm[3], Gp[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) { Gm[c] = __shfl_up_sync(full, G[c], 1); Gp[c] = __shfl_down_sync(full, G[c], 1); }
-  const double bfm = __shfl_up_sync(full, ffm, 1);     // back cells of node m = front cells of node m-1
-  if (lane < 2 || lane >= 2 + kLineUpd || !valid) return;
-  if (inner) {
-    const bool on_plane = (D != 0 && (idx[0] == 0 || idx[0] == dm.nx)) || (D != 1 && (idx[1] == 0 || idx[1] == dm.ny)) ||
-                          (D != 2 && (idx[2] == 0 || idx[2] == dm.nz));
-    if (on_plane && grad_on) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
-    dual_update(D, order2, dt, bfm, ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
-  }
+  const double bfm = __shfl_up_sync(full, in.ffm, 1);  // back cells of node m = front cells of node m-1
+  if (!upd) return;
+  if (inner) dual_update(D, order2, dt, bfm, in.ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
   if (!LAST) {
 #pragma unroll
-    for (int c = 0; c < 5; ++c) udout[c * N + n] = ud[c];
+    for (int c = 0; c < 5; ++c) out[c] = ud[c];
   } else {
-    finalize_node(dm, n, idx[0], idx[1], idx[2], ud, vh, mass, vout, nm_out, vnorm);
+    const double m = ud[3];
+    D3 u;
+    if (m != 0.) {
+      const double rm = 1.0 / m;
+      u = d3(qdiv(ud[0], m, rm), qdiv(ud[1], m, rm), qdiv(ud[2], m, rm));
+    } else {
+      u = d3(in.vh[0], in.vh[1], in.vh[2]);
+    }
+    out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = .125 * in.msum; out[4] = norm2(u);
+  }
+}
+
+// inner along an earlier direction of this cycle: Phi_dual = U_dual / m there
+__device__ __forceinline__ bool node_updated(const Dims& dm, int D, int prev_inner, const int idx[3]) {
+  bool updated = false;
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd)
+    if (dd != D && (prev_inner >> dd & 1) && idx[dd] > 0 && idx[dd] < dm.ncd(dd)) updated = true;
+  return updated;
+}
+
+// the node lies on a boundary plane of another direction: its gradient is
+// kept for later cycles, where it is read as a stale value
+__device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int idx[3]) {
+  return (D != 0 && (idx[0] == 0 || idx[0] == dm.nx)) || (D != 1 && (idx[1] == 0 || idx[1] == dm.ny)) ||
+         (D != 2 && (idx[2] == 0 || idx[2] == dm.nz));
+}
+
+// Node sweep along x: lanes run along the rows of nodes.
+template <bool FIRST, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  if (j > dm.ny) return;                               // whole warp leaves together
+  const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
+  const int m = blockIdx.x * kLineUpd - 2 + lane;      // position of this lane's node along x
+  const bool valid = m >= 0 && m <= nx;
+  const bool inner = m >= 1 && m <= nx - 1;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  const int idx[3] = {valid ? m : 0, j, k};
+  const int n = idx[0] + (nx + 1) * (j + (ny + 1) * k);
+  const bool updated = node_updated(dm, 0, prev_inner, idx);
+  const bool grad_on = ph.ordre_projection > 1;
+  NodeIn in;
+  in.vh[0] = in.vh[1] = in.vh[2] = 0.; in.x0d = 0.; in.nm = 0.;
+  in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
+  double G[3] = {0., 0., 0.};
+  if (valid) {
+    in.vh[0] = vh[n]; in.vh[1] = vh[N + n]; in.vh[2] = vh[2 * N + n]; in.x0d = x0[n];
+    if (FIRST) in.nm = nm_in[n];
+    else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) in.ud[c] = udin[c * N + n];
+    }
+    // flux of the 4 cells in front (x index m), in the order of DualPhaseRemap.cc:299-340
+    // (s1 over y, s2 over z)
+    if (m < nx) {
+      double f = 0.;
+#pragma unroll
+      for (int s1 = -1; s1 <= 0; ++s1)
+#pragma unroll
+        for (int s2 = -1; s2 <= 0; ++s2) {
+          const int cj = j + s1, ck = k + s2;
+          if (cj >= 0 && cj < ny && ck >= 0 && ck < nz) f += 0.25 * dpf[m + nx * (cj + ny * ck)];
+        }
+      in.ffm = f;
+    }
+    if (!(inner && grad_on)) { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
+    if (LAST && upd) {
+      double sm = 0.;
+#pragma unroll
+      for (int dk = 1; dk >= 0; --dk)
+#pragma unroll
+        for (int dj = 1; dj >= 0; --dj)
+#pragma unroll
+          for (int di = 1; di >= 0; --di) {
+            const int ci = m - di, cj = j - dj, ck = k - dk;
+            if (ci < 0 || cj < 0 || ck < 0 || ci >= nx || cj >= ny || ck >= nz) continue;
+            sm += mass[ci + nx * (cj + ny * ck)];
+          }
+      in.msum = sm;
+    }
+  }
+  double out[kNodeOut];
+  node_line<0, FIRST, LAST>(ph, S->dt, valid, inner, updated, upd, in, G, out);
+  if (!upd) return;
+  if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
+  if (!LAST) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) udout[c * N + n] = out[c];
+  } else {
+    vout[n] = out[0]; vout[N + n] = out[1]; vout[2 * N + n] = out[2]; nm_out[n] = out[3]; vnorm[n] = out[4];
+  }
+}
+
+// Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
+// Block (bx, by, bz): node x = 8 bx .. 8 bx + 7, positions 28 by - 2 ..
+// 28 by + 29 along D, bz = the remaining node coordinate o (z for D = 1, y
+// for D = 2).  The cells around those nodes have x = 8 bx - 1 .. 8 bx + 7 and
+// o - 1 .. o along the remaining axis: their dual mass fluxes (and masses on
+// the last sweep) are staged as [o - 1 + q][x - 8 bx + 1][position], with zero
+// for cells outside the mesh (adding +0 to these sums changes no bit).
+template <int D, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
+  constexpr int NA = FIRST ? 5 : 9;                   // vh x3, x0[D], nm or U_dual x5
+  constexpr int NT = LAST ? 2 : 1;                    // cell tiles: dual mass flux (+ mass)
+  constexpr int CT = 2 * (kLineWarps + 1) * 32;       // elements of one cell tile
+  constexpr int CLd = 32;                             // row length of a cell tile
+  __shared__ double tile[NA * kTileArr];
+  __shared__ double ctile[NT * CT];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
+  const int nn = dm.ncd(D) + 1, no = D == 1 ? nz : ny;   // cells along D; cells along the remaining axis
+  auto node_id = [&](int i, int m) { return D == 1 ? i + (nx + 1) * (m + (ny + 1) * o) : i + (nx + 1) * (o + (ny + 1) * m); };
+  const int sx = tid & 7, sp = tid >> 3;
+  const int si = i0 + sx, sm_ = seg0 + sp;
+  const bool s_valid = si <= nx && sm_ >= 0 && sm_ < nn;
+  const int sn = s_valid ? node_id(si, sm_) : 0;
+  {
+    double v[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) v[a] = 0.;
+    if (s_valid) {
+      v[0] = vh[sn]; v[1] = vh[N + sn]; v[2] = vh[2 * N + sn]; v[3] = x0[D * N + sn];
+      if (FIRST) v[4] = nm_in[sn];
+      else {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v[4 + c] = udin[c * N + sn];
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < NA; ++a) tile[a * kTileArr + sx * kTileLd + sp] = v[a];
+    // cell tiles: element e = (q * 9 + xx) * 32 + p, loaded with xx fastest
+    for (int e = tid; e < CT; e += 32 * kLineWarps) {
+      const int xx = e % (kLineWarps + 1), r = e / (kLineWarps + 1);
+      const int p = r & 31, q = r >> 5;
+      const int ci = i0 - 1 + xx, cd = seg0 + p, co = o - 1 + q;
+      const bool cv = ci >= 0 && ci < nx && cd >= 0 && cd < nn - 1 && co >= 0 && co < no;
+      const int c = D == 1 ? ci + nx * (cd + ny * co) : ci + nx * (co + ny * cd);
+      const int at = (q * (kLineWarps + 1) + xx) * CLd + p;
+      ctile[at] = cv ? dpf[c] : 0.;
+      if (LAST) ctile[CT + at] = cv ? mass[c] : 0.;
+    }
+  }
+  __syncthreads();
+  const int m = seg0 + lane;
+  const int i = i0 + w;
+  const bool valid = i <= nx && m >= 0 && m < nn;
+  const bool inner = i <= nx && m >= 1 && m <= nn - 2;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  int idx[3];
+  idx[0] = i; idx[D] = m; idx[3 - D] = o;               // D = 1: (i, m, o); D = 2: (i, o, m)
+  const bool updated = node_updated(dm, D, prev_inner, idx);
+  const bool grad_on = ph.ordre_projection > 1;
+  double* row = tile + w * kTileLd + lane;
+  NodeIn in;
+  in.vh[0] = row[0]; in.vh[1] = row[kTileArr]; in.vh[2] = row[2 * kTileArr]; in.x0d = row[3 * kTileArr];
+  in.nm = FIRST ? row[4 * kTileArr] : 0.;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) in.ud[c] = FIRST ? 0. : row[(4 + c) * kTileArr];
+  // cells in front of the node along D have index m along D; transverse
+  // (x - 1, x) = columns (w, w + 1) and (o - 1, o) = tile rows (0, 1)
+  const double* cr = ctile + w * CLd + lane;
+  constexpr int QS = (kLineWarps + 1) * CLd;          // stride between the two tile rows
+  const double f00 = cr[0], f01 = cr[CLd], f10 = cr[QS], f11 = cr[QS + CLd];   // f[q][dx]
+  // DualPhaseRemap.cc:299-340 order: s1 over d1 = (D+1)%3, s2 over d2 = (D+2)%3.
+  // D = 1: s1 over z (q), s2 over x; D = 2: s1 over x, s2 over y (q).
+  double f = 0.;
+  if (D == 1) { f += 0.25 * f00; f += 0.25 * f01; f += 0.25 * f10; f += 0.25 * f11; }
+  else { f += 0.25 * f00; f += 0.25 * f10; f += 0.25 * f01; f += 0.25 * f11; }
+  in.ffm = (valid && m < nn - 1) ? f : 0.;
+  in.msum = 0.;
+  if (LAST) {
+    const double* mr = cr + CT;
+    const double a00 = mr[0], a01 = mr[CLd], a10 = mr[QS], a11 = mr[QS + CLd];   // cells at index m along D
+    const unsigned full = 0xffffffffu;
+    const double b00 = __shfl_up_sync(full, a00, 1), b01 = __shfl_up_sync(full, a01, 1),
+                 b10 = __shfl_up_sync(full, a10, 1), b11 = __shfl_up_sync(full, a11, 1);   // index m - 1
+    // increasing cell id: z outer, y, x inner
+    double sm = 0.;
+    if (D == 1) {   // (x, y=m-1|m, z=o-1|o): q = z
+      sm += b00; sm += b01; sm += a00; sm += a01; sm += b10; sm += b11; sm += a10; sm += a11;
+    } else {        // (x, y=o-1|o, z=m-1|m): q = y
+      sm += b00; sm += b01; sm += b10; sm += b11; sm += a00; sm += a01; sm += a10; sm += a11;
+    }
+    in.msum = sm;
+  }
+  double G[3] = {0., 0., 0.};
+  const int n = valid ? node_id(i, m) : 0;
+  if (valid && !(inner && grad_on)) { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
+  double out[kNodeOut];
+  node_line<D, FIRST, LAST>(ph, S->dt, valid, inner, updated, upd, in, G, out);
+  if (upd) {
+    if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
+    // each lane overwrites only the tile column it read itself
+#pragma unroll
+    for (int c = 0; c < kNodeOut; ++c) row[c * kTileArr] = out[c];
+  }
+  __syncthreads();
+  if (!(s_valid && sp >= 2 && sp < 2 + kLineUpd)) return;
+  const double* r = tile + sx * kTileLd + sp;
+  if (!LAST) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) udout[c * N + sn] = r[c * kTileArr];
+  } else {
+    vout[sn] = r[0]; vout[N + sn] = r[kTileArr]; vout[2 * N + sn] = r[2 * kTileArr];
+    nm_out[sn] = r[3 * kTileArr]; vnorm[sn] = r[4 * kTileArr];
   }
 }
 
@@ -694,24 +918,33 @@ template <int D>
 static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
-  dim3 g;
-  if (D == 0) g = dim3(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
-  else if (D == 1) g = dim3((dm.nx + kLineWarps - 1) / kLineWarps, nseg, dm.nz);
-  else g = dim3((dm.nx + kLineWarps - 1) / kLineWarps, nseg, dm.ny);
-  if (last) k_cyc_sweep_cells<D, true><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-  else k_cyc_sweep_cells<D, false><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  const int bx = (dm.nx + kLineWarps - 1) / kLineWarps;
+  const int T = 32 * kLineWarps;
+  if constexpr (D == 0) {
+    const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
+    if (last) k_cyc_sweep_cells_x<true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    else k_cyc_sweep_cells_x<false><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  } else {
+    const dim3 g(bx, nseg, D == 1 ? dm.nz : dm.ny);
+    if (last) k_cyc_sweep_cells_t<D, true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    else k_cyc_sweep_cells_t<D, false><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+  }
 }
 
 template <int D, bool FIRST, bool LAST>
 static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
-  dim3 g;
-  if (D == 0) g = dim3(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
-  else if (D == 1) g = dim3((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, dm.nz + 1);
-  else g = dim3((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, dm.ny + 1);
-  k_cyc_sweep_nodes<D, FIRST, LAST><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout,
-                                                                  a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+  const int T = 32 * kLineWarps;
+  if constexpr (D == 0) {
+    const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
+    k_cyc_sweep_nodes_x<FIRST, LAST><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd,
+                                                     a.st.mass, a.v, a.nm, a.vnorm);
+  } else {
+    const dim3 g((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, (D == 1 ? dm.nz : dm.ny) + 1);
+    k_cyc_sweep_nodes_t<D, FIRST, LAST><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf,
+                                                        a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+  }
 }
 
 template <int D>
@@ -721,7 +954,6 @@ static void sweep_nodes_d(const CycleArgs& a, bool first, bool last, int prev, c
   else if (last) sweep_nodes_launch<D, false, true>(a, prev, udin, udout, s);
   else sweep_nodes_launch<D, false, false>(a, prev, udin, udout, s);
 }
-
 
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbn((a.dm.nx + 1 + 127) / 128, a.dm.ny + 1, a.dm.nz + 1);

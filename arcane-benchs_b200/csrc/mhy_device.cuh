@@ -33,8 +33,15 @@ __device__ __forceinline__ double comp(D3 a, int d) { return d == 0 ? a.x : (d =
 // plain division is taken.  Checked against x / y on 3e10 random and
 // adversarial operand pairs with no difference.  Used wherever several
 // quotients share a denominator.
+// A zero numerator over a normal or infinite y is answered by q0 = x r:
+// r is then a nonzero finite number or a signed zero with the sign of y, so
+// q0 is the zero whose sign is sign(x) xor sign(y), which is IEEE x / y.
+// Zeros are the common case on quiescent regions of the mesh (velocity,
+// pseudo-viscosity and their differences), and would otherwise pay for a
+// full division.
 __device__ __forceinline__ double qdiv(double x, double y, double r) {
   const double q0 = x * r;
+  if (x == 0.0 && fabs(y) >= 0x1p-1022) return q0;
   const double ax = fabs(x), aq = fabs(q0);
   if (!(ax >= 0x1p-960 && ax <= 0x1p+960 && aq >= 0x1p-960 && aq <= 0x1p+960)) return x / y;
   return __fma_rn(__fma_rn(-q0, y, x), r, q0);
