@@ -268,6 +268,11 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Sc
 
 constexpr int kLineUpd = 28;    // items updated per warp (32 lanes, 2 halo lanes on each side)
 constexpr int kLineWarps = 8;   // warps (lines) per block
+// The sweeps are latency bound (long dependent chains of divisions and
+// shuffles per lane); 4 resident blocks (32 warps, 64 registers, a few bytes
+// of spill) per SM run them 15 % faster than the 2-3 blocks the compiler's
+// own register choice allows (Sedov 128^3 on B200).
+constexpr int kLineMinBlocks = 4;
 // Row length (doubles) of a staged tile [array][line][position].  Staging
 // stores by thread (x = tid % 8, p = tid / 8) hit address 36 x + p, whose
 // 8-byte bank pairs (4 x + p) mod 16 cover every pair exactly twice per warp,
@@ -452,7 +457,7 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
 template <bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
@@ -499,7 +504,7 @@ __global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells_x(Dims dm, 
 // Block (bx, by, bz): x = 8 bx .. 8 bx + 7, positions 28 by - 2 .. 28 by + 29
 // along D, and bz = the remaining coordinate (z for D = 1, y for D = 2).
 template <int D, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
@@ -723,7 +728,7 @@ __device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int i
 
 // Node sweep along x: lanes run along the rows of nodes.
 template <bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
@@ -800,7 +805,7 @@ __global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes_x(Dims dm, 
 // the last sweep) are staged as [o - 1 + q][x - 8 bx + 1][position], with zero
 // for cells outside the mesh (adding +0 to these sums changes no bit).
 template <int D, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
