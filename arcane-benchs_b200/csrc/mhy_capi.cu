@@ -56,6 +56,10 @@ struct mhy_ctx {
   double *rho = nullptr, *e = nullptr, *q = nullptr, *p = nullptr, *cs = nullptr, *mass = nullptr;
   double *L = nullptr, *Ve = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr, *xc = nullptr;
   double *U[2] = {nullptr, nullptr};
+  // environments (K > 1)
+  int K = 1;
+  EnvState env{};
+  double* Vlag = nullptr;
   // faces
   double* n0 = nullptr;
   FaceData fd{};
@@ -84,6 +88,7 @@ struct mhy_ctx {
     a.U[0] = U[0]; a.U[1] = U[1]; a.ud[0] = ud[0]; a.ud[1] = ud[1];
     a.fd = fd;
     a.st.rho = rho; a.st.e = e; a.st.q = q; a.st.p = p; a.st.cs = cs; a.st.mass = mass; a.st.Ve = Ve;
+    a.K = K; a.env = env; a.Vlag = Vlag;
     return a;
   }
 };
@@ -127,7 +132,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
         3 * F >= (1LL << 31))
       return fail(MHY_ERR_ARG, "mesh too large for one context (at most 89 million cells)");
   }
-  if (opt->nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "only one environment is implemented on the device");
+  if (opt->nb_env < 1 || opt->nb_env > kMaxEnvDevice)
+    return fail(MHY_ERR_UNSUPPORTED, "nb_env must be 1.." + std::to_string(kMaxEnvDevice) + " on the device");
+  for (int k = 0; k < opt->nb_env; ++k)
+    if (!(opt->adiabatic_cst[k] > 1.)) return fail(MHY_ERR_ARG, "adiabatic-cst must be > 1");
   if (opt->ordre_projection < 1 || opt->ordre_projection > 2)
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
@@ -153,7 +161,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   dm.Fy = (long long)dm.nx * (dm.ny + 1) * dm.nz;
   dm.F = dm.Fx + dm.Fy + (long long)dm.nx * dm.ny * (dm.nz + 1);
   Phys& ph = c->ph;
-  ph.gamma = opt->adiabatic_cst[0]; ph.threshold = opt->threshold; ph.cfl = opt->cfl;
+  ph.gamma = opt->adiabatic_cst[0];
+  c->K = opt->nb_env;
+  for (int k = 0; k < c->K; ++k) c->env.gamma[k] = opt->adiabatic_cst[k];
+  ph.threshold = opt->threshold; ph.cfl = opt->cfl;
   ph.deltat_min = opt->deltat_min; ph.deltat_max = opt->deltat_max; ph.final_time = opt->final_time;
   ph.lc_mode = opt->longueur_caracteristique; ph.pseudo_centree = opt->pseudo_centree;
   ph.ordre_projection = opt->ordre_projection; ph.limiteur_id = opt->projection_limiteur_id;
@@ -167,7 +178,15 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   A_(&c->x0, 3 * N); A_(&c->v, 3 * N); A_(&c->vh, 3 * N); A_(&c->nm, N); A_(&c->Gd, 3 * N); A_(&c->vnorm, N);
   A_(&c->ud[0], 5 * N); A_(&c->ud[1], 5 * N);
   A_(&c->rho, C); A_(&c->e, C); A_(&c->q, C); A_(&c->p, C); A_(&c->cs, C); A_(&c->mass, C); A_(&c->L, C);
-  A_(&c->Ve, C); A_(&c->dpf, C); A_(&c->xc, 3 * C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C); A_(&c->U[0], 4 * C); A_(&c->U[1], 4 * C);
+  const int K = c->K, NV = 3 * K + 1;
+  A_(&c->Ve, C); A_(&c->dpf, K * C); A_(&c->xc, 3 * C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C);
+  A_(&c->U[0], NV * C); A_(&c->U[1], NV * C);
+  if (K > 1) {
+    EnvState& ev = c->env;
+    A_(&ev.f, K * C); A_(&ev.x, K * C); A_(&ev.rho, K * C); A_(&ev.e, K * C); A_(&ev.p, K * C);
+    A_(&ev.cs, K * C); A_(&ev.q, K * C); A_(&ev.m, K * C); A_(&ev.fg, C); A_(&ev.xg, C); A_(&c->Vlag, C);
+    if (rc == MHY_OK) rc = c->alloc(&ev.mask, (size_t)C);
+  }
   A_(&c->n0, 3 * F);
   {
     const long long nf[3] = {dm.Fx, dm.Fy, dm.F - dm.Fx - dm.Fy};
@@ -236,7 +255,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.inv_dt = 1.0 / opt->deltat_init; s0.min_bits = 0x7fefffffffffffffull;
   err = cudaMemcpy(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  c->kernels_per_cycle = kKernelsPerCycle;
+  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv : kKernelsPerCycle;
   err = cudaDeviceSynchronize();  // the memsets above ran on the legacy stream
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   *out = c;
@@ -246,10 +265,54 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
 int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
   if (!c || !st || !st->fracvol || !st->density || !st->pressure || !st->velocity) return fail(MHY_ERR_ARG, "null argument");
   const long long C = c->dm.C, N = c->dm.N;
-  for (long long i = 0; i < C; ++i)
-    if (!(st->fracvol[i] > 0.)) return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
-  MHY_CUDA(cudaMemcpy(c->rho, st->density, C * sizeof(double), cudaMemcpyHostToDevice));
-  MHY_CUDA(cudaMemcpy(c->p, st->pressure, C * sizeof(double), cudaMemcpyHostToDevice));
+  const int K = c->K;
+  if (K == 1) {
+    for (long long i = 0; i < C; ++i)
+      if (!(st->fracvol[i] > 0.)) return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
+    MHY_CUDA(cudaMemcpy(c->rho, st->density, C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(c->p, st->pressure, C * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    // Environments from the volume fractions and the initial per-environment
+    // state, as HydroStartInit sets them up on the host (MahycoModule.cc:48-127
+    // with the test case's initMat/initVar): a pure cell takes its
+    // environment's density and pressure as global values; a mixed cell keeps
+    // f_k, rho_k, p_k per environment, the mass fractions f_k rho_k / sum f rho,
+    // and the averages sum f_k rho_k, sum f_k p_k as global values.
+    std::vector<uint32_t> mask(C, 0);
+    std::vector<double> rho(C, 0.), pg(C, 0.), f((size_t)K * C, 0.), x((size_t)K * C, 0.), r((size_t)K * C, 0.),
+        pk((size_t)K * C, 0.);
+    for (long long i = 0; i < C; ++i) {
+      uint32_t m = 0;
+      for (int k = 0; k < K; ++k) if (st->fracvol[(size_t)k * C + i] > 0.) m |= 1u << k;
+      if (!m) return fail(MHY_ERR_ARG, "a cell belongs to no environment (all fracvol <= 0)");
+      mask[i] = m;
+      if (__builtin_popcount(m) == 1) {
+        const int e = __builtin_ctz(m);
+        rho[i] = st->density[(size_t)e * C + i]; pg[i] = st->pressure[(size_t)e * C + i];
+      } else {
+        double rg = 0., pp = 0., mt = 0.;
+        for (int k = 0; k < K; ++k) if (m >> k & 1) {
+          const size_t o = (size_t)k * C + i;
+          const double fk = st->fracvol[o], rk = st->density[o], pk_ = st->pressure[o];
+          f[o] = fk; r[o] = rk; pk[o] = pk_;
+          rg += fk * rk; pp += fk * pk_; mt += fk * rk;
+        }
+        for (int k = 0; k < K; ++k) if (m >> k & 1) {
+          const size_t o = (size_t)k * C + i;
+          x[o] = f[o] * r[o] / mt;
+        }
+        rho[i] = rg; pg[i] = pp;
+      }
+    }
+    const EnvState& ev = c->env;
+    MHY_CUDA(cudaMemcpy(ev.mask, mask.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(c->rho, rho.data(), C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(c->p, pg.data(), C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(ev.f, f.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(ev.x, x.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(ev.rho, r.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpy(ev.p, pk.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
+  }
   std::vector<double> soa(3 * N);
   for (long long n = 0; n < N; ++n)
     for (int a = 0; a < 3; ++a) soa[a * N + n] = st->velocity[3 * n + a];
@@ -270,7 +333,8 @@ int mhy_hydro_start_init(mhy_ctx* c) {
   k_init_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, xc0, c->cqs, c->Ve, c->L, c->ph.lc_mode);
   k_init_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->x0, c->n0, xf0);
   k_init_outer_normals<<<blocks(dm.C), kThreads, 0, s>>>(dm, xc0, xf0, c->ofn);
-  k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph.gamma, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
+  if (c->K == 1) k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph.gamma, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
+  else launch_init_env(c->args(), s);
   k_node_mass<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->mass, c->nm);
   MHY_CUDA(cudaGetLastError());
   MHY_CUDA(cudaStreamSynchronize(s));
@@ -286,8 +350,16 @@ int mhy_hydro_start_init(mhy_ctx* c) {
 namespace {
 
 int launch_velocity(mhy_ctx* c) { launch_lagrange_nodes(c->args(), c->stream); return MHY_OK; }
-int launch_geometry(mhy_ctx* c) { launch_lagrange_cells(c->args(), c->stream); return MHY_OK; }
-int launch_remap_(mhy_ctx* c, int sens) { launch_remap(c->args(), sens, c->stream); return MHY_OK; }
+int launch_geometry(mhy_ctx* c) {
+  if (c->K == 1) launch_lagrange_cells(c->args(), c->stream);
+  else launch_lagrange_cells_env(c->args(), c->stream);
+  return MHY_OK;
+}
+int launch_remap_(mhy_ctx* c, int sens) {
+  if (c->K == 1) launch_remap(c->args(), sens, c->stream);
+  else launch_remap_env(c->args(), sens, c->stream);
+  return MHY_OK;
+}
 int launch_delta_t_(mhy_ctx* c) { launch_delta_t(c->args(), c->stream); return MHY_OK; }
 
 int launch_cycle(mhy_ctx* c, int sens) {
@@ -433,6 +505,58 @@ int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
     double* o = static_cast<double*>(dst);
     for (long long i = 0; i < n; ++i)
       for (int a = 0; a < 3; ++a) o[3 * i + a] = soa[a * n + i];
+  }
+  return MHY_OK;
+}
+
+int mhy_get_env_mask(mhy_ctx* c, uint32_t* dst, size_t bytes) {
+  if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  const long long C = c->dm.C;
+  if (bytes < (size_t)C * sizeof(uint32_t)) return fail(MHY_ERR_ARG, "destination too small");
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->K == 1) {
+    for (long long i = 0; i < C; ++i) dst[i] = 1u;
+    return MHY_OK;
+  }
+  MHY_CUDA(cudaMemcpy(dst, c->env.mask, C * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return MHY_OK;
+}
+
+int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
+  if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  if (env < 0 || env >= c->K) return fail(MHY_ERR_ARG, "environment index out of range");
+  const long long C = c->dm.C;
+  if (bytes < (size_t)C * sizeof(double)) return fail(MHY_ERR_ARG, "destination too small");
+  const EnvState& ev = c->env;
+  const double *glob = nullptr, *part = nullptr;
+  switch (field) {
+    case MHY_ENV_FRACVOL: glob = ev.fg; part = ev.f; break;
+    case MHY_ENV_DENSITY: glob = c->rho; part = ev.rho; break;
+    case MHY_ENV_INTERNAL_ENERGY: glob = c->e; part = ev.e; break;
+    case MHY_ENV_PRESSURE: glob = c->p; part = ev.p; break;
+    case MHY_ENV_SOUND_SPEED: glob = c->cs; part = ev.cs; break;
+    case MHY_ENV_MASS_FRACTION: glob = ev.xg; part = ev.x; break;
+    case MHY_ENV_CELL_MASS: glob = c->mass; part = ev.m; break;
+    default: return fail(MHY_ERR_ARG, "unknown environment field");
+  }
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  double* o = static_cast<double*>(dst);
+  if (c->K == 1) {
+    if (field == MHY_ENV_FRACVOL || field == MHY_ENV_MASS_FRACTION) {
+      for (long long i = 0; i < C; ++i) o[i] = 1.;
+      return MHY_OK;
+    }
+    MHY_CUDA(cudaMemcpy(o, glob, C * sizeof(double), cudaMemcpyDeviceToHost));
+    return MHY_OK;
+  }
+  std::vector<uint32_t> mask(C);
+  std::vector<double> g(C), pt(C);
+  MHY_CUDA(cudaMemcpy(mask.data(), ev.mask, C * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  MHY_CUDA(cudaMemcpy(g.data(), glob, C * sizeof(double), cudaMemcpyDeviceToHost));
+  MHY_CUDA(cudaMemcpy(pt.data(), part + (size_t)env * C, C * sizeof(double), cudaMemcpyDeviceToHost));
+  for (long long i = 0; i < C; ++i) {
+    const uint32_t m = mask[i];
+    o[i] = !(m >> env & 1) ? 0. : (__builtin_popcount(m) == 1 ? g[i] : pt[i]);
   }
   return MHY_OK;
 }

@@ -15,7 +15,8 @@
 //
 // Every expression keeps the operation order of the reference (see the
 // citations), so with --fmad=false the results equal the CPU oracle bit for bit.
-#include "mhy_kernels.cuh"
+#include "mhy_lagrange.cuh"
+#include "mhy_line.cuh"
 
 namespace mhy {
 
@@ -58,402 +59,6 @@ __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scala
   vh[n] = u.x; vh[dm.N + n] = u.y; vh[2 * dm.N + n] = u.z;
 }
 
-// ------------------------------------------------------------------------
-// Lagrange phase, cells: UpdatePosition (cell centre), ComputeGeometricValues,
-// UpdateDensity, ComputeArtificialViscosity, UpdateEnergyAndPressure (GP),
-// computeVariablesForRemap_PBorn0 and computeFaceQuantitesForRemap for the
-// cell's low faces, with the face-only terms of computeGradPhiFace and the
-// upwind reconstruction precomputed (dx_f, (x_f - x_c).n0 for both cells).
-// (MahycoModule.cc:913-928, 1054-1262, 1331-1370, 517-528, 1715-1726;
-// PrepareRemap.cc:33-55, 93-117, 311-332; RemapADIService.cc:171-172, 710.)
-__device__ __forceinline__ D3 load_xl(const Dims& dm, const double* __restrict__ x0, const double* __restrict__ vh,
-                                      double dt, long long n) {
-  return d3(x0[n], x0[dm.N + n], x0[2 * dm.N + n]) + dt * d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
-}
-
-// Half cross product 0.5 * (a - c) x (b - c) (MahycoModule.cc:2206-2239).
-__device__ __forceinline__ D3 half_cross(D3 a, D3 b, D3 c) { return 0.5 * cross(a - c, b - c); }
-
-// Corner vectors accumulated face by face.  Each corner's two six-term sums
-// of MahycoModule.cc:2242-2257 take two consecutive terms from each of its
-// three faces, in increasing face order, so adding them as the faces are
-// visited keeps the reference's order; a corner is finished as soon as its
-// third face is done.
-struct CornerAcc { D3 s1, s2; };
-__device__ __forceinline__ void acc_start(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) { a.s1 = t1 + t2; a.s2 = u1 + u2; }
-__device__ __forceinline__ void acc_add(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) {
-  a.s1 = a.s1 + t1; a.s1 = a.s1 + t2; a.s2 = a.s2 + u1; a.s2 = a.s2 + u2;
-}
-
-__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Scalars* __restrict__ S, Phys ph,
-    const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
-    const double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
-    const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
-    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= dm.nx) return;
-  const long long c = dm.cid(i, j, k);
-  const long long C = dm.C;
-  const double dt = S->dt;
-  D3 x[8];
-#pragma unroll
-  for (int a = 0; a < 8; ++a)
-    x[a] = load_xl(dm, x0, vh, dt, dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]));
-  D3 sm = d3(0., 0., 0.);
-#pragma unroll
-  for (int a = 0; a < 8; ++a) sm = sm + x[a];
-  const D3 xc = .125 * sm;
-  xcs[c] = xc.x; xcs[C + c] = xc.y; xcs[2 * C + c] = xc.z;
-
-  // corner vectors, face by face (face centres as in MahycoModule.cc:1080-1087)
-  const double t12 = 1. / 12.;
-  double dv[8];
-  auto finish = [&](int a, const CornerAcc& ac) {
-    const D3 o = t12 * (5. * ac.s1 + ac.s2);
-    cqs[(a * 3 + 0) * C + c] = o.x; cqs[(a * 3 + 1) * C + c] = o.y; cqs[(a * 3 + 2) * C + c] = o.z;
-    dv[a] = dot(x[a], o);
-  };
-  CornerAcc k0, k1, k2, k3, k4, k5, k6, k7;
-  {
-    const D3 c0 = 0.25 * (x[0] + x[3] + x[2] + x[1]);
-    const D3 n04 = half_cross(x[0], x[3], c0), n03 = half_cross(x[3], x[2], c0);
-    const D3 n02 = half_cross(x[2], x[1], c0), n01 = half_cross(x[1], x[0], c0);
-    acc_start(k0, n01, n04, n02, n03);
-    acc_start(k1, n01, n02, n04, n03);
-    acc_start(k2, n02, n03, n01, n04);
-    acc_start(k3, n03, n04, n01, n02);
-  }
-  {
-    const D3 c1 = 0.25 * (x[0] + x[4] + x[7] + x[3]);
-    const D3 n05 = half_cross(x[0], x[4], c1), n12 = half_cross(x[4], x[7], c1);
-    const D3 n08 = half_cross(x[7], x[3], c1), n04 = half_cross(x[3], x[0], c1);
-    acc_add(k0, n04, n05, n08, n12);
-    acc_add(k3, n08, n04, n05, n12);
-    acc_start(k4, n05, n12, n08, n04);
-    acc_start(k7, n08, n12, n04, n05);
-  }
-  {
-    const D3 c2 = 0.25 * (x[0] + x[1] + x[5] + x[4]);
-    const D3 n01 = half_cross(x[0], x[1], c2), n06 = half_cross(x[1], x[5], c2);
-    const D3 n09 = half_cross(x[5], x[4], c2), n05 = half_cross(x[4], x[0], c2);
-    acc_add(k0, n05, n01, n06, n09);
-    finish(0, k0);
-    acc_add(k1, n01, n06, n09, n05);
-    acc_add(k4, n05, n09, n01, n06);
-    acc_start(k5, n06, n09, n01, n05);
-  }
-  {
-    const D3 c3 = 0.25 * (x[4] + x[5] + x[6] + x[7]);
-    const D3 n09 = half_cross(x[4], x[5], c3), n10 = half_cross(x[5], x[6], c3);
-    const D3 n11 = half_cross(x[6], x[7], c3), n12 = half_cross(x[7], x[4], c3);
-    acc_add(k4, n09, n12, n10, n11);
-    finish(4, k4);
-    acc_add(k5, n09, n10, n12, n11);
-    acc_start(k6, n11, n10, n12, n09);
-    acc_add(k7, n12, n11, n09, n10);
-  }
-  {
-    const D3 c4 = 0.25 * (x[1] + x[2] + x[6] + x[5]);
-    const D3 n02 = half_cross(x[1], x[2], c4), n07 = half_cross(x[2], x[6], c4);
-    const D3 n10 = half_cross(x[6], x[5], c4), n06 = half_cross(x[5], x[1], c4);
-    acc_add(k1, n06, n02, n10, n07);
-    finish(1, k1);
-    acc_add(k2, n07, n02, n06, n10);
-    acc_add(k5, n10, n06, n07, n02);
-    finish(5, k5);
-    acc_add(k6, n10, n07, n06, n02);
-  }
-  {
-    const D3 c5 = 0.25 * (x[2] + x[3] + x[7] + x[6]);
-    const D3 n03 = half_cross(x[2], x[3], c5), n08 = half_cross(x[3], x[7], c5);
-    const D3 n11 = half_cross(x[7], x[6], c5), n07 = half_cross(x[6], x[2], c5);
-    acc_add(k2, n07, n03, n11, n08);
-    finish(2, k2);
-    acc_add(k3, n08, n03, n07, n11);
-    finish(3, k3);
-    acc_add(k6, n07, n11, n03, n08);
-    finish(6, k6);
-    acc_add(k7, n11, n08, n07, n03);
-    finish(7, k7);
-  }
-  double V = 0;
-#pragma unroll
-  for (int a = 0; a < 8; ++a) V += dv[a];
-  V *= 1. / 3;
-  double Lc;
-  if (ph.lc_mode == 0) Lc = pow_third(V);
-  else {
-    D3 fc[6];
-    face_centres(x, fc);
-    const double d1 = norm2(fc[0] - fc[3]), d2 = norm2(fc[2] - fc[5]), d3_ = norm2(fc[1] - fc[4]);
-    Lc = (d1 * d2 * d3_) / (d1 * d2 + d1 * d3_ + d2 * d3_);
-  }
-  L[c] = Lc;
-  {
-    const double inv_deltat = S->inv_dt;                        // 1.0 / dt
-    const double rn = rho[c];
-    const double nd = mass[c] / V;
-    const double irn = 1.0 / rn, ind = 1.0 / nd;
-    const double tau = 0.5 * (irn + ind);
-    const double itau = 1. / tau;
-    const double du = qdiv(inv_deltat * (ind - irn), tau, itau);
-    double qn = 0.;
-    const double g = ph.gamma;
-    if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-    const double en = compute_eint(ph.pseudo_centree != 0, g, q[c], qn, ind, irn, nd, p[c], e[c]);
-    U[c] = V;
-    U[C + c] = V * nd;
-    U[2 * C + c] = V * nd * en;
-    U[3 * C + c] = V * qn;
-  }
-  // Remap face data from this cell's nodes (PrepareRemap.cc:41-55, 105-117;
-  // RemapADIService.cc:710): for the low face of each direction (an inner
-  // face) |A| along d, u_f and (x_f - x_c).n0 with this cell as the next cell;
-  // for the high face (an inner face) (x_f - x_c).n0 with this cell as the
-  // previous one.  Face node order: X (0,3,7,4), Y (0,1,5,4), Z (0,1,2,3) low;
-  // X (1,2,6,5), Y (3,2,6,7), Z (4,5,6,7) high, in SN_trigo cell-node numbers.
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int id = d == 0 ? i : (d == 1 ? j : k);
-    const int lo[3][4] = {{0, 3, 7, 4}, {0, 1, 5, 4}, {0, 1, 2, 3}};
-    const int hi[3][4] = {{1, 2, 6, 5}, {3, 2, 6, 7}, {4, 5, 6, 7}};
-    const long long off = d == 0 ? 0 : (d == 1 ? dm.Fx : dm.Fx + dm.Fy);
-    if (id > 0) {
-      const long long f = dm.fid(d, i, j, k);
-      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
-      const D3 a0 = x[lo[d][0]], a1 = x[lo[d][1]], a2 = x[lo[d][2]], a3 = x[lo[d][3]];
-      D3 xf = d3(0., 0., 0.);
-      xf = xf + .25 * a0; xf = xf + .25 * a1; xf = xf + .25 * a2; xf = xf + .25 * a3;
-      D3 vs = d3(0., 0., 0.);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int a = lo[d][b];
-        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
-        vs = vs + d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]);
-      }
-      const D3 cr = 0.5 * cross(a2 - a0, a3 - a1);
-      double A = fabs(comp(cr, d));
-      if (!(fabs(comp(nrm, d)) >= 1.0E-10)) A = 0.;   // RemapADIService.cc:925 filter: no flux
-      const long long t = f - off;
-      fd.A[d][t] = A;
-      fd.u[d][t] = dot(.25 * vs, nrm);
-      fd.df[d][t] = dot(xf - xc, nrm);
-    }
-    if (id + 1 < dm.ncd(d)) {
-      const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
-      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
-      D3 xf = d3(0., 0., 0.);
-      xf = xf + .25 * x[hi[d][0]]; xf = xf + .25 * x[hi[d][1]]; xf = xf + .25 * x[hi[d][2]]; xf = xf + .25 * x[hi[d][3]];
-      fd.db[d][f - off] = dot(xf - xc, nrm);
-    }
-  }
-}
-
-
-// ------------------------------------------------------------------------
-// Directional sweeps.  The stencil of the remap runs along one direction d,
-// so each line of cells (or nodes) along d is independent.  A warp holds 32
-// consecutive items of one line, one per lane, exchanges neighbours with
-// shuffles and updates the 28 inner ones; a block holds 8 lines.
-//   d = x: the 8 lines are neighbouring rows and a lane's loads and stores
-//          are coalesced along x as they are.
-//   d = y, z: the 8 lines are 8 consecutive x at one (z or y), and a warp's
-//          items are a stride apart in memory.  The block therefore stages
-//          its 8 x 32 tile of every input array in shared memory with loads
-//          that run along x (8 doubles = 64 contiguous bytes per row), each
-//          warp reads its line from there, writes its results back into its
-//          own rows, and the block stores them along x again.
-// All index arithmetic is 32-bit (mhy_create bounds the mesh so that every
-// element offset fits).
-
-constexpr int kLineUpd = 28;    // items updated per warp (32 lanes, 2 halo lanes on each side)
-constexpr int kLineWarps = 8;   // warps (lines) per block
-// The sweeps are latency bound (long dependent chains of divisions and
-// shuffles per lane); 4 resident blocks (32 warps, 64 registers, a few bytes
-// of spill) per SM run them 15 % faster than the 2-3 blocks the compiler's
-// own register choice allows (Sedov 128^3 on B200).
-constexpr int kLineMinBlocks = 4;
-// Row length (doubles) of a staged tile [array][line][position].  Staging
-// stores by thread (x = tid % 8, p = tid / 8) hit address 36 x + p, whose
-// 8-byte bank pairs (4 x + p) mod 16 cover every pair exactly twice per warp,
-// and line reads run along p, so both are free of bank conflicts.
-constexpr int kTileLd = 36;
-constexpr int kTileArr = kLineWarps * kTileLd;   // doubles per staged array
-
-// remapVariables "moy" kernel for a single-environment cell and the PerfectGas
-// EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
-// PrepareRemap.cc:553-559).  out = rho, e, q, mass, p, c.
-__device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, double vol, const double u[4],
-                                              double out[6]) {
-  const double thr = ph.threshold;
-  const double U0 = u[0], U1 = u[1], U2 = u[2], U3 = u[3];
-  const double volt = 0. + U0, masset = 0. + U1;
-  const double unsurvolt = 1. / volt;
-  const double unsurvol = 1. / vol;
-  double fvol = U0 * unsurvolt;
-  if (fvol < thr) fvol = 0.;
-  const double somme_frac = 0. + fvol;
-  const double unsursomme_frac = 1. / somme_frac;
-  fvol = fvol * unsursomme_frac;
-  double mf = 1.;
-  if (masset != 0.) {
-    const double unsurmasset = 1. / masset;
-    mf = U1 * unsurmasset;
-    if (fvol < thr) mf = 0.;
-    const double fmasset = 0. + mf;
-    if (fmasset != 0.) { const double unsurfmasset = 1. / fmasset; mf = mf * unsurfmasset; }
-  } else {
-    atomicOr(&const_cast<Scalars*>(S)->status, MHY_STATUS_ZERO_MASS);
-  }
-  double de = 0.;
-  if (fvol > thr) { const double vn = U0 * vol * unsurvolt; de = U1 / vn; }
-  const double density_nplus1 = 0. + fvol * de;
-  const double cm = vol * density_nplus1;
-  double ee = 0.;
-  if (fvol > thr && U1 != 0.) ee = qdiv(U2, U1, 1. / masset);   // masset = 0 + U1 = U1
-  double energie = 0. + mf * ee;
-  const double pv = U3 * unsurvol;
-  const double pseudo = 0. + fvol * pv;
-  double r = de;
-  if (r < 0. || energie < 0.) { energie = 0.; r = 0.; }
-  const double g = ph.gamma;
-  const double pr = (g - 1.) * r * energie;
-  out[0] = r;
-  out[1] = energie;
-  out[2] = pseudo;
-  out[3] = mf * cm;
-  out[4] = pr;
-  out[5] = sqrt(g * pr / r);
-}
-
-// Phi = U / sum of the environment volumes = U / U0 for one environment
-// (RemapADIService.cc:962-970, PrepareRemap.cc:394-398); Phi0 = U0/U0 = 1.
-__device__ __forceinline__ void phi_of(const double U[4], double P[4]) {
-  const double U0 = U[0], r = 1.0 / U0;
-  P[0] = 1.0;
-  P[1] = qdiv(U[1], U0, r); P[2] = qdiv(U[2], U0, r); P[3] = qdiv(U[3], U0, r);
-}
-
-// Face gradients (R:174-177) of variables 1..3; variable 0 is zero.
-__device__ __forceinline__ void face_grad(bool inner, double dx, const double Pn[4], const double Pp[4], double g[4]) {
-  g[0] = 0.;
-  const double r = inner ? 1.0 / dx : 0.;
-#pragma unroll
-  for (int v = 1; v < 4; ++v) g[v] = inner ? qdiv(Pn[v] - Pp[v], dx, r) : 0.;
-}
-
-// Limited cell gradient from the back and front face gradients (R:497-506):
-//   gc = 0; if (gb != 0) gc += 0.5*(phi(gf/gb)*gb); if (gf != 0) gc += 0.5*(phi(gb/gf)*gf).
-// For minmod, phi(r) = max(0, min(1, r)): with finite gb, gf of opposite signs or
-// a zero the two terms are signed zeros and gc = +0; with equal signs the ratio
-// whose numerator is the smaller magnitude is the only one below 1, the other
-// term is exactly 0.5*g.  So one division gives the reference's bits.
-__device__ __forceinline__ double limited_one(int lim, double gb, double gf) {
-  if (lim == 0) {
-    if (gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.))) return 0.;
-    const bool fsmall = fabs(gf) < fabs(gb);
-    const double r = fsmall ? gf / gb : gb / gf;
-    const double t1 = fsmall ? 0.5 * (r * gb) : 0.5 * (1.0 * gb);
-    const double t2 = fsmall ? 0.5 * (1.0 * gf) : 0.5 * (r * gf);
-    return (0. + t1) + t2;
-  }
-  double gc = 0.;
-  if (gb != 0.) gc += 0.5 * (limiter(lim, gf / gb) * gb);
-  if (gf != 0.) gc += 0.5 * (limiter(lim, gb / gf) * gf);
-  return gc;
-}
-
-// Variable 0 (the volume) has Phi = U0/U0 = 1 on every cell of a
-// single-environment mesh, so its face gradients are zero and its limited
-// gradient is +0; only variables 1..3 are computed.
-__device__ __forceinline__ void limited_grad(int lim, const double gb[4], const double gf[4], double G[4]) {
-  G[0] = 0.;
-#pragma unroll
-  for (int v = 1; v < 4; ++v) G[v] = limited_one(lim, gb[v], gf[v]);
-}
-
-// Upwind face value (R:707-714): from the previous cell when u_f dx_f > 0.
-__device__ __forceinline__ void face_value(double order2, double u, double dx, double db, double df,
-                                           const double Pp[4], const double Gp[4], const double Pn[4],
-                                           const double Gn[4], double Pf[4]) {
-  const bool back = u * dx > 0.0;
-  const double dot_xf = back ? db : df;
-#pragma unroll
-  for (int v = 0; v < 4; ++v) Pf[v] = back ? (Pp[v] + order2 * dot_xf * Gp[v]) : (Pn[v] + order2 * dot_xf * Gn[v]);
-}
-
-// ---- cells ---------------------------------------------------------------
-// Inputs of one lane (one cell of a line along d).
-struct CellIn {
-  double U[4], xc[3];
-  double db, df, u, A, n[3];   // low face of the cell along d (inner faces only)
-  double ob, of;               // outward-normal component along d of the back and front faces
-  double vol;                  // initial cell volume (last sweep only)
-};
-constexpr int kCellOutLast = 7;   // rho, e, q, mass, p, c, dual mass flux
-constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
-
-// One line step of computeGradPhiFace, computeGradPhiCell, the upwind face
-// values and computeUremap_PBorn0 (RemapADIService.cc:91-271, 447-517, 658-720,
-// 909-987).  Every lane takes part in the shuffles; lanes with upd set get
-// their cell's results in out.  The boundary faces of d carry Phi_f = 0 and
-// contribute nothing.
-template <bool LAST>
-__device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
-                                          bool infr, bool upd, const CellIn& in, double* out) {
-  const double order2 = (double)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  double P[4] = {0., 0., 0., 0.};
-  if (valid) phi_of(in.U, P);
-  const unsigned full = 0xffffffffu;
-  const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
-               xpz = __shfl_up_sync(full, in.xc[2], 1);
-  // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172)
-  const double dx = inner ? dot(d3(in.xc[0], in.xc[1], in.xc[2]) - d3(xpx, xpy, xpz), d3(in.n[0], in.n[1], in.n[2]))
-                          : 0.;
-  double g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
-#pragma unroll
-  for (int v = 0; v < 4; ++v) Pp[v] = __shfl_up_sync(full, P[v], 1);
-  face_grad(inner, dx, P, Pp, g);
-#pragma unroll
-  for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
-  limited_grad(lim, g, gr, G);
-#pragma unroll
-  for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
-  if (inner) face_value(order2, in.u, dx, in.db, in.df, Pp, Gp, P, G, Pf);
-  else {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) Pf[v] = 0.;
-  }
-  double Pfn[4];
-#pragma unroll
-  for (int v = 0; v < 4; ++v) Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
-  const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
-  if (!upd) return;
-  // fluxes o*u*A*dt*Phi_f through the back and front faces, U -= sum, dual
-  // mass flux sum 0.5*flux*o, clamping of mass and energy (R:909-987)
-  const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
-  const double cf = infr ? in.of * un * An * dt : 0.;
-  double u[4], dpm = 0.;
-#pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    double flux_face = 0., dp = 0.;
-    if (inner) { const double fl = cb * Pf[v]; flux_face += fl; dp += 0.5 * fl * in.ob; }
-    if (infr) { const double fl = cf * Pfn[v]; flux_face += fl; dp += 0.5 * fl * in.of; }
-    u[v] = in.U[v] - flux_face;
-    if (v == 1) dpm = dp;
-  }
-  if (u[1] < 0.) u[1] = 0.;
-  if (u[2] < 0.) u[2] = 0.;
-  if (!LAST) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) out[v] = u[v];
-    out[4] = dpm;
-  } else {
-    finalize_cell(ph, S, in.vol, u, out);
-    out[6] = dpm;
-  }
-}
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
 template <bool LAST>
@@ -577,345 +182,6 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_c
   }
 }
 
-// ---- nodes ---------------------------------------------------------------
-// Dual update of one inner node (DualPhaseRemap.cc:382-521).
-__device__ __forceinline__ void dual_update(int D, double order2, double dt, double bfm, double ffm,
-                                            const double Pm[4], const double Pn[4], const double Pp[4],
-                                            const double Gm[3], const double Gn[3], const double Gp[3],
-                                            double xm, double xn, double xp, double ud[5]) {
-  const double u3 = ud[3] + (bfm - ffm);
-  const double pnd = Pn[D];
-  const double ufront = 0.5 * (pnd + pnd);                     // DualPhaseRemap.cc:391
-  const double sfront = (ufront > 0) ? 1.0 : -1.0;
-  const double uback = 0.5 * (Pm[D] + pnd);
-  const double sback = (uback > 0) ? 1.0 : -1.0;
-  const bool fup = ffm < 0., bup = bfm > 0.;
-  const double tf = sfront * (xp - xn) - dt * ufront;
-  const double tb = sback * (xn - xm) - dt * uback;
-  double out[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const double gfa = c < 3 ? (fup ? Gp[c] : Gn[c]) : 0.;    // index 4 never set (DualPhaseRemap.cc:771)
-    const double gba = c < 3 ? (bup ? Gm[c] : Gn[c]) : 0.;
-    const double FV = (fup ? Pp[c] : Pn[c]) + order2 * (0.5 * gfa * tf);
-    const double BV = (bup ? Pm[c] : Pn[c]) + order2 * (0.5 * gba * tb);
-    out[c] = ud[c < 3 ? c : 4] + (bfm * BV - ffm * FV);
-  }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) if (fabs(out[c]) < 1.e-300) out[c] = 0.;
-  ud[0] = out[0]; ud[1] = out[1]; ud[2] = out[2]; ud[3] = u3; ud[4] = out[3];
-}
-
-// One limited nodal gradient component (DualPhaseRemap.cc:736-777) from the
-// back and front differences; the terms are (0.5*phi(r))*g here, and the same
-// single-division reading of minmod applies.
-__device__ __forceinline__ double dual_limited(int lim, double gb, double gf) {
-  double g = 0.;
-  if (lim == 0) {
-    if (!(gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.)))) {
-      const bool fsmall = fabs(gf) < fabs(gb);
-      const double r = fsmall ? gf / gb : gb / gf;
-      const double t1 = fsmall ? 0.5 * r * gb : 0.5 * 1.0 * gb;
-      const double t2 = fsmall ? 0.5 * 1.0 * gf : 0.5 * r * gf;
-      g = (0. + t1) + t2;
-    }
-  } else {
-    if (gb != 0.) g += 0.5 * limiter(lim, gf / gb) * gb;
-    if (gf != 0.) g += 0.5 * limiter(lim, gb / gf) * gf;
-  }
-  return g;
-}
-
-// Inputs of one lane (one node of a line along d).
-struct NodeIn {
-  double vh[3];    // Lagrange velocity
-  double x0d;      // initial coordinate along d
-  double nm;       // node mass (first sweep)
-  double ud[5];    // U_dual (later sweeps)
-  double ffm;      // sum of 0.25 * dual mass flux of the 4 cells in front (DualPhaseRemap.cc:299-340)
-  double msum;     // sum of the masses of the up to 8 cells around the node (last sweep)
-};
-constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| on the last sweep
-
-// One line step of computeDualUremap and computeDualGradPhi_LimC
-// (DualPhaseRemap.cc:22-523, 700-778), then remapVariables for the node
-// velocity and mass on the last sweep (RemapADIFinal.cc:660-672, 697-719;
-// |v| is kept for the dt reduction, MahycoModule.cc:2053).  The state at the
-// start of a sweep is PrepareRemap.cc:411-433 on the first sweep or for nodes
-// not yet updated this cycle, else U_dual / m.  G holds the node's stale
-// gradient on entry and its gradient on return.
-template <int D, bool FIRST, bool LAST>
-__device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
-                                          bool upd, const NodeIn& in, double G[3], double* out) {
-  const double order2 = (double)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  const bool grad_on = ph.ordre_projection > 1;
-  double ud[5] = {0., 0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, x = 0.;
-  if (valid) {
-    const D3 u = d3(in.vh[0], in.vh[1], in.vh[2]);
-    if (FIRST) {
-      const double m = in.nm;
-      const double un = norm2(u);
-      ud[0] = m * u.x; ud[1] = m * u.y; ud[2] = m * u.z; ud[3] = m; ud[4] = 0.5 * m * un;
-      P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
-    } else {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) ud[c] = in.ud[c];
-      if (updated) {
-        const double m = ud[3], rm = 1.0 / m;
-        P[0] = qdiv(ud[0], m, rm); P[1] = qdiv(ud[1], m, rm); P[2] = qdiv(ud[2], m, rm); P[3] = qdiv(ud[4], m, rm);
-      } else {
-        P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
-      }
-    }
-    x = in.x0d + in.vh[D] * dt;
-  }
-  const unsigned full = 0xffffffffu;
-  double Pm[4], Pp[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) { Pm[c] = __shfl_up_sync(full, P[c], 1); Pp[c] = __shfl_down_sync(full, P[c], 1); }
-  const double xm = __shfl_up_sync(full, x, 1), xp = __shfl_down_sync(full, x, 1);
-  if (grad_on) {
-    // front difference quotient of this node = back difference quotient of the next
-    const double hf = xp - x, rf = 1.0 / hf;
-    double gf[3], gb[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gf[c] = qdiv(Pp[c] - P[c], hf, rf);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) gb[c] = __shfl_up_sync(full, gf[c], 1);
-    if (valid && inner) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) G[c] = dual_limited(lim, gb[c], gf[c]);
-    }
-  }
-  double Gm[3], Gp[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) { Gm[c] = __shfl_up_sync(full, G[c], 1); Gp[c] = __shfl_down_sync(full, G[c], 1); }
-  const double bfm = __shfl_up_sync(full, in.ffm, 1);  // back cells of node m = front cells of node m-1
-  if (!upd) return;
-  if (inner) dual_update(D, order2, dt, bfm, in.ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
-  if (!LAST) {
-#pragma unroll
-    for (int c = 0; c < 5; ++c) out[c] = ud[c];
-  } else {
-    const double m = ud[3];
-    D3 u;
-    if (m != 0.) {
-      const double rm = 1.0 / m;
-      u = d3(qdiv(ud[0], m, rm), qdiv(ud[1], m, rm), qdiv(ud[2], m, rm));
-    } else {
-      u = d3(in.vh[0], in.vh[1], in.vh[2]);
-    }
-    out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = .125 * in.msum; out[4] = norm2(u);
-  }
-}
-
-// inner along an earlier direction of this cycle: Phi_dual = U_dual / m there
-__device__ __forceinline__ bool node_updated(const Dims& dm, int D, int prev_inner, const int idx[3]) {
-  bool updated = false;
-#pragma unroll
-  for (int dd = 0; dd < 3; ++dd)
-    if (dd != D && (prev_inner >> dd & 1) && idx[dd] > 0 && idx[dd] < dm.ncd(dd)) updated = true;
-  return updated;
-}
-
-// the node lies on a boundary plane of another direction: its gradient is
-// kept for later cycles, where it is read as a stale value
-__device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int idx[3]) {
-  return (D != 0 && (idx[0] == 0 || idx[0] == dm.nx)) || (D != 1 && (idx[1] == 0 || idx[1] == dm.ny)) ||
-         (D != 2 && (idx[2] == 0 || idx[2] == dm.nz));
-}
-
-// Node sweep along x: lanes run along the rows of nodes.
-template <bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
-    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
-    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  const int lane = threadIdx.x & 31;
-  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
-  if (j > dm.ny) return;                               // whole warp leaves together
-  const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
-  const int m = blockIdx.x * kLineUpd - 2 + lane;      // position of this lane's node along x
-  const bool valid = m >= 0 && m <= nx;
-  const bool inner = m >= 1 && m <= nx - 1;
-  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
-  const int idx[3] = {valid ? m : 0, j, k};
-  const int n = idx[0] + (nx + 1) * (j + (ny + 1) * k);
-  const bool updated = node_updated(dm, 0, prev_inner, idx);
-  const bool grad_on = ph.ordre_projection > 1;
-  NodeIn in;
-  in.vh[0] = in.vh[1] = in.vh[2] = 0.; in.x0d = 0.; in.nm = 0.;
-  in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
-  double G[3] = {0., 0., 0.};
-  if (valid) {
-    in.vh[0] = vh[n]; in.vh[1] = vh[N + n]; in.vh[2] = vh[2 * N + n]; in.x0d = x0[n];
-    if (FIRST) in.nm = nm_in[n];
-    else {
-#pragma unroll
-      for (int c = 0; c < 5; ++c) in.ud[c] = udin[c * N + n];
-    }
-    // flux of the 4 cells in front (x index m), in the order of DualPhaseRemap.cc:299-340
-    // (s1 over y, s2 over z)
-    if (m < nx) {
-      double f = 0.;
-#pragma unroll
-      for (int s1 = -1; s1 <= 0; ++s1)
-#pragma unroll
-        for (int s2 = -1; s2 <= 0; ++s2) {
-          const int cj = j + s1, ck = k + s2;
-          if (cj >= 0 && cj < ny && ck >= 0 && ck < nz) f += 0.25 * dpf[m + nx * (cj + ny * ck)];
-        }
-      in.ffm = f;
-    }
-    if (!(inner && grad_on)) { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
-    if (LAST && upd) {
-      double sm = 0.;
-#pragma unroll
-      for (int dk = 1; dk >= 0; --dk)
-#pragma unroll
-        for (int dj = 1; dj >= 0; --dj)
-#pragma unroll
-          for (int di = 1; di >= 0; --di) {
-            const int ci = m - di, cj = j - dj, ck = k - dk;
-            if (ci < 0 || cj < 0 || ck < 0 || ci >= nx || cj >= ny || ck >= nz) continue;
-            sm += mass[ci + nx * (cj + ny * ck)];
-          }
-      in.msum = sm;
-    }
-  }
-  double out[kNodeOut];
-  node_line<0, FIRST, LAST>(ph, S->dt, valid, inner, updated, upd, in, G, out);
-  if (!upd) return;
-  if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
-  if (!LAST) {
-#pragma unroll
-    for (int c = 0; c < 5; ++c) udout[c * N + n] = out[c];
-  } else {
-    vout[n] = out[0]; vout[N + n] = out[1]; vout[2 * N + n] = out[2]; nm_out[n] = out[3]; vnorm[n] = out[4];
-  }
-}
-
-// Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
-// Block (bx, by, bz): node x = 8 bx .. 8 bx + 7, positions 28 by - 2 ..
-// 28 by + 29 along D, bz = the remaining node coordinate o (z for D = 1, y
-// for D = 2).  The cells around those nodes have x = 8 bx - 1 .. 8 bx + 7 and
-// o - 1 .. o along the remaining axis: their dual mass fluxes (and masses on
-// the last sweep) are staged as [o - 1 + q][x - 8 bx + 1][position], with zero
-// for cells outside the mesh (adding +0 to these sums changes no bit).
-template <int D, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
-    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
-    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  constexpr int NA = FIRST ? 5 : 9;                   // vh x3, x0[D], nm or U_dual x5
-  constexpr int NT = LAST ? 2 : 1;                    // cell tiles: dual mass flux (+ mass)
-  constexpr int CT = 2 * (kLineWarps + 1) * 32;       // elements of one cell tile
-  constexpr int CLd = 32;                             // row length of a cell tile
-  __shared__ double tile[NA * kTileArr];
-  __shared__ double ctile[NT * CT];
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
-  const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
-  const int nn = dm.ncd(D) + 1, no = D == 1 ? nz : ny;   // cells along D; cells along the remaining axis
-  auto node_id = [&](int i, int m) { return D == 1 ? i + (nx + 1) * (m + (ny + 1) * o) : i + (nx + 1) * (o + (ny + 1) * m); };
-  const int sx = tid & 7, sp = tid >> 3;
-  const int si = i0 + sx, sm_ = seg0 + sp;
-  const bool s_valid = si <= nx && sm_ >= 0 && sm_ < nn;
-  const int sn = s_valid ? node_id(si, sm_) : 0;
-  {
-    double v[NA];
-#pragma unroll
-    for (int a = 0; a < NA; ++a) v[a] = 0.;
-    if (s_valid) {
-      v[0] = vh[sn]; v[1] = vh[N + sn]; v[2] = vh[2 * N + sn]; v[3] = x0[D * N + sn];
-      if (FIRST) v[4] = nm_in[sn];
-      else {
-#pragma unroll
-        for (int c = 0; c < 5; ++c) v[4 + c] = udin[c * N + sn];
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < NA; ++a) tile[a * kTileArr + sx * kTileLd + sp] = v[a];
-    // cell tiles: element e = (q * 9 + xx) * 32 + p, loaded with xx fastest
-    for (int e = tid; e < CT; e += 32 * kLineWarps) {
-      const int xx = e % (kLineWarps + 1), r = e / (kLineWarps + 1);
-      const int p = r & 31, q = r >> 5;
-      const int ci = i0 - 1 + xx, cd = seg0 + p, co = o - 1 + q;
-      const bool cv = ci >= 0 && ci < nx && cd >= 0 && cd < nn - 1 && co >= 0 && co < no;
-      const int c = D == 1 ? ci + nx * (cd + ny * co) : ci + nx * (co + ny * cd);
-      const int at = (q * (kLineWarps + 1) + xx) * CLd + p;
-      ctile[at] = cv ? dpf[c] : 0.;
-      if (LAST) ctile[CT + at] = cv ? mass[c] : 0.;
-    }
-  }
-  __syncthreads();
-  const int m = seg0 + lane;
-  const int i = i0 + w;
-  const bool valid = i <= nx && m >= 0 && m < nn;
-  const bool inner = i <= nx && m >= 1 && m <= nn - 2;
-  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
-  int idx[3];
-  idx[0] = i; idx[D] = m; idx[3 - D] = o;               // D = 1: (i, m, o); D = 2: (i, o, m)
-  const bool updated = node_updated(dm, D, prev_inner, idx);
-  const bool grad_on = ph.ordre_projection > 1;
-  double* row = tile + w * kTileLd + lane;
-  NodeIn in;
-  in.vh[0] = row[0]; in.vh[1] = row[kTileArr]; in.vh[2] = row[2 * kTileArr]; in.x0d = row[3 * kTileArr];
-  in.nm = FIRST ? row[4 * kTileArr] : 0.;
-#pragma unroll
-  for (int c = 0; c < 5; ++c) in.ud[c] = FIRST ? 0. : row[(4 + c) * kTileArr];
-  // cells in front of the node along D have index m along D; transverse
-  // (x - 1, x) = columns (w, w + 1) and (o - 1, o) = tile rows (0, 1)
-  const double* cr = ctile + w * CLd + lane;
-  constexpr int QS = (kLineWarps + 1) * CLd;          // stride between the two tile rows
-  const double f00 = cr[0], f01 = cr[CLd], f10 = cr[QS], f11 = cr[QS + CLd];   // f[q][dx]
-  // DualPhaseRemap.cc:299-340 order: s1 over d1 = (D+1)%3, s2 over d2 = (D+2)%3.
-  // D = 1: s1 over z (q), s2 over x; D = 2: s1 over x, s2 over y (q).
-  double f = 0.;
-  if (D == 1) { f += 0.25 * f00; f += 0.25 * f01; f += 0.25 * f10; f += 0.25 * f11; }
-  else { f += 0.25 * f00; f += 0.25 * f10; f += 0.25 * f01; f += 0.25 * f11; }
-  in.ffm = (valid && m < nn - 1) ? f : 0.;
-  in.msum = 0.;
-  if (LAST) {
-    const double* mr = cr + CT;
-    const double a00 = mr[0], a01 = mr[CLd], a10 = mr[QS], a11 = mr[QS + CLd];   // cells at index m along D
-    const unsigned full = 0xffffffffu;
-    const double b00 = __shfl_up_sync(full, a00, 1), b01 = __shfl_up_sync(full, a01, 1),
-                 b10 = __shfl_up_sync(full, a10, 1), b11 = __shfl_up_sync(full, a11, 1);   // index m - 1
-    // increasing cell id: z outer, y, x inner
-    double sm = 0.;
-    if (D == 1) {   // (x, y=m-1|m, z=o-1|o): q = z
-      sm += b00; sm += b01; sm += a00; sm += a01; sm += b10; sm += b11; sm += a10; sm += a11;
-    } else {        // (x, y=o-1|o, z=m-1|m): q = y
-      sm += b00; sm += b01; sm += b10; sm += b11; sm += a00; sm += a01; sm += a10; sm += a11;
-    }
-    in.msum = sm;
-  }
-  double G[3] = {0., 0., 0.};
-  const int n = valid ? node_id(i, m) : 0;
-  if (valid && !(inner && grad_on)) { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
-  double out[kNodeOut];
-  node_line<D, FIRST, LAST>(ph, S->dt, valid, inner, updated, upd, in, G, out);
-  if (upd) {
-    if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
-    // each lane overwrites only the tile column it read itself
-#pragma unroll
-    for (int c = 0; c < kNodeOut; ++c) row[c * kTileArr] = out[c];
-  }
-  __syncthreads();
-  if (!(s_valid && sp >= 2 && sp < 2 + kLineUpd)) return;
-  const double* r = tile + sx * kTileLd + sp;
-  if (!LAST) {
-#pragma unroll
-    for (int c = 0; c < 5; ++c) udout[c * N + sn] = r[c * kTileArr];
-  } else {
-    vout[sn] = r[0]; vout[N + sn] = r[kTileArr]; vout[2 * N + sn] = r[2 * kTileArr];
-    nm_out[sn] = r[3 * kTileArr]; vnorm[sn] = r[4 * kTileArr];
-  }
-}
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
@@ -936,30 +202,6 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
   }
 }
 
-template <int D, bool FIRST, bool LAST>
-static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
-  const Dims& dm = a.dm;
-  const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
-  const int T = 32 * kLineWarps;
-  if constexpr (D == 0) {
-    const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
-    k_cyc_sweep_nodes_x<FIRST, LAST><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd,
-                                                     a.st.mass, a.v, a.nm, a.vnorm);
-  } else {
-    const dim3 g((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, (D == 1 ? dm.nz : dm.ny) + 1);
-    k_cyc_sweep_nodes_t<D, FIRST, LAST><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf,
-                                                        a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
-  }
-}
-
-template <int D>
-static void sweep_nodes_d(const CycleArgs& a, bool first, bool last, int prev, const double* udin, double* udout,
-                          cudaStream_t s) {
-  if (first) sweep_nodes_launch<D, true, false>(a, prev, udin, udout, s);
-  else if (last) sweep_nodes_launch<D, false, true>(a, prev, udin, udout, s);
-  else sweep_nodes_launch<D, false, false>(a, prev, udin, udout, s);
-}
-
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbn((a.dm.nx + 1 + 127) / 128, a.dm.ny + 1, a.dm.nz + 1);
   k_cyc_lagrange_nodes<<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh);
@@ -967,8 +209,8 @@ void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
 
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
-  k_cyc_lagrange_cells<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
-                                           a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd);
+  k_cyc_lagrange_cells<1><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
+                                              a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag);
 }
 
 // Three sweeps d = (i + sens) % 3 (RemapADIService.cc:28-30).  U: Lagrange
@@ -987,9 +229,7 @@ void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
     if (d == 0) sweep_cells_d<0>(a, last, uin, uout, s);
     else if (d == 1) sweep_cells_d<1>(a, last, uin, uout, s);
     else sweep_cells_d<2>(a, last, uin, uout, s);
-    if (d == 0) sweep_nodes_d<0>(a, first, last, prev, udin, udout, s);
-    else if (d == 1) sweep_nodes_d<1>(a, first, last, prev, udin, udout, s);
-    else sweep_nodes_d<2>(a, first, last, prev, udin, udout, s);
+    sweep_nodes<1>(a, d, first, last, prev, udin, udout, s);
     prev |= 1 << d;
   }
 }

@@ -48,6 +48,21 @@ struct CellState {
   const double* Ve;
 };
 
+// Environments (materials) of a mesh with K > 1 of them.  A cell that
+// belongs to one environment only keeps that environment's values in the
+// global cell arrays (CellState); a cell that belongs to several ("mixed")
+// keeps each environment's values in the [K][C] planes below (Arcane's
+// partial values, accenv/MultiEnvUtils.h:303-442) and the mixed averages in
+// the global arrays.  fg and xg are the global volume and mass fractions.
+struct EnvState {
+  uint32_t* mask;       // bit k set: the cell belongs to environment k
+  double *f, *x;        // [K][C] volume fraction, mass fraction
+  double *rho, *e, *p, *cs, *q, *m;   // [K][C] density, specific internal energy, pressure, sound speed,
+                                      // pseudo-viscosity, mass
+  double *fg, *xg;      // [C]
+  double gamma[MHY_MAX_ENV];
+};
+
 struct CycleArgs {
   Dims dm;
   Scalars* S;
@@ -60,6 +75,9 @@ struct CycleArgs {
   double* ud[2];
   FaceData fd;
   CellState st;
+  int K;                // number of environments
+  EnvState env;         // K > 1 only
+  double* Vlag;         // Lagrangian cell volume (K > 1: divisor of Phi on the first sweep)
 };
 
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s);
@@ -67,6 +85,12 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s);
 void launch_remap(const CycleArgs& a, int sens, cudaStream_t s);
 void launch_delta_t(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycle = 10;
+// meshes with 2..kMaxEnvDevice environments (mhy_multi.cu)
+constexpr int kMaxEnvDevice = 4;
+void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s);
+void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s);
+void launch_init_env(const CycleArgs& a, cudaStream_t s);
+constexpr int kKernelsPerCycleEnv = 11;
 
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);
 __global__ void k_init_faces(Dims dm, const double* x0, double* n0, double* xf0);

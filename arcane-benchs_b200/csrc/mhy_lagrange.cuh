@@ -1,0 +1,272 @@
+// mhy_lagrange.cuh -- the Lagrange-phase cell kernel (geometry, corner
+// vectors, density, pseudo-viscosity, energy, remap variables and the face
+// data of the remap), templated on the number of environments K.
+#pragma once
+
+#include "mhy_kernels.cuh"
+
+namespace mhy {
+
+// ------------------------------------------------------------------------
+// Lagrange phase, cells: UpdatePosition (cell centre), ComputeGeometricValues,
+// UpdateDensity, ComputeArtificialViscosity, UpdateEnergyAndPressure (GP),
+// computeVariablesForRemap_PBorn0 and computeFaceQuantitesForRemap for the
+// cell's low faces, with the face-only terms of computeGradPhiFace and the
+// upwind reconstruction precomputed (dx_f, (x_f - x_c).n0 for both cells).
+// (MahycoModule.cc:913-928, 1054-1262, 1331-1370, 517-528, 1715-1726;
+// PrepareRemap.cc:33-55, 93-117, 311-332; RemapADIService.cc:171-172, 710.)
+__device__ __forceinline__ D3 load_xl(const Dims& dm, const double* __restrict__ x0, const double* __restrict__ vh,
+                                      double dt, long long n) {
+  return d3(x0[n], x0[dm.N + n], x0[2 * dm.N + n]) + dt * d3(vh[n], vh[dm.N + n], vh[2 * dm.N + n]);
+}
+
+// Half cross product 0.5 * (a - c) x (b - c) (MahycoModule.cc:2206-2239).
+__device__ __forceinline__ D3 half_cross(D3 a, D3 b, D3 c) { return 0.5 * cross(a - c, b - c); }
+
+// Corner vectors accumulated face by face.  Each corner's two six-term sums
+// of MahycoModule.cc:2242-2257 take two consecutive terms from each of its
+// three faces, in increasing face order, so adding them as the faces are
+// visited keeps the reference's order; a corner is finished as soon as its
+// third face is done.
+struct CornerAcc { D3 s1, s2; };
+__device__ __forceinline__ void acc_start(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) { a.s1 = t1 + t2; a.s2 = u1 + u2; }
+__device__ __forceinline__ void acc_add(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) {
+  a.s1 = a.s1 + t1; a.s1 = a.s1 + t2; a.s2 = a.s2 + u1; a.s2 = a.s2 + u2;
+}
+
+// Lagrange thermodynamics of a mesh with K > 1 environments, then the remap
+// variables (MahycoModule.cc:1331-1426 updateDensity, :454-578
+// computeArtificialViscosity, :1659-1770 updateEnergyAndPressureforGP,
+// PrepareRemap.cc:258-437 computeVariablesForRemap_PBorn0).  Pure cells take
+// the single-environment formulas with their environment's gamma; a mixed
+// cell works environment by environment on V_k = f_k V (MahycoModule.cc:1274-1295).
+// U holds the 3K+1 non-zero remap variables [V_k | V_k rho_k | V_k rho_k e_k |
+// V q] as planes; V is kept in Vlag, the divisor of Phi on the first sweep.
+// The global density m/V is stored for every cell: the remap keeps it in a
+// mixed cell whose fractions leave one environment only (RemapADIFinal.cc:561-562).
+template <int K>
+__device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalars* S, const EnvState& env, int c,
+                                                    int C, double V, double Lc, double* __restrict__ rho,
+                                                    const double* __restrict__ e, const double* __restrict__ q,
+                                                    const double* __restrict__ p, const double* __restrict__ cs,
+                                                    const double* __restrict__ mass, double* __restrict__ U,
+                                                    double* __restrict__ Vlag) {
+  constexpr int NV = 3 * K + 1;
+  const double inv_deltat = S->inv_dt;
+  const double rn = rho[c];
+  const double nd = mass[c] / V;
+  const double irn = 1.0 / rn, ind = 1.0 / nd;
+  const double tau = 0.5 * (irn + ind);
+  const double itau = 1. / tau;
+  const double du = qdiv(inv_deltat * (ind - irn), tau, itau);
+  const uint32_t mk = env.mask[c];
+  const bool pc = ph.pseudo_centree != 0;
+  double u[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u[v] = 0.;
+  if (__popc(mk) == 1) {
+    const int ke = __ffs(mk) - 1;
+    const double g = env.gamma[ke];
+    double qn = 0.;
+    if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
+    const double en = compute_eint(pc, g, q[c], qn, ind, irn, nd, p[c], e[c]);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k == ke) { u[k] = V; u[K + k] = V * nd; u[2 * K + k] = V * nd * en; }
+    u[3 * K] = V * qn;
+  } else {
+    const double csc = cs[c];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!(mk >> k & 1)) continue;
+      const int o = k * C + c;
+      const double vk = env.f[o] * V;
+      const double rk = env.m[o] / vk;
+      const double irnk = 1.0 / env.rho[o], irk = 1.0 / rk;
+      const double tauk = 0.5 * (irnk + irk);
+      const double g = env.gamma[k];
+      double qk = 0.;
+      if (du < 0.0) qk = 1. / tauk * (-0.5 * Lc * csc * du + (g + 1) / 2.0 * Lc * Lc * du * du);
+      const double ek = compute_eint(pc, g, env.q[o], qk, irk, irnk, rk, env.p[o], env.e[o]);
+      u[k] = vk;
+      u[K + k] = vk * rk;
+      u[2 * K + k] = vk * rk * ek;
+      u[3 * K] = vk * qk;                                        // the last environment wins (P:318-330)
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) U[v * C + c] = u[v];
+  Vlag[c] = V;
+  rho[c] = nd;
+}
+
+template <int K>
+__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Scalars* __restrict__ S, Phys ph,
+    const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
+    double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
+    const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
+    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
+    EnvState env, double* __restrict__ Vlag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= dm.nx) return;
+  const long long c = dm.cid(i, j, k);
+  const long long C = dm.C;
+  const double dt = S->dt;
+  D3 x[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    x[a] = load_xl(dm, x0, vh, dt, dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]));
+  D3 sm = d3(0., 0., 0.);
+#pragma unroll
+  for (int a = 0; a < 8; ++a) sm = sm + x[a];
+  const D3 xc = .125 * sm;
+  xcs[c] = xc.x; xcs[C + c] = xc.y; xcs[2 * C + c] = xc.z;
+
+  // corner vectors, face by face (face centres as in MahycoModule.cc:1080-1087)
+  const double t12 = 1. / 12.;
+  double dv[8];
+  auto finish = [&](int a, const CornerAcc& ac) {
+    const D3 o = t12 * (5. * ac.s1 + ac.s2);
+    cqs[(a * 3 + 0) * C + c] = o.x; cqs[(a * 3 + 1) * C + c] = o.y; cqs[(a * 3 + 2) * C + c] = o.z;
+    dv[a] = dot(x[a], o);
+  };
+  CornerAcc k0, k1, k2, k3, k4, k5, k6, k7;
+  {
+    const D3 c0 = 0.25 * (x[0] + x[3] + x[2] + x[1]);
+    const D3 n04 = half_cross(x[0], x[3], c0), n03 = half_cross(x[3], x[2], c0);
+    const D3 n02 = half_cross(x[2], x[1], c0), n01 = half_cross(x[1], x[0], c0);
+    acc_start(k0, n01, n04, n02, n03);
+    acc_start(k1, n01, n02, n04, n03);
+    acc_start(k2, n02, n03, n01, n04);
+    acc_start(k3, n03, n04, n01, n02);
+  }
+  {
+    const D3 c1 = 0.25 * (x[0] + x[4] + x[7] + x[3]);
+    const D3 n05 = half_cross(x[0], x[4], c1), n12 = half_cross(x[4], x[7], c1);
+    const D3 n08 = half_cross(x[7], x[3], c1), n04 = half_cross(x[3], x[0], c1);
+    acc_add(k0, n04, n05, n08, n12);
+    acc_add(k3, n08, n04, n05, n12);
+    acc_start(k4, n05, n12, n08, n04);
+    acc_start(k7, n08, n12, n04, n05);
+  }
+  {
+    const D3 c2 = 0.25 * (x[0] + x[1] + x[5] + x[4]);
+    const D3 n01 = half_cross(x[0], x[1], c2), n06 = half_cross(x[1], x[5], c2);
+    const D3 n09 = half_cross(x[5], x[4], c2), n05 = half_cross(x[4], x[0], c2);
+    acc_add(k0, n05, n01, n06, n09);
+    finish(0, k0);
+    acc_add(k1, n01, n06, n09, n05);
+    acc_add(k4, n05, n09, n01, n06);
+    acc_start(k5, n06, n09, n01, n05);
+  }
+  {
+    const D3 c3 = 0.25 * (x[4] + x[5] + x[6] + x[7]);
+    const D3 n09 = half_cross(x[4], x[5], c3), n10 = half_cross(x[5], x[6], c3);
+    const D3 n11 = half_cross(x[6], x[7], c3), n12 = half_cross(x[7], x[4], c3);
+    acc_add(k4, n09, n12, n10, n11);
+    finish(4, k4);
+    acc_add(k5, n09, n10, n12, n11);
+    acc_start(k6, n11, n10, n12, n09);
+    acc_add(k7, n12, n11, n09, n10);
+  }
+  {
+    const D3 c4 = 0.25 * (x[1] + x[2] + x[6] + x[5]);
+    const D3 n02 = half_cross(x[1], x[2], c4), n07 = half_cross(x[2], x[6], c4);
+    const D3 n10 = half_cross(x[6], x[5], c4), n06 = half_cross(x[5], x[1], c4);
+    acc_add(k1, n06, n02, n10, n07);
+    finish(1, k1);
+    acc_add(k2, n07, n02, n06, n10);
+    acc_add(k5, n10, n06, n07, n02);
+    finish(5, k5);
+    acc_add(k6, n10, n07, n06, n02);
+  }
+  {
+    const D3 c5 = 0.25 * (x[2] + x[3] + x[7] + x[6]);
+    const D3 n03 = half_cross(x[2], x[3], c5), n08 = half_cross(x[3], x[7], c5);
+    const D3 n11 = half_cross(x[7], x[6], c5), n07 = half_cross(x[6], x[2], c5);
+    acc_add(k2, n07, n03, n11, n08);
+    finish(2, k2);
+    acc_add(k3, n08, n03, n07, n11);
+    finish(3, k3);
+    acc_add(k6, n07, n11, n03, n08);
+    finish(6, k6);
+    acc_add(k7, n11, n08, n07, n03);
+    finish(7, k7);
+  }
+  double V = 0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) V += dv[a];
+  V *= 1. / 3;
+  double Lc;
+  if (ph.lc_mode == 0) Lc = pow_third(V);
+  else {
+    D3 fc[6];
+    face_centres(x, fc);
+    const double d1 = norm2(fc[0] - fc[3]), d2 = norm2(fc[2] - fc[5]), d3_ = norm2(fc[1] - fc[4]);
+    Lc = (d1 * d2 * d3_) / (d1 * d2 + d1 * d3_ + d2 * d3_);
+  }
+  L[c] = Lc;
+  if constexpr (K == 1) {
+    const double inv_deltat = S->inv_dt;                        // 1.0 / dt
+    const double rn = rho[c];
+    const double nd = mass[c] / V;
+    const double irn = 1.0 / rn, ind = 1.0 / nd;
+    const double tau = 0.5 * (irn + ind);
+    const double itau = 1. / tau;
+    const double du = qdiv(inv_deltat * (ind - irn), tau, itau);
+    double qn = 0.;
+    const double g = ph.gamma;
+    if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
+    const double en = compute_eint(ph.pseudo_centree != 0, g, q[c], qn, ind, irn, nd, p[c], e[c]);
+    U[c] = V;
+    U[C + c] = V * nd;
+    U[2 * C + c] = V * nd * en;
+    U[3 * C + c] = V * qn;
+  } else {
+    lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag);
+  }
+  // Remap face data from this cell's nodes (PrepareRemap.cc:41-55, 105-117;
+  // RemapADIService.cc:710): for the low face of each direction (an inner
+  // face) |A| along d, u_f and (x_f - x_c).n0 with this cell as the next cell;
+  // for the high face (an inner face) (x_f - x_c).n0 with this cell as the
+  // previous one.  Face node order: X (0,3,7,4), Y (0,1,5,4), Z (0,1,2,3) low;
+  // X (1,2,6,5), Y (3,2,6,7), Z (4,5,6,7) high, in SN_trigo cell-node numbers.
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int id = d == 0 ? i : (d == 1 ? j : k);
+    const int lo[3][4] = {{0, 3, 7, 4}, {0, 1, 5, 4}, {0, 1, 2, 3}};
+    const int hi[3][4] = {{1, 2, 6, 5}, {3, 2, 6, 7}, {4, 5, 6, 7}};
+    const long long off = d == 0 ? 0 : (d == 1 ? dm.Fx : dm.Fx + dm.Fy);
+    if (id > 0) {
+      const long long f = dm.fid(d, i, j, k);
+      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
+      const D3 a0 = x[lo[d][0]], a1 = x[lo[d][1]], a2 = x[lo[d][2]], a3 = x[lo[d][3]];
+      D3 xf = d3(0., 0., 0.);
+      xf = xf + .25 * a0; xf = xf + .25 * a1; xf = xf + .25 * a2; xf = xf + .25 * a3;
+      D3 vs = d3(0., 0., 0.);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int a = lo[d][b];
+        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+        vs = vs + d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]);
+      }
+      const D3 cr = 0.5 * cross(a2 - a0, a3 - a1);
+      double A = fabs(comp(cr, d));
+      if (!(fabs(comp(nrm, d)) >= 1.0E-10)) A = 0.;   // RemapADIService.cc:925 filter: no flux
+      const long long t = f - off;
+      fd.A[d][t] = A;
+      fd.u[d][t] = dot(.25 * vs, nrm);
+      fd.df[d][t] = dot(xf - xc, nrm);
+    }
+    if (id + 1 < dm.ncd(d)) {
+      const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
+      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
+      D3 xf = d3(0., 0., 0.);
+      xf = xf + .25 * x[hi[d][0]]; xf = xf + .25 * x[hi[d][1]]; xf = xf + .25 * x[hi[d][2]]; xf = xf + .25 * x[hi[d][3]];
+      fd.db[d][f - off] = dot(xf - xc, nrm);
+    }
+  }
+}
+
+
+}  // namespace mhy

@@ -1,0 +1,530 @@
+// mhy_multi.cu -- the cycle of a mesh with K = 2..4 environments (materials),
+// each an ideal gas with its own adiabatic constant.
+//
+// Eleven launches per cycle: the Lagrange node kernel (shared with K = 1),
+// k_cyc_lagrange_cells<K>, three directional sweeps of cells and of nodes,
+// k_env_finalize_cells<K> between the last cell sweep and the last node sweep,
+// and the dt reduction.
+//   - Remap variables: the 3K+1 non-zero components of U
+//     (V_k, V_k rho_k, V_k rho_k e_k for each environment, then V q) as planes
+//     of C doubles (PrepareRemap.cc:318-330, 360-372); Phi = U / V on the first
+//     sweep and U / sum_k V_k afterwards (PrepareRemap.cc:394-398,
+//     RemapADIService.cc:962-970).  No component is constant here, so every
+//     one gets gradients, limiters and fluxes.
+//   - Dual mass flux: one plane per environment (the mass variables), summed
+//     environment by environment by the node sweeps (DualPhaseRemap.cc:299-340).
+//   - Environment membership changes (RemapADIFinal.cc:94-226) depend only on
+//     the cell's own remapped U, so k_env_finalize_cells decides them cell by
+//     cell on the device, with the remapVariables "moy" kernel
+//     (RemapADIFinal.cc:406-644), the PerfectGas EOS per environment and the
+//     mixed-cell pressure and sound speed (MahycoModule.cc:1836-1915) in the
+//     same thread: no host round trip and no list rebuild.
+// The operation order is the reference's throughout (the CPU oracle matches
+// bit for bit).
+#include <mutex>
+
+#include "mhy_lagrange.cuh"
+#include "mhy_line.cuh"
+
+namespace mhy {
+
+// The K-environment sweeps carry 3K+1 components per lane; two resident
+// blocks (128 registers) per SM keep them from spilling.
+constexpr int kEnvMinBlocks = 2;
+
+template <int K>
+struct CellInK {
+  double U[3 * K + 1], xc[3];
+  double db, df, u, A, n[3];   // low face of the cell along d (inner faces only)
+  double ob, of;               // outward-normal component along d of the back and front faces
+  double den;                  // divisor of Phi on the first sweep: the Lagrangian volume
+};
+
+// One line step of the remap of a K-environment cell (RemapADIService.cc:91-271,
+// 447-517, 658-720, 883-1040).  out = the 3K+1 updated components, then the
+// K dual mass fluxes.
+template <int K, bool FIRST>
+__device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
+                                              bool upd, const CellInK<K>& in, double* out) {
+  constexpr int NV = 3 * K + 1;
+  const double order2 = (double)(ph.ordre_projection - 1);
+  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  double P[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) P[v] = 0.;
+  if (valid) {
+    double den;
+    if (FIRST) den = in.den;
+    else {
+      den = 0.;
+#pragma unroll
+      for (int k = 0; k < K; ++k) den += in.U[k];
+    }
+    const double r = 1.0 / den;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) P[v] = qdiv(in.U[v], den, r);
+  }
+  const unsigned full = 0xffffffffu;
+  const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
+               xpz = __shfl_up_sync(full, in.xc[2], 1);
+  const double dx = inner ? dot(d3(in.xc[0], in.xc[1], in.xc[2]) - d3(xpx, xpy, xpz), d3(in.n[0], in.n[1], in.n[2]))
+                          : 0.;
+  const double rdx = inner ? 1.0 / dx : 0.;
+  double G[NV], Pp[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    Pp[v] = __shfl_up_sync(full, P[v], 1);
+    const double g = inner ? qdiv(P[v] - Pp[v], dx, rdx) : 0.;
+    const double gr = __shfl_down_sync(full, g, 1);
+    G[v] = limited_one(lim, g, gr);
+  }
+  const bool back = in.u * dx > 0.0;
+  const double dot_xf = back ? in.db : in.df;
+  double Pf[NV], Pfn[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double Gp = __shfl_up_sync(full, G[v], 1);
+    Pf[v] = inner ? (back ? (Pp[v] + order2 * dot_xf * Gp) : (P[v] + order2 * dot_xf * G[v])) : 0.;
+    Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
+  }
+  const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
+  if (!upd) return;
+  const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
+  const double cf = infr ? in.of * un * An * dt : 0.;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double flux_face = 0., dp = 0.;
+    if (inner) { const double fl = cb * Pf[v]; flux_face += fl; dp += 0.5 * fl * in.ob; }
+    if (infr) { const double fl = cf * Pfn[v]; flux_face += fl; dp += 0.5 * fl * in.of; }
+    out[v] = in.U[v] - flux_face;
+    if (v >= K && v < 2 * K) out[NV + v - K] = dp;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (out[K + k] < 0.) out[K + k] = 0.;
+    if (out[2 * K + k] < 0.) out[2 * K + k] = 0.;
+  }
+}
+
+// K-environment cell sweep along x (lanes along the rows).
+template <int K, bool FIRST>
+__global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
+    const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
+    const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
+  constexpr int NV = 3 * K + 1;
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  if (j >= dm.ny) return;                              // whole warp leaves together
+  const int nd = dm.nx, C = (int)dm.C, F = (int)dm.F;
+  const int s = blockIdx.x * kLineUpd - 2 + lane;
+  const bool valid = s >= 0 && s < nd;
+  const bool inner = s >= 1 && s <= nd - 1;
+  const bool infr = s + 1 <= nd - 1;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  const int c = valid ? s + dm.nx * (j + dm.ny * k) : 0;
+  const int t = inner ? s + (dm.nx + 1) * (j + dm.ny * k) : 0;
+  CellInK<K> in;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) in.U[v] = 0.;
+  in.xc[0] = in.xc[1] = in.xc[2] = 0.;
+  in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = 0.; in.den = 0.;
+  if (valid) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in.U[v] = Uin[v * C + c];
+    in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
+    if (FIRST) in.den = Vlag[c];
+  }
+  if (inner) {
+    in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
+    in.n[0] = n0[t]; in.n[1] = n0[F + t]; in.n[2] = n0[2 * F + t];
+  }
+  if (upd) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }
+  double out[NV + K];
+  cell_line_env<K, FIRST>(ph, S->dt, valid, inner, infr, upd, in, out);
+  if (!upd) return;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Uout[v * C + c] = out[v];
+#pragma unroll
+  for (int e = 0; e < K; ++e) dpf[e * C + c] = out[NV + e];
+}
+
+// K-environment cell sweep along y (D = 1) or z (D = 2), staged through
+// shared memory exactly as the single-environment one (dynamic shared
+// memory: NA * kTileArr doubles).
+template <int K, bool FIRST>
+__host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
+
+template <int K, int D, bool FIRST>
+__global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_t(Dims dm,
+    const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
+    const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
+  constexpr int NV = 3 * K + 1;
+  constexpr int NA = env_cells_staged_arrays<K, FIRST>();
+  constexpr int AX = NV, AF = NV + 3, AN = NV + 7, AO = NV + 10, AD = NV + 12;   // array offsets
+  extern __shared__ double tile[];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int nd = dm.ncd(D), C = (int)dm.C, F = (int)dm.F;
+  const int foff = D == 1 ? (int)dm.Fx : (int)(dm.Fx + dm.Fy);
+  const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;
+  const int sx = tid & 7, sp = tid >> 3;
+  const int si = i0 + sx, ss = seg0 + sp;
+  const bool s_valid = si < dm.nx && ss >= 0 && ss < nd;
+  const int sc = D == 1 ? si + dm.nx * (ss + dm.ny * o) : si + dm.nx * (o + dm.ny * ss);
+  {
+    const bool s_inner = si < dm.nx && ss >= 1 && ss <= nd - 1;
+    const int st_ = D == 1 ? si + dm.nx * (ss + (dm.ny + 1) * o) : sc;
+    double* wr = tile + sx * kTileLd + sp;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) wr[v * kTileArr] = s_valid ? Uin[v * C + sc] : 0.;
+    wr[(AX + 0) * kTileArr] = s_valid ? xcs[sc] : 0.;
+    wr[(AX + 1) * kTileArr] = s_valid ? xcs[C + sc] : 0.;
+    wr[(AX + 2) * kTileArr] = s_valid ? xcs[2 * C + sc] : 0.;
+    wr[(AF + 0) * kTileArr] = s_inner ? fd.db[D][st_] : 0.;
+    wr[(AF + 1) * kTileArr] = s_inner ? fd.df[D][st_] : 0.;
+    wr[(AF + 2) * kTileArr] = s_inner ? fd.u[D][st_] : 0.;
+    wr[(AF + 3) * kTileArr] = s_inner ? fd.A[D][st_] : 0.;
+    const int f = foff + st_;
+    wr[(AN + 0) * kTileArr] = s_inner ? n0[f] : 0.;
+    wr[(AN + 1) * kTileArr] = s_inner ? n0[F + f] : 0.;
+    wr[(AN + 2) * kTileArr] = s_inner ? n0[2 * F + f] : 0.;
+    wr[(AO + 0) * kTileArr] = s_valid ? ofn[lb * C + sc] : 0.;
+    wr[(AO + 1) * kTileArr] = s_valid ? ofn[lf * C + sc] : 0.;
+    if (FIRST) wr[AD * kTileArr] = s_valid ? Vlag[sc] : 0.;
+  }
+  __syncthreads();
+  const int s = seg0 + lane;
+  const bool line_ok = i0 + w < dm.nx;
+  const bool valid = line_ok && s >= 0 && s < nd;
+  const bool inner = line_ok && s >= 1 && s <= nd - 1;
+  const bool infr = s + 1 <= nd - 1;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  double* row = tile + w * kTileLd + lane;
+  CellInK<K> in;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) in.U[v] = row[v * kTileArr];
+  in.xc[0] = row[AX * kTileArr]; in.xc[1] = row[(AX + 1) * kTileArr]; in.xc[2] = row[(AX + 2) * kTileArr];
+  in.db = row[AF * kTileArr]; in.df = row[(AF + 1) * kTileArr]; in.u = row[(AF + 2) * kTileArr];
+  in.A = row[(AF + 3) * kTileArr];
+  in.n[0] = row[AN * kTileArr]; in.n[1] = row[(AN + 1) * kTileArr]; in.n[2] = row[(AN + 2) * kTileArr];
+  in.ob = row[AO * kTileArr]; in.of = row[(AO + 1) * kTileArr];
+  in.den = FIRST ? row[AD * kTileArr] : 0.;
+  constexpr int NO = NV + K;
+  static_assert(NO <= NA, "outputs reuse the staged rows");
+  double out[NO];
+  cell_line_env<K, FIRST>(ph, S->dt, valid, inner, infr, upd, in, out);
+  if (upd) {
+#pragma unroll
+    for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];
+  }
+  __syncthreads();
+  if (!(s_valid && sp >= 2 && sp < 2 + kLineUpd)) return;
+  const double* r = tile + sx * kTileLd + sp;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Uout[v * C + sc] = r[v * kTileArr];
+#pragma unroll
+  for (int e = 0; e < K; ++e) dpf[e * C + sc] = r[(NV + e) * kTileArr];
+}
+
+// ---- end of the remap, per cell ----------------------------------------
+// Environment add/remove (RemapADIFinal.cc:94-226, decided from the
+// membership before the update), the "moy" kernel (RemapADIFinal.cc:406-644),
+// PerfectGas EOS per environment (PerfectGasEOSService.cc:72-136) and the
+// mixed-cell averages (MahycoModule.cc:1836-1915).  When a cell changes
+// membership the values of the environments involved move between the global
+// and the partial slots as Arcane's material modifier moves them; of those
+// only the mass fraction can outlive this kernel (it is kept when the cell's
+// mass is exactly zero), so only it is moved.
+template <int K>
+__global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __restrict__ S, Phys ph,
+                                                            EnvState env, const double* __restrict__ U,
+                                                            CellState st) {
+  constexpr int NV = 3 * K + 1;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int C = (int)dm.C;
+  if (c >= C) return;
+  double u[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u[v] = U[v * C + c];
+  const double vol = st.Ve[c];
+  const double thr = ph.threshold;
+  uint32_t mask = env.mask[c];
+  // membership changes (RemapADIFinal.cc:94-148)
+  uint32_t nmask = mask;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double fv = u[k] / vol;
+    const bool in_env = mask >> k & 1;
+    if (fv < thr && in_env) nmask &= ~(1u << k);
+    else if (fv > thr && !in_env) {
+      double volt = 0.;
+#pragma unroll
+      for (int kk = 0; kk < K; ++kk) volt += u[kk];
+      const double f2 = u[k] / volt;
+      if (f2 > thr && u[K + k] != 0.) nmask |= 1u << k;
+    }
+  }
+  if (nmask != mask) {
+    const bool was_pure = __popc(mask) == 1, now_pure = __popc(nmask) == 1;
+    if (was_pure && !now_pure) {
+      const int oe = __ffs(mask) - 1;
+#pragma unroll
+      for (int k = 0; k < K; ++k) env.x[k * C + c] = (k == oe && (nmask >> oe & 1)) ? env.xg[c] : 0.;
+    } else if (!was_pure && now_pure) {
+      env.xg[c] = env.x[(__ffs(nmask) - 1) * C + c];
+    } else if (!now_pure) {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if ((nmask >> k & 1) && !(mask >> k & 1)) env.x[k * C + c] = 0.;
+    }
+    mask = nmask;
+    env.mask[c] = nmask;
+  }
+  const bool pure = __popc(mask) == 1;
+  const int ke = pure ? __ffs(mask) - 1 : -1;
+  // "moy" kernel
+  double volt = 0., masset = 0.;
+#pragma unroll
+  for (int k = 0; k < K; ++k) { volt += u[k]; masset += u[K + k]; }
+  const double unsurvolt = 1. / volt;
+  const double unsurvol = 1. / vol;
+  double f[K], x[K], r[K], e[K], q[K], m[K];
+  double somme_frac = 0.;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    f[k] = x[k] = r[k] = e[k] = q[k] = m[k] = 0.;
+    if (!(mask >> k & 1)) continue;
+    double fvol = u[k] * unsurvolt;
+    if (fvol < thr) fvol = 0.;
+    f[k] = fvol;
+    somme_frac += fvol;
+  }
+  const double unsursomme_frac = 1. / somme_frac;
+  int matcell = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(mask >> k & 1)) continue;
+    const double fvol = f[k] * unsursomme_frac;
+    if (fvol > 0.) matcell++;
+    f[k] = fvol;
+  }
+  const bool est_mixte = matcell > 1;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (mask >> k & 1) x[k] = pure ? env.xg[c] : env.x[k * C + c];
+  if (masset != 0.) {
+    const double unsurmasset = 1. / masset;
+    double fmasset = 0.;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!(mask >> k & 1)) continue;
+      double mf = u[K + k] * unsurmasset;
+      if (f[k] < thr) mf = 0.;
+      fmasset += mf;
+      x[k] = mf;
+    }
+    if (fmasset != 0.) {
+      const double unsurfmasset = 1. / fmasset;
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (mask >> k & 1) x[k] = x[k] * unsurfmasset;
+    }
+  } else {
+    atomicOr(&S->status, MHY_STATUS_ZERO_MASS);
+  }
+  double density_nplus1 = 0.;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(mask >> k & 1)) continue;
+    double de = 0.;
+    if (f[k] > thr) {
+      const double vn = u[k] * vol * unsurvolt;
+      de = u[K + k] / vn;
+    }
+    r[k] = de;
+    density_nplus1 += f[k] * de;
+  }
+  const double cell_mass = vol * density_nplus1;
+  double energie_nplus1 = 0., pseudo_nplus1 = 0.;
+  const double pv = u[3 * K] * unsurvol;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(mask >> k & 1)) continue;
+    double ee = 0.;
+    if (f[k] > thr && u[K + k] != 0.) ee = u[2 * K + k] / u[K + k];
+    e[k] = ee;
+    energie_nplus1 += x[k] * ee;
+    m[k] = x[k] * cell_mass;
+    q[k] = pv;
+    pseudo_nplus1 += f[k] * pv;
+  }
+  // A pure cell's environment value is its global value, so the global
+  // energy and pseudo-viscosity written after the loop are its values too.
+  if (pure) { e[ke] = energie_nplus1; q[ke] = pseudo_nplus1; }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(mask >> k & 1)) continue;
+    if (r[k] < 0. || e[k] < 0.) { e[k] = 0.; r[k] = 0.; f[k] = 0.; x[k] = 0.; }
+  }
+  double pk[K], ck[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    pk[k] = ck[k] = 0.;
+    if (!(mask >> k & 1)) continue;
+    const double g = env.gamma[k];
+    pk[k] = (g - 1.) * r[k] * e[k];
+    ck[k] = sqrt(g * pk[k] / r[k]);
+  }
+  if (pure) {
+    st.rho[c] = r[ke]; st.e[c] = e[ke]; st.q[c] = q[ke]; st.mass[c] = m[ke];
+    st.p[c] = pk[ke]; st.cs[c] = ck[ke];
+    env.fg[c] = f[ke]; env.xg[c] = x[ke];
+  } else {
+    double pm = 0., cm = 1.e-20;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!(mask >> k & 1)) continue;
+      const int o = k * C + c;
+      env.f[o] = f[k]; env.x[o] = x[k]; env.rho[o] = r[k]; env.e[o] = e[k]; env.q[o] = q[k]; env.m[o] = m[k];
+      env.p[o] = pk[k]; env.cs[o] = ck[k];
+      pm += f[k] * pk[k];
+      cm = amax(ck[k], cm);
+    }
+    if (est_mixte) st.rho[c] = density_nplus1;
+    st.e[c] = energie_nplus1; st.q[c] = pseudo_nplus1; st.mass[c] = cell_mass;
+    st.p[c] = pm; st.cs[c] = cm;
+  }
+}
+
+// Initial thermodynamic state of a K-environment mesh, after the initial
+// geometry: PerfectGas initEOS per environment (E:20-32), the mixed-cell
+// energy and sound speed (MahycoModule.cc:116-127) and ComputeCellMass
+// (MahycoModule.cc:199-225).  Fractions, partial densities and pressures,
+// mass fractions and the global density and pressure come from the host.
+template <int K>
+__global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int C = (int)dm.C;
+  if (c >= C) return;
+  const uint32_t mask = env.mask[c];
+  const double V = st.Ve[c];
+  st.q[c] = 0.;
+  if (__popc(mask) == 1) {
+    const double g = env.gamma[__ffs(mask) - 1];
+    const double p = st.p[c], r = st.rho[c];
+    st.e[c] = p / ((g - 1.) * r);
+    st.cs[c] = sqrt(g * p / r);
+    st.mass[c] = r * V;
+    env.fg[c] = 1.; env.xg[c] = 1.;
+    return;
+  }
+  double eg = 0., cg = 0.;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(mask >> k & 1)) continue;
+    const int o = k * C + c;
+    const double g = env.gamma[k];
+    const double p = env.p[o], r = env.rho[o];
+    const double ek = p / ((g - 1.) * r);
+    const double ck = sqrt(g * p / r);
+    env.e[o] = ek; env.cs[o] = ck; env.q[o] = 0.;
+    eg += ek * env.x[o];
+    cg = smax(ck, cg);
+  }
+  st.e[c] = eg;
+  st.cs[c] = cg;
+  const double mg = st.rho[c] * V;
+  st.mass[c] = mg;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (mask >> k & 1) env.m[k * C + c] = env.x[k * C + c] * mg;
+  env.fg[c] = 1.; env.xg[c] = 1.;
+}
+
+// ------------------------------------------------------------------------
+// Host-side launchers.
+template <int K, int D, bool FIRST>
+static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+  const Dims& dm = a.dm;
+  const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
+  const dim3 g((dm.nx + kLineWarps - 1) / kLineWarps, nseg, D == 1 ? dm.nz : dm.ny);
+  const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * kTileArr * sizeof(double);
+  k_env_sweep_cells_t<K, D, FIRST><<<g, 32 * kLineWarps, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin,
+                                                                     Uout, a.dpf, a.Vlag);
+}
+
+template <int K, bool FIRST>
+static void env_cells(const CycleArgs& a, int d, const double* Uin, double* Uout, cudaStream_t s) {
+  const Dims& dm = a.dm;
+  if (d == 0) {
+    const int nseg = (dm.nx + kLineUpd - 1) / kLineUpd;
+    const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
+    k_env_sweep_cells_x<K, FIRST><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout,
+                                                                a.dpf, a.Vlag);
+  } else if (d == 1) {
+    env_cells_staged<K, 1, FIRST>(a, Uin, Uout, s);
+  } else {
+    env_cells_staged<K, 2, FIRST>(a, Uin, Uout, s);
+  }
+}
+
+template <int K>
+static void remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
+  int prev = 0;
+  for (int it = 0; it < 3; ++it) {
+    const int d = (it + sens) % 3;
+    const bool first = it == 0, last = it == 2;
+    const double* uin = a.U[it & 1];
+    double* uout = a.U[(it + 1) & 1];
+    const double* udin = a.ud[(it + 1) & 1];
+    double* udout = a.ud[it & 1];
+    if (first) env_cells<K, true>(a, d, uin, uout, s);
+    else env_cells<K, false>(a, d, uin, uout, s);
+    if (last) {
+      const unsigned nb = (unsigned)((a.dm.C + 255) / 256);
+      k_env_finalize_cells<K><<<nb, 256, 0, s>>>(a.dm, a.S, a.ph, a.env, uout, a.st);
+    }
+    sweep_nodes<K>(a, d, first, last, prev, udin, udout, s);
+    prev |= 1 << d;
+  }
+}
+
+template <int K>
+static void set_env_attributes() {
+  const int mx = (int)(env_cells_staged_arrays<K, true>() * kTileArr * sizeof(double));
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
+void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
+  const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
+#define MHY_LAG_ENV(KK)                                                                                         \
+  k_cyc_lagrange_cells<KK><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q,    \
+                                               a.st.p, a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd,     \
+                                               a.env, a.Vlag)
+  if (a.K == 2) MHY_LAG_ENV(2);
+  else if (a.K == 3) MHY_LAG_ENV(3);
+  else MHY_LAG_ENV(4);
+#undef MHY_LAG_ENV
+}
+
+void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
+  if (a.K == 2) remap_env<2>(a, sens, s);
+  else if (a.K == 3) remap_env<3>(a, sens, s);
+  else remap_env<4>(a, sens, s);
+}
+
+// Called once per context before any cycle (and so before any graph capture).
+void launch_init_env(const CycleArgs& a, cudaStream_t s) {
+  static std::once_flag once[kMaxEnvDevice + 1];
+  const unsigned nb = (unsigned)((a.dm.C + 255) / 256);
+  if (a.K == 2) { std::call_once(once[2], set_env_attributes<2>); k_env_init_state<2><<<nb, 256, 0, s>>>(a.dm, a.env, a.st); }
+  else if (a.K == 3) { std::call_once(once[3], set_env_attributes<3>); k_env_init_state<3><<<nb, 256, 0, s>>>(a.dm, a.env, a.st); }
+  else { std::call_once(once[4], set_env_attributes<4>); k_env_init_state<4><<<nb, 256, 0, s>>>(a.dm, a.env, a.st); }
+}
+
+}  // namespace mhy

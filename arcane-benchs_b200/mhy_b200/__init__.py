@@ -32,7 +32,10 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_compute_artificial_viscosity", "mhy_update_energy_and_pressure", "mhy_remap",
             "mhy_compute_delta_t", "mhy_step", "mhy_synchronize", "mhy_get_field", "mhy_get_dt",
             "mhy_get_time", "mhy_get_status", "mhy_get_sizes", "mhy_get_stream", "mhy_kernels_per_cycle",
-            "mhy_last_error", "mhy_destroy", "mhy_compute_hydro_dt_noalloc"]
+            "mhy_last_error", "mhy_destroy", "mhy_compute_hydro_dt_noalloc", "mhy_get_env_field",
+            "mhy_get_env_mask"]
+ENV_FIELDS = {"fracvol": 0, "density": 1, "internal_energy": 2, "pressure": 3, "sound_speed": 4,
+              "mass_fraction": 5, "cell_mass": 6}
 
 
 class MhyError(RuntimeError):
@@ -101,6 +104,8 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_destroy.restype = None
     L.mhy_compute_hydro_dt_noalloc.argtypes = [ctypes.c_int32] * 3 + [vp] * 3 + [ctypes.c_double] * 3 + [vp, vp]
     L.mhy_compute_hydro_dt_noalloc.restype = ctypes.c_int
+    L.mhy_get_env_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t]
+    L.mhy_get_env_mask.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_size_t]
     _lib = L
     return L
 
@@ -201,6 +206,18 @@ class Context:
         else:
             out = np.empty(c.ncells)
         _check(load().mhy_get_field(self.h, fid, out.ctypes.data_as(ctypes.c_void_p), out.nbytes))
+        return out
+
+    def env_field(self, name: str, k: int) -> np.ndarray:
+        """Value of environment k in every cell (0 where the cell does not hold it)."""
+        out = np.empty(self.case.ncells)
+        _check(load().mhy_get_env_field(self.h, ENV_FIELDS[name], int(k), out.ctypes.data_as(ctypes.c_void_p),
+                                        out.nbytes))
+        return out
+
+    def env_mask(self) -> np.ndarray:
+        out = np.empty(self.case.ncells, dtype=np.uint32)
+        _check(load().mhy_get_env_mask(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), out.nbytes))
         return out
 
     def close(self):

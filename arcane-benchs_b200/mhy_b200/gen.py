@@ -208,6 +208,42 @@ def _two_env_case(name, nx, ny, nz, lx, ly, lz, fa, cycles, options):
                 np.zeros_like(coords), options or Options(), cycles)
 
 
+def three_material(nx=48, ny=16, nz=16, lx=1.0, ly=0.3, lz=0.3, seed=6, cycles=100, amp=0.03,
+                   radius=0.08, options=None) -> Case:
+    """Three ideal gases: A (gamma 1.4, rho 1, p 1) for x < x_I(y,z), B (gamma
+    1.67, rho 0.3, p 0.2) beyond, and a cylinder of C (gamma 1.3, rho 0.6,
+    p 0.05) along z of the given radius centred on the interface at y = ly/2,
+    so that cells hold one, two or all three environments.  x_I = lx/2 +
+    amp sin(2 pi y/ly + phi) cos(2 pi z/lz + psi), phases from the seed;
+    fractions by 4^3 sampling."""
+    ph = uniform01(seed, 2) * 2.0 * math.pi
+    sub = 4
+    hx, hy, hz = lx / nx, ly / ny, lz / nz
+    frac = np.zeros((3, nz, ny, nx))
+    offs = (np.arange(sub) + 0.5) / sub
+    xs = np.arange(nx)[None, None, :] * hx
+    ys = np.arange(ny)[None, :, None] * hy
+    zs = np.arange(nz)[:, None, None] * hz
+    for a in offs:
+        for b in offs:
+            for c in offs:
+                x, y, z = xs + a * hx, ys + b * hy, zs + c * hz
+                xi = 0.5 * lx + amp * np.sin(2 * math.pi * y / ly + ph[0]) * np.cos(2 * math.pi * z / lz + ph[1])
+                inc = (x - 0.5 * lx) ** 2 + (y - 0.5 * ly) ** 2 < radius ** 2
+                isa = (x < xi) & ~inc
+                frac[0] += isa
+                frac[1] += ~isa & ~inc
+                frac[2] += inc
+    fr = (frac / sub ** 3).reshape(3, -1)
+    coords = cartesian_nodes(nx, ny, nz, lx, ly, lz)
+    rho = (1.0, 0.3, 0.6)
+    p = (1.0, 0.2, 0.05)
+    dens = np.stack([np.where(fr[k] > 0, rho[k], 0.0) for k in range(3)])
+    pres = np.stack([np.where(fr[k] > 0, p[k], 0.0) for k in range(3)])
+    return Case("three_material", nx, ny, nz, coords, np.array([1.4, 1.67, 1.3]), fr, dens, pres,
+                np.zeros_like(coords), options or Options(), cycles)
+
+
 def _real_sph_harm(l, m, theta, phi):
     """Real spherical harmonic Y_lm (unnormalised associated Legendre form)."""
     from scipy.special import lpmv  # scipy is in the image

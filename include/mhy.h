@@ -70,7 +70,7 @@ typedef struct mhy_options {
   int32_t projection_limiteur_id;    /* 0 minmod, 1 superBee, 2 vanLeer */
   int32_t nb_bc;
   mhy_bc bc[MHY_MAX_BC];             /* default: walls on the six planes */
-  int32_t nb_env;                    /* number of environments (one ideal gas each) */
+  int32_t nb_env;                    /* number of environments (one ideal gas each; 1..4 on the device) */
   double adiabatic_cst[MHY_MAX_ENV]; /* PerfectGas adiabatic-cst per environment */
   int32_t precision;                 /* 0: plain FP64 */
   int32_t reserved[7];
@@ -145,6 +145,18 @@ int mhy_step(mhy_ctx* ctx, int ncycles);
 int mhy_synchronize(mhy_ctx* ctx);
 
 int mhy_get_field(mhy_ctx* ctx, int field, void* dst, size_t bytes);
+/* Per-environment cell values (Arcane's environment views, e.g. the
+ * EnvCellVariableRealRef fields of Mahyco.axl read through an IMeshEnvironment):
+ * for every cell, the value of environment `env` when the cell belongs to it
+ * (the cell's own value for a pure cell), else 0.  ncells doubles. */
+typedef enum mhy_env_field {
+  MHY_ENV_FRACVOL = 0, MHY_ENV_DENSITY = 1, MHY_ENV_INTERNAL_ENERGY = 2, MHY_ENV_PRESSURE = 3,
+  MHY_ENV_SOUND_SPEED = 4, MHY_ENV_MASS_FRACTION = 5, MHY_ENV_CELL_MASS = 6
+} mhy_env_field;
+int mhy_get_env_field(mhy_ctx* ctx, int field, int env, void* dst, size_t bytes);
+/* Environment membership: bit k of dst[c] set when cell c belongs to
+ * environment k (ncells uint32). */
+int mhy_get_env_mask(mhy_ctx* ctx, uint32_t* dst, size_t bytes);
 /* dt of the next cycle (m_global_deltat), dt of the last cycle (m_old_deltat) */
 int mhy_get_dt(mhy_ctx* ctx, double* dt, double* dt_old);
 int mhy_get_time(mhy_ctx* ctx, double* time, int64_t* iteration);

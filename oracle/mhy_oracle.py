@@ -116,6 +116,12 @@ class Oracle:
             raise KeyError(which)
         return out
 
+    def env_mask(self) -> np.ndarray:
+        out = np.zeros(self.case.ncells)
+        if lib().orc_get_field(self.h, 50, _dp(out)) != 0:
+            raise KeyError("env_mask")
+        return out.astype(np.uint32)
+
     def close(self):
         if self.h:
             lib().orc_destroy(self.h)
