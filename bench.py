@@ -32,8 +32,17 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "arcane-benchs_b200"))
 
 METRIC = "cell-cycles/s"
-def workload_name(n):
-    return f"sedov-{n}^3-jitter1%-fp64"
+WORKLOADS = ("sedov", "two_material", "sphere_inclusion")
+
+
+def make_case(args):
+    """The workload's mesh and initial state (seeded, synthetic) and its name."""
+    from mhy_b200 import gen
+    if args.workload == "sedov":
+        return gen.sedov(n=args.n), f"sedov-{args.n}^3-jitter1%-fp64"
+    if args.workload == "two_material":
+        return gen.two_material(256, 128, 128), "two-material-256x128x128-fp64"
+    return gen.sphere_inclusion(384, 384, 192), "sphere-inclusion-384x384x192-fp64"
 
 
 def parse():
@@ -42,7 +51,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=128, help="mesh cells per direction")
+    ap.add_argument("--workload", choices=WORKLOADS, default="sedov",
+                    help="sedov: Sedov 128^3 (the headline); two_material: 256x128x128, two gases; "
+                         "sphere_inclusion: 384x384x192, two gases")
+    ap.add_argument("--n", type=int, default=128, help="Sedov mesh cells per direction")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-cycles", type=int, default=5)
@@ -106,7 +118,7 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(case, cycles):
+def cpu_baseline(case, cycles, wname):
     """The oracle (CPU restatement of the reference algorithm) on this host, all cores."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import mhy_oracle
@@ -118,7 +130,7 @@ def cpu_baseline(case, cycles):
     dt = time.perf_counter() - t0
     o.close()
     return {"value": case.ncells * cycles / dt, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"Sedov {case.nx}^3 (same mesh and state), cycles 2..{cycles + 1} after init, "
+            "sample": f"{wname} (same mesh and state), cycles 2..{cycles + 1} after init, "
                       f"OpenMP {threads} threads, oracle built -O3 -ffp-contract=off"}
 
 
@@ -128,10 +140,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from mhy_b200 import gen
     sys.path.insert(0, str(ROOT / "oracle"))
     import mhy_oracle
-    case = gen.sedov(n=args.n)
+    case, wname = make_case(args)
     threads = os.cpu_count() or 1
     o = mhy_oracle.Oracle(case, pow_mode="libm", threads=threads)
     t0 = time.perf_counter()
@@ -143,12 +154,12 @@ def run_reference(args):
     o.step(k)
     el = time.perf_counter() - t0
     val = case.ncells * k / el
-    sample = (f"Sedov {args.n}^3, {k} of {args.steps} requested cycles timed after {max(1, args.warmup)} warm-up "
+    sample = (f"{wname}, {k} of {args.steps} requested cycles timed after {max(1, args.warmup)} warm-up "
               f"(bounded to ~{budget_s:.0f} s), OpenMP {threads} threads")
     line = {"metric": METRIC, "value": val, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
             "steps": k, "warmup": max(1, args.warmup), "ms_per_step": el / k * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(args.n), "cells": case.ncells, "nodes": case.nnodes},
+            "config": {"workload": wname, "cells": case.ncells, "nodes": case.nnodes},
             "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -158,21 +169,18 @@ def run_reference(args):
 def run_ours(args):
     import numpy as np
     import torch
-    import torch.distributed as dist
     import mhy_b200
-    from mhy_b200 import gen, bytes_model
+    from mhy_b200 import gen, bytes_model, replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = replicas.ranks()
     if world != args.gpus:
         raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        replicas.init("nccl", device=dev)
 
-    case = gen.sedov(n=args.n)
+    case, wname = make_case(args)
     ctx = mhy_b200.Context(case, device=local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
     kpc = ctx.kernels_per_cycle()
@@ -182,23 +190,17 @@ def run_ours(args):
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         start.record(stream)
         ctx.step(args.steps)
         stop.record(stream)
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-    ms = start.elapsed_time(stop)
+        replicas.barrier()
+    ms_local = start.elapsed_time(stop)
     ctx.synchronize()
     status = ctx.status()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * case.ncells * args.steps / (ms / 1e3)
+    ms, value = replicas.aggregate(case.ncells, args.steps, ms_local, dev)
     ctx.close()
 
     # end to end through the per-entry-point C ABI, host buffers in pinned memory
@@ -214,8 +216,7 @@ def run_ours(args):
         out_rho = pinned(np.zeros(case.ncells)); out_e = pinned(np.zeros(case.ncells))
         out_v = pinned(np.zeros((case.nnodes, 3)))
         L = mhy_b200.load()
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         c2 = mhy_b200.Context(hcase, device=local)
@@ -224,21 +225,19 @@ def run_ours(args):
             c2.dt()                                   # D2H of the step's result (dt, 16 B) + sync
         for name, arr in (("density", out_rho), ("internal_energy", out_e), ("velocity", out_v)):
             mhy_b200._check(L.mhy_get_field(c2.h, mhy_b200.FIELDS[name], arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes))
-        el = time.perf_counter() - t0
+        el_local = time.perf_counter() - t0
         c2.close()
-        if world > 1:
-            t = torch.tensor([el], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el_ms, e2e_value = replicas.aggregate(case.ncells, args.steps, el_local * 1e3, dev)
         h2d = (case.coords.nbytes + case.fracvol.nbytes + case.density.nbytes + case.pressure.nbytes
                + case.velocity.nbytes) / args.steps
         d2h = 16 + (out_rho.nbytes + out_e.nbytes + out_v.nbytes) / args.steps
-        e2e = {"value": world * case.ncells * args.steps / el, "unit": METRIC,
+        e2e = {"value": e2e_value, "unit": METRIC,
                "h2d_bytes_per_step": round(h2d, 1), "d2h_bytes_per_step": round(d2h, 1),
                "path": "mhy_create+mhy_set_state+mhy_hydro_start_init, per-cycle entry points + mhy_get_dt, "
                        "mhy_get_field x3; wall clock, max over ranks"}
 
-    b_alg = bytes_model.bytes_per_cell_cycle(case.ncells, case.nnodes)
+    mixed_fraction = float(((case.fracvol > 0).sum(0) > 1).mean()) if case.nenv > 1 else 0.0
+    b_alg = bytes_model.bytes_per_cell_cycle(case.ncells, case.nnodes, case.nenv, mixed_fraction)
     peak, peak_kind = measured_peak()
     per_gpu_cells_per_s = case.ncells * args.steps / (ms / 1e3)
     achieved = b_alg * per_gpu_cells_per_s / 1e9
@@ -249,20 +248,20 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(case, args.cpu_sample_cycles)
+        cpu = cpu_baseline(case, args.cpu_sample_cycles, wname)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_name(args.n), "cells": case.ncells, "nodes": case.nnodes,
+                "config": {"workload": wname, "cells": case.ncells, "nodes": case.nnodes,
+                           "environments": case.nenv,
                            "cells_per_gpu": case.ncells, "parallelism": f"replicas{world}",
                            "l2": "working set ~2 GB > 126 MB L2 (no flush needed)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 

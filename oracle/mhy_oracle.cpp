@@ -1156,6 +1156,10 @@ void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
 
 void orc_set_threads(int n) { omp_set_num_threads(n); }
 
+// V^(1./3.) as the oracle evaluates it: the project cube root (project != 0)
+// or std::pow, the reference's call (MahycoModule.cc:1259).
+double orc_pow_third(double v, int project) { return project ? mhy::pow_third(v) : std::pow(v, 1. / 3.); }
+
 // scalars: [dt, old_dt, time, sens, iteration, status]
 void orc_get_scalars(void* h, double* out) {
   Oracle* o = static_cast<Oracle*>(h);

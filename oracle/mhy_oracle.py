@@ -51,12 +51,19 @@ def lib():
         L.orc_get_scalars.argtypes = [ctypes.c_void_p, dp]
         L.orc_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.orc_get_field.restype = ctypes.c_int
+        L.orc_pow_third.argtypes = [ctypes.c_double, ctypes.c_int]
+        L.orc_pow_third.restype = ctypes.c_double
         _lib = L
     return _lib
 
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def pow_third(v: float, project: bool = True) -> float:
+    """V^(1./3.) as the oracle computes it (project cube root or std::pow)."""
+    return lib().orc_pow_third(float(v), 1 if project else 0)
 
 
 class Oracle:

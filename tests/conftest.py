@@ -3,7 +3,7 @@ import pathlib
 import sys
 
 ROOT = pathlib.Path(__file__).resolve().parent.parent
-for p in (ROOT / "arcane-benchs_b200", ROOT / "oracle", ROOT):
+for p in (ROOT / "arcane-benchs_b200", ROOT / "oracle", ROOT, ROOT / "tests" / "golden", ROOT / "tests"):
     if str(p) not in sys.path:
         sys.path.insert(0, str(p))
 
