@@ -460,6 +460,148 @@ int mhy_synchronize(mhy_ctx* c) {
   return MHY_OK;
 }
 
+// ---- batches ---------------------------------------------------------------
+}  // extern "C"
+
+struct mhy_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<mhy_ctx*> inst;
+  CycleArgs* d_descs = nullptr;
+  int4* d_work[BK_COUNT] = {};
+  BatchPlan plan{};
+  int sens = 0;
+  bool initialized = false;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+};
+
+extern "C" {
+
+void mhy_batch_destroy(mhy_batch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (int s = 0; s < 3; ++s) if (b->graph[s]) cudaGraphExecDestroy(b->graph[s]);
+  for (int k = 0; k < BK_COUNT; ++k) if (b->d_work[k]) cudaFree(b->d_work[k]);
+  if (b->d_descs) cudaFree(b->d_descs);
+  for (mhy_ctx* c : b->inst) mhy_destroy(c);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts, int device, mhy_batch** out) {
+  if (!meshes || !opts || !out || n <= 0) return fail(MHY_ERR_ARG, "null argument or empty batch");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i)
+    if (opts[i].nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "batched instances must have one environment");
+  mhy_batch* b = new mhy_batch();
+  for (int i = 0; i < n; ++i) {
+    mhy_ctx* c = nullptr;
+    const int rc = mhy_create(&meshes[i], &opts[i], device, &c);
+    if (rc != MHY_OK) { mhy_batch_destroy(b); return rc; }
+    b->inst.push_back(c);
+  }
+  b->device = b->inst[0]->device;
+  cudaError_t err = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  // work tables: every block of every instance's grid, instance-major
+  for (int k = 0; k < BK_COUNT; ++k) {
+    std::vector<int4> w;
+    for (int i = 0; i < n; ++i) {
+      int gx, gy, gz;
+      batch_work_shape(b->inst[i]->dm, k, gx, gy, gz);
+      for (int z = 0; z < gz; ++z)
+        for (int y = 0; y < gy; ++y)
+          for (int x = 0; x < gx; ++x) w.push_back(make_int4(i, x, y, z));
+    }
+    err = cudaMalloc(&b->d_work[k], w.size() * sizeof(int4));
+    if (err == cudaSuccess) err = cudaMemcpy(b->d_work[k], w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
+    b->plan.work[k] = b->d_work[k];
+    b->plan.nwork[k] = (int)w.size();
+  }
+  err = cudaMalloc(&b->d_descs, n * sizeof(CycleArgs));
+  if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
+  b->plan.descs = b->d_descs;
+  b->plan.ninst = n;
+  *out = b;
+  return MHY_OK;
+}
+
+int mhy_batch_set_state(mhy_batch* b, int i, const mhy_state* st) {
+  if (!b || i < 0 || i >= (int)b->inst.size()) return fail(MHY_ERR_ARG, "bad batch or instance index");
+  return mhy_set_state(b->inst[i], st);
+}
+
+int mhy_batch_hydro_start_init(mhy_batch* b) {
+  if (!b) return fail(MHY_ERR_ARG, "null batch");
+  std::vector<CycleArgs> d;
+  for (mhy_ctx* c : b->inst) {
+    const int rc = mhy_hydro_start_init(c);
+    if (rc != MHY_OK) return rc;
+    d.push_back(c->args());
+  }
+  MHY_CUDA(cudaMemcpy(b->d_descs, d.data(), d.size() * sizeof(CycleArgs), cudaMemcpyHostToDevice));
+  b->initialized = true;
+  return MHY_OK;
+}
+
+int mhy_batch_step(mhy_batch* b, int ncycles) {
+  if (!b) return fail(MHY_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(MHY_ERR_STATE, "mhy_batch_hydro_start_init must come first");
+  if (ncycles < 0) return fail(MHY_ERR_ARG, "ncycles < 0");
+  for (int it = 0; it < ncycles; ++it) {
+    const int s = b->sens;
+    if (!b->graph[s]) {
+      cudaGraph_t g = nullptr;
+      MHY_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      launch_batch_cycle(b->plan, s, b->stream);
+      cudaError_t le = cudaGetLastError();
+      cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+      if (le != cudaSuccess || ee != cudaSuccess)
+        return fail(MHY_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
+      cudaError_t ie = cudaGraphInstantiate(&b->graph[s], g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) { b->graph[s] = nullptr; return fail(MHY_ERR_CUDA, cudaGetErrorString(ie)); }
+    }
+    MHY_CUDA(cudaGraphLaunch(b->graph[s], b->stream));
+    b->sens = (s + 1) % 3;
+  }
+  for (mhy_ctx* c : b->inst) c->sens = b->sens;
+  return MHY_OK;
+}
+
+int mhy_batch_synchronize(mhy_batch* b) {
+  if (!b) return fail(MHY_ERR_ARG, "null batch");
+  MHY_CUDA(cudaStreamSynchronize(b->stream));
+  for (mhy_ctx* c : b->inst) {
+    const int rc = mhy_synchronize(c);
+    if (rc != MHY_OK) return rc;
+  }
+  return MHY_OK;
+}
+
+int mhy_batch_get_field(mhy_batch* b, int i, int field, void* dst, size_t bytes) {
+  if (!b || i < 0 || i >= (int)b->inst.size()) return fail(MHY_ERR_ARG, "bad batch or instance index");
+  MHY_CUDA(cudaStreamSynchronize(b->stream));
+  return mhy_get_field(b->inst[i], field, dst, bytes);
+}
+
+int mhy_batch_get_dt(mhy_batch* b, int i, double* dt, double* dt_old) {
+  if (!b || i < 0 || i >= (int)b->inst.size()) return fail(MHY_ERR_ARG, "bad batch or instance index");
+  MHY_CUDA(cudaStreamSynchronize(b->stream));
+  return mhy_get_dt(b->inst[i], dt, dt_old);
+}
+
+int mhy_batch_get_status(mhy_batch* b, int i, uint32_t* flags) {
+  if (!b || i < 0 || i >= (int)b->inst.size()) return fail(MHY_ERR_ARG, "bad batch or instance index");
+  MHY_CUDA(cudaStreamSynchronize(b->stream));
+  return mhy_get_status(b->inst[i], flags);
+}
+
+int mhy_batch_size(mhy_batch* b) { return b ? (int)b->inst.size() : 0; }
+int mhy_batch_kernels_per_cycle(mhy_batch* b) { return b ? kKernelsPerCycleBatch : 0; }
+void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
+
 int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
   const long long C = c->dm.C, N = c->dm.N;

@@ -15,6 +15,9 @@
 //
 // Every expression keeps the operation order of the reference (see the
 // citations), so with --fmad=false the results equal the CPU oracle bit for bit.
+#include <map>
+#include <mutex>
+
 #include "mhy_lagrange.cuh"
 #include "mhy_line.cuh"
 
@@ -23,11 +26,12 @@ namespace mhy {
 // ------------------------------------------------------------------------
 // Lagrange phase, nodes: SaveValuesAtN (v_n = v, x = x0), UpdateVelocity,
 // ApplyBoundaryCondition (MahycoModule.cc:308-450, 589-665, 936-1004).
-__global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scalars* __restrict__ S,
+__device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars* __restrict__ S,
     const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ cqs,
     const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
-    double* __restrict__ vh) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    double* __restrict__ vh,
+    int bx_, int by_, int bz_) {
+  const int i = bx_ * blockDim.x + threadIdx.x, j = by_, k = bz_;
   if (i > dm.nx) return;
   const long long n = dm.nid(i, j, k);
   const double dtv = 0.5 * (S->old_dt + S->dt);
@@ -59,18 +63,26 @@ __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scala
   vh[n] = u.x; vh[dm.N + n] = u.y; vh[2 * dm.N + n] = u.z;
 }
 
+__global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ cqs,
+    const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
+    double* __restrict__ vh) {
+  k_cyc_lagrange_nodes_body(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
 template <bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
+__device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
-    double* __restrict__ dpf, CellState st) {
+    double* __restrict__ dpf, CellState st,
+    int bx_, int by_, int bz_) {
   const int lane = threadIdx.x & 31;
-  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
   if (j >= dm.ny) return;                              // whole warp leaves together
   const int nd = dm.nx, C = (int)dm.C, F = (int)dm.F;
-  const int s = blockIdx.x * kLineUpd - 2 + lane;      // position of this lane's cell along x
+  const int s = bx_ * kLineUpd - 2 + lane;      // position of this lane's cell along x
   const bool valid = s >= 0 && s < nd;
   const bool inner = s >= 1 && s <= nd - 1;            // this lane's low face is an inner face
   const bool infr = s + 1 <= nd - 1;
@@ -105,18 +117,27 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_c
   }
 }
 
+template <bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st) {
+  k_cyc_sweep_cells_x_body<LAST>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // Cell sweep along y (D = 1) or z (D = 2), staged through shared memory.
 // Block (bx, by, bz): x = 8 bx .. 8 bx + 7, positions 28 by - 2 .. 28 by + 29
 // along D, and bz = the remaining coordinate (z for D = 1, y for D = 2).
 template <int D, bool LAST>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
+__device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
-    double* __restrict__ dpf, CellState st) {
+    double* __restrict__ dpf, CellState st,
+    int bx_, int by_, int bz_) {
   constexpr int NA = LAST ? 17 : 16;                  // staged input arrays
   __shared__ double tile[NA * kTileArr];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int i0 = bx_ * kLineWarps, seg0 = by_ * kLineUpd - 2, o = bz_;
   const int nd = dm.ncd(D), C = (int)dm.C, F = (int)dm.F;
   const int foff = D == 1 ? (int)dm.Fx : (int)(dm.Fx + dm.Fy);
   const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;   // back / front faces of d in cell-face order
@@ -182,6 +203,14 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_c
   }
 }
 
+template <int D, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st) {
+  k_cyc_sweep_cells_t_body<D, LAST>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
@@ -238,6 +267,180 @@ void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
   k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.vnorm);
   k_dt_finish<<<1, 1, 0, s>>>(a.S, a.ph);
+}
+
+// ------------------------------------------------------------------------
+// Batched cycle: the same kernel bodies, driven by per-kernel work tables over
+// many instances (persistent grids).  Kernels with shared memory start each
+// work item with a barrier, since the previous item's last reads of the tile
+// may still be in flight in other warps.
+
+void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz) {
+  const int nx = dm.nx, ny = dm.ny, nz = dm.nz;
+  auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
+  switch (kind) {
+    case BK_LNODES: gx = cdiv(nx + 1, 128); gy = ny + 1; gz = nz + 1; break;
+    case BK_LCELLS: gx = cdiv(nx, 128); gy = ny; gz = nz; break;
+    case BK_CELLS_X: gx = cdiv(nx, kLineUpd); gy = cdiv(ny, kLineWarps); gz = nz; break;
+    case BK_CELLS_Y: gx = cdiv(nx, kLineWarps); gy = cdiv(ny, kLineUpd); gz = nz; break;
+    case BK_CELLS_Z: gx = cdiv(nx, kLineWarps); gy = cdiv(nz, kLineUpd); gz = ny; break;
+    case BK_NODES_X: gx = cdiv(nx + 1, kLineUpd); gy = cdiv(ny + 1, kLineWarps); gz = nz + 1; break;
+    case BK_NODES_Y: gx = cdiv(nx + 1, kLineWarps); gy = cdiv(ny + 1, kLineUpd); gz = nz + 1; break;
+    default: gx = cdiv(nx + 1, kLineWarps); gy = cdiv(nz + 1, kLineUpd); gz = ny + 1; break;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_bat_lagrange_nodes(const CycleArgs* __restrict__ D,
+                                                            const int4* __restrict__ W, int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    k_cyc_lagrange_nodes_body(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, t.y, t.z, t.w);
+  }
+}
+
+__global__ void __launch_bounds__(128, 3) k_bat_lagrange_cells(const CycleArgs* __restrict__ D,
+                                                               const int4* __restrict__ W, int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    k_cyc_lagrange_cells_body<1>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
+                                 a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
+  }
+}
+
+template <bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_x(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    k_cyc_sweep_cells_x_body<LAST>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1], a.dpf,
+                                   a.st, t.y, t.z, t.w);
+  }
+}
+
+template <int DD, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_t(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    __syncthreads();
+    k_cyc_sweep_cells_t_body<DD, LAST>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+                                       a.dpf, a.st, t.y, t.z, t.w);
+  }
+}
+
+template <bool FIRST, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_nodes_x(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+                                             a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
+  }
+}
+
+template <int DD, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_nodes_t(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    __syncthreads();
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+                                                 a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y,
+                                                 t.z, t.w);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_bat_dt_min(const CycleArgs* __restrict__ D, const int4* __restrict__ W,
+                                                    int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    __syncthreads();
+    dt_min_body(a.dm, a.S, a.L, a.st.cs, a.vnorm, t.y, t.z, t.w);
+  }
+}
+
+// one thread per instance: each instance's own dt (per-instance options)
+__global__ void k_bat_dt_finish(const CycleArgs* __restrict__ D, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dt_finish_body(D[i].S, D[i].ph);
+}
+
+// Resident blocks of a persistent grid for `kernel`: SMs x blocks per SM
+// (queried once per kernel and device).
+template <class Kern>
+static int persistent_blocks(Kern kernel, int threads, int nwork) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int g = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+    auto itc = cache.find(key);
+    if (itc == cache.end()) {
+      int sms = 0, per = 0;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+      itc = cache.emplace(key, (per > 0 ? per : 1) * (sms > 0 ? sms : 1)).first;
+    }
+    g = itc->second;
+  }
+  return nwork < g ? (nwork > 0 ? nwork : 1) : g;
+}
+
+template <class Kern, class... Args>
+static void launch_persistent(Kern kernel, int threads, int nwork, cudaStream_t s, Args... args) {
+  if (nwork <= 0) return;
+  kernel<<<persistent_blocks(kernel, threads, nwork), threads, 0, s>>>(args...);
+}
+
+template <int DD, bool LAST>
+static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s) {
+  const int T = 32 * kLineWarps, kind = BK_CELLS_X + DD;
+  if constexpr (DD == 0) launch_persistent(k_bat_sweep_cells_x<LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
+  else launch_persistent(k_bat_sweep_cells_t<DD, LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
+}
+
+template <int DD, bool FIRST, bool LAST>
+static void bat_nodes_d(const BatchPlan& P, int it, int prev, cudaStream_t s) {
+  const int T = 32 * kLineWarps, kind = BK_NODES_X + DD;
+  if constexpr (DD == 0)
+    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
+  else
+    launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
+}
+
+template <int DD>
+static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s) {
+  const bool first = it == 0, last = it == 2;
+  if (last) bat_cells_d<DD, true>(P, it, s);
+  else bat_cells_d<DD, false>(P, it, s);
+  if (first) bat_nodes_d<DD, true, false>(P, it, prev, s);
+  else if (last) bat_nodes_d<DD, false, true>(P, it, prev, s);
+  else bat_nodes_d<DD, false, false>(P, it, prev, s);
+}
+
+void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s) {
+  launch_persistent(k_bat_lagrange_nodes, 128, P.nwork[BK_LNODES], s, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+  launch_persistent(k_bat_lagrange_cells, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  int prev = 0;
+  for (int it = 0; it < 3; ++it) {
+    const int d = (it + sens) % 3;
+    if (d == 0) bat_sweep<0>(P, it, prev, s);
+    else if (d == 1) bat_sweep<1>(P, it, prev, s);
+    else bat_sweep<2>(P, it, prev, s);
+    prev |= 1 << d;
+  }
+  launch_persistent(k_bat_dt_min, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  k_bat_dt_finish<<<(P.ninst + 127) / 128, 128, 0, s>>>(P.descs, P.ninst);
 }
 
 }  // namespace mhy

@@ -112,57 +112,13 @@ __global__ void k_node_mass(Dims dm, const double* __restrict__ mass, double* __
   nm[n] = .125 * s;
 }
 
-// computeHydroDeltaT (MahycoModule.cc:2047-2061): min over cells of
-// L / (c + max |v|) (|v| per node precomputed), warp shuffle + block
-// reduction, one atomicMin per block on the bit pattern (non-negative doubles
-// order like unsigned integers).
+// The dt reduction kernels; their bodies (dt_min_body, dt_finish_body) are in
+// mhy_kernels.cuh so that the batched cycle can run them per instance.
 __global__ void k_dt_min(Dims dm, Scalars* __restrict__ S, const double* __restrict__ L,
                          const double* __restrict__ cs, const double* __restrict__ vnorm) {
-  __shared__ unsigned long long wmin[32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  unsigned long long best = 0x7fefffffffffffffull;  // DBL_MAX
-  if (i < dm.nx) {
-    const long long c = dm.cid(i, j, k);
-    double vmax = 0.;
-    for (int a = 0; a < 8; ++a) {
-      long long n = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
-      vmax = amax(vnorm[n], vmax);
-    }
-    double dx_sound = L[c] / (cs[c] + vmax);
-    if (dx_sound >= 0.) best = (unsigned long long)__double_as_longlong(dx_sound);
-    else atomicOr(&S->status, MHY_STATUS_NAN_DT);
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
-    best = other < best ? other : best;
-  }
-  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    best = threadIdx.x < (blockDim.x >> 5) ? wmin[threadIdx.x] : 0x7fefffffffffffffull;
-    for (int o = 16; o > 0; o >>= 1) {
-      unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
-      best = other < best ? other : best;
-    }
-    if (threadIdx.x == 0) atomicMin(&S->min_bits, best);
-  }
+  dt_min_body(dm, S, L, cs, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-// computeDeltaT (MahycoModule.cc:2076-2191): new dt from the reduced minimum.
-__global__ void k_dt_finish(Scalars* S, Phys ph) {
-  S->time += S->dt;
-  const double gold = S->dt;
-  S->old_dt = gold;
-  const double minimum_aux = __longlong_as_double((long long)S->min_bits);
-  double new_dt = ph.cfl * minimum_aux;
-  new_dt = amin(new_dt, 1.05 * gold);
-  new_dt = amin(new_dt, ph.deltat_max);
-  if (new_dt < ph.deltat_min) S->status |= MHY_STATUS_DT_MIN;
-  S->dt = new_dt;
-  S->inv_dt = 1.0 / new_dt;
-  if (S->time > ph.final_time) S->status |= MHY_STATUS_FINAL_TIME;
-  S->min_bits = 0x7fefffffffffffffull;
-  S->iteration += 1;
-}
+__global__ void k_dt_finish(Scalars* S, Phys ph) { dt_finish_body(S, ph); }
 
 }  // namespace mhy

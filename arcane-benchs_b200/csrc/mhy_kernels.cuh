@@ -92,6 +92,22 @@ void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s);
 void launch_init_env(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycleEnv = 11;
 
+// Batched cycle of many independent single-environment meshes.  Each kernel
+// type has a work table: one (instance, bx, by, bz) entry per block of the
+// instance's own grid; a persistent grid of resident blocks walks the table.
+// The arguments of instance i are descs[i] in device memory.
+enum BatchKernel { BK_LNODES = 0, BK_LCELLS, BK_CELLS_X, BK_CELLS_Y, BK_CELLS_Z, BK_NODES_X, BK_NODES_Y, BK_NODES_Z,
+                   BK_COUNT };
+struct BatchPlan {
+  const CycleArgs* descs;       // device, one per instance
+  int ninst;
+  const int4* work[BK_COUNT];   // device work tables
+  int nwork[BK_COUNT];
+};
+void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz);
+void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s);
+constexpr int kKernelsPerCycleBatch = 10;
+
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);
 __global__ void k_init_faces(Dims dm, const double* x0, double* n0, double* xf0);
 __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* xf0, double* ofn);
@@ -100,5 +116,59 @@ __global__ void k_init_state(Dims dm, double gamma, const double* vol, double* r
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
 __global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm);
 __global__ void k_dt_finish(Scalars* S, Phys ph);
+
+// computeHydroDeltaT (MahycoModule.cc:2047-2061): min over cells of
+// L / (c + max |v|) (|v| per node precomputed), warp shuffle + block
+// reduction, one atomicMin per block on the bit pattern (non-negative doubles
+// order like unsigned integers).
+__device__ __forceinline__ void dt_min_body(Dims dm, Scalars* __restrict__ S, const double* __restrict__ L,
+                                            const double* __restrict__ cs, const double* __restrict__ vnorm,
+                                            int bx_, int by_, int bz_) {
+  __shared__ unsigned long long wmin[32];
+  const int i = bx_ * blockDim.x + threadIdx.x, j = by_, k = bz_;
+  unsigned long long best = 0x7fefffffffffffffull;  // DBL_MAX
+  if (i < dm.nx) {
+    const long long c = dm.cid(i, j, k);
+    double vmax = 0.;
+    for (int a = 0; a < 8; ++a) {
+      long long n = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+      vmax = amax(vnorm[n], vmax);
+    }
+    double dx_sound = L[c] / (cs[c] + vmax);
+    if (dx_sound >= 0.) best = (unsigned long long)__double_as_longlong(dx_sound);
+    else atomicOr(&S->status, MHY_STATUS_NAN_DT);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
+    best = other < best ? other : best;
+  }
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    best = threadIdx.x < (blockDim.x >> 5) ? wmin[threadIdx.x] : 0x7fefffffffffffffull;
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
+      best = other < best ? other : best;
+    }
+    if (threadIdx.x == 0) atomicMin(&S->min_bits, best);
+  }
+}
+
+// computeDeltaT (MahycoModule.cc:2076-2191): new dt from the reduced minimum.
+__device__ __forceinline__ void dt_finish_body(Scalars* S, const Phys& ph) {
+  S->time += S->dt;
+  const double gold = S->dt;
+  S->old_dt = gold;
+  const double minimum_aux = __longlong_as_double((long long)S->min_bits);
+  double new_dt = ph.cfl * minimum_aux;
+  new_dt = amin(new_dt, 1.05 * gold);
+  new_dt = amin(new_dt, ph.deltat_max);
+  if (new_dt < ph.deltat_min) S->status |= MHY_STATUS_DT_MIN;
+  S->dt = new_dt;
+  S->inv_dt = 1.0 / new_dt;
+  if (S->time > ph.final_time) S->status |= MHY_STATUS_FINAL_TIME;
+  S->min_bits = 0x7fefffffffffffffull;
+  S->iteration += 1;
+}
 
 }  // namespace mhy

@@ -101,13 +101,14 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
 }
 
 template <int K>
-__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Scalars* __restrict__ S, Phys ph,
+__device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
     double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
     const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
     double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
-    EnvState env, double* __restrict__ Vlag) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    EnvState env, double* __restrict__ Vlag,
+    int bx_, int by_, int bz_) {
+  const int i = bx_ * blockDim.x + threadIdx.x, j = by_, k = bz_;
   if (i >= dm.nx) return;
   const long long c = dm.cid(i, j, k);
   const long long C = dm.C;
@@ -266,6 +267,16 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Sc
       fd.db[d][f - off] = dot(xf - xc, nrm);
     }
   }
+}
+
+template <int K>
+__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Scalars* __restrict__ S, Phys ph,
+    const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
+    double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
+    const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
+    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
+    EnvState env, double* __restrict__ Vlag) {
+  k_cyc_lagrange_cells_body<K>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, L, U, xcs, fd, env, Vlag, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 

@@ -364,16 +364,17 @@ __device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int i
 
 // Node sweep along x: lanes run along the rows of nodes.
 template <bool FIRST, bool LAST, int K>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
+__device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
+    int bx_, int by_, int bz_) {
   const int lane = threadIdx.x & 31;
-  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
   if (j > dm.ny) return;                               // whole warp leaves together
   const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
-  const int m = blockIdx.x * kLineUpd - 2 + lane;      // position of this lane's node along x
+  const int m = bx_ * kLineUpd - 2 + lane;      // position of this lane's node along x
   const bool valid = m >= 0 && m <= nx;
   const bool inner = m >= 1 && m <= nx - 1;
   const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
@@ -438,6 +439,15 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
   }
 }
 
+template <bool FIRST, bool LAST, int K>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
+  k_cyc_sweep_nodes_x_body<FIRST, LAST, K>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
 // Block (bx, by, bz): node x = 8 bx .. 8 bx + 7, positions 28 by - 2 ..
 // 28 by + 29 along D, bz = the remaining node coordinate o (z for D = 1, y
@@ -446,11 +456,12 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
 // the last sweep) are staged as [o - 1 + q][x - 8 bx + 1][position], with zero
 // for cells outside the mesh (adding +0 to these sums changes no bit).
 template <int D, bool FIRST, bool LAST, int K>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
+__device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
+    int bx_, int by_, int bz_) {
   constexpr int NA = FIRST ? 5 : 9;                   // vh x3, x0[D], nm or U_dual x5
   constexpr int NT = LAST ? K + 1 : K;                // cell tiles: dual mass flux per environment (+ mass)
   constexpr int CT = 2 * (kLineWarps + 1) * 32;       // elements of one cell tile
@@ -458,7 +469,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
   __shared__ double tile[NA * kTileArr];
   __shared__ double ctile[NT * CT];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int i0 = bx_ * kLineWarps, seg0 = by_ * kLineUpd - 2, o = bz_;
   const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
   const int nn = dm.ncd(D) + 1, no = D == 1 ? nz : ny;   // cells along D; cells along the remaining axis
   auto node_id = [&](int i, int m) { return D == 1 ? i + (nx + 1) * (m + (ny + 1) * o) : i + (nx + 1) * (o + (ny + 1) * m); };
@@ -564,6 +575,15 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
     vout[sn] = r[0]; vout[N + sn] = r[kTileArr]; vout[2 * N + sn] = r[2 * kTileArr];
     nm_out[sn] = r[3 * kTileArr]; vnorm[sn] = r[4 * kTileArr];
   }
+}
+
+template <int D, bool FIRST, bool LAST, int K>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
+  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------------

@@ -33,7 +33,10 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_compute_delta_t", "mhy_step", "mhy_synchronize", "mhy_get_field", "mhy_get_dt",
             "mhy_get_time", "mhy_get_status", "mhy_get_sizes", "mhy_get_stream", "mhy_kernels_per_cycle",
             "mhy_last_error", "mhy_destroy", "mhy_compute_hydro_dt_noalloc", "mhy_get_env_field",
-            "mhy_get_env_mask"]
+            "mhy_get_env_mask", "mhy_batch_create", "mhy_batch_set_state", "mhy_batch_hydro_start_init",
+            "mhy_batch_step", "mhy_batch_synchronize", "mhy_batch_get_field", "mhy_batch_get_dt",
+            "mhy_batch_get_status", "mhy_batch_size", "mhy_batch_kernels_per_cycle", "mhy_batch_get_stream",
+            "mhy_batch_destroy"]
 ENV_FIELDS = {"fracvol": 0, "density": 1, "internal_energy": 2, "pressure": 3, "sound_speed": 4,
               "mass_fraction": 5, "cell_mass": 6}
 
@@ -106,6 +109,21 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_compute_hydro_dt_noalloc.restype = ctypes.c_int
     L.mhy_get_env_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t]
     L.mhy_get_env_mask.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_size_t]
+    L.mhy_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(CMesh), ctypes.POINTER(COptions), ctypes.c_int,
+                                   ctypes.POINTER(vp)]
+    L.mhy_batch_set_state.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CState)]
+    for name in ["mhy_batch_hydro_start_init", "mhy_batch_synchronize", "mhy_batch_size",
+                 "mhy_batch_kernels_per_cycle"]:
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = ctypes.c_int
+    L.mhy_batch_step.argtypes = [vp, ctypes.c_int]
+    L.mhy_batch_get_field.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t]
+    L.mhy_batch_get_dt.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.mhy_batch_get_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]
+    L.mhy_batch_get_stream.argtypes = [vp]
+    L.mhy_batch_get_stream.restype = vp
+    L.mhy_batch_destroy.argtypes = [vp]
+    L.mhy_batch_destroy.restype = None
     _lib = L
     return L
 
@@ -223,6 +241,77 @@ class Context:
     def close(self):
         if getattr(self, "h", None):
             load().mhy_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent single-environment meshes advanced together on one GPU (mhy_batch)."""
+
+    def __init__(self, cases, device: int = -1, init: bool = True):
+        L = load()
+        self.cases = list(cases)
+        n = len(self.cases)
+        self._keep = []
+        meshes = (CMesh * n)()
+        opts = (COptions * n)()
+        for i, c in enumerate(self.cases):
+            xyz = np.ascontiguousarray(c.coords, dtype=np.float64)
+            self._keep.append(xyz)
+            meshes[i] = CMesh(c.nx, c.ny, c.nz, _dp(xyz))
+            opts[i] = make_options(c.options, c.gamma)
+        h = ctypes.c_void_p()
+        _check(L.mhy_batch_create(n, meshes, opts, device, ctypes.byref(h)))
+        self.h = h
+        for i, c in enumerate(self.cases):
+            arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (c.fracvol, c.density, c.pressure, c.velocity)]
+            st = CState(*[_dp(a) for a in arrs])
+            _check(L.mhy_batch_set_state(self.h, i, ctypes.byref(st)))
+        if init:
+            _check(L.mhy_batch_hydro_start_init(self.h))
+
+    def step(self, ncycles: int = 1):
+        _check(load().mhy_batch_step(self.h, int(ncycles)))
+
+    def synchronize(self):
+        _check(load().mhy_batch_synchronize(self.h))
+
+    def dt(self, i: int):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(load().mhy_batch_get_dt(self.h, int(i), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def status(self, i: int) -> int:
+        f = ctypes.c_uint32()
+        _check(load().mhy_batch_get_status(self.h, int(i), ctypes.byref(f)))
+        return f.value
+
+    def kernels_per_cycle(self) -> int:
+        return load().mhy_batch_kernels_per_cycle(self.h)
+
+    def stream(self) -> int:
+        return load().mhy_batch_get_stream(self.h) or 0
+
+    def field(self, i: int, name: str) -> np.ndarray:
+        c = self.cases[i]
+        if name in ("velocity", "node_coord"):
+            out = np.empty((c.nnodes, 3))
+        elif name == "node_mass":
+            out = np.empty(c.nnodes)
+        else:
+            out = np.empty(c.ncells)
+        _check(load().mhy_batch_get_field(self.h, int(i), FIELDS[name], out.ctypes.data_as(ctypes.c_void_p),
+                                          out.nbytes))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().mhy_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

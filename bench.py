@@ -32,7 +32,7 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "arcane-benchs_b200"))
 
 METRIC = "cell-cycles/s"
-WORKLOADS = ("sedov", "two_material", "sphere_inclusion")
+WORKLOADS = ("sedov", "two_material", "sphere_inclusion", "batched")
 
 
 def make_case(args):
@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=WORKLOADS, default="sedov",
                     help="sedov: Sedov 128^3 (the headline); two_material: 256x128x128, two gases; "
-                         "sphere_inclusion: 384x384x192, two gases")
+                         "sphere_inclusion: 384x384x192, two gases; batched: 64 Sod/Sedov instances of "
+                         "32^3..96^3 advanced together (instances split across GPUs)")
     ap.add_argument("--n", type=int, default=128, help="Sedov mesh cells per direction")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -142,8 +143,10 @@ def run_reference(args):
         return 0
     sys.path.insert(0, str(ROOT / "oracle"))
     import mhy_oracle
-    case, wname = make_case(args)
     threads = os.cpu_count() or 1
+    if args.workload == "batched":
+        return run_reference_batched(args, threads)
+    case, wname = make_case(args)
     o = mhy_oracle.Oracle(case, pow_mode="libm", threads=threads)
     t0 = time.perf_counter()
     o.step(max(1, args.warmup))
@@ -163,6 +166,134 @@ def run_reference(args):
             "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_batched(args, threads):
+    """--impl reference --workload batched: the instances advanced one after
+    the other on the host cores by the oracle, a bounded sample: every
+    instance in turn for two cycles until the time budget is spent."""
+    import mhy_oracle
+    from mhy_b200 import gen
+    cases = gen.batched()
+    budget_s, done, el, n_inst = 90.0, 0, 0.0, 0
+    for c in cases:
+        o = mhy_oracle.Oracle(c, pow_mode="libm", threads=threads)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(2)
+        el += time.perf_counter() - t0
+        done += 2 * c.ncells
+        n_inst += 1
+        o.close()
+        if el > budget_s:
+            break
+    val = done / el
+    sample = (f"{n_inst} of {len(cases)} instances, 2 cycles each after 1 untimed cycle "
+              f"(bounded to ~{budget_s:.0f} s), OpenMP {threads} threads")
+    line = {"metric": METRIC, "value": val, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+            "steps": 2, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched-64-sod-sedov-32..96^3-fp64", "instances": len(cases),
+                       "cells": sum(c.ncells for c in cases)},
+            "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours_batched(args):
+    """The batched form: 64 independent uneven instances in one set of
+    persistent launches per cycle, per-instance dt on the device.  With N GPUs
+    the instance list is split round-robin (strong scaling: the job is fixed)."""
+    import numpy as np
+    import torch
+    import mhy_b200
+    from mhy_b200 import gen, bytes_model, replicas
+
+    world, rank, local = replicas.ranks()
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        replicas.init("nccl", device=dev)
+    all_cases = gen.batched()
+    mine = [c for i, c in enumerate(all_cases) if i % world == rank]
+    cells = sum(c.ncells for c in mine)
+    b = mhy_b200.Batch(mine, device=local)
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    b.step(args.warmup)
+    b.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        replicas.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        b.step(args.steps)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        replicas.barrier()
+    ms, value = replicas.aggregate(cells, args.steps, start.elapsed_time(stop), dev)
+    status = max(b.status(i) for i in range(len(mine)))
+    kpc = b.kernels_per_cycle()
+    b.close()
+
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+        hcases = [gen.Case(c.name, c.nx, c.ny, c.nz, pinned(c.coords), c.gamma, pinned(c.fracvol), pinned(c.density),
+                           pinned(c.pressure), pinned(c.velocity), c.options, c.cycles) for c in mine]
+        outs = [(pinned(np.zeros(c.ncells)), pinned(np.zeros(c.ncells)), pinned(np.zeros((c.nnodes, 3))))
+                for c in mine]
+        L = mhy_b200.load()
+        replicas.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b2 = mhy_b200.Batch(hcases, device=local)
+        for _ in range(args.steps):
+            b2.step(1)
+            b2.dt(0)                                   # D2H of a step result + sync, every cycle
+        for i, (r, e, v) in enumerate(outs):
+            for name, arr in (("density", r), ("internal_energy", e), ("velocity", v)):
+                mhy_b200._check(L.mhy_batch_get_field(b2.h, i, mhy_b200.FIELDS[name],
+                                                      arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes))
+        el = time.perf_counter() - t0
+        b2.close()
+        el_ms, e2e_value = replicas.aggregate(cells, args.steps, el * 1e3, dev)
+        h2d = sum(c.coords.nbytes + c.fracvol.nbytes + c.density.nbytes + c.pressure.nbytes + c.velocity.nbytes
+                  for c in mine) / args.steps
+        d2h = 16 + sum(r.nbytes + e.nbytes + v.nbytes for r, e, v in outs) / args.steps
+        e2e = {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": round(h2d, 1),
+               "d2h_bytes_per_step": round(d2h, 1),
+               "path": "mhy_batch_create+set_state+hydro_start_init, per-cycle mhy_batch_step + mhy_batch_get_dt, "
+                       "mhy_batch_get_field x3 per instance; wall clock, max over ranks"}
+
+    b_cells = sum(c.ncells * bytes_model.bytes_per_cell_cycle(c.ncells, c.nnodes) for c in mine)
+    peak, peak_kind = measured_peak()
+    achieved = b_cells * args.steps / (ms / 1e3) / 1e9 / (world if world > 1 else 1)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "kernel": f"one batched cycle graph ({kpc} persistent launches), algorithmic bytes "
+                          f"{b_cells / cells:.1f} B/cell-cycle averaged over this GPU's instances"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(mine[1], args.cpu_sample_cycles, f"batch instance 1 ({mine[1].nx}^3 Sedov)")
+    if rank == 0:
+        total = sum(c.ncells for c in all_cases)
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "batched-64-sod-sedov-32..96^3-fp64", "instances": len(all_cases),
+                           "cells": total, "cells_per_gpu": cells, "parallelism": f"instances split over {world}",
+                           "l2": "working set > 126 MB L2 (no flush needed)"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kpc * args.steps,
+                "clocks": clk.summary(), "device_status": status}
+        print(json.dumps(line), flush=True)
+    replicas.finish()
     return 0
 
 
@@ -269,6 +400,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_ours_batched(args)
     return run_ours(args)
 
 

@@ -169,6 +169,28 @@ int mhy_kernels_per_cycle(mhy_ctx* ctx);
 const char* mhy_last_error(void);
 void mhy_destroy(mhy_ctx* ctx);
 
+/* ---- batches: many independent single-environment meshes on one GPU ----
+ * No counterpart in the reference (one Arcane process runs one mesh): a batch
+ * advances n instances of uneven sizes, options and initial states together,
+ * each kernel of the cycle launched once for all instances (persistent grids
+ * walking a per-instance work table), each instance with its own dt on the
+ * device; the whole cycle is replayed from a CUDA graph.  Instance i is set up
+ * exactly as a context (mesh i, options i, state i) and its results equal a
+ * context's bit for bit.  Every instance must have nb_env == 1. */
+typedef struct mhy_batch mhy_batch;
+int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts, int device, mhy_batch** out);
+int mhy_batch_set_state(mhy_batch* b, int i, const mhy_state* st);
+int mhy_batch_hydro_start_init(mhy_batch* b);          /* all instances */
+int mhy_batch_step(mhy_batch* b, int ncycles);         /* ncycles cycles of every instance */
+int mhy_batch_synchronize(mhy_batch* b);               /* MHY_ERR_DT_MIN / MHY_ERR_NUMERIC if any instance raised it */
+int mhy_batch_get_field(mhy_batch* b, int i, int field, void* dst, size_t bytes);
+int mhy_batch_get_dt(mhy_batch* b, int i, double* dt, double* dt_old);
+int mhy_batch_get_status(mhy_batch* b, int i, uint32_t* flags);
+int mhy_batch_size(mhy_batch* b);
+int mhy_batch_kernels_per_cycle(mhy_batch* b);
+void* mhy_batch_get_stream(mhy_batch* b);
+void mhy_batch_destroy(mhy_batch* b);
+
 /* CFL time step from device-resident fields, for callers that cannot allocate
  * device memory (a host framework that owns all device allocations, or code
  * recording into a stream capture).  No counterpart in the reference: it is the
