@@ -509,6 +509,10 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
     for (int i = 0; i < n; ++i) {
       int gx, gy, gz;
       batch_work_shape(b->inst[i]->dm, k, gx, gy, gz);
+      if (gy < 0) {                             // linear chunks of consecutive items
+        for (int x = 0; x < gx; ++x) w.push_back(make_int4(i, x, -1, 0));
+        continue;
+      }
       for (int z = 0; z < gz; ++z)
         for (int y = 0; y < gy; ++y)
           for (int x = 0; x < gx; ++x) w.push_back(make_int4(i, x, y, z));

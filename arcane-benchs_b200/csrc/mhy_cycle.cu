@@ -31,8 +31,8 @@ __device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars
     const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
     double* __restrict__ vh,
     int bx_, int by_, int bz_) {
-  const int i = bx_ * blockDim.x + threadIdx.x, j = by_, k = bz_;
-  if (i > dm.nx) return;
+  int i, j, k;
+  if (!block_item(dm.nx + 1, dm.ny + 1, dm.nz + 1, bx_, by_, bz_, i, j, k)) return;
   const long long n = dm.nid(i, j, k);
   const double dtv = 0.5 * (S->old_dt + S->dt);
   const int loc[2][2][2] = {{{0, 4}, {3, 7}}, {{1, 5}, {2, 6}}};
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scala
     const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ cqs,
     const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
     double* __restrict__ vh) {
-  k_cyc_lagrange_nodes_body(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_lagrange_nodes_body(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, blockIdx.x, -1, 0);
 }
 
 
@@ -231,15 +231,27 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
   }
 }
 
+// Node kernel: 128 consecutive nodes per block (rows of nx+1 nodes would leave
+// most of a second block idle).
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
-  const dim3 nbn((a.dm.nx + 1 + 127) / 128, a.dm.ny + 1, a.dm.nz + 1);
+  const unsigned nbn = (unsigned)((a.dm.N + 127) / 128);
   k_cyc_lagrange_nodes<<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh);
 }
 
+// Cell kernels: rows of 128 cells when nx is a multiple of 128, else 128
+// consecutive cells per block.
+dim3 cell_grid(const Dims& dm, int& linear) {
+  linear = dm.nx % 128 != 0;
+  if (linear) return dim3((unsigned)((dm.C + 127) / 128), 1, 1);
+  return dim3(dm.nx / 128, dm.ny, dm.nz);
+}
+
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
-  const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
+  int linear;
+  const dim3 nbc = cell_grid(a.dm, linear);
   k_cyc_lagrange_cells<1><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
-                                              a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag);
+                                              a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag,
+                                              linear);
 }
 
 // Three sweeps d = (i + sens) % 3 (RemapADIService.cc:28-30).  U: Lagrange
@@ -264,8 +276,9 @@ void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
 }
 
 void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
-  const dim3 nbc((a.dm.nx + 127) / 128, a.dm.ny, a.dm.nz);
-  k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.vnorm);
+  int linear;
+  const dim3 nbc = cell_grid(a.dm, linear);
+  k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.vnorm, linear);
   k_dt_finish<<<1, 1, 0, s>>>(a.S, a.ph);
 }
 
@@ -279,8 +292,11 @@ void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz) {
   const int nx = dm.nx, ny = dm.ny, nz = dm.nz;
   auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
   switch (kind) {
-    case BK_LNODES: gx = cdiv(nx + 1, 128); gy = ny + 1; gz = nz + 1; break;
-    case BK_LCELLS: gx = cdiv(nx, 128); gy = ny; gz = nz; break;
+    case BK_LNODES: gx = (int)cdiv((int)dm.N, 128); gy = -1; gz = 1; break;      // linear chunks
+    case BK_LCELLS:
+      if (nx % 128) { gx = (int)cdiv((int)dm.C, 128); gy = -1; gz = 1; }        // linear chunks
+      else { gx = nx / 128; gy = ny; gz = nz; }
+      break;
     case BK_CELLS_X: gx = cdiv(nx, kLineUpd); gy = cdiv(ny, kLineWarps); gz = nz; break;
     case BK_CELLS_Y: gx = cdiv(nx, kLineWarps); gy = cdiv(ny, kLineUpd); gz = nz; break;
     case BK_CELLS_Z: gx = cdiv(nx, kLineWarps); gy = cdiv(nz, kLineUpd); gz = ny; break;

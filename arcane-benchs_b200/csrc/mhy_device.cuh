@@ -151,6 +151,25 @@ struct Dims {
   }
 };
 
+// Item (i, j, k) of thread threadIdx.x in block (bx, by, bz) over an
+// ex x ey x ez lattice: by >= 0: rows of blockDim.x items along x (block
+// (bx, by, bz) = x chunk, y, z); by < 0: blockDim.x consecutive items of the
+// whole lattice (block bx), which wastes no thread when ex is not a multiple
+// of the block size.  False when the thread has no item.
+__device__ __forceinline__ bool block_item(int ex, int ey, int ez, int bx, int by, int bz, int& i, int& j, int& k) {
+  if (by >= 0) {
+    i = bx * blockDim.x + threadIdx.x; j = by; k = bz;
+    return i < ex;
+  }
+  const int c = bx * blockDim.x + threadIdx.x;
+  if (c >= ex * ey * ez) { i = j = k = 0; return false; }
+  i = c % ex;
+  const int t = c / ex;
+  j = t % ey;
+  k = t / ey;
+  return true;
+}
+
 // SN_trigo node offsets of a cell, cartesian/CartConnectivityCellNode.h:83-94
 __device__ __constant__ const int kCellNodeOff[8][3] = {{0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1}};
 

@@ -115,8 +115,8 @@ __global__ void k_node_mass(Dims dm, const double* __restrict__ mass, double* __
 // The dt reduction kernels; their bodies (dt_min_body, dt_finish_body) are in
 // mhy_kernels.cuh so that the batched cycle can run them per instance.
 __global__ void k_dt_min(Dims dm, Scalars* __restrict__ S, const double* __restrict__ L,
-                         const double* __restrict__ cs, const double* __restrict__ vnorm) {
-  dt_min_body(dm, S, L, cs, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+                         const double* __restrict__ cs, const double* __restrict__ vnorm, int linear) {
+  dt_min_body(dm, S, L, cs, vnorm, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
 }
 
 __global__ void k_dt_finish(Scalars* S, Phys ph) { dt_finish_body(S, ph); }

@@ -114,7 +114,8 @@ __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* x
 __global__ void k_init_state(Dims dm, double gamma, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
-__global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm);
+__global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm, int linear);
+dim3 cell_grid(const Dims& dm, int& linear);
 __global__ void k_dt_finish(Scalars* S, Phys ph);
 
 // computeHydroDeltaT (MahycoModule.cc:2047-2061): min over cells of
@@ -125,9 +126,10 @@ __device__ __forceinline__ void dt_min_body(Dims dm, Scalars* __restrict__ S, co
                                             const double* __restrict__ cs, const double* __restrict__ vnorm,
                                             int bx_, int by_, int bz_) {
   __shared__ unsigned long long wmin[32];
-  const int i = bx_ * blockDim.x + threadIdx.x, j = by_, k = bz_;
+  int i, j, k;
+  const bool has = block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k);
   unsigned long long best = 0x7fefffffffffffffull;  // DBL_MAX
-  if (i < dm.nx) {
+  if (has) {
     const long long c = dm.cid(i, j, k);
     double vmax = 0.;
     for (int a = 0; a < 8; ++a) {

@@ -108,8 +108,8 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
     EnvState env, double* __restrict__ Vlag,
     int bx_, int by_, int bz_) {
-  const int i = bx_ * blockDim.x + threadIdx.x, j = by_, k = bz_;
-  if (i >= dm.nx) return;
+  int i, j, k;
+  if (!block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k)) return;
   const long long c = dm.cid(i, j, k);
   const long long C = dm.C;
   const double dt = S->dt;
@@ -275,8 +275,8 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Sc
     double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
     const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
     double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
-    EnvState env, double* __restrict__ Vlag) {
-  k_cyc_lagrange_cells_body<K>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, L, U, xcs, fd, env, Vlag, blockIdx.x, blockIdx.y, blockIdx.z);
+    EnvState env, double* __restrict__ Vlag, int linear) {
+  k_cyc_lagrange_cells_body<K>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, L, U, xcs, fd, env, Vlag, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
 }
 
 
