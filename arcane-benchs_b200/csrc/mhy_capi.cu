@@ -141,7 +141,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
     return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0 (minmod), 1 (superBee) or 2 (vanLeer)");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
-  if (opt->precision != 0) return fail(MHY_ERR_UNSUPPORTED, "precision mode not implemented");
+  if (opt->precision < 0 || opt->precision > 1) return fail(MHY_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
+  if (opt->precision == 1 && opt->nb_env != 1)
+    return fail(MHY_ERR_UNSUPPORTED, "the mixed-precision form is implemented for one environment");
   for (int b = 0; b < opt->nb_bc; ++b)
     if (opt->bc[b].surface < 0 || opt->bc[b].surface > 5 || opt->bc[b].type < 0 || opt->bc[b].type > 2)
       return fail(MHY_ERR_ARG, "bad boundary condition");
@@ -168,6 +170,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   ph.deltat_min = opt->deltat_min; ph.deltat_max = opt->deltat_max; ph.final_time = opt->final_time;
   ph.lc_mode = opt->longueur_caracteristique; ph.pseudo_centree = opt->pseudo_centree;
   ph.ordre_projection = opt->ordre_projection; ph.limiteur_id = opt->projection_limiteur_id;
+  ph.precision = opt->precision;
   c->bct.nb = opt->nb_bc;
   for (int b = 0; b < opt->nb_bc; ++b) { c->bct.type[b] = opt->bc[b].type; c->bct.value[b] = opt->bc[b].value; }
   c->h_coords.assign(mesh->node_coords, mesh->node_coords + 3 * dm.N);
@@ -491,8 +494,10 @@ void mhy_batch_destroy(mhy_batch* b) {
 int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts, int device, mhy_batch** out) {
   if (!meshes || !opts || !out || n <= 0) return fail(MHY_ERR_ARG, "null argument or empty batch");
   *out = nullptr;
-  for (int i = 0; i < n; ++i)
+  for (int i = 0; i < n; ++i) {
     if (opts[i].nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "batched instances must have one environment");
+    if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
+  }
   mhy_batch* b = new mhy_batch();
   for (int i = 0; i < n; ++i) {
     mhy_ctx* c = nullptr;
@@ -527,6 +532,7 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
   b->plan.descs = b->d_descs;
   b->plan.ninst = n;
+  b->plan.precision = opts[0].precision;
   *out = b;
   return MHY_OK;
 }

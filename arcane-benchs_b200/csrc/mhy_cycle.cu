@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scala
 
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
-template <bool LAST>
+template <bool LAST, typename R>
 __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -105,7 +105,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
     if (LAST) in.vol = st.Ve[c];
   }
   double out[LAST ? kCellOutLast : kCellOutMid];
-  cell_line<LAST>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   if (!upd) return;
   if (!LAST) {
 #pragma unroll
@@ -117,18 +117,18 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   }
 }
 
-template <bool LAST>
+template <bool LAST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_x_body<LAST>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_cells_x_body<LAST, R>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Cell sweep along y (D = 1) or z (D = 2), staged through shared memory.
 // Block (bx, by, bz): x = 8 bx .. 8 bx + 7, positions 28 by - 2 .. 28 by + 29
 // along D, and bz = the remaining coordinate (z for D = 1, y for D = 2).
-template <int D, bool LAST>
+template <int D, bool LAST, typename R>
 __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -184,7 +184,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   in.vol = LAST ? row[(NA - 1) * kTileArr] : 0.;
   constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
   double out[NO];
-  cell_line<LAST>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   // each lane overwrites only the tile column it read itself
   if (upd) {
 #pragma unroll
@@ -203,18 +203,18 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool LAST>
+template <int D, bool LAST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_t_body<D, LAST>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_cells_t_body<D, LAST, R>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int D>
+template <int D, typename R>
 static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
@@ -222,12 +222,12 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
   const int T = 32 * kLineWarps;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
-    if (last) k_cyc_sweep_cells_x<true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-    else k_cyc_sweep_cells_x<false><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    if (last) k_cyc_sweep_cells_x<true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    else k_cyc_sweep_cells_x<false, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
   } else {
     const dim3 g(bx, nseg, D == 1 ? dm.nz : dm.ny);
-    if (last) k_cyc_sweep_cells_t<D, true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-    else k_cyc_sweep_cells_t<D, false><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    if (last) k_cyc_sweep_cells_t<D, true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    else k_cyc_sweep_cells_t<D, false, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
   }
 }
 
@@ -258,7 +258,8 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
 // writes U[0]; sweeps read U[0] -> U[1] -> U[0] and the last one finalises.
 // U_dual: the first sweep builds it from the Lagrange velocity and writes
 // ud[0]; then ud[0] -> ud[1]; the last one writes the node velocity and mass.
-void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
+template <typename R>
+static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s) {
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
@@ -267,12 +268,17 @@ void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
     double* uout = a.U[(it + 1) & 1];
     const double* udin = a.ud[(it + 1) & 1];
     double* udout = a.ud[it & 1];
-    if (d == 0) sweep_cells_d<0>(a, last, uin, uout, s);
-    else if (d == 1) sweep_cells_d<1>(a, last, uin, uout, s);
-    else sweep_cells_d<2>(a, last, uin, uout, s);
-    sweep_nodes<1>(a, d, first, last, prev, udin, udout, s);
+    if (d == 0) sweep_cells_d<0, R>(a, last, uin, uout, s);
+    else if (d == 1) sweep_cells_d<1, R>(a, last, uin, uout, s);
+    else sweep_cells_d<2, R>(a, last, uin, uout, s);
+    sweep_nodes<1, R>(a, d, first, last, prev, udin, udout, s);
     prev |= 1 << d;
   }
+}
+
+void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
+  if (a.ph.precision) remap_impl<float>(a, sens, s);
+  else remap_impl<double>(a, sens, s);
 }
 
 void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
@@ -325,48 +331,48 @@ __global__ void __launch_bounds__(128, 3) k_bat_lagrange_cells(const CycleArgs* 
   }
 }
 
-template <bool LAST>
+template <bool LAST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_cells_x_body<LAST>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1], a.dpf,
+    k_cyc_sweep_cells_x_body<LAST, R>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1], a.dpf,
                                    a.st, t.y, t.z, t.w);
   }
 }
 
-template <int DD, bool LAST>
+template <int DD, bool LAST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_cells_t_body<DD, LAST>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+    k_cyc_sweep_cells_t_body<DD, LAST, R>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
                                        a.dpf, a.st, t.y, t.z, t.w);
   }
 }
 
-template <bool FIRST, bool LAST>
+template <bool FIRST, bool LAST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_nodes_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
                                              a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
   }
 }
 
-template <int DD, bool FIRST, bool LAST>
+template <int DD, bool FIRST, bool LAST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_nodes_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
                                                  a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y,
                                                  t.z, t.w);
   }
@@ -418,30 +424,30 @@ static void launch_persistent(Kern kernel, int threads, int nwork, cudaStream_t 
   kernel<<<persistent_blocks(kernel, threads, nwork), threads, 0, s>>>(args...);
 }
 
-template <int DD, bool LAST>
+template <int DD, bool LAST, typename R>
 static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s) {
   const int T = 32 * kLineWarps, kind = BK_CELLS_X + DD;
-  if constexpr (DD == 0) launch_persistent(k_bat_sweep_cells_x<LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
-  else launch_persistent(k_bat_sweep_cells_t<DD, LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
+  if constexpr (DD == 0) launch_persistent(k_bat_sweep_cells_x<LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
+  else launch_persistent(k_bat_sweep_cells_t<DD, LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
 }
 
-template <int DD, bool FIRST, bool LAST>
+template <int DD, bool FIRST, bool LAST, typename R>
 static void bat_nodes_d(const BatchPlan& P, int it, int prev, cudaStream_t s) {
   const int T = 32 * kLineWarps, kind = BK_NODES_X + DD;
   if constexpr (DD == 0)
-    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
+    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
   else
-    launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
+    launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
 }
 
-template <int DD>
+template <int DD, typename R>
 static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s) {
   const bool first = it == 0, last = it == 2;
-  if (last) bat_cells_d<DD, true>(P, it, s);
-  else bat_cells_d<DD, false>(P, it, s);
-  if (first) bat_nodes_d<DD, true, false>(P, it, prev, s);
-  else if (last) bat_nodes_d<DD, false, true>(P, it, prev, s);
-  else bat_nodes_d<DD, false, false>(P, it, prev, s);
+  if (last) bat_cells_d<DD, true, R>(P, it, s);
+  else bat_cells_d<DD, false, R>(P, it, s);
+  if (first) bat_nodes_d<DD, true, false, R>(P, it, prev, s);
+  else if (last) bat_nodes_d<DD, false, true, R>(P, it, prev, s);
+  else bat_nodes_d<DD, false, false, R>(P, it, prev, s);
 }
 
 void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s) {
@@ -450,9 +456,15 @@ void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s) {
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
-    if (d == 0) bat_sweep<0>(P, it, prev, s);
-    else if (d == 1) bat_sweep<1>(P, it, prev, s);
-    else bat_sweep<2>(P, it, prev, s);
+    if (P.precision) {
+      if (d == 0) bat_sweep<0, float>(P, it, prev, s);
+      else if (d == 1) bat_sweep<1, float>(P, it, prev, s);
+      else bat_sweep<2, float>(P, it, prev, s);
+    } else {
+      if (d == 0) bat_sweep<0, double>(P, it, prev, s);
+      else if (d == 1) bat_sweep<1, double>(P, it, prev, s);
+      else bat_sweep<2, double>(P, it, prev, s);
+    }
     prev |= 1 << d;
   }
   launch_persistent(k_bat_dt_min, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);

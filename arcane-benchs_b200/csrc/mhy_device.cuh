@@ -54,14 +54,32 @@ __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b 
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 
 // Flux limiters, mahyco/src/Remap/RemapADIService.h:260-286
-__device__ __forceinline__ double limiter(int id, double r) {
+template <typename R> __device__ __forceinline__ R tmin(R a, R b) { return (b < a) ? b : a; }   // std::min
+template <typename R> __device__ __forceinline__ R tmax(R a, R b) { return (a < b) ? b : a; }   // std::max
+template <typename R>
+__device__ __forceinline__ R limiter(int id, R r) {
   switch (id) {
-    case 0: return smax(0.0, smin(1.0, r));
-    case 1: return smax(0.0, smax(smin(2.0 * r, 1.0), smin(r, 2.0)));
-    case 2: return (r <= 0.0 ? 0.0 : 2.0 * r / (1.0 + r));
-    default: return 0.0;
+    case 0: return tmax(R(0), tmin(R(1), r));
+    case 1: return tmax(R(0), tmax(tmin(R(2) * r, R(1)), tmin(r, R(2))));
+    case 2: return (r <= R(0) ? R(0) : R(2) * r / (R(1) + r));
+    default: return R(0);
   }
 }
+
+// Arithmetic of the remap evaluation in precision R.  double: the reference's
+// operations exactly (qdiv gives x / y bit for bit).  float (the mixed
+// precision form): one reciprocal per shared denominator and products.
+template <typename R> struct Ar;
+template <> struct Ar<double> {
+  __device__ static __forceinline__ double rcp(double y) { return 1.0 / y; }
+  __device__ static __forceinline__ double div(double x, double y, double r) { return qdiv(x, y, r); }
+  __device__ static __forceinline__ double quo(double x, double y) { return x / y; }
+};
+template <> struct Ar<float> {
+  __device__ static __forceinline__ float rcp(float y) { return 1.0f / y; }
+  __device__ static __forceinline__ float div(float x, float, float r) { return x * r; }
+  __device__ static __forceinline__ float quo(float x, float y) { return __fdividef(x, y); }
+};
 
 // compute_eint, mahyco/src/MahycoModule.cc:1630-1654; ir = 1.0/r and irn = 1.0/rn given.
 __device__ __forceinline__ double compute_eint(bool pc, double g, double qn, double q, double ir, double irn,

@@ -24,6 +24,7 @@ struct Scalars {
 struct Phys {
   double gamma, threshold, cfl, deltat_min, deltat_max, final_time;
   int lc_mode, pseudo_centree, ordre_projection, limiteur_id;
+  int precision;        // 0: FP64; 1: mixed (FP32 evaluation of the remap, FP64 state and sums)
 };
 
 struct BCTable {
@@ -103,6 +104,7 @@ struct BatchPlan {
   int ninst;
   const int4* work[BK_COUNT];   // device work tables
   int nwork[BK_COUNT];
+  int precision;                // all instances share it
 };
 void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz);
 void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s);

@@ -86,18 +86,20 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
 
 // Phi = U / sum of the environment volumes = U / U0 for one environment
 // (RemapADIService.cc:962-970, PrepareRemap.cc:394-398); Phi0 = U0/U0 = 1.
-__device__ __forceinline__ void phi_of(const double U[4], double P[4]) {
-  const double U0 = U[0], r = 1.0 / U0;
-  P[0] = 1.0;
-  P[1] = qdiv(U[1], U0, r); P[2] = qdiv(U[2], U0, r); P[3] = qdiv(U[3], U0, r);
+template <typename R>
+__device__ __forceinline__ void phi_of(const double U[4], R P[4]) {
+  const R U0 = (R)U[0], r = Ar<R>::rcp(U0);
+  P[0] = 1;
+  P[1] = Ar<R>::div((R)U[1], U0, r); P[2] = Ar<R>::div((R)U[2], U0, r); P[3] = Ar<R>::div((R)U[3], U0, r);
 }
 
 // Face gradients (R:174-177) of variables 1..3; variable 0 is zero.
-__device__ __forceinline__ void face_grad(bool inner, double dx, const double Pn[4], const double Pp[4], double g[4]) {
-  g[0] = 0.;
-  const double r = inner ? 1.0 / dx : 0.;
+template <typename R>
+__device__ __forceinline__ void face_grad(bool inner, R dx, const R Pn[4], const R Pp[4], R g[4]) {
+  g[0] = 0;
+  const R r = inner ? Ar<R>::rcp(dx) : R(0);
 #pragma unroll
-  for (int v = 1; v < 4; ++v) g[v] = inner ? qdiv(Pn[v] - Pp[v], dx, r) : 0.;
+  for (int v = 1; v < 4; ++v) g[v] = inner ? Ar<R>::div(Pn[v] - Pp[v], dx, r) : R(0);
 }
 
 // Limited cell gradient from the back and front face gradients (R:497-506):
@@ -106,36 +108,37 @@ __device__ __forceinline__ void face_grad(bool inner, double dx, const double Pn
 // a zero the two terms are signed zeros and gc = +0; with equal signs the ratio
 // whose numerator is the smaller magnitude is the only one below 1, the other
 // term is exactly 0.5*g.  So one division gives the reference's bits.
-__device__ __forceinline__ double limited_one(int lim, double gb, double gf) {
+template <typename R>
+__device__ __forceinline__ R limited_one(int lim, R gb, R gf) {
+  const R h = R(0.5), one = R(1), zero = R(0);
   if (lim == 0) {
-    if (gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.))) return 0.;
+    if (gb == zero || gf == zero || ((gb > zero) != (gf > zero))) return zero;
     const bool fsmall = fabs(gf) < fabs(gb);
-    const double r = fsmall ? gf / gb : gb / gf;
-    const double t1 = fsmall ? 0.5 * (r * gb) : 0.5 * (1.0 * gb);
-    const double t2 = fsmall ? 0.5 * (1.0 * gf) : 0.5 * (r * gf);
-    return (0. + t1) + t2;
+    const R r = fsmall ? Ar<R>::quo(gf, gb) : Ar<R>::quo(gb, gf);
+    const R t1 = fsmall ? h * (r * gb) : h * (one * gb);
+    const R t2 = fsmall ? h * (one * gf) : h * (r * gf);
+    return (zero + t1) + t2;
   }
-  double gc = 0.;
-  if (gb != 0.) gc += 0.5 * (limiter(lim, gf / gb) * gb);
-  if (gf != 0.) gc += 0.5 * (limiter(lim, gb / gf) * gf);
+  R gc = zero;
+  if (gb != zero) gc += h * (limiter<R>(lim, Ar<R>::quo(gf, gb)) * gb);
+  if (gf != zero) gc += h * (limiter<R>(lim, Ar<R>::quo(gb, gf)) * gf);
   return gc;
 }
 
 // Variable 0 (the volume) has Phi = U0/U0 = 1 on every cell of a
 // single-environment mesh, so its face gradients are zero and its limited
 // gradient is +0; only variables 1..3 are computed.
-__device__ __forceinline__ void limited_grad(int lim, const double gb[4], const double gf[4], double G[4]) {
-  G[0] = 0.;
+template <typename R>
+__device__ __forceinline__ void limited_grad(int lim, const R gb[4], const R gf[4], R G[4]) {
+  G[0] = 0;
 #pragma unroll
-  for (int v = 1; v < 4; ++v) G[v] = limited_one(lim, gb[v], gf[v]);
+  for (int v = 1; v < 4; ++v) G[v] = limited_one<R>(lim, gb[v], gf[v]);
 }
 
 // Upwind face value (R:707-714): from the previous cell when u_f dx_f > 0.
-__device__ __forceinline__ void face_value(double order2, double u, double dx, double db, double df,
-                                           const double Pp[4], const double Gp[4], const double Pn[4],
-                                           const double Gn[4], double Pf[4]) {
-  const bool back = u * dx > 0.0;
-  const double dot_xf = back ? db : df;
+template <typename R>
+__device__ __forceinline__ void face_value(R order2, bool back, R dot_xf, const R Pp[4], const R Gp[4],
+                                           const R Pn[4], const R Gn[4], R Pf[4]) {
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pf[v] = back ? (Pp[v] + order2 * dot_xf * Gp[v]) : (Pn[v] + order2 * dot_xf * Gn[v]);
 }
@@ -156,48 +159,53 @@ constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
 // 909-987).  Every lane takes part in the shuffles; lanes with upd set get
 // their cell's results in out.  The boundary faces of d carry Phi_f = 0 and
 // contribute nothing.
-template <bool LAST>
+template <bool LAST, typename R = double>
 __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
                                           bool infr, bool upd, const CellIn& in, double* out) {
-  const double order2 = (double)(ph.ordre_projection - 1);
+  const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  double P[4] = {0., 0., 0., 0.};
-  if (valid) phi_of(in.U, P);
+  R P[4] = {0, 0, 0, 0};
+  if (valid) phi_of<R>(in.U, P);
   const unsigned full = 0xffffffffu;
   const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
                xpz = __shfl_up_sync(full, in.xc[2], 1);
-  // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172)
+  // dx_f = (x_c(next) - x_c(prev)).n0 (RemapADIService.cc:171-172), from the
+  // FP64 cell centres in every precision
   const double dx = inner ? dot(d3(in.xc[0], in.xc[1], in.xc[2]) - d3(xpx, xpy, xpz), d3(in.n[0], in.n[1], in.n[2]))
                           : 0.;
-  double g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
+  R g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pp[v] = __shfl_up_sync(full, P[v], 1);
-  face_grad(inner, dx, P, Pp, g);
+  face_grad<R>(inner, (R)dx, P, Pp, g);
 #pragma unroll
   for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
-  limited_grad(lim, g, gr, G);
+  limited_grad<R>(lim, g, gr, G);
 #pragma unroll
   for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
-  if (inner) face_value(order2, in.u, dx, in.db, in.df, Pp, Gp, P, G, Pf);
-  else {
+  if (inner) {
+    const bool back = in.u * dx > 0.0;
+    face_value<R>(order2, back, (R)(back ? in.db : in.df), Pp, Gp, P, G, Pf);
+  } else {
 #pragma unroll
-    for (int v = 0; v < 4; ++v) Pf[v] = 0.;
+    for (int v = 0; v < 4; ++v) Pf[v] = 0;
   }
-  double Pfn[4];
+  R Pfn[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
   const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
   if (!upd) return;
   // fluxes o*u*A*dt*Phi_f through the back and front faces, U -= sum, dual
-  // mass flux sum 0.5*flux*o, clamping of mass and energy (R:909-987)
+  // mass flux sum 0.5*flux*o, clamping of mass and energy (R:909-987); the
+  // sums are FP64 in every precision (each face flux is one rounded value,
+  // subtracted from one cell and added to the other)
   const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
   const double cf = infr ? in.of * un * An * dt : 0.;
   double u[4], dpm = 0.;
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     double flux_face = 0., dp = 0.;
-    if (inner) { const double fl = cb * Pf[v]; flux_face += fl; dp += 0.5 * fl * in.ob; }
-    if (infr) { const double fl = cf * Pfn[v]; flux_face += fl; dp += 0.5 * fl * in.of; }
+    if (inner) { const double fl = (double)((R)cb * Pf[v]); flux_face += fl; dp += 0.5 * fl * in.ob; }
+    if (infr) { const double fl = (double)((R)cf * Pfn[v]); flux_face += fl; dp += 0.5 * fl * in.of; }
     u[v] = in.U[v] - flux_face;
     if (v == 1) dpm = dp;
   }
@@ -215,27 +223,29 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
 
 // ---- nodes ---------------------------------------------------------------
 // Dual update of one inner node (DualPhaseRemap.cc:382-521).
-__device__ __forceinline__ void dual_update(int D, double order2, double dt, double bfm, double ffm,
-                                            const double Pm[4], const double Pn[4], const double Pp[4],
-                                            const double Gm[3], const double Gn[3], const double Gp[3],
-                                            double xm, double xn, double xp, double ud[5]) {
+template <typename R>
+__device__ __forceinline__ void dual_update(int D, R order2, R dt, double bfm, double ffm,
+                                            const R Pm[4], const R Pn[4], const R Pp[4],
+                                            const R Gm[3], const R Gn[3], const R Gp[3],
+                                            R hb, R hf, double ud[5]) {
   const double u3 = ud[3] + (bfm - ffm);
-  const double pnd = Pn[D];
-  const double ufront = 0.5 * (pnd + pnd);                     // DualPhaseRemap.cc:391
-  const double sfront = (ufront > 0) ? 1.0 : -1.0;
-  const double uback = 0.5 * (Pm[D] + pnd);
-  const double sback = (uback > 0) ? 1.0 : -1.0;
+  const R h = R(0.5), zero = R(0);
+  const R pnd = Pn[D];
+  const R ufront = h * (pnd + pnd);                            // DualPhaseRemap.cc:391
+  const R sfront = (ufront > zero) ? R(1) : R(-1);
+  const R uback = h * (Pm[D] + pnd);
+  const R sback = (uback > zero) ? R(1) : R(-1);
   const bool fup = ffm < 0., bup = bfm > 0.;
-  const double tf = sfront * (xp - xn) - dt * ufront;
-  const double tb = sback * (xn - xm) - dt * uback;
+  const R tf = sfront * hf - dt * ufront;                      // hf = x(front) - x, hb = x - x(back)
+  const R tb = sback * hb - dt * uback;
   double out[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const double gfa = c < 3 ? (fup ? Gp[c] : Gn[c]) : 0.;    // index 4 never set (DualPhaseRemap.cc:771)
-    const double gba = c < 3 ? (bup ? Gm[c] : Gn[c]) : 0.;
-    const double FV = (fup ? Pp[c] : Pn[c]) + order2 * (0.5 * gfa * tf);
-    const double BV = (bup ? Pm[c] : Pn[c]) + order2 * (0.5 * gba * tb);
-    out[c] = ud[c < 3 ? c : 4] + (bfm * BV - ffm * FV);
+    const R gfa = c < 3 ? (fup ? Gp[c] : Gn[c]) : zero;        // index 4 never set (DualPhaseRemap.cc:771)
+    const R gba = c < 3 ? (bup ? Gm[c] : Gn[c]) : zero;
+    const R FV = (fup ? Pp[c] : Pn[c]) + order2 * (h * gfa * tf);
+    const R BV = (bup ? Pm[c] : Pn[c]) + order2 * (h * gba * tb);
+    out[c] = ud[c < 3 ? c : 4] + (bfm * (double)BV - ffm * (double)FV);
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) if (fabs(out[c]) < 1.e-300) out[c] = 0.;
@@ -245,19 +255,21 @@ __device__ __forceinline__ void dual_update(int D, double order2, double dt, dou
 // One limited nodal gradient component (DualPhaseRemap.cc:736-777) from the
 // back and front differences; the terms are (0.5*phi(r))*g here, and the same
 // single-division reading of minmod applies.
-__device__ __forceinline__ double dual_limited(int lim, double gb, double gf) {
-  double g = 0.;
+template <typename R>
+__device__ __forceinline__ R dual_limited(int lim, R gb, R gf) {
+  const R h = R(0.5), one = R(1), zero = R(0);
+  R g = zero;
   if (lim == 0) {
-    if (!(gb == 0. || gf == 0. || ((gb > 0.) != (gf > 0.)))) {
+    if (!(gb == zero || gf == zero || ((gb > zero) != (gf > zero)))) {
       const bool fsmall = fabs(gf) < fabs(gb);
-      const double r = fsmall ? gf / gb : gb / gf;
-      const double t1 = fsmall ? 0.5 * r * gb : 0.5 * 1.0 * gb;
-      const double t2 = fsmall ? 0.5 * 1.0 * gf : 0.5 * r * gf;
-      g = (0. + t1) + t2;
+      const R r = fsmall ? Ar<R>::quo(gf, gb) : Ar<R>::quo(gb, gf);
+      const R t1 = fsmall ? h * r * gb : h * one * gb;
+      const R t2 = fsmall ? h * one * gf : h * r * gf;
+      g = (zero + t1) + t2;
     }
   } else {
-    if (gb != 0.) g += 0.5 * limiter(lim, gf / gb) * gb;
-    if (gf != 0.) g += 0.5 * limiter(lim, gb / gf) * gf;
+    if (gb != zero) g += h * limiter<R>(lim, Ar<R>::quo(gf, gb)) * gb;
+    if (gf != zero) g += h * limiter<R>(lim, Ar<R>::quo(gb, gf)) * gf;
   }
   return g;
 }
@@ -280,56 +292,58 @@ constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| 
 // start of a sweep is PrepareRemap.cc:411-433 on the first sweep or for nodes
 // not yet updated this cycle, else U_dual / m.  G holds the node's stale
 // gradient on entry and its gradient on return.
-template <int D, bool FIRST, bool LAST>
+template <int D, bool FIRST, bool LAST, typename R = double>
 __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
-                                          bool upd, const NodeIn& in, double G[3], double* out) {
-  const double order2 = (double)(ph.ordre_projection - 1);
+                                          bool upd, const NodeIn& in, R G[3], double* out) {
+  const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
   const bool grad_on = ph.ordre_projection > 1;
-  double ud[5] = {0., 0., 0., 0., 0.}, P[4] = {0., 0., 0., 0.}, x = 0.;
+  double ud[5] = {0., 0., 0., 0., 0.}, x = 0.;
+  R P[4] = {0, 0, 0, 0};
   if (valid) {
     const D3 u = d3(in.vh[0], in.vh[1], in.vh[2]);
     if (FIRST) {
       const double m = in.nm;
       const double un = norm2(u);
       ud[0] = m * u.x; ud[1] = m * u.y; ud[2] = m * u.z; ud[3] = m; ud[4] = 0.5 * m * un;
-      P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * un;
+      P[0] = (R)u.x; P[1] = (R)u.y; P[2] = (R)u.z; P[3] = (R)(0.5 * un);
     } else {
 #pragma unroll
       for (int c = 0; c < 5; ++c) ud[c] = in.ud[c];
       if (updated) {
-        const double m = ud[3], rm = 1.0 / m;
-        P[0] = qdiv(ud[0], m, rm); P[1] = qdiv(ud[1], m, rm); P[2] = qdiv(ud[2], m, rm); P[3] = qdiv(ud[4], m, rm);
+        const R m = (R)ud[3], rm = Ar<R>::rcp(m);
+        P[0] = Ar<R>::div((R)ud[0], m, rm); P[1] = Ar<R>::div((R)ud[1], m, rm);
+        P[2] = Ar<R>::div((R)ud[2], m, rm); P[3] = Ar<R>::div((R)ud[4], m, rm);
       } else {
-        P[0] = u.x; P[1] = u.y; P[2] = u.z; P[3] = 0.5 * norm2(u);
+        P[0] = (R)u.x; P[1] = (R)u.y; P[2] = (R)u.z; P[3] = (R)(0.5 * norm2(u));
       }
     }
     x = in.x0d + in.vh[D] * dt;
   }
   const unsigned full = 0xffffffffu;
-  double Pm[4], Pp[4];
+  R Pm[4], Pp[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) { Pm[c] = __shfl_up_sync(full, P[c], 1); Pp[c] = __shfl_down_sync(full, P[c], 1); }
   const double xm = __shfl_up_sync(full, x, 1), xp = __shfl_down_sync(full, x, 1);
   if (grad_on) {
     // front difference quotient of this node = back difference quotient of the next
-    const double hf = xp - x, rf = 1.0 / hf;
-    double gf[3], gb[3];
+    const R hf = (R)(xp - x), rf = Ar<R>::rcp(hf);
+    R gf[3], gb[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) gf[c] = qdiv(Pp[c] - P[c], hf, rf);
+    for (int c = 0; c < 3; ++c) gf[c] = Ar<R>::div(Pp[c] - P[c], hf, rf);
 #pragma unroll
     for (int c = 0; c < 3; ++c) gb[c] = __shfl_up_sync(full, gf[c], 1);
     if (valid && inner) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) G[c] = dual_limited(lim, gb[c], gf[c]);
+      for (int c = 0; c < 3; ++c) G[c] = dual_limited<R>(lim, gb[c], gf[c]);
     }
   }
-  double Gm[3], Gp[3];
+  R Gm[3], Gp[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) { Gm[c] = __shfl_up_sync(full, G[c], 1); Gp[c] = __shfl_down_sync(full, G[c], 1); }
   const double bfm = __shfl_up_sync(full, in.ffm, 1);  // back cells of node m = front cells of node m-1
   if (!upd) return;
-  if (inner) dual_update(D, order2, dt, bfm, in.ffm, Pm, P, Pp, Gm, G, Gp, xm, x, xp, ud);
+  if (inner) dual_update<R>(D, order2, (R)dt, bfm, in.ffm, Pm, P, Pp, Gm, G, Gp, (R)(x - xm), (R)(xp - x), ud);
   if (!LAST) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) out[c] = ud[c];
@@ -363,7 +377,7 @@ __device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int i
 }
 
 // Node sweep along x: lanes run along the rows of nodes.
-template <bool FIRST, bool LAST, int K>
+template <bool FIRST, bool LAST, int K, typename R>
 __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
@@ -385,7 +399,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   NodeIn in;
   in.vh[0] = in.vh[1] = in.vh[2] = 0.; in.x0d = 0.; in.nm = 0.;
   in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
-  double G[3] = {0., 0., 0.};
+  R G[3] = {0, 0, 0};
   if (valid) {
     in.vh[0] = vh[n]; in.vh[1] = vh[N + n]; in.vh[2] = vh[2 * N + n]; in.x0d = x0[n];
     if (FIRST) in.nm = nm_in[n];
@@ -411,7 +425,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
         }
       in.ffm = f;
     }
-    if (!(inner && grad_on)) { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
+    if (!(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
     if (LAST && upd) {
       double sm = 0.;
 #pragma unroll
@@ -428,9 +442,9 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
     }
   }
   double out[kNodeOut];
-  node_line<0, FIRST, LAST>(ph, S->dt, valid, inner, updated, upd, in, G, out);
+  node_line<0, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out);
   if (!upd) return;
-  if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
+  if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
   if (!LAST) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) udout[c * N + n] = out[c];
@@ -439,13 +453,13 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   }
 }
 
-template <bool FIRST, bool LAST, int K>
+template <bool FIRST, bool LAST, int K, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_x_body<FIRST, LAST, K>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
@@ -455,7 +469,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
 // o - 1 .. o along the remaining axis: their dual mass fluxes (and masses on
 // the last sweep) are staged as [o - 1 + q][x - 8 bx + 1][position], with zero
 // for cells outside the mesh (adding +0 to these sums changes no bit).
-template <int D, bool FIRST, bool LAST, int K>
+template <int D, bool FIRST, bool LAST, int K, typename R>
 __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
@@ -554,13 +568,13 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
     }
     in.msum = sm;
   }
-  double G[3] = {0., 0., 0.};
+  R G[3] = {0, 0, 0};
   const int n = valid ? node_id(i, m) : 0;
-  if (valid && !(inner && grad_on)) { G[0] = Gd[n]; G[1] = Gd[N + n]; G[2] = Gd[2 * N + n]; }
+  if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
   double out[kNodeOut];
-  node_line<D, FIRST, LAST>(ph, S->dt, valid, inner, updated, upd, in, G, out);
+  node_line<D, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out);
   if (upd) {
-    if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = G[0]; Gd[N + n] = G[1]; Gd[2 * N + n] = G[2]; }
+    if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
     // each lane overwrites only the tile column it read itself
 #pragma unroll
     for (int c = 0; c < kNodeOut; ++c) row[c * kTileArr] = out[c];
@@ -577,48 +591,49 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool FIRST, bool LAST, int K>
+template <int D, bool FIRST, bool LAST, int K, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------------
 // Host-side node sweep launchers.
-template <int D, bool FIRST, bool LAST, int K>
+template <int D, bool FIRST, bool LAST, int K, typename R>
 static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
   const int T = 32 * kLineWarps;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
-    k_cyc_sweep_nodes_x<FIRST, LAST, K><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd,
+    k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd,
                                                      a.st.mass, a.v, a.nm, a.vnorm);
   } else {
     const dim3 g((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, (D == 1 ? dm.nz : dm.ny) + 1);
-    k_cyc_sweep_nodes_t<D, FIRST, LAST, K><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf,
+    k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf,
                                                         a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
   }
 }
 
 // One node sweep along D of a mesh with K environments (dual mass fluxes in K planes).
-template <int D, int K>
+template <int D, int K, typename R>
 static void sweep_nodes_d(const CycleArgs& a, bool first, bool last, int prev, const double* udin, double* udout,
                           cudaStream_t s) {
-  if (first) sweep_nodes_launch<D, true, false, K>(a, prev, udin, udout, s);
-  else if (last) sweep_nodes_launch<D, false, true, K>(a, prev, udin, udout, s);
-  else sweep_nodes_launch<D, false, false, K>(a, prev, udin, udout, s);
+  if (first) sweep_nodes_launch<D, true, false, K, R>(a, prev, udin, udout, s);
+  else if (last) sweep_nodes_launch<D, false, true, K, R>(a, prev, udin, udout, s);
+  else sweep_nodes_launch<D, false, false, K, R>(a, prev, udin, udout, s);
 }
 
-template <int K>
+// R: evaluation precision of the sweep (double, or float in the mixed form).
+template <int K, typename R = double>
 static void sweep_nodes(const CycleArgs& a, int d, bool first, bool last, int prev, const double* udin,
                         double* udout, cudaStream_t s) {
-  if (d == 0) sweep_nodes_d<0, K>(a, first, last, prev, udin, udout, s);
-  else if (d == 1) sweep_nodes_d<1, K>(a, first, last, prev, udin, udout, s);
-  else sweep_nodes_d<2, K>(a, first, last, prev, udin, udout, s);
+  if (d == 0) sweep_nodes_d<0, K, R>(a, first, last, prev, udin, udout, s);
+  else if (d == 1) sweep_nodes_d<1, K, R>(a, first, last, prev, udin, udout, s);
+  else sweep_nodes_d<2, K, R>(a, first, last, prev, udin, udout, s);
 }
 
 

@@ -151,6 +151,7 @@ def make_options(opts, gammas) -> COptions:
     o.nb_bc = len(opts.boundary_conditions)
     for b, (s, t, v) in enumerate(opts.boundary_conditions):
         o.bc[b] = BC(s, t, v)
+    o.precision = int(getattr(opts, "precision", 0))
     o.nb_env = len(gammas)
     for k, g in enumerate(gammas):
         o.adiabatic_cst[k] = float(g)

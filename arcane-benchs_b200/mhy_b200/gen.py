@@ -65,6 +65,7 @@ class Options:
     ordre_projection: int = 2
     projection_limiteur_id: int = 0         # 0 minmod, 1 superBee, 2 vanLeer
     boundary_conditions: tuple = WALLS
+    precision: int = 0                      # device only: 0 FP64, 1 mixed (FP32 remap evaluation)
 
 
 @dataclasses.dataclass

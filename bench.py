@@ -38,11 +38,15 @@ WORKLOADS = ("sedov", "two_material", "sphere_inclusion", "batched")
 def make_case(args):
     """The workload's mesh and initial state (seeded, synthetic) and its name."""
     from mhy_b200 import gen
+    tag = "fp64" if args.precision == "fp64" else "mixed"
     if args.workload == "sedov":
-        return gen.sedov(n=args.n), f"sedov-{args.n}^3-jitter1%-fp64"
-    if args.workload == "two_material":
-        return gen.two_material(256, 128, 128), "two-material-256x128x128-fp64"
-    return gen.sphere_inclusion(384, 384, 192), "sphere-inclusion-384x384x192-fp64"
+        c, name = gen.sedov(n=args.n), f"sedov-{args.n}^3-jitter1%-{tag}"
+    elif args.workload == "two_material":
+        c, name = gen.two_material(256, 128, 128), f"two-material-256x128x128-{tag}"
+    else:
+        c, name = gen.sphere_inclusion(384, 384, 192), f"sphere-inclusion-384x384x192-{tag}"
+    c.options.precision = 0 if args.precision == "fp64" else 1
+    return c, name
 
 
 def parse():
@@ -56,6 +60,8 @@ def parse():
                          "sphere_inclusion: 384x384x192, two gases; batched: 64 Sod/Sedov instances of "
                          "32^3..96^3 advanced together (instances split across GPUs)")
     ap.add_argument("--n", type=int, default=128, help="Sedov mesh cells per direction")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="fp64: the reference's arithmetic bit for bit; mixed: FP32 remap evaluation, FP64 state")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-cycles", type=int, default=5)
@@ -169,6 +175,36 @@ def run_reference(args):
     return 0
 
 
+def mixed_accuracy(cases, densities, cycles, device, batched=False):
+    """Density L1 error of the mixed-precision run against the FP64 path on the
+    same inputs and cycle count (the FP64 device path equals the oracle bit for
+    bit, which the GPU parity tests check): sum |rho_mixed - rho_fp64| / sum |rho_fp64|."""
+    import copy
+    import math
+    import numpy as np
+    import mhy_b200
+    ref_cases = []
+    for c in cases:
+        r = copy.copy(c)
+        r.options = copy.copy(c.options)
+        r.options.precision = 0
+        ref_cases.append(r)
+    if batched:
+        b = mhy_b200.Batch(ref_cases, device=device)
+        b.step(cycles)
+        refs = [b.field(i, "density") for i in range(len(ref_cases))]
+        b.close()
+    else:
+        g = mhy_b200.Context(ref_cases[0], device=device)
+        g.step(cycles)
+        refs = [g.field("density")]
+        g.close()
+    num = math.fsum(float(np.abs(a - r).sum()) for a, r in zip(densities, refs))
+    den = math.fsum(float(np.abs(r).sum()) for r in refs)
+    return {"density_l1_rel_vs_fp64": num / den, "cycles": cycles,
+            "reference": "FP64 device path on the same inputs (bitwise equal to the CPU oracle)"}
+
+
 def run_reference_batched(args, threads):
     """--impl reference --workload batched: the instances advanced one after
     the other on the host cores by the oracle, a bounded sample: every
@@ -219,6 +255,8 @@ def run_ours_batched(args):
     if world > 1:
         replicas.init("nccl", device=dev)
     all_cases = gen.batched()
+    for c in all_cases:
+        c.options.precision = 0 if args.precision == "fp64" else 1
     mine = [c for i, c in enumerate(all_cases) if i % world == rank]
     cells = sum(c.ncells for c in mine)
     b = mhy_b200.Batch(mine, device=local)
@@ -237,6 +275,10 @@ def run_ours_batched(args):
     ms, value = replicas.aggregate(cells, args.steps, start.elapsed_time(stop), dev)
     status = max(b.status(i) for i in range(len(mine)))
     kpc = b.kernels_per_cycle()
+    accuracy = None
+    if args.precision == "mixed":
+        accuracy = mixed_accuracy(mine, [b.field(i, "density") for i in range(len(mine))],
+                                  args.warmup + args.steps, local, batched=True)
     b.close()
 
     e2e = None
@@ -287,11 +329,15 @@ def run_ours_batched(args):
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "batched-64-sod-sedov-32..96^3-fp64", "instances": len(all_cases),
+                "config": {"workload": f"batched-64-sod-sedov-32..96^3-{'fp64' if args.precision == 'fp64' else 'mixed'}",
+                           "instances": len(all_cases),
                            "cells": total, "cells_per_gpu": cells, "parallelism": f"instances split over {world}",
                            "l2": "working set > 126 MB L2 (no flush needed)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kpc * args.steps,
                 "clocks": clk.summary(), "device_status": status}
+        if accuracy:
+            line["accuracy"] = accuracy
+            line["dtype"] = "f32 remap evaluation / f64 state"
         print(json.dumps(line), flush=True)
     replicas.finish()
     return 0
@@ -332,6 +378,9 @@ def run_ours(args):
     ctx.synchronize()
     status = ctx.status()
     ms, value = replicas.aggregate(case.ncells, args.steps, ms_local, dev)
+    accuracy = None
+    if args.precision == "mixed":
+        accuracy = mixed_accuracy([case], [ctx.field("density")], args.warmup + args.steps, local)
     ctx.close()
 
     # end to end through the per-entry-point C ABI, host buffers in pinned memory
@@ -391,6 +440,9 @@ def run_ours(args):
                            "l2": "working set ~2 GB > 126 MB L2 (no flush needed)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status}
+        if accuracy:
+            line["accuracy"] = accuracy
+            line["dtype"] = "f32 remap evaluation / f64 state"
         print(json.dumps(line), flush=True)
     replicas.finish()
     return 0

@@ -72,7 +72,10 @@ typedef struct mhy_options {
   mhy_bc bc[MHY_MAX_BC];             /* default: walls on the six planes */
   int32_t nb_env;                    /* number of environments (one ideal gas each; 1..4 on the device) */
   double adiabatic_cst[MHY_MAX_ENV]; /* PerfectGas adiabatic-cst per environment */
-  int32_t precision;                 /* 0: plain FP64 */
+  int32_t precision;                 /* 0: plain FP64 (bit for bit the reference's arithmetic);
+                                        1: mixed: the remap's Phi, gradients, limiters, face values and
+                                        flux terms in FP32; state, coordinates, volumes, conserved sums
+                                        and the dt reduction in FP64 (one environment) */
   int32_t reserved[7];
 } mhy_options;
 

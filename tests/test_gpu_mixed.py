@@ -1,0 +1,67 @@
+"""GPU: the mixed-precision form (precision = 1: Phi, gradients, limiters,
+face values and flux terms of the remap in FP32; state, coordinates, volumes
+and every conserved sum in FP64) against the FP64 oracle.
+
+Bars: density L1 error at most 1e-5 relative to the FP64 oracle; total mass
+conserved to 1e-12 on lattice meshes (where the reference's scheme itself
+conserves it); the batched mixed form equals single mixed contexts bit for
+bit."""
+import math
+
+import numpy as np
+import pytest
+
+import mhy_oracle
+from mhy_b200 import Batch, Context, gen
+
+pytestmark = pytest.mark.gpu
+
+
+def l1_rel(a, b):
+    return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+
+def mixed(case):
+    case.options.precision = 1
+    return case
+
+
+@pytest.mark.parametrize("make,cycles", [
+    (lambda: gen.sedov(n=24, jitter=0.01, seed=1, cycles=150), 150),
+    (lambda: gen.sod(cycles=200), 200),
+    (lambda: gen.sod(nx=30, ny=24, nz=6, lx=1.0, ly=1.0, lz=0.25, axis=1, jitter=0.01, seed=8, cycles=120), 120),
+])
+def test_mixed_density_l1_vs_fp64_oracle(make, cycles):
+    ref = make()
+    o = mhy_oracle.Oracle(ref)
+    o.step(cycles)
+    g = Context(mixed(make()))
+    g.step(cycles)
+    g.synchronize()
+    err = {f: l1_rel(g.field(f), o.field(f)) for f in ("density", "internal_energy", "pressure")}
+    err["velocity"] = l1_rel(g.field("velocity"), o.field("velocity")) if np.abs(o.field("velocity")).sum() else 0.0
+    assert err["density"] <= 1e-5, err
+    assert err["internal_energy"] <= 1e-4 and err["pressure"] <= 1e-4, err
+    # not the FP64 result: the mixed path really evaluates in FP32
+    assert not np.array_equal(g.field("density"), o.field("density"))
+
+
+def test_mixed_mass_conservation_on_lattice():
+    case = mixed(gen.sod(nx=40, ny=6, nz=6, cycles=150))
+    g = Context(case)
+    m0 = math.fsum(g.field("cell_mass"))
+    g.step(150)
+    g.synchronize()
+    m1 = math.fsum(g.field("cell_mass"))
+    assert abs(m1 - m0) / m0 <= 1e-12
+
+
+def test_batched_mixed_equals_single_mixed():
+    cases = [mixed(c) for c in gen.batched(count=4, seed=41, side_lo=10, side_hi=18, cycles=30)]
+    b = Batch(cases)
+    b.step(30)
+    for i, c in enumerate(cases):
+        g = Context(c)
+        g.step(30)
+        for f in ("density", "internal_energy", "velocity"):
+            assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
