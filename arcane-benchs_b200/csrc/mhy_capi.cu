@@ -55,6 +55,7 @@ struct mhy_ctx {
   // cells
   double *rho = nullptr, *e = nullptr, *q = nullptr, *p = nullptr, *cs = nullptr, *mass = nullptr;
   double *L = nullptr, *Ve = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr, *xc = nullptr;
+  float* cqs32 = nullptr;
   double *U[2] = {nullptr, nullptr};
   // environments (K > 1)
   int K = 1;
@@ -84,7 +85,7 @@ struct mhy_ctx {
     CycleArgs a{};
     a.dm = dm; a.S = S; a.ph = ph; a.bct = bct; a.bcmask = bcmask;
     a.x0 = x0; a.n0 = n0; a.ofn = ofn;
-    a.v = v; a.vh = vh; a.nm = nm; a.cqs = cqs; a.L = L; a.dpf = dpf; a.Gd = Gd; a.xc = xc; a.vnorm = vnorm;
+    a.v = v; a.vh = vh; a.nm = nm; a.cqs = cqs; a.cqs32 = cqs32; a.L = L; a.dpf = dpf; a.Gd = Gd; a.xc = xc; a.vnorm = vnorm;
     a.U[0] = U[0]; a.U[1] = U[1]; a.ud[0] = ud[0]; a.ud[1] = ud[1];
     a.fd = fd;
     a.st.rho = rho; a.st.e = e; a.st.q = q; a.st.p = p; a.st.cs = cs; a.st.mass = mass; a.st.Ve = Ve;
@@ -182,7 +183,11 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   A_(&c->ud[0], 5 * N); A_(&c->ud[1], 5 * N);
   A_(&c->rho, C); A_(&c->e, C); A_(&c->q, C); A_(&c->p, C); A_(&c->cs, C); A_(&c->mass, C); A_(&c->L, C);
   const int K = c->K, NV = 3 * K + 1;
-  A_(&c->Ve, C); A_(&c->dpf, K * C); A_(&c->xc, 3 * C); A_(&c->cqs, 24 * C); A_(&c->ofn, 6 * C);
+  A_(&c->Ve, C); A_(&c->dpf, K * C); A_(&c->xc, 3 * C); A_(&c->ofn, 6 * C);
+  // corner vectors: FP64, and FP32 in the mixed form (hydro_start_init
+  // converts the FP64 ones of t = 0)
+  A_(&c->cqs, 24 * C);
+  if (opt->precision == 1 && rc == MHY_OK) rc = c->alloc(&c->cqs32, (size_t)(24 * C));
   A_(&c->U[0], NV * C); A_(&c->U[1], NV * C);
   if (K > 1) {
     EnvState& ev = c->env;
@@ -339,6 +344,7 @@ int mhy_hydro_start_init(mhy_ctx* c) {
   if (c->K == 1) k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph.gamma, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
   else launch_init_env(c->args(), s);
   k_node_mass<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->mass, c->nm);
+  if (c->cqs32) k_to_f32<<<blocks(24 * dm.C), kThreads, 0, s>>>(24 * dm.C, c->cqs, c->cqs32);
   MHY_CUDA(cudaGetLastError());
   MHY_CUDA(cudaStreamSynchronize(s));
   cudaFree(xc0);

@@ -26,8 +26,9 @@ namespace mhy {
 // ------------------------------------------------------------------------
 // Lagrange phase, nodes: SaveValuesAtN (v_n = v, x = x0), UpdateVelocity,
 // ApplyBoundaryCondition (MahycoModule.cc:308-450, 589-665, 936-1004).
+template <typename CQ>
 __device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars* __restrict__ S,
-    const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ cqs,
+    const double* __restrict__ p, const double* __restrict__ q, const CQ* __restrict__ cqs,
     const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
     double* __restrict__ vh,
     int bx_, int by_, int bz_) {
@@ -48,7 +49,8 @@ __device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars
         const long long c = dm.cid(ci, cj, ck);
         const int l = loc[di][dj][dk];
         const double pq = p[c] + q[c];
-        F = F + pq * d3(cqs[(l * 3 + 0) * dm.C + c], cqs[(l * 3 + 1) * dm.C + c], cqs[(l * 3 + 2) * dm.C + c]);
+        F = F + pq * d3((double)cqs[(l * 3 + 0) * dm.C + c], (double)cqs[(l * 3 + 1) * dm.C + c],
+                        (double)cqs[(l * 3 + 2) * dm.C + c]);
       }
   const double s = dtv / nm[n];
   D3 u = d3(v[n], v[dm.N + n], v[2 * dm.N + n]) + s * F;
@@ -63,11 +65,12 @@ __device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars
   vh[n] = u.x; vh[dm.N + n] = u.y; vh[2 * dm.N + n] = u.z;
 }
 
+template <typename CQ>
 __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scalars* __restrict__ S,
-    const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ cqs,
+    const double* __restrict__ p, const double* __restrict__ q, const CQ* __restrict__ cqs,
     const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
     double* __restrict__ vh) {
-  k_cyc_lagrange_nodes_body(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, blockIdx.x, -1, 0);
+  k_cyc_lagrange_nodes_body<CQ>(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, blockIdx.x, -1, 0);
 }
 
 
@@ -235,7 +238,8 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
 // most of a second block idle).
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
   const unsigned nbn = (unsigned)((a.dm.N + 127) / 128);
-  k_cyc_lagrange_nodes<<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh);
+  if (a.ph.precision) k_cyc_lagrange_nodes<float><<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh);
+  else k_cyc_lagrange_nodes<double><<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh);
 }
 
 // Cell kernels: rows of 128 cells when nx is a multiple of 128, else 128
@@ -249,9 +253,14 @@ dim3 cell_grid(const Dims& dm, int& linear) {
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
-  k_cyc_lagrange_cells<1><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
-                                              a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag,
-                                              linear);
+  if (a.ph.precision)
+    k_cyc_lagrange_cells<1, float><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q,
+                                                       a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc,
+                                                       a.fd, a.env, a.Vlag, linear);
+  else
+    k_cyc_lagrange_cells<1, double><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q,
+                                                        a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc,
+                                                        a.fd, a.env, a.Vlag, linear);
 }
 
 // Three sweeps d = (i + sens) % 3 (RemapADIService.cc:28-30).  U: Lagrange
@@ -312,22 +321,27 @@ void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz) {
   }
 }
 
+template <typename R>
 __global__ void __launch_bounds__(128) k_bat_lagrange_nodes(const CycleArgs* __restrict__ D,
                                                             const int4* __restrict__ W, int nw) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_lagrange_nodes_body(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, t.y, t.z, t.w);
+    if constexpr (sizeof(R) == 4)
+      k_cyc_lagrange_nodes_body<float>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh, t.y, t.z, t.w);
+    else
+      k_cyc_lagrange_nodes_body<double>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, t.y, t.z, t.w);
   }
 }
 
-__global__ void __launch_bounds__(128, 3) k_bat_lagrange_cells(const CycleArgs* __restrict__ D,
-                                                               const int4* __restrict__ W, int nw) {
+template <typename R>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_lagrange_cells(const CycleArgs* __restrict__ D,
+                                                                                   const int4* __restrict__ W, int nw) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_lagrange_cells_body<1>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
-                                 a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
+    k_cyc_lagrange_cells_body<1, R>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
+                                    a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
   }
 }
 
@@ -451,8 +465,13 @@ static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s) {
 }
 
 void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s) {
-  launch_persistent(k_bat_lagrange_nodes, 128, P.nwork[BK_LNODES], s, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
-  launch_persistent(k_bat_lagrange_cells, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  if (P.precision) {
+    launch_persistent(k_bat_lagrange_nodes<float>, 128, P.nwork[BK_LNODES], s, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+    launch_persistent(k_bat_lagrange_cells<float>, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  } else {
+    launch_persistent(k_bat_lagrange_nodes<double>, 128, P.nwork[BK_LNODES], s, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+    launch_persistent(k_bat_lagrange_cells<double>, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  }
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;

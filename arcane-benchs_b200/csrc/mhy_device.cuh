@@ -12,17 +12,26 @@
 
 namespace mhy {
 
-struct D3 { double x, y, z; };
+// 3-vectors in double (D3) or float (F3, the mixed-precision geometry).
+template <typename T> struct Vec3 { T x, y, z; };
+using D3 = Vec3<double>;
+using F3 = Vec3<float>;
 __device__ __forceinline__ D3 d3(double x, double y, double z) { return D3{x, y, z}; }
-__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return D3{a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ D3 operator*(double s, D3 v) { return D3{v.x * s, v.y * s, v.z * s}; }
-__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ D3 cross(D3 u, D3 v) {
-  return D3{u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+template <typename T>
+__device__ __forceinline__ Vec3<T> operator+(Vec3<T> a, Vec3<T> b) { return Vec3<T>{a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <typename T>
+__device__ __forceinline__ Vec3<T> operator-(Vec3<T> a, Vec3<T> b) { return Vec3<T>{a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <typename T>
+__device__ __forceinline__ Vec3<T> operator*(T s, Vec3<T> v) { return Vec3<T>{v.x * s, v.y * s, v.z * s}; }
+template <typename T>
+__device__ __forceinline__ T dot(Vec3<T> a, Vec3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <typename T>
+__device__ __forceinline__ Vec3<T> cross(Vec3<T> u, Vec3<T> v) {
+  return Vec3<T>{u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
 }
 __device__ __forceinline__ double norm2(D3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
-__device__ __forceinline__ double comp(D3 a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
+template <typename T>
+__device__ __forceinline__ T comp(Vec3<T> a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
 // x / y with the reciprocal r = 1.0/y already at hand: q0 = RN(x r),
 // e = x - y q0 (exact with one fma), q = RN(q0 + e r).  With r the correctly
 // rounded reciprocal this is the correctly rounded quotient (P. Markstein,

@@ -97,6 +97,12 @@ __global__ void k_init_state(Dims dm, double gamma, const double* __restrict__ v
   q[c] = 0.;
 }
 
+// FP64 -> FP32 copy (the initial corner vectors of the mixed form).
+__global__ void k_to_f32(long long n, const double* __restrict__ src, float* __restrict__ dst) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (float)src[i];
+}
+
 // Node mass = 1/8 sum of the cell masses, increasing cell id (MahycoModule.cc:235-266).
 __global__ void k_node_mass(Dims dm, const double* __restrict__ mass, double* __restrict__ nm) {
   long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;

@@ -72,6 +72,7 @@ struct CycleArgs {
   const uint16_t* bcmask;
   const double *x0, *n0, *ofn;
   double *v, *vh, *nm, *cqs, *L, *dpf, *Gd, *xc, *vnorm;
+  float* cqs32;         // corner vectors of the mixed form (FP32)
   double* U[2];
   double* ud[2];
   FaceData fd;
@@ -116,6 +117,7 @@ __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* x
 __global__ void k_init_state(Dims dm, double gamma, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
+__global__ void k_to_f32(long long n, const double* src, float* dst);
 __global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm, int linear);
 dim3 cell_grid(const Dims& dm, int& linear);
 __global__ void k_dt_finish(Scalars* S, Phys ph);

@@ -21,17 +21,146 @@ __device__ __forceinline__ D3 load_xl(const Dims& dm, const double* __restrict__
 }
 
 // Half cross product 0.5 * (a - c) x (b - c) (MahycoModule.cc:2206-2239).
-__device__ __forceinline__ D3 half_cross(D3 a, D3 b, D3 c) { return 0.5 * cross(a - c, b - c); }
+template <typename T>
+__device__ __forceinline__ Vec3<T> half_cross(Vec3<T> a, Vec3<T> b, Vec3<T> c) { return T(0.5) * cross(a - c, b - c); }
 
 // Corner vectors accumulated face by face.  Each corner's two six-term sums
 // of MahycoModule.cc:2242-2257 take two consecutive terms from each of its
 // three faces, in increasing face order, so adding them as the faces are
 // visited keeps the reference's order; a corner is finished as soon as its
 // third face is done.
-struct CornerAcc { D3 s1, s2; };
-__device__ __forceinline__ void acc_start(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) { a.s1 = t1 + t2; a.s2 = u1 + u2; }
-__device__ __forceinline__ void acc_add(CornerAcc& a, D3 t1, D3 t2, D3 u1, D3 u2) {
+template <typename T> struct CornerAcc { Vec3<T> s1, s2; };
+template <typename T>
+__device__ __forceinline__ void acc_start(CornerAcc<T>& a, Vec3<T> t1, Vec3<T> t2, Vec3<T> u1, Vec3<T> u2) {
+  a.s1 = t1 + t2; a.s2 = u1 + u2;
+}
+template <typename T>
+__device__ __forceinline__ void acc_add(CornerAcc<T>& a, Vec3<T> t1, Vec3<T> t2, Vec3<T> u1, Vec3<T> u2) {
   a.s1 = a.s1 + t1; a.s1 = a.s1 + t2; a.s2 = a.s2 + u1; a.s2 = a.s2 + u2;
+}
+
+// The 8 corner vectors of a hexahedron with nodes x (SN_trigo order),
+// streamed: finish(a, cqs_a) is called as soon as corner a is complete
+// (MahycoModule.cc:2195-2258, face centres as in :1080-1087).  T = double is
+// the reference's arithmetic; T = float (mixed form) takes x relative to the
+// cell centre, where every term has the size of the cell and nothing cancels.
+template <typename T, typename Finish>
+__device__ __forceinline__ void corner_vectors(const Vec3<T> x[8], Finish&& finish) {
+  const T t12 = T(1.) / T(12.), q = T(0.25);
+  auto fin = [&](int a, const CornerAcc<T>& ac) { finish(a, t12 * (T(5.) * ac.s1 + ac.s2)); };
+  CornerAcc<T> k0, k1, k2, k3, k4, k5, k6, k7;
+  {
+    const Vec3<T> c0 = q * (x[0] + x[3] + x[2] + x[1]);
+    const Vec3<T> n04 = half_cross(x[0], x[3], c0), n03 = half_cross(x[3], x[2], c0);
+    const Vec3<T> n02 = half_cross(x[2], x[1], c0), n01 = half_cross(x[1], x[0], c0);
+    acc_start(k0, n01, n04, n02, n03);
+    acc_start(k1, n01, n02, n04, n03);
+    acc_start(k2, n02, n03, n01, n04);
+    acc_start(k3, n03, n04, n01, n02);
+  }
+  {
+    const Vec3<T> c1 = q * (x[0] + x[4] + x[7] + x[3]);
+    const Vec3<T> n05 = half_cross(x[0], x[4], c1), n12 = half_cross(x[4], x[7], c1);
+    const Vec3<T> n08 = half_cross(x[7], x[3], c1), n04 = half_cross(x[3], x[0], c1);
+    acc_add(k0, n04, n05, n08, n12);
+    acc_add(k3, n08, n04, n05, n12);
+    acc_start(k4, n05, n12, n08, n04);
+    acc_start(k7, n08, n12, n04, n05);
+  }
+  {
+    const Vec3<T> c2 = q * (x[0] + x[1] + x[5] + x[4]);
+    const Vec3<T> n01 = half_cross(x[0], x[1], c2), n06 = half_cross(x[1], x[5], c2);
+    const Vec3<T> n09 = half_cross(x[5], x[4], c2), n05 = half_cross(x[4], x[0], c2);
+    acc_add(k0, n05, n01, n06, n09);
+    fin(0, k0);
+    acc_add(k1, n01, n06, n09, n05);
+    acc_add(k4, n05, n09, n01, n06);
+    acc_start(k5, n06, n09, n01, n05);
+  }
+  {
+    const Vec3<T> c3 = q * (x[4] + x[5] + x[6] + x[7]);
+    const Vec3<T> n09 = half_cross(x[4], x[5], c3), n10 = half_cross(x[5], x[6], c3);
+    const Vec3<T> n11 = half_cross(x[6], x[7], c3), n12 = half_cross(x[7], x[4], c3);
+    acc_add(k4, n09, n12, n10, n11);
+    fin(4, k4);
+    acc_add(k5, n09, n10, n12, n11);
+    acc_start(k6, n11, n10, n12, n09);
+    acc_add(k7, n12, n11, n09, n10);
+  }
+  {
+    const Vec3<T> c4 = q * (x[1] + x[2] + x[6] + x[5]);
+    const Vec3<T> n02 = half_cross(x[1], x[2], c4), n07 = half_cross(x[2], x[6], c4);
+    const Vec3<T> n10 = half_cross(x[6], x[5], c4), n06 = half_cross(x[5], x[1], c4);
+    acc_add(k1, n06, n02, n10, n07);
+    fin(1, k1);
+    acc_add(k2, n07, n02, n06, n10);
+    acc_add(k5, n10, n06, n07, n02);
+    fin(5, k5);
+    acc_add(k6, n10, n07, n06, n02);
+  }
+  {
+    const Vec3<T> c5 = q * (x[2] + x[3] + x[7] + x[6]);
+    const Vec3<T> n03 = half_cross(x[2], x[3], c5), n08 = half_cross(x[3], x[7], c5);
+    const Vec3<T> n11 = half_cross(x[7], x[6], c5), n07 = half_cross(x[6], x[2], c5);
+    acc_add(k2, n07, n03, n11, n08);
+    fin(2, k2);
+    acc_add(k3, n08, n03, n07, n11);
+    fin(3, k3);
+    acc_add(k6, n07, n11, n03, n08);
+    fin(6, k6);
+    acc_add(k7, n11, n08, n07, n03);
+    fin(7, k7);
+  }
+}
+
+// Remap face data from a cell's nodes (PrepareRemap.cc:41-55, 105-117;
+// RemapADIService.cc:710): for the low face of each direction (an inner
+// face) |A| along d, u_f and (x_f - x_c).n0 with this cell as the next cell;
+// for the high face (an inner face) (x_f - x_c).n0 with this cell as the
+// previous one.  Face node order: X (0,3,7,4), Y (0,1,5,4), Z (0,1,2,3) low;
+// X (1,2,6,5), Y (3,2,6,7), Z (4,5,6,7) high, in SN_trigo cell-node numbers.
+// T = float takes x relative to the cell centre (xc = 0).
+template <typename T>
+__device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, const Vec3<T> x[8], Vec3<T> xc,
+                                          const double* __restrict__ n0, const double* __restrict__ vh,
+                                          const FaceData& fd) {
+  const T q = T(.25);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int id = d == 0 ? i : (d == 1 ? j : k);
+    const int lo[3][4] = {{0, 3, 7, 4}, {0, 1, 5, 4}, {0, 1, 2, 3}};
+    const int hi[3][4] = {{1, 2, 6, 5}, {3, 2, 6, 7}, {4, 5, 6, 7}};
+    const long long off = d == 0 ? 0 : (d == 1 ? dm.Fx : dm.Fx + dm.Fy);
+    if (id > 0) {
+      const long long f = dm.fid(d, i, j, k);
+      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
+      const Vec3<T> nr = Vec3<T>{(T)nrm.x, (T)nrm.y, (T)nrm.z};
+      const Vec3<T> a0 = x[lo[d][0]], a1 = x[lo[d][1]], a2 = x[lo[d][2]], a3 = x[lo[d][3]];
+      Vec3<T> xf = Vec3<T>{0, 0, 0};
+      xf = xf + q * a0; xf = xf + q * a1; xf = xf + q * a2; xf = xf + q * a3;
+      D3 vs = d3(0., 0., 0.);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int a = lo[d][b];
+        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+        vs = vs + d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]);
+      }
+      const Vec3<T> cr = T(0.5) * cross(a2 - a0, a3 - a1);
+      double A = fabs((double)comp(cr, d));
+      if (!(fabs(comp(nrm, d)) >= 1.0E-10)) A = 0.;   // RemapADIService.cc:925 filter: no flux
+      const long long t = f - off;
+      fd.A[d][t] = A;
+      fd.u[d][t] = dot(.25 * vs, nrm);
+      fd.df[d][t] = (double)dot(xf - xc, nr);
+    }
+    if (id + 1 < dm.ncd(d)) {
+      const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
+      const Vec3<T> nr = Vec3<T>{(T)n0[f], (T)n0[dm.F + f], (T)n0[2 * dm.F + f]};
+      Vec3<T> xf = Vec3<T>{0, 0, 0};
+      xf = xf + q * x[hi[d][0]]; xf = xf + q * x[hi[d][1]]; xf = xf + q * x[hi[d][2]]; xf = xf + q * x[hi[d][3]];
+      fd.db[d][f - off] = (double)dot(xf - xc, nr);
+    }
+  }
 }
 
 // Lagrange thermodynamics of a mesh with K > 1 environments, then the remap
@@ -100,13 +229,13 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
   rho[c] = nd;
 }
 
-template <int K>
+template <int K, typename R>
 __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
     double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
     const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
-    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
-    EnvState env, double* __restrict__ Vlag,
+    double* __restrict__ cqs, float* __restrict__ cqs32, double* __restrict__ L, double* __restrict__ U,
+    double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag,
     int bx_, int by_, int bz_) {
   int i, j, k;
   if (!block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k)) return;
@@ -123,86 +252,45 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
   const D3 xc = .125 * sm;
   xcs[c] = xc.x; xcs[C + c] = xc.y; xcs[2 * C + c] = xc.z;
 
-  // corner vectors, face by face (face centres as in MahycoModule.cc:1080-1087)
-  const double t12 = 1. / 12.;
-  double dv[8];
-  auto finish = [&](int a, const CornerAcc& ac) {
-    const D3 o = t12 * (5. * ac.s1 + ac.s2);
-    cqs[(a * 3 + 0) * C + c] = o.x; cqs[(a * 3 + 1) * C + c] = o.y; cqs[(a * 3 + 2) * C + c] = o.z;
-    dv[a] = dot(x[a], o);
-  };
-  CornerAcc k0, k1, k2, k3, k4, k5, k6, k7;
-  {
-    const D3 c0 = 0.25 * (x[0] + x[3] + x[2] + x[1]);
-    const D3 n04 = half_cross(x[0], x[3], c0), n03 = half_cross(x[3], x[2], c0);
-    const D3 n02 = half_cross(x[2], x[1], c0), n01 = half_cross(x[1], x[0], c0);
-    acc_start(k0, n01, n04, n02, n03);
-    acc_start(k1, n01, n02, n04, n03);
-    acc_start(k2, n02, n03, n01, n04);
-    acc_start(k3, n03, n04, n01, n02);
-  }
-  {
-    const D3 c1 = 0.25 * (x[0] + x[4] + x[7] + x[3]);
-    const D3 n05 = half_cross(x[0], x[4], c1), n12 = half_cross(x[4], x[7], c1);
-    const D3 n08 = half_cross(x[7], x[3], c1), n04 = half_cross(x[3], x[0], c1);
-    acc_add(k0, n04, n05, n08, n12);
-    acc_add(k3, n08, n04, n05, n12);
-    acc_start(k4, n05, n12, n08, n04);
-    acc_start(k7, n08, n12, n04, n05);
-  }
-  {
-    const D3 c2 = 0.25 * (x[0] + x[1] + x[5] + x[4]);
-    const D3 n01 = half_cross(x[0], x[1], c2), n06 = half_cross(x[1], x[5], c2);
-    const D3 n09 = half_cross(x[5], x[4], c2), n05 = half_cross(x[4], x[0], c2);
-    acc_add(k0, n05, n01, n06, n09);
-    finish(0, k0);
-    acc_add(k1, n01, n06, n09, n05);
-    acc_add(k4, n05, n09, n01, n06);
-    acc_start(k5, n06, n09, n01, n05);
-  }
-  {
-    const D3 c3 = 0.25 * (x[4] + x[5] + x[6] + x[7]);
-    const D3 n09 = half_cross(x[4], x[5], c3), n10 = half_cross(x[5], x[6], c3);
-    const D3 n11 = half_cross(x[6], x[7], c3), n12 = half_cross(x[7], x[4], c3);
-    acc_add(k4, n09, n12, n10, n11);
-    finish(4, k4);
-    acc_add(k5, n09, n10, n12, n11);
-    acc_start(k6, n11, n10, n12, n09);
-    acc_add(k7, n12, n11, n09, n10);
-  }
-  {
-    const D3 c4 = 0.25 * (x[1] + x[2] + x[6] + x[5]);
-    const D3 n02 = half_cross(x[1], x[2], c4), n07 = half_cross(x[2], x[6], c4);
-    const D3 n10 = half_cross(x[6], x[5], c4), n06 = half_cross(x[5], x[1], c4);
-    acc_add(k1, n06, n02, n10, n07);
-    finish(1, k1);
-    acc_add(k2, n07, n02, n06, n10);
-    acc_add(k5, n10, n06, n07, n02);
-    finish(5, k5);
-    acc_add(k6, n10, n07, n06, n02);
-  }
-  {
-    const D3 c5 = 0.25 * (x[2] + x[3] + x[7] + x[6]);
-    const D3 n03 = half_cross(x[2], x[3], c5), n08 = half_cross(x[3], x[7], c5);
-    const D3 n11 = half_cross(x[7], x[6], c5), n07 = half_cross(x[6], x[2], c5);
-    acc_add(k2, n07, n03, n11, n08);
-    finish(2, k2);
-    acc_add(k3, n08, n03, n07, n11);
-    finish(3, k3);
-    acc_add(k6, n07, n11, n03, n08);
-    finish(6, k6);
-    acc_add(k7, n11, n08, n07, n03);
-    finish(7, k7);
-  }
+  // corner vectors and volume V = 1/3 sum x_a . cqs_a (MahycoModule.cc:1224-1262)
+  constexpr bool F32 = sizeof(R) == 4;
   double V = 0;
+  F3 xr[8];
+  if constexpr (F32) {
+    // mixed form: FP32 corner vectors from coordinates relative to the
+    // centre (kept in FP32 for the force), volume summed in FP64
 #pragma unroll
-  for (int a = 0; a < 8; ++a) V += dv[a];
+    for (int a = 0; a < 8; ++a)
+      xr[a] = F3{(float)(x[a].x - xc.x), (float)(x[a].y - xc.y), (float)(x[a].z - xc.z)};
+    float dv[8];
+    corner_vectors<float>(xr, [&](int a, F3 o) {
+      cqs32[(a * 3 + 0) * C + c] = o.x; cqs32[(a * 3 + 1) * C + c] = o.y; cqs32[(a * 3 + 2) * C + c] = o.z;
+      dv[a] = dot(xr[a], o);
+    });
+#pragma unroll
+    for (int a = 0; a < 8; ++a) V += (double)dv[a];
+  } else {
+    double dv[8];
+    corner_vectors<double>(x, [&](int a, D3 o) {
+      cqs[(a * 3 + 0) * C + c] = o.x; cqs[(a * 3 + 1) * C + c] = o.y; cqs[(a * 3 + 2) * C + c] = o.z;
+      dv[a] = dot(x[a], o);
+    });
+#pragma unroll
+    for (int a = 0; a < 8; ++a) V += dv[a];
+  }
   V *= 1. / 3;
   double Lc;
   if (ph.lc_mode == 0) Lc = pow_third(V);
   else {
     D3 fc[6];
-    face_centres(x, fc);
+    if constexpr (F32) {
+      D3 xx[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) xx[a] = d3(xr[a].x, xr[a].y, xr[a].z);
+      face_centres(xx, fc);
+    } else {
+      face_centres(x, fc);
+    }
     const double d1 = norm2(fc[0] - fc[3]), d2 = norm2(fc[2] - fc[5]), d3_ = norm2(fc[1] - fc[4]);
     Lc = (d1 * d2 * d3_) / (d1 * d2 + d1 * d3_ + d2 * d3_);
   }
@@ -226,57 +314,20 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
   } else {
     lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag);
   }
-  // Remap face data from this cell's nodes (PrepareRemap.cc:41-55, 105-117;
-  // RemapADIService.cc:710): for the low face of each direction (an inner
-  // face) |A| along d, u_f and (x_f - x_c).n0 with this cell as the next cell;
-  // for the high face (an inner face) (x_f - x_c).n0 with this cell as the
-  // previous one.  Face node order: X (0,3,7,4), Y (0,1,5,4), Z (0,1,2,3) low;
-  // X (1,2,6,5), Y (3,2,6,7), Z (4,5,6,7) high, in SN_trigo cell-node numbers.
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int id = d == 0 ? i : (d == 1 ? j : k);
-    const int lo[3][4] = {{0, 3, 7, 4}, {0, 1, 5, 4}, {0, 1, 2, 3}};
-    const int hi[3][4] = {{1, 2, 6, 5}, {3, 2, 6, 7}, {4, 5, 6, 7}};
-    const long long off = d == 0 ? 0 : (d == 1 ? dm.Fx : dm.Fx + dm.Fy);
-    if (id > 0) {
-      const long long f = dm.fid(d, i, j, k);
-      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
-      const D3 a0 = x[lo[d][0]], a1 = x[lo[d][1]], a2 = x[lo[d][2]], a3 = x[lo[d][3]];
-      D3 xf = d3(0., 0., 0.);
-      xf = xf + .25 * a0; xf = xf + .25 * a1; xf = xf + .25 * a2; xf = xf + .25 * a3;
-      D3 vs = d3(0., 0., 0.);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int a = lo[d][b];
-        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
-        vs = vs + d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]);
-      }
-      const D3 cr = 0.5 * cross(a2 - a0, a3 - a1);
-      double A = fabs(comp(cr, d));
-      if (!(fabs(comp(nrm, d)) >= 1.0E-10)) A = 0.;   // RemapADIService.cc:925 filter: no flux
-      const long long t = f - off;
-      fd.A[d][t] = A;
-      fd.u[d][t] = dot(.25 * vs, nrm);
-      fd.df[d][t] = dot(xf - xc, nrm);
-    }
-    if (id + 1 < dm.ncd(d)) {
-      const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
-      const D3 nrm = d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]);
-      D3 xf = d3(0., 0., 0.);
-      xf = xf + .25 * x[hi[d][0]]; xf = xf + .25 * x[hi[d][1]]; xf = xf + .25 * x[hi[d][2]]; xf = xf + .25 * x[hi[d][3]];
-      fd.db[d][f - off] = dot(xf - xc, nrm);
-    }
-  }
+  if constexpr (F32) face_data<float>(dm, i, j, k, xr, F3{0.f, 0.f, 0.f}, n0, vh, fd);
+  else face_data<double>(dm, i, j, k, x, xc, n0, vh, fd);
 }
 
-template <int K>
-__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells(Dims dm, const Scalars* __restrict__ S, Phys ph,
+template <int K, typename R>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_cyc_lagrange_cells(Dims dm,
+    const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
     double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
     const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
-    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U, double* __restrict__ xcs, FaceData fd,
-    EnvState env, double* __restrict__ Vlag, int linear) {
-  k_cyc_lagrange_cells_body<K>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, L, U, xcs, fd, env, Vlag, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
+    double* __restrict__ cqs, float* __restrict__ cqs32, double* __restrict__ L, double* __restrict__ U,
+    double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag, int linear) {
+  k_cyc_lagrange_cells_body<K, R>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, cqs32, L, U, xcs, fd, env, Vlag,
+                                  blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
 }
 
 

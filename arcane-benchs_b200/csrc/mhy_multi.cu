@@ -504,9 +504,9 @@ void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
 #define MHY_LAG_ENV(KK)                                                                                         \
-  k_cyc_lagrange_cells<KK><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q,    \
-                                               a.st.p, a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd,     \
-                                               a.env, a.Vlag, linear)
+  k_cyc_lagrange_cells<KK, double><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e,     \
+                                                       a.st.q, a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L,  \
+                                                       a.U[0], a.xc, a.fd, a.env, a.Vlag, linear)
   if (a.K == 2) MHY_LAG_ENV(2);
   else if (a.K == 3) MHY_LAG_ENV(3);
   else MHY_LAG_ENV(4);
