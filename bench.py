@@ -68,6 +68,11 @@ def parse():
     return ap.parse_args()
 
 
+# DRAM bytes (read + write) of one whole cycle, summed over its kernels, from
+# one ncu capture of the 128^3 Sedov cycle (profiles/dram_traffic_sedov128_cycle.md).
+TRAFFIC_PER_CYCLE = {("sedov", 128, "fp64"): 3477780736.0, ("sedov", 128, "mixed"): 2921549568.0}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -422,8 +427,11 @@ def run_ours(args):
     per_gpu_cells_per_s = case.ncells * args.steps / (ms / 1e3)
     achieved = b_alg * per_gpu_cells_per_s / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "kernel": f"one cycle graph ({kpc} kernels), algorithmic bytes {b_alg:.1f} B/cell-cycle",
+                "frac": round(achieved / peak, 4),
+                "traffic": TRAFFIC_PER_CYCLE.get((args.workload, args.n, args.precision)),
+                "algorithmic_bytes_per_launch": round(b_alg * case.ncells, 1),
+                "kernel": f"one cycle graph ({kpc} kernels, launched as one unit), algorithmic bytes "
+                          f"{b_alg:.1f} B/cell-cycle x {case.ncells} cells; traffic = DRAM bytes of one cycle (ncu)",
                 "peak_kind": peak_kind}
 
     cpu = None
