@@ -143,8 +143,6 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0 (minmod), 1 (superBee) or 2 (vanLeer)");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
   if (opt->precision < 0 || opt->precision > 1) return fail(MHY_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
-  if (opt->precision == 1 && opt->nb_env != 1)
-    return fail(MHY_ERR_UNSUPPORTED, "the mixed-precision form is implemented for one environment");
   for (int b = 0; b < opt->nb_bc; ++b)
     if (opt->bc[b].surface < 0 || opt->bc[b].surface > 5 || opt->bc[b].type < 0 || opt->bc[b].type > 2)
       return fail(MHY_ERR_ARG, "bad boundary condition");

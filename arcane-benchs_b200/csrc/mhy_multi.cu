@@ -43,15 +43,15 @@ struct CellInK {
 // One line step of the remap of a K-environment cell (RemapADIService.cc:91-271,
 // 447-517, 658-720, 883-1040).  out = the 3K+1 updated components, then the
 // K dual mass fluxes.
-template <int K, bool FIRST>
+template <int K, bool FIRST, typename R>
 __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
                                               bool upd, const CellInK<K>& in, double* out) {
   constexpr int NV = 3 * K + 1;
-  const double order2 = (double)(ph.ordre_projection - 1);
+  const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
-  double P[NV];
+  R P[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) P[v] = 0.;
+  for (int v = 0; v < NV; ++v) P[v] = 0;
   if (valid) {
     double den;
     if (FIRST) den = in.den;
@@ -60,42 +60,43 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
 #pragma unroll
       for (int k = 0; k < K; ++k) den += in.U[k];
     }
-    const double r = 1.0 / den;
+    const R dR = (R)den, r = Ar<R>::rcp(dR);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) P[v] = qdiv(in.U[v], den, r);
+    for (int v = 0; v < NV; ++v) P[v] = Ar<R>::div((R)in.U[v], dR, r);
   }
   const unsigned full = 0xffffffffu;
   const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
                xpz = __shfl_up_sync(full, in.xc[2], 1);
   const double dx = inner ? dot(d3(in.xc[0], in.xc[1], in.xc[2]) - d3(xpx, xpy, xpz), d3(in.n[0], in.n[1], in.n[2]))
                           : 0.;
-  const double rdx = inner ? 1.0 / dx : 0.;
-  double G[NV], Pp[NV];
+  const R dxR = (R)dx, rdx = inner ? Ar<R>::rcp(dxR) : R(0);
+  R G[NV], Pp[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     Pp[v] = __shfl_up_sync(full, P[v], 1);
-    const double g = inner ? qdiv(P[v] - Pp[v], dx, rdx) : 0.;
-    const double gr = __shfl_down_sync(full, g, 1);
-    G[v] = limited_one(lim, g, gr);
+    const R g = inner ? Ar<R>::div(P[v] - Pp[v], dxR, rdx) : R(0);
+    const R gr = __shfl_down_sync(full, g, 1);
+    G[v] = limited_one<R>(lim, g, gr);
   }
   const bool back = in.u * dx > 0.0;
-  const double dot_xf = back ? in.db : in.df;
-  double Pf[NV], Pfn[NV];
+  const R dot_xf = (R)(back ? in.db : in.df);
+  R Pf[NV], Pfn[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    const double Gp = __shfl_up_sync(full, G[v], 1);
-    Pf[v] = inner ? (back ? (Pp[v] + order2 * dot_xf * Gp) : (P[v] + order2 * dot_xf * G[v])) : 0.;
+    const R Gp = __shfl_up_sync(full, G[v], 1);
+    Pf[v] = inner ? (back ? (Pp[v] + order2 * dot_xf * Gp) : (P[v] + order2 * dot_xf * G[v])) : R(0);
     Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
   }
   const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
   if (!upd) return;
+  // flux sums in FP64 in every precision (each face flux is one rounded value)
   const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
   const double cf = infr ? in.of * un * An * dt : 0.;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     double flux_face = 0., dp = 0.;
-    if (inner) { const double fl = cb * Pf[v]; flux_face += fl; dp += 0.5 * fl * in.ob; }
-    if (infr) { const double fl = cf * Pfn[v]; flux_face += fl; dp += 0.5 * fl * in.of; }
+    if (inner) { const double fl = (double)((R)cb * Pf[v]); flux_face += fl; dp += 0.5 * fl * in.ob; }
+    if (infr) { const double fl = (double)((R)cf * Pfn[v]); flux_face += fl; dp += 0.5 * fl * in.of; }
     out[v] = in.U[v] - flux_face;
     if (v >= K && v < 2 * K) out[NV + v - K] = dp;
   }
@@ -107,7 +108,7 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
 }
 
 // K-environment cell sweep along x (lanes along the rows).
-template <int K, bool FIRST>
+template <int K, bool FIRST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
   }
   if (upd) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }
   double out[NV + K];
-  cell_line_env<K, FIRST>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (!upd) return;
 #pragma unroll
   for (int v = 0; v < NV; ++v) Uout[v * C + c] = out[v];
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
 template <int K, bool FIRST>
 __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
 
-template <int K, int D, bool FIRST>
+template <int K, int D, bool FIRST, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_t(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
   constexpr int NO = NV + K;
   static_assert(NO <= NA, "outputs reuse the staged rows");
   double out[NO];
-  cell_line_env<K, FIRST>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (upd) {
 #pragma unroll
     for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];
@@ -445,32 +446,33 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int K, int D, bool FIRST>
+template <int K, int D, bool FIRST, typename R>
 static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + kLineWarps - 1) / kLineWarps, nseg, D == 1 ? dm.nz : dm.ny);
   const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * kTileArr * sizeof(double);
-  k_env_sweep_cells_t<K, D, FIRST><<<g, 32 * kLineWarps, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin,
-                                                                     Uout, a.dpf, a.Vlag);
+  k_env_sweep_cells_t<K, D, FIRST, R><<<g, 32 * kLineWarps, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin,
+                                                                        Uout, a.dpf, a.Vlag);
 }
 
-template <int K, bool FIRST>
+template <int K, bool FIRST, typename R>
 static void env_cells(const CycleArgs& a, int d, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   if (d == 0) {
     const int nseg = (dm.nx + kLineUpd - 1) / kLineUpd;
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
-    k_env_sweep_cells_x<K, FIRST><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout,
-                                                                a.dpf, a.Vlag);
+    k_env_sweep_cells_x<K, FIRST, R><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin,
+                                                                   Uout, a.dpf, a.Vlag);
   } else if (d == 1) {
-    env_cells_staged<K, 1, FIRST>(a, Uin, Uout, s);
+    env_cells_staged<K, 1, FIRST, R>(a, Uin, Uout, s);
   } else {
-    env_cells_staged<K, 2, FIRST>(a, Uin, Uout, s);
+    env_cells_staged<K, 2, FIRST, R>(a, Uin, Uout, s);
   }
 }
 
-template <int K>
+// R: evaluation type of the sweeps (double, or float in the mixed form).
+template <int K, typename R>
 static void remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
@@ -480,43 +482,61 @@ static void remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
     double* uout = a.U[(it + 1) & 1];
     const double* udin = a.ud[(it + 1) & 1];
     double* udout = a.ud[it & 1];
-    if (first) env_cells<K, true>(a, d, uin, uout, s);
-    else env_cells<K, false>(a, d, uin, uout, s);
+    if (first) env_cells<K, true, R>(a, d, uin, uout, s);
+    else env_cells<K, false, R>(a, d, uin, uout, s);
     if (last) {
       const unsigned nb = (unsigned)((a.dm.C + 255) / 256);
       k_env_finalize_cells<K><<<nb, 256, 0, s>>>(a.dm, a.S, a.ph, a.env, uout, a.st);
     }
-    sweep_nodes<K>(a, d, first, last, prev, udin, udout, s);
+    sweep_nodes<K, R>(a, d, first, last, prev, udin, udout, s);
     prev |= 1 << d;
   }
 }
 
+template <int K, typename R>
+static void set_env_attributes_r() {
+  const int mx = (int)(env_cells_staged_arrays<K, true>() * kTileArr * sizeof(double));
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
+
 template <int K>
 static void set_env_attributes() {
-  const int mx = (int)(env_cells_staged_arrays<K, true>() * kTileArr * sizeof(double));
-  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  set_env_attributes_r<K, double>();
+  set_env_attributes_r<K, float>();
 }
 
 void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
-#define MHY_LAG_ENV(KK)                                                                                         \
-  k_cyc_lagrange_cells<KK, double><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e,     \
+#define MHY_LAG_ENV(KK, RR)                                                                                     \
+  k_cyc_lagrange_cells<KK, RR><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e,     \
                                                        a.st.q, a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L,  \
                                                        a.U[0], a.xc, a.fd, a.env, a.Vlag, linear)
-  if (a.K == 2) MHY_LAG_ENV(2);
-  else if (a.K == 3) MHY_LAG_ENV(3);
-  else MHY_LAG_ENV(4);
+  if (a.ph.precision) {
+    if (a.K == 2) MHY_LAG_ENV(2, float);
+    else if (a.K == 3) MHY_LAG_ENV(3, float);
+    else MHY_LAG_ENV(4, float);
+  } else {
+    if (a.K == 2) MHY_LAG_ENV(2, double);
+    else if (a.K == 3) MHY_LAG_ENV(3, double);
+    else MHY_LAG_ENV(4, double);
+  }
 #undef MHY_LAG_ENV
 }
 
 void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
-  if (a.K == 2) remap_env<2>(a, sens, s);
-  else if (a.K == 3) remap_env<3>(a, sens, s);
-  else remap_env<4>(a, sens, s);
+  if (a.ph.precision) {
+    if (a.K == 2) remap_env<2, float>(a, sens, s);
+    else if (a.K == 3) remap_env<3, float>(a, sens, s);
+    else remap_env<4, float>(a, sens, s);
+  } else {
+    if (a.K == 2) remap_env<2, double>(a, sens, s);
+    else if (a.K == 3) remap_env<3, double>(a, sens, s);
+    else remap_env<4, double>(a, sens, s);
+  }
 }
 
 // Called once per context before any cycle (and so before any graph capture).

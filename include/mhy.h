@@ -75,7 +75,7 @@ typedef struct mhy_options {
   int32_t precision;                 /* 0: plain FP64 (bit for bit the reference's arithmetic);
                                         1: mixed: the remap's Phi, gradients, limiters, face values and
                                         flux terms in FP32; state, coordinates, volumes, conserved sums
-                                        and the dt reduction in FP64 (one environment) */
+                                        and the dt reduction in FP64 */
   int32_t reserved[7];
 } mhy_options;
 

@@ -65,3 +65,24 @@ def test_batched_mixed_equals_single_mixed():
         g.step(30)
         for f in ("density", "internal_energy", "velocity"):
             assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
+
+
+@pytest.mark.parametrize("make,cycles,K", [
+    (lambda: gen.two_material(32, 16, 16, cycles=120), 120, 2),
+    (lambda: gen.three_material(36, 12, 12, cycles=80), 80, 3),
+])
+def test_mixed_multi_material_vs_fp64_oracle(make, cycles, K):
+    """Several gases in the mixed form: global density within 1e-5 L1 of the
+    FP64 oracle, and each gas's volume within 1e-5 (relative to the domain)."""
+    ref = make()
+    o = mhy_oracle.Oracle(ref)
+    o.step(cycles)
+    g = Context(mixed(make()))
+    g.step(cycles)
+    g.synchronize()
+    assert g.status() == 0
+    assert l1_rel(g.field("density"), o.field("density")) <= 1e-5
+    vol = o.field("cell_volume")
+    for k in range(K):
+        fo, fg = o.env_field("fracvol", k), g.env_field("fracvol", k)
+        assert abs(float(((fg - fo) * vol).sum())) / float(vol.sum()) <= 1e-5, k
