@@ -327,26 +327,48 @@ int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
   return MHY_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Initial geometry from the mesh: cell centres and corner vectors, Eulerian
+// volumes and lengths, face normals, outward face normals
+// (MahycoAnnexe.cc:102-109, MahycoModule.cc:1008-1050, 1054-1262 at t = 0).
+int init_geometry(mhy_ctx* c) {
+  const Dims& dm = c->dm;
+  cudaStream_t s = c->stream;
+  double *xc0 = nullptr, *xf0 = nullptr;          // temporaries: initial cell and face centres
+  MHY_CUDA(cudaMalloc(&xc0, 3 * dm.C * sizeof(double)));
+  cudaError_t err = cudaMalloc(&xf0, 3 * dm.F * sizeof(double));
+  if (err != cudaSuccess) { cudaFree(xc0); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
+  k_init_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, xc0, c->cqs, c->Ve, c->L, c->ph.lc_mode);
+  k_init_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->x0, c->n0, xf0);
+  k_init_outer_normals<<<blocks(dm.C), kThreads, 0, s>>>(dm, xc0, xf0, c->ofn);
+  err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  cudaFree(xc0);
+  cudaFree(xf0);
+  if (err != cudaSuccess) return fail(MHY_ERR_CUDA, cudaGetErrorString(err));
+  return MHY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mhy_hydro_start_init(mhy_ctx* c) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
   if (!c->state_set) return fail(MHY_ERR_STATE, "mhy_set_state must come first");
   const Dims& dm = c->dm;
   cudaStream_t s = c->stream;
-  // temporaries: initial cell and face centres
-  double *xc0 = nullptr, *xf0 = nullptr;
-  MHY_CUDA(cudaMalloc(&xc0, 3 * dm.C * sizeof(double)));
-  MHY_CUDA(cudaMalloc(&xf0, 3 * dm.F * sizeof(double)));
-  k_init_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, xc0, c->cqs, c->Ve, c->L, c->ph.lc_mode);
-  k_init_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->x0, c->n0, xf0);
-  k_init_outer_normals<<<blocks(dm.C), kThreads, 0, s>>>(dm, xc0, xf0, c->ofn);
+  const int rc = init_geometry(c);
+  if (rc != MHY_OK) return rc;
   if (c->K == 1) k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph.gamma, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
   else launch_init_env(c->args(), s);
   k_node_mass<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->mass, c->nm);
   if (c->cqs32) k_to_f32<<<blocks(24 * dm.C), kThreads, 0, s>>>(24 * dm.C, c->cqs, c->cqs32);
   MHY_CUDA(cudaGetLastError());
   MHY_CUDA(cudaStreamSynchronize(s));
-  cudaFree(xc0);
-  cudaFree(xf0);
   c->initialized = true;
   c->phase = PH_SAVE;
   return MHY_OK;
@@ -662,6 +684,144 @@ int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
     for (long long i = 0; i < n; ++i)
       for (int a = 0; a < 3; ++a) o[3 * i + a] = soa[a * n + i];
   }
+  return MHY_OK;
+}
+
+// ---- restart dump ------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// Layout of a restart dump: CkptHeader, nfields CkptField records, then the
+// arrays (each at its record's offset from the start of the dump, 64-byte
+// aligned).  Field names are the reference's variable names (Mahyco.axl).
+struct CkptHeader {
+  char magic[8];
+  int32_t version, nx, ny, nz, nenv, precision, nfields, sens;
+  double dt, old_dt, time;
+  int64_t iteration;
+  uint32_t status, pad;
+};
+struct CkptField {
+  char name[40];
+  int32_t dtype;        // 0 double, 1 float, 2 uint32
+  int32_t pad;
+  int64_t count, offset;
+};
+constexpr char kCkptMagic[8] = {'M', 'H', 'Y', 'C', 'K', 'P', 'T', '1'};
+
+struct CkField { const char* name; void* dev; int dtype; long long count; };
+
+// The state a cycle starts from: everything a kernel reads before writing it.
+std::vector<CkField> ckpt_fields(mhy_ctx* c) {
+  const long long C = c->dm.C, N = c->dm.N;
+  const int K = c->K;
+  std::vector<CkField> f = {
+      {"Density", c->rho, 0, C}, {"InternalEnergy", c->e, 0, C}, {"Pressure", c->p, 0, C},
+      {"SoundSpeed", c->cs, 0, C}, {"PseudoViscosity", c->q, 0, C}, {"CellMass", c->mass, 0, C},
+      {"Velocity", c->v, 0, 3 * N}, {"NodeMass", c->nm, 0, N}, {"DualGradPhi", c->Gd, 0, 3 * N}};
+  if (c->cqs32) f.push_back({"CellCQS", c->cqs32, 1, 24 * C});
+  else f.push_back({"CellCQS", c->cqs, 0, 24 * C});
+  if (K > 1) {
+    const EnvState& ev = c->env;
+    f.push_back({"EnvMask", ev.mask, 2, C});
+    f.push_back({"FracVol.env", ev.f, 0, K * C}); f.push_back({"MassFraction.env", ev.x, 0, K * C});
+    f.push_back({"Density.env", ev.rho, 0, K * C}); f.push_back({"InternalEnergy.env", ev.e, 0, K * C});
+    f.push_back({"Pressure.env", ev.p, 0, K * C}); f.push_back({"SoundSpeed.env", ev.cs, 0, K * C});
+    f.push_back({"PseudoViscosity.env", ev.q, 0, K * C}); f.push_back({"CellMass.env", ev.m, 0, K * C});
+    f.push_back({"FracVol", ev.fg, 0, C}); f.push_back({"MassFraction", ev.xg, 0, C});
+  }
+  return f;
+}
+
+size_t ckpt_elem(int dtype) { return dtype == 0 ? 8 : 4; }
+
+size_t ckpt_layout(const std::vector<CkField>& f, std::vector<int64_t>& offsets) {
+  size_t off = sizeof(CkptHeader) + f.size() * sizeof(CkptField);
+  offsets.clear();
+  for (const CkField& x : f) {
+    off = (off + 63) & ~size_t(63);
+    offsets.push_back((int64_t)off);
+    off += (size_t)x.count * ckpt_elem(x.dtype);
+  }
+  return off;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhy_checkpoint_size(mhy_ctx* c, size_t* bytes) {
+  if (!c || !bytes) return fail(MHY_ERR_ARG, "null argument");
+  std::vector<int64_t> off;
+  *bytes = ckpt_layout(ckpt_fields(c), off);
+  return MHY_OK;
+}
+
+int mhy_checkpoint_save(mhy_ctx* c, void* dst, size_t bytes) {
+  if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
+  if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "a restart dump is taken between cycles");
+  const std::vector<CkField> f = ckpt_fields(c);
+  std::vector<int64_t> off;
+  const size_t need = ckpt_layout(f, off);
+  if (bytes < need) return fail(MHY_ERR_ARG, "destination too small (mhy_checkpoint_size)");
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
+  Scalars h{};
+  MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
+  char* base = static_cast<char*>(dst);
+  std::memset(base, 0, sizeof(CkptHeader) + f.size() * sizeof(CkptField));
+  CkptHeader hd{};
+  std::memcpy(hd.magic, kCkptMagic, 8);
+  hd.version = 1; hd.nx = c->dm.nx; hd.ny = c->dm.ny; hd.nz = c->dm.nz; hd.nenv = c->K;
+  hd.precision = c->ph.precision; hd.nfields = (int32_t)f.size(); hd.sens = c->sens;
+  hd.dt = h.dt; hd.old_dt = h.old_dt; hd.time = h.time; hd.iteration = h.iteration; hd.status = h.status;
+  std::memcpy(base, &hd, sizeof(hd));
+  for (size_t i = 0; i < f.size(); ++i) {
+    CkptField r{};
+    std::strncpy(r.name, f[i].name, sizeof(r.name) - 1);
+    r.dtype = f[i].dtype; r.count = f[i].count; r.offset = off[i];
+    std::memcpy(base + sizeof(CkptHeader) + i * sizeof(CkptField), &r, sizeof(r));
+    MHY_CUDA(cudaMemcpy(base + off[i], f[i].dev, (size_t)f[i].count * ckpt_elem(f[i].dtype), cudaMemcpyDeviceToHost));
+  }
+  return MHY_OK;
+}
+
+int mhy_checkpoint_load(mhy_ctx* c, const void* src, size_t bytes) {
+  if (!c || !src) return fail(MHY_ERR_ARG, "null argument");
+  if (bytes < sizeof(CkptHeader)) return fail(MHY_ERR_ARG, "not a restart dump");
+  const char* base = static_cast<const char*>(src);
+  CkptHeader hd;
+  std::memcpy(&hd, base, sizeof(hd));
+  if (std::memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1) return fail(MHY_ERR_ARG, "not a restart dump");
+  if (hd.nx != c->dm.nx || hd.ny != c->dm.ny || hd.nz != c->dm.nz || hd.nenv != c->K ||
+      hd.precision != c->ph.precision)
+    return fail(MHY_ERR_ARG, "restart dump of another mesh, environment count or precision");
+  if (hd.sens < 0 || hd.sens > 2) return fail(MHY_ERR_ARG, "corrupt restart dump");
+  const std::vector<CkField> f = ckpt_fields(c);
+  if (hd.nfields != (int32_t)f.size() || bytes < sizeof(CkptHeader) + f.size() * sizeof(CkptField))
+    return fail(MHY_ERR_ARG, "restart dump field list does not match this context");
+  // geometry of t = 0 from the mesh, then the dumped state over it
+  const int rc = init_geometry(c);
+  if (rc != MHY_OK) return rc;
+  for (size_t i = 0; i < f.size(); ++i) {
+    CkptField r;
+    std::memcpy(&r, base + sizeof(CkptHeader) + i * sizeof(CkptField), sizeof(r));
+    r.name[sizeof(r.name) - 1] = 0;
+    const size_t nb = (size_t)f[i].count * ckpt_elem(f[i].dtype);
+    if (std::strcmp(r.name, f[i].name) != 0 || r.dtype != f[i].dtype || r.count != f[i].count || r.offset < 0 ||
+        (size_t)r.offset + nb > bytes)
+      return fail(MHY_ERR_ARG, std::string("restart dump field mismatch: ") + f[i].name);
+    MHY_CUDA(cudaMemcpy(f[i].dev, base + r.offset, nb, cudaMemcpyHostToDevice));
+  }
+  Scalars h{};
+  h.dt = hd.dt; h.old_dt = hd.old_dt; h.inv_dt = 1.0 / hd.dt; h.time = hd.time;
+  h.min_bits = 0x7fefffffffffffffull; h.status = hd.status; h.iteration = hd.iteration;
+  MHY_CUDA(cudaMemcpy(c->S, &h, sizeof(h), cudaMemcpyHostToDevice));
+  c->sens = hd.sens;
+  c->state_set = true;
+  c->initialized = true;
+  c->phase = PH_SAVE;
   return MHY_OK;
 }
 

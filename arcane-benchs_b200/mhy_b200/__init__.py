@@ -36,7 +36,7 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_get_env_mask", "mhy_batch_create", "mhy_batch_set_state", "mhy_batch_hydro_start_init",
             "mhy_batch_step", "mhy_batch_synchronize", "mhy_batch_get_field", "mhy_batch_get_dt",
             "mhy_batch_get_status", "mhy_batch_size", "mhy_batch_kernels_per_cycle", "mhy_batch_get_stream",
-            "mhy_batch_destroy"]
+            "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load"]
 ENV_FIELDS = {"fracvol": 0, "density": 1, "internal_energy": 2, "pressure": 3, "sound_speed": 4,
               "mass_fraction": 5, "cell_mass": 6}
 
@@ -124,6 +124,9 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_batch_get_stream.restype = vp
     L.mhy_batch_destroy.argtypes = [vp]
     L.mhy_batch_destroy.restype = None
+    L.mhy_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.mhy_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
+    L.mhy_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
     _lib = L
     return L
 
@@ -226,6 +229,31 @@ class Context:
             out = np.empty(c.ncells)
         _check(load().mhy_get_field(self.h, fid, out.ctypes.data_as(ctypes.c_void_p), out.nbytes))
         return out
+
+    def save_checkpoint(self) -> bytes:
+        """Restart dump of the state between cycles (mhy_checkpoint_save)."""
+        L = load()
+        n = ctypes.c_size_t()
+        _check(L.mhy_checkpoint_size(self.h, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(L.mhy_checkpoint_save(self.h, buf, n.value))
+        return buf.raw
+
+    @classmethod
+    def from_checkpoint(cls, case, blob: bytes, device: int = -1):
+        """A context on case's mesh and options, resumed from a restart dump."""
+        self = cls.__new__(cls)
+        L = load()
+        self.case = case
+        self._coords = np.ascontiguousarray(case.coords, dtype=np.float64)
+        mesh = CMesh(case.nx, case.ny, case.nz, _dp(self._coords))
+        opt = make_options(case.options, case.gamma)
+        h = ctypes.c_void_p()
+        _check(L.mhy_create(ctypes.byref(mesh), ctypes.byref(opt), device, ctypes.byref(h)))
+        self.h = h
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        _check(L.mhy_checkpoint_load(self.h, buf, len(blob)))
+        return self
 
     def env_field(self, name: str, k: int) -> np.ndarray:
         """Value of environment k in every cell (0 where the cell does not hold it)."""

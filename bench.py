@@ -445,7 +445,7 @@ def run_ours(args):
                 "config": {"workload": wname, "cells": case.ncells, "nodes": case.nnodes,
                            "environments": case.nenv,
                            "cells_per_gpu": case.ncells, "parallelism": f"replicas{world}",
-                           "l2": "working set ~2 GB > 126 MB L2 (no flush needed)"},
+                           "l2": "working set > 1 GB, far above the 126 MB L2 (no flush needed)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status}
         if accuracy:

@@ -172,6 +172,21 @@ int mhy_kernels_per_cycle(mhy_ctx* ctx);
 const char* mhy_last_error(void);
 void mhy_destroy(mhy_ctx* ctx);
 
+/* ---- restart dump (checkpoint / resume) ----
+ * The state a cycle starts from, as one host buffer: dt, old dt, time,
+ * iteration, remap direction, and the cell and node variables the reference
+ * dumps for a restart (Mahyco.axl variables with dump="true": Density,
+ * InternalEnergy, Pressure, SoundSpeed, PseudoViscosity, CellMass, Velocity,
+ * NodeMass, CellCQS, DualGradPhi, and the per-environment values), in a
+ * self-describing layout (header, named field records, arrays).  Save between
+ * cycles; load into a context created with the same mesh and options (in
+ * place of mhy_set_state + mhy_hydro_start_init: the "continue-init"
+ * entry point hydroContinueInit, MahycoModule.cc:269-305, Mahyco.axl:153).  The continued run equals the uninterrupted one bit for
+ * bit. */
+int mhy_checkpoint_size(mhy_ctx* ctx, size_t* bytes);
+int mhy_checkpoint_save(mhy_ctx* ctx, void* dst, size_t bytes);
+int mhy_checkpoint_load(mhy_ctx* ctx, const void* src, size_t bytes);
+
 /* ---- batches: many independent single-environment meshes on one GPU ----
  * No counterpart in the reference (one Arcane process runs one mesh): a batch
  * advances n instances of uneven sizes, options and initial states together,
