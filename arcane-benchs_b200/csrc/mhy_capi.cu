@@ -46,8 +46,9 @@ struct mhy_ctx {
   Phys ph{};
   BCTable bct{};
   mhy_options opt{};
-  std::vector<double> h_coords;
   std::vector<void*> allocs;
+  std::vector<std::pair<void**, size_t>> plan;   // arena requests (pointer, bytes)
+  double* setup = nullptr;                       // 1024 doubles of set-up scratch
   // nodes
   double *x0 = nullptr, *v = nullptr, *vh = nullptr, *nm = nullptr, *Gd = nullptr, *vnorm = nullptr;
   double *ud[2] = {nullptr, nullptr};
@@ -71,13 +72,26 @@ struct mhy_ctx {
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int kernels_per_cycle = 0;
 
+  // Device arrays come from one allocation: alloc() records a request,
+  // commit() allocates the sum (256-byte aligned pieces) and sets the pointers.
   template <class T>
   int alloc(T** ptr, size_t count) {
-    void* p_ = nullptr;
-    cudaError_t err = cudaMalloc(&p_, count * sizeof(T) + 16);
+    plan.emplace_back(reinterpret_cast<void**>(ptr), count * sizeof(T));
+    return MHY_OK;
+  }
+  int commit() {
+    size_t total = 0;
+    for (auto& r : plan) total += (r.second + 255) & ~size_t(255);
+    void* base = nullptr;
+    cudaError_t err = cudaMalloc(&base, total + 256);
     if (err != cudaSuccess) return fail(MHY_ERR_OOM, "cudaMalloc failed: " + std::string(cudaGetErrorString(err)));
-    allocs.push_back(p_);
-    *ptr = static_cast<T*>(p_);
+    allocs.push_back(base);
+    char* p_ = static_cast<char*>(base);
+    for (auto& r : plan) {
+      *r.first = p_;
+      p_ += (r.second + 255) & ~size_t(255);
+    }
+    plan.clear();
     return MHY_OK;
   }
 
@@ -172,7 +186,6 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   ph.precision = opt->precision;
   c->bct.nb = opt->nb_bc;
   for (int b = 0; b < opt->nb_bc; ++b) { c->bct.type[b] = opt->bc[b].type; c->bct.value[b] = opt->bc[b].value; }
-  c->h_coords.assign(mesh->node_coords, mesh->node_coords + 3 * dm.N);
 
   int rc = MHY_OK;
   auto A_ = [&](double** pp, long long n) { if (rc == MHY_OK) rc = c->alloc(pp, (size_t)n); };
@@ -203,67 +216,44 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
+  if (rc == MHY_OK) rc = c->alloc(&c->setup, 1024);
+  if (rc == MHY_OK) rc = c->commit();
   if (rc != MHY_OK) { mhy_destroy(c); return rc; }
   cudaError_t err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
 
-  // node coordinates xyz-interleaved -> SoA
+  // Set-up on the device: the interleaved coordinates are staged in ud[0]
+  // (5N doubles) and the node groups in vh, arrays the first cycle
+  // overwrites; the per-block coordinate maxima and the BC surfaces go to
+  // the set-up scratch.
   {
-    std::vector<double> soa(3 * N);
-    for (long long n = 0; n < N; ++n)
-      for (int a = 0; a < 3; ++a) soa[a * N + n] = c->h_coords[3 * n + a];
-    err = cudaMemcpy(c->x0, soa.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice);
-    if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  }
-  // dual gradients of nodes never inner so far read 0 (the reference's
-  // variables start at zero)
-  cudaMemset(c->Gd, 0, 3 * N * sizeof(double));
-
-  // Boundary node groups by coordinate threshold, PrepareFaceGroup
-  // (MahycoAnnexe.cc:183-251); bit b of bcmask[n] set when BC entry b applies.
-  {
-    const int nx = dm.nx, ny = dm.ny, nz = dm.nz;
-    const double* X = c->h_coords.data();
-    double mx[3] = {-1., -1., -1.};
-    for (long long n = 0; n < N; ++n)
-      for (int a = 0; a < 3; ++a) mx[a] = (mx[a] < X[3 * n + a]) ? X[3 * n + a] : mx[a];
-    std::vector<uint8_t> grp(N, 0);
-    const double thr = opt->threshold;
-    auto nid = [&](int i, int j, int k) { return (long long)i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k); };
-    auto face = [&](long long f0, long long f1, long long f2, long long f3) {
-      long long fn[4] = {f0, f1, f2, f3};
-      uint8_t fl = 0x3f;
-      for (int a = 0; a < 4; ++a) {
-        const double* x = X + 3 * fn[a];
-        if (x[0] > thr) fl &= ~(1u << MHY_XMIN);
-        if (x[1] > thr) fl &= ~(1u << MHY_YMIN);
-        if (x[2] > thr) fl &= ~(1u << MHY_ZMIN);
-        if (std::fabs(x[0] - mx[0]) > thr) fl &= ~(1u << MHY_XMAX);
-        if (std::fabs(x[1] - mx[1]) > thr) fl &= ~(1u << MHY_YMAX);
-        if (std::fabs(x[2] - mx[2]) > thr) fl &= ~(1u << MHY_ZMAX);
-      }
-      if (fl) for (int a = 0; a < 4; ++a) grp[fn[a]] |= fl;
-    };
-    for (int k = 0; k < nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i <= nx; ++i)
-      face(nid(i, j, k), nid(i, j + 1, k), nid(i, j + 1, k + 1), nid(i, j, k + 1));
-    for (int k = 0; k < nz; ++k) for (int j = 0; j <= ny; ++j) for (int i = 0; i < nx; ++i)
-      face(nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j, k + 1), nid(i, j, k + 1));
-    for (int k = 0; k <= nz; ++k) for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i)
-      face(nid(i, j, k), nid(i + 1, j, k), nid(i + 1, j + 1, k), nid(i, j + 1, k));
-    std::vector<uint16_t> mask(N, 0);
-    for (long long n = 0; n < N; ++n)
-      for (int b = 0; b < opt->nb_bc; ++b)
-        if (grp[n] >> opt->bc[b].surface & 1u) mask[n] |= (uint16_t)(1u << b);
-    err = cudaMemcpy(c->bcmask, mask.data(), N * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    const long long nb = (N + 255) / 256;
+    const int nparts = 256;
+    err = cudaMemcpyAsync(c->ud[0], mesh->node_coords, 3 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (err == cudaSuccess) {
+      k_soa3<<<(unsigned)nb, 256, 0, c->stream>>>(N, c->ud[0], c->x0);
+      // dual gradients of nodes never inner so far read 0 (the reference's variables start at zero)
+      cudaMemsetAsync(c->Gd, 0, 3 * N * sizeof(double), c->stream);
+      k_max3_partial<<<nparts, 256, 0, c->stream>>>(N, c->x0, c->setup);
+      unsigned* grp = reinterpret_cast<unsigned*>(c->vh);
+      cudaMemsetAsync(grp, 0, N * sizeof(unsigned), c->stream);
+      k_face_groups<<<(unsigned)((F + 255) / 256), 256, 0, c->stream>>>(dm, c->x0, c->setup, nparts, opt->threshold, grp);
+      int* surf = reinterpret_cast<int*>(c->setup + 3 * nparts);
+      int hs[MHY_MAX_BC] = {};
+      for (int b = 0; b < opt->nb_bc; ++b) hs[b] = opt->bc[b].surface;
+      err = cudaMemcpyAsync(surf, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream);
+      k_bc_mask<<<(unsigned)nb, 256, 0, c->stream>>>(N, grp, opt->nb_bc, surf, c->bcmask);
+      if (err == cudaSuccess) err = cudaGetLastError();
+      if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
+    }
     if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   }
   Scalars s0{};
   s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.inv_dt = 1.0 / opt->deltat_init; s0.min_bits = 0x7fefffffffffffffull;
-  err = cudaMemcpy(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice);
+  err = cudaMemcpyAsync(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv : kKernelsPerCycle;
-  err = cudaDeviceSynchronize();  // the memsets above ran on the legacy stream
-  if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   *out = c;
   return MHY_OK;
 }
@@ -275,8 +265,8 @@ int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
   if (K == 1) {
     for (long long i = 0; i < C; ++i)
       if (!(st->fracvol[i] > 0.)) return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
-    MHY_CUDA(cudaMemcpy(c->rho, st->density, C * sizeof(double), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(c->p, st->pressure, C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpyAsync(c->rho, st->density, C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(c->p, st->pressure, C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   } else {
     // Environments from the volume fractions and the initial per-environment
     // state, as HydroStartInit sets them up on the host (MahycoModule.cc:48-127
@@ -311,18 +301,19 @@ int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
       }
     }
     const EnvState& ev = c->env;
-    MHY_CUDA(cudaMemcpy(ev.mask, mask.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(c->rho, rho.data(), C * sizeof(double), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(c->p, pg.data(), C * sizeof(double), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(ev.f, f.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(ev.x, x.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(ev.rho, r.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
-    MHY_CUDA(cudaMemcpy(ev.p, pk.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice));
+    MHY_CUDA(cudaMemcpyAsync(ev.mask, mask.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(c->rho, rho.data(), C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(c->p, pg.data(), C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(ev.f, f.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(ev.x, x.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(ev.rho, r.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(ev.p, pk.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   }
-  std::vector<double> soa(3 * N);
-  for (long long n = 0; n < N; ++n)
-    for (int a = 0; a < 3; ++a) soa[a * N + n] = st->velocity[3 * n + a];
-  MHY_CUDA(cudaMemcpy(c->v, soa.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice));
+  // interleaved velocity staged in ud[0] (unused until the first cycle), then planes
+  MHY_CUDA(cudaMemcpyAsync(c->ud[0], st->velocity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_soa3<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(N, c->ud[0], c->v);
+  MHY_CUDA(cudaGetLastError());
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
   c->state_set = true;
   return MHY_OK;
 }

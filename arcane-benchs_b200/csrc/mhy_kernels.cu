@@ -97,6 +97,73 @@ __global__ void k_init_state(Dims dm, double gamma, const double* __restrict__ v
   q[c] = 0.;
 }
 
+// ------------------------------------------------------------ set-up ----
+
+// xyz-interleaved (n x 3) -> three planes (3 x n).
+__global__ void k_soa3(long long n, const double* __restrict__ aos, double* __restrict__ soa) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  soa[i] = aos[3 * i]; soa[n + i] = aos[3 * i + 1]; soa[2 * n + i] = aos[3 * i + 2];
+}
+
+// Maximum node coordinate per axis, from -1 as PrepareFaceGroup starts it
+// (MahycoAnnexe.cc:189-199): per-block maxima, then one block over them.
+// The maximum does not depend on the order in which it is taken.
+__global__ void k_max3_partial(long long n, const double* __restrict__ x, double* __restrict__ part) {
+  __shared__ double sm[3][256];
+  double m[3] = {-1., -1., -1.};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    for (int a = 0; a < 3; ++a) m[a] = (m[a] < x[a * n + i]) ? x[a * n + i] : m[a];
+  for (int a = 0; a < 3; ++a) sm[a][threadIdx.x] = m[a];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int a = 0; a < 3; ++a) sm[a][threadIdx.x] = (sm[a][threadIdx.x] < sm[a][threadIdx.x + w]) ? sm[a][threadIdx.x + w] : sm[a][threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int a = 0; a < 3; ++a) part[3 * blockIdx.x + a] = sm[a][0];
+}
+
+// Boundary node groups by coordinate threshold over every face, PrepareFaceGroup
+// (MahycoAnnexe.cc:183-251): bit s of grp[n] when the node belongs to a face
+// lying on plane s (XMIN..ZMAX).  mx: the per-block maxima of k_max3_partial.
+__global__ void k_face_groups(Dims dm, const double* __restrict__ x0, const double* __restrict__ part, int nparts,
+                              double thr, unsigned* __restrict__ grp) {
+  const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= dm.F) return;
+  double mx[3] = {-1., -1., -1.};
+  for (int b = 0; b < nparts; ++b)
+    for (int a = 0; a < 3; ++a) mx[a] = (mx[a] < part[3 * b + a]) ? part[3 * b + a] : mx[a];
+  int d; long long t;
+  if (f < dm.Fx) { d = 0; t = f; } else if (f < dm.Fx + dm.Fy) { d = 1; t = f - dm.Fx; } else { d = 2; t = f - dm.Fx - dm.Fy; }
+  int i, j, k; dm.fdijk(d, t, i, j, k);
+  long long fn[4]; face_node_ids(dm, d, i, j, k, fn);
+  unsigned fl = 0x3f;
+  for (int a = 0; a < 4; ++a) {
+    const double x = x0[fn[a]], y = x0[dm.N + fn[a]], z = x0[2 * dm.N + fn[a]];
+    if (x > thr) fl &= ~(1u << MHY_XMIN);
+    if (y > thr) fl &= ~(1u << MHY_YMIN);
+    if (z > thr) fl &= ~(1u << MHY_ZMIN);
+    if (fabs(x - mx[0]) > thr) fl &= ~(1u << MHY_XMAX);
+    if (fabs(y - mx[1]) > thr) fl &= ~(1u << MHY_YMAX);
+    if (fabs(z - mx[2]) > thr) fl &= ~(1u << MHY_ZMAX);
+  }
+  if (fl)
+    for (int a = 0; a < 4; ++a) atomicOr(&grp[fn[a]], fl);
+}
+
+// bcmask bit b of a node: boundary condition b applies (its surface group holds the node).
+__global__ void k_bc_mask(long long n, const unsigned* __restrict__ grp, int nbc, const int* __restrict__ surf,
+                          uint16_t* __restrict__ mask) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned m = 0;
+  for (int b = 0; b < nbc; ++b)
+    if (grp[i] >> surf[b] & 1u) m |= 1u << b;
+  mask[i] = (uint16_t)m;
+}
+
 // FP64 -> FP32 copy (the initial corner vectors of the mixed form).
 __global__ void k_to_f32(long long n, const double* __restrict__ src, float* __restrict__ dst) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;

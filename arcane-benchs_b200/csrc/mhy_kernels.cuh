@@ -118,6 +118,10 @@ __global__ void k_init_state(Dims dm, double gamma, const double* vol, double* r
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
 __global__ void k_to_f32(long long n, const double* src, float* dst);
+__global__ void k_soa3(long long n, const double* aos, double* soa);
+__global__ void k_max3_partial(long long n, const double* x, double* part);
+__global__ void k_face_groups(Dims dm, const double* x0, const double* part, int nparts, double thr, unsigned* grp);
+__global__ void k_bc_mask(long long n, const unsigned* grp, int nbc, const int* surf, uint16_t* mask);
 __global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm, int linear);
 dim3 cell_grid(const Dims& dm, int& linear);
 __global__ void k_dt_finish(Scalars* S, Phys ph);
