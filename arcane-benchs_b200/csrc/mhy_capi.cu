@@ -131,6 +131,7 @@ void mhy_options_default(mhy_options* o) {
   o->nb_env = 1;
   o->adiabatic_cst[0] = 1.4;
   o->precision = 0;
+  for (int k = 0; k < MHY_MAX_ENV; ++k) o->limit_tension[k] = 0.01;   // StiffenedGasEOS.axl:104
 }
 
 int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mhy_ctx** out) {
@@ -149,8 +150,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   }
   if (opt->nb_env < 1 || opt->nb_env > kMaxEnvDevice)
     return fail(MHY_ERR_UNSUPPORTED, "nb_env must be 1.." + std::to_string(kMaxEnvDevice) + " on the device");
-  for (int k = 0; k < opt->nb_env; ++k)
+  for (int k = 0; k < opt->nb_env; ++k) {
     if (!(opt->adiabatic_cst[k] > 1.)) return fail(MHY_ERR_ARG, "adiabatic-cst must be > 1");
+    if (opt->eos[k] < 0 || opt->eos[k] > 1) return fail(MHY_ERR_ARG, "eos must be 0 (PerfectGas) or 1 (StiffenedGas)");
+  }
   if (opt->ordre_projection < 1 || opt->ordre_projection > 2)
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
@@ -178,7 +181,13 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   Phys& ph = c->ph;
   ph.gamma = opt->adiabatic_cst[0];
   c->K = opt->nb_env;
-  for (int k = 0; k < c->K; ++k) c->env.gamma[k] = opt->adiabatic_cst[k];
+  for (int k = 0; k < c->K; ++k) {
+    c->env.gamma[k] = opt->adiabatic_cst[k];
+    c->env.eos[k] = opt->eos[k];
+    c->env.pinf[k] = opt->limit_tension[k];
+  }
+  ph.eos = opt->eos[0];
+  ph.pinf = opt->limit_tension[0];
   ph.threshold = opt->threshold; ph.cfl = opt->cfl;
   ph.deltat_min = opt->deltat_min; ph.deltat_max = opt->deltat_max; ph.final_time = opt->final_time;
   ph.lc_mode = opt->longueur_caracteristique; ph.pseudo_centree = opt->pseudo_centree;
@@ -354,7 +363,7 @@ int mhy_hydro_start_init(mhy_ctx* c) {
   cudaStream_t s = c->stream;
   const int rc = init_geometry(c);
   if (rc != MHY_OK) return rc;
-  if (c->K == 1) k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph.gamma, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
+  if (c->K == 1) k_init_state<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->ph, c->Ve, c->rho, c->p, c->e, c->cs, c->mass, c->q);
   else launch_init_env(c->args(), s);
   k_node_mass<<<blocks(dm.N), kThreads, 0, s>>>(dm, c->mass, c->nm);
   if (c->cqs32) k_to_f32<<<blocks(24 * dm.C), kThreads, 0, s>>>(24 * dm.C, c->cqs, c->cqs32);

@@ -90,6 +90,20 @@ template <> struct Ar<float> {
   __device__ static __forceinline__ float quo(float x, float y) { return __fdividef(x, y); }
 };
 
+// Equations of state.  After the remap, p and c from rho and e:
+// PerfectGas (eos/perfectgas/PerfectGasEOSService.cc:92-106) and StiffenedGas
+// (eos/stiffenedgas/StiffenedGasEOSService.cc:29-44, pinf = limit-tension).
+__device__ __forceinline__ void eos_pc(int kind, double g, double pinf, double r, double e, double& p, double& c) {
+  if (kind == 1) { p = ((g - 1.) * r * e) - (g * pinf); c = sqrt((g / r) * (p + pinf)); }
+  else { p = (g - 1.) * r * e; c = sqrt(g * p / r); }
+}
+// initEOS: e and c from rho and p (PerfectGasEOSService.cc:20-32,
+// StiffenedGasEOSService.cc:10-24).
+__device__ __forceinline__ void eos_init(int kind, double g, double pinf, double r, double p, double& e, double& c) {
+  if (kind == 1) { e = (p + (g * pinf)) / ((g - 1.) * r); c = sqrt((g / r) * (p + pinf)); }
+  else { e = p / ((g - 1.) * r); c = sqrt(g * p / r); }
+}
+
 // compute_eint, mahyco/src/MahycoModule.cc:1630-1654; ir = 1.0/r and irn = 1.0/rn given.
 __device__ __forceinline__ double compute_eint(bool pc, double g, double qn, double q, double ir, double irn,
                                                double r, double p, double en) {

@@ -83,16 +83,17 @@ __global__ void k_init_outer_normals(Dims dm, const double* __restrict__ xc0, co
   }
 }
 
-// Initial thermodynamic state of a single-environment mesh: PerfectGas
-// initEOS (E:20-32) and ComputeCellMass (MahycoModule.cc:199-225).
-__global__ void k_init_state(Dims dm, double gamma, const double* __restrict__ vol, double* __restrict__ rho,
+// Initial thermodynamic state of a single-environment mesh: initEOS
+// (PerfectGas E:20-32 or StiffenedGas) and ComputeCellMass (MahycoModule.cc:199-225).
+__global__ void k_init_state(Dims dm, Phys ph, const double* __restrict__ vol, double* __restrict__ rho,
                              const double* __restrict__ pres, double* __restrict__ e, double* __restrict__ cs,
                              double* __restrict__ mass, double* __restrict__ q) {
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= dm.C) return;
-  double p = pres[c], r = rho[c];
-  e[c] = p / ((gamma - 1.) * r);
-  cs[c] = sqrt(gamma * p / r);
+  double p = pres[c], r = rho[c], ec, cc;
+  eos_init(ph.eos, ph.gamma, ph.pinf, r, p, ec, cc);
+  e[c] = ec;
+  cs[c] = cc;
   mass[c] = r * vol[c];
   q[c] = 0.;
 }

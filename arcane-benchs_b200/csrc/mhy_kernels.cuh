@@ -25,6 +25,8 @@ struct Phys {
   double gamma, threshold, cfl, deltat_min, deltat_max, final_time;
   int lc_mode, pseudo_centree, ordre_projection, limiteur_id;
   int precision;        // 0: FP64; 1: mixed (FP32 evaluation of the remap, FP64 state and sums)
+  int eos;              // environment 0: 0 PerfectGas, 1 StiffenedGas
+  double pinf;          // its limit-tension
 };
 
 struct BCTable {
@@ -62,6 +64,8 @@ struct EnvState {
                                       // pseudo-viscosity, mass
   double *fg, *xg;      // [C]
   double gamma[MHY_MAX_ENV];
+  int eos[MHY_MAX_ENV];           // 0 PerfectGas, 1 StiffenedGas
+  double pinf[MHY_MAX_ENV];       // StiffenedGas limit-tension
 };
 
 struct CycleArgs {
@@ -114,7 +118,7 @@ constexpr int kKernelsPerCycleBatch = 10;
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);
 __global__ void k_init_faces(Dims dm, const double* x0, double* n0, double* xf0);
 __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* xf0, double* ofn);
-__global__ void k_init_state(Dims dm, double gamma, const double* vol, double* rho, const double* pres, double* e,
+__global__ void k_init_state(Dims dm, Phys ph, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
 __global__ void k_to_f32(long long n, const double* src, float* dst);

@@ -74,14 +74,14 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
   const double pseudo = 0. + fvol * pv;
   double r = de;
   if (r < 0. || energie < 0.) { energie = 0.; r = 0.; }
-  const double g = ph.gamma;
-  const double pr = (g - 1.) * r * energie;
+  double pr, cc;
+  eos_pc(ph.eos, ph.gamma, ph.pinf, r, energie, pr, cc);
   out[0] = r;
   out[1] = energie;
   out[2] = pseudo;
   out[3] = mf * cm;
   out[4] = pr;
-  out[5] = sqrt(g * pr / r);
+  out[5] = cc;
 }
 
 // Phi = U / sum of the environment volumes = U / U0 for one environment

@@ -374,9 +374,7 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
   for (int k = 0; k < K; ++k) {
     pk[k] = ck[k] = 0.;
     if (!(mask >> k & 1)) continue;
-    const double g = env.gamma[k];
-    pk[k] = (g - 1.) * r[k] * e[k];
-    ck[k] = sqrt(g * pk[k] / r[k]);
+    eos_pc(env.eos[k], env.gamma[k], env.pinf[k], r[k], e[k], pk[k], ck[k]);
   }
   if (pure) {
     st.rho[c] = r[ke]; st.e[c] = e[ke]; st.q[c] = q[ke]; st.mass[c] = m[ke];
@@ -400,7 +398,7 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
 }
 
 // Initial thermodynamic state of a K-environment mesh, after the initial
-// geometry: PerfectGas initEOS per environment (E:20-32), the mixed-cell
+// geometry: initEOS per environment (PerfectGas E:20-32 or StiffenedGas), the mixed-cell
 // energy and sound speed (MahycoModule.cc:116-127) and ComputeCellMass
 // (MahycoModule.cc:199-225).  Fractions, partial densities and pressures,
 // mass fractions and the global density and pressure come from the host.
@@ -413,10 +411,12 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
   const double V = st.Ve[c];
   st.q[c] = 0.;
   if (__popc(mask) == 1) {
-    const double g = env.gamma[__ffs(mask) - 1];
-    const double p = st.p[c], r = st.rho[c];
-    st.e[c] = p / ((g - 1.) * r);
-    st.cs[c] = sqrt(g * p / r);
+    const int ke = __ffs(mask) - 1;
+    double ec, cc;
+    eos_init(env.eos[ke], env.gamma[ke], env.pinf[ke], st.rho[c], st.p[c], ec, cc);
+    st.e[c] = ec;
+    st.cs[c] = cc;
+    const double r = st.rho[c];
     st.mass[c] = r * V;
     env.fg[c] = 1.; env.xg[c] = 1.;
     return;
@@ -426,10 +426,8 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
   for (int k = 0; k < K; ++k) {
     if (!(mask >> k & 1)) continue;
     const int o = k * C + c;
-    const double g = env.gamma[k];
-    const double p = env.p[o], r = env.rho[o];
-    const double ek = p / ((g - 1.) * r);
-    const double ck = sqrt(g * p / r);
+    double ek, ck;
+    eos_init(env.eos[k], env.gamma[k], env.pinf[k], env.rho[o], env.p[o], ek, ck);
     env.e[o] = ek; env.cs[o] = ck; env.q[o] = 0.;
     eg += ek * env.x[o];
     cg = smax(ck, cg);

@@ -66,6 +66,8 @@ class Options:
     projection_limiteur_id: int = 0         # 0 minmod, 1 superBee, 2 vanLeer
     boundary_conditions: tuple = WALLS
     precision: int = 0                      # device only: 0 FP64, 1 mixed (FP32 remap evaluation)
+    eos: tuple = ()                         # per environment: 0 PerfectGas (default), 1 StiffenedGas
+    limit_tension: tuple = ()               # per environment: StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
 
 
 @dataclasses.dataclass

@@ -76,6 +76,9 @@ typedef struct mhy_options {
                                         1: mixed: the remap's Phi, gradients, limiters, face values and
                                         flux terms in FP32; state, coordinates, volumes, conserved sums
                                         and the dt reduction in FP64 */
+  int32_t eos[MHY_MAX_ENV];           /* per environment: 0 PerfectGas (eos/perfectgas), 1 StiffenedGas
+                                        (eos/stiffenedgas/StiffenedGasEOSService.cc) */
+  double limit_tension[MHY_MAX_ENV]; /* StiffenedGas limit-tension (StiffenedGasEOS.axl:104, default 0.01) */
   int32_t reserved[7];
 } mhy_options;
 

@@ -92,6 +92,8 @@ struct Oracle {
   int lc_mode;          // 0 racine-cubique-volume, 1 faces-opposees
   int pseudo_centree, ordre_projection, limiteur_id, use_project_pow;
   std::vector<double> gamma;
+  std::vector<int> eos;             // per environment: 0 PerfectGas, 1 StiffenedGas
+  std::vector<double> pinf;         // StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
   struct BC { int surface, type; double value; std::vector<int> nodes; };
   std::vector<BC> bcs;
 
@@ -315,14 +317,20 @@ struct Oracle {
 
     computeGeometricValues();                                           // M:96
     prepareFaceGroup();                                                 // M:99-100
-    // initEOS per environment, E:20-32
+    // initEOS per environment: PerfectGas E:20-32, StiffenedGas
+    // (eos/stiffenedgas/StiffenedGasEOSService.cc:10-24)
     for (int k = 0; k < K; ++k) {
-      const double g = gamma[k];
+      const double g = gamma[k], pi = pinf[k];
       for (long c = 0; c < C; ++c) {
         if (!(env_mask[c] >> k & 1)) continue;
         double p = mv(pressure, k, c), r = mv(density, k, c);
-        mv(internal_energy, k, c) = p / ((g - 1.) * r);
-        mv(sound_speed, k, c) = std::sqrt(g * p / r);
+        if (eos[k] == 1) {
+          mv(internal_energy, k, c) = (p + (g * pi)) / ((g - 1.) * r);
+          mv(sound_speed, k, c) = std::sqrt((g / r) * (p + pi));
+        } else {
+          mv(internal_energy, k, c) = p / ((g - 1.) * r);
+          mv(sound_speed, k, c) = std::sqrt(g * p / r);
+        }
       }
     }
     // mixed-cell averages, M:116-127
@@ -989,16 +997,25 @@ struct Oracle {
   std::vector<uint32_t> prev_mask_scratch;
   bool env_mask_prev_bit(long c, int k) const { return !prev_mask_scratch.empty() && (prev_mask_scratch[c] >> k & 1); }
 
-  void applyEOS() {  // E:50-137 for every environment
+  // applyEOS for every environment: PerfectGas E:50-137, StiffenedGas
+  // (eos/stiffenedgas/StiffenedGasEOSService.cc:29-44)
+  void applyEOS() {
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < C; ++c) {
       for (int k = 0; k < K; ++k) {
         if (!(env_mask[c] >> k & 1)) continue;
         const double g = gamma[k];
         double r = mv(density, k, c), e = mv(internal_energy, k, c);
-        double p = (g - 1.) * r * e;
-        mv(pressure, k, c) = p;
-        mv(sound_speed, k, c) = std::sqrt(g * p / r);
+        if (eos[k] == 1) {
+          const double pi = pinf[k];
+          double p = ((g - 1.) * r * e) - (g * pi);
+          mv(pressure, k, c) = p;
+          mv(sound_speed, k, c) = std::sqrt((g / r) * (p + pi));
+        } else {
+          double p = (g - 1.) * r * e;
+          mv(pressure, k, c) = p;
+          mv(sound_speed, k, c) = std::sqrt(g * p / r);
+        }
         mv(dpde, k, c) = (g - 1.) * r;
       }
     }
@@ -1104,7 +1121,7 @@ struct orc_bc { int surface; int type; double value; };
 void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, const double* gammas,
                  double cfl, double threshold, double deltat_init, double deltat_min, double deltat_max,
                  double final_time, int lc_mode, int pseudo_centree, int ordre_projection, int limiteur_id,
-                 int nbc, const orc_bc* bcs, int use_project_pow) {
+                 int nbc, const orc_bc* bcs, int use_project_pow, const int* eos, const double* pinf) {
   Oracle* o = new Oracle();
   o->nx = nx; o->ny = ny; o->nz = nz; o->NX = nx + 1; o->NY = ny + 1; o->NZ = nz + 1;
   o->C = (long)nx * ny * nz; o->N = (long)o->NX * o->NY * o->NZ;
@@ -1115,6 +1132,12 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
   o->deltat_max = deltat_max; o->final_time = final_time; o->lc_mode = lc_mode; o->pseudo_centree = pseudo_centree;
   o->ordre_projection = ordre_projection; o->limiteur_id = limiteur_id; o->use_project_pow = use_project_pow;
   o->gamma.assign(gammas, gammas + nenv);
+  o->eos.assign(nenv, 0);
+  o->pinf.assign(nenv, 0.);
+  for (int k = 0; k < nenv; ++k) {
+    if (eos) o->eos[k] = eos[k];
+    if (pinf) o->pinf[k] = pinf[k];
+  }
   for (int b = 0; b < nbc; ++b) o->bcs.push_back(Oracle::BC{bcs[b].surface, bcs[b].type, bcs[b].value, {}});
   const long C = o->C, N = o->N, F = o->F; const int K = nenv, nv = o->nvars;
   o->node_coord.resize(N); o->node_coord_0.resize(N); o->velocity.assign(N, r3(0, 0, 0));

@@ -43,7 +43,7 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         L.orc_create.restype = ctypes.c_void_p
         L.orc_create.argtypes = [ctypes.c_int] * 3 + [dp, ctypes.c_int, dp] + [ctypes.c_double] * 6 + \
-            [ctypes.c_int] * 5 + [ctypes.POINTER(_BC), ctypes.c_int]
+            [ctypes.c_int] * 5 + [ctypes.POINTER(_BC), ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp]
         L.orc_init.argtypes = [ctypes.c_void_p, dp, dp, dp, dp]
         L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
@@ -82,12 +82,19 @@ class Oracle:
         coords = np.ascontiguousarray(case.coords, dtype=np.float64)
         gam = np.ascontiguousarray(case.gamma, dtype=np.float64)
         bcs = (_BC * max(1, len(o.boundary_conditions)))(*[_BC(s, t, v) for s, t, v in o.boundary_conditions])
-        self._keep = (coords, gam, bcs)
+        eos = np.zeros(case.nenv, dtype=np.int32)
+        pinf = np.full(case.nenv, 0.01)                 # StiffenedGasEOS.axl:104 default
+        for k, kind in enumerate(getattr(o, "eos", ()) or ()):
+            eos[k] = kind
+        for k, v in enumerate(getattr(o, "limit_tension", ()) or ()):
+            pinf[k] = v
+        self._keep = (coords, gam, bcs, eos, pinf)
         self.h = L.orc_create(case.nx, case.ny, case.nz, _dp(coords), case.nenv, _dp(gam),
                               o.cfl, o.threshold, o.deltat_init, o.deltat_min, o.deltat_max, o.final_time,
                               o.longueur_caracteristique, o.pseudo_centree, o.ordre_projection,
                               o.projection_limiteur_id, len(o.boundary_conditions), bcs,
-                              1 if pow_mode == "project" else 0)
+                              1 if pow_mode == "project" else 0,
+                              eos.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(pinf))
         fv = np.ascontiguousarray(case.fracvol, dtype=np.float64)
         de = np.ascontiguousarray(case.density, dtype=np.float64)
         pr = np.ascontiguousarray(case.pressure, dtype=np.float64)

@@ -1,10 +1,15 @@
-"""Exact solution of the Riemann problem for one ideal gas (test support).
+"""Exact solution of the Riemann problem for one ideal or stiffened gas
+(test support).
 
 Written from the standard relations of gas dynamics (e.g. E. F. Toro,
 "Riemann Solvers and Numerical Methods for Fluid Dynamics", ch. 4): the star
 pressure solves f_L(p) + f_R(p) + u_R - u_L = 0, with f_K the shock
 (Rankine-Hugoniot) or rarefaction (isentropic) branch; the solution is then
-sampled on x/t."""
+sampled on x/t.  A stiffened gas (p = (g-1) rho e - g pinf) has the
+Rankine-Hugoniot relations and isentropes of an ideal gas in the shifted
+pressure p + pinf (the pinf terms of the Hugoniot energy jump cancel), and
+sound speed sqrt(g (p + pinf) / rho): its solution is the ideal-gas one in
+p + pinf."""
 import math
 
 
@@ -18,7 +23,10 @@ def _f(p, rho, pk, c, g):
     return 2.0 * c / (g - 1.0) * (r ** ((g - 1.0) / (2.0 * g)) - 1.0), 1.0 / (rho * c) * r ** (-(g + 1.0) / (2.0 * g))
 
 
-def star_state(left, right, g):
+def star_state(left, right, g, pinf=0.0):
+    if pinf:
+        ps, us = star_state(_shift(left, pinf), _shift(right, pinf), g)
+        return ps - pinf, us
     (rl, ul, pl), (rr, ur, pr) = left, right
     cl, cr = math.sqrt(g * pl / rl), math.sqrt(g * pr / rr)
     p = max(1e-12, 0.5 * (pl + pr))
@@ -36,8 +44,15 @@ def star_state(left, right, g):
     return p, 0.5 * (ul + ur) + 0.5 * (fr - fl)
 
 
-def sample(left, right, g, xi):
+def _shift(state, pinf):
+    return state[0], state[1], state[2] + pinf
+
+
+def sample(left, right, g, xi, pinf=0.0):
     """(rho, u, p) at x/t = xi."""
+    if pinf:
+        r, u, p = sample(_shift(left, pinf), _shift(right, pinf), g, xi)
+        return r, u, p - pinf
     (rl, ul, pl), (rr, ur, pr) = left, right
     cl, cr = math.sqrt(g * pl / rl), math.sqrt(g * pr / rr)
     ps, us = star_state(left, right, g)
