@@ -154,6 +154,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     if (!(opt->adiabatic_cst[k] > 1.)) return fail(MHY_ERR_ARG, "adiabatic-cst must be > 1");
     if (opt->eos[k] < 0 || opt->eos[k] > 1) return fail(MHY_ERR_ARG, "eos must be 0 (PerfectGas) or 1 (StiffenedGas)");
   }
+  if (opt->with_newton != 0 && opt->with_newton != 1) return fail(MHY_ERR_ARG, "with_newton must be 0 or 1");
   if (opt->ordre_projection < 1 || opt->ordre_projection > 2)
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
@@ -186,6 +187,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     c->env.eos[k] = opt->eos[k];
     c->env.pinf[k] = opt->limit_tension[k];
   }
+  ph.with_newton = opt->with_newton;
   ph.eos = opt->eos[0];
   ph.pinf = opt->limit_tension[0];
   ph.threshold = opt->threshold; ph.cfl = opt->cfl;

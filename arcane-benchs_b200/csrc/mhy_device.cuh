@@ -115,6 +115,42 @@ __device__ __forceinline__ double compute_eint(bool pc, double g, double qn, dou
   return numer / denom;
 }
 
+// updateEnergyAndPressurebyNewton without schema-csts, MahycoModule.cc:1482-1535:
+// Newton iterations on fvnr(e) = e - en + 0.5 (p + pn + 2 q*) (1/r - 1/rn),
+// derivative 1 + 0.5 dpde (1/r - 1/rn) (MahycoModule.h:420-429), p and dpde
+// from the environment's EOS at the current e and the new density
+// (applyOneCellEOS); the loop test takes fvnr at the updated e with those p,
+// dpde.  The reference makes its first test before any EOS call (p and dpde
+// not yet set); here the first iteration always runs.  Only e is kept: p and
+// c are recomputed by the EOS after the remap.
+__device__ __forceinline__ double newton_eint(bool pc, int kind, double g, double pinf, double epsilon, double qn,
+                                              double q, double ir, double irn, double r, double pn, double en) {
+  double pseudo = 0.;
+  if (pc && ((qn + q) * (ir - irn) < 0.)) pseudo = 0.5 * (q + qn);
+  if (!pc && (q * (ir - irn) < 0.)) pseudo = q;
+  const double itermax = 50;
+  double e = en, p, dpde;
+  int i = 0;
+  do {
+    if (kind == 1) p = ((g - 1.) * r * e) - (g * pinf);
+    else p = (g - 1.) * r * e;
+    dpde = (g - 1.) * r;
+    const double enew = e - (e - en + 0.5 * (p + pn + 2. * pseudo) * (ir - irn)) / (1. + 0.5 * dpde * (ir - irn));
+    e = enew;
+    i++;
+  } while (i < itermax && fabs(e - en + 0.5 * (p + pn + 2. * pseudo) * (ir - irn)) >= epsilon);
+  return e;
+}
+
+// The Lagrange energy update of one environment cell: the closed form of
+// updateEnergyAndPressureforGP, or the Newton iterations when with-newton is set.
+__device__ __forceinline__ double energy_update(bool newton, bool pc, int kind, double g, double pinf, double epsilon,
+                                                double qn, double q, double ir, double irn, double r, double p,
+                                                double en) {
+  if (newton) return newton_eint(pc, kind, g, pinf, epsilon, qn, q, ir, irn, r, p, en);
+  return compute_eint(pc, g, qn, q, ir, irn, r, p, en);
+}
+
 // Corner vectors (CQS) of a hexahedron, mahyco/src/MahycoModule.cc:2195-2258,
 // face centres from :1080-1087.  Node order SN_trigo.
 __device__ __forceinline__ void face_centres(const D3 x[8], D3 fc[6]) {

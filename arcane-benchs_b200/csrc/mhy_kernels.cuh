@@ -27,6 +27,7 @@ struct Phys {
   int precision;        // 0: FP64; 1: mixed (FP32 evaluation of the remap, FP64 state and sums)
   int eos;              // environment 0: 0 PerfectGas, 1 StiffenedGas
   double pinf;          // its limit-tension
+  int with_newton;      // Lagrange energy update by Newton iterations
 };
 
 struct BCTable {

@@ -198,7 +198,8 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
     const double g = env.gamma[ke];
     double qn = 0.;
     if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-    const double en = compute_eint(pc, g, q[c], qn, ind, irn, nd, p[c], e[c]);
+    const double en = energy_update(ph.with_newton != 0, pc, env.eos[ke], g, env.pinf[ke], ph.threshold, q[c], qn, ind,
+                                    irn, nd, p[c], e[c]);
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k == ke) { u[k] = V; u[K + k] = V * nd; u[2 * K + k] = V * nd * en; }
@@ -216,7 +217,8 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
       const double g = env.gamma[k];
       double qk = 0.;
       if (du < 0.0) qk = 1. / tauk * (-0.5 * Lc * csc * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-      const double ek = compute_eint(pc, g, env.q[o], qk, irk, irnk, rk, env.p[o], env.e[o]);
+      const double ek = energy_update(ph.with_newton != 0, pc, env.eos[k], g, env.pinf[k], ph.threshold, env.q[o], qk,
+                                      irk, irnk, rk, env.p[o], env.e[o]);
       u[k] = vk;
       u[K + k] = vk * rk;
       u[2 * K + k] = vk * rk * ek;
@@ -306,7 +308,8 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     double qn = 0.;
     const double g = ph.gamma;
     if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-    const double en = compute_eint(ph.pseudo_centree != 0, g, q[c], qn, ind, irn, nd, p[c], e[c]);
+    const double en = energy_update(ph.with_newton != 0, ph.pseudo_centree != 0, ph.eos, g, ph.pinf, ph.threshold, q[c],
+                                    qn, ind, irn, nd, p[c], e[c]);
     U[c] = V;
     U[C + c] = V * nd;
     U[2 * C + c] = V * nd * en;

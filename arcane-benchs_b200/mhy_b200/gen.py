@@ -68,6 +68,7 @@ class Options:
     precision: int = 0                      # device only: 0 FP64, 1 mixed (FP32 remap evaluation)
     eos: tuple = ()                         # per environment: 0 PerfectGas (default), 1 StiffenedGas
     limit_tension: tuple = ()               # per environment: StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
+    with_newton: int = 0                    # energy update by Newton iterations (Mahyco.axl:308)
 
 
 @dataclasses.dataclass

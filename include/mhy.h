@@ -79,7 +79,9 @@ typedef struct mhy_options {
   int32_t eos[MHY_MAX_ENV];           /* per environment: 0 PerfectGas (eos/perfectgas), 1 StiffenedGas
                                         (eos/stiffenedgas/StiffenedGasEOSService.cc) */
   double limit_tension[MHY_MAX_ENV]; /* StiffenedGas limit-tension (StiffenedGasEOS.axl:104, default 0.01) */
-  int32_t reserved[7];
+  int32_t with_newton;               /* 0; 1: Lagrange energy update by Newton iterations on the EOS
+                                        (Mahyco.axl:308, MahycoModule.cc:1482-1535; schema-csts false) */
+  int32_t reserved[6];
 } mhy_options;
 
 /* Structured hexahedral mesh: (nx+1)(ny+1)(nz+1) nodes, node (i,j,k) at

@@ -91,6 +91,7 @@ struct Oracle {
   double cfl, threshold, deltat_init, deltat_min, deltat_max, final_time;
   int lc_mode;          // 0 racine-cubique-volume, 1 faces-opposees
   int pseudo_centree, ordre_projection, limiteur_id, use_project_pow;
+  int with_newton = 0;              // Mahyco.axl:308 with-newton (schema-csts false)
   std::vector<double> gamma;
   std::vector<int> eos;             // per environment: 0 PerfectGas, 1 StiffenedGas
   std::vector<double> pinf;         // StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
@@ -542,19 +543,52 @@ struct Oracle {
     return numer / denom;
   }
 
-  void updateEnergyAndPressure() {  // M:1439-1478 -> updateEnergyAndPressureforGP M:1659-1770 (#else)
+  // updateEnergyAndPressurebyNewton without schema-csts (M:1482-1535):
+  // Newton iterations on fvnr(e) = e - en + 0.5 (p + pn + 2 q*) (1/rn1 - 1/rn)
+  // with derivative 1 + 0.5 dpde (1/rn1 - 1/rn) (MahycoModule.h:420-429); each
+  // iteration sets p and dpde by applyOneCellEOS at the current e and the new
+  // density (PerfectGasEOSService.cc:38-45, StiffenedGasEOSService.cc:47-58),
+  // and the loop test evaluates fvnr at the updated e with those p, dpde.  The
+  // reference makes its first test before any EOS call, with p and dpde not yet
+  // set; this restatement always runs the first iteration.  Only e is kept: p
+  // and c are recomputed by the EOS after the remap.
+  double newton_eint(int k, double qn, double q, double rn, double r, double pn, double en) const {
     const bool pc = pseudo_centree != 0;
+    double pseudo = 0.;
+    if (pc && ((qn + q) * (1.0 / r - 1.0 / rn) < 0.)) pseudo = 0.5 * (q + qn);
+    if (!pc && (q * (1.0 / r - 1.0 / rn) < 0.)) pseudo = q;
+    const double g = gamma[k], epsilon = threshold, itermax = 50;
+    auto fvnr = [&](double e, double p) { return e - en + 0.5 * (p + pn + 2. * pseudo) * (1. / r - 1. / rn); };
+    double e = en, p, dpde;
+    int i = 0;
+    do {
+      if (eos[k] == 1) p = ((g - 1.) * r * e) - (g * pinf[k]);
+      else p = (g - 1.) * r * e;
+      dpde = (g - 1.) * r;
+      const double enew = e - fvnr(e, p) / (1. + 0.5 * dpde * (1. / r - 1. / rn));
+      e = enew;
+      i++;
+    } while (i < itermax && std::fabs(fvnr(e, p)) >= epsilon);
+    return e;
+  }
+
+  double energy_update(int k, double qn, double q, double rn, double r, double p, double en) const {
+    if (with_newton) return newton_eint(k, qn, q, rn, r, p, en);
+    return compute_eint(pseudo_centree != 0, gamma[k], qn, q, rn, r, p, en);
+  }
+
+  void updateEnergyAndPressure() {  // M:1439-1478 -> updateEnergyAndPressureforGP M:1659-1770 (#else)
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < C; ++c) {
       internal_energy.g[c] = 0.;
       int e = env_id[c];
       if (e >= 0) {
-        internal_energy.g[c] = compute_eint(pc, gamma[e], pseudo_viscosity_n.g[c], pseudo_viscosity.g[c],
-                                            density_n.g[c], density.g[c], pressure.g[c], internal_energy_n.g[c]);
+        internal_energy.g[c] = energy_update(e, pseudo_viscosity_n.g[c], pseudo_viscosity.g[c],
+                                             density_n.g[c], density.g[c], pressure.g[c], internal_energy_n.g[c]);
       } else {
         for (int k = 0; k < K; ++k) if (env_mask[c] >> k & 1) {
-          double ek = compute_eint(pc, gamma[k], pseudo_viscosity_n.p[k][c], pseudo_viscosity.p[k][c],
-                                   density_n.p[k][c], density.p[k][c], pressure.p[k][c], internal_energy_n.p[k][c]);
+          double ek = energy_update(k, pseudo_viscosity_n.p[k][c], pseudo_viscosity.p[k][c],
+                                    density_n.p[k][c], density.p[k][c], pressure.p[k][c], internal_energy_n.p[k][c]);
           internal_energy.p[k][c] = ek;
           internal_energy.g[c] += mass_fraction.p[k][c] * ek;
         }
@@ -1121,7 +1155,8 @@ struct orc_bc { int surface; int type; double value; };
 void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, const double* gammas,
                  double cfl, double threshold, double deltat_init, double deltat_min, double deltat_max,
                  double final_time, int lc_mode, int pseudo_centree, int ordre_projection, int limiteur_id,
-                 int nbc, const orc_bc* bcs, int use_project_pow, const int* eos, const double* pinf) {
+                 int nbc, const orc_bc* bcs, int use_project_pow, const int* eos, const double* pinf,
+                 int with_newton) {
   Oracle* o = new Oracle();
   o->nx = nx; o->ny = ny; o->nz = nz; o->NX = nx + 1; o->NY = ny + 1; o->NZ = nz + 1;
   o->C = (long)nx * ny * nz; o->N = (long)o->NX * o->NY * o->NZ;
@@ -1131,6 +1166,7 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
   o->cfl = cfl; o->threshold = threshold; o->deltat_init = deltat_init; o->deltat_min = deltat_min;
   o->deltat_max = deltat_max; o->final_time = final_time; o->lc_mode = lc_mode; o->pseudo_centree = pseudo_centree;
   o->ordre_projection = ordre_projection; o->limiteur_id = limiteur_id; o->use_project_pow = use_project_pow;
+  o->with_newton = with_newton;
   o->gamma.assign(gammas, gammas + nenv);
   o->eos.assign(nenv, 0);
   o->pinf.assign(nenv, 0.);

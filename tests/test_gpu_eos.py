@@ -3,7 +3,8 @@
 ((g-1) rho), p = (g-1) rho e - g pinf, c = sqrt(g/rho (p + pinf))) against
 the oracle, bit for bit: one environment, two and three environments with
 stiffened and perfect gases side by side, the batched form with a different
-EOS per instance, and the mixed-precision form within its tolerance."""
+EOS per instance, the Newton energy update (with-newton), and the
+mixed-precision form within its tolerance."""
 import numpy as np
 import pytest
 
@@ -86,6 +87,22 @@ def test_batch_per_instance_eos_matches_single_contexts():
         for f in ("density", "internal_energy", "pressure", "velocity", "sound_speed"):
             assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
         assert b.dt(i) == g.dt()
+
+
+@pytest.mark.parametrize("deck", ["sod", "sod_stiffened", "sedov", "two_material"])
+def test_newton_energy_update_bitwise(deck):
+    """with-newton (MahycoModule.cc:1482-1535) on the device, bit for bit."""
+    if deck == "sod":
+        case = gen.sod(cycles=150, options=gen.Options(with_newton=1))
+    elif deck == "sod_stiffened":
+        case = gen.sod(cycles=150, options=gen.Options(with_newton=1, eos=(1,), limit_tension=(0.5,)))
+    elif deck == "sedov":
+        case = gen.sedov(n=20, cycles=60, options=gen.Options(with_newton=1))
+    else:
+        case = gen.two_material(32, 16, 16, cycles=80,
+                                options=gen.Options(with_newton=1, eos=(1, 0), limit_tension=(0.3, 0.0)))
+    o, g, dto, dtg = run_both(case, case.cycles, chunk=case.cycles // 4)
+    assert_bitwise(o, g, dto, dtg, case.nenv)
 
 
 @pytest.mark.parametrize("K", [1, 2])
