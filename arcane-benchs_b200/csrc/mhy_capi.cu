@@ -227,6 +227,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
+  static_assert(6 * kTotalsBlocks + 3 <= 1024, "set-up scratch holds the totals partials");
   if (rc == MHY_OK) rc = c->alloc(&c->setup, 1024);
   if (rc == MHY_OK) rc = c->commit();
   if (rc != MHY_OK) { mhy_destroy(c); return rc; }
@@ -636,6 +637,12 @@ int mhy_batch_get_status(mhy_batch* b, int i, uint32_t* flags) {
   return mhy_get_status(b->inst[i], flags);
 }
 
+int mhy_batch_get_totals(mhy_batch* b, int i, double* out) {
+  if (!b || i < 0 || i >= (int)b->inst.size()) return fail(MHY_ERR_ARG, "bad batch or instance index");
+  MHY_CUDA(cudaStreamSynchronize(b->stream));
+  return mhy_get_totals(b->inst[i], out);
+}
+
 int mhy_batch_size(mhy_batch* b) { return b ? (int)b->inst.size() : 0; }
 int mhy_batch_kernels_per_cycle(mhy_batch* b) { return b ? kKernelsPerCycleBatch : 0; }
 void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
@@ -913,6 +920,19 @@ int mhy_get_sizes(mhy_ctx* c, int64_t* ncells, int64_t* nnodes, int64_t* nfaces)
   if (ncells) *ncells = c->dm.C;
   if (nnodes) *nnodes = c->dm.N;
   if (nfaces) *nfaces = c->dm.F;
+  return MHY_OK;
+}
+
+int mhy_get_totals(mhy_ctx* c, double* out) {
+  if (!c || !out) return fail(MHY_ERR_ARG, "null argument");
+  if (!c->initialized) return fail(MHY_ERR_ORDER, "mhy_hydro_start_init has not run");
+  double* part = c->setup;                       // 6 x kTotalsBlocks partials, then the 3 totals
+  double* res = c->setup + 6 * kTotalsBlocks;
+  k_totals_partial<<<kTotalsBlocks, kTotalsThreads, 0, c->stream>>>(c->dm, c->mass, c->e, c->nm, c->v, part);
+  k_totals_finish<<<1, 1, 0, c->stream>>>(part, kTotalsBlocks, res);
+  MHY_CUDA(cudaGetLastError());
+  MHY_CUDA(cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
   return MHY_OK;
 }
 

@@ -186,6 +186,65 @@ __global__ void k_node_mass(Dims dm, const double* __restrict__ mass, double* __
   nm[n] = .125 * s;
 }
 
+// ------------------------------------------------------- conservation ----
+// Conserved totals by compensated summation: every addition is Knuth's
+// TwoSum (exact rounding error of s + x, accumulated in a second word), with
+// a fixed grid and a fixed reduction tree, so the result is deterministic and
+// its error does not grow with the number of terms.
+struct Comp {
+  double s, c;
+  __device__ void add(double x) {
+    const double t = s + x;
+    const double bp = t - s;
+    c += (s - (t - bp)) + (x - bp);
+    s = t;
+  }
+  __device__ void merge(const Comp& o) { add(o.s); c += o.c; }
+};
+
+// part[6 * block + 2 q + {0, 1}] = (sum, compensation) of quantity q over this
+// block's share: q = 0 cell mass, 1 cell internal energy m e, 2 node kinetic
+// energy 0.5 m |v|^2.
+__global__ void __launch_bounds__(kTotalsThreads) k_totals_partial(Dims dm, const double* __restrict__ mass,
+    const double* __restrict__ e, const double* __restrict__ nm, const double* __restrict__ v,
+    double* __restrict__ part) {
+  __shared__ double sm[kTotalsThreads / 32][6];
+  Comp q[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < dm.C; c += stride) {
+    const double m = mass[c];
+    q[0].add(m);
+    q[1].add(m * e[c]);
+  }
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < dm.N; n += stride) {
+    const double vx = v[n], vy = v[dm.N + n], vz = v[2 * dm.N + n];
+    q[2].add(0.5 * nm[n] * ((vx * vx + vy * vy) + vz * vz));
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int a = 0; a < 3; ++a) {
+      Comp other{__shfl_down_sync(0xffffffffu, q[a].s, o), __shfl_down_sync(0xffffffffu, q[a].c, o)};
+      q[a].merge(other);
+    }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int a = 0; a < 3; ++a) { sm[w][2 * a] = q[a].s; sm[w][2 * a + 1] = q[a].c; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Comp r[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    for (int ww = 0; ww < kTotalsThreads / 32; ++ww)
+      for (int a = 0; a < 3; ++a) r[a].merge(Comp{sm[ww][2 * a], sm[ww][2 * a + 1]});
+    for (int a = 0; a < 3; ++a) { part[6 * blockIdx.x + 2 * a] = r[a].s; part[6 * blockIdx.x + 2 * a + 1] = r[a].c; }
+  }
+}
+
+// One thread: the block partials in block order; out[q] = sum + compensation.
+__global__ void k_totals_finish(const double* __restrict__ part, int nparts, double* __restrict__ out) {
+  Comp r[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+  for (int b = 0; b < nparts; ++b)
+    for (int a = 0; a < 3; ++a) r[a].merge(Comp{part[6 * b + 2 * a], part[6 * b + 2 * a + 1]});
+  for (int a = 0; a < 3; ++a) out[a] = r[a].s + r[a].c;
+}
+
 // The dt reduction kernels; their bodies (dt_min_body, dt_finish_body) are in
 // mhy_kernels.cuh so that the batched cycle can run them per instance.
 __global__ void k_dt_min(Dims dm, Scalars* __restrict__ S, const double* __restrict__ L,

@@ -119,6 +119,11 @@ constexpr int kKernelsPerCycleBatch = 10;
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);
 __global__ void k_init_faces(Dims dm, const double* x0, double* n0, double* xf0);
 __global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* xf0, double* ofn);
+constexpr int kTotalsThreads = 256;
+constexpr int kTotalsBlocks = 148;   // one per SM; partials: 6 doubles per block
+__global__ void k_totals_partial(Dims dm, const double* mass, const double* e, const double* nm, const double* v,
+                                 double* part);
+__global__ void k_totals_finish(const double* part, int nparts, double* out);
 __global__ void k_init_state(Dims dm, Phys ph, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);

@@ -36,7 +36,8 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_get_env_mask", "mhy_batch_create", "mhy_batch_set_state", "mhy_batch_hydro_start_init",
             "mhy_batch_step", "mhy_batch_synchronize", "mhy_batch_get_field", "mhy_batch_get_dt",
             "mhy_batch_get_status", "mhy_batch_size", "mhy_batch_kernels_per_cycle", "mhy_batch_get_stream",
-            "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load"]
+            "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load",
+            "mhy_get_totals", "mhy_batch_get_totals"]
 ENV_FIELDS = {"fracvol": 0, "density": 1, "internal_energy": 2, "pressure": 3, "sound_speed": 4,
               "mass_fraction": 5, "cell_mass": 6}
 
@@ -125,6 +126,8 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_batch_get_stream.restype = vp
     L.mhy_batch_destroy.argtypes = [vp]
     L.mhy_batch_destroy.restype = None
+    L.mhy_get_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.mhy_batch_get_totals.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.mhy_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.mhy_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
     L.mhy_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
@@ -217,6 +220,13 @@ class Context:
         f = ctypes.c_uint32()
         _check(load().mhy_get_status(self.h, ctypes.byref(f)))
         return f.value
+
+    def totals(self) -> dict:
+        """Compensated device sums: mass, internal, kinetic and total energy."""
+        out = (ctypes.c_double * 3)()
+        _check(load().mhy_get_totals(self.h, out))
+        return {"mass": out[0], "internal_energy": out[1], "kinetic_energy": out[2],
+                "total_energy": out[1] + out[2]}
 
     def kernels_per_cycle(self) -> int:
         return load().mhy_kernels_per_cycle(self.h)
@@ -325,6 +335,12 @@ class Batch:
         f = ctypes.c_uint32()
         _check(load().mhy_batch_get_status(self.h, int(i), ctypes.byref(f)))
         return f.value
+
+    def totals(self, i: int) -> dict:
+        out = (ctypes.c_double * 3)()
+        _check(load().mhy_batch_get_totals(self.h, int(i), out))
+        return {"mass": out[0], "internal_energy": out[1], "kinetic_energy": out[2],
+                "total_energy": out[1] + out[2]}
 
     def kernels_per_cycle(self) -> int:
         return load().mhy_batch_kernels_per_cycle(self.h)

@@ -180,10 +180,22 @@ def run_reference(args):
     return 0
 
 
-def mixed_accuracy(cases, densities, cycles, device, batched=False):
+def conservation(t0, t1, cycles):
+    """Drift of the conserved totals over the run: t0, t1 are lists of
+    mhy_get_totals results (one per instance) before and after."""
+    import math
+    m0, m1 = math.fsum(t["mass"] for t in t0), math.fsum(t["mass"] for t in t1)
+    e0, e1 = math.fsum(t["total_energy"] for t in t0), math.fsum(t["total_energy"] for t in t1)
+    return {"mass_drift_rel": (m1 - m0) / m0, "total_energy_drift_rel": (e1 - e0) / e0, "cycles": cycles,
+            "sum": "compensated TwoSum on the device (mhy_get_totals), fixed order"}
+
+
+def mixed_accuracy(cases, densities, cycles, device, batched=False, totals=None):
     """Density L1 error of the mixed-precision run against the FP64 path on the
     same inputs and cycle count (the FP64 device path equals the oracle bit for
-    bit, which the GPU parity tests check): sum |rho_mixed - rho_fp64| / sum |rho_fp64|."""
+    bit, which the GPU parity tests check): sum |rho_mixed - rho_fp64| / sum |rho_fp64|;
+    with totals (the mixed run's mhy_get_totals per instance), the relative
+    difference of total mass and total energy from the FP64 run's."""
     import copy
     import math
     import numpy as np
@@ -198,16 +210,24 @@ def mixed_accuracy(cases, densities, cycles, device, batched=False):
         b = mhy_b200.Batch(ref_cases, device=device)
         b.step(cycles)
         refs = [b.field(i, "density") for i in range(len(ref_cases))]
+        ref_tot = [b.totals(i) for i in range(len(ref_cases))]
         b.close()
     else:
         g = mhy_b200.Context(ref_cases[0], device=device)
         g.step(cycles)
         refs = [g.field("density")]
+        ref_tot = [g.totals()]
         g.close()
     num = math.fsum(float(np.abs(a - r).sum()) for a, r in zip(densities, refs))
     den = math.fsum(float(np.abs(r).sum()) for r in refs)
-    return {"density_l1_rel_vs_fp64": num / den, "cycles": cycles,
-            "reference": "FP64 device path on the same inputs (bitwise equal to the CPU oracle)"}
+    out = {"density_l1_rel_vs_fp64": num / den, "cycles": cycles,
+           "reference": "FP64 device path on the same inputs (bitwise equal to the CPU oracle)"}
+    if totals is not None:
+        for key, q in (("mass_rel_vs_fp64", "mass"), ("total_energy_rel_vs_fp64", "total_energy")):
+            a = math.fsum(t[q] for t in totals)
+            r = math.fsum(t[q] for t in ref_tot)
+            out[key] = (a - r) / r
+    return out
 
 
 def run_reference_batched(args, threads):
@@ -266,6 +286,7 @@ def run_ours_batched(args):
     cells = sum(c.ncells for c in mine)
     b = mhy_b200.Batch(mine, device=local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    tot0 = [b.totals(i) for i in range(len(mine))]
     b.step(args.warmup)
     b.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -280,10 +301,12 @@ def run_ours_batched(args):
     ms, value = replicas.aggregate(cells, args.steps, start.elapsed_time(stop), dev)
     status = max(b.status(i) for i in range(len(mine)))
     kpc = b.kernels_per_cycle()
+    tot1 = [b.totals(i) for i in range(len(mine))]
+    cons = conservation(tot0, tot1, args.warmup + args.steps)
     accuracy = None
     if args.precision == "mixed":
         accuracy = mixed_accuracy(mine, [b.field(i, "density") for i in range(len(mine))],
-                                  args.warmup + args.steps, local, batched=True)
+                                  args.warmup + args.steps, local, batched=True, totals=tot1)
     b.close()
 
     e2e = None
@@ -339,7 +362,7 @@ def run_ours_batched(args):
                            "cells": total, "cells_per_gpu": cells, "parallelism": f"instances split over {world}",
                            "l2": "working set > 126 MB L2 (no flush needed)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kpc * args.steps,
-                "clocks": clk.summary(), "device_status": status}
+                "clocks": clk.summary(), "device_status": status, "conservation": cons}
         if accuracy:
             line["accuracy"] = accuracy
             line["dtype"] = "f32 remap evaluation / f64 state"
@@ -366,6 +389,7 @@ def run_ours(args):
     ctx = mhy_b200.Context(case, device=local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
     kpc = ctx.kernels_per_cycle()
+    tot0 = [ctx.totals()]
 
     ctx.step(args.warmup)
     ctx.synchronize()
@@ -383,9 +407,11 @@ def run_ours(args):
     ctx.synchronize()
     status = ctx.status()
     ms, value = replicas.aggregate(case.ncells, args.steps, ms_local, dev)
+    tot1 = [ctx.totals()]
+    cons = conservation(tot0, tot1, args.warmup + args.steps)
     accuracy = None
     if args.precision == "mixed":
-        accuracy = mixed_accuracy([case], [ctx.field("density")], args.warmup + args.steps, local)
+        accuracy = mixed_accuracy([case], [ctx.field("density")], args.warmup + args.steps, local, totals=tot1)
     ctx.close()
 
     # end to end through the per-entry-point C ABI, host buffers in pinned memory
@@ -447,7 +473,8 @@ def run_ours(args):
                            "cells_per_gpu": case.ncells, "parallelism": f"replicas{world}",
                            "l2": "working set > 1 GB, far above the 126 MB L2 (no flush needed)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status}
+                "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status,
+                "conservation": cons}
         if accuracy:
             line["accuracy"] = accuracy
             line["dtype"] = "f32 remap evaluation / f64 state"

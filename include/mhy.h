@@ -170,6 +170,12 @@ int mhy_get_dt(mhy_ctx* ctx, double* dt, double* dt_old);
 int mhy_get_time(mhy_ctx* ctx, double* time, int64_t* iteration);
 int mhy_get_status(mhy_ctx* ctx, uint32_t* flags);
 int mhy_get_sizes(mhy_ctx* ctx, int64_t* ncells, int64_t* nnodes, int64_t* nfaces);
+/* Conserved totals at the current cycle boundary, summed on the device with
+ * compensated (TwoSum) additions in a fixed order: out[0] = total mass
+ * sum_c m_c, out[1] = internal energy sum_c m_c e_c, out[2] = kinetic energy
+ * sum_n 0.5 m_n |v_n|^2 (node mass as remapVariables sets it,
+ * RemapADIFinal.cc:712-718).  Total energy = out[1] + out[2]. */
+int mhy_get_totals(mhy_ctx* ctx, double out[3]);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own work after it. */
 void* mhy_get_stream(mhy_ctx* ctx);
 /* Number of kernels one cycle launches. */
@@ -209,6 +215,7 @@ int mhy_batch_synchronize(mhy_batch* b);               /* MHY_ERR_DT_MIN / MHY_E
 int mhy_batch_get_field(mhy_batch* b, int i, int field, void* dst, size_t bytes);
 int mhy_batch_get_dt(mhy_batch* b, int i, double* dt, double* dt_old);
 int mhy_batch_get_status(mhy_batch* b, int i, uint32_t* flags);
+int mhy_batch_get_totals(mhy_batch* b, int i, double out[3]);
 int mhy_batch_size(mhy_batch* b);
 int mhy_batch_kernels_per_cycle(mhy_batch* b);
 void* mhy_batch_get_stream(mhy_batch* b);
