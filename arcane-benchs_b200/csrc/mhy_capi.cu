@@ -4,7 +4,11 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -47,6 +51,7 @@ struct mhy_ctx {
   BCTable bct{};
   mhy_options opt{};
   std::vector<void*> allocs;
+  std::vector<size_t> alloc_bytes;               // size of each allocation (device state snapshots)
   std::vector<std::pair<void**, size_t>> plan;   // arena requests (pointer, bytes)
   double* setup = nullptr;                       // 1024 doubles of set-up scratch
   // nodes
@@ -86,6 +91,7 @@ struct mhy_ctx {
     cudaError_t err = cudaMalloc(&base, total + 256);
     if (err != cudaSuccess) return fail(MHY_ERR_OOM, "cudaMalloc failed: " + std::string(cudaGetErrorString(err)));
     allocs.push_back(base);
+    alloc_bytes.push_back(total + 256);
     char* p_ = static_cast<char*>(base);
     for (auto& r : plan) {
       *r.first = p_;
@@ -501,11 +507,52 @@ struct mhy_batch {
   std::vector<mhy_ctx*> inst;
   CycleArgs* d_descs = nullptr;
   int4* d_work[BK_COUNT] = {};
+  int order[BK_COUNT] = {};                     // work-table order of each kind (mhy_batch_tuning.order)
   BatchPlan plan{};
   int sens = 0;
   bool initialized = false;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  mhy_batch_tuning tuning{};
 };
+
+namespace {
+
+// Work table of one kernel kind: every block of every instance's grid, in
+// one of three orders (mhy_batch_tuning.order).
+std::vector<int4> build_work(const std::vector<mhy_ctx*>& inst, int kind, int order) {
+  const int n = (int)inst.size();
+  std::vector<int> ids(n);
+  std::iota(ids.begin(), ids.end(), 0);
+  if (order == 1)
+    std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return inst[a]->dm.C > inst[b]->dm.C; });
+  std::vector<std::vector<int4>> per(n);
+  for (int i = 0; i < n; ++i) {
+    int gx, gy, gz;
+    batch_work_shape(inst[i]->dm, kind, gx, gy, gz);
+    if (gy < 0) {                               // linear chunks of consecutive items
+      for (int x = 0; x < gx; ++x) per[i].push_back(make_int4(i, x, -1, 0));
+      continue;
+    }
+    for (int z = 0; z < gz; ++z)
+      for (int y = 0; y < gy; ++y)
+        for (int x = 0; x < gx; ++x) per[i].push_back(make_int4(i, x, y, z));
+  }
+  std::vector<int4> w;
+  if (order == 2) {                             // instances interleaved, 16 consecutive tiles at a time
+    constexpr size_t kChunk = 16;
+    for (size_t off = 0;; off += kChunk) {
+      bool any = false;
+      for (int i : ids)
+        for (size_t t = off; t < std::min(off + kChunk, per[i].size()); ++t) { w.push_back(per[i][t]); any = true; }
+      if (!any) break;
+    }
+  } else {
+    for (int i : ids) w.insert(w.end(), per[i].begin(), per[i].end());
+  }
+  return w;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -539,18 +586,7 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   // work tables: every block of every instance's grid, instance-major
   for (int k = 0; k < BK_COUNT; ++k) {
-    std::vector<int4> w;
-    for (int i = 0; i < n; ++i) {
-      int gx, gy, gz;
-      batch_work_shape(b->inst[i]->dm, k, gx, gy, gz);
-      if (gy < 0) {                             // linear chunks of consecutive items
-        for (int x = 0; x < gx; ++x) w.push_back(make_int4(i, x, -1, 0));
-        continue;
-      }
-      for (int z = 0; z < gz; ++z)
-        for (int y = 0; y < gy; ++y)
-          for (int x = 0; x < gx; ++x) w.push_back(make_int4(i, x, y, z));
-    }
+    const std::vector<int4> w = build_work(b->inst, k, 0);
     err = cudaMalloc(&b->d_work[k], w.size() * sizeof(int4));
     if (err == cudaSuccess) err = cudaMemcpy(b->d_work[k], w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
@@ -562,6 +598,11 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   b->plan.descs = b->d_descs;
   b->plan.ninst = n;
   b->plan.precision = opts[0].precision;
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
+    b->plan.occ_pct[k] = 100;
+    b->tuning.occupancy_pct[k] = 100;
+    b->tuning.order[k] = 0;
+  }
   *out = b;
   return MHY_OK;
 }
@@ -644,6 +685,204 @@ int mhy_batch_get_totals(mhy_batch* b, int i, double* out) {
 }
 
 int mhy_batch_size(mhy_batch* b) { return b ? (int)b->inst.size() : 0; }
+
+}  // extern "C"
+
+namespace {
+
+static_assert(MHY_TUNE_SLOTS == BK_TUNE_SLOTS, "tuning slots of the ABI and the batch plan");
+constexpr int kTuneOrders = 3;
+constexpr int kTunePcts[] = {100, 75, 50};
+
+// Work tables and grid sizes of the plan from a tuning; the cycle graphs are
+// re-captured at the next step.
+int apply_tuning(mhy_batch* b, const mhy_batch_tuning& t) {
+  for (int k = 0; k < BK_COUNT; ++k) {
+    if (t.order[k] == b->order[k]) continue;
+    const std::vector<int4> w = build_work(b->inst, k, t.order[k]);
+    MHY_CUDA(cudaMemcpyAsync(b->d_work[k], w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice, b->stream));
+    MHY_CUDA(cudaStreamSynchronize(b->stream));                 // w is a host temporary
+    b->order[k] = t.order[k];
+  }
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) b->plan.occ_pct[k] = t.occupancy_pct[k];
+  for (int s = 0; s < 3; ++s)
+    if (b->graph[s]) { cudaGraphExecDestroy(b->graph[s]); b->graph[s] = nullptr; }
+  return MHY_OK;
+}
+
+int check_tuning(const mhy_batch_tuning& t) {
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
+    if (t.order[k] < 0 || t.order[k] >= kTuneOrders) return fail(MHY_ERR_ARG, "tuning order must be 0, 1 or 2");
+    if (t.occupancy_pct[k] < 1 || t.occupancy_pct[k] > 100) return fail(MHY_ERR_ARG, "occupancy_pct must be 1..100");
+  }
+  return MHY_OK;
+}
+
+// Cache key: the precision and the sorted list of mesh sizes.
+std::string tune_key(const mhy_batch* b) {
+  std::vector<std::string> sz;
+  for (const mhy_ctx* c : b->inst)
+    sz.push_back(std::to_string(c->dm.nx) + "x" + std::to_string(c->dm.ny) + "x" + std::to_string(c->dm.nz));
+  std::sort(sz.begin(), sz.end());
+  std::string key = "p" + std::to_string(b->plan.precision);
+  for (const auto& x : sz) key += ":" + x;
+  return key;
+}
+
+std::mutex g_tune_mu;
+std::map<std::string, mhy_batch_tuning> g_tune_cache;
+
+// Per-slot GPU time of `cycles` eager cycles (after one untimed cycle).
+int time_cycles(mhy_batch* b, int cycles, double ms[BK_TUNE_SLOTS]) {
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) ms[k] = 0.;
+  KernelMarks m{};
+  cudaEvent_t start = nullptr;
+  MHY_CUDA(cudaEventCreate(&start));
+  for (int i = 0; i < KernelMarks::kMax; ++i) MHY_CUDA(cudaEventCreate(&m.ev[i]));
+  int rc = MHY_OK;
+  launch_batch_cycle(b->plan, b->sens, b->stream);
+  b->sens = (b->sens + 1) % 3;
+  for (int c = 0; c < cycles && rc == MHY_OK; ++c) {
+    m.n = 0;
+    cudaEventRecord(start, b->stream);
+    launch_batch_cycle(b->plan, b->sens, b->stream, &m);
+    b->sens = (b->sens + 1) % 3;
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess) {
+      rc = fail(MHY_ERR_CUDA, "autotune cycle failed");
+      break;
+    }
+    cudaEvent_t prev = start;
+    for (int i = 0; i < m.n; ++i) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, prev, m.ev[i]);
+      ms[m.kind[i]] += t;
+      prev = m.ev[i];
+    }
+  }
+  for (int i = 0; i < KernelMarks::kMax; ++i) cudaEventDestroy(m.ev[i]);
+  cudaEventDestroy(start);
+  if (rc == MHY_OK)
+    for (int k = 0; k < BK_TUNE_SLOTS; ++k) ms[k] /= cycles;
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhy_batch_get_tuning(mhy_batch* b, mhy_batch_tuning* out) {
+  if (!b || !out) return fail(MHY_ERR_ARG, "null argument");
+  *out = b->tuning;
+  return MHY_OK;
+}
+
+int mhy_batch_set_tuning(mhy_batch* b, const mhy_batch_tuning* t) {
+  if (!b || !t) return fail(MHY_ERR_ARG, "null argument");
+  mhy_batch_tuning u = *t;
+  u.order[BK_DT_MIN] = u.order[BK_LCELLS];
+  u.order[BK_DT_FINISH] = 0;
+  int rc = check_tuning(u);
+  if (rc == MHY_OK) rc = apply_tuning(b, u);
+  if (rc == MHY_OK) b->tuning = u;
+  return rc;
+}
+
+int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_batch_tuning* out) {
+  if (!b) return fail(MHY_ERR_ARG, "null batch");
+  if (!b->initialized) return fail(MHY_ERR_STATE, "mhy_batch_hydro_start_init must come first");
+  if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
+  const std::string key = tune_key(b);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      mhy_batch_tuning t = it->second;
+      t.from_cache = 1;
+      int rc = apply_tuning(b, t);
+      if (rc != MHY_OK) return rc;
+      b->tuning = t;
+      if (out) *out = t;
+      return MHY_OK;
+    }
+  }
+  MHY_CUDA(cudaSetDevice(b->device));
+  // snapshot of every instance's device state (its arena), restored at the end
+  size_t total = 0;
+  for (const mhy_ctx* c : b->inst)
+    for (size_t x : c->alloc_bytes) total += (x + 255) & ~size_t(255);
+  char* snap = nullptr;
+  if (cudaMalloc(&snap, total) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MHY_ERR_OOM, "autotune: no device memory for the state snapshot");
+  }
+  MHY_CUDA(cudaStreamSynchronize(b->stream));
+  {
+    size_t off = 0;
+    for (const mhy_ctx* c : b->inst)
+      for (size_t a = 0; a < c->allocs.size(); ++a) {
+        MHY_CUDA(cudaMemcpyAsync(snap + off, c->allocs[a], c->alloc_bytes[a], cudaMemcpyDeviceToDevice, b->stream));
+        off += (c->alloc_bytes[a] + 255) & ~size_t(255);
+      }
+  }
+  const int sens0 = b->sens;
+  const mhy_batch_tuning before = b->tuning;
+  // trials: every (order, occupancy) setting on every slot at once
+  constexpr int kNP = sizeof(kTunePcts) / sizeof(kTunePcts[0]);
+  double ms[kTuneOrders][kNP][BK_TUNE_SLOTS];
+  int rc = MHY_OK;
+  for (int o = 0; o < kTuneOrders && rc == MHY_OK; ++o)
+    for (int q = 0; q < kNP && rc == MHY_OK; ++q) {
+      mhy_batch_tuning t{};
+      for (int k = 0; k < BK_TUNE_SLOTS; ++k) { t.order[k] = o; t.occupancy_pct[k] = kTunePcts[q]; }
+      rc = apply_tuning(b, t);
+      if (rc == MHY_OK) rc = time_cycles(b, cycles, ms[o][q]);
+    }
+  mhy_batch_tuning best{};
+  if (rc == MHY_OK) {
+    for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
+      int bo = 0, bq = 0;
+      const int o_lo = k == BK_DT_MIN ? best.order[BK_LCELLS] : 0;   // the dt reduction walks slot 1's table
+      const int o_hi = k == BK_DT_MIN ? o_lo + 1 : (k == BK_DT_FINISH ? 1 : kTuneOrders);
+      bo = o_lo;
+      for (int o = o_lo; o < o_hi; ++o)
+        for (int q = 0; q < (k == BK_DT_FINISH ? 1 : kNP); ++q)
+          if (ms[o][q][k] < 0.98 * ms[bo][bq][k]) { bo = o; bq = q; }
+      best.order[k] = bo;
+      best.occupancy_pct[k] = kTunePcts[bq];
+      best.ms_default[k] = ms[0][0][k];
+      best.ms_tuned[k] = ms[bo][bq][k];
+    }
+    best.trials = kTuneOrders * kNP;
+    best.from_cache = 0;
+  }
+  // restore the state and the rotation of the sweep directions
+  {
+    size_t off = 0;
+    for (const mhy_ctx* c : b->inst)
+      for (size_t a = 0; a < c->allocs.size(); ++a) {
+        cudaMemcpyAsync(c->allocs[a], snap + off, c->alloc_bytes[a], cudaMemcpyDeviceToDevice, b->stream);
+        off += (c->alloc_bytes[a] + 255) & ~size_t(255);
+      }
+  }
+  const cudaError_t se = cudaStreamSynchronize(b->stream);
+  cudaFree(snap);
+  b->sens = sens0;
+  for (mhy_ctx* c : b->inst) c->sens = b->sens;
+  if (se != cudaSuccess && rc == MHY_OK) rc = fail(MHY_ERR_CUDA, cudaGetErrorString(se));
+  if (rc != MHY_OK) {
+    apply_tuning(b, before);
+    return rc;
+  }
+  rc = apply_tuning(b, best);
+  if (rc != MHY_OK) return rc;
+  b->tuning = best;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  if (out) *out = best;
+  return MHY_OK;
+}
 int mhy_batch_kernels_per_cycle(mhy_batch* b) { return b ? kKernelsPerCycleBatch : 0; }
 void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
 

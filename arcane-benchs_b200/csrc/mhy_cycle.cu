@@ -409,9 +409,9 @@ __global__ void k_bat_dt_finish(const CycleArgs* __restrict__ D, int n) {
 }
 
 // Resident blocks of a persistent grid for `kernel`: SMs x blocks per SM
-// (queried once per kernel and device).
+// (queried once per kernel and device), scaled by pct percent.
 template <class Kern>
-static int persistent_blocks(Kern kernel, int threads, int nwork) {
+static int persistent_blocks(Kern kernel, int threads, int nwork, int pct) {
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, int> cache;
   int dev = 0;
@@ -429,65 +429,80 @@ static int persistent_blocks(Kern kernel, int threads, int nwork) {
     }
     g = itc->second;
   }
+  if (pct > 0 && pct < 100) g = (int)(((long long)g * pct + 99) / 100);
+  if (g < 1) g = 1;
   return nwork < g ? (nwork > 0 ? nwork : 1) : g;
 }
 
+static void mark(KernelMarks* m, int kind, cudaStream_t s) {
+  if (!m || m->n >= KernelMarks::kMax) return;
+  cudaEventRecord(m->ev[m->n], s);
+  m->kind[m->n++] = kind;
+}
+
+// One persistent launch over the work table of `kind`; tk is the tuning slot
+// (grid percentage and timing mark): the kind itself, or BK_DT_MIN.
 template <class Kern, class... Args>
-static void launch_persistent(Kern kernel, int threads, int nwork, cudaStream_t s, Args... args) {
-  if (nwork <= 0) return;
-  kernel<<<persistent_blocks(kernel, threads, nwork), threads, 0, s>>>(args...);
+static void launch_persistent(Kern kernel, int threads, const BatchPlan& P, int kind, int tk, cudaStream_t s,
+                              KernelMarks* marks, Args... args) {
+  const int nwork = P.nwork[kind];
+  if (nwork > 0) kernel<<<persistent_blocks(kernel, threads, nwork, P.occ_pct[tk]), threads, 0, s>>>(args...);
+  mark(marks, tk, s);
 }
 
 template <int DD, bool LAST, typename R>
-static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s) {
+static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int T = 32 * kLineWarps, kind = BK_CELLS_X + DD;
-  if constexpr (DD == 0) launch_persistent(k_bat_sweep_cells_x<LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
-  else launch_persistent(k_bat_sweep_cells_t<DD, LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it);
+  if constexpr (DD == 0) launch_persistent(k_bat_sweep_cells_x<LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it);
+  else launch_persistent(k_bat_sweep_cells_t<DD, LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it);
 }
 
 template <int DD, bool FIRST, bool LAST, typename R>
-static void bat_nodes_d(const BatchPlan& P, int it, int prev, cudaStream_t s) {
+static void bat_nodes_d(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const int T = 32 * kLineWarps, kind = BK_NODES_X + DD;
   if constexpr (DD == 0)
-    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
+    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it, prev);
   else
-    launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R>, T, P.nwork[kind], s, P.descs, P.work[kind], P.nwork[kind], it, prev);
+    launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it,
+                      prev);
 }
 
 template <int DD, typename R>
-static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s) {
+static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const bool first = it == 0, last = it == 2;
-  if (last) bat_cells_d<DD, true, R>(P, it, s);
-  else bat_cells_d<DD, false, R>(P, it, s);
-  if (first) bat_nodes_d<DD, true, false, R>(P, it, prev, s);
-  else if (last) bat_nodes_d<DD, false, true, R>(P, it, prev, s);
-  else bat_nodes_d<DD, false, false, R>(P, it, prev, s);
+  if (last) bat_cells_d<DD, true, R>(P, it, s, m);
+  else bat_cells_d<DD, false, R>(P, it, s, m);
+  if (first) bat_nodes_d<DD, true, false, R>(P, it, prev, s, m);
+  else if (last) bat_nodes_d<DD, false, true, R>(P, it, prev, s, m);
+  else bat_nodes_d<DD, false, false, R>(P, it, prev, s, m);
 }
 
-void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s) {
+void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
   if (P.precision) {
-    launch_persistent(k_bat_lagrange_nodes<float>, 128, P.nwork[BK_LNODES], s, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
-    launch_persistent(k_bat_lagrange_cells<float>, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+    launch_persistent(k_bat_lagrange_nodes<float>, 128, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+    launch_persistent(k_bat_lagrange_cells<float>, 128, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   } else {
-    launch_persistent(k_bat_lagrange_nodes<double>, 128, P.nwork[BK_LNODES], s, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
-    launch_persistent(k_bat_lagrange_cells<double>, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+    launch_persistent(k_bat_lagrange_nodes<double>, 128, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+    launch_persistent(k_bat_lagrange_cells<double>, 128, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   }
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
     if (P.precision) {
-      if (d == 0) bat_sweep<0, float>(P, it, prev, s);
-      else if (d == 1) bat_sweep<1, float>(P, it, prev, s);
-      else bat_sweep<2, float>(P, it, prev, s);
+      if (d == 0) bat_sweep<0, float>(P, it, prev, s, m);
+      else if (d == 1) bat_sweep<1, float>(P, it, prev, s, m);
+      else bat_sweep<2, float>(P, it, prev, s, m);
     } else {
-      if (d == 0) bat_sweep<0, double>(P, it, prev, s);
-      else if (d == 1) bat_sweep<1, double>(P, it, prev, s);
-      else bat_sweep<2, double>(P, it, prev, s);
+      if (d == 0) bat_sweep<0, double>(P, it, prev, s, m);
+      else if (d == 1) bat_sweep<1, double>(P, it, prev, s, m);
+      else bat_sweep<2, double>(P, it, prev, s, m);
     }
     prev |= 1 << d;
   }
-  launch_persistent(k_bat_dt_min, 128, P.nwork[BK_LCELLS], s, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  // the dt reduction walks the cell tiles of the Lagrange cell kernel
+  launch_persistent(k_bat_dt_min, 128, P, BK_LCELLS, BK_DT_MIN, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   k_bat_dt_finish<<<(P.ninst + 127) / 128, 128, 0, s>>>(P.descs, P.ninst);
+  mark(m, BK_DT_FINISH, s);
 }
 
 }  // namespace mhy

@@ -104,16 +104,28 @@ constexpr int kKernelsPerCycleEnv = 11;
 // instance's own grid; a persistent grid of resident blocks walks the table.
 // The arguments of instance i are descs[i] in device memory.
 enum BatchKernel { BK_LNODES = 0, BK_LCELLS, BK_CELLS_X, BK_CELLS_Y, BK_CELLS_Z, BK_NODES_X, BK_NODES_Y, BK_NODES_Z,
-                   BK_COUNT };
+                   BK_COUNT,
+                   BK_DT_MIN = BK_COUNT,      // tuning slots beyond the work tables: the dt reduction (cell
+                   BK_DT_FINISH,              // tiles of BK_LCELLS) and the per-instance dt finish
+                   BK_TUNE_SLOTS };
 struct BatchPlan {
   const CycleArgs* descs;       // device, one per instance
   int ninst;
   const int4* work[BK_COUNT];   // device work tables
   int nwork[BK_COUNT];
   int precision;                // all instances share it
+  int occ_pct[BK_TUNE_SLOTS];   // persistent grid of each slot: % of the resident-block capacity
+};
+// Events recorded after each launch of a cycle (autotuning), with the tuning
+// slot of each launch.
+struct KernelMarks {
+  static constexpr int kMax = 16;
+  cudaEvent_t ev[kMax];
+  int kind[kMax];
+  int n;
 };
 void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz);
-void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s);
+void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 constexpr int kKernelsPerCycleBatch = 10;
 
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);

@@ -37,7 +37,11 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_batch_step", "mhy_batch_synchronize", "mhy_batch_get_field", "mhy_batch_get_dt",
             "mhy_batch_get_status", "mhy_batch_size", "mhy_batch_kernels_per_cycle", "mhy_batch_get_stream",
             "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load",
-            "mhy_get_totals", "mhy_batch_get_totals"]
+            "mhy_get_totals", "mhy_batch_get_totals", "mhy_batch_autotune", "mhy_batch_set_tuning",
+            "mhy_batch_get_tuning"]
+MHY_TUNE_SLOTS = 10
+TUNE_SLOTS = ("lagrange_nodes", "lagrange_cells", "cells_x", "cells_y", "cells_z", "nodes_x", "nodes_y", "nodes_z",
+              "dt_min", "dt_finish")
 ENV_FIELDS = {"fracvol": 0, "density": 1, "internal_energy": 2, "pressure": 3, "sound_speed": 4,
               "mass_fraction": 5, "cell_mass": 6}
 
@@ -50,6 +54,18 @@ class MhyError(RuntimeError):
 
 class BC(ctypes.Structure):
     _fields_ = [("surface", ctypes.c_int32), ("type", ctypes.c_int32), ("value", ctypes.c_double)]
+
+
+class CTuning(ctypes.Structure):
+    _fields_ = [("order", ctypes.c_int32 * MHY_TUNE_SLOTS), ("occupancy_pct", ctypes.c_int32 * MHY_TUNE_SLOTS),
+                ("ms_default", ctypes.c_double * MHY_TUNE_SLOTS), ("ms_tuned", ctypes.c_double * MHY_TUNE_SLOTS),
+                ("from_cache", ctypes.c_int32), ("trials", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"slots": {name: {"order": self.order[k], "occupancy_pct": self.occupancy_pct[k],
+                                 "ms_default": round(self.ms_default[k], 4), "ms_tuned": round(self.ms_tuned[k], 4)}
+                          for k, name in enumerate(TUNE_SLOTS)},
+                "from_cache": bool(self.from_cache), "trials": self.trials}
 
 
 class COptions(ctypes.Structure):
@@ -127,6 +143,9 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_batch_destroy.argtypes = [vp]
     L.mhy_batch_destroy.restype = None
     L.mhy_get_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.mhy_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CTuning)]
+    L.mhy_batch_set_tuning.argtypes = [vp, ctypes.POINTER(CTuning)]
+    L.mhy_batch_get_tuning.argtypes = [vp, ctypes.POINTER(CTuning)]
     L.mhy_batch_get_totals.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.mhy_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.mhy_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
@@ -323,6 +342,9 @@ class Batch:
     def step(self, ncycles: int = 1):
         _check(load().mhy_batch_step(self.h, int(ncycles)))
 
+    def size(self) -> int:
+        return load().mhy_batch_size(self.h)
+
     def synchronize(self):
         _check(load().mhy_batch_synchronize(self.h))
 
@@ -335,6 +357,21 @@ class Batch:
         f = ctypes.c_uint32()
         _check(load().mhy_batch_get_status(self.h, int(i), ctypes.byref(f)))
         return f.value
+
+    def autotune(self, cycles: int = 2) -> CTuning:
+        """mhy_batch_autotune: the fastest work order and persistent grid per
+        kernel slot, timed on this batch's state (restored afterwards)."""
+        t = CTuning()
+        _check(load().mhy_batch_autotune(self.h, int(cycles), ctypes.byref(t)))
+        return t
+
+    def tuning(self) -> CTuning:
+        t = CTuning()
+        _check(load().mhy_batch_get_tuning(self.h, ctypes.byref(t)))
+        return t
+
+    def set_tuning(self, t: CTuning):
+        _check(load().mhy_batch_set_tuning(self.h, ctypes.byref(t)))
 
     def totals(self, i: int) -> dict:
         out = (ctypes.c_double * 3)()
