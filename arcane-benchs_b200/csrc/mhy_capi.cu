@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -76,6 +77,9 @@ struct mhy_ctx {
   bool state_set = false, initialized = false;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int kernels_per_cycle = 0;
+  int lines[BK_COUNT] = {kLineWarps, kLineWarps, kLineWarps, kLineWarps, kLineWarps, kLineWarps, kLineWarps,
+                         kLineWarps};                  // lines per block of the sweeps (the tuning)
+  mhy_tuning tuning{};
 
   // Device arrays come from one allocation: alloc() records a request,
   // commit() allocates the sum (256-byte aligned pieces) and sets the pointers.
@@ -110,6 +114,7 @@ struct mhy_ctx {
     a.fd = fd;
     a.st.rho = rho; a.st.e = e; a.st.q = q; a.st.p = p; a.st.cs = cs; a.st.mass = mass; a.st.Ve = Ve;
     a.K = K; a.env = env; a.Vlag = Vlag;
+    for (int k = 0; k < BK_COUNT; ++k) a.lines[k] = lines[k];
     return a;
   }
 };
@@ -172,6 +177,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       return fail(MHY_ERR_ARG, "bad boundary condition");
 
   mhy_ctx* c = new mhy_ctx();
+  for (int k = 0; k < MHY_TUNE_SLOTS; ++k) {
+    c->tuning.order[k] = 0; c->tuning.occupancy_pct[k] = 100; c->tuning.lines_per_block[k] = kLineWarps;
+  }
   c->opt = *opt;
   if (device >= 0) {
     cudaError_t err = cudaSetDevice(device);
@@ -507,19 +515,19 @@ struct mhy_batch {
   std::vector<mhy_ctx*> inst;
   CycleArgs* d_descs = nullptr;
   int4* d_work[BK_COUNT] = {};
-  int order[BK_COUNT] = {};                     // work-table order of each kind (mhy_batch_tuning.order)
+  int order[BK_COUNT] = {};                     // work-table order of each kind (mhy_tuning.order)
   BatchPlan plan{};
   int sens = 0;
   bool initialized = false;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-  mhy_batch_tuning tuning{};
+  mhy_tuning tuning{};
 };
 
 namespace {
 
 // Work table of one kernel kind: every block of every instance's grid, in
-// one of three orders (mhy_batch_tuning.order).
-std::vector<int4> build_work(const std::vector<mhy_ctx*>& inst, int kind, int order) {
+// one of three orders (mhy_tuning.order), for the given lines per block.
+std::vector<int4> build_work(const std::vector<mhy_ctx*>& inst, int kind, int order, int lines) {
   const int n = (int)inst.size();
   std::vector<int> ids(n);
   std::iota(ids.begin(), ids.end(), 0);
@@ -528,7 +536,7 @@ std::vector<int4> build_work(const std::vector<mhy_ctx*>& inst, int kind, int or
   std::vector<std::vector<int4>> per(n);
   for (int i = 0; i < n; ++i) {
     int gx, gy, gz;
-    batch_work_shape(inst[i]->dm, kind, gx, gy, gz);
+    batch_work_shape(inst[i]->dm, kind, lines, gx, gy, gz);
     if (gy < 0) {                               // linear chunks of consecutive items
       for (int x = 0; x < gx; ++x) per[i].push_back(make_int4(i, x, -1, 0));
       continue;
@@ -586,8 +594,11 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   // work tables: every block of every instance's grid, instance-major
   for (int k = 0; k < BK_COUNT; ++k) {
-    const std::vector<int4> w = build_work(b->inst, k, 0);
-    err = cudaMalloc(&b->d_work[k], w.size() * sizeof(int4));
+    // capacity for the largest table any tuning builds (8 lines per block)
+    size_t cap = 0;
+    for (int lw : kLineOptions) cap = std::max(cap, build_work(b->inst, k, 0, lw).size());
+    const std::vector<int4> w = build_work(b->inst, k, 0, kLineWarps);
+    err = cudaMalloc(&b->d_work[k], cap * sizeof(int4));
     if (err == cudaSuccess) err = cudaMemcpy(b->d_work[k], w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
     b->plan.work[k] = b->d_work[k];
@@ -602,7 +613,9 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
     b->plan.occ_pct[k] = 100;
     b->tuning.occupancy_pct[k] = 100;
     b->tuning.order[k] = 0;
+    b->tuning.lines_per_block[k] = kLineWarps;
   }
+  for (int k = 0; k < BK_COUNT; ++k) b->plan.lines[k] = kLineWarps;
   *out = b;
   return MHY_OK;
 }
@@ -693,16 +706,40 @@ namespace {
 static_assert(MHY_TUNE_SLOTS == BK_TUNE_SLOTS, "tuning slots of the ABI and the batch plan");
 constexpr int kTuneOrders = 3;
 constexpr int kTunePcts[] = {100, 75, 50};
+constexpr int kNP = sizeof(kTunePcts) / sizeof(kTunePcts[0]);
+constexpr int kNL = sizeof(kLineOptions) / sizeof(kLineOptions[0]);
+inline bool line_slot(int k) {
+  return k == BK_CELLS_Y || k == BK_CELLS_Z || k == BK_NODES_Y || k == BK_NODES_Z;
+}
 
-// Work tables and grid sizes of the plan from a tuning; the cycle graphs are
-// re-captured at the next step.
-int apply_tuning(mhy_batch* b, const mhy_batch_tuning& t) {
+mhy_tuning default_tuning() {
+  mhy_tuning t{};
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) { t.order[k] = 0; t.occupancy_pct[k] = 100; t.lines_per_block[k] = kLineWarps; }
+  return t;
+}
+
+int check_tuning(const mhy_tuning& t) {
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
+    if (t.order[k] < 0 || t.order[k] >= kTuneOrders) return fail(MHY_ERR_ARG, "tuning order must be 0, 1 or 2");
+    if (t.occupancy_pct[k] < 1 || t.occupancy_pct[k] > 100) return fail(MHY_ERR_ARG, "occupancy_pct must be 1..100");
+    const int w = t.lines_per_block[k];
+    if (w != 8 && w != 16 && w != 32) return fail(MHY_ERR_ARG, "lines_per_block must be 8, 16 or 32");
+    if (w != kLineWarps && !line_slot(k)) return fail(MHY_ERR_ARG, "lines_per_block applies to the y/z sweeps only");
+  }
+  return MHY_OK;
+}
+
+// The tuning of a batch: work tables (order and shape) and grid sizes; the
+// cycle graphs are re-captured at the next step.
+int apply_tuning(mhy_batch* b, const mhy_tuning& t) {
   for (int k = 0; k < BK_COUNT; ++k) {
-    if (t.order[k] == b->order[k]) continue;
-    const std::vector<int4> w = build_work(b->inst, k, t.order[k]);
+    if (t.order[k] == b->order[k] && t.lines_per_block[k] == b->plan.lines[k]) continue;
+    const std::vector<int4> w = build_work(b->inst, k, t.order[k], t.lines_per_block[k]);
     MHY_CUDA(cudaMemcpyAsync(b->d_work[k], w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice, b->stream));
     MHY_CUDA(cudaStreamSynchronize(b->stream));                 // w is a host temporary
     b->order[k] = t.order[k];
+    b->plan.lines[k] = t.lines_per_block[k];
+    b->plan.nwork[k] = (int)w.size();
   }
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) b->plan.occ_pct[k] = t.occupancy_pct[k];
   for (int s = 0; s < 3; ++s)
@@ -710,44 +747,77 @@ int apply_tuning(mhy_batch* b, const mhy_batch_tuning& t) {
   return MHY_OK;
 }
 
-int check_tuning(const mhy_batch_tuning& t) {
-  for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
-    if (t.order[k] < 0 || t.order[k] >= kTuneOrders) return fail(MHY_ERR_ARG, "tuning order must be 0, 1 or 2");
-    if (t.occupancy_pct[k] < 1 || t.occupancy_pct[k] > 100) return fail(MHY_ERR_ARG, "occupancy_pct must be 1..100");
-  }
+// The tuning of a context: lines per block; the graphs are re-captured.
+int apply_tuning(mhy_ctx* c, const mhy_tuning& t) {
+  for (int k = 0; k < BK_COUNT; ++k) c->lines[k] = t.lines_per_block[k];
+  for (int s = 0; s < 3; ++s)
+    if (c->graph[s]) { cudaGraphExecDestroy(c->graph[s]); c->graph[s] = nullptr; }
   return MHY_OK;
 }
 
-// Cache key: the precision and the sorted list of mesh sizes.
-std::string tune_key(const mhy_batch* b) {
+// Cache key: the precision, the number of environments and the sorted mesh sizes.
+std::string tune_key(const std::vector<mhy_ctx*>& inst, const char* kind) {
   std::vector<std::string> sz;
-  for (const mhy_ctx* c : b->inst)
+  for (const mhy_ctx* c : inst)
     sz.push_back(std::to_string(c->dm.nx) + "x" + std::to_string(c->dm.ny) + "x" + std::to_string(c->dm.nz));
   std::sort(sz.begin(), sz.end());
-  std::string key = "p" + std::to_string(b->plan.precision);
+  std::string key = std::string(kind) + ":p" + std::to_string(inst[0]->ph.precision) + ":k" +
+                    std::to_string(inst[0]->K);
   for (const auto& x : sz) key += ":" + x;
   return key;
 }
 
 std::mutex g_tune_mu;
-std::map<std::string, mhy_batch_tuning> g_tune_cache;
+std::map<std::string, mhy_tuning> g_tune_cache;
 
-// Per-slot GPU time of `cycles` eager cycles (after one untimed cycle).
-int time_cycles(mhy_batch* b, int cycles, double ms[BK_TUNE_SLOTS]) {
+// Device snapshot of the state (every allocation) of some contexts.
+struct Snapshot {
+  char* buf = nullptr;
+  int save(const std::vector<mhy_ctx*>& inst, cudaStream_t s) {
+    size_t total = 0;
+    for (const mhy_ctx* c : inst)
+      for (size_t x : c->alloc_bytes) total += (x + 255) & ~size_t(255);
+    if (cudaMalloc(&buf, total) != cudaSuccess) {
+      cudaGetLastError();
+      buf = nullptr;
+      return fail(MHY_ERR_OOM, "autotune: no device memory for the state snapshot");
+    }
+    return copy(inst, s, true);
+  }
+  int copy(const std::vector<mhy_ctx*>& inst, cudaStream_t s, bool to_snap) {
+    size_t off = 0;
+    for (const mhy_ctx* c : inst)
+      for (size_t a = 0; a < c->allocs.size(); ++a) {
+        char* dev = static_cast<char*>(c->allocs[a]);
+        const cudaError_t e = cudaMemcpyAsync(to_snap ? buf + off : dev, to_snap ? dev : buf + off, c->alloc_bytes[a],
+                                              cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return fail(MHY_ERR_CUDA, cudaGetErrorString(e));
+        off += (c->alloc_bytes[a] + 255) & ~size_t(255);
+      }
+    const cudaError_t e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? MHY_OK : fail(MHY_ERR_CUDA, cudaGetErrorString(e));
+  }
+  ~Snapshot() { if (buf) cudaFree(buf); }
+};
+
+// Per-slot GPU time of `cycles` eager cycles (after one untimed cycle);
+// launch(marks) enqueues one cycle and advances the direction rotation.
+template <class Launch>
+int time_cycles(cudaStream_t stream, int cycles, Launch&& launch, double ms[BK_TUNE_SLOTS]) {
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) ms[k] = 0.;
   KernelMarks m{};
   cudaEvent_t start = nullptr;
-  MHY_CUDA(cudaEventCreate(&start));
-  for (int i = 0; i < KernelMarks::kMax; ++i) MHY_CUDA(cudaEventCreate(&m.ev[i]));
-  int rc = MHY_OK;
-  launch_batch_cycle(b->plan, b->sens, b->stream);
-  b->sens = (b->sens + 1) % 3;
+  if (cudaEventCreate(&start) != cudaSuccess) return fail(MHY_ERR_CUDA, "event");
+  int made = 0;
+  for (; made < KernelMarks::kMax; ++made)
+    if (cudaEventCreate(&m.ev[made]) != cudaSuccess) break;
+  int rc = made == KernelMarks::kMax ? MHY_OK : fail(MHY_ERR_CUDA, "event");
+  if (rc == MHY_OK) launch(nullptr);
   for (int c = 0; c < cycles && rc == MHY_OK; ++c) {
     m.n = 0;
-    cudaEventRecord(start, b->stream);
-    launch_batch_cycle(b->plan, b->sens, b->stream, &m);
-    b->sens = (b->sens + 1) % 3;
-    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess) {
+    cudaEventRecord(start, stream);
+    launch(&m);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
       rc = fail(MHY_ERR_CUDA, "autotune cycle failed");
       break;
     }
@@ -759,44 +829,174 @@ int time_cycles(mhy_batch* b, int cycles, double ms[BK_TUNE_SLOTS]) {
       prev = m.ev[i];
     }
   }
-  for (int i = 0; i < KernelMarks::kMax; ++i) cudaEventDestroy(m.ev[i]);
+  for (int i = 0; i < made; ++i) cudaEventDestroy(m.ev[i]);
   cudaEventDestroy(start);
   if (rc == MHY_OK)
     for (int k = 0; k < BK_TUNE_SLOTS; ++k) ms[k] /= cycles;
   return rc;
 }
 
+// Best setting per slot: the trials are grouped by the slot's own setting
+// (order, occupancy, lines) and each group's times averaged, since trials
+// that differ only in other slots time the same kernel; trial 0 is the
+// default, and another setting must be 2 % faster.  allowed(k, i) restricts
+// the trials of slot k.
+template <class Allowed>
+void pick(const std::vector<mhy_tuning>& tr, const std::vector<std::array<double, BK_TUNE_SLOTS>>& ms, Allowed&& allowed,
+          mhy_tuning& best) {
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
+    auto same = [&](int a, int b) {
+      return tr[a].order[k] == tr[b].order[k] && tr[a].occupancy_pct[k] == tr[b].occupancy_pct[k] &&
+             tr[a].lines_per_block[k] == tr[b].lines_per_block[k];
+    };
+    auto mean = [&](int a) {
+      double sum = 0.;
+      int n = 0;
+      for (int i = 0; i < (int)tr.size(); ++i)
+        if (allowed(k, i) && same(i, a)) { sum += ms[i][k]; ++n; }
+      return n ? sum / n : ms[a][k];
+    };
+    int bi = -1;
+    double bt = 0.;
+    for (int i = 0; i < (int)tr.size(); ++i) {
+      if (!allowed(k, i)) continue;
+      bool first = true;                       // first trial of its group
+      for (int j = 0; j < i && first; ++j) first = !(allowed(k, j) && same(j, i));
+      if (!first) continue;
+      const double t = mean(i);
+      if (bi < 0 || t < 0.98 * bt) { bi = i; bt = t; }
+    }
+    if (bi < 0) { bi = 0; bt = ms[0][k]; }
+    best.order[k] = tr[bi].order[k];
+    best.occupancy_pct[k] = tr[bi].occupancy_pct[k];
+    best.lines_per_block[k] = tr[bi].lines_per_block[k];
+    best.ms_default[k] = mean(0);
+    best.ms_tuned[k] = bt;
+  }
+  best.trials = (int)tr.size();
+  best.from_cache = 0;
+}
+
 }  // namespace
 
 extern "C" {
 
-int mhy_batch_get_tuning(mhy_batch* b, mhy_batch_tuning* out) {
+int mhy_get_tuning(mhy_ctx* c, mhy_tuning* out) {
+  if (!c || !out) return fail(MHY_ERR_ARG, "null argument");
+  *out = c->tuning;
+  return MHY_OK;
+}
+
+int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
+  if (!c || !t) return fail(MHY_ERR_ARG, "null argument");
+  mhy_tuning u = *t;
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k) { u.order[k] = 0; u.occupancy_pct[k] = 100; }
+  int rc = check_tuning(u);
+  if (rc != MHY_OK) return rc;
+  if (c->K > 1)
+    for (int k = 0; k < BK_TUNE_SLOTS; ++k)
+      if (u.lines_per_block[k] != kLineWarps) return fail(MHY_ERR_UNSUPPORTED, "lines_per_block: one environment only");
+  apply_tuning(c, u);
+  c->tuning = u;
+  return MHY_OK;
+}
+
+int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
+  if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "autotune runs between cycles");
+  if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
+  if (c->K > 1) {                                   // nothing to tune: the K-plane sweeps keep 8 lines
+    c->tuning = default_tuning();
+    if (out) *out = c->tuning;
+    return MHY_OK;
+  }
+  const std::vector<mhy_ctx*> inst{c};
+  const std::string key = tune_key(inst, "ctx");
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      mhy_tuning t = it->second;
+      t.from_cache = 1;
+      apply_tuning(c, t);
+      c->tuning = t;
+      if (out) *out = t;
+      return MHY_OK;
+    }
+  }
+  Snapshot snap;
+  int rc = snap.save(inst, c->stream);
+  if (rc != MHY_OK) return rc;
+  const int sens0 = c->sens;
+  std::vector<mhy_tuning> tr;
+  for (int l = 0; l < kNL; ++l) {
+    mhy_tuning t = default_tuning();
+    for (int k = 0; k < BK_TUNE_SLOTS; ++k)
+      if (line_slot(k)) t.lines_per_block[k] = kLineOptions[l];
+    tr.push_back(t);
+  }
+  std::vector<std::array<double, BK_TUNE_SLOTS>> ms(tr.size());
+  for (size_t i = 0; i < tr.size() && rc == MHY_OK; ++i) {
+    apply_tuning(c, tr[i]);
+    rc = time_cycles(c->stream, cycles, [&](KernelMarks* m) {
+      launch_velocity(c);
+      mark(m, BK_LNODES, c->stream);
+      launch_geometry(c);
+      mark(m, BK_LCELLS, c->stream);
+      launch_remap(c->args(), c->sens, c->stream, m);
+      launch_delta_t_(c);
+      mark(m, BK_DT_FINISH, c->stream);
+      c->sens = (c->sens + 1) % 3;
+    }, ms[i].data());
+  }
+  const int rr = snap.copy(inst, c->stream, false);
+  c->sens = sens0;
+  if (rc == MHY_OK) rc = rr;
+  if (rc != MHY_OK) {
+    apply_tuning(c, c->tuning);
+    return rc;
+  }
+  mhy_tuning best = default_tuning();
+  pick(tr, ms, [](int, int) { return true; }, best);
+  apply_tuning(c, best);
+  c->tuning = best;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  if (out) *out = best;
+  return MHY_OK;
+}
+
+int mhy_batch_get_tuning(mhy_batch* b, mhy_tuning* out) {
   if (!b || !out) return fail(MHY_ERR_ARG, "null argument");
   *out = b->tuning;
   return MHY_OK;
 }
 
-int mhy_batch_set_tuning(mhy_batch* b, const mhy_batch_tuning* t) {
+int mhy_batch_set_tuning(mhy_batch* b, const mhy_tuning* t) {
   if (!b || !t) return fail(MHY_ERR_ARG, "null argument");
-  mhy_batch_tuning u = *t;
+  mhy_tuning u = *t;
   u.order[BK_DT_MIN] = u.order[BK_LCELLS];
   u.order[BK_DT_FINISH] = 0;
+  u.occupancy_pct[BK_DT_FINISH] = 100;
   int rc = check_tuning(u);
   if (rc == MHY_OK) rc = apply_tuning(b, u);
   if (rc == MHY_OK) b->tuning = u;
   return rc;
 }
 
-int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_batch_tuning* out) {
+int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
   if (!b) return fail(MHY_ERR_ARG, "null batch");
   if (!b->initialized) return fail(MHY_ERR_STATE, "mhy_batch_hydro_start_init must come first");
   if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
-  const std::string key = tune_key(b);
+  const std::string key = tune_key(b->inst, "batch");
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      mhy_batch_tuning t = it->second;
+      mhy_tuning t = it->second;
       t.from_cache = 1;
       int rc = apply_tuning(b, t);
       if (rc != MHY_OK) return rc;
@@ -806,72 +1006,58 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_batch_tuning* out) {
     }
   }
   MHY_CUDA(cudaSetDevice(b->device));
-  // snapshot of every instance's device state (its arena), restored at the end
-  size_t total = 0;
-  for (const mhy_ctx* c : b->inst)
-    for (size_t x : c->alloc_bytes) total += (x + 255) & ~size_t(255);
-  char* snap = nullptr;
-  if (cudaMalloc(&snap, total) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(MHY_ERR_OOM, "autotune: no device memory for the state snapshot");
-  }
   MHY_CUDA(cudaStreamSynchronize(b->stream));
-  {
-    size_t off = 0;
-    for (const mhy_ctx* c : b->inst)
-      for (size_t a = 0; a < c->allocs.size(); ++a) {
-        MHY_CUDA(cudaMemcpyAsync(snap + off, c->allocs[a], c->alloc_bytes[a], cudaMemcpyDeviceToDevice, b->stream));
-        off += (c->alloc_bytes[a] + 255) & ~size_t(255);
-      }
-  }
+  Snapshot snap;
+  int rc = snap.save(b->inst, b->stream);
+  if (rc != MHY_OK) return rc;
   const int sens0 = b->sens;
-  const mhy_batch_tuning before = b->tuning;
-  // trials: every (order, occupancy) setting on every slot at once
-  constexpr int kNP = sizeof(kTunePcts) / sizeof(kTunePcts[0]);
-  double ms[kTuneOrders][kNP][BK_TUNE_SLOTS];
-  int rc = MHY_OK;
-  for (int o = 0; o < kTuneOrders && rc == MHY_OK; ++o)
-    for (int q = 0; q < kNP && rc == MHY_OK; ++q) {
-      mhy_batch_tuning t{};
-      for (int k = 0; k < BK_TUNE_SLOTS; ++k) { t.order[k] = o; t.occupancy_pct[k] = kTunePcts[q]; }
-      rc = apply_tuning(b, t);
-      if (rc == MHY_OK) rc = time_cycles(b, cycles, ms[o][q]);
-    }
-  mhy_batch_tuning best{};
-  if (rc == MHY_OK) {
-    for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
-      int bo = 0, bq = 0;
-      const int o_lo = k == BK_DT_MIN ? best.order[BK_LCELLS] : 0;   // the dt reduction walks slot 1's table
-      const int o_hi = k == BK_DT_MIN ? o_lo + 1 : (k == BK_DT_FINISH ? 1 : kTuneOrders);
-      bo = o_lo;
-      for (int o = o_lo; o < o_hi; ++o)
-        for (int q = 0; q < (k == BK_DT_FINISH ? 1 : kNP); ++q)
-          if (ms[o][q][k] < 0.98 * ms[bo][bq][k]) { bo = o; bq = q; }
-      best.order[k] = bo;
-      best.occupancy_pct[k] = kTunePcts[bq];
-      best.ms_default[k] = ms[0][0][k];
-      best.ms_tuned[k] = ms[bo][bq][k];
-    }
-    best.trials = kTuneOrders * kNP;
-    best.from_cache = 0;
-  }
-  // restore the state and the rotation of the sweep directions
-  {
-    size_t off = 0;
-    for (const mhy_ctx* c : b->inst)
-      for (size_t a = 0; a < c->allocs.size(); ++a) {
-        cudaMemcpyAsync(c->allocs[a], snap + off, c->alloc_bytes[a], cudaMemcpyDeviceToDevice, b->stream);
-        off += (c->alloc_bytes[a] + 255) & ~size_t(255);
+  const mhy_tuning before = b->tuning;
+  // trials: every (order, occupancy, lines) setting on every slot at once
+  std::vector<mhy_tuning> tr;
+  for (int o = 0; o < kTuneOrders; ++o)
+    for (int q = 0; q < kNP; ++q)
+      for (int l = 0; l < kNL; ++l) {
+        mhy_tuning t = default_tuning();
+        for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
+          if (k != BK_DT_FINISH) { t.order[k] = o; t.occupancy_pct[k] = kTunePcts[q]; }
+          if (line_slot(k)) t.lines_per_block[k] = kLineOptions[l];
+        }
+        tr.push_back(t);
       }
+  std::vector<std::array<double, BK_TUNE_SLOTS>> ms(tr.size());
+  for (size_t i = 0; i < tr.size() && rc == MHY_OK; ++i) {
+    rc = apply_tuning(b, tr[i]);
+    if (rc == MHY_OK)
+      rc = time_cycles(b->stream, cycles, [&](KernelMarks* m) {
+        launch_batch_cycle(b->plan, b->sens, b->stream, m);
+        b->sens = (b->sens + 1) % 3;
+      }, ms[i].data());
   }
-  const cudaError_t se = cudaStreamSynchronize(b->stream);
-  cudaFree(snap);
+  const int rr = snap.copy(b->inst, b->stream, false);
   b->sens = sens0;
   for (mhy_ctx* c : b->inst) c->sens = b->sens;
-  if (se != cudaSuccess && rc == MHY_OK) rc = fail(MHY_ERR_CUDA, cudaGetErrorString(se));
+  if (rc == MHY_OK) rc = rr;
   if (rc != MHY_OK) {
     apply_tuning(b, before);
     return rc;
+  }
+  mhy_tuning best = default_tuning();
+  // slots 0-7 pick freely; the dt reduction only among the trials that ran
+  // slot 1's chosen order (it walks that table); the dt finish keeps the default
+  pick(tr, ms, [&](int k, int i) {
+    if (k == BK_DT_FINISH) return i == 0;
+    if (k == BK_DT_MIN) return tr[i].order[BK_LCELLS] == tr[0].order[BK_LCELLS];
+    return true;
+  }, best);
+  {
+    // the dt reduction walks slot 1's table: among the trials with slot 1's
+    // chosen order, its best occupancy
+    mhy_tuning dt = default_tuning();
+    const int o1 = best.order[BK_LCELLS];
+    pick(tr, ms, [&](int k, int i) { return k != BK_DT_MIN || tr[i].order[BK_LCELLS] == o1; }, dt);
+    best.order[BK_DT_MIN] = o1;
+    best.occupancy_pct[BK_DT_MIN] = dt.occupancy_pct[BK_DT_MIN];
+    best.ms_tuned[BK_DT_MIN] = dt.ms_tuned[BK_DT_MIN];
   }
   rc = apply_tuning(b, best);
   if (rc != MHY_OK) return rc;

@@ -131,21 +131,29 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_c
 // Cell sweep along y (D = 1) or z (D = 2), staged through shared memory.
 // Block (bx, by, bz): x = 8 bx .. 8 bx + 7, positions 28 by - 2 .. 28 by + 29
 // along D, and bz = the remaining coordinate (z for D = 1, y for D = 2).
-template <int D, bool LAST, typename R>
+template <bool LAST, int W>
+struct CellTileSize {
+  static constexpr int NA = LAST ? 17 : 16;           // staged input arrays
+  static constexpr size_t bytes = (size_t)NA * TileGeom<W>::arr * sizeof(double);
+};
+
+template <int D, bool LAST, typename R, int W>
 __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st,
     int bx_, int by_, int bz_) {
-  constexpr int NA = LAST ? 17 : 16;                  // staged input arrays
-  __shared__ double tile[NA * kTileArr];
+  constexpr int NA = CellTileSize<LAST, W>::NA;
+  constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
+  extern __shared__ double smem_dyn[];
+  double* tile = smem_dyn;                            // [NA][W][ld]
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = bx_ * kLineWarps, seg0 = by_ * kLineUpd - 2, o = bz_;
+  const int i0 = bx_ * W, seg0 = by_ * kLineUpd - 2, o = bz_;
   const int nd = dm.ncd(D), C = (int)dm.C, F = (int)dm.F;
   const int foff = D == 1 ? (int)dm.Fx : (int)(dm.Fx + dm.Fy);
   const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;   // back / front faces of d in cell-face order
   // thread (x, p) of the staging layout; also used for the stores at the end
-  const int sx = tid & 7, sp = tid >> 3;
+  const int sx = tid % W, sp = tid / W;
   const int si = i0 + sx, ss = seg0 + sp;
   const bool s_valid = si < dm.nx && ss >= 0 && ss < nd;
   const int sc = D == 1 ? si + dm.nx * (ss + dm.ny * o) : si + dm.nx * (o + dm.ny * ss);
@@ -206,31 +214,61 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool LAST, typename R>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
+template <int D, bool LAST, typename R, int W>
+__global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_t_body<D, LAST, R>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_cells_t_body<D, LAST, R, W>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+void smem_opt_in(const void* kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& have = done[std::make_pair(kernel, dev)];
+  if (have >= bytes) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  have = bytes;
 }
 
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
+template <int D, bool LAST, typename R, int W>
+static void sweep_cells_t_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+  const Dims& dm = a.dm;
+  const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
+  const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
+  const size_t smem = CellTileSize<LAST, W>::bytes;
+  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W>;
+  smem_opt_in((const void*)kern, smem);
+  kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+}
+
+template <int D, bool LAST, typename R>
+static void sweep_cells_t(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+  const int w = a.lines[BK_CELLS_X + D];
+  if (w == 32) sweep_cells_t_w<D, LAST, R, 32>(a, Uin, Uout, s);
+  else if (w == 16) sweep_cells_t_w<D, LAST, R, 16>(a, Uin, Uout, s);
+  else sweep_cells_t_w<D, LAST, R, 8>(a, Uin, Uout, s);
+}
+
 template <int D, typename R>
 static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
-  const int bx = (dm.nx + kLineWarps - 1) / kLineWarps;
   const int T = 32 * kLineWarps;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
     if (last) k_cyc_sweep_cells_x<true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
     else k_cyc_sweep_cells_x<false, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
   } else {
-    const dim3 g(bx, nseg, D == 1 ? dm.nz : dm.ny);
-    if (last) k_cyc_sweep_cells_t<D, true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-    else k_cyc_sweep_cells_t<D, false, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    if (last) sweep_cells_t<D, true, R>(a, Uin, Uout, s);
+    else sweep_cells_t<D, false, R>(a, Uin, Uout, s);
   }
 }
 
@@ -268,7 +306,7 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
 // U_dual: the first sweep builds it from the Lagrange velocity and writes
 // ud[0]; then ud[0] -> ud[1]; the last one writes the node velocity and mass.
 template <typename R>
-static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s) {
+static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
@@ -280,14 +318,16 @@ static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s) {
     if (d == 0) sweep_cells_d<0, R>(a, last, uin, uout, s);
     else if (d == 1) sweep_cells_d<1, R>(a, last, uin, uout, s);
     else sweep_cells_d<2, R>(a, last, uin, uout, s);
+    mark(m, BK_CELLS_X + d, s);
     sweep_nodes<1, R>(a, d, first, last, prev, udin, udout, s);
+    mark(m, BK_NODES_X + d, s);
     prev |= 1 << d;
   }
 }
 
-void launch_remap(const CycleArgs& a, int sens, cudaStream_t s) {
-  if (a.ph.precision) remap_impl<float>(a, sens, s);
-  else remap_impl<double>(a, sens, s);
+void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
+  if (a.ph.precision) remap_impl<float>(a, sens, s, m);
+  else remap_impl<double>(a, sens, s, m);
 }
 
 void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
@@ -303,9 +343,10 @@ void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
 // work item with a barrier, since the previous item's last reads of the tile
 // may still be in flight in other warps.
 
-void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz) {
+void batch_work_shape(const Dims& dm, int kind, int lines, int& gx, int& gy, int& gz) {
   const int nx = dm.nx, ny = dm.ny, nz = dm.nz;
   auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
+  const int W = lines;                            // lines per block of the y/z sweeps
   switch (kind) {
     case BK_LNODES: gx = (int)cdiv((int)dm.N, 128); gy = -1; gz = 1; break;      // linear chunks
     case BK_LCELLS:
@@ -313,11 +354,11 @@ void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz) {
       else { gx = nx / 128; gy = ny; gz = nz; }
       break;
     case BK_CELLS_X: gx = cdiv(nx, kLineUpd); gy = cdiv(ny, kLineWarps); gz = nz; break;
-    case BK_CELLS_Y: gx = cdiv(nx, kLineWarps); gy = cdiv(ny, kLineUpd); gz = nz; break;
-    case BK_CELLS_Z: gx = cdiv(nx, kLineWarps); gy = cdiv(nz, kLineUpd); gz = ny; break;
+    case BK_CELLS_Y: gx = cdiv(nx, W); gy = cdiv(ny, kLineUpd); gz = nz; break;
+    case BK_CELLS_Z: gx = cdiv(nx, W); gy = cdiv(nz, kLineUpd); gz = ny; break;
     case BK_NODES_X: gx = cdiv(nx + 1, kLineUpd); gy = cdiv(ny + 1, kLineWarps); gz = nz + 1; break;
-    case BK_NODES_Y: gx = cdiv(nx + 1, kLineWarps); gy = cdiv(ny + 1, kLineUpd); gz = nz + 1; break;
-    default: gx = cdiv(nx + 1, kLineWarps); gy = cdiv(nz + 1, kLineUpd); gz = ny + 1; break;
+    case BK_NODES_Y: gx = cdiv(nx + 1, W); gy = cdiv(ny + 1, kLineUpd); gz = nz + 1; break;
+    default: gx = cdiv(nx + 1, W); gy = cdiv(nz + 1, kLineUpd); gz = ny + 1; break;
   }
 }
 
@@ -356,15 +397,15 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_c
   }
 }
 
-template <int DD, bool LAST, typename R>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_t(
+template <int DD, bool LAST, typename R, int LW>
+__global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_cells_t_body<DD, LAST, R>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
-                                       a.dpf, a.st, t.y, t.z, t.w);
+    k_cyc_sweep_cells_t_body<DD, LAST, R, LW>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+                                           a.dpf, a.st, t.y, t.z, t.w);
   }
 }
 
@@ -379,16 +420,16 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_n
   }
 }
 
-template <int DD, bool FIRST, bool LAST, typename R>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_nodes_t(
+template <int DD, bool FIRST, bool LAST, typename R, int LW>
+__global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_nodes_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
-                                                 a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y,
-                                                 t.z, t.w);
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+                                                     a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y,
+                                                     t.z, t.w);
   }
 }
 
@@ -411,7 +452,7 @@ __global__ void k_bat_dt_finish(const CycleArgs* __restrict__ D, int n) {
 // Resident blocks of a persistent grid for `kernel`: SMs x blocks per SM
 // (queried once per kernel and device), scaled by pct percent.
 template <class Kern>
-static int persistent_blocks(Kern kernel, int threads, int nwork, int pct) {
+static int persistent_blocks(Kern kernel, int threads, size_t smem, int nwork, int pct) {
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, int> cache;
   int dev = 0;
@@ -424,7 +465,7 @@ static int persistent_blocks(Kern kernel, int threads, int nwork, int pct) {
     if (itc == cache.end()) {
       int sms = 0, per = 0;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
       itc = cache.emplace(key, (per > 0 ? per : 1) * (sms > 0 ? sms : 1)).first;
     }
     g = itc->second;
@@ -434,7 +475,7 @@ static int persistent_blocks(Kern kernel, int threads, int nwork, int pct) {
   return nwork < g ? (nwork > 0 ? nwork : 1) : g;
 }
 
-static void mark(KernelMarks* m, int kind, cudaStream_t s) {
+void mark(KernelMarks* m, int kind, cudaStream_t s) {
   if (!m || m->n >= KernelMarks::kMax) return;
   cudaEventRecord(m->ev[m->n], s);
   m->kind[m->n++] = kind;
@@ -443,28 +484,54 @@ static void mark(KernelMarks* m, int kind, cudaStream_t s) {
 // One persistent launch over the work table of `kind`; tk is the tuning slot
 // (grid percentage and timing mark): the kind itself, or BK_DT_MIN.
 template <class Kern, class... Args>
-static void launch_persistent(Kern kernel, int threads, const BatchPlan& P, int kind, int tk, cudaStream_t s,
-                              KernelMarks* marks, Args... args) {
+static void launch_persistent(Kern kernel, int threads, size_t smem, const BatchPlan& P, int kind, int tk,
+                              cudaStream_t s, KernelMarks* marks, Args... args) {
   const int nwork = P.nwork[kind];
-  if (nwork > 0) kernel<<<persistent_blocks(kernel, threads, nwork, P.occ_pct[tk]), threads, 0, s>>>(args...);
+  smem_opt_in((const void*)kernel, smem);
+  if (nwork > 0) kernel<<<persistent_blocks(kernel, threads, smem, nwork, P.occ_pct[tk]), threads, smem, s>>>(args...);
   mark(marks, tk, s);
+}
+
+template <int DD, bool LAST, typename R, int LW>
+static void bat_cells_t(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
+  const int kind = BK_CELLS_X + DD;
+  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW>, 32 * LW, CellTileSize<LAST, LW>::bytes, P, kind, kind, s, m,
+                    P.descs, P.work[kind], P.nwork[kind], it);
 }
 
 template <int DD, bool LAST, typename R>
 static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
-  const int T = 32 * kLineWarps, kind = BK_CELLS_X + DD;
-  if constexpr (DD == 0) launch_persistent(k_bat_sweep_cells_x<LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it);
-  else launch_persistent(k_bat_sweep_cells_t<DD, LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it);
+  const int kind = BK_CELLS_X + DD;
+  if constexpr (DD == 0) {
+    launch_persistent(k_bat_sweep_cells_x<LAST, R>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs, P.work[kind],
+                      P.nwork[kind], it);
+  } else {
+    const int w = P.lines[kind];
+    if (w == 32) bat_cells_t<DD, LAST, R, 32>(P, it, s, m);
+    else if (w == 16) bat_cells_t<DD, LAST, R, 16>(P, it, s, m);
+    else bat_cells_t<DD, LAST, R, 8>(P, it, s, m);
+  }
+}
+
+template <int DD, bool FIRST, bool LAST, typename R, int LW>
+static void bat_nodes_t(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
+  const int kind = BK_NODES_X + DD;
+  launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R, LW>, 32 * LW, NodeTileSize<DD, FIRST, LAST, 1, LW>::bytes,
+                    P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it, prev);
 }
 
 template <int DD, bool FIRST, bool LAST, typename R>
 static void bat_nodes_d(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
-  const int T = 32 * kLineWarps, kind = BK_NODES_X + DD;
-  if constexpr (DD == 0)
-    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it, prev);
-  else
-    launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R>, T, P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it,
-                      prev);
+  const int kind = BK_NODES_X + DD;
+  if constexpr (DD == 0) {
+    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
+                      P.work[kind], P.nwork[kind], it, prev);
+  } else {
+    const int w = P.lines[kind];
+    if (w == 32) bat_nodes_t<DD, FIRST, LAST, R, 32>(P, it, prev, s, m);
+    else if (w == 16) bat_nodes_t<DD, FIRST, LAST, R, 16>(P, it, prev, s, m);
+    else bat_nodes_t<DD, FIRST, LAST, R, 8>(P, it, prev, s, m);
+  }
 }
 
 template <int DD, typename R>
@@ -479,11 +546,11 @@ static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s, Kern
 
 void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
   if (P.precision) {
-    launch_persistent(k_bat_lagrange_nodes<float>, 128, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
-    launch_persistent(k_bat_lagrange_cells<float>, 128, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+    launch_persistent(k_bat_lagrange_nodes<float>, 128, 0, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+    launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   } else {
-    launch_persistent(k_bat_lagrange_nodes<double>, 128, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
-    launch_persistent(k_bat_lagrange_cells<double>, 128, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+    launch_persistent(k_bat_lagrange_nodes<double>, 128, 0, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+    launch_persistent(k_bat_lagrange_cells<double>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   }
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
@@ -500,7 +567,7 @@ void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMark
     prev |= 1 << d;
   }
   // the dt reduction walks the cell tiles of the Lagrange cell kernel
-  launch_persistent(k_bat_dt_min, 128, P, BK_LCELLS, BK_DT_MIN, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  launch_persistent(k_bat_dt_min, 128, 0, P, BK_LCELLS, BK_DT_MIN, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   k_bat_dt_finish<<<(P.ninst + 127) / 128, 128, 0, s>>>(P.descs, P.ninst);
   mark(m, BK_DT_FINISH, s);
 }

@@ -85,11 +85,13 @@ struct CycleArgs {
   int K;                // number of environments
   EnvState env;         // K > 1 only
   double* Vlag;         // Lagrangian cell volume (K > 1: divisor of Phi on the first sweep)
+  int lines[8];         // lines per block of each sweep (indexed like BatchKernel; y/z sweeps of K = 1: 8, 16, 32)
 };
 
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s);
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s);
-void launch_remap(const CycleArgs& a, int sens, cudaStream_t s);
+struct KernelMarks;
+void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 void launch_delta_t(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycle = 10;
 // meshes with 2..kMaxEnvDevice environments (mhy_multi.cu)
@@ -103,6 +105,8 @@ constexpr int kKernelsPerCycleEnv = 11;
 // type has a work table: one (instance, bx, by, bz) entry per block of the
 // instance's own grid; a persistent grid of resident blocks walks the table.
 // The arguments of instance i are descs[i] in device memory.
+constexpr int kLineWarps = 8;                   // warps (lines) per block of the sweeps (default)
+constexpr int kLineOptions[3] = {8, 16, 32};    // the y/z sweeps' tunable lines per block
 enum BatchKernel { BK_LNODES = 0, BK_LCELLS, BK_CELLS_X, BK_CELLS_Y, BK_CELLS_Z, BK_NODES_X, BK_NODES_Y, BK_NODES_Z,
                    BK_COUNT,
                    BK_DT_MIN = BK_COUNT,      // tuning slots beyond the work tables: the dt reduction (cell
@@ -115,6 +119,7 @@ struct BatchPlan {
   int nwork[BK_COUNT];
   int precision;                // all instances share it
   int occ_pct[BK_TUNE_SLOTS];   // persistent grid of each slot: % of the resident-block capacity
+  int lines[BK_COUNT];          // lines per block of the y/z sweeps (8, 16, 32); the work shapes follow it
 };
 // Events recorded after each launch of a cycle (autotuning), with the tuning
 // slot of each launch.
@@ -124,7 +129,9 @@ struct KernelMarks {
   int kind[kMax];
   int n;
 };
-void batch_work_shape(const Dims& dm, int kind, int& gx, int& gy, int& gz);
+void batch_work_shape(const Dims& dm, int kind, int lines, int& gx, int& gy, int& gz);
+// Records an event after a launch (autotuning): slot `kind` of the marks.
+void mark(KernelMarks* m, int kind, cudaStream_t s);
 void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 constexpr int kKernelsPerCycleBatch = 10;
 

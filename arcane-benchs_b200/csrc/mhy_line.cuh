@@ -25,7 +25,6 @@ namespace mhy {
 // element offset fits).
 
 constexpr int kLineUpd = 28;    // items updated per warp (32 lanes, 2 halo lanes on each side)
-constexpr int kLineWarps = 8;   // warps (lines) per block
 // The sweeps are latency bound (long dependent chains of divisions and
 // shuffles per lane); 4 resident blocks (32 warps, 64 registers, a few bytes
 // of spill) per SM run them 15 % faster than the 2-3 blocks the compiler's
@@ -37,6 +36,21 @@ constexpr int kLineMinBlocks = 4;
 // and line reads run along p, so both are free of bank conflicts.
 constexpr int kTileLd = 36;
 constexpr int kTileArr = kLineWarps * kTileLd;   // doubles per staged array
+
+// The y/z sweeps take the number of lines per block W (8, 16 or 32) as a
+// tuning parameter: a block stages W consecutive x of 32 positions, so each
+// row of its loads and stores spans W doubles (64, 128 or 256 contiguous
+// bytes).  Row length ld: for W = 8 the 36 above; for W >= 16 staging stores
+// by thread (x = tid % W, p = tid / W) hit 33 x + p, whose 8-byte bank pairs
+// (x + p) mod 16 take every pair twice per warp, and line reads run along p.
+// Every W keeps 64 registers a thread: 32 / W resident blocks of 32 W threads.
+template <int W> struct TileGeom {
+  static_assert(W == 8 || W == 16 || W == 32, "lines per block");
+  static constexpr int ld = W == 8 ? kTileLd : 33;
+  static constexpr int arr = W * ld;                 // doubles per staged array
+  static constexpr int minb = 32 / W;                // resident blocks at 64 registers
+  static constexpr int cld = W == 8 ? 32 : 33;       // row length of a node sweep's cell tile
+};
 
 // remapVariables "moy" kernel for a single-environment cell and the PerfectGas
 // EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
@@ -469,25 +483,34 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
 // o - 1 .. o along the remaining axis: their dual mass fluxes (and masses on
 // the last sweep) are staged as [o - 1 + q][x - 8 bx + 1][position], with zero
 // for cells outside the mesh (adding +0 to these sums changes no bit).
-template <int D, bool FIRST, bool LAST, int K, typename R>
+template <int D, bool FIRST, bool LAST, int K, int W>
+struct NodeTileSize {
+  static constexpr int NA = FIRST ? 5 : 9;                   // vh x3, x0[D], nm or U_dual x5
+  static constexpr int NT = LAST ? K + 1 : K;                // cell tiles: dual mass flux per environment (+ mass)
+  static constexpr int CT = 2 * (W + 1) * TileGeom<W>::cld;  // elements of one cell tile
+  static constexpr size_t bytes = (size_t)(NA * TileGeom<W>::arr + NT * CT) * sizeof(double);
+};
+
+template <int D, bool FIRST, bool LAST, int K, typename R, int W = kLineWarps>
 __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
     int bx_, int by_, int bz_) {
-  constexpr int NA = FIRST ? 5 : 9;                   // vh x3, x0[D], nm or U_dual x5
-  constexpr int NT = LAST ? K + 1 : K;                // cell tiles: dual mass flux per environment (+ mass)
-  constexpr int CT = 2 * (kLineWarps + 1) * 32;       // elements of one cell tile
-  constexpr int CLd = 32;                             // row length of a cell tile
-  __shared__ double tile[NA * kTileArr];
-  __shared__ double ctile[NT * CT];
+  using TS = NodeTileSize<D, FIRST, LAST, K, W>;
+  constexpr int NA = TS::NA, CT = TS::CT;
+  constexpr int CLd = TileGeom<W>::cld;               // row length of a cell tile
+  constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
+  extern __shared__ double smem_dyn[];
+  double* tile = smem_dyn;                            // [NA][W][ld]
+  double* ctile = smem_dyn + NA * kTileArr;           // [NT][2][W + 1][cld]
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = bx_ * kLineWarps, seg0 = by_ * kLineUpd - 2, o = bz_;
+  const int i0 = bx_ * W, seg0 = by_ * kLineUpd - 2, o = bz_;
   const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
   const int nn = dm.ncd(D) + 1, no = D == 1 ? nz : ny;   // cells along D; cells along the remaining axis
   auto node_id = [&](int i, int m) { return D == 1 ? i + (nx + 1) * (m + (ny + 1) * o) : i + (nx + 1) * (o + (ny + 1) * m); };
-  const int sx = tid & 7, sp = tid >> 3;
+  const int sx = tid % W, sp = tid / W;
   const int si = i0 + sx, sm_ = seg0 + sp;
   const bool s_valid = si <= nx && sm_ >= 0 && sm_ < nn;
   const int sn = s_valid ? node_id(si, sm_) : 0;
@@ -506,13 +529,13 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
 #pragma unroll
     for (int a = 0; a < NA; ++a) tile[a * kTileArr + sx * kTileLd + sp] = v[a];
     // cell tiles: element e = (q * 9 + xx) * 32 + p, loaded with xx fastest
-    for (int e = tid; e < CT; e += 32 * kLineWarps) {
-      const int xx = e % (kLineWarps + 1), r = e / (kLineWarps + 1);
+    for (int e = tid; e < 2 * (W + 1) * 32; e += 32 * W) {
+      const int xx = e % (W + 1), r = e / (W + 1);
       const int p = r & 31, q = r >> 5;
       const int ci = i0 - 1 + xx, cd = seg0 + p, co = o - 1 + q;
       const bool cv = ci >= 0 && ci < nx && cd >= 0 && cd < nn - 1 && co >= 0 && co < no;
       const int c = D == 1 ? ci + nx * (cd + ny * co) : ci + nx * (co + ny * cd);
-      const int at = (q * (kLineWarps + 1) + xx) * CLd + p;
+      const int at = (q * (W + 1) + xx) * CLd + p;
 #pragma unroll
       for (int q2 = 0; q2 < K; ++q2) ctile[q2 * CT + at] = cv ? dpf[q2 * (int)dm.C + c] : 0.;
       if (LAST) ctile[K * CT + at] = cv ? mass[c] : 0.;
@@ -537,7 +560,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   // cells in front of the node along D have index m along D; transverse
   // (x - 1, x) = columns (w, w + 1) and (o - 1, o) = tile rows (0, 1)
   const double* cr = ctile + w * CLd + lane;
-  constexpr int QS = (kLineWarps + 1) * CLd;          // stride between the two tile rows
+  constexpr int QS = (W + 1) * CLd;                   // stride between the two tile rows
   // DualPhaseRemap.cc:299-340 order: s1 over d1 = (D+1)%3, s2 over d2 = (D+2)%3,
   // environments innermost.  D = 1: s1 over z (q), s2 over x; D = 2: s1 over
   // x, s2 over y (q).  Tile offsets of the cells (q, dx): q * QS + dx * CLd.
@@ -591,17 +614,33 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool FIRST, bool LAST, int K, typename R>
-__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
+template <int D, bool FIRST, bool LAST, int K, typename R, int W>
+__global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------------
 // Host-side node sweep launchers.
+
+// Dynamic shared memory above the default 48 KB needs an opt-in per kernel and device.
+void smem_opt_in(const void* kernel, size_t bytes);
+
+template <int D, bool FIRST, bool LAST, int K, typename R, int W>
+static void sweep_nodes_launch_w(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
+  const Dims& dm = a.dm;
+  const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
+  const dim3 g((dm.nx + 1 + W - 1) / W, nseg, (D == 1 ? dm.nz : dm.ny) + 1);
+  const size_t smem = NodeTileSize<D, FIRST, LAST, K, W>::bytes;
+  auto kern = k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R, W>;
+  smem_opt_in((const void*)kern, smem);
+  kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm,
+                               a.vnorm);
+}
+
 template <int D, bool FIRST, bool LAST, int K, typename R>
 static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
   const Dims& dm = a.dm;
@@ -612,9 +651,11 @@ static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin,
     k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd,
                                                      a.st.mass, a.v, a.nm, a.vnorm);
   } else {
-    const dim3 g((dm.nx + 1 + kLineWarps - 1) / kLineWarps, nseg, (D == 1 ? dm.nz : dm.ny) + 1);
-    k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf,
-                                                        a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+    // lines per block of this sweep (the tuning; K > 1 meshes keep 8)
+    const int w = K == 1 ? a.lines[BK_NODES_X + D] : kLineWarps;
+    if (w == 32) sweep_nodes_launch_w<D, FIRST, LAST, K, R, 32>(a, prev, udin, udout, s);
+    else if (w == 16) sweep_nodes_launch_w<D, FIRST, LAST, K, R, 16>(a, prev, udin, udout, s);
+    else sweep_nodes_launch_w<D, FIRST, LAST, K, R, 8>(a, prev, udin, udout, s);
   }
 }
 

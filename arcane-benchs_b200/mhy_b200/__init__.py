@@ -37,8 +37,8 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_batch_step", "mhy_batch_synchronize", "mhy_batch_get_field", "mhy_batch_get_dt",
             "mhy_batch_get_status", "mhy_batch_size", "mhy_batch_kernels_per_cycle", "mhy_batch_get_stream",
             "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load",
-            "mhy_get_totals", "mhy_batch_get_totals", "mhy_batch_autotune", "mhy_batch_set_tuning",
-            "mhy_batch_get_tuning"]
+            "mhy_get_totals", "mhy_batch_get_totals", "mhy_autotune", "mhy_set_tuning", "mhy_get_tuning",
+            "mhy_batch_autotune", "mhy_batch_set_tuning", "mhy_batch_get_tuning"]
 MHY_TUNE_SLOTS = 10
 TUNE_SLOTS = ("lagrange_nodes", "lagrange_cells", "cells_x", "cells_y", "cells_z", "nodes_x", "nodes_y", "nodes_z",
               "dt_min", "dt_finish")
@@ -57,12 +57,23 @@ class BC(ctypes.Structure):
 
 
 class CTuning(ctypes.Structure):
+    """mhy_tuning: per kernel slot (TUNE_SLOTS) the work order and grid
+    percentage (batches) and the lines per block of the y/z sweeps."""
     _fields_ = [("order", ctypes.c_int32 * MHY_TUNE_SLOTS), ("occupancy_pct", ctypes.c_int32 * MHY_TUNE_SLOTS),
+                ("lines_per_block", ctypes.c_int32 * MHY_TUNE_SLOTS),
                 ("ms_default", ctypes.c_double * MHY_TUNE_SLOTS), ("ms_tuned", ctypes.c_double * MHY_TUNE_SLOTS),
                 ("from_cache", ctypes.c_int32), ("trials", ctypes.c_int32)]
 
+    @classmethod
+    def default(cls) -> "CTuning":
+        t = cls()
+        for k in range(MHY_TUNE_SLOTS):
+            t.order[k], t.occupancy_pct[k], t.lines_per_block[k] = 0, 100, 8
+        return t
+
     def as_dict(self) -> dict:
         return {"slots": {name: {"order": self.order[k], "occupancy_pct": self.occupancy_pct[k],
+                                 "lines_per_block": self.lines_per_block[k],
                                  "ms_default": round(self.ms_default[k], 4), "ms_tuned": round(self.ms_tuned[k], 4)}
                           for k, name in enumerate(TUNE_SLOTS)},
                 "from_cache": bool(self.from_cache), "trials": self.trials}
@@ -143,6 +154,9 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_batch_destroy.argtypes = [vp]
     L.mhy_batch_destroy.restype = None
     L.mhy_get_totals.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.mhy_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CTuning)]
+    L.mhy_set_tuning.argtypes = [vp, ctypes.POINTER(CTuning)]
+    L.mhy_get_tuning.argtypes = [vp, ctypes.POINTER(CTuning)]
     L.mhy_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CTuning)]
     L.mhy_batch_set_tuning.argtypes = [vp, ctypes.POINTER(CTuning)]
     L.mhy_batch_get_tuning.argtypes = [vp, ctypes.POINTER(CTuning)]
@@ -239,6 +253,21 @@ class Context:
         f = ctypes.c_uint32()
         _check(load().mhy_get_status(self.h, ctypes.byref(f)))
         return f.value
+
+    def autotune(self, cycles: int = 2) -> CTuning:
+        """mhy_autotune: lines per block of the y/z sweeps, timed on this
+        context's state (restored afterwards)."""
+        t = CTuning()
+        _check(load().mhy_autotune(self.h, int(cycles), ctypes.byref(t)))
+        return t
+
+    def tuning(self) -> CTuning:
+        t = CTuning()
+        _check(load().mhy_get_tuning(self.h, ctypes.byref(t)))
+        return t
+
+    def set_tuning(self, t: CTuning):
+        _check(load().mhy_set_tuning(self.h, ctypes.byref(t)))
 
     def totals(self) -> dict:
         """Compensated device sums: mass, internal, kinetic and total energy."""
@@ -359,8 +388,9 @@ class Batch:
         return f.value
 
     def autotune(self, cycles: int = 2) -> CTuning:
-        """mhy_batch_autotune: the fastest work order and persistent grid per
-        kernel slot, timed on this batch's state (restored afterwards)."""
+        """mhy_batch_autotune: the fastest work order, persistent grid and
+        lines per block per kernel slot, timed on this batch's state (restored
+        afterwards)."""
         t = CTuning()
         _check(load().mhy_batch_autotune(self.h, int(cycles), ctypes.byref(t)))
         return t

@@ -217,35 +217,42 @@ int mhy_batch_get_dt(mhy_batch* b, int i, double* dt, double* dt_old);
 int mhy_batch_get_status(mhy_batch* b, int i, uint32_t* flags);
 int mhy_batch_get_totals(mhy_batch* b, int i, double out[3]);
 
-/* Tuning of the batched cycle: per kernel slot, the order of its work table
- * and the size of its persistent grid.  Slots: 0 Lagrange nodes, 1 Lagrange
- * cells, 2-4 cell sweeps x/y/z, 5-7 node sweeps x/y/z, 8 dt reduction (walks
- * the work table of slot 1, so its order is slot 1's), 9 per-instance dt
- * finish (one thread per instance; nothing to tune).  Results do not depend on
- * the tuning: every work item computes the same values whatever its order or
- * the grid that runs it. */
+/* Tuning of the cycle: per kernel slot, the lines per block of the staged
+ * y/z sweeps and, in a batch, the order of the work table and the size of the
+ * persistent grid.  Slots: 0 Lagrange nodes, 1 Lagrange cells, 2-4 cell
+ * sweeps x/y/z, 5-7 node sweeps x/y/z, 8 dt reduction (walks the work table
+ * of slot 1, so its order is slot 1's), 9 dt finish (nothing to tune).
+ * Results do not depend on the tuning: every work item computes the same
+ * values whatever its tile shape, its order or the grid that runs it. */
 #define MHY_TUNE_SLOTS 10
-typedef struct mhy_batch_tuning {
-  int32_t order[MHY_TUNE_SLOTS];         /* 0 instance-major (default), 1 largest instance first,
-                                            2 instances interleaved 16 tiles at a time */
-  int32_t occupancy_pct[MHY_TUNE_SLOTS]; /* persistent grid as % of the resident-block capacity, 1..100 (100) */
-  double ms_default[MHY_TUNE_SLOTS];     /* mhy_batch_autotune: measured ms per cycle of each slot with the
-                                            defaults ... */
-  double ms_tuned[MHY_TUNE_SLOTS];       /* ... and with the chosen settings */
-  int32_t from_cache;                    /* 1: taken from the in-process cache, keyed on the instances' mesh
-                                            sizes and the precision, without trials */
-  int32_t trials;                        /* settings tried */
-} mhy_batch_tuning;
+typedef struct mhy_tuning {
+  int32_t order[MHY_TUNE_SLOTS];           /* batch: 0 instance-major (default), 1 largest instance first,
+                                              2 instances interleaved 16 tiles at a time */
+  int32_t occupancy_pct[MHY_TUNE_SLOTS];   /* batch: persistent grid as % of the resident-block capacity,
+                                              1..100 (100) */
+  int32_t lines_per_block[MHY_TUNE_SLOTS]; /* slots 3, 4, 6, 7 (y/z sweeps) of one-environment meshes: 8 (default),
+                                              16 or 32 lines of 32 positions per block, i.e. rows of 64, 128 or
+                                              256 contiguous bytes in the staged loads; other slots 8 */
+  double ms_default[MHY_TUNE_SLOTS];       /* autotune: measured ms per cycle of each slot with the defaults ... */
+  double ms_tuned[MHY_TUNE_SLOTS];         /* ... and with the chosen settings */
+  int32_t from_cache;                      /* 1: taken from the in-process cache (keyed on the mesh sizes, the
+                                              number of environments and the precision) without trials */
+  int32_t trials;                          /* settings tried */
+} mhy_tuning;
 
-/* Autotuner: tries every (order, occupancy 100/75/50 %) setting on the
- * batch's own state for `cycles` timed cycles each (1..20; after
- * mhy_batch_hydro_start_init), keeps per slot the fastest (a setting must beat
- * the default by 2 %), and restores the state bit for bit afterwards (device
- * snapshot: needs free device memory the size of the batch's state).  The
- * choice is cached per set of mesh sizes and precision for the process. */
-int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_batch_tuning* out);
-int mhy_batch_set_tuning(mhy_batch* b, const mhy_batch_tuning* t);
-int mhy_batch_get_tuning(mhy_batch* b, mhy_batch_tuning* out);
+/* Autotuner: times every candidate setting on the context's (batch's) own
+ * state for `cycles` cycles each (1..20, after mhy_hydro_start_init), keeps
+ * per slot the fastest (a setting must beat the default by 2 %) and restores
+ * the state bit for bit afterwards (device snapshot: needs free device memory
+ * the size of the state).  Candidates: lines per block 8/16/32 on the y/z
+ * sweeps; in a batch also 3 work orders x occupancy 100/75/50 %.  The choice
+ * is cached for the process per set of mesh sizes. */
+int mhy_autotune(mhy_ctx* ctx, int cycles, mhy_tuning* out);
+int mhy_set_tuning(mhy_ctx* ctx, const mhy_tuning* t);
+int mhy_get_tuning(mhy_ctx* ctx, mhy_tuning* out);
+int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out);
+int mhy_batch_set_tuning(mhy_batch* b, const mhy_tuning* t);
+int mhy_batch_get_tuning(mhy_batch* b, mhy_tuning* out);
 int mhy_batch_size(mhy_batch* b);
 int mhy_batch_kernels_per_cycle(mhy_batch* b);
 void* mhy_batch_get_stream(mhy_batch* b);
