@@ -63,6 +63,7 @@ struct mhy_ctx {
   double *rho = nullptr, *e = nullptr, *q = nullptr, *p = nullptr, *cs = nullptr, *mass = nullptr;
   double *L = nullptr, *Ve = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr, *xc = nullptr;
   float* cqs32 = nullptr;
+  double *vnb = nullptr, *vf = nullptr, *xl = nullptr, *pf = nullptr;   // schema-csts
   double *U[2] = {nullptr, nullptr};
   // environments (K > 1)
   int K = 1;
@@ -115,6 +116,7 @@ struct mhy_ctx {
     a.st.rho = rho; a.st.e = e; a.st.q = q; a.st.p = p; a.st.cs = cs; a.st.mass = mass; a.st.Ve = Ve;
     a.K = K; a.env = env; a.Vlag = Vlag;
     for (int k = 0; k < BK_COUNT; ++k) a.lines[k] = lines[k];
+    a.vnb = vnb; a.vf = vf; a.xl = xl; a.pf = pf;
     return a;
   }
 };
@@ -172,6 +174,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0 (minmod), 1 (superBee) or 2 (vanLeer)");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
   if (opt->precision < 0 || opt->precision > 1) return fail(MHY_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
+  if (opt->schema_csts != 0 && opt->schema_csts != 1) return fail(MHY_ERR_ARG, "schema_csts must be 0 or 1");
+  if (opt->schema_csts && (opt->nb_env != 1 || opt->precision != 0))
+    return fail(MHY_ERR_UNSUPPORTED, "schema-csts: one environment in FP64 on the device");
   for (int b = 0; b < opt->nb_bc; ++b)
     if (opt->bc[b].surface < 0 || opt->bc[b].surface > 5 || opt->bc[b].type < 0 || opt->bc[b].type > 2)
       return fail(MHY_ERR_ARG, "bad boundary condition");
@@ -209,6 +214,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   ph.lc_mode = opt->longueur_caracteristique; ph.pseudo_centree = opt->pseudo_centree;
   ph.ordre_projection = opt->ordre_projection; ph.limiteur_id = opt->projection_limiteur_id;
   ph.precision = opt->precision;
+  ph.csts = opt->schema_csts;
   c->bct.nb = opt->nb_bc;
   for (int b = 0; b < opt->nb_bc; ++b) { c->bct.type[b] = opt->bc[b].type; c->bct.value[b] = opt->bc[b].value; }
 
@@ -224,6 +230,12 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   // converts the FP64 ones of t = 0)
   A_(&c->cqs, 24 * C);
   if (opt->precision == 1 && rc == MHY_OK) rc = c->alloc(&c->cqs32, (size_t)(24 * C));
+  if (opt->schema_csts && rc == MHY_OK) {           // backward / forward velocities, coordinates, pressure
+    rc = c->alloc(&c->vnb, (size_t)(3 * N));
+    if (rc == MHY_OK) rc = c->alloc(&c->vf, (size_t)(3 * N));
+    if (rc == MHY_OK) rc = c->alloc(&c->xl, (size_t)(3 * N));
+    if (rc == MHY_OK) rc = c->alloc(&c->pf, (size_t)C);
+  }
   A_(&c->U[0], NV * C); A_(&c->U[1], NV * C);
   if (K > 1) {
     EnvState& ev = c->env;
@@ -279,7 +291,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   err = cudaMemcpyAsync(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv : kKernelsPerCycle;
+  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv : kKernelsPerCycle + (opt->schema_csts ? 2 : 0);
   *out = c;
   return MHY_OK;
 }
@@ -401,9 +413,13 @@ int launch_geometry(mhy_ctx* c) {
   else launch_lagrange_cells_env(c->args(), c->stream);
   return MHY_OK;
 }
-int launch_remap_(mhy_ctx* c, int sens) {
-  if (c->K == 1) launch_remap(c->args(), sens, c->stream);
-  else launch_remap_env(c->args(), sens, c->stream);
+int launch_remap_(mhy_ctx* c, int sens, KernelMarks* m = nullptr) {
+  if (c->K == 1) {
+    if (c->ph.csts) launch_csts_forward(c->args(), c->stream);   // PrepareRemap.cc:456, then the face velocities
+    launch_remap(c->args(), sens, c->stream, m);
+  } else {
+    launch_remap_env(c->args(), sens, c->stream);
+  }
   return MHY_OK;
 }
 int launch_delta_t_(mhy_ctx* c) { launch_delta_t(c->args(), c->stream); return MHY_OK; }
@@ -580,6 +596,7 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   *out = nullptr;
   for (int i = 0; i < n; ++i) {
     if (opts[i].nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "batched instances must have one environment");
+    if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();
@@ -944,7 +961,7 @@ int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
       mark(m, BK_LNODES, c->stream);
       launch_geometry(c);
       mark(m, BK_LCELLS, c->stream);
-      launch_remap(c->args(), c->sens, c->stream, m);
+      launch_remap_(c, c->sens, m);
       launch_delta_t_(c);
       mark(m, BK_DT_FINISH, c->stream);
       c->sens = (c->sens + 1) % 3;

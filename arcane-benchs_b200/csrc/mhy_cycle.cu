@@ -26,16 +26,13 @@ namespace mhy {
 // ------------------------------------------------------------------------
 // Lagrange phase, nodes: SaveValuesAtN (v_n = v, x = x0), UpdateVelocity,
 // ApplyBoundaryCondition (MahycoModule.cc:308-450, 589-665, 936-1004).
-template <typename CQ>
-__device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars* __restrict__ S,
-    const double* __restrict__ p, const double* __restrict__ q, const CQ* __restrict__ cqs,
-    const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
-    double* __restrict__ vh,
-    int bx_, int by_, int bz_) {
-  int i, j, k;
-  if (!block_item(dm.nx + 1, dm.ny + 1, dm.nz + 1, bx_, by_, bz_, i, j, k)) return;
-  const long long n = dm.nid(i, j, k);
-  const double dtv = 0.5 * (S->old_dt + S->dt);
+
+// Nodal force sum_c (p_c + q_c) cqs_c[node] over the up to 8 cells of node
+// (i, j, k) in increasing cell id (updateForceAndVelocity, MahycoModule.cc:638-651).
+// SUMMED: p already holds p + q (q unused).
+template <typename CQ, bool SUMMED = false>
+__device__ __forceinline__ D3 node_force(const Dims& dm, int i, int j, int k, const double* __restrict__ p,
+                                         const double* __restrict__ q, const CQ* __restrict__ cqs) {
   const int loc[2][2][2] = {{{0, 4}, {3, 7}}, {{1, 5}, {2, 6}}};
   D3 F = d3(0, 0, 0);
 #pragma unroll
@@ -48,12 +45,35 @@ __device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars
         if (ci < 0 || cj < 0 || ck < 0 || ci >= dm.nx || cj >= dm.ny || ck >= dm.nz) continue;
         const long long c = dm.cid(ci, cj, ck);
         const int l = loc[di][dj][dk];
-        const double pq = p[c] + q[c];
+        const double pq = SUMMED ? p[c] : p[c] + q[c];
         F = F + pq * d3((double)cqs[(l * 3 + 0) * dm.C + c], (double)cqs[(l * 3 + 1) * dm.C + c],
                         (double)cqs[(l * 3 + 2) * dm.C + c]);
       }
+  return F;
+}
+
+// vnb (schema-csts only, else null): v_n taken back from n to n-1/2 with
+// the same force first, updateVelocityBackward (MahycoModule.cc:693, 743-781),
+// and kept for the energy and the remap face velocities.
+template <typename CQ>
+__device__ __forceinline__ void k_cyc_lagrange_nodes_body(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ p, const double* __restrict__ q, const CQ* __restrict__ cqs,
+    const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
+    double* __restrict__ vh, double* __restrict__ vnb,
+    int bx_, int by_, int bz_) {
+  int i, j, k;
+  if (!block_item(dm.nx + 1, dm.ny + 1, dm.nz + 1, bx_, by_, bz_, i, j, k)) return;
+  const long long n = dm.nid(i, j, k);
+  const double dtv = 0.5 * (S->old_dt + S->dt);
+  const D3 F = node_force<CQ>(dm, i, j, k, p, q, cqs);
   const double s = dtv / nm[n];
-  D3 u = d3(v[n], v[dm.N + n], v[2 * dm.N + n]) + s * F;
+  D3 vb = d3(v[n], v[dm.N + n], v[2 * dm.N + n]);
+  if (vnb) {
+    const double sb = (-0.5 * S->old_dt) / nm[n];
+    vb = vb + sb * F;
+    vnb[n] = vb.x; vnb[dm.N + n] = vb.y; vnb[2 * dm.N + n] = vb.z;
+  }
+  D3 u = vb + s * F;
   const unsigned mask = bcmask[n];
   if (mask)
     for (int b = 0; b < bct.nb; ++b)
@@ -69,8 +89,51 @@ template <typename CQ>
 __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scalars* __restrict__ S,
     const double* __restrict__ p, const double* __restrict__ q, const CQ* __restrict__ cqs,
     const double* __restrict__ nm, const double* __restrict__ v, const uint16_t* __restrict__ bcmask, BCTable bct,
-    double* __restrict__ vh) {
-  k_cyc_lagrange_nodes_body<CQ>(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, blockIdx.x, -1, 0);
+    double* __restrict__ vh, double* __restrict__ vnb) {
+  k_cyc_lagrange_nodes_body<CQ>(dm, S, p, q, cqs, nm, v, bcmask, bct, vh, vnb, blockIdx.x, -1, 0);
+}
+
+// schema-csts, updateVelocityForward (PrepareRemap.cc:456, MahycoModule.cc:
+// 792-831): vf = v_h + (0.5 dt / m) F with this cycle's corner vectors and the
+// current pressure plus this cycle's pseudo-viscosity (pq, summed by the cell
+// kernel; no boundary condition); xl = the Lagrangian node coordinates
+// x0 + v_h dt, which the remap keeps.
+__global__ void __launch_bounds__(128) k_csts_forward(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ pq, const double* __restrict__ cqs,
+    const double* __restrict__ nm, const double* __restrict__ x0, const double* __restrict__ vh,
+    double* __restrict__ vf, double* __restrict__ xl) {
+  int i, j, k;
+  if (!block_item(dm.nx + 1, dm.ny + 1, dm.nz + 1, blockIdx.x, -1, 0, i, j, k)) return;
+  const long long n = dm.nid(i, j, k), N = dm.N;
+  const double dt = S->dt;
+  const D3 F = node_force<double, true>(dm, i, j, k, pq, nullptr, cqs);
+  const double s = (0.5 * dt) / nm[n];
+  const D3 u = d3(vh[n], vh[N + n], vh[2 * N + n]);
+  const D3 w = u + s * F;
+  vf[n] = w.x; vf[N + n] = w.y; vf[2 * N + n] = w.z;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) xl[a * N + n] = x0[a * N + n] + vh[a * N + n] * dt;
+}
+
+// schema-csts remap face velocities (PrepareRemap.cc:69-79): u_f =
+// (0.25 sum over the face nodes of 0.5 (v + v_n)) . n0, with v the forward
+// velocity and v_n the backward one, for every face of every direction.
+__global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __restrict__ vf,
+    const double* __restrict__ vnb, const double* __restrict__ n0, FaceData fd) {
+  const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= dm.F) return;
+  int d; long long t;
+  if (f < dm.Fx) { d = 0; t = f; } else if (f < dm.Fx + dm.Fy) { d = 1; t = f - dm.Fx; } else { d = 2; t = f - dm.Fx - dm.Fy; }
+  int i, j, k; dm.fdijk(d, t, i, j, k);
+  long long fn[4]; face_node_ids(dm, d, i, j, k, fn);
+  const long long N = dm.N;
+  D3 vm = d3(0., 0., 0.);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const long long m = fn[a];
+    vm = vm + 0.5 * (d3(vf[m], vf[N + m], vf[2 * N + m]) + d3(vnb[m], vnb[N + m], vnb[2 * N + m]));
+  }
+  fd.u[d][t] = dot(.25 * vm, d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]));
 }
 
 
@@ -276,8 +339,31 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
 // most of a second block idle).
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s) {
   const unsigned nbn = (unsigned)((a.dm.N + 127) / 128);
-  if (a.ph.precision) k_cyc_lagrange_nodes<float><<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh);
-  else k_cyc_lagrange_nodes<double><<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh);
+  if (a.ph.precision)
+    k_cyc_lagrange_nodes<float><<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh,
+                                                    nullptr);
+  else
+    k_cyc_lagrange_nodes<double><<<nbn, 128, 0, s>>>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh,
+                                                     a.ph.csts ? a.vnb : nullptr);
+}
+
+void launch_csts_forward(const CycleArgs& a, cudaStream_t s) {
+  const unsigned nbn = (unsigned)((a.dm.N + 127) / 128);
+  k_csts_forward<<<nbn, 128, 0, s>>>(a.dm, a.S, a.pf, a.cqs, a.nm, a.x0, a.vh, a.vf, a.xl);
+  k_csts_face_u<<<(unsigned)((a.dm.F + 127) / 128), 128, 0, s>>>(a.dm, a.vf, a.vnb, a.n0, a.fd);
+}
+
+// The schema-csts form of the one-environment FP64 cell kernel.
+__global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells_csts(Dims dm,
+    const Scalars* __restrict__ S, Phys ph,
+    const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
+    double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
+    const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
+    double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U,
+    double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag, int linear,
+    const double* __restrict__ vnb, double* __restrict__ pf) {
+  k_cyc_lagrange_cells_body<1, double, true>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, nullptr, L, U, xcs, fd,
+                                             env, Vlag, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, vnb, pf);
 }
 
 // Cell kernels: rows of 128 cells when nx is a multiple of 128, else 128
@@ -291,7 +377,11 @@ dim3 cell_grid(const Dims& dm, int& linear) {
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
-  if (a.ph.precision)
+  if (a.ph.csts)
+    k_cyc_lagrange_cells_csts<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
+                                                 a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag,
+                                                 linear, a.vnb, a.pf);
+  else if (a.ph.precision)
     k_cyc_lagrange_cells<1, float><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q,
                                                        a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc,
                                                        a.fd, a.env, a.Vlag, linear);
@@ -326,8 +416,16 @@ static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks
 }
 
 void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
-  if (a.ph.precision) remap_impl<float>(a, sens, s, m);
-  else remap_impl<double>(a, sens, s, m);
+  if (a.ph.precision) { remap_impl<float>(a, sens, s, m); return; }
+  if (a.ph.csts) {
+    // schema-csts: the remap starts from the forward velocity (U_dual,
+    // Phi_dual, PrepareRemap.cc:411-433) on the Lagrangian coordinates
+    CycleArgs b = a;
+    b.vh = a.vf;
+    remap_impl<double>(b, sens, s, m);
+    return;
+  }
+  remap_impl<double>(a, sens, s, m);
 }
 
 void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
@@ -369,9 +467,11 @@ __global__ void __launch_bounds__(128) k_bat_lagrange_nodes(const CycleArgs* __r
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     if constexpr (sizeof(R) == 4)
-      k_cyc_lagrange_nodes_body<float>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh, t.y, t.z, t.w);
+      k_cyc_lagrange_nodes_body<float>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh, nullptr,
+                                       t.y, t.z, t.w);
     else
-      k_cyc_lagrange_nodes_body<double>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, t.y, t.z, t.w);
+      k_cyc_lagrange_nodes_body<double>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, nullptr,
+                                        t.y, t.z, t.w);
   }
 }
 
@@ -415,7 +515,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_n
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm, a.ud[(it + 1) & 1],
                                              a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
   }
 }
@@ -427,7 +527,7 @@ __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_nodes
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW>(a.dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, a.ud[(it + 1) & 1],
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm, a.ud[(it + 1) & 1],
                                                      a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y,
                                                      t.z, t.w);
   }

@@ -28,6 +28,7 @@ struct Phys {
   int eos;              // environment 0: 0 PerfectGas, 1 StiffenedGas
   double pinf;          // its limit-tension
   int with_newton;      // Lagrange energy update by Newton iterations
+  int csts;             // schema-csts time scheme (one environment, FP64)
 };
 
 struct BCTable {
@@ -86,9 +87,12 @@ struct CycleArgs {
   EnvState env;         // K > 1 only
   double* Vlag;         // Lagrangian cell volume (K > 1: divisor of Phi on the first sweep)
   int lines[8];         // lines per block of each sweep (indexed like BatchKernel; y/z sweeps of K = 1: 8, 16, 32)
+  double *vnb, *vf, *xl;  // schema-csts: backward v_n, forward v, Lagrangian node coordinates (3N each)
+  double* pf;             // schema-csts: p + q of the forward step (C)
 };
 
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s);
+void launch_csts_forward(const CycleArgs& a, cudaStream_t s);
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s);
 struct KernelMarks;
 void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* marks = nullptr);

@@ -231,14 +231,55 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
   rho[c] = nd;
 }
 
-template <int K, typename R>
+// schema-csts energy of a one-environment cell (MahycoModule.cc:1776-1810,
+// updateEnergyAndPressureforGP; or by Newton on f, :1552-1613 with
+// MahycoModule.h:433-445, the first iteration always run as in newton_eint).
+// cn1, cn, cdn, con: the corner-vector sums v.cqs dt, v.cqs_n dt,
+// (v - v_n).cqs_n (dt - dt_old), v_n.cqs_n dt_old.  The n-1 pseudo-viscosity
+// is zero: the remap resets the n-level fields (PrepareRemap.cc:485-550)
+// before saveValuesAtN copies them into it.  pf gets the pressure that
+// updateVelocityForward reads: p_n, or the last Newton EOS value; the
+// kernel stores it plus this cycle's pseudo-viscosity.
+__device__ __forceinline__ double csts_eint(const Phys& ph, double cn1, double cn, double cdn, double con, double e0,
+                                            double r, double m, double pn, double qn, double q, double& pf) {
+  const double g = ph.gamma, qnm1 = 0.;
+  if (!ph.with_newton) {
+    const double denom = 1 + 0.5 * (g - 1.0) * r * cn1 / m;
+    const double numer = e0 - (0.5 * (pn + qn) * cn / m) - (0.5 * q * cn1 / m) + (0.25 * (pn + qn) * cdn / m) -
+                         (0.5 * (qn - qnm1) * con / m);
+    pf = pn;
+    return numer / denom;
+  }
+  const double cdon = 0., epsilon = ph.threshold, itermax = 50;
+  const double en = e0;
+  double e = en, pp, dpde;
+  int i = 0;
+  do {
+    if (ph.eos == 1) pp = ((g - 1.) * r * e) - (g * ph.pinf);
+    else pp = (g - 1.) * r * e;
+    dpde = (g - 1.) * r;
+    const double fe = e - en + 0.5 * (pp + q) * cn1 / m + 0.5 * (pn + qn) * cn / m - 0.25 * (pn + qn) * cdn / m +
+                      0.5 * (q - qnm1) * cdon / m;
+    const double enew = e - fe / (1. + 0.5 * dpde * cn1 / m);
+    e = enew;
+    i++;
+  } while (i < itermax && fabs(e - en + 0.5 * (pp + q) * cn1 / m + 0.5 * (pn + qn) * cn / m -
+                                0.25 * (pn + qn) * cdn / m + 0.5 * (q - qnm1) * cdon / m) >= epsilon);
+  pf = pp;
+  return e;
+}
+
+// CSTS (schema-csts, one environment, FP64 only): vnb = the backward node
+// velocity of this cycle, pf = the pressure for the forward step.
+template <int K, typename R, bool CSTS = false>
 __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
     double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
     const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
     double* __restrict__ cqs, float* __restrict__ cqs32, double* __restrict__ L, double* __restrict__ U,
     double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag,
-    int bx_, int by_, int bz_) {
+    int bx_, int by_, int bz_, const double* __restrict__ vnb = nullptr, double* __restrict__ pf = nullptr) {
+  static_assert(!CSTS || (K == 1 && sizeof(R) == 8), "schema-csts: one environment, FP64");
   int i, j, k;
   if (!block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k)) return;
   const long long c = dm.cid(i, j, k);
@@ -256,6 +297,7 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
 
   // corner vectors and volume V = 1/3 sum x_a . cqs_a (MahycoModule.cc:1224-1262)
   constexpr bool F32 = sizeof(R) == 4;
+  double cs_cn1 = 0., cs_cn = 0., cs_cdn = 0., cs_con = 0.;   // schema-csts sums
   double V = 0;
   F3 xr[8];
   if constexpr (F32) {
@@ -272,13 +314,34 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
 #pragma unroll
     for (int a = 0; a < 8; ++a) V += (double)dv[a];
   } else {
-    double dv[8];
+    double dv[8], dv1[8];
+    if constexpr (CSTS) {
+      // the sums over the previous corner vectors, before they are overwritten
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+        const D3 va = d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]);
+        const D3 vb = d3(vnb[nn], vnb[dm.N + nn], vnb[2 * dm.N + nn]);
+        const D3 cq = d3(cqs[(a * 3 + 0) * C + c], cqs[(a * 3 + 1) * C + c], cqs[(a * 3 + 2) * C + c]);
+        cs_cn += dot(va, cq) * dt;
+        cs_cdn += dot(va - vb, cq) * (dt - S->old_dt);
+        cs_con += dot(vb, cq) * S->old_dt;
+      }
+    }
     corner_vectors<double>(x, [&](int a, D3 o) {
       cqs[(a * 3 + 0) * C + c] = o.x; cqs[(a * 3 + 1) * C + c] = o.y; cqs[(a * 3 + 2) * C + c] = o.z;
       dv[a] = dot(x[a], o);
+      if constexpr (CSTS) {
+        const long long nn = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+        dv1[a] = dot(d3(vh[nn], vh[dm.N + nn], vh[2 * dm.N + nn]), o) * dt;
+      }
     });
 #pragma unroll
     for (int a = 0; a < 8; ++a) V += dv[a];
+    if constexpr (CSTS) {
+#pragma unroll
+      for (int a = 0; a < 8; ++a) cs_cn1 += dv1[a];
+    }
   }
   V *= 1. / 3;
   double Lc;
@@ -308,8 +371,15 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     double qn = 0.;
     const double g = ph.gamma;
     if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-    const double en = energy_update(ph.with_newton != 0, ph.pseudo_centree != 0, ph.eos, g, ph.pinf, ph.threshold, q[c],
-                                    qn, ind, irn, nd, p[c], e[c]);
+    double en;
+    if constexpr (CSTS) {
+      double pforward;
+      en = csts_eint(ph, cs_cn1, cs_cn, cs_cdn, cs_con, e[c], nd, mass[c], p[c], q[c], qn, pforward);
+      pf[c] = pforward + qn;                                    // the forward force's p + q (q: this cycle's)
+    } else {
+      en = energy_update(ph.with_newton != 0, ph.pseudo_centree != 0, ph.eos, g, ph.pinf, ph.threshold, q[c], qn, ind,
+                         irn, nd, p[c], e[c]);
+    }
     U[c] = V;
     U[C + c] = V * nd;
     U[2 * C + c] = V * nd * en;
@@ -332,6 +402,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_cyc_lagrange_ce
   k_cyc_lagrange_cells_body<K, R>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, cqs32, L, U, xcs, fd, env, Vlag,
                                   blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
 }
+
 
 
 }  // namespace mhy

@@ -291,7 +291,7 @@ __device__ __forceinline__ R dual_limited(int lim, R gb, R gf) {
 // Inputs of one lane (one node of a line along d).
 struct NodeIn {
   double vh[3];    // Lagrange velocity
-  double x0d;      // initial coordinate along d
+  double x0d;      // initial coordinate along d (the Lagrangian one with schema-csts)
   double nm;       // node mass (first sweep)
   double ud[5];    // U_dual (later sweeps)
   double ffm;      // sum of 0.25 * dual mass flux of the 4 cells in front (DualPhaseRemap.cc:299-340)
@@ -308,7 +308,7 @@ constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| 
 // gradient on entry and its gradient on return.
 template <int D, bool FIRST, bool LAST, typename R = double>
 __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
-                                          bool upd, const NodeIn& in, R G[3], double* out) {
+                                          bool upd, const NodeIn& in, R G[3], double* out, bool xabs = false) {
   const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
   const bool grad_on = ph.ordre_projection > 1;
@@ -332,7 +332,7 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
         P[0] = (R)u.x; P[1] = (R)u.y; P[2] = (R)u.z; P[3] = (R)(0.5 * norm2(u));
       }
     }
-    x = in.x0d + in.vh[D] * dt;
+    x = xabs ? in.x0d : in.x0d + in.vh[D] * dt;       // xabs: x0d holds the Lagrangian coordinate
   }
   const unsigned full = 0xffffffffu;
   R Pm[4], Pp[4];
@@ -393,7 +393,7 @@ __device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int i
 // Node sweep along x: lanes run along the rows of nodes.
 template <bool FIRST, bool LAST, int K, typename R>
 __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
@@ -415,7 +415,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
   R G[3] = {0, 0, 0};
   if (valid) {
-    in.vh[0] = vh[n]; in.vh[1] = vh[N + n]; in.vh[2] = vh[2 * N + n]; in.x0d = x0[n];
+    in.vh[0] = vh[n]; in.vh[1] = vh[N + n]; in.vh[2] = vh[2 * N + n]; in.x0d = xl ? xl[n] : x0[n];
     if (FIRST) in.nm = nm_in[n];
     else {
 #pragma unroll
@@ -456,7 +456,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
     }
   }
   double out[kNodeOut];
-  node_line<0, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out);
+  node_line<0, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr);
   if (!upd) return;
   if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
   if (!LAST) {
@@ -469,11 +469,11 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
 
 template <bool FIRST, bool LAST, int K, typename R>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
@@ -493,7 +493,7 @@ struct NodeTileSize {
 
 template <int D, bool FIRST, bool LAST, int K, typename R, int W = kLineWarps>
 __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
@@ -519,7 +519,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
 #pragma unroll
     for (int a = 0; a < NA; ++a) v[a] = 0.;
     if (s_valid) {
-      v[0] = vh[sn]; v[1] = vh[N + sn]; v[2] = vh[2 * N + sn]; v[3] = x0[D * N + sn];
+      v[0] = vh[sn]; v[1] = vh[N + sn]; v[2] = vh[2 * N + sn]; v[3] = xl ? xl[D * N + sn] : x0[D * N + sn];
       if (FIRST) v[4] = nm_in[sn];
       else {
 #pragma unroll
@@ -595,7 +595,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   const int n = valid ? node_id(i, m) : 0;
   if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
   double out[kNodeOut];
-  node_line<D, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out);
+  node_line<D, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr);
   if (upd) {
     if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
     // each lane overwrites only the tile column it read itself
@@ -616,11 +616,11 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
 
 template <int D, bool FIRST, bool LAST, int K, typename R, int W>
 __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ vh,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W>(dm, S, ph, prev_inner, x0, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------------
@@ -637,8 +637,8 @@ static void sweep_nodes_launch_w(const CycleArgs& a, int prev, const double* udi
   const size_t smem = NodeTileSize<D, FIRST, LAST, K, W>::bytes;
   auto kern = k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R, W>;
   smem_opt_in((const void*)kern, smem);
-  kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm,
-                               a.vnorm);
+  kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout, a.dpf, a.Gd, a.st.mass, a.v,
+                               a.nm, a.vnorm);
 }
 
 template <int D, bool FIRST, bool LAST, int K, typename R>
@@ -648,8 +648,8 @@ static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin,
   const int T = 32 * kLineWarps;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
-    k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.vh, a.nm, udin, udout, a.dpf, a.Gd,
-                                                     a.st.mass, a.v, a.nm, a.vnorm);
+    k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout,
+                                                     a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
   } else {
     // lines per block of this sweep (the tuning; K > 1 meshes keep 8)
     const int w = K == 1 ? a.lines[BK_NODES_X + D] : kLineWarps;

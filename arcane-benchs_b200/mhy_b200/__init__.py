@@ -87,7 +87,7 @@ class COptions(ctypes.Structure):
                 ("nb_bc", ctypes.c_int32), ("bc", BC * MHY_MAX_BC), ("nb_env", ctypes.c_int32),
                 ("adiabatic_cst", ctypes.c_double * MHY_MAX_ENV), ("precision", ctypes.c_int32),
                 ("eos", ctypes.c_int32 * MHY_MAX_ENV), ("limit_tension", ctypes.c_double * MHY_MAX_ENV),
-                ("with_newton", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+                ("with_newton", ctypes.c_int32), ("schema_csts", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 class CMesh(ctypes.Structure):
@@ -196,6 +196,7 @@ def make_options(opts, gammas) -> COptions:
     for k, g in enumerate(gammas):
         o.adiabatic_cst[k] = float(g)
     o.with_newton = int(getattr(opts, "with_newton", 0))
+    o.schema_csts = int(getattr(opts, "schema_csts", 0))
     for k, kind in enumerate(getattr(opts, "eos", ()) or ()):
         o.eos[k] = int(kind)
     for k, v in enumerate(getattr(opts, "limit_tension", ()) or ()):

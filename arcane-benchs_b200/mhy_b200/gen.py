@@ -69,6 +69,7 @@ class Options:
     eos: tuple = ()                         # per environment: 0 PerfectGas (default), 1 StiffenedGas
     limit_tension: tuple = ()               # per environment: StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
     with_newton: int = 0                    # energy update by Newton iterations (Mahyco.axl:308)
+    schema_csts: int = 0                    # the CSTS time scheme (Mahyco.axl:238)
 
 
 @dataclasses.dataclass

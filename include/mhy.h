@@ -81,7 +81,11 @@ typedef struct mhy_options {
   double limit_tension[MHY_MAX_ENV]; /* StiffenedGas limit-tension (StiffenedGasEOS.axl:104, default 0.01) */
   int32_t with_newton;               /* 0; 1: Lagrange energy update by Newton iterations on the EOS
                                         (Mahyco.axl:308, MahycoModule.cc:1482-1535; schema-csts false) */
-  int32_t reserved[6];
+  int32_t schema_csts;               /* 0; 1: the CSTS time scheme (Mahyco.axl:238): velocity taken back to n-1/2
+                                        before the Lagrange step and forward to n+1 before the remap, energy from
+                                        the corner vectors of n and n+1 (MahycoModule.cc:693-831, 1776-1810,
+                                        PrepareRemap.cc:69-79, 456); one environment, precision 0 */
+  int32_t reserved[5];
 } mhy_options;
 
 /* Structured hexahedral mesh: (nx+1)(ny+1)(nz+1) nodes, node (i,j,k) at

@@ -91,7 +91,8 @@ struct Oracle {
   double cfl, threshold, deltat_init, deltat_min, deltat_max, final_time;
   int lc_mode;          // 0 racine-cubique-volume, 1 faces-opposees
   int pseudo_centree, ordre_projection, limiteur_id, use_project_pow;
-  int with_newton = 0;              // Mahyco.axl:308 with-newton (schema-csts false)
+  int with_newton = 0;              // Mahyco.axl:308 with-newton
+  int schema_csts = 0;              // Mahyco.axl:238 schema-csts
   std::vector<double> gamma;
   std::vector<int> eos;             // per environment: 0 PerfectGas, 1 StiffenedGas
   std::vector<double> pinf;         // StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
@@ -457,18 +458,40 @@ struct Oracle {
     for (long n = 0; n < N; ++n) { velocity_n[n] = velocity[n]; node_coord[n] = node_coord_0[n]; }
   }
 
+  // Nodal force gather of updateForceAndVelocity (M:589-665) from global
+  // cell pressures and pseudo-viscosities and the given corner vectors.
+  R3 node_force(long n, const MatVar& pres, const MatVar& q, const std::vector<R3>& cq) const {
+    long cells[8]; int li[8]; int cnt = node_cells(n, cells, li);
+    R3 f = r3(0, 0, 0);
+    for (int a = 0; a < cnt; ++a) {
+      long c = cells[a];
+      f += (pres.g[c] + q.g[c]) * cq[8 * c + li[a]];
+    }
+    return f;
+  }
+
   void updateVelocity() {  // M:678-731 -> updateForceAndVelocity M:589-665
     const double dt = 0.5 * (global_old_deltat + global_deltat);
 #pragma omp parallel for schedule(static)
     for (long n = 0; n < N; ++n) {
-      long cells[8]; int li[8]; int cnt = node_cells(n, cells, li);
-      R3 f = r3(0, 0, 0);
-      for (int a = 0; a < cnt; ++a) {
-        long c = cells[a];
-        f += (pressure_n.g[c] + pseudo_viscosity_n.g[c]) * cqs_n[8 * c + li[a]];
-      }
+      const R3 f = node_force(n, pressure_n, pseudo_viscosity_n, cqs_n);
       force[n] = f;
+      // schema-csts with projection: updateVelocityBackward first (M:693,
+      // 743-781), v_n from n to n-1/2 with the same force
+      if (schema_csts) velocity_n[n] = velocity_n[n] + ((-0.5 * global_old_deltat) / node_mass[n]) * f;
       velocity[n] = velocity_n[n] + (dt / node_mass[n]) * f;
+    }
+  }
+
+  // updateVelocityForward (PrepareRemap.cc:456, M:792-831): v from n+1/2 to
+  // n+1 with the force of this cycle's corner vectors and the current global
+  // pressure and pseudo-viscosity; no boundary condition follows.
+  void updateVelocityForward() {
+    const double dt = 0.5 * global_deltat;
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) {
+      const R3 f = node_force(n, pressure, pseudo_viscosity, cqs);
+      velocity[n] = velocity[n] + (dt / node_mass[n]) * f;
     }
   }
 
@@ -577,11 +600,83 @@ struct Oracle {
     return compute_eint(pseudo_centree != 0, gamma[k], qn, q, rn, r, p, en);
   }
 
+  // schema-csts: the four corner-vector sums of a cell (M:1556-1571,
+  // 1776-1791): sum over the cell's nodes of v.cqs dt, v.cqs_n dt,
+  // (v - v_n).cqs_n (dt - dt_old), v_n.cqs_n dt_old, in node order.
+  struct CstsSums { double cn1, cn, cdn, con; };
+  CstsSums csts_sums(long c) const {
+    long cn[8]; cell_nodes(c, cn);
+    CstsSums s{0., 0., 0., 0.};
+    for (int a = 0; a < 8; ++a) {
+      const R3 v = velocity[cn[a]], vn = velocity_n[cn[a]];
+      s.cn1 += dot(v, cqs[8 * c + a]) * global_deltat;
+      s.cn += dot(v, cqs_n[8 * c + a]) * global_deltat;
+      s.cdn += dot(v - vn, cqs_n[8 * c + a]) * (global_deltat - global_old_deltat);
+      s.con += dot(vn, cqs_n[8 * c + a]) * global_old_deltat;
+    }
+    return s;
+  }
+
+  // schema-csts energy of one environment cell, updateEnergyAndPressureforGP
+  // (M:1795-1810) or by Newton on f (M:1538-1613, MahycoModule.h:433-445;
+  // the first iteration always runs, as in newton_eint).  e = the current
+  // energy, m = the environment's mass; qnm1 is the n-1 pseudo-viscosity.
+  // Newton leaves p and c of its last EOS call (M:1605-1609), returned in pc.
+  double csts_eint(int k, const CstsSums& s, double e0, double r, double m, double pn, double qn, double q,
+                   double qnm1, double en, double* pc) const {
+    const double g = gamma[k];
+    if (!with_newton) {
+      const double denom = 1 + 0.5 * (g - 1.0) * r * s.cn1 / m;
+      const double numer = e0 - (0.5 * (pn + qn) * s.cn / m) - (0.5 * q * s.cn1 / m) +
+                           (0.25 * (pn + qn) * s.cdn / m) - (0.5 * (qn - qnm1) * s.con / m);
+      return numer / denom;
+    }
+    const double cdon = 0., epsilon = threshold, itermax = 50;
+    auto f = [&](double e, double p) {
+      return e - en + 0.5 * (p + q) * s.cn1 / m + 0.5 * (pn + qn) * s.cn / m - 0.25 * (pn + qn) * s.cdn / m +
+             0.5 * (q - qnm1) * cdon / m;
+    };
+    double e = en, p, c, dpde;
+    int i = 0;
+    do {
+      if (eos[k] == 1) { p = ((g - 1.) * r * e) - (g * pinf[k]); c = std::sqrt((g / r) * (p + pinf[k])); }
+      else { p = (g - 1.) * r * e; c = std::sqrt(g * p / r); }
+      dpde = (g - 1.) * r;
+      const double enew = e - f(e, p) / (1. + 0.5 * dpde * s.cn1 / m);
+      e = enew;
+      i++;
+    } while (i < itermax && std::fabs(f(e, p)) >= epsilon);
+    pc[0] = p; pc[1] = c;
+    return e;
+  }
+
   void updateEnergyAndPressure() {  // M:1439-1478 -> updateEnergyAndPressureforGP M:1659-1770 (#else)
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < C; ++c) {
+      const double e_cur = internal_energy.g[c];
       internal_energy.g[c] = 0.;
       int e = env_id[c];
+      if (schema_csts) {
+        const CstsSums sm = csts_sums(c);
+        double pc[2];
+        if (e >= 0) {
+          const double ee = csts_eint(e, sm, e_cur, density.g[c], cell_mass.g[c], pressure_n.g[c],
+                                      pseudo_viscosity_n.g[c], pseudo_viscosity.g[c], pseudo_viscosity_nmoins1.g[c],
+                                      internal_energy_n.g[c], pc);
+          internal_energy.g[c] = ee;
+          if (with_newton) { pressure.g[c] = pc[0]; sound_speed.g[c] = pc[1]; }
+        } else {
+          for (int k = 0; k < K; ++k) if (env_mask[c] >> k & 1) {
+            const double ek = csts_eint(k, sm, internal_energy.p[k][c], density.p[k][c], cell_mass.p[k][c],
+                                        pressure_n.p[k][c], pseudo_viscosity_n.p[k][c], pseudo_viscosity.p[k][c],
+                                        pseudo_viscosity_nmoins1.p[k][c], internal_energy_n.p[k][c], pc);
+            internal_energy.p[k][c] = ek;
+            if (with_newton) { pressure.p[k][c] = pc[0]; sound_speed.p[k][c] = pc[1]; }
+            internal_energy.g[c] += mass_fraction.p[k][c] * ek;
+          }
+        }
+        continue;
+      }
       if (e >= 0) {
         internal_energy.g[c] = energy_update(e, pseudo_viscosity_n.g[c], pseudo_viscosity.g[c],
                                              density_n.g[c], density.g[c], pressure.g[c], internal_energy_n.g[c]);
@@ -636,7 +731,7 @@ struct Oracle {
     }
   }
 
-  void computeFaceQuantitesForRemap() {  // P:15-123 (3D, non-CSTS)
+  void computeFaceQuantitesForRemap() {  // P:15-123 (3D); schema-csts: P:69-79
     const double one_over_nbnode = .25;
 #pragma omp parallel for schedule(static)
     for (long f = 0; f < F; ++f) {
@@ -645,7 +740,11 @@ struct Oracle {
       R3 v2 = node_coord[fn[3]] - node_coord[fn[1]];
       face_length[f] = absolute(0.5 * cross(v1, v2));
       R3 vm = r3(0., 0., 0.), fc = r3(0., 0., 0.);
-      for (int a = 0; a < 4; ++a) { fc += one_over_nbnode * node_coord[fn[a]]; vm += velocity[fn[a]]; }
+      for (int a = 0; a < 4; ++a) {
+        fc += one_over_nbnode * node_coord[fn[a]];
+        if (schema_csts) vm += 0.5 * (velocity[fn[a]] + velocity_n[fn[a]]);
+        else vm += velocity[fn[a]];
+      }
       face_coord[f] = fc;
       face_normal_velocity[f] = dot(one_over_nbnode * vm, face_normal[f]);
     }
@@ -1069,6 +1168,7 @@ struct Oracle {
   }
 
   void remap() {  // P:448-563
+    if (schema_csts) updateVelocityForward();             // P:456
     computeVariablesForRemap_PBorn0();
     computeFaceQuantitesForRemap();
     // IRemap::appliRemap, R:19-60
@@ -1156,7 +1256,7 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
                  double cfl, double threshold, double deltat_init, double deltat_min, double deltat_max,
                  double final_time, int lc_mode, int pseudo_centree, int ordre_projection, int limiteur_id,
                  int nbc, const orc_bc* bcs, int use_project_pow, const int* eos, const double* pinf,
-                 int with_newton) {
+                 int with_newton, int schema_csts) {
   Oracle* o = new Oracle();
   o->nx = nx; o->ny = ny; o->nz = nz; o->NX = nx + 1; o->NY = ny + 1; o->NZ = nz + 1;
   o->C = (long)nx * ny * nz; o->N = (long)o->NX * o->NY * o->NZ;
@@ -1167,6 +1267,7 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
   o->deltat_max = deltat_max; o->final_time = final_time; o->lc_mode = lc_mode; o->pseudo_centree = pseudo_centree;
   o->ordre_projection = ordre_projection; o->limiteur_id = limiteur_id; o->use_project_pow = use_project_pow;
   o->with_newton = with_newton;
+  o->schema_csts = schema_csts;
   o->gamma.assign(gammas, gammas + nenv);
   o->eos.assign(nenv, 0);
   o->pinf.assign(nenv, 0.);

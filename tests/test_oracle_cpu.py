@@ -82,6 +82,22 @@ def test_newton_energy_update():
     assert l1[1] < 0.9 * l1[0] and l1[1] < 1.0e-2, l1
 
 
+@pytest.mark.parametrize("newton", [0, 1])
+def test_csts_sod_against_exact_riemann_solution(newton):
+    """schema-csts (MahycoModule.cc:693-831, 1538-1613, 1776-1810): the shock
+    tube against the exact solution, as accurate as the default scheme."""
+    case = gen.sod(cycles=200, options=gen.Options(schema_csts=1, with_newton=newton))
+    o = mhy_oracle.Oracle(case)
+    o.step(200)
+    t = o.scalars()["time"]
+    rho = o.field("density").reshape(5, 5, 100).mean(axis=(0, 1))
+    x = (np.arange(100) + 0.5) / 100
+    exact = np.array([riemann.sample((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 1.4, (xi - 0.5) / t)[0] for xi in x])
+    l1 = float(np.abs(rho - exact).sum() / 100)
+    # measured 5.2e-3 (closed form) and 5.6e-3 (Newton) at t = 0.16
+    assert l1 < 7.0e-3, l1
+
+
 def test_riemann_solver_known_star_state():
     p, u = riemann.star_state((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 1.4)
     assert abs(p - 0.30313) < 1e-5 and abs(u - 0.92745) < 1e-5
