@@ -65,13 +65,18 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tuning (no autotuner trials)")
+    ap.add_argument("--tune-lines", default=None,
+                    help="set lines per block of the cell y, cell z, node y, node z sweeps (e.g. 16,16,8,8) instead "
+                         "of autotuning (profiling runs: timings under a profiler mislead the autotuner)")
     ap.add_argument("--cpu-sample-cycles", type=int, default=5)
     return ap.parse_args()
 
 
 # DRAM bytes (read + write) of one whole cycle, summed over its kernels, from
 # one ncu capture of the 128^3 Sedov cycle (profiles/dram_traffic_sedov128_cycle.md).
-TRAFFIC_PER_CYCLE = {("sedov", 128, "fp64"): 3477780736.0, ("sedov", 128, "mixed"): 2921549568.0}
+# DRAM bytes of one cycle from ncu (dram__bytes_read.sum + dram__bytes_write.sum over the 10 kernels of the
+# fourth cycle, cell y/z sweeps at 16 lines per block as the autotuner picks them)
+TRAFFIC_PER_CYCLE = {("sedov", 128, "fp64"): 3465343744.0, ("sedov", 128, "mixed"): 2912002560.0}
 
 
 def measured_peak():
@@ -181,6 +186,27 @@ def run_reference(args):
     return 0
 
 
+def apply_tuning(obj, args):
+    """Autotune (default), a fixed --tune-lines setting, or nothing; returns
+    the tuning for the JSON line."""
+    import mhy_b200
+    if args.tune_lines:
+        t = mhy_b200.CTuning.default()
+        for slot, w in zip((3, 4, 6, 7), (int(x) for x in args.tune_lines.split(","))):
+            t.lines_per_block[slot] = w
+        obj.set_tuning(t)
+        d = obj.tuning().as_dict()
+        d["set_by"] = "--tune-lines"
+        return d
+    if args.no_autotune:
+        return None
+    t = obj.autotune(2)                                 # trials on this state, restored; outside the timed region
+    d = t.as_dict()
+    d["cycle_ms_default"] = round(sum(t.ms_default), 3)
+    d["cycle_ms_tuned"] = round(sum(t.ms_tuned), 3)
+    return d
+
+
 def conservation(t0, t1, cycles):
     """Drift of the conserved totals over the run: t0, t1 are lists of
     mhy_get_totals results (one per instance) before and after."""
@@ -288,12 +314,7 @@ def run_ours_batched(args):
     b = mhy_b200.Batch(mine, device=local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
     tot0 = [b.totals(i) for i in range(len(mine))]
-    tuning = None
-    if not args.no_autotune:
-        t = b.autotune(2)                               # trials on this state, restored; outside the timed region
-        tuning = t.as_dict()
-        tuning["cycle_ms_default"] = round(sum(t.ms_default), 3)
-        tuning["cycle_ms_tuned"] = round(sum(t.ms_tuned), 3)
+    tuning = apply_tuning(b, args)
     b.step(args.warmup)
     b.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -331,8 +352,7 @@ def run_ours_batched(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         b2 = mhy_b200.Batch(hcases, device=local)
-        if not args.no_autotune:
-            b2.autotune(2)                                 # the cached choice for these mesh sizes
+        apply_tuning(b2, args)                             # the cached choice for these mesh sizes
         for _ in range(args.steps):
             b2.step(1)
             b2.dt(0)                                   # D2H of a step result + sync, every cycle
@@ -399,12 +419,7 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
     kpc = ctx.kernels_per_cycle()
     tot0 = [ctx.totals()]
-    tuning = None
-    if not args.no_autotune:
-        t = ctx.autotune(2)                             # trials on this state, restored; outside the timed region
-        tuning = t.as_dict()
-        tuning["cycle_ms_default"] = round(sum(t.ms_default), 3)
-        tuning["cycle_ms_tuned"] = round(sum(t.ms_tuned), 3)
+    tuning = apply_tuning(ctx, args)
 
     ctx.step(args.warmup)
     ctx.synchronize()
@@ -446,8 +461,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         c2 = mhy_b200.Context(hcase, device=local)
-        if not args.no_autotune:
-            c2.autotune(2)                                 # the cached choice for this mesh size
+        apply_tuning(c2, args)                             # the cached choice for this mesh size
         for _ in range(args.steps):
             c2.cycle_by_entry_points()
             c2.dt()                                   # D2H of the step's result (dt, 16 B) + sync
