@@ -168,8 +168,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     if (opt->eos[k] < 0 || opt->eos[k] > 1) return fail(MHY_ERR_ARG, "eos must be 0 (PerfectGas) or 1 (StiffenedGas)");
   }
   if (opt->with_newton != 0 && opt->with_newton != 1) return fail(MHY_ERR_ARG, "with_newton must be 0 or 1");
-  if (opt->ordre_projection < 1 || opt->ordre_projection > 2)
-    return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1 or 2");
+  if (opt->ordre_projection < 1 || opt->ordre_projection > 3)
+    return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
+  if (opt->ordre_projection == 3 && (opt->nb_env != 1 || opt->precision != 0))
+    return fail(MHY_ERR_UNSUPPORTED, "ordre-projection 3: one environment in FP64 on the device");
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
     return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0 (minmod), 1 (superBee) or 2 (vanLeer)");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
@@ -250,6 +252,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       A_(&c->fd.db[d], nf[d]); A_(&c->fd.df[d], nf[d]); A_(&c->fd.A[d], nf[d]);
       A_(&c->fd.u[d], nf[d]);
     }
+    if (opt->ordre_projection == 3) {                 // cell widths and the face values of one sweep
+      A_(&c->fd.h, 3 * C);
+      A_(&c->fd.phi3, 4 * std::max(nf[0], std::max(nf[1], nf[2])));
+    }
   }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
@@ -291,7 +297,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   err = cudaMemcpyAsync(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv : kKernelsPerCycle + (opt->schema_csts ? 2 : 0);
+  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv
+                               : kKernelsPerCycle + (opt->schema_csts ? 2 : 0) + (opt->ordre_projection == 3 ? 3 : 0);
   *out = c;
   return MHY_OK;
 }
@@ -597,6 +604,7 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   for (int i = 0; i < n; ++i) {
     if (opts[i].nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "batched instances must have one environment");
     if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
+    if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();
@@ -910,9 +918,10 @@ int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) { u.order[k] = 0; u.occupancy_pct[k] = 100; }
   int rc = check_tuning(u);
   if (rc != MHY_OK) return rc;
-  if (c->K > 1)
+  if (c->K > 1 || c->ph.ordre_projection == 3)
     for (int k = 0; k < BK_TUNE_SLOTS; ++k)
-      if (u.lines_per_block[k] != kLineWarps) return fail(MHY_ERR_UNSUPPORTED, "lines_per_block: one environment only");
+      if (u.lines_per_block[k] != kLineWarps)
+        return fail(MHY_ERR_UNSUPPORTED, "lines_per_block: one environment, order 1 or 2 only");
   apply_tuning(c, u);
   c->tuning = u;
   return MHY_OK;
@@ -923,7 +932,7 @@ int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "autotune runs between cycles");
   if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
-  if (c->K > 1) {                                   // nothing to tune: the K-plane sweeps keep 8 lines
+  if (c->K > 1 || c->ph.ordre_projection == 3) {    // nothing to tune: these sweeps keep 8 lines
     c->tuning = default_tuning();
     if (out) *out = c->tuning;
     return MHY_OK;

@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __re
 
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
-template <bool LAST, typename R>
+template <bool LAST, typename R, bool O3 = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -165,13 +165,18 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   if (inner) {
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
     in.n[0] = n0[t]; in.n[1] = n0[F + t]; in.n[2] = n0[2 * F + t];
+    if constexpr (O3) {
+      const int Fd = (int)dm.Fx;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) in.pf3[v] = fd.phi3[v * Fd + t];
+    }
   }
   if (upd) {
     in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c];
     if (LAST) in.vol = st.Ve[c];
   }
   double out[LAST ? kCellOutLast : kCellOutMid];
-  cell_line<LAST, R>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   if (!upd) return;
   if (!LAST) {
 #pragma unroll
@@ -183,30 +188,32 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   }
 }
 
-template <bool LAST, typename R>
+template <bool LAST, typename R, bool O3 = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_x_body<LAST, R>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_cells_x_body<LAST, R, O3>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
+                                        blockIdx.z);
 }
 
 // Cell sweep along y (D = 1) or z (D = 2), staged through shared memory.
 // Block (bx, by, bz): x = 8 bx .. 8 bx + 7, positions 28 by - 2 .. 28 by + 29
 // along D, and bz = the remaining coordinate (z for D = 1, y for D = 2).
-template <bool LAST, int W>
+template <bool LAST, int W, bool O3 = false>
 struct CellTileSize {
-  static constexpr int NA = LAST ? 17 : 16;           // staged input arrays
+  static constexpr int NB = LAST ? 17 : 16;           // staged input arrays
+  static constexpr int NA = NB + (O3 ? 4 : 0);        // + the order-3 face values
   static constexpr size_t bytes = (size_t)NA * TileGeom<W>::arr * sizeof(double);
 };
 
-template <int D, bool LAST, typename R, int W>
+template <int D, bool LAST, typename R, int W, bool O3 = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st,
     int bx_, int by_, int bz_) {
-  constexpr int NA = CellTileSize<LAST, W>::NA;
+  constexpr int NA = CellTileSize<LAST, W, O3>::NA, NB = CellTileSize<LAST, W, O3>::NB;
   constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
   extern __shared__ double smem_dyn[];
   double* tile = smem_dyn;                            // [NA][W][ld]
@@ -230,12 +237,17 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
       v[0] = Uin[sc]; v[1] = Uin[C + sc]; v[2] = Uin[2 * C + sc]; v[3] = Uin[3 * C + sc];
       v[4] = xcs[sc]; v[5] = xcs[C + sc]; v[6] = xcs[2 * C + sc];
       v[14] = ofn[lb * C + sc]; v[15] = ofn[lf * C + sc];
-      if (LAST) v[NA - 1] = st.Ve[sc];
+      if (LAST) v[NB - 1] = st.Ve[sc];
     }
     if (s_inner) {
       v[7] = fd.db[D][st_]; v[8] = fd.df[D][st_]; v[9] = fd.u[D][st_]; v[10] = fd.A[D][st_];
       const int f = foff + st_;
       v[11] = n0[f]; v[12] = n0[F + f]; v[13] = n0[2 * F + f];
+      if constexpr (O3) {
+        const int Fd = (int)(D == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) v[NB + a] = fd.phi3[a * Fd + st_];
+      }
     }
 #pragma unroll
     for (int a = 0; a < NA; ++a) tile[a * kTileArr + sx * kTileLd + sp] = v[a];
@@ -255,10 +267,14 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   in.db = row[7 * kTileArr]; in.df = row[8 * kTileArr]; in.u = row[9 * kTileArr]; in.A = row[10 * kTileArr];
   in.n[0] = row[11 * kTileArr]; in.n[1] = row[12 * kTileArr]; in.n[2] = row[13 * kTileArr];
   in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
-  in.vol = LAST ? row[(NA - 1) * kTileArr] : 0.;
+  in.vol = LAST ? row[(NB - 1) * kTileArr] : 0.;
+  if constexpr (O3) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) in.pf3[a] = row[(NB + a) * kTileArr];
+  }
   constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
   double out[NO];
-  cell_line<LAST, R>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   // each lane overwrites only the tile column it read itself
   if (upd) {
 #pragma unroll
@@ -277,12 +293,13 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool LAST, typename R, int W>
+template <int D, bool LAST, typename R, int W, bool O3 = false>
 __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_t_body<D, LAST, R, W>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_cells_t_body<D, LAST, R, W, O3>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
+                                              blockIdx.z);
 }
 
 void smem_opt_in(const void* kernel, size_t bytes) {
@@ -301,19 +318,22 @@ void smem_opt_in(const void* kernel, size_t bytes) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int D, bool LAST, typename R, int W>
+template <int D, bool LAST, typename R, int W, bool O3 = false>
 static void sweep_cells_t_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
-  const size_t smem = CellTileSize<LAST, W>::bytes;
-  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W>;
+  const size_t smem = CellTileSize<LAST, W, O3>::bytes;
+  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W, O3>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
 }
 
 template <int D, bool LAST, typename R>
 static void sweep_cells_t(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+  if constexpr (sizeof(R) == 8) {
+    if (a.ph.ordre_projection == 3) { sweep_cells_t_w<D, LAST, R, kLineWarps, true>(a, Uin, Uout, s); return; }
+  }
   const int w = a.lines[BK_CELLS_X + D];
   if (w == 32) sweep_cells_t_w<D, LAST, R, 32>(a, Uin, Uout, s);
   else if (w == 16) sweep_cells_t_w<D, LAST, R, 16>(a, Uin, Uout, s);
@@ -327,8 +347,14 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
   const int T = 32 * kLineWarps;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
-    if (last) k_cyc_sweep_cells_x<true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-    else k_cyc_sweep_cells_x<false, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    if (sizeof(R) == 8 && a.ph.ordre_projection == 3) {
+      if (last) k_cyc_sweep_cells_x<true, R, true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+      else k_cyc_sweep_cells_x<false, R, true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    } else if (last) {
+      k_cyc_sweep_cells_x<true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    } else {
+      k_cyc_sweep_cells_x<false, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    }
   } else {
     if (last) sweep_cells_t<D, true, R>(a, Uin, Uout, s);
     else sweep_cells_t<D, false, R>(a, Uin, Uout, s);
@@ -395,6 +421,82 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
 // writes U[0]; sweeps read U[0] -> U[1] -> U[0] and the last one finalises.
 // U_dual: the first sweep builds it from the Lagrange velocity and writes
 // ud[0]; then ud[0] -> ud[1]; the last one writes the node velocity and mass.
+// Order-3 face values of direction D (RemapADIService.cc:583-641,
+// Remap-ordre-3.cc:7-131) for one environment: Phi of the six cells around
+// each inner face (clamped at the ends of the line) from the sweep's input U,
+// the cell widths h along D and u_f dt; written to fd.phi3 [4][F_D].
+__device__ __forceinline__ double o3_grad(double hm, double h0, double hp, double ym, double y0, double yp) {
+  return h0 / (hm + h0 + hp) * ((2. * hm + h0) / (h0 + hp) * (yp - y0) + (h0 + 2. * hp) / (hm + h0) * (y0 - ym));
+}
+__device__ __forceinline__ double o3_ystar(double hmm, double hm, double hp, double hpp, double ymm, double ym,
+                                           double yp, double ypp, double gradm, double gradp) {
+  const double tmp1 = (2. * hp * hm) / (hm + hp) * ((hmm + hm) / (2. * hm + hp) - (hpp + hp) / (2. * hp + hm)) * (yp - ym);
+  const double tmp2 = -hm * (hmm + hm) / (2. * hm + hp) * gradp + hp * (hp + hpp) / (hm + 2. * hp) * gradm;
+  return ym + hm / (hm + hp) * (yp - ym) + 1. / (hmm + hm + hp + hpp) * (tmp1 + tmp2);
+}
+__device__ __forceinline__ double o3_flux(const double y[6], const double h[6], double vdt) {
+  const double ymmm = y[0], ymm = y[1], ym = y[2], yp = y[3], ypp = y[4], yppp = y[5];
+  const double hmmm = h[0], hmm = h[1], hm = h[2], hp = h[3], hpp = h[4], hppp = h[5];
+  const double gradmm = o3_grad(hmmm, hmm, hm, ymmm, ymm, ym);
+  const double gradm = o3_grad(hmm, hm, hp, ymm, ym, yp);
+  const double gradp = o3_grad(hm, hp, hpp, ym, yp, ypp);
+  const double gradpp = o3_grad(hp, hpp, hppp, yp, ypp, yppp);
+  const double ystarm = o3_ystar(hmmm, hmm, hm, hp, ymmm, ymm, ym, yp, gradmm, gradm);
+  const double ystar = o3_ystar(hmm, hm, hp, hpp, ymm, ym, yp, ypp, gradm, gradp);
+  const double ystarp = o3_ystar(hm, hp, hpp, hppp, ym, yp, ypp, yppp, gradp, gradpp);
+  const double ym_m = ystarm, ym_p = ystar, yp_m = ystar, yp_p = ystarp;
+  const double grad_m = ym_p - ym_m, grad_p = yp_p - yp_m;
+  const double ym6 = 6. * (ym - 0.5 * (ym_m + ym_p));
+  const double yp6 = 6. * (yp - 0.5 * (yp_m + yp_p));
+  double flux;
+  if (vdt > 0.) { const double x = vdt, dx = hm; flux = ym_p - 0.5 * x / dx * (grad_m - (1. - 2. / 3. * x / dx) * ym6); }
+  else if (vdt < 0.) { const double x = -vdt, dx = hp; flux = yp_m + 0.5 * x / dx * (grad_p - (1. - 2. / 3. * x / dx) * yp6); }
+  else return 0.;
+  const double num = vdt / hm, nup = vdt / hp;
+  const double ym_ym = ym + (1. - num) / num * (ym - ymm);
+  const double yp_ym = yp - (1. + nup) / nup * (yp - ypp);
+  const double i10 = amin(ym, yp), i11 = amax(ym, yp);
+  double i20, i21;
+  if (vdt >= 0.) { i20 = amin(ym, ym_ym); i21 = amax(ym, ym_ym); }
+  else { i20 = amin(yp, yp_ym); i21 = amax(yp, yp_ym); }
+  double l0, l1;
+  if ((i11 < i20) || (i21 < i10)) { l0 = 0.; l1 = 0.; }
+  else { l0 = amax(i10, i20); l1 = amin(i11, i21); }
+  if (flux < l0) flux = l0;
+  if (flux > l1) flux = l1;
+  return flux;
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_o3_faces(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ Uin, FaceData fd) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long Fd = D == 0 ? dm.Fx : (D == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
+  if (t >= Fd) return;
+  int i, j, k; dm.fdijk(D, t, i, j, k);
+  const int id = D == 0 ? i : (D == 1 ? j : k), n = dm.ncd(D);
+  if (id <= 0 || id >= n) return;                     // boundary faces carry no flux
+  // cells bbb, bb, b | f, ff, fff along D, clamped at the ends of the line
+  int pos[6];
+  pos[2] = id - 1; pos[1] = pos[2] > 0 ? pos[2] - 1 : pos[2]; pos[0] = pos[1] > 0 ? pos[1] - 1 : pos[1];
+  pos[3] = id; pos[4] = pos[3] + 1 < n ? pos[3] + 1 : pos[3]; pos[5] = pos[4] + 1 < n ? pos[4] + 1 : pos[4];
+  const long long C = dm.C;
+  double y[4][6], h[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    const long long c = D == 0 ? dm.cid(pos[a], j, k) : (D == 1 ? dm.cid(i, pos[a], k) : dm.cid(i, j, pos[a]));
+    const double U[4] = {Uin[c], Uin[C + c], Uin[2 * C + c], Uin[3 * C + c]};
+    double P[4];
+    phi_of<double>(U, P);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) y[v][a] = P[v];
+    h[a] = fd.h[D * C + c];
+  }
+  const double vdt = fd.u[D][t] * S->dt;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) fd.phi3[v * Fd + t] = o3_flux(y[v], h, vdt);
+}
+
 template <typename R>
 static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
   int prev = 0;
@@ -405,6 +507,13 @@ static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks
     double* uout = a.U[(it + 1) & 1];
     const double* udin = a.ud[(it + 1) & 1];
     double* udout = a.ud[it & 1];
+    if (sizeof(R) == 8 && a.ph.ordre_projection == 3) {
+      const long long Fd = d == 0 ? a.dm.Fx : (d == 1 ? a.dm.Fy : a.dm.F - a.dm.Fx - a.dm.Fy);
+      const unsigned nb = (unsigned)((Fd + 127) / 128);
+      if (d == 0) k_o3_faces<0><<<nb, 128, 0, s>>>(a.dm, a.S, uin, a.fd);
+      else if (d == 1) k_o3_faces<1><<<nb, 128, 0, s>>>(a.dm, a.S, uin, a.fd);
+      else k_o3_faces<2><<<nb, 128, 0, s>>>(a.dm, a.S, uin, a.fd);
+    }
     if (d == 0) sweep_cells_d<0, R>(a, last, uin, uout, s);
     else if (d == 1) sweep_cells_d<1, R>(a, last, uin, uout, s);
     else sweep_cells_d<2, R>(a, last, uin, uout, s);

@@ -45,6 +45,8 @@ struct FaceData {
   double* df[3];
   double* A[3];
   double* u[3];
+  double* h;      // order 3: cell widths along each direction, 3 planes of C (RemapADIService.cc:225-258)
+  double* phi3;   // order 3: face values of the current sweep, [4][faces of its direction]
 };
 
 // Persistent cell state (global values of a single-environment mesh).

@@ -128,6 +128,7 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const int id = d == 0 ? i : (d == 1 ? j : k);
+    double hsum = 0;            // order 3: cell width along d (RemapADIService.cc:240-257)
     const int lo[3][4] = {{0, 3, 7, 4}, {0, 1, 5, 4}, {0, 1, 2, 3}};
     const int hi[3][4] = {{1, 2, 6, 5}, {3, 2, 6, 7}, {4, 5, 6, 7}};
     const long long off = d == 0 ? 0 : (d == 1 ? dm.Fx : dm.Fx + dm.Fy);
@@ -152,6 +153,7 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
       fd.A[d][t] = A;
       fd.u[d][t] = dot(.25 * vs, nrm);
       fd.df[d][t] = (double)dot(xf - xc, nr);
+      if constexpr (sizeof(T) == 8) { if (fd.h) hsum += norm2(xf - xc); }
     }
     if (id + 1 < dm.ncd(d)) {
       const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
@@ -159,7 +161,9 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
       Vec3<T> xf = Vec3<T>{0, 0, 0};
       xf = xf + q * x[hi[d][0]]; xf = xf + q * x[hi[d][1]]; xf = xf + q * x[hi[d][2]]; xf = xf + q * x[hi[d][3]];
       fd.db[d][f - off] = (double)dot(xf - xc, nr);
+      if constexpr (sizeof(T) == 8) { if (fd.h) hsum += norm2(xf - xc); }
     }
+    if constexpr (sizeof(T) == 8) { if (fd.h) fd.h[d * dm.C + dm.cid(i, j, k)] = hsum; }
   }
 }
 

@@ -164,6 +164,7 @@ struct CellIn {
   double db, df, u, A, n[3];   // low face of the cell along d (inner faces only)
   double ob, of;               // outward-normal component along d of the back and front faces
   double vol;                  // initial cell volume (last sweep only)
+  double pf3[4];               // order 3: Phi of the low face from k_o3_faces
 };
 constexpr int kCellOutLast = 7;   // rho, e, q, mass, p, c, dual mass flux
 constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
@@ -173,7 +174,7 @@ constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
 // 909-987).  Every lane takes part in the shuffles; lanes with upd set get
 // their cell's results in out.  The boundary faces of d carry Phi_f = 0 and
 // contribute nothing.
-template <bool LAST, typename R = double>
+template <bool LAST, typename R = double, bool O3 = false>
 __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
                                           bool infr, bool upd, const CellIn& in, double* out) {
   const R order2 = (R)(ph.ordre_projection - 1);
@@ -197,8 +198,13 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
 #pragma unroll
   for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
   if (inner) {
-    const bool back = in.u * dx > 0.0;
-    face_value<R>(order2, back, (R)(back ? in.db : in.df), Pp, Gp, P, G, Pf);
+    if constexpr (O3) {                                   // order 3: R:583-641, computed per face beforehand
+#pragma unroll
+      for (int v = 0; v < 4; ++v) Pf[v] = (R)in.pf3[v];
+    } else {
+      const bool back = in.u * dx > 0.0;
+      face_value<R>(order2, back, (R)(back ? in.db : in.df), Pp, Gp, P, G, Pf);
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < 4; ++v) Pf[v] = 0;

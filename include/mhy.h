@@ -66,7 +66,7 @@ typedef struct mhy_options {
   double final_time;                 /* 0.2 */
   int32_t longueur_caracteristique;  /* 0 "racine-cubique-volume", 1 "faces-opposees" */
   int32_t pseudo_centree;            /* 0 */
-  int32_t ordre_projection;          /* 2 (1 and 2 supported) */
+  int32_t ordre_projection;          /* 2 (1, 2, and 3 for one environment in FP64: Remap-ordre-3.cc) */
   int32_t projection_limiteur_id;    /* 0 minmod, 1 superBee, 2 vanLeer */
   int32_t nb_bc;
   mhy_bc bc[MHY_MAX_BC];             /* default: walls on the six planes */

@@ -116,6 +116,7 @@ struct Oracle {
   std::vector<double> back_flux_mass, front_flux_mass, back_flux_mass_env, front_flux_mass_env;
   std::vector<double> back_flux_contrib_env, front_flux_contrib_env;
   std::vector<int> est_mixte, est_pure;
+  std::vector<double> h_cell;                  // cell width along the sweep direction (order 3)
   double global_deltat = 0, global_old_deltat = 0, old_deltat = 0, global_time = 0;
   int sens_projection = 0;
   long iteration = 0;
@@ -761,7 +762,70 @@ struct Oracle {
   long face_begin(int d) const { return d == 0 ? 0 : (d == 1 ? Fx : Fx + Fy); }
   long face_end(int d) const { return d == 0 ? Fx : (d == 1 ? Fx + Fy : F); }
 
-  void computeGradPhiFace(int idir) {  // R:91-271 (h_cell is unused at order 2 and omitted)
+  // Order 3 (Remap-ordre-3.cc:7-131), restated with the same operation order.
+  static double evaluate_grad(double hm, double h0, double hp, double ym, double y0, double yp) {
+    return h0 / (hm + h0 + hp) * ((2. * hm + h0) / (h0 + hp) * (yp - y0) + (h0 + 2. * hp) / (hm + h0) * (y0 - ym));
+  }
+  static double evaluate_ystar(double hmm, double hm, double hp, double hpp, double ymm, double ym, double yp,
+                               double ypp, double gradm, double gradp) {
+    const double tmp1 = (2. * hp * hm) / (hm + hp) * ((hmm + hm) / (2. * hm + hp) - (hpp + hp) / (2. * hp + hm)) * (yp - ym);
+    const double tmp2 = -hm * (hmm + hm) / (2. * hm + hp) * gradp + hp * (hp + hpp) / (hm + 2. * hp) * gradm;
+    return ym + hm / (hm + hp) * (yp - ym) + 1. / (hmm + hm + hp + hpp) * (tmp1 + tmp2);
+  }
+  static double evaluate_fm(double x, double dx, double up, double du, double u6) {
+    return up - 0.5 * x / dx * (du - (1. - 2. / 3. * x / dx) * u6);
+  }
+  static double evaluate_fp(double x, double dx, double um, double du, double u6) {
+    return um + 0.5 * x / dx * (du - (1. - 2. / 3. * x / dx) * u6);
+  }
+  static double flux_ordre3(double ymmm, double ymm, double ym, double yp, double ypp, double yppp, double hmmm,
+                            double hmm, double hm, double hp, double hpp, double hppp, double vdt) {
+    const double gradmm = evaluate_grad(hmmm, hmm, hm, ymmm, ymm, ym);
+    const double gradm = evaluate_grad(hmm, hm, hp, ymm, ym, yp);
+    const double gradp = evaluate_grad(hm, hp, hpp, ym, yp, ypp);
+    const double gradpp = evaluate_grad(hp, hpp, hppp, yp, ypp, yppp);
+    const double ystarm = evaluate_ystar(hmmm, hmm, hm, hp, ymmm, ymm, ym, yp, gradmm, gradm);
+    const double ystar = evaluate_ystar(hmm, hm, hp, hpp, ymm, ym, yp, ypp, gradm, gradp);
+    const double ystarp = evaluate_ystar(hm, hp, hpp, hppp, ym, yp, ypp, yppp, gradp, gradpp);
+    const double ym_m = ystarm, ym_p = ystar, yp_m = ystar, yp_p = ystarp;
+    const double grad_m = ym_p - ym_m, grad_p = yp_p - yp_m;
+    const double ym6 = 6. * (ym - 0.5 * (ym_m + ym_p));
+    const double yp6 = 6. * (yp - 0.5 * (yp_m + yp_p));
+    double flux;
+    if (vdt > 0.) flux = evaluate_fm(vdt, hm, ym_p, grad_m, ym6);
+    else if (vdt < 0.) flux = evaluate_fp(-vdt, hp, yp_m, grad_p, yp6);
+    else return 0.;
+    // TVD limitation
+    const double num = vdt / hm, nup = vdt / hp;
+    const double ym_ym = ym + (1. - num) / num * (ym - ymm);
+    const double yp_ym = yp - (1. + nup) / nup * (yp - ypp);
+    double i1[2], i2[2], lim[2];
+    i1[0] = amin(ym, yp); i1[1] = amax(ym, yp);
+    if (vdt >= 0.) { i2[0] = amin(ym, ym_ym); i2[1] = amax(ym, ym_ym); }
+    else { i2[0] = amin(yp, yp_ym); i2[1] = amax(yp, yp_ym); }
+    if ((i1[1] < i2[0]) || (i2[1] < i1[0])) { lim[0] = 0.; lim[1] = 0.; }
+    else { lim[0] = amax(i1[0], i2[0]); lim[1] = amin(i1[1], i2[1]); }
+    if (flux < lim[0]) flux = lim[0];
+    if (flux > lim[1]) flux = lim[1];
+    return flux;
+  }
+
+  void computeGradPhiFace(int idir) {  // R:91-271 (h_cell by cells, R:225-258; read at order 3 only)
+    if (ordre_projection == 3) {
+#pragma omp parallel for schedule(static)
+      for (long c = 0; c < C; ++c) {
+        long cf[6]; cell_faces(c, cf);
+        int ii, jj, kk; cijk(c, ii, jj, kk);
+        const int id = idir == 0 ? ii : (idir == 1 ? jj : kk);
+        double h = 0;
+        if (id > 0) h += std::sqrt(dot(face_coord[cf[back_local_face(idir)]] - cell_coord[c],
+                                       face_coord[cf[back_local_face(idir)]] - cell_coord[c]));
+        if (id < ncell_dir(idir) - 1)
+          h += std::sqrt(dot(face_coord[cf[front_local_face(idir)]] - cell_coord[c],
+                             face_coord[cf[front_local_face(idir)]] - cell_coord[c]));
+        h_cell[c] = h;
+      }
+    }
 #pragma omp parallel for schedule(static)
     for (long f = face_begin(idir); f < face_end(idir); ++f) {
       long pc, nc;
@@ -791,8 +855,48 @@ struct Oracle {
     }
   }
 
+  // the cell next to c along d in direction s (+1 / -1), or c on the boundary
+  long along(long c, int d, int s) const {
+    int i, j, k; cijk(c, i, j, k);
+    int* id = d == 0 ? &i : (d == 1 ? &j : &k);
+    const int t = *id + s;
+    if (t < 0 || t >= ncell_dir(d)) return c;
+    *id = t;
+    return cid(i, j, k);
+  }
+
   void computeUpwindFaceQuantitiesForProjection(int idir) {  // R:530-545 -> _PBorn0_O2 R:658-720
     std::fill(phi_face.begin(), phi_face.end(), 0.0);
+    if (ordre_projection == 3) {  // R:583-641
+      const double deltat = global_deltat;
+      const int nbmat = K;
+#pragma omp parallel for schedule(static)
+      for (long f = face_begin(idir); f < face_end(idir); ++f) {
+        long cb, cf;
+        if (!face_prev_next(f, idir, cb, cf)) continue;
+        const long cbb = along(cb, idir, -1), cbbb = along(cbb, idir, -1);
+        const long cff = along(cf, idir, +1), cfff = along(cff, idir, +1);
+        const double vdt = face_normal_velocity[f] * deltat;
+        double* pf = &phi_face[(size_t)f * nvars];
+        auto ph = [&](long c, int v) { return phi_lag[(size_t)c * nvars + v]; };
+        for (int v = 0; v < nvars; ++v)
+          pf[v] = flux_ordre3(ph(cbbb, v), ph(cbb, v), ph(cb, v), ph(cf, v), ph(cff, v), ph(cfff, v), h_cell[cbbb],
+                              h_cell[cbb], h_cell[cb], h_cell[cf], h_cell[cff], h_cell[cfff], vdt);
+        const bool voisinage_pure = (est_mixte[cb] == 0 && est_mixte[cf] == 0 && est_pure[cb] == est_pure[cf]);
+        if (!voisinage_pure) {
+          for (int imat = 0; imat < nbmat; imat++) {
+            if (vdt > 0. && ph(cb, imat) != 0. && ph(cb, nbmat + imat) != 0.) {
+              pf[nbmat + imat] = (ph(cb, nbmat + imat) / ph(cb, imat)) * pf[imat];
+              pf[2 * nbmat + imat] = (ph(cb, 2 * nbmat + imat) / ph(cb, nbmat + imat)) * pf[nbmat + imat];
+            } else if (vdt < 0. && ph(cf, imat) != 0. && ph(cf, nbmat + imat) != 0.) {
+              pf[nbmat + imat] = (ph(cf, nbmat + imat) / ph(cf, imat)) * pf[imat];
+              pf[2 * nbmat + imat] = (ph(cf, 2 * nbmat + imat) / ph(cf, nbmat + imat)) * pf[nbmat + imat];
+            }
+          }
+        }
+      }
+      return;
+    }
     const double order2 = (double)(ordre_projection - 1);
 #pragma omp parallel for schedule(static)
     for (long f = face_begin(idir); f < face_end(idir); ++f) {
@@ -1298,7 +1402,7 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
   o->back_flux_mass.assign(N, 0.); o->front_flux_mass.assign(N, 0.);
   o->back_flux_mass_env.assign((size_t)N * K, 0.); o->front_flux_mass_env.assign((size_t)N * K, 0.);
   o->back_flux_contrib_env.assign((size_t)C * K, 0.); o->front_flux_contrib_env.assign((size_t)C * K, 0.);
-  o->est_mixte.assign(C, 0); o->est_pure.assign(C, 0);
+  o->est_mixte.assign(C, 0); o->est_pure.assign(C, 0); o->h_cell.assign(C, 0.);
   return o;
 }
 

@@ -98,6 +98,22 @@ def test_csts_sod_against_exact_riemann_solution(newton):
     assert l1 < 7.0e-3, l1
 
 
+def test_order3_sod_against_exact_riemann_solution():
+    """ordre-projection 3 (Remap-ordre-3.cc): the shock tube at least as
+    accurate as order 2, and order 1 clearly worse."""
+    l1 = {}
+    for order in (1, 2, 3):
+        o = mhy_oracle.Oracle(gen.sod(cycles=200, options=gen.Options(ordre_projection=order)))
+        o.step(200)
+        t = o.scalars()["time"]
+        rho = o.field("density").reshape(5, 5, 100).mean(axis=(0, 1))
+        x = (np.arange(100) + 0.5) / 100
+        exact = np.array([riemann.sample((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 1.4, (xi - 0.5) / t)[0] for xi in x])
+        l1[order] = float(np.abs(rho - exact).sum() / 100)
+    # measured 1.28e-2, 6.0e-3, 5.9e-3
+    assert l1[3] <= l1[2] and l1[1] > 1.0e-2 and l1[3] < 6.5e-3, l1
+
+
 def test_riemann_solver_known_star_state():
     p, u = riemann.star_state((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 1.4)
     assert abs(p - 0.30313) < 1e-5 and abs(u - 0.92745) < 1e-5
