@@ -172,8 +172,12 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
   if (opt->ordre_projection == 3 && (opt->nb_env != 1 || opt->precision != 0))
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection 3: one environment in FP64 on the device");
-  if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 2)
-    return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0 (minmod), 1 (superBee) or 2 (vanLeer)");
+  if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 7)
+    return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0..7 (TypesMahyco.h:65-74)");
+  if (opt->projection_limiteur_id >= 3 && (opt->nb_env != 1 || opt->precision != 0))
+    return fail(MHY_ERR_UNSUPPORTED, "the generalised (G) limiters: one environment in FP64 on the device");
+  if (opt->projection_limiteur_id >= 3 && (mesh->nx < 3 || mesh->ny < 3 || mesh->nz < 3))
+    return fail(MHY_ERR_UNSUPPORTED, "the generalised (G) limiters need 3 cells or more along every direction");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
   if (opt->precision < 0 || opt->precision > 1) return fail(MHY_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
   if (opt->schema_csts != 0 && opt->schema_csts != 1) return fail(MHY_ERR_ARG, "schema_csts must be 0 or 1");
@@ -252,10 +256,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       A_(&c->fd.db[d], nf[d]); A_(&c->fd.df[d], nf[d]); A_(&c->fd.A[d], nf[d]);
       A_(&c->fd.u[d], nf[d]);
     }
-    if (opt->ordre_projection == 3) {                 // cell widths and the face values of one sweep
-      A_(&c->fd.h, 3 * C);
-      A_(&c->fd.phi3, 4 * std::max(nf[0], std::max(nf[1], nf[2])));
-    }
+    if (opt->ordre_projection == 3 || opt->projection_limiteur_id >= 3) A_(&c->fd.h, 3 * C);   // cell widths
+    if (opt->ordre_projection == 3) A_(&c->fd.phi3, 4 * std::max(nf[0], std::max(nf[1], nf[2])));
   }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
@@ -605,6 +607,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
     if (opts[i].nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "batched instances must have one environment");
     if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
     if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
+    if (opts[i].projection_limiteur_id >= 3)
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters are not batched");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();

@@ -157,10 +157,11 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   const int t = inner ? s + (dm.nx + 1) * (j + dm.ny * k) : 0;   // x faces come first: t is also the face id
   CellIn in;
   in.U[0] = in.U[1] = in.U[2] = in.U[3] = 0.; in.xc[0] = in.xc[1] = in.xc[2] = 0.;
-  in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = in.vol = 0.;
+  in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = in.vol = 0.; in.h = 0.;
   if (valid) {
     in.U[0] = Uin[c]; in.U[1] = Uin[C + c]; in.U[2] = Uin[2 * C + c]; in.U[3] = Uin[3 * C + c];
     in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
+    if (ph.limiteur_id >= 3) in.h = fd.h[c];
   }
   if (inner) {
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
@@ -268,6 +269,11 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   in.n[0] = row[11 * kTileArr]; in.n[1] = row[12 * kTileArr]; in.n[2] = row[13 * kTileArr];
   in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
   in.vol = LAST ? row[(NB - 1) * kTileArr] : 0.;
+  in.h = 0.;
+  if (ph.limiteur_id >= 3 && valid) {
+    const int i = i0 + w;
+    in.h = fd.h[D * C + (D == 1 ? i + dm.nx * (s + dm.ny * o) : i + dm.nx * (o + dm.ny * s))];
+  }
   if constexpr (O3) {
 #pragma unroll
     for (int a = 0; a < 4; ++a) in.pf3[a] = row[(NB + a) * kTileArr];

@@ -65,6 +65,43 @@ __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b 
 // Flux limiters, mahyco/src/Remap/RemapADIService.h:260-286
 template <typename R> __device__ __forceinline__ R tmin(R a, R b) { return (b < a) ? b : a; }   // std::min
 template <typename R> __device__ __forceinline__ R tmax(R a, R b) { return (a < b) ? b : a; }   // std::max
+// fluxLimiterG, mahyco/src/Remap/UtilesRemap.cc:127-175: the generalised
+// limiters for uneven widths (ids TypesMahyco.h:65-74: 3 minmodG, 4
+// superBeeG, 5 vanLeerG, 6 arithmeticG, 7 ultrabeeG), std::min / std::max.
+template <typename R>
+__device__ __forceinline__ R flux_limiter_g(int id, R gradplus, R gradmoins, R y0, R yplus, R ymoins, R h0, R hplus,
+                                            R hmoins) {
+  const R zero = R(0), half = R(0.5);
+  R grady = zero;
+  if (gradplus * gradmoins < zero) return zero;
+  if (id == 3) {
+    if ((yplus - ymoins) > zero) grady = tmin(fabs(gradplus), fabs(gradmoins));
+    else grady = -tmin(fabs(gradplus), fabs(gradmoins));
+  } else if (id == 4) {
+    if ((yplus - ymoins) > zero) grady = tmax(fabs(gradplus), fabs(gradmoins));
+    else grady = -tmax(fabs(gradplus), fabs(gradmoins));
+  } else if (id == 5) {
+    const R lambdaplus = (h0 / R(2) + hplus) / (h0 + hplus + hmoins);
+    const R lambdamoins = (h0 / R(2) + hmoins) / (h0 + hplus + hmoins);
+    if ((lambdaplus * gradplus + lambdamoins * gradmoins) != zero)
+      grady = gradplus * gradmoins / (lambdaplus * gradplus + lambdamoins * gradmoins);
+    else grady = zero;
+  } else if (id == 7) {
+    grady = (yplus - ymoins) / h0;
+  } else if (id == 6) {
+    const R lambdaplus = (h0 / R(2) + hplus) / (h0 + hplus + hmoins);
+    const R lambdamoins = (h0 / R(2) + hmoins) / (h0 + hplus + hmoins);
+    grady = lambdamoins * gradplus + lambdaplus * gradmoins;
+  }
+  (void)half; (void)y0;
+  const R gradMplus = gradplus * (h0 + hplus) / h0;
+  const R gradMmoins = gradmoins * (h0 + hmoins) / h0;
+  const R gradM = tmin(fabs(gradMplus), fabs(gradMmoins));
+  if ((yplus - ymoins) > zero) grady = tmin(fabs(gradM), fabs(grady));
+  else grady = -tmin(fabs(gradM), fabs(grady));
+  return grady;
+}
+
 template <typename R>
 __device__ __forceinline__ R limiter(int id, R r) {
   switch (id) {

@@ -165,6 +165,7 @@ struct CellIn {
   double ob, of;               // outward-normal component along d of the back and front faces
   double vol;                  // initial cell volume (last sweep only)
   double pf3[4];               // order 3: Phi of the low face from k_o3_faces
+  double h;                    // G limiters: cell width along d (RemapADIService.cc:225-258)
 };
 constexpr int kCellOutLast = 7;   // rho, e, q, mass, p, c, dual mass flux
 constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
@@ -194,7 +195,20 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
   face_grad<R>(inner, (R)dx, P, Pp, g);
 #pragma unroll
   for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
-  limited_grad<R>(lim, g, gr, G);
+  if (lim >= 3) {
+    // generalised limiters (RemapADIService.cc:319-437 -> UtilesRemap.cc:295-330):
+    // back and front cells are the cell itself at the ends of the line
+    R Pn[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Pn[v] = __shfl_down_sync(full, P[v], 1);
+    const double hb = __shfl_up_sync(full, in.h, 1), hn = __shfl_down_sync(full, in.h, 1);
+    const R h0 = (R)in.h, hm = (R)(inner ? hb : in.h), hp = (R)(infr ? hn : in.h);
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      G[v] = flux_limiter_g<R>(lim, gr[v], g[v], P[v], infr ? Pn[v] : P[v], inner ? Pp[v] : P[v], h0, hp, hm);
+  } else {
+    limited_grad<R>(lim, g, gr, G);
+  }
 #pragma unroll
   for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
   if (inner) {
@@ -302,6 +316,8 @@ struct NodeIn {
   double ud[5];    // U_dual (later sweeps)
   double ffm;      // sum of 0.25 * dual mass flux of the 4 cells in front (DualPhaseRemap.cc:299-340)
   double msum;     // sum of the masses of the up to 8 cells around the node (last sweep)
+  double x2[2];    // G limiters, halo lanes 1 and 30: the coordinates along d two nodes back / ahead,
+                   // which lie outside the warp's segment
 };
 constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| on the last sweep
 
@@ -314,7 +330,8 @@ constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| 
 // gradient on entry and its gradient on return.
 template <int D, bool FIRST, bool LAST, typename R = double>
 __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
-                                          bool upd, const NodeIn& in, R G[3], double* out, bool xabs = false) {
+                                          bool upd, const NodeIn& in, R G[3], double* out, bool xabs = false,
+                                          bool bb_ok = true, bool ff_ok = true) {
   const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
   const bool grad_on = ph.ordre_projection > 1;
@@ -353,7 +370,25 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
     for (int c = 0; c < 3; ++c) gf[c] = Ar<R>::div(Pp[c] - P[c], hf, rf);
 #pragma unroll
     for (int c = 0; c < 3; ++c) gb[c] = __shfl_up_sync(full, gf[c], 1);
-    if (valid && inner) {
+    if (lim >= 3) {
+      // generalised limiters (DualPhaseRemap.cc:48-64, UtilesRemap.cc:15-80,
+      // 346-377): every gradient zeroed, inner nodes from the dual widths
+      const int lane = threadIdx.x & 31;
+      double xm2 = __shfl_up_sync(full, x, 2), xp2 = __shfl_down_sync(full, x, 2);
+      if (lane == 1) xm2 = in.x2[0];
+      if (lane == 30) xp2 = in.x2[1];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) G[c] = R(0);
+      if (valid && inner) {
+        const R h0 = (R)(0.5 * (xp - xm));
+        R hmo, hpl;
+        if (!bb_ok) { hmo = R(0); hpl = (R)(0.5 * (xp2 - x)); }
+        else if (!ff_ok) { hpl = R(0); hmo = (R)(0.5 * (x - xm2)); }
+        else { hmo = (R)(0.5 * (x - xm2)); hpl = (R)(0.5 * (xp2 - x)); }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) G[c] = flux_limiter_g<R>(lim, gf[c], gb[c], P[c], Pp[c], Pm[c], h0, hpl, hmo);
+      }
+    } else if (valid && inner) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) G[c] = dual_limited<R>(lim, gb[c], gf[c]);
     }
@@ -419,7 +454,15 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   NodeIn in;
   in.vh[0] = in.vh[1] = in.vh[2] = 0.; in.x0d = 0.; in.nm = 0.;
   in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
+  in.x2[0] = in.x2[1] = 0.;
   R G[3] = {0, 0, 0};
+  if (valid && ph.limiteur_id >= 3 && (lane == 1 || lane == 30)) {
+    const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
+    if (q >= 0 && q <= nx) {
+      const int nq = n + (q - m);
+      in.x2[lane == 1 ? 0 : 1] = xl ? xl[nq] : x0[nq] + vh[nq] * S->dt;
+    }
+  }
   if (valid) {
     in.vh[0] = vh[n]; in.vh[1] = vh[N + n]; in.vh[2] = vh[2 * N + n]; in.x0d = xl ? xl[n] : x0[n];
     if (FIRST) in.nm = nm_in[n];
@@ -462,7 +505,8 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
     }
   }
   double out[kNodeOut];
-  node_line<0, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr);
+  node_line<0, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
+                               m + 2 <= nx);
   if (!upd) return;
   if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
   if (!LAST) {
@@ -597,11 +641,20 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
     }
     in.msum = sm;
   }
+  in.x2[0] = in.x2[1] = 0.;
+  if (valid && ph.limiteur_id >= 3 && (lane == 1 || lane == 30)) {
+    const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
+    if (q >= 0 && q < nn) {
+      const int nq = node_id(i, q);
+      in.x2[lane == 1 ? 0 : 1] = xl ? xl[D * N + nq] : x0[D * N + nq] + vh[D * N + nq] * S->dt;
+    }
+  }
   R G[3] = {0, 0, 0};
   const int n = valid ? node_id(i, m) : 0;
   if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
   double out[kNodeOut];
-  node_line<D, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr);
+  node_line<D, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
+                               m + 2 <= nn - 1);
   if (upd) {
     if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
     // each lane overwrites only the tile column it read itself

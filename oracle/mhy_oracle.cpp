@@ -810,8 +810,42 @@ struct Oracle {
     return flux;
   }
 
-  void computeGradPhiFace(int idir) {  // R:91-271 (h_cell by cells, R:225-258; read at order 3 only)
-    if (ordre_projection == 3) {
+  // fluxLimiterG, UtilesRemap.cc:127-175: the generalised limiters for
+  // uneven cell widths (ids of TypesMahyco.h:65-74: 3 minmodG, 4 superBeeG,
+  // 5 vanLeerG, 6 arithmeticG, 7 ultrabeeG); std::min / std::max semantics.
+  static double flux_limiter_g(int id, double gradplus, double gradmoins, double y0, double yplus, double ymoins,
+                               double h0, double hplus, double hmoins) {
+    double grady = 0., gradM, gradMplus, gradMmoins;
+    if (gradplus * gradmoins < 0.0) return 0.;
+    if (id == 3) {
+      if ((yplus - ymoins) > 0.) grady = smin(std::fabs(gradplus), std::fabs(gradmoins));
+      else grady = -smin(std::fabs(gradplus), std::fabs(gradmoins));
+    } else if (id == 4) {
+      if ((yplus - ymoins) > 0.) grady = smax(std::fabs(gradplus), std::fabs(gradmoins));
+      else grady = -smax(std::fabs(gradplus), std::fabs(gradmoins));
+    } else if (id == 5) {
+      const double lambdaplus = (h0 / 2. + hplus) / (h0 + hplus + hmoins);
+      const double lambdamoins = (h0 / 2. + hmoins) / (h0 + hplus + hmoins);
+      if ((lambdaplus * gradplus + lambdamoins * gradmoins) != 0.)
+        grady = gradplus * gradmoins / (lambdaplus * gradplus + lambdamoins * gradmoins);
+      else grady = 0.;
+    } else if (id == 7) {
+      grady = (yplus - ymoins) / h0;
+    } else if (id == 6) {
+      const double lambdaplus = (h0 / 2. + hplus) / (h0 + hplus + hmoins);
+      const double lambdamoins = (h0 / 2. + hmoins) / (h0 + hplus + hmoins);
+      grady = lambdamoins * gradplus + lambdaplus * gradmoins;
+    }
+    gradMplus = gradplus * (h0 + hplus) / h0;
+    gradMmoins = gradmoins * (h0 + hmoins) / h0;
+    gradM = smin(std::fabs(gradMplus), std::fabs(gradMmoins));
+    if ((yplus - ymoins) > 0.) grady = smin(std::fabs(gradM), std::fabs(grady));
+    else grady = -smin(std::fabs(gradM), std::fabs(grady));
+    return grady;
+  }
+
+  void computeGradPhiFace(int idir) {  // R:91-271 (h_cell by cells, R:225-258; read at order 3 and by the G limiters)
+    if (ordre_projection == 3 || limiteur_id >= 3) {
 #pragma omp parallel for schedule(static)
       for (long c = 0; c < C; ++c) {
         long cf[6]; cell_faces(c, cf);
@@ -841,6 +875,20 @@ struct Oracle {
     for (long c = 0; c < C; ++c)
       for (int v = 0; v < nvars; ++v) grad_phi[(size_t)c * nvars + v] = 0.;
     if (ordre_projection <= 1) return;
+    if (limiteur_id >= 3) {  // general path R:319-437 -> computeAndLimitGradPhi R/UtilesRemap.cc:295-330
+#pragma omp parallel for schedule(static)
+      for (long c = 0; c < C; ++c) {
+        long cf[6]; cell_faces(c, cf);
+        long bf = cf[back_local_face(idir)], ff = cf[front_local_face(idir)];
+        const long bc = along(c, idir, -1), fc = along(c, idir, +1);   // the cell itself at the ends
+        for (int v = 0; v < nvars; ++v)
+          grad_phi[(size_t)c * nvars + v] =
+              flux_limiter_g(limiteur_id, grad_phi_face[(size_t)ff * nvars + v], grad_phi_face[(size_t)bf * nvars + v],
+                             phi_lag[(size_t)c * nvars + v], phi_lag[(size_t)fc * nvars + v],
+                             phi_lag[(size_t)bc * nvars + v], h_cell[c], h_cell[fc], h_cell[bc]);
+      }
+      return;
+    }
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < C; ++c) {
       long cf[6]; cell_faces(c, cf);
@@ -986,10 +1034,40 @@ struct Oracle {
     }
   }
 
+  // D:48-64 with computeDualGradPhi (UtilesRemap.cc:15-80) and
+  // computeAndLimitGradPhiDual (UtilesRemap.cc:346-377): every gradient
+  // zeroed, then the inner nodes' first three components by fluxLimiterG on
+  // the dual cell widths.
+  void computeDualGradPhi_G(int idir) {
+    std::fill(dual_grad_phi.begin(), dual_grad_phi.end(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) {
+      if (!node_inner(n, idir)) continue;
+      const long bn = node_shift(n, idir, -1), fn = node_shift(n, idir, +1);
+      const long bbn = node_shift(bn, idir, -1), ffn = node_shift(fn, idir, +1);
+      const double* Pn = &phi_dual[(size_t)n * nvars];
+      const double* Pb = &phi_dual[(size_t)bn * nvars];
+      const double* Pf = &phi_dual[(size_t)fn * nvars];
+      const double xn = comp(node_coord[n], idir), xb = comp(node_coord[bn], idir), xf = comp(node_coord[fn], idir);
+      double gf[3], gb[3];
+      for (int a = 0; a < 3; ++a) { gf[a] = (Pf[a] - Pn[a]) / (xf - xn); gb[a] = (Pn[a] - Pb[a]) / (xn - xb); }
+      const double h0 = 0.5 * (xf - xb);
+      double hmoins, hplus;
+      if (bbn < 0) { hmoins = 0.; hplus = 0.5 * (comp(node_coord[ffn], idir) - xn); }
+      else if (ffn < 0) { hplus = 0.; hmoins = 0.5 * (xn - comp(node_coord[bbn], idir)); }
+      else { hmoins = 0.5 * (xn - comp(node_coord[bbn], idir)); hplus = 0.5 * (comp(node_coord[ffn], idir) - xn); }
+      for (int a = 0; a < 3; ++a)
+        dual_grad_phi[(size_t)n * nvars + a] = flux_limiter_g(limiteur_id, gf[a], gb[a], Pn[a], Pf[a], Pb[a], h0, hplus, hmoins);
+    }
+  }
+
   void computeDualUremap(int idir) {  // D:22-676 (#else at :127, #if 1 at :351)
     const double deltat = global_deltat;
     const int nb_env = K;
-    if (ordre_projection > 1) computeDualGradPhi_LimC(idir);
+    if (ordre_projection > 1) {
+      if (limiteur_id < 3) computeDualGradPhi_LimC(idir);
+      else computeDualGradPhi_G(idir);
+    }
     // fcontrib, D:129-189
     const double oneovernbcell = 0.25;
     for (long f = face_begin(idir); f < face_end(idir); ++f) {
