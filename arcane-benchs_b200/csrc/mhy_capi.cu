@@ -262,6 +262,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
   static_assert(6 * kTotalsBlocks + 3 <= 1024, "set-up scratch holds the totals partials");
+  static_assert(3 * 256 + 64 + 3 <= 1024 && MHY_MAX_BC <= 128, "set-up scratch holds the coordinate maxima");
   if (rc == MHY_OK) rc = c->alloc(&c->setup, 1024);
   if (rc == MHY_OK) rc = c->commit();
   if (rc != MHY_OK) { mhy_destroy(c); return rc; }
@@ -283,7 +284,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       k_max3_partial<<<nparts, 256, 0, c->stream>>>(N, c->x0, c->setup);
       unsigned* grp = reinterpret_cast<unsigned*>(c->vh);
       cudaMemsetAsync(grp, 0, N * sizeof(unsigned), c->stream);
-      k_face_groups<<<(unsigned)((F + 255) / 256), 256, 0, c->stream>>>(dm, c->x0, c->setup, nparts, opt->threshold, grp);
+      double* mx = c->setup + 3 * nparts + 64;           // after the partials and the BC surfaces
+      k_max3_finish<<<1, 1, 0, c->stream>>>(c->setup, nparts, mx);
+      k_face_groups<<<(unsigned)((F + 255) / 256), 256, 0, c->stream>>>(dm, c->x0, mx, 1, opt->threshold, grp);
       int* surf = reinterpret_cast<int*>(c->setup + 3 * nparts);
       int hs[MHY_MAX_BC] = {};
       for (int b = 0; b < opt->nb_bc; ++b) hs[b] = opt->bc[b].surface;

@@ -126,6 +126,15 @@ __global__ void k_max3_partial(long long n, const double* __restrict__ x, double
     for (int a = 0; a < 3; ++a) part[3 * blockIdx.x + a] = sm[a][0];
 }
 
+// One thread: the maxima over the per-block maxima, in block order (the order
+// in which every face thread used to take them), into out[0..2].
+__global__ void k_max3_finish(const double* __restrict__ part, int nparts, double* __restrict__ out) {
+  double mx[3] = {-1., -1., -1.};
+  for (int b = 0; b < nparts; ++b)
+    for (int a = 0; a < 3; ++a) mx[a] = (mx[a] < part[3 * b + a]) ? part[3 * b + a] : mx[a];
+  for (int a = 0; a < 3; ++a) out[a] = mx[a];
+}
+
 // Boundary node groups by coordinate threshold over every face, PrepareFaceGroup
 // (MahycoAnnexe.cc:183-251): bit s of grp[n] when the node belongs to a face
 // lying on plane s (XMIN..ZMAX).  mx: the per-block maxima of k_max3_partial.

@@ -149,6 +149,7 @@ constexpr int kTotalsBlocks = 148;   // one per SM; partials: 6 doubles per bloc
 __global__ void k_totals_partial(Dims dm, const double* mass, const double* e, const double* nm, const double* v,
                                  double* part);
 __global__ void k_totals_finish(const double* part, int nparts, double* out);
+__global__ void k_max3_finish(const double* part, int nparts, double* out);
 __global__ void k_init_state(Dims dm, Phys ph, const double* vol, double* rho, const double* pres, double* e,
                              double* cs, double* mass, double* q);
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
