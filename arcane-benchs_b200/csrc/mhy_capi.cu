@@ -80,6 +80,11 @@ struct mhy_ctx {
   int kernels_per_cycle = 0;
   int lines[BK_COUNT] = {kLineWarps, kLineWarps, kLineWarps, kLineWarps, kLineWarps, kLineWarps, kLineWarps,
                          kLineWarps};                  // lines per block of the sweeps (the tuning)
+  // Entry points record their work and launch it late: at mhy_compute_delta_t a
+  // whole recorded cycle becomes one launch of the cycle graph; any call that
+  // reads or waits on the device launches what is pending first.
+  int pend = 0;                                  // bit 0 velocity, 1 geometry, 2 remap
+  int pend_sens = 0;                             // direction rotation of the pending remap
   mhy_tuning tuning{};
 
   // Device arrays come from one allocation: alloc() records a request,
@@ -444,6 +449,39 @@ int launch_cycle(mhy_ctx* c, int sens) {
   return MHY_OK;
 }
 
+// The cycle graph of direction rotation s (captured once).
+int cycle_graph(mhy_ctx* c, int s) {
+  if (c->graph[s]) return MHY_OK;
+  cudaGraph_t g = nullptr;
+  MHY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  launch_cycle(c, s);
+  cudaError_t le = cudaGetLastError();
+  cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+  if (le != cudaSuccess || ee != cudaSuccess)
+    return fail(MHY_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
+  cudaError_t ie = cudaGraphInstantiate(&c->graph[s], g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) { c->graph[s] = nullptr; return fail(MHY_ERR_CUDA, cudaGetErrorString(ie)); }
+  return MHY_OK;
+}
+
+// Launches the entry-point work recorded so far, in order.
+int flush(mhy_ctx* c) {
+  if (!c || !c->pend) return MHY_OK;
+  if (c->pend & 1) launch_velocity(c);
+  if (c->pend & 2) launch_geometry(c);
+  if (c->pend & 4) launch_remap_(c, c->pend_sens);
+  c->pend = 0;
+  MHY_CUDA(cudaGetLastError());
+  return MHY_OK;
+}
+
+#define MHY_FLUSH(c)                  \
+  do {                                \
+    const int frc_ = flush(c);        \
+    if (frc_ != MHY_OK) return frc_;  \
+  } while (0)
+
 int check_phase(mhy_ctx* c, int expected) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
@@ -461,7 +499,7 @@ int mhy_save_values_at_n(mhy_ctx* c) {
 }
 int mhy_update_velocity(mhy_ctx* c) {
   int rc = check_phase(c, PH_VELOCITY); if (rc) return rc;
-  launch_velocity(c); MHY_CUDA(cudaGetLastError());
+  c->pend |= 1;
   c->phase = PH_BC; return MHY_OK;
 }
 int mhy_apply_boundary_condition(mhy_ctx* c) {
@@ -474,7 +512,7 @@ int mhy_update_position(mhy_ctx* c) {
 }
 int mhy_compute_geometric_values(mhy_ctx* c) {
   int rc = check_phase(c, PH_GEOMETRY); if (rc) return rc;
-  launch_geometry(c); MHY_CUDA(cudaGetLastError());
+  c->pend |= 2;
   c->phase = PH_DENSITY; return MHY_OK;
 }
 int mhy_update_density(mhy_ctx* c) {
@@ -491,13 +529,22 @@ int mhy_update_energy_and_pressure(mhy_ctx* c) {
 }
 int mhy_remap(mhy_ctx* c) {
   int rc = check_phase(c, PH_REMAP); if (rc) return rc;
-  launch_remap_(c, c->sens); MHY_CUDA(cudaGetLastError());
+  c->pend |= 4;
+  c->pend_sens = c->sens;
   c->sens = (c->sens + 1) % 3;
   c->phase = PH_DELTA_T; return MHY_OK;
 }
 int mhy_compute_delta_t(mhy_ctx* c) {
   int rc = check_phase(c, PH_DELTA_T); if (rc) return rc;
-  launch_delta_t_(c); MHY_CUDA(cudaGetLastError());
+  if (c->pend == 7) {                                // a whole cycle recorded: one graph launch
+    rc = cycle_graph(c, c->pend_sens);
+    if (rc != MHY_OK) return rc;
+    MHY_CUDA(cudaGraphLaunch(c->graph[c->pend_sens], c->stream));
+    c->pend = 0;
+  } else {
+    MHY_FLUSH(c);
+    launch_delta_t_(c); MHY_CUDA(cudaGetLastError());
+  }
   c->phase = PH_SAVE; return MHY_OK;
 }
 
@@ -506,18 +553,8 @@ int mhy_step(mhy_ctx* c, int ncycles) {
   if (ncycles < 0) return fail(MHY_ERR_ARG, "ncycles < 0");
   for (int it = 0; it < ncycles; ++it) {
     const int s = c->sens;
-    if (!c->graph[s]) {
-      cudaGraph_t g = nullptr;
-      MHY_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      launch_cycle(c, s);
-      cudaError_t le = cudaGetLastError();
-      cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
-      if (le != cudaSuccess || ee != cudaSuccess)
-        return fail(MHY_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ee));
-      cudaError_t ie = cudaGraphInstantiate(&c->graph[s], g, 0);
-      cudaGraphDestroy(g);
-      if (ie != cudaSuccess) { c->graph[s] = nullptr; return fail(MHY_ERR_CUDA, cudaGetErrorString(ie)); }
-    }
+    rc = cycle_graph(c, s);
+    if (rc != MHY_OK) return rc;
     MHY_CUDA(cudaGraphLaunch(c->graph[s], c->stream));
     c->sens = (s + 1) % 3;
   }
@@ -526,6 +563,7 @@ int mhy_step(mhy_ctx* c, int ncycles) {
 
 int mhy_synchronize(mhy_ctx* c) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  MHY_FLUSH(c);
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   Scalars h{};
   MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
@@ -921,14 +959,15 @@ int mhy_get_tuning(mhy_ctx* c, mhy_tuning* out) {
 
 int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
   if (!c || !t) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   mhy_tuning u = *t;
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) { u.order[k] = 0; u.occupancy_pct[k] = 100; }
   int rc = check_tuning(u);
   if (rc != MHY_OK) return rc;
-  if (c->K > 1 || c->ph.ordre_projection == 3)
+  if (c->K > 1 || c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3)
     for (int k = 0; k < BK_TUNE_SLOTS; ++k)
       if (u.lines_per_block[k] != kLineWarps)
-        return fail(MHY_ERR_UNSUPPORTED, "lines_per_block: one environment, order 1 or 2 only");
+        return fail(MHY_ERR_UNSUPPORTED, "lines_per_block: one environment, order 1 or 2, classic limiters only");
   apply_tuning(c, u);
   c->tuning = u;
   return MHY_OK;
@@ -936,10 +975,11 @@ int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
 
 int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  MHY_FLUSH(c);
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "autotune runs between cycles");
   if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
-  if (c->K > 1 || c->ph.ordre_projection == 3) {    // nothing to tune: these sweeps keep 8 lines
+  if (c->K > 1 || c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3) {   // these sweeps keep 8 lines
     c->tuning = default_tuning();
     if (out) *out = c->tuning;
     return MHY_OK;
@@ -1107,6 +1147,7 @@ void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr
 
 int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   const long long C = c->dm.C, N = c->dm.N;
   const double* src = nullptr;
   bool vec = false;
@@ -1220,6 +1261,7 @@ extern "C" {
 
 int mhy_checkpoint_size(mhy_ctx* c, size_t* bytes) {
   if (!c || !bytes) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   std::vector<int64_t> off;
   *bytes = ckpt_layout(ckpt_fields(c), off);
   return MHY_OK;
@@ -1227,6 +1269,7 @@ int mhy_checkpoint_size(mhy_ctx* c, size_t* bytes) {
 
 int mhy_checkpoint_save(mhy_ctx* c, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "a restart dump is taken between cycles");
   const std::vector<CkField> f = ckpt_fields(c);
@@ -1256,6 +1299,7 @@ int mhy_checkpoint_save(mhy_ctx* c, void* dst, size_t bytes) {
 
 int mhy_checkpoint_load(mhy_ctx* c, const void* src, size_t bytes) {
   if (!c || !src) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   if (bytes < sizeof(CkptHeader)) return fail(MHY_ERR_ARG, "not a restart dump");
   const char* base = static_cast<const char*>(src);
   CkptHeader hd;
@@ -1294,6 +1338,7 @@ int mhy_checkpoint_load(mhy_ctx* c, const void* src, size_t bytes) {
 
 int mhy_get_env_mask(mhy_ctx* c, uint32_t* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   const long long C = c->dm.C;
   if (bytes < (size_t)C * sizeof(uint32_t)) return fail(MHY_ERR_ARG, "destination too small");
   MHY_CUDA(cudaStreamSynchronize(c->stream));
@@ -1307,6 +1352,7 @@ int mhy_get_env_mask(mhy_ctx* c, uint32_t* dst, size_t bytes) {
 
 int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   if (env < 0 || env >= c->K) return fail(MHY_ERR_ARG, "environment index out of range");
   const long long C = c->dm.C;
   if (bytes < (size_t)C * sizeof(double)) return fail(MHY_ERR_ARG, "destination too small");
@@ -1346,6 +1392,7 @@ int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
 
 int mhy_get_dt(mhy_ctx* c, double* dt, double* dt_old) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  MHY_FLUSH(c);
   Scalars h{};
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
@@ -1356,6 +1403,7 @@ int mhy_get_dt(mhy_ctx* c, double* dt, double* dt_old) {
 
 int mhy_get_time(mhy_ctx* c, double* time, int64_t* iteration) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  MHY_FLUSH(c);
   Scalars h{};
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
@@ -1366,6 +1414,7 @@ int mhy_get_time(mhy_ctx* c, double* time, int64_t* iteration) {
 
 int mhy_get_status(mhy_ctx* c, uint32_t* flags) {
   if (!c || !flags) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   Scalars h{};
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
@@ -1383,6 +1432,7 @@ int mhy_get_sizes(mhy_ctx* c, int64_t* ncells, int64_t* nnodes, int64_t* nfaces)
 
 int mhy_get_totals(mhy_ctx* c, double* out) {
   if (!c || !out) return fail(MHY_ERR_ARG, "null argument");
+  MHY_FLUSH(c);
   if (!c->initialized) return fail(MHY_ERR_ORDER, "mhy_hydro_start_init has not run");
   double* part = c->setup;                       // 6 x kTotalsBlocks partials, then the 3 totals
   double* res = c->setup + 6 * kTotalsBlocks;
@@ -1394,7 +1444,11 @@ int mhy_get_totals(mhy_ctx* c, double* out) {
   return MHY_OK;
 }
 
-void* mhy_get_stream(mhy_ctx* c) { return c ? (void*)c->stream : nullptr; }
+void* mhy_get_stream(mhy_ctx* c) {
+  if (!c) return nullptr;
+  flush(c);                                        // work the caller enqueues follows the entry points
+  return (void*)c->stream;
+}
 
 int mhy_kernels_per_cycle(mhy_ctx* c) { return c ? c->kernels_per_cycle : 0; }
 

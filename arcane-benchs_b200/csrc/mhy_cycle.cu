@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __re
 
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
-template <bool LAST, typename R, bool O3 = false>
+template <bool LAST, typename R, bool O3 = false, bool GL = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -161,7 +161,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   if (valid) {
     in.U[0] = Uin[c]; in.U[1] = Uin[C + c]; in.U[2] = Uin[2 * C + c]; in.U[3] = Uin[3 * C + c];
     in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
-    if (ph.limiteur_id >= 3) in.h = fd.h[c];
+    if constexpr (GL) in.h = fd.h[c];
   }
   if (inner) {
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
@@ -177,7 +177,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
     if (LAST) in.vol = st.Ve[c];
   }
   double out[LAST ? kCellOutLast : kCellOutMid];
-  cell_line<LAST, R, O3>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3, GL>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   if (!upd) return;
   if (!LAST) {
 #pragma unroll
@@ -189,12 +189,12 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   }
 }
 
-template <bool LAST, typename R, bool O3 = false>
+template <bool LAST, typename R, bool O3 = false, bool GL = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_x_body<LAST, R, O3>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
+  k_cyc_sweep_cells_x_body<LAST, R, O3, GL>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
                                         blockIdx.z);
 }
 
@@ -208,7 +208,7 @@ struct CellTileSize {
   static constexpr size_t bytes = (size_t)NA * TileGeom<W>::arr * sizeof(double);
 };
 
-template <int D, bool LAST, typename R, int W, bool O3 = false>
+template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -270,7 +270,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
   in.vol = LAST ? row[(NB - 1) * kTileArr] : 0.;
   in.h = 0.;
-  if (ph.limiteur_id >= 3 && valid) {
+  if (GL && valid) {
     const int i = i0 + w;
     in.h = fd.h[D * C + (D == 1 ? i + dm.nx * (s + dm.ny * o) : i + dm.nx * (o + dm.ny * s))];
   }
@@ -280,7 +280,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
   constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
   double out[NO];
-  cell_line<LAST, R, O3>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3, GL>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   // each lane overwrites only the tile column it read itself
   if (upd) {
 #pragma unroll
@@ -299,12 +299,12 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool LAST, typename R, int W, bool O3 = false>
+template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false>
 __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_t_body<D, LAST, R, W, O3>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
+  k_cyc_sweep_cells_t_body<D, LAST, R, W, O3, GL>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
                                               blockIdx.z);
 }
 
@@ -324,13 +324,13 @@ void smem_opt_in(const void* kernel, size_t bytes) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int D, bool LAST, typename R, int W, bool O3 = false>
+template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false>
 static void sweep_cells_t_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
   const size_t smem = CellTileSize<LAST, W, O3>::bytes;
-  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W, O3>;
+  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W, O3, GL>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
 }
@@ -338,7 +338,10 @@ static void sweep_cells_t_w(const CycleArgs& a, const double* Uin, double* Uout,
 template <int D, bool LAST, typename R>
 static void sweep_cells_t(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   if constexpr (sizeof(R) == 8) {
-    if (a.ph.ordre_projection == 3) { sweep_cells_t_w<D, LAST, R, kLineWarps, true>(a, Uin, Uout, s); return; }
+    const bool o3 = a.ph.ordre_projection == 3, gl = a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
+    if (o3 && gl) { sweep_cells_t_w<D, LAST, R, kLineWarps, true, true>(a, Uin, Uout, s); return; }
+    if (o3) { sweep_cells_t_w<D, LAST, R, kLineWarps, true, false>(a, Uin, Uout, s); return; }
+    if (gl) { sweep_cells_t_w<D, LAST, R, kLineWarps, false, true>(a, Uin, Uout, s); return; }
   }
   const int w = a.lines[BK_CELLS_X + D];
   if (w == 32) sweep_cells_t_w<D, LAST, R, 32>(a, Uin, Uout, s);
@@ -353,9 +356,13 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
   const int T = 32 * kLineWarps;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
-    if (sizeof(R) == 8 && a.ph.ordre_projection == 3) {
-      if (last) k_cyc_sweep_cells_x<true, R, true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
-      else k_cyc_sweep_cells_x<false, R, true><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+    const bool o3 = sizeof(R) == 8 && a.ph.ordre_projection == 3;
+    const bool gl = sizeof(R) == 8 && a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
+    if (o3 || gl) {
+      auto kern = o3 ? (gl ? (last ? k_cyc_sweep_cells_x<true, R, true, true> : k_cyc_sweep_cells_x<false, R, true, true>)
+                           : (last ? k_cyc_sweep_cells_x<true, R, true, false> : k_cyc_sweep_cells_x<false, R, true, false>))
+                     : (last ? k_cyc_sweep_cells_x<true, R, false, true> : k_cyc_sweep_cells_x<false, R, false, true>);
+      kern<<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
     } else if (last) {
       k_cyc_sweep_cells_x<true, R><<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
     } else {
@@ -386,6 +393,7 @@ void launch_csts_forward(const CycleArgs& a, cudaStream_t s) {
 }
 
 // The schema-csts form of the one-environment FP64 cell kernel.
+template <bool HC>
 __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells_csts(Dims dm,
     const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
@@ -394,7 +402,7 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells_csts(Dims dm,
     double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U,
     double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag, int linear,
     const double* __restrict__ vnb, double* __restrict__ pf) {
-  k_cyc_lagrange_cells_body<1, double, true>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, nullptr, L, U, xcs, fd,
+  k_cyc_lagrange_cells_body<1, double, true, HC>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, nullptr, L, U, xcs, fd,
                                              env, Vlag, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, vnb, pf);
 }
 
@@ -409,11 +417,16 @@ dim3 cell_grid(const Dims& dm, int& linear) {
 void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
-  if (a.ph.csts)
-    k_cyc_lagrange_cells_csts<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
-                                                 a.st.cs, a.st.mass, a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag,
-                                                 linear, a.vnb, a.pf);
-  else if (a.ph.precision)
+  const bool hc = a.fd.h != nullptr;               // cell widths: order 3 or the generalised limiters
+  if (a.ph.csts) {
+    auto kern = hc ? k_cyc_lagrange_cells_csts<true> : k_cyc_lagrange_cells_csts<false>;
+    kern<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs, a.st.mass,
+                             a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, linear, a.vnb, a.pf);
+  } else if (hc && !a.ph.precision) {
+    k_cyc_lagrange_cells<1, double, true><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e,
+                                                              a.st.q, a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L,
+                                                              a.U[0], a.xc, a.fd, a.env, a.Vlag, linear);
+  } else if (a.ph.precision)
     k_cyc_lagrange_cells<1, float><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q,
                                                        a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc,
                                                        a.fd, a.env, a.Vlag, linear);

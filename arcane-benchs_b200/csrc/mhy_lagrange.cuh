@@ -119,8 +119,9 @@ __device__ __forceinline__ void corner_vectors(const Vec3<T> x[8], Finish&& fini
 // for the high face (an inner face) (x_f - x_c).n0 with this cell as the
 // previous one.  Face node order: X (0,3,7,4), Y (0,1,5,4), Z (0,1,2,3) low;
 // X (1,2,6,5), Y (3,2,6,7), Z (4,5,6,7) high, in SN_trigo cell-node numbers.
-// T = float takes x relative to the cell centre (xc = 0).
-template <typename T>
+// T = float takes x relative to the cell centre (xc = 0).  HC: also the cell
+// widths along each direction into fd.h (order 3 and the generalised limiters).
+template <typename T, bool HC = false>
 __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, const Vec3<T> x[8], Vec3<T> xc,
                                           const double* __restrict__ n0, const double* __restrict__ vh,
                                           const FaceData& fd) {
@@ -153,7 +154,7 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
       fd.A[d][t] = A;
       fd.u[d][t] = dot(.25 * vs, nrm);
       fd.df[d][t] = (double)dot(xf - xc, nr);
-      if constexpr (sizeof(T) == 8) { if (fd.h) hsum += norm2(xf - xc); }
+      if constexpr (HC) hsum += norm2(xf - xc);
     }
     if (id + 1 < dm.ncd(d)) {
       const long long f = dm.fid(d, i + (d == 0), j + (d == 1), k + (d == 2));
@@ -161,9 +162,9 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
       Vec3<T> xf = Vec3<T>{0, 0, 0};
       xf = xf + q * x[hi[d][0]]; xf = xf + q * x[hi[d][1]]; xf = xf + q * x[hi[d][2]]; xf = xf + q * x[hi[d][3]];
       fd.db[d][f - off] = (double)dot(xf - xc, nr);
-      if constexpr (sizeof(T) == 8) { if (fd.h) hsum += norm2(xf - xc); }
+      if constexpr (HC) hsum += norm2(xf - xc);
     }
-    if constexpr (sizeof(T) == 8) { if (fd.h) fd.h[d * dm.C + dm.cid(i, j, k)] = hsum; }
+    if constexpr (HC) fd.h[d * dm.C + dm.cid(i, j, k)] = hsum;
   }
 }
 
@@ -275,7 +276,7 @@ __device__ __forceinline__ double csts_eint(const Phys& ph, double cn1, double c
 
 // CSTS (schema-csts, one environment, FP64 only): vnb = the backward node
 // velocity of this cycle, pf = the pressure for the forward step.
-template <int K, typename R, bool CSTS = false>
+template <int K, typename R, bool CSTS = false, bool HC = false>
 __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
     double* __restrict__ rho, const double* __restrict__ e, const double* __restrict__ q,
@@ -392,10 +393,10 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag);
   }
   if constexpr (F32) face_data<float>(dm, i, j, k, xr, F3{0.f, 0.f, 0.f}, n0, vh, fd);
-  else face_data<double>(dm, i, j, k, x, xc, n0, vh, fd);
+  else face_data<double, HC>(dm, i, j, k, x, xc, n0, vh, fd);
 }
 
-template <int K, typename R>
+template <int K, typename R, bool HC = false>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_cyc_lagrange_cells(Dims dm,
     const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
@@ -403,8 +404,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_cyc_lagrange_ce
     const double* __restrict__ p, const double* __restrict__ cs, const double* __restrict__ mass,
     double* __restrict__ cqs, float* __restrict__ cqs32, double* __restrict__ L, double* __restrict__ U,
     double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag, int linear) {
-  k_cyc_lagrange_cells_body<K, R>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, cqs32, L, U, xcs, fd, env, Vlag,
-                                  blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
+  k_cyc_lagrange_cells_body<K, R, false, HC>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, cqs32, L, U, xcs, fd,
+                                             env, Vlag, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z);
 }
 
 

@@ -175,7 +175,7 @@ constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
 // 909-987).  Every lane takes part in the shuffles; lanes with upd set get
 // their cell's results in out.  The boundary faces of d carry Phi_f = 0 and
 // contribute nothing.
-template <bool LAST, typename R = double, bool O3 = false>
+template <bool LAST, typename R = double, bool O3 = false, bool GL = false>
 __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
                                           bool infr, bool upd, const CellIn& in, double* out) {
   const R order2 = (R)(ph.ordre_projection - 1);
@@ -195,7 +195,7 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
   face_grad<R>(inner, (R)dx, P, Pp, g);
 #pragma unroll
   for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
-  if (lim >= 3) {
+  if constexpr (GL) {
     // generalised limiters (RemapADIService.cc:319-437 -> UtilesRemap.cc:295-330):
     // back and front cells are the cell itself at the ends of the line
     R Pn[4];
@@ -328,7 +328,7 @@ constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| 
 // start of a sweep is PrepareRemap.cc:411-433 on the first sweep or for nodes
 // not yet updated this cycle, else U_dual / m.  G holds the node's stale
 // gradient on entry and its gradient on return.
-template <int D, bool FIRST, bool LAST, typename R = double>
+template <int D, bool FIRST, bool LAST, typename R = double, bool GL = false>
 __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
                                           bool upd, const NodeIn& in, R G[3], double* out, bool xabs = false,
                                           bool bb_ok = true, bool ff_ok = true) {
@@ -370,7 +370,7 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
     for (int c = 0; c < 3; ++c) gf[c] = Ar<R>::div(Pp[c] - P[c], hf, rf);
 #pragma unroll
     for (int c = 0; c < 3; ++c) gb[c] = __shfl_up_sync(full, gf[c], 1);
-    if (lim >= 3) {
+    if constexpr (GL) {
       // generalised limiters (DualPhaseRemap.cc:48-64, UtilesRemap.cc:15-80,
       // 346-377): every gradient zeroed, inner nodes from the dual widths
       const int lane = threadIdx.x & 31;
@@ -432,7 +432,7 @@ __device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int i
 }
 
 // Node sweep along x: lanes run along the rows of nodes.
-template <bool FIRST, bool LAST, int K, typename R>
+template <bool FIRST, bool LAST, int K, typename R, bool GL = false>
 __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
@@ -456,7 +456,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
   in.x2[0] = in.x2[1] = 0.;
   R G[3] = {0, 0, 0};
-  if (valid && ph.limiteur_id >= 3 && (lane == 1 || lane == 30)) {
+  if (GL && valid && (lane == 1 || lane == 30)) {
     const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
     if (q >= 0 && q <= nx) {
       const int nq = n + (q - m);
@@ -505,8 +505,8 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
     }
   }
   double out[kNodeOut];
-  node_line<0, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
-                               m + 2 <= nx);
+  node_line<0, FIRST, LAST, R, GL>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
+                                   m + 2 <= nx);
   if (!upd) return;
   if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
   if (!LAST) {
@@ -517,13 +517,13 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   }
 }
 
-template <bool FIRST, bool LAST, int K, typename R>
+template <bool FIRST, bool LAST, int K, typename R, bool GL = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_nodes_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
@@ -541,7 +541,7 @@ struct NodeTileSize {
   static constexpr size_t bytes = (size_t)(NA * TileGeom<W>::arr + NT * CT) * sizeof(double);
 };
 
-template <int D, bool FIRST, bool LAST, int K, typename R, int W = kLineWarps>
+template <int D, bool FIRST, bool LAST, int K, typename R, int W = kLineWarps, bool GL = false>
 __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
@@ -642,7 +642,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
     in.msum = sm;
   }
   in.x2[0] = in.x2[1] = 0.;
-  if (valid && ph.limiteur_id >= 3 && (lane == 1 || lane == 30)) {
+  if (GL && valid && (lane == 1 || lane == 30)) {
     const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
     if (q >= 0 && q < nn) {
       const int nq = node_id(i, q);
@@ -653,8 +653,8 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   const int n = valid ? node_id(i, m) : 0;
   if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
   double out[kNodeOut];
-  node_line<D, FIRST, LAST, R>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
-                               m + 2 <= nn - 1);
+  node_line<D, FIRST, LAST, R, GL>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
+                                   m + 2 <= nn - 1);
   if (upd) {
     if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
     // each lane overwrites only the tile column it read itself
@@ -673,13 +673,13 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool FIRST, bool LAST, int K, typename R, int W>
+template <int D, bool FIRST, bool LAST, int K, typename R, int W, bool GL = false>
 __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_nodes_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------------
@@ -688,13 +688,13 @@ __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_nodes_t
 // Dynamic shared memory above the default 48 KB needs an opt-in per kernel and device.
 void smem_opt_in(const void* kernel, size_t bytes);
 
-template <int D, bool FIRST, bool LAST, int K, typename R, int W>
+template <int D, bool FIRST, bool LAST, int K, typename R, int W, bool GL = false>
 static void sweep_nodes_launch_w(const CycleArgs& a, int prev, const double* udin, double* udout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + 1 + W - 1) / W, nseg, (D == 1 ? dm.nz : dm.ny) + 1);
   const size_t smem = NodeTileSize<D, FIRST, LAST, K, W>::bytes;
-  auto kern = k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R, W>;
+  auto kern = k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R, W, GL>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout, a.dpf, a.Gd, a.st.mass, a.v,
                                a.nm, a.vnorm);
@@ -705,11 +705,20 @@ static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin,
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
   const int T = 32 * kLineWarps;
+  // the generalised limiters (one environment, FP64) have their own kernels
+  const bool gl = K == 1 && sizeof(R) == 8 && a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
-    k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout,
-                                                     a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+    if (gl)
+      k_cyc_sweep_nodes_x<FIRST, LAST, K, R, true><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin,
+                                                                udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+    else
+      k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout,
+                                                       a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
   } else {
+    if constexpr (K == 1 && sizeof(R) == 8) {
+      if (gl) { sweep_nodes_launch_w<D, FIRST, LAST, K, R, kLineWarps, true>(a, prev, udin, udout, s); return; }
+    }
     // lines per block of this sweep (the tuning; K > 1 meshes keep 8)
     const int w = K == 1 ? a.lines[BK_NODES_X + D] : kLineWarps;
     if (w == 32) sweep_nodes_launch_w<D, FIRST, LAST, K, R, 32>(a, prev, udin, udout, s);
