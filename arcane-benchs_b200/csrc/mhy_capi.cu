@@ -184,6 +184,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (opt->projection_limiteur_id >= 3 && (mesh->nx < 3 || mesh->ny < 3 || mesh->nz < 3))
     return fail(MHY_ERR_UNSUPPORTED, "the generalised (G) limiters need 3 cells or more along every direction");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");
+  if (!(opt->cfl > 0.) || !(opt->deltat_init > 0.) || !(opt->deltat_max > 0.) || !(opt->deltat_min >= 0.) ||
+      !(opt->threshold >= 0.) || !(opt->final_time > 0.))
+    return fail(MHY_ERR_ARG, "cfl, deltat-init, deltat-max and final-time must be > 0, deltat-min and threshold >= 0");
   if (opt->precision < 0 || opt->precision > 1) return fail(MHY_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
   if (opt->schema_csts != 0 && opt->schema_csts != 1) return fail(MHY_ERR_ARG, "schema_csts must be 0 or 1");
   if (opt->schema_csts && (opt->nb_env != 1 || opt->precision != 0))
