@@ -438,7 +438,7 @@ int launch_remap_(mhy_ctx* c, int sens, KernelMarks* m = nullptr) {
     if (c->ph.csts) launch_csts_forward(c->args(), c->stream);   // PrepareRemap.cc:456, then the face velocities
     launch_remap(c->args(), sens, c->stream, m);
   } else {
-    launch_remap_env(c->args(), sens, c->stream);
+    launch_remap_env(c->args(), sens, c->stream, m);
   }
   return MHY_OK;
 }
@@ -785,6 +785,17 @@ inline bool line_slot(int k) {
   return k == BK_CELLS_Y || k == BK_CELLS_Z || k == BK_NODES_Y || k == BK_NODES_Z;
 }
 
+// The line counts a context's sweeps are built for: 8, 16 or 32 on the y/z
+// sweeps of one environment at order 1 or 2 with the classic limiters; 8 or 16
+// on the cell y/z sweeps of several environments (their node sweeps keep 8);
+// 8 everywhere at order 3 or with the G limiters.
+bool tunable_lines(const mhy_ctx* c, int k, int w) {
+  if (!line_slot(k)) return w == kLineWarps;
+  if (c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3) return w == kLineWarps;
+  if (c->K > 1) return w == kLineWarps || ((k == BK_CELLS_Y || k == BK_CELLS_Z) && w == 16);
+  return true;
+}
+
 mhy_tuning default_tuning() {
   mhy_tuning t{};
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) { t.order[k] = 0; t.occupancy_pct[k] = 100; t.lines_per_block[k] = kLineWarps; }
@@ -967,10 +978,10 @@ int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) { u.order[k] = 0; u.occupancy_pct[k] = 100; }
   int rc = check_tuning(u);
   if (rc != MHY_OK) return rc;
-  if (c->K > 1 || c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3)
-    for (int k = 0; k < BK_TUNE_SLOTS; ++k)
-      if (u.lines_per_block[k] != kLineWarps)
-        return fail(MHY_ERR_UNSUPPORTED, "lines_per_block: one environment, order 1 or 2, classic limiters only");
+  for (int k = 0; k < BK_TUNE_SLOTS; ++k)
+    if (u.lines_per_block[k] != kLineWarps && !tunable_lines(c, k, u.lines_per_block[k]))
+      return fail(MHY_ERR_UNSUPPORTED,
+                  "lines_per_block: 8 or 16 on the cell y/z sweeps of several environments; 8 with order 3 or the G limiters");
   apply_tuning(c, u);
   c->tuning = u;
   return MHY_OK;
@@ -982,7 +993,7 @@ int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "autotune runs between cycles");
   if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
-  if (c->K > 1 || c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3) {   // these sweeps keep 8 lines
+  if (c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3) {   // these sweeps keep 8 lines
     c->tuning = default_tuning();
     if (out) *out = c->tuning;
     return MHY_OK;
@@ -1008,9 +1019,10 @@ int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
   std::vector<mhy_tuning> tr;
   for (int l = 0; l < kNL; ++l) {
     mhy_tuning t = default_tuning();
+    bool any = false;
     for (int k = 0; k < BK_TUNE_SLOTS; ++k)
-      if (line_slot(k)) t.lines_per_block[k] = kLineOptions[l];
-    tr.push_back(t);
+      if (line_slot(k) && tunable_lines(c, k, kLineOptions[l])) { t.lines_per_block[k] = kLineOptions[l]; any = true; }
+    if (l == 0 || any) tr.push_back(t);
   }
   std::vector<std::array<double, BK_TUNE_SLOTS>> ms(tr.size());
   for (size_t i = 0; i < tr.size() && rc == MHY_OK; ++i) {

@@ -103,7 +103,7 @@ constexpr int kKernelsPerCycle = 10;
 // meshes with 2..kMaxEnvDevice environments (mhy_multi.cu)
 constexpr int kMaxEnvDevice = 4;
 void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s);
-void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s);
+void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m = nullptr);
 void launch_init_env(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycleEnv = 11;
 

@@ -156,21 +156,23 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
 template <int K, bool FIRST>
 __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
 
-template <int K, int D, bool FIRST, typename R>
-__global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_t(Dims dm,
+// W: lines per block (8 or 16, the tuning; the register budget stays 128).
+template <int K, int D, bool FIRST, typename R, int W = kLineWarps>
+__global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_sweep_cells_t(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
     double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
   constexpr int NV = 3 * K + 1;
   constexpr int NA = env_cells_staged_arrays<K, FIRST>();
   constexpr int AX = NV, AF = NV + 3, AN = NV + 7, AO = NV + 10, AD = NV + 12;   // array offsets
+  constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
   extern __shared__ double tile[];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = blockIdx.x * kLineWarps, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int i0 = blockIdx.x * W, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
   const int nd = dm.ncd(D), C = (int)dm.C, F = (int)dm.F;
   const int foff = D == 1 ? (int)dm.Fx : (int)(dm.Fx + dm.Fy);
   const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;
-  const int sx = tid & 7, sp = tid >> 3;
+  const int sx = tid % W, sp = tid / W;
   const int si = i0 + sx, ss = seg0 + sp;
   const bool s_valid = si < dm.nx && ss >= 0 && ss < nd;
   const int sc = D == 1 ? si + dm.nx * (ss + dm.ny * o) : si + dm.nx * (o + dm.ny * ss);
@@ -444,14 +446,22 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int K, int D, bool FIRST, typename R>
-static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+template <int K, int D, bool FIRST, typename R, int W>
+static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
-  const dim3 g((dm.nx + kLineWarps - 1) / kLineWarps, nseg, D == 1 ? dm.nz : dm.ny);
-  const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * kTileArr * sizeof(double);
-  k_env_sweep_cells_t<K, D, FIRST, R><<<g, 32 * kLineWarps, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin,
-                                                                        Uout, a.dpf, a.Vlag);
+  const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
+  const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<W>::arr * sizeof(double);
+  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W>;
+  smem_opt_in((const void*)kern, smem);
+  kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
+}
+
+// lines per block of this sweep: the tuning's (8 or 16)
+template <int K, int D, bool FIRST, typename R>
+static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+  if (a.lines[BK_CELLS_X + D] == 16) env_cells_staged_w<K, D, FIRST, R, 16>(a, Uin, Uout, s);
+  else env_cells_staged_w<K, D, FIRST, R, kLineWarps>(a, Uin, Uout, s);
 }
 
 template <int K, bool FIRST, typename R>
@@ -471,7 +481,7 @@ static void env_cells(const CycleArgs& a, int d, const double* Uin, double* Uout
 
 // R: evaluation type of the sweeps (double, or float in the mixed form).
 template <int K, typename R>
-static void remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
+static void remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
@@ -486,7 +496,9 @@ static void remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
       const unsigned nb = (unsigned)((a.dm.C + 255) / 256);
       k_env_finalize_cells<K><<<nb, 256, 0, s>>>(a.dm, a.S, a.ph, a.env, uout, a.st);
     }
+    mark(m, BK_CELLS_X + d, s);
     sweep_nodes<K, R>(a, d, first, last, prev, udin, udout, s);
+    mark(m, BK_NODES_X + d, s);
     prev |= 1 << d;
   }
 }
@@ -525,15 +537,15 @@ void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
 #undef MHY_LAG_ENV
 }
 
-void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s) {
+void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
   if (a.ph.precision) {
-    if (a.K == 2) remap_env<2, float>(a, sens, s);
-    else if (a.K == 3) remap_env<3, float>(a, sens, s);
-    else remap_env<4, float>(a, sens, s);
+    if (a.K == 2) remap_env<2, float>(a, sens, s, m);
+    else if (a.K == 3) remap_env<3, float>(a, sens, s, m);
+    else remap_env<4, float>(a, sens, s, m);
   } else {
-    if (a.K == 2) remap_env<2, double>(a, sens, s);
-    else if (a.K == 3) remap_env<3, double>(a, sens, s);
-    else remap_env<4, double>(a, sens, s);
+    if (a.K == 2) remap_env<2, double>(a, sens, s, m);
+    else if (a.K == 3) remap_env<3, double>(a, sens, s, m);
+    else remap_env<4, double>(a, sens, s, m);
   }
 }
 

@@ -1,6 +1,7 @@
 """GPU: the autotuner (mhy_autotune, mhy_batch_autotune) and explicit
-tunings.  Any lines per block of the y/z sweeps, work order and persistent
-grid gives the same bits; autotuning restores the state it trials on; a
+tunings.  Any lines per block of the y/z sweeps (one environment: 8, 16 or
+32; the cell sweeps of several environments: 8 or 16), work order and
+persistent grid gives the same bits; autotuning restores the state it trials on; a
 second context or batch with the same mesh sizes takes the cached choice."""
 import numpy as np
 import pytest
@@ -10,6 +11,7 @@ from mhy_b200 import Batch, Context, CTuning, MhyError, gen
 pytestmark = pytest.mark.gpu
 
 FIELDS = ("density", "internal_energy", "pressure", "velocity", "node_mass")
+ENV_FIELDS = ("fracvol", "density", "internal_energy")
 
 
 def cases():
@@ -22,16 +24,19 @@ def run(b, n):
     return [{f: b.field(i, f) for f in FIELDS} | {"dt": b.dt(i)} for i in range(b.size())]
 
 
-def run_ctx(g, n):
+def run_ctx(g, n, K=1):
     g.step(n)
     g.synchronize()
-    return [{f: g.field(f) for f in FIELDS} | {"dt": g.dt()}]
+    env = {f"{f}{k}": g.env_field(f, k) for f in ENV_FIELDS for k in range(K)} if K > 1 else {}
+    return [{f: g.field(f) for f in FIELDS} | env | {"dt": g.dt()}]
 
 
 def assert_same(a, b):
     for i, (x, y) in enumerate(zip(a, b)):
-        for f in FIELDS:
-            assert np.array_equal(x[f], y[f]), (i, f)
+        assert x.keys() == y.keys()
+        for f in x:
+            if f != "dt":
+                assert np.array_equal(x[f], y[f]), (i, f)
         assert x["dt"] == y["dt"], i
 
 
@@ -90,6 +95,34 @@ def test_context_autotune_keeps_results_and_caches():
     assert Context(mk()).autotune(2).from_cache
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("K", [2, 3])
+def test_multi_environment_lines_per_block_give_the_same_bits(K, precision):
+    """The cell y/z sweeps of several environments at 16 lines per block."""
+    opts = gen.Options(precision=precision)
+    mk = (lambda: gen.two_material(32, 20, 18, cycles=40, options=opts)) if K == 2 else \
+         (lambda: gen.three_material(36, 17, 12, cycles=40, options=opts))
+    ref = run_ctx(Context(mk()), 40, K)
+    g = Context(mk())
+    t = CTuning.default()
+    t.lines_per_block[3] = t.lines_per_block[4] = 16
+    g.set_tuning(t)
+    assert list(g.tuning().lines_per_block)[3:5] == [16, 16]
+    assert_same(ref, run_ctx(g, 40, K))
+
+
+def test_multi_environment_autotune_keeps_results():
+    mk = lambda: gen.two_material(40, 24, 24, cycles=30)
+    ref = run_ctx(Context(mk()), 30, 2)
+    g = Context(mk())
+    t = g.autotune(2)
+    assert t.trials == 2 and not t.from_cache
+    assert all(t.lines_per_block[k] in (8, 16) for k in (3, 4))
+    assert all(t.lines_per_block[k] == 8 for k in (0, 1, 2, 5, 6, 7))
+    assert_same(ref, run_ctx(g, 30, 2))
+    assert Context(mk()).autotune(2).from_cache
+
+
 def test_bad_tunings_are_refused():
     b = Batch(cases())
     t = CTuning.default()
@@ -106,6 +139,15 @@ def test_bad_tunings_are_refused():
         b.set_tuning(t)
     g = Context(gen.two_material(16, 8, 8, cycles=5))
     t = CTuning.default()
-    t.lines_per_block[3] = 16                     # K > 1 meshes keep 8 lines
+    t.lines_per_block[3] = 32                     # several environments: cell y/z sweeps 8 or 16
+    with pytest.raises(MhyError):
+        g.set_tuning(t)
+    t = CTuning.default()
+    t.lines_per_block[6] = 16                     # and their node sweeps keep 8
+    with pytest.raises(MhyError):
+        g.set_tuning(t)
+    g = Context(gen.sod(cycles=5, options=gen.Options(ordre_projection=3)))
+    t = CTuning.default()
+    t.lines_per_block[4] = 16                     # order 3 keeps 8 lines
     with pytest.raises(MhyError):
         g.set_tuning(t)
