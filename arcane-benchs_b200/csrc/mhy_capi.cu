@@ -191,6 +191,18 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (opt->schema_csts != 0 && opt->schema_csts != 1) return fail(MHY_ERR_ARG, "schema_csts must be 0 or 1");
   if (opt->schema_csts && (opt->nb_env != 1 || opt->precision != 0))
     return fail(MHY_ERR_UNSUPPORTED, "schema-csts: one environment in FP64 on the device");
+  if (opt->projection_pente_borne != 0 && opt->projection_pente_borne != 1)
+    return fail(MHY_ERR_ARG, "projection_pente_borne must be 0 or 1");
+  if (opt->pente_borne_mixte != 0 && opt->pente_borne_mixte != 1)
+    return fail(MHY_ERR_ARG, "pente_borne_mixte must be 0 or 1");
+  if (opt->pente_borne_debar_fix < 0 || opt->pente_borne_debar_fix > 2)
+    return fail(MHY_ERR_ARG, "pente_borne_debar_fix must be 0, 1 or 2");
+  if (opt->limiteur_pure_id < 0 || opt->limiteur_pure_id > 7)
+    return fail(MHY_ERR_ARG, "limiteur_pure_id must be 0..7 (TypesMahyco.h:65-74)");
+  if ((opt->projection_pente_borne || opt->pente_borne_mixte) && (opt->nb_env != 1 || opt->precision != 0))
+    return fail(MHY_ERR_UNSUPPORTED, "pente-borne: one environment in FP64 on the device");
+  if (opt->projection_pente_borne && opt->ordre_projection != 2)
+    return fail(MHY_ERR_UNSUPPORTED, "pente-borne: ordre-projection 2 on the device");
   for (int b = 0; b < opt->nb_bc; ++b)
     if (opt->bc[b].surface < 0 || opt->bc[b].surface > 5 || opt->bc[b].type < 0 || opt->bc[b].type > 2)
       return fail(MHY_ERR_ARG, "bad boundary condition");
@@ -229,6 +241,15 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   ph.ordre_projection = opt->ordre_projection; ph.limiteur_id = opt->projection_limiteur_id;
   ph.precision = opt->precision;
   ph.csts = opt->schema_csts;
+  // with one environment every cell and its neighbours are pure, so
+  // projection-pente-borne-mixte selects the pure-cell forms everywhere
+  // (voisinage_pure, RemapADIService.cc:369-375)
+  ph.lim_cell = (opt->pente_borne_mixte && opt->limiteur_pure_id == 1) ? 1 : opt->projection_limiteur_id;
+  ph.pb = opt->projection_pente_borne;
+  ph.pb_pure = opt->pente_borne_mixte;
+  ph.pb_debar = opt->pente_borne_debar_fix;
+  ph.pb_lim_y0 = opt->pente_borne_mixte ? opt->limiteur_pure_id : opt->projection_limiteur_id;
+  ph.pb_first = 0;
   c->bct.nb = opt->nb_bc;
   for (int b = 0; b < opt->nb_bc; ++b) { c->bct.type[b] = opt->bc[b].type; c->bct.value[b] = opt->bc[b].value; }
 
@@ -264,7 +285,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       A_(&c->fd.db[d], nf[d]); A_(&c->fd.df[d], nf[d]); A_(&c->fd.A[d], nf[d]);
       A_(&c->fd.u[d], nf[d]);
     }
-    if (opt->ordre_projection == 3 || opt->projection_limiteur_id >= 3) A_(&c->fd.h, 3 * C);   // cell widths
+    if (opt->ordre_projection == 3 || opt->projection_limiteur_id >= 3 || opt->projection_pente_borne)
+      A_(&c->fd.h, 3 * C);                                                                      // cell widths
+    if (opt->projection_pente_borne) A_(&c->fd.pbphi, 3 * C);
     if (opt->ordre_projection == 3) A_(&c->fd.phi3, 4 * std::max(nf[0], std::max(nf[1], nf[2])));
   }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
@@ -653,6 +676,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
     if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
     if (opts[i].projection_limiteur_id >= 3)
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters are not batched");
+    if (opts[i].projection_pente_borne || opts[i].pente_borne_mixte)
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: pente-borne is not batched");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();
@@ -788,10 +813,10 @@ inline bool line_slot(int k) {
 // The line counts a context's sweeps are built for: 8, 16 or 32 on the y/z
 // sweeps of one environment at order 1 or 2 with the classic limiters; 8 or 16
 // on the cell y/z sweeps of several environments (their node sweeps keep 8);
-// 8 everywhere at order 3 or with the G limiters.
+// 8 everywhere at order 3, with the G limiters or with pente-borne.
 bool tunable_lines(const mhy_ctx* c, int k, int w) {
   if (!line_slot(k)) return w == kLineWarps;
-  if (c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3) return w == kLineWarps;
+  if (c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3 || c->ph.pb) return w == kLineWarps;
   if (c->K > 1) return w == kLineWarps || ((k == BK_CELLS_Y || k == BK_CELLS_Z) && w == 16);
   return true;
 }
@@ -981,7 +1006,8 @@ int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
   for (int k = 0; k < BK_TUNE_SLOTS; ++k)
     if (u.lines_per_block[k] != kLineWarps && !tunable_lines(c, k, u.lines_per_block[k]))
       return fail(MHY_ERR_UNSUPPORTED,
-                  "lines_per_block: 8 or 16 on the cell y/z sweeps of several environments; 8 with order 3 or the G limiters");
+                  "lines_per_block: 8 or 16 on the cell y/z sweeps of several environments; 8 with order 3, "
+                  "the G limiters or pente-borne");
   apply_tuning(c, u);
   c->tuning = u;
   return MHY_OK;
@@ -993,7 +1019,7 @@ int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "autotune runs between cycles");
   if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
-  if (c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3) {   // these sweeps keep 8 lines
+  if (c->ph.ordre_projection == 3 || c->ph.limiteur_id >= 3 || c->ph.pb) {   // these sweeps keep 8 lines
     c->tuning = default_tuning();
     if (out) *out = c->tuning;
     return MHY_OK;

@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __re
 
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
-template <bool LAST, typename R, bool O3 = false, bool GL = false>
+template <bool LAST, typename R, bool O3 = false, bool GL = false, bool PB = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -161,7 +161,12 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   if (valid) {
     in.U[0] = Uin[c]; in.U[1] = Uin[C + c]; in.U[2] = Uin[2 * C + c]; in.U[3] = Uin[3 * C + c];
     in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
-    if constexpr (GL) in.h = fd.h[c];
+    if constexpr (GL || PB) in.h = fd.h[c];
+    if constexpr (PB) {
+      in.pb[0] = ph.pb_first ? fd.pbphi[c] : 0.; in.pb[1] = ph.pb_first ? fd.pbphi[C + c] : 0.;
+      in.pb[2] = fd.pbphi[2 * C + c];
+      in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c];      // every lane's two faces take part
+    }
   }
   if (inner) {
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
@@ -177,7 +182,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
     if (LAST) in.vol = st.Ve[c];
   }
   double out[LAST ? kCellOutLast : kCellOutMid];
-  cell_line<LAST, R, O3, GL>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3, GL, PB>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   if (!upd) return;
   if (!LAST) {
 #pragma unroll
@@ -189,12 +194,12 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   }
 }
 
-template <bool LAST, typename R, bool O3 = false, bool GL = false>
+template <bool LAST, typename R, bool O3 = false, bool GL = false, bool PB = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_cells_x(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_x_body<LAST, R, O3, GL>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
+  k_cyc_sweep_cells_x_body<LAST, R, O3, GL, PB>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
                                         blockIdx.z);
 }
 
@@ -208,7 +213,7 @@ struct CellTileSize {
   static constexpr size_t bytes = (size_t)NA * TileGeom<W>::arr * sizeof(double);
 };
 
-template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false>
+template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false, bool PB = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
@@ -270,9 +275,15 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
   in.vol = LAST ? row[(NB - 1) * kTileArr] : 0.;
   in.h = 0.;
-  if (GL && valid) {
+  in.pb[0] = in.pb[1] = in.pb[2] = 0.;
+  if ((GL || PB) && valid) {
     const int i = i0 + w;
-    in.h = fd.h[D * C + (D == 1 ? i + dm.nx * (s + dm.ny * o) : i + dm.nx * (o + dm.ny * s))];
+    const int c = D == 1 ? i + dm.nx * (s + dm.ny * o) : i + dm.nx * (o + dm.ny * s);
+    in.h = fd.h[D * C + c];
+    if constexpr (PB) {
+      if (ph.pb_first) { in.pb[0] = fd.pbphi[c]; in.pb[1] = fd.pbphi[C + c]; }
+      in.pb[2] = fd.pbphi[2 * C + c];
+    }
   }
   if constexpr (O3) {
 #pragma unroll
@@ -280,7 +291,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
   constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
   double out[NO];
-  cell_line<LAST, R, O3, GL>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3, GL, PB>(ph, S->dt, S, valid, inner, infr, upd, in, out);
   // each lane overwrites only the tile column it read itself
   if (upd) {
 #pragma unroll
@@ -299,12 +310,12 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   }
 }
 
-template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false>
+template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false, bool PB = false>
 __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_cells_t(Dims dm, const Scalars* __restrict__ S,
     Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
     const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
     double* __restrict__ dpf, CellState st) {
-  k_cyc_sweep_cells_t_body<D, LAST, R, W, O3, GL>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
+  k_cyc_sweep_cells_t_body<D, LAST, R, W, O3, GL, PB>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, st, blockIdx.x, blockIdx.y,
                                               blockIdx.z);
 }
 
@@ -324,13 +335,13 @@ void smem_opt_in(const void* kernel, size_t bytes) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false>
+template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false, bool PB = false>
 static void sweep_cells_t_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
   const size_t smem = CellTileSize<LAST, W, O3>::bytes;
-  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W, O3, GL>;
+  auto kern = k_cyc_sweep_cells_t<D, LAST, R, W, O3, GL, PB>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
 }
@@ -338,7 +349,8 @@ static void sweep_cells_t_w(const CycleArgs& a, const double* Uin, double* Uout,
 template <int D, bool LAST, typename R>
 static void sweep_cells_t(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   if constexpr (sizeof(R) == 8) {
-    const bool o3 = a.ph.ordre_projection == 3, gl = a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
+    const bool o3 = a.ph.ordre_projection == 3, gl = a.ph.ordre_projection > 1 && a.ph.lim_cell >= 3;
+    if (a.ph.pb) { sweep_cells_t_w<D, LAST, R, kLineWarps, false, false, true>(a, Uin, Uout, s); return; }
     if (o3 && gl) { sweep_cells_t_w<D, LAST, R, kLineWarps, true, true>(a, Uin, Uout, s); return; }
     if (o3) { sweep_cells_t_w<D, LAST, R, kLineWarps, true, false>(a, Uin, Uout, s); return; }
     if (gl) { sweep_cells_t_w<D, LAST, R, kLineWarps, false, true>(a, Uin, Uout, s); return; }
@@ -357,7 +369,14 @@ static void sweep_cells_d(const CycleArgs& a, bool last, const double* Uin, doub
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
     const bool o3 = sizeof(R) == 8 && a.ph.ordre_projection == 3;
-    const bool gl = sizeof(R) == 8 && a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
+    const bool gl = sizeof(R) == 8 && a.ph.ordre_projection > 1 && a.ph.lim_cell >= 3;
+    if constexpr (sizeof(R) == 8) {
+      if (a.ph.pb) {
+        auto kern = last ? k_cyc_sweep_cells_x<true, R, false, false, true> : k_cyc_sweep_cells_x<false, R, false, false, true>;
+        kern<<<g, T, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.st);
+        return;
+      }
+    }
     if (o3 || gl) {
       auto kern = o3 ? (gl ? (last ? k_cyc_sweep_cells_x<true, R, true, true> : k_cyc_sweep_cells_x<false, R, true, true>)
                            : (last ? k_cyc_sweep_cells_x<true, R, true, false> : k_cyc_sweep_cells_x<false, R, true, false>))
@@ -517,11 +536,13 @@ __global__ void __launch_bounds__(128) k_o3_faces(Dims dm, const Scalars* __rest
 }
 
 template <typename R>
-static void remap_impl(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
+static void remap_impl(const CycleArgs& a0, int sens, cudaStream_t s, KernelMarks* m) {
   int prev = 0;
+  CycleArgs a = a0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
     const bool first = it == 0, last = it == 2;
+    a.ph.pb_first = first;
     const double* uin = a.U[it & 1];
     double* uout = a.U[(it + 1) & 1];
     const double* udin = a.ud[(it + 1) & 1];

@@ -29,6 +29,12 @@ struct Phys {
   double pinf;          // its limit-tension
   int with_newton;      // Lagrange energy update by Newton iterations
   int csts;             // schema-csts time scheme (one environment, FP64)
+  int lim_cell;         // limiter of the cell gradients: limiteur_id, or the pure-cell limiter when
+                        // projection-pente-borne-mixte and projection-limiteur-pure-id 1 (RemapADIService.cc:369-375)
+  // projection-pente-borne (one environment, FP64, order 2): the flux variant
+  // (0: computeFluxPP, 1: computeFluxPPPure), its debar fix, the limiter of its
+  // reconstruction (computeY0), and whether the sweep is the first of the cycle
+  int pb, pb_pure, pb_debar, pb_lim_y0, pb_first;
 };
 
 struct BCTable {
@@ -47,6 +53,8 @@ struct FaceData {
   double* u[3];
   double* h;      // order 3: cell widths along each direction, 3 planes of C (RemapADIService.cc:225-258)
   double* phi3;   // order 3: face values of the current sweep, [4][faces of its direction]
+  double* pbphi;  // pente-borne: rho, e and q after the Lagrange step, 3 planes of C (Phi of the first
+                  // sweep, PrepareRemap.cc:201-212; q stays the Phi of q in every sweep)
 };
 
 // Persistent cell state (global values of a single-environment mesh).

@@ -389,6 +389,7 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     U[C + c] = V * nd;
     U[2 * C + c] = V * nd * en;
     U[3 * C + c] = V * qn;
+    if (fd.pbphi) { fd.pbphi[c] = nd; fd.pbphi[C + c] = en; fd.pbphi[2 * C + c] = qn; }
   } else {
     lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag);
   }

@@ -157,6 +157,113 @@ __device__ __forceinline__ void face_value(R order2, bool back, R dot_xf, const 
   for (int v = 0; v < 4; ++v) Pf[v] = back ? (Pp[v] + order2 * dot_xf * Gp[v]) : (Pn[v] + order2 * dot_xf * Gn[v]);
 }
 
+// ---- pente-borne (projection-pente-borne; FP64, one environment) ----------
+// INTY (UtilesRemap.cc:83-93): integral from -infinity to X of the segment
+// from (x0, y0) to (x1, y1), zero left of it and constant right of it.
+__device__ __forceinline__ double pb_inty(double X, double x0, double y0, double x1, double y1, double thr) {
+  double flux = 0.;
+  if (fabs(x1 - x0) > thr) {
+    const double eta = amin(amax(0., (X - x0) / (x1 - x0)), 1.);
+    flux = (y0 + 0.5 * eta * (y1 - y0)) * (x1 - x0) * eta;
+  }
+  return flux;
+}
+
+// computeY0 (UtilesRemap.cc:184-238): the values of the reconstruction at the
+// back and front ends of the cell, by limiter (ids of TypesMahyco.h:65-74).
+__device__ __forceinline__ void pb_y0(int id, double yplus, double ymoins, double h0, double hplus, double hmoins,
+                                      double& y0plus, double& y0moins) {
+  y0plus = 0.; y0moins = 0.;
+  if (id == 3 || id == 0) {
+    y0plus = yplus; y0moins = ymoins;
+  } else if (id == 4 || id == 1) {
+    y0plus = ((h0 + hmoins) * yplus + h0 * ymoins) / (2 * h0 + hmoins);
+    y0moins = ((h0 + hplus) * ymoins + h0 * yplus) / (2 * h0 + hplus);
+  } else if (id == 5 || id == 2) {
+    const double a = amin(yplus, ymoins), b = amax(yplus, ymoins);
+    double xplus = (h0 * h0 + 3 * h0 * hmoins + 2 * hmoins * hmoins) * yplus;
+    double xmoins = (h0 * h0 + 3 * h0 * hplus + 2 * hplus * hplus) * ymoins;
+    xplus += (h0 * h0 - h0 * hplus - 2 * hplus * hplus + 2 * h0 * hmoins) * ymoins;
+    xmoins += (h0 * h0 - h0 * hmoins - 2 * hmoins * hmoins + 2 * h0 * hplus) * yplus;
+    xplus /= (2 * h0 * h0 + 5 * h0 * hmoins + 2 * hmoins * hmoins - h0 * hplus - 2 * hplus * hplus);
+    xmoins /= (2 * h0 * h0 + 5 * h0 * hplus + 2 * hplus * hplus - h0 * hmoins - 2 * hmoins * hmoins);
+    y0plus = amin(amax(xplus, a), b);
+    y0moins = amin(amax(xmoins, a), b);
+  } else if (id == 7) {
+    y0plus = (yplus + ymoins) / 2.;
+    y0moins = (yplus + ymoins) / 2.;
+  } else if (id == 6) {
+    y0plus = ((h0 + hmoins + hplus) * yplus + h0 * ymoins) / (2 * h0 + hmoins + hplus);
+    y0moins = ((h0 + hmoins + hplus) * ymoins + h0 * yplus) / (2 * h0 + hmoins + hplus);
+  }
+}
+
+// One variable of computeFluxPP / computeFluxPPPure (UtilesRemap.cc:406-489,
+// 628-705) before the debar fix: the integral of the three-piece
+// reconstruction (computexgxd :246-266, computeygyd :276-296) over the
+// length ppv next to the back (type 0) or front (type 1) face, or
+// y0 * ppv where the cell is an extremum (formule 16).
+__device__ __forceinline__ double pb_flux_var(int type, int lim_y0, double thr, double ppv, double y0, double yplus,
+                                              double ymoins, double h0, double hplus, double hmoins, double grady) {
+  double y0plus, y0moins;
+  pb_y0(lim_y0, yplus, ymoins, h0, hplus, hmoins, y0plus, y0moins);
+  double xplus = 1.;
+  if (fabs(y0plus - yplus) > thr) xplus = (y0 - yplus) / (y0plus - yplus) - 1. / 2.;
+  double xmoins = 1.;
+  if (fabs(y0moins - ymoins) > thr) xmoins = (y0 - ymoins) / (y0moins - ymoins) - 1. / 2.;
+  const double xd = +h0 * amin(amax(xplus, -1. / 2.), 1. / 2.);
+  const double xg = -h0 * amin(amax(xmoins, -1. / 2.), 1. / 2.);
+  const double xtd = y0 + h0 / 2 * grady;
+  const double xtg = y0 - h0 / 2 * grady;
+  const double ad = amin(yplus, 2. * y0moins - ymoins), bd = amax(yplus, 2. * y0moins - ymoins);
+  const double ag = amin(ymoins, 2. * y0plus - yplus), bg = amax(ymoins, 2. * y0plus - yplus);
+  const double yd = amin(amax(xtd, ad), bd);
+  const double yg = amin(amax(xtg, ag), bg);
+  double f1, f2, f3, f1m, f2m, f3m;
+  if (type == 0) {
+    f1m = pb_inty(-h0 / 2. + ppv, -h0 / 2., ymoins, xg, yg, thr);
+    f1 = pb_inty(-h0 / 2., -h0 / 2., ymoins, xg, yg, thr);
+    f2m = pb_inty(-h0 / 2. + ppv, xg, yg, xd, yd, thr);
+    f2 = pb_inty(-h0 / 2., xg, yg, xd, yd, thr);
+    f3m = pb_inty(-h0 / 2. + ppv, xd, yd, h0 / 2., yplus, thr);
+    f3 = pb_inty(-h0 / 2., xd, yd, h0 / 2., yplus, thr);
+  } else {
+    f1 = pb_inty(h0 / 2. - ppv, -h0 / 2., ymoins, xg, yg, thr);
+    f1m = pb_inty(h0 / 2., -h0 / 2., ymoins, xg, yg, thr);
+    f2 = pb_inty(h0 / 2. - ppv, xg, yg, xd, yd, thr);
+    f2m = pb_inty(h0 / 2., xg, yg, xd, yd, thr);
+    f3 = pb_inty(h0 / 2. - ppv, xd, yd, h0 / 2., yplus, thr);
+    f3m = pb_inty(h0 / 2., xd, yd, h0 / 2., yplus, thr);
+  }
+  double flux = tmax<double>(((f1m - f1) + (f2m - f2) + (f3m - f3)), 0.);
+  if (((yplus - y0) * (ymoins - y0)) >= 0.) flux = y0 * ppv;
+  return flux;
+}
+
+// The four fluxes (volume, mass, energy, q) leaving the cell through one
+// face, debar fix included (UtilesRemap.cc:518-619, 709-819; the momentum and
+// kinetic-energy variables have Phi = 0 and move nothing).
+__device__ __forceinline__ void pb_fluxes(const Phys& ph, int type, double ppv, const double P[4], const double Pn[4],
+                                          const double Pp[4], double h0, double hp, double hm, const double G[4],
+                                          double F[4]) {
+  const double thr = ph.threshold;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) F[v] = pb_flux_var(type, ph.pb_lim_y0, thr, ppv, P[v], Pn[v], Pp[v], h0, hp, hm, G[v]);
+  if (ph.pb_debar == 1) {
+    const double svol = 0. + F[0];
+    if (fabs(svol) > thr) {
+      if (!ph.pb_pure) F[1] = (F[1] / svol) * F[0];
+      F[2] = (F[2] / svol) * F[1];
+    } else {
+      F[0] = F[1] = F[2] = F[3] = 0.;
+    }
+  } else if (ph.pb_debar == 2) {
+    if (!ph.pb_pure) F[1] = P[1] * F[0];
+    F[2] = P[2] * F[1];
+  }
+  if (ppv == 0.) F[0] = F[1] = F[2] = F[3] = 0.;
+}
+
 // ---- cells ---------------------------------------------------------------
 // Inputs of one lane (one cell of a line along d).
 struct CellIn {
@@ -166,6 +273,7 @@ struct CellIn {
   double vol;                  // initial cell volume (last sweep only)
   double pf3[4];               // order 3: Phi of the low face from k_o3_faces
   double h;                    // G limiters: cell width along d (RemapADIService.cc:225-258)
+  double pb[3];                // pente-borne: rho and e (first sweep only) and the q of the remap's start
 };
 constexpr int kCellOutLast = 7;   // rho, e, q, mass, p, c, dual mass flux
 constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
@@ -174,14 +282,30 @@ constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
 // values and computeUremap_PBorn0 (RemapADIService.cc:91-271, 447-517, 658-720,
 // 909-987).  Every lane takes part in the shuffles; lanes with upd set get
 // their cell's results in out.  The boundary faces of d carry Phi_f = 0 and
-// contribute nothing.
-template <bool LAST, typename R = double, bool O3 = false, bool GL = false>
+// contribute nothing.  PB: the pente-borne form (R = double): Phi of
+// PrepareRemap.cc:201-212 (first sweep) or RemapADIService.cc:805-834, the
+// general gradient (R:319-378), face values from the fluxes leaving the two
+// cells (R:380-431, 574-578) and fluxes o*A*Phi_f (R:770-774).
+template <bool LAST, typename R = double, bool O3 = false, bool GL = false, bool PB = false>
 __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
                                           bool infr, bool upd, const CellIn& in, double* out) {
   const R order2 = (R)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  const int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
   R P[4] = {0, 0, 0, 0};
-  if (valid) phi_of<R>(in.U, P);
+  if constexpr (PB) {
+    if (valid) {
+      if (ph.pb_first) {
+        P[0] = 1.; P[1] = in.pb[0]; P[2] = in.pb[1];      // volume fraction, density, internal energy
+      } else {
+        P[0] = in.U[0] / (0. + in.U[0]);
+        P[1] = in.U[0] != 0. ? in.U[1] / in.U[0] : 0.;
+        P[2] = in.U[1] != 0. ? in.U[2] / in.U[1] : 0.;
+      }
+      P[3] = in.pb[2];
+    }
+  } else {
+    if (valid) phi_of<R>(in.U, P);
+  }
   const unsigned full = 0xffffffffu;
   const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
                xpz = __shfl_up_sync(full, in.xc[2], 1);
@@ -192,10 +316,39 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
   R g[4], gr[4], G[4], Pp[4], Gp[4], Pf[4];
 #pragma unroll
   for (int v = 0; v < 4; ++v) Pp[v] = __shfl_up_sync(full, P[v], 1);
-  face_grad<R>(inner, (R)dx, P, Pp, g);
+  if constexpr (PB) {
+    const R r = inner ? Ar<R>::rcp((R)dx) : R(0);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) g[v] = inner ? Ar<R>::div(P[v] - Pp[v], (R)dx, r) : R(0);
+  } else {
+    face_grad<R>(inner, (R)dx, P, Pp, g);
+  }
 #pragma unroll
   for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
-  if constexpr (GL) {
+  if constexpr (PB) {
+    static_assert(sizeof(R) == 8, "pente-borne is FP64");
+    double Pn[4], Pne[4], Ppe[4], ar[4], av[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Pn[v] = __shfl_down_sync(full, P[v], 1);
+    const double hb = __shfl_up_sync(full, in.h, 1), hn = __shfl_down_sync(full, in.h, 1);
+    const double h0 = in.h, hm = inner ? hb : in.h, hp = infr ? hn : in.h;   // the cell itself at the ends
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { Pne[v] = infr ? Pn[v] : P[v]; Ppe[v] = inner ? Pp[v] : P[v]; }
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      G[v] = lim < 3 ? limited_one<R>(lim, g[v], gr[v])
+                     : flux_limiter_g<R>(lim, gr[v], g[v], P[v], Pne[v], Ppe[v], h0, hp, hm);
+    const double un = __shfl_down_sync(full, in.u, 1);
+    const double ob = in.ob * in.u, of = in.of * un;                 // outward velocities of the two faces
+    pb_fluxes(ph, 0, 0.5 * (ob + fabs(ob)) * dt, P, Pne, Ppe, h0, hp, hm, G, ar);
+    pb_fluxes(ph, 1, 0.5 * (of + fabs(of)) * dt, P, Pne, Ppe, h0, hp, hm, G, av);
+    // back face: what leaves the previous cell forwards minus what leaves this one backwards
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double avp = __shfl_up_sync(full, av[v], 1);
+      Pf[v] = inner ? avp - ar[v] : 0.;
+    }
+  } else if constexpr (GL) {
     // generalised limiters (RemapADIService.cc:319-437 -> UtilesRemap.cc:295-330):
     // back and front cells are the cell itself at the ends of the line
     R Pn[4];
@@ -211,7 +364,8 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
   }
 #pragma unroll
   for (int v = 0; v < 4; ++v) Gp[v] = __shfl_up_sync(full, G[v], 1);
-  if (inner) {
+  if constexpr (PB) {
+  } else if (inner) {
     if constexpr (O3) {                                   // order 3: R:583-641, computed per face beforehand
 #pragma unroll
       for (int v = 0; v < 4; ++v) Pf[v] = (R)in.pf3[v];
@@ -232,8 +386,8 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
   // mass flux sum 0.5*flux*o, clamping of mass and energy (R:909-987); the
   // sums are FP64 in every precision (each face flux is one rounded value,
   // subtracted from one cell and added to the other)
-  const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
-  const double cf = infr ? in.of * un * An * dt : 0.;
+  const double cb = inner ? (PB ? in.ob * in.A : in.ob * in.u * in.A * dt) : 0.;
+  const double cf = infr ? (PB ? in.of * An : in.of * un * An * dt) : 0.;
   double u[4], dpm = 0.;
 #pragma unroll
   for (int v = 0; v < 4; ++v) {

@@ -48,7 +48,7 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
                                               bool upd, const CellInK<K>& in, double* out) {
   constexpr int NV = 3 * K + 1;
   const R order2 = (R)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
+  const int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
   R P[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) P[v] = 0;

@@ -87,7 +87,10 @@ class COptions(ctypes.Structure):
                 ("nb_bc", ctypes.c_int32), ("bc", BC * MHY_MAX_BC), ("nb_env", ctypes.c_int32),
                 ("adiabatic_cst", ctypes.c_double * MHY_MAX_ENV), ("precision", ctypes.c_int32),
                 ("eos", ctypes.c_int32 * MHY_MAX_ENV), ("limit_tension", ctypes.c_double * MHY_MAX_ENV),
-                ("with_newton", ctypes.c_int32), ("schema_csts", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("with_newton", ctypes.c_int32), ("schema_csts", ctypes.c_int32),
+                ("projection_pente_borne", ctypes.c_int32), ("pente_borne_debar_fix", ctypes.c_int32),
+                ("pente_borne_mixte", ctypes.c_int32), ("limiteur_pure_id", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 1)]
 
 
 class CMesh(ctypes.Structure):
@@ -197,6 +200,10 @@ def make_options(opts, gammas) -> COptions:
         o.adiabatic_cst[k] = float(g)
     o.with_newton = int(getattr(opts, "with_newton", 0))
     o.schema_csts = int(getattr(opts, "schema_csts", 0))
+    o.projection_pente_borne = int(getattr(opts, "pente_borne", 0))
+    o.pente_borne_debar_fix = int(getattr(opts, "pente_borne_debar_fix", 0))
+    o.pente_borne_mixte = int(getattr(opts, "pente_borne_mixte", 0))
+    o.limiteur_pure_id = int(getattr(opts, "limiteur_pure_id", 0))
     for k, kind in enumerate(getattr(opts, "eos", ()) or ()):
         o.eos[k] = int(kind)
     for k, v in enumerate(getattr(opts, "limit_tension", ()) or ()):

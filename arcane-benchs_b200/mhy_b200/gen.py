@@ -70,6 +70,10 @@ class Options:
     limit_tension: tuple = ()               # per environment: StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
     with_newton: int = 0                    # energy update by Newton iterations (Mahyco.axl:308)
     schema_csts: int = 0                    # the CSTS time scheme (Mahyco.axl:238)
+    pente_borne: int = 0                    # projection-pente-borne (RemapADI.axl:167)
+    pente_borne_debar_fix: int = 0          # projection-pente-borne-debar-fix: 0, 1 or 2 (RemapADI.axl:171)
+    pente_borne_mixte: int = 0              # projection-pente-borne-mixte (RemapADI.axl:155)
+    limiteur_pure_id: int = 0               # projection-limiteur-pure-id (RemapADI.axl:163)
 
 
 @dataclasses.dataclass

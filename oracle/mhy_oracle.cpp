@@ -93,6 +93,9 @@ struct Oracle {
   int pseudo_centree, ordre_projection, limiteur_id, use_project_pow;
   int with_newton = 0;              // Mahyco.axl:308 with-newton
   int schema_csts = 0;              // Mahyco.axl:238 schema-csts
+  // RemapADI.axl:155-173: projection-pente-borne, -debar-fix (0, 1, 2),
+  // projection-pente-borne-mixte, projection-limiteur-pure-id
+  int pente_borne = 0, pb_debar_fix = 0, pb_mixte = 0, limiteur_pure_id = 0;
   std::vector<double> gamma;
   std::vector<int> eos;             // per environment: 0 PerfectGas, 1 StiffenedGas
   std::vector<double> pinf;         // StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
@@ -117,6 +120,7 @@ struct Oracle {
   std::vector<double> back_flux_contrib_env, front_flux_contrib_env;
   std::vector<int> est_mixte, est_pure;
   std::vector<double> h_cell;                  // cell width along the sweep direction (order 3)
+  std::vector<double> delta_phi_face_av, delta_phi_face_ar;   // pente-borne: C*nvars
   double global_deltat = 0, global_old_deltat = 0, old_deltat = 0, global_time = 0;
   int sens_projection = 0;
   long iteration = 0;
@@ -693,7 +697,7 @@ struct Oracle {
   }
 
   // ---------------- remap (P:448-563) ----------------
-  void computeVariablesForRemap_PBorn0() {  // P:258-437
+  void computeVariablesForRemap() {  // P:159-245, and its specialisation _PBorn0 P:258-437
     const int ne = K;
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < C; ++c) {
@@ -717,7 +721,19 @@ struct Oracle {
         }
       }
       double* P = &phi_lag[(size_t)c * nvars];
-      for (int v = 0; v < nvars; ++v) P[v] = U[v] / cell_volume.g[c];
+      if (pente_borne) {  // P:201-212: volume fraction, density, internal energy, q of each environment
+        auto set_phi = [&](int k, double f, double r, double e, double q) {
+          P[k] = f; P[ne + k] = r; P[2 * ne + k] = e;
+          P[3 * ne + 0] = 0.; P[3 * ne + 1] = 0.; P[3 * ne + 2] = 0.; P[3 * ne + 3] = 0.;
+          P[3 * ne + 4] = q;
+        };
+        if (e >= 0) set_phi(e, fracvol.g[c], density.g[c], internal_energy.g[c], pseudo_viscosity.g[c]);
+        else
+          for (int k = 0; k < K; ++k) if (env_mask[c] >> k & 1)
+            set_phi(k, fracvol.p[k][c], density.p[k][c], internal_energy.p[k][c], pseudo_viscosity.p[k][c]);
+      } else {
+        for (int v = 0; v < nvars; ++v) P[v] = U[v] / cell_volume.g[c];
+      }
     }
 #pragma omp parallel for schedule(static)
     for (long n = 0; n < N; ++n) {
@@ -844,8 +860,129 @@ struct Oracle {
     return grady;
   }
 
+  // ---- pente-borne (projection-pente-borne), UtilesRemap.cc ----
+  // INTY, :83-93: integral from -infinity to X of the segment (x0,y0)-(x1,y1)
+  double inty(double X, double x0, double y0, double x1, double y1) const {
+    double flux = 0.;
+    if (std::fabs(x1 - x0) > threshold) {
+      const double eta = amin(amax(0., (X - x0) / (x1 - x0)), 1.);
+      flux = (y0 + 0.5 * eta * (y1 - y0)) * (x1 - x0) * eta;
+    }
+    return flux;
+  }
+  // computeY0, :184-238 (limiter ids of TypesMahyco.h:65-74; 3000 as minmod)
+  static void compute_y0(int id, double yplus, double ymoins, double h0, double hplus, double hmoins, double& y0plus,
+                         double& y0moins) {
+    y0plus = 0.; y0moins = 0.;
+    if (id == 3 || id == 0 || id == 3000) {
+      y0plus = yplus; y0moins = ymoins;
+    } else if (id == 4 || id == 1) {
+      y0plus = ((h0 + hmoins) * yplus + h0 * ymoins) / (2 * h0 + hmoins);
+      y0moins = ((h0 + hplus) * ymoins + h0 * yplus) / (2 * h0 + hplus);
+    } else if (id == 5 || id == 2) {
+      const double a = amin(yplus, ymoins), b = amax(yplus, ymoins);
+      double xplus = (h0 * h0 + 3 * h0 * hmoins + 2 * hmoins * hmoins) * yplus;
+      double xmoins = (h0 * h0 + 3 * h0 * hplus + 2 * hplus * hplus) * ymoins;
+      xplus += (h0 * h0 - h0 * hplus - 2 * hplus * hplus + 2 * h0 * hmoins) * ymoins;
+      xmoins += (h0 * h0 - h0 * hmoins - 2 * hmoins * hmoins + 2 * h0 * hplus) * yplus;
+      xplus /= (2 * h0 * h0 + 5 * h0 * hmoins + 2 * hmoins * hmoins - h0 * hplus - 2 * hplus * hplus);
+      xmoins /= (2 * h0 * h0 + 5 * h0 * hplus + 2 * hplus * hplus - h0 * hmoins - 2 * hmoins * hmoins);
+      y0plus = amin(amax(xplus, a), b);
+      y0moins = amin(amax(xmoins, a), b);
+    } else if (id == 7) {
+      y0plus = (yplus + ymoins) / 2.;
+      y0moins = (yplus + ymoins) / 2.;
+    } else if (id == 6) {
+      y0plus = ((h0 + hmoins + hplus) * yplus + h0 * ymoins) / (2 * h0 + hmoins + hplus);
+      y0moins = ((h0 + hmoins + hplus) * ymoins + h0 * yplus) / (2 * h0 + hmoins + hplus);
+    }
+  }
+  // computeFluxPP / computeFluxPPPure, :406-623 / :628-823: the integral of
+  // the three-piece reconstruction (computexgxd :246-266, computeygyd
+  // :276-296) over the part of the cell that leaves through the back (type
+  // 0) or front (type 1) face in dt; the debar fixes on top.  The reference
+  // calls abs() on doubles (the floating-point overload).
+  void compute_flux_pp(long c, long fc, long bc, double face_normal_velocity_out, double deltat_n, int type,
+                       bool pure, double* Flux) const {
+    const int nbmat = K;
+    for (int v = 0; v < nvars; ++v) Flux[v] = 0.;
+    const double ppv = 0.5 * (face_normal_velocity_out + std::fabs(face_normal_velocity_out)) * deltat_n;
+    const int lim_y0 = pure ? limiteur_pure_id : limiteur_id;
+    const double* P0 = &phi_lag[(size_t)c * nvars];
+    const double* Pf = &phi_lag[(size_t)fc * nvars];
+    const double* Pb = &phi_lag[(size_t)bc * nvars];
+    const double h0 = h_cell[c], hplus = h_cell[fc], hmoins = h_cell[bc];
+    for (int v = 0; v < nvars; ++v) {
+      double y0plus, y0moins;
+      compute_y0(lim_y0, Pf[v], Pb[v], h0, hplus, hmoins, y0plus, y0moins);
+      // computexgxd
+      double xplus = 1.;
+      if (std::fabs(y0plus - Pf[v]) > threshold) xplus = (P0[v] - Pf[v]) / (y0plus - Pf[v]) - 1. / 2.;
+      double xmoins = 1.;
+      if (std::fabs(y0moins - Pb[v]) > threshold) xmoins = (P0[v] - Pb[v]) / (y0moins - Pb[v]) - 1. / 2.;
+      const double xd = +h0 * amin(amax(xplus, -1. / 2.), 1. / 2.);
+      const double xg = -h0 * amin(amax(xmoins, -1. / 2.), 1. / 2.);
+      // computeygyd
+      const double grady = grad_phi[(size_t)c * nvars + v];
+      const double xtd = P0[v] + h0 / 2 * grady;
+      const double xtg = P0[v] - h0 / 2 * grady;
+      const double ad = amin(Pf[v], 2. * y0moins - Pb[v]), bd = amax(Pf[v], 2. * y0moins - Pb[v]);
+      const double ag = amin(Pb[v], 2. * y0plus - Pf[v]), bg = amax(Pb[v], 2. * y0plus - Pf[v]);
+      const double yd = amin(amax(xtd, ad), bd);
+      const double yg = amin(amax(xtg, ag), bg);
+      double flux1, flux2, flux3, flux1m, flux2m, flux3m;
+      if (type == 0) {
+        flux1m = inty(-h0 / 2. + ppv, -h0 / 2., Pb[v], xg, yg);
+        flux1 = inty(-h0 / 2., -h0 / 2., Pb[v], xg, yg);
+        flux2m = inty(-h0 / 2. + ppv, xg, yg, xd, yd);
+        flux2 = inty(-h0 / 2., xg, yg, xd, yd);
+        flux3m = inty(-h0 / 2. + ppv, xd, yd, h0 / 2., Pf[v]);
+        flux3 = inty(-h0 / 2., xd, yd, h0 / 2., Pf[v]);
+      } else {
+        flux1 = inty(h0 / 2. - ppv, -h0 / 2., Pb[v], xg, yg);
+        flux1m = inty(h0 / 2., -h0 / 2., Pb[v], xg, yg);
+        flux2 = inty(h0 / 2. - ppv, xg, yg, xd, yd);
+        flux2m = inty(h0 / 2., xg, yg, xd, yd);
+        flux3 = inty(h0 / 2. - ppv, xd, yd, h0 / 2., Pf[v]);
+        flux3m = inty(h0 / 2., xd, yd, h0 / 2., Pf[v]);
+      }
+      Flux[v] = smax(((flux1m - flux1) + (flux2m - flux2) + (flux3m - flux3)), 0.);
+      if (((Pf[v] - P0[v]) * (Pb[v] - P0[v])) >= 0.) Flux[v] = P0[v] * ppv;   // formule 16
+    }
+    if (pb_debar_fix == 1) {
+      double somme_flux_masse = 0., somme_flux_volume = 0.;
+      for (int m = 0; m < nbmat; m++) somme_flux_volume += Flux[m];
+      if (std::fabs(somme_flux_volume) > threshold) {
+        for (int m = 0; m < nbmat; m++) {
+          if (!pure) Flux[nbmat + m] = (Flux[nbmat + m] / somme_flux_volume) * Flux[m];
+          Flux[2 * nbmat + m] = (Flux[2 * nbmat + m] / somme_flux_volume) * Flux[nbmat + m];
+          somme_flux_masse += Flux[nbmat + m];
+        }
+        Flux[3 * nbmat] = (Flux[3 * nbmat] / somme_flux_volume) * somme_flux_masse;
+        Flux[3 * nbmat + 1] = (Flux[3 * nbmat + 1] / somme_flux_volume) * somme_flux_masse;
+        Flux[3 * nbmat + 2] = (Flux[3 * nbmat + 2] / somme_flux_volume) * somme_flux_masse;
+        Flux[3 * nbmat + 3] = P0[3 * nbmat + 3] * somme_flux_volume;
+      } else {
+        for (int v = 0; v < nvars; ++v) Flux[v] = 0.;
+      }
+    } else if (pb_debar_fix == 2) {
+      double somme_flux_masse = 0., somme_flux_volume = 0.;
+      for (int m = 0; m < nbmat; m++) {
+        if (!pure) Flux[nbmat + m] = P0[nbmat + m] * Flux[m];
+        Flux[2 * nbmat + m] = P0[2 * nbmat + m] * Flux[nbmat + m];
+        somme_flux_masse += Flux[nbmat + m];
+        somme_flux_volume += Flux[m];
+      }
+      Flux[3 * nbmat] = P0[3 * nbmat] * somme_flux_masse;
+      Flux[3 * nbmat + 1] = P0[3 * nbmat + 1] * somme_flux_masse;
+      Flux[3 * nbmat + 2] = P0[3 * nbmat + 2] * somme_flux_masse;
+      Flux[3 * nbmat + 3] = P0[3 * nbmat + 3] * somme_flux_volume;
+    }
+    if (ppv == 0.) for (int v = 0; v < nvars; ++v) Flux[v] = 0.;
+  }
+
   void computeGradPhiFace(int idir) {  // R:91-271 (h_cell by cells, R:225-258; read at order 3 and by the G limiters)
-    if (ordre_projection == 3 || limiteur_id >= 3) {
+    if (ordre_projection == 3 || limiteur_id >= 3 || pente_borne) {
 #pragma omp parallel for schedule(static)
       for (long c = 0; c < C; ++c) {
         long cf[6]; cell_faces(c, cf);
@@ -874,18 +1011,46 @@ struct Oracle {
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < C; ++c)
       for (int v = 0; v < nvars; ++v) grad_phi[(size_t)c * nvars + v] = 0.;
+    if (pente_borne) {  // R:324-326
+      std::fill(delta_phi_face_av.begin(), delta_phi_face_av.end(), 0.0);
+      std::fill(delta_phi_face_ar.begin(), delta_phi_face_ar.end(), 0.0);
+    }
     if (ordre_projection <= 1) return;
-    if (limiteur_id >= 3) {  // general path R:319-437 -> computeAndLimitGradPhi R/UtilesRemap.cc:295-330
+    if (limiteur_id >= 3 || pente_borne || pb_mixte) {  // general path R:319-437
+      const R3 dirproj = r3(0.5 * (1 - idir) * (2 - idir), 1.0 * idir * (2 - idir), -0.5 * idir * (1 - idir));
+      const double deltat = global_deltat;
 #pragma omp parallel for schedule(static)
       for (long c = 0; c < C; ++c) {
         long cf[6]; cell_faces(c, cf);
-        long bf = cf[back_local_face(idir)], ff = cf[front_local_face(idir)];
+        const int lb = back_local_face(idir), lf = front_local_face(idir);
+        long bf = cf[lb], ff = cf[lf];
         const long bc = along(c, idir, -1), fc = along(c, idir, +1);   // the cell itself at the ends
-        for (int v = 0; v < nvars; ++v)
-          grad_phi[(size_t)c * nvars + v] =
-              flux_limiter_g(limiteur_id, grad_phi_face[(size_t)ff * nvars + v], grad_phi_face[(size_t)bf * nvars + v],
-                             phi_lag[(size_t)c * nvars + v], phi_lag[(size_t)fc * nvars + v],
-                             phi_lag[(size_t)bc * nvars + v], h_cell[c], h_cell[fc], h_cell[bc]);
+        const bool voisinage_pure = pb_mixte && est_mixte[c] == 0 && est_mixte[fc] == 0 && est_mixte[bc] == 0 &&
+                                    est_pure[c] == est_pure[fc] && est_pure[c] == est_pure[bc];
+        int lim = limiteur_id;
+        if (limiteur_pure_id == 1 && voisinage_pure) lim = limiteur_pure_id;
+        // computeAndLimitGradPhi, UtilesRemap.cc:306-333
+        for (int v = 0; v < nvars; ++v) {
+          const double gf = grad_phi_face[(size_t)ff * nvars + v], gb = grad_phi_face[(size_t)bf * nvars + v];
+          double g;
+          if (lim < 3) {
+            g = 0.;
+            if (gb != 0.) g += 0.5 * (limiter(lim, gf / gb) * gb);
+            if (gf != 0.) g += 0.5 * (limiter(lim, gb / gf) * gf);
+          } else {
+            g = flux_limiter_g(lim, gf, gb, phi_lag[(size_t)c * nvars + v], phi_lag[(size_t)fc * nvars + v],
+                               phi_lag[(size_t)bc * nvars + v], h_cell[c], h_cell[fc], h_cell[bc]);
+          }
+          grad_phi[(size_t)c * nvars + v] = g;
+        }
+        if (!pente_borne) continue;
+        // R:380-431: the pente-borne fluxes leaving the cell through its back
+        // (type 0) and front (type 1) faces; the dual flux computed there is
+        // overwritten by computeUremap (R:751), so it is not formed here
+        const double out_ar = dot(outer_face_normal[6 * c + lb], dirproj) * face_normal_velocity[bf];
+        const double out_av = dot(outer_face_normal[6 * c + lf], dirproj) * face_normal_velocity[ff];
+        compute_flux_pp(c, fc, bc, out_ar, deltat, 0, voisinage_pure, &delta_phi_face_ar[(size_t)c * nvars]);
+        compute_flux_pp(c, fc, bc, out_av, deltat, 1, voisinage_pure, &delta_phi_face_av[(size_t)c * nvars]);
       }
       return;
     }
@@ -913,7 +1078,7 @@ struct Oracle {
     return cid(i, j, k);
   }
 
-  void computeUpwindFaceQuantitiesForProjection(int idir) {  // R:530-545 -> _PBorn0_O2 R:658-720
+  void computeUpwindFaceQuantitiesForProjection(int idir) {  // R:530-581, its specialisation _PBorn0_O2 R:658-720
     std::fill(phi_face.begin(), phi_face.end(), 0.0);
     if (ordre_projection == 3) {  // R:583-641
       const double deltat = global_deltat;
@@ -945,6 +1110,17 @@ struct Oracle {
       }
       return;
     }
+    if (pente_borne) {  // R:574-578: the flux out of the previous cell minus the flux out of the next
+#pragma omp parallel for schedule(static)
+      for (long f = face_begin(idir); f < face_end(idir); ++f) {
+        long cb, cf;
+        if (!face_prev_next(f, idir, cb, cf)) continue;
+        for (int v = 0; v < nvars; ++v)
+          phi_face[(size_t)f * nvars + v] =
+              delta_phi_face_av[(size_t)cb * nvars + v] - delta_phi_face_ar[(size_t)cf * nvars + v];
+      }
+      return;
+    }
     const double order2 = (double)(ordre_projection - 1);
 #pragma omp parallel for schedule(static)
     for (long f = face_begin(idir); f < face_end(idir); ++f) {
@@ -957,7 +1133,7 @@ struct Oracle {
     }
   }
 
-  void computeUremap(int idir) {  // R:733-743 -> computeUremap_PBorn0 R:883-1040
+  void computeUremap(int idir) {  // R:733-840 (pente-borne), its specialisation computeUremap_PBorn0 R:883-1040
     const double deltat = global_deltat;
     const int nbmat = K;
 #pragma omp parallel for schedule(static)
@@ -974,7 +1150,9 @@ struct Oracle {
             double len = comp(face_length[f], idir);
             R3 ofn = outer_face_normal[6 * c + a];
             double od = comp(ofn, idir);
-            flux = od * u * len * deltat * phi_face[(size_t)f * nvars + v];
+            // pente-borne (R:770-774): Phi_f already holds the integrated flux
+            flux = pente_borne ? od * len * phi_face[(size_t)f * nvars + v]
+                               : od * u * len * deltat * phi_face[(size_t)f * nvars + v];
             flux_face += flux;
             dpf += 0.5 * flux * comp(ofn, idir);
           }
@@ -992,7 +1170,25 @@ struct Oracle {
       }
       double somme_volume = 0.;
       for (int m = 0; m < nbmat; ++m) somme_volume += U[m];
-      for (int v = 0; v < nvars; ++v) P[v] = U[v] / somme_volume;
+      if (pente_borne) {  // R:805-834: volume fractions, densities, velocity (x, y), specific energies
+        double somme_masse = 0.;
+        for (int m = 0; m < nbmat; ++m) {
+          P[m] = U[m] / somme_volume;
+          if (U[m] != 0.) P[nbmat + m] = U[nbmat + m] / U[m];
+          else P[nbmat + m] = 0.;
+          somme_masse += U[nbmat + m];
+        }
+        if (somme_masse != 0) {
+          P[3 * nbmat] = U[3 * nbmat] / somme_masse;
+          P[3 * nbmat + 1] = U[3 * nbmat + 1] / somme_masse;
+        }
+        for (int m = 0; m < nbmat; ++m) {
+          if (U[nbmat + m] != 0.) P[2 * nbmat + m] = U[2 * nbmat + m] / U[nbmat + m];
+          else P[2 * nbmat + m] = 0.;
+        }
+      } else {
+        for (int v = 0; v < nvars; ++v) P[v] = U[v] / somme_volume;
+      }
       int imatcell = 0, imatpure = -1;
       for (int m = 0; m < nbmat; ++m) {
         if (P[m] > 0.) { imatcell++; imatpure = m; }
@@ -1351,7 +1547,7 @@ struct Oracle {
 
   void remap() {  // P:448-563
     if (schema_csts) updateVelocityForward();             // P:456
-    computeVariablesForRemap_PBorn0();
+    computeVariablesForRemap();
     computeFaceQuantitesForRemap();
     // IRemap::appliRemap, R:19-60
     for (int i = 0; i < 3; ++i) {
@@ -1438,7 +1634,8 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
                  double cfl, double threshold, double deltat_init, double deltat_min, double deltat_max,
                  double final_time, int lc_mode, int pseudo_centree, int ordre_projection, int limiteur_id,
                  int nbc, const orc_bc* bcs, int use_project_pow, const int* eos, const double* pinf,
-                 int with_newton, int schema_csts) {
+                 int with_newton, int schema_csts, int pente_borne, int pb_debar_fix, int pb_mixte,
+                 int limiteur_pure_id) {
   Oracle* o = new Oracle();
   o->nx = nx; o->ny = ny; o->nz = nz; o->NX = nx + 1; o->NY = ny + 1; o->NZ = nz + 1;
   o->C = (long)nx * ny * nz; o->N = (long)o->NX * o->NY * o->NZ;
@@ -1450,6 +1647,8 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
   o->ordre_projection = ordre_projection; o->limiteur_id = limiteur_id; o->use_project_pow = use_project_pow;
   o->with_newton = with_newton;
   o->schema_csts = schema_csts;
+  o->pente_borne = pente_borne; o->pb_debar_fix = pb_debar_fix; o->pb_mixte = pb_mixte;
+  o->limiteur_pure_id = limiteur_pure_id;
   o->gamma.assign(gammas, gammas + nenv);
   o->eos.assign(nenv, 0);
   o->pinf.assign(nenv, 0.);
@@ -1481,6 +1680,7 @@ void* orc_create(int nx, int ny, int nz, const double* node_coords, int nenv, co
   o->back_flux_mass_env.assign((size_t)N * K, 0.); o->front_flux_mass_env.assign((size_t)N * K, 0.);
   o->back_flux_contrib_env.assign((size_t)C * K, 0.); o->front_flux_contrib_env.assign((size_t)C * K, 0.);
   o->est_mixte.assign(C, 0); o->est_pure.assign(C, 0); o->h_cell.assign(C, 0.);
+  if (pente_borne) { o->delta_phi_face_av.assign((size_t)C * nv, 0.); o->delta_phi_face_ar.assign((size_t)C * nv, 0.); }
   return o;
 }
 

@@ -43,7 +43,7 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         L.orc_create.restype = ctypes.c_void_p
         L.orc_create.argtypes = [ctypes.c_int] * 3 + [dp, ctypes.c_int, dp] + [ctypes.c_double] * 6 + \
-            [ctypes.c_int] * 5 + [ctypes.POINTER(_BC), ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp, ctypes.c_int, ctypes.c_int]
+            [ctypes.c_int] * 5 + [ctypes.POINTER(_BC), ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp] + [ctypes.c_int] * 6
         L.orc_init.argtypes = [ctypes.c_void_p, dp, dp, dp, dp]
         L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
@@ -95,7 +95,9 @@ class Oracle:
                               o.projection_limiteur_id, len(o.boundary_conditions), bcs,
                               1 if pow_mode == "project" else 0,
                               eos.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(pinf),
-                              int(getattr(o, "with_newton", 0)), int(getattr(o, "schema_csts", 0)))
+                              int(getattr(o, "with_newton", 0)), int(getattr(o, "schema_csts", 0)),
+                              int(getattr(o, "pente_borne", 0)), int(getattr(o, "pente_borne_debar_fix", 0)),
+                              int(getattr(o, "pente_borne_mixte", 0)), int(getattr(o, "limiteur_pure_id", 0)))
         fv = np.ascontiguousarray(case.fracvol, dtype=np.float64)
         de = np.ascontiguousarray(case.density, dtype=np.float64)
         pr = np.ascontiguousarray(case.pressure, dtype=np.float64)

@@ -1,0 +1,108 @@
+"""GPU parity of the pente-borne remap (projection-pente-borne: Phi of
+PrepareRemap.cc:201-212 and RemapADIService.cc:805-834, the general cell
+gradient R:319-378, the fluxes of computeFluxPP / computeFluxPPPure
+UtilesRemap.cc:406-823 with the reconstruction of :184-296 and INTY :83-93,
+the debar fixes, face values R:574-578 and fluxes o*A*Phi_f R:770-774)
+against the oracle, bit for bit; and the pure-neighbourhood limiter switch
+of projection-pente-borne-mixte (R:369-375) on the default remap."""
+import numpy as np
+import pytest
+
+import mhy_oracle
+from mhy_b200 import Batch, Context, MhyError, gen
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("density", "internal_energy", "velocity", "pressure", "pseudo_viscosity", "cell_mass", "node_mass",
+          "sound_speed")
+ERR_ARG, ERR_UNSUPPORTED = -1, -4
+
+
+def compare(case, cycles, chunk):
+    o, g = mhy_oracle.Oracle(case), Context(case)
+    dto, dtg = [o.scalars()["dt"]], [g.dt()[0]]
+    done = 0
+    while done < cycles:
+        n = min(chunk, cycles - done)
+        o.step(n)
+        g.step(n)
+        done += n
+        dto.append(o.scalars()["dt"])
+        dtg.append(g.dt()[0])
+    g.synchronize()
+    assert np.array_equal(np.array(dto), np.array(dtg)), "dt sequences differ"
+    for f in FIELDS:
+        a, b = o.field(f), g.field(f)
+        assert np.array_equal(a, b), f"{f}: {int((a != b).sum())} values differ"
+    assert g.status() == 0
+    return g
+
+
+@pytest.mark.parametrize("debar", [0, 1, 2])
+def test_pente_borne_sod_bitwise(debar):
+    compare(gen.sod(cycles=150, options=gen.Options(pente_borne=1, pente_borne_debar_fix=debar)), 150, 30)
+
+
+@pytest.mark.parametrize("limiter,debar", [(0, 1), (1, 2), (2, 1), (5, 2), (6, 1), (7, 0)])
+def test_pente_borne_sedov_jittered_bitwise(limiter, debar):
+    opts = gen.Options(pente_borne=1, pente_borne_debar_fix=debar, projection_limiteur_id=limiter)
+    compare(gen.sedov(n=18, cycles=60, options=opts), 60, 20)
+
+
+@pytest.mark.parametrize("pure_id,debar", [(1, 1), (2, 2), (4, 1), (0, 0)])
+def test_pente_borne_mixte_pure_forms_bitwise(pure_id, debar):
+    """One environment: every neighbourhood is pure, so the pure-cell fluxes
+    (computeFluxPPPure) with projection-limiteur-pure-id apply, and the
+    gradient takes that limiter when it is 1."""
+    opts = gen.Options(pente_borne=1, pente_borne_mixte=1, limiteur_pure_id=pure_id, pente_borne_debar_fix=debar)
+    compare(gen.sedov(n=16, cycles=50, options=opts), 50, 25)
+
+
+def test_pente_borne_sod_along_z_with_newton_bitwise():
+    case = gen.sod(nx=5, ny=5, nz=60, lx=0.05, ly=0.05, lz=1.0, axis=2, cycles=100,
+                   options=gen.Options(pente_borne=1, pente_borne_debar_fix=1, with_newton=1))
+    compare(case, 100, 25)
+
+
+def test_pure_limiter_switch_without_pente_borne_bitwise():
+    """projection-pente-borne-mixte alone: the default remap, with the cell
+    gradients limited by superBee (limiteur-pure-id 1) while the dual ones
+    keep projection-limiteur-id."""
+    opts = gen.Options(pente_borne_mixte=1, limiteur_pure_id=1, projection_limiteur_id=2)
+    compare(gen.sedov(n=18, cycles=60, options=opts), 60, 30)
+
+
+def test_pente_borne_entry_points_match_graph():
+    case = gen.sedov(n=14, cycles=30, options=gen.Options(pente_borne=1, pente_borne_debar_fix=1))
+    a, b = Context(case), Context(case)
+    for _ in range(30):
+        a.cycle_by_entry_points()
+    b.step(30)
+    for f in ("density", "internal_energy", "velocity", "pseudo_viscosity"):
+        assert np.array_equal(a.field(f), b.field(f)), f
+
+
+def code_of(fn):
+    with pytest.raises(MhyError) as ei:
+        fn()
+    return ei.value.code
+
+
+@pytest.mark.parametrize("opts,code", [
+    (dict(pente_borne=1, ordre_projection=1), ERR_UNSUPPORTED),
+    (dict(pente_borne=1, ordre_projection=3), ERR_UNSUPPORTED),
+    (dict(pente_borne=1, precision=1), ERR_UNSUPPORTED),
+    (dict(pente_borne=1, pente_borne_debar_fix=3), ERR_ARG),
+    (dict(pente_borne=2), ERR_ARG),
+    (dict(pente_borne_mixte=1, limiteur_pure_id=8), ERR_ARG),
+])
+def test_unsupported_pente_borne_options_are_refused(opts, code):
+    assert code_of(lambda: Context(gen.sod(cycles=1, options=gen.Options(**opts)))) == code
+
+
+def test_pente_borne_refused_for_several_environments_and_batches():
+    opts = gen.Options(pente_borne=1)
+    assert code_of(lambda: Context(gen.two_material(16, 8, 8, cycles=1, options=opts))) == ERR_UNSUPPORTED
+    cases = gen.batched(count=2, seed=3, side_lo=8, side_hi=10, cycles=1)
+    cases[1].options.pente_borne = 1
+    assert code_of(lambda: Batch(cases)) == ERR_UNSUPPORTED
