@@ -1046,7 +1046,7 @@ struct Oracle {
         if (!pente_borne) continue;
         // R:380-431: the pente-borne fluxes leaving the cell through its back
         // (type 0) and front (type 1) faces; the dual flux computed there is
-        // overwritten by computeUremap (R:751), so it is not formed here
+        // overwritten by computeUremap (R:752), so it is not formed here
         const double out_ar = dot(outer_face_normal[6 * c + lb], dirproj) * face_normal_velocity[bf];
         const double out_av = dot(outer_face_normal[6 * c + lf], dirproj) * face_normal_velocity[ff];
         compute_flux_pp(c, fc, bc, out_ar, deltat, 0, voisinage_pure, &delta_phi_face_ar[(size_t)c * nvars]);
