@@ -350,8 +350,13 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
   }
   V *= 1. / 3;
   double Lc;
-  if (ph.lc_mode == 0) Lc = pow_third(V);
-  else {
+  // racine-cubique-volume: the project cube root (the reference's bits) in
+  // FP64; the mixed form takes CUDA's FP32 cube root of the FP64 volume (L
+  // feeds the viscosity and the CFL bound only)
+  if (ph.lc_mode == 0) {
+    if constexpr (F32) Lc = (double)cbrtf((float)V);
+    else Lc = pow_third(V);
+  } else {
     D3 fc[6];
     if constexpr (F32) {
       D3 xx[8];
