@@ -1204,35 +1204,21 @@ int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
     case MHY_FIELD_CARACTERISTIC_LENGTH: src = c->L; break;
     case MHY_FIELD_VELOCITY: src = c->v; vec = true; n = N; break;
     case MHY_FIELD_NODE_MASS: src = c->nm; n = N; break;
-    case MHY_FIELD_NODE_COORD: {
-      // Lagrangian coordinates of the last cycle: x0 + dt * v_half (MahycoModule.cc:899-901)
-      if (bytes < (size_t)N * 3 * sizeof(double)) return fail(MHY_ERR_ARG, "destination too small");
-      MHY_CUDA(cudaStreamSynchronize(c->stream));
-      std::vector<double> x0h(3 * N), vhh(3 * N);
-      Scalars h{};
-      MHY_CUDA(cudaMemcpy(&h, c->S, sizeof(h), cudaMemcpyDeviceToHost));
-      MHY_CUDA(cudaMemcpy(x0h.data(), c->x0, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
-      MHY_CUDA(cudaMemcpy(vhh.data(), c->vh, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
-      double* o = static_cast<double*>(dst);
-      const double dtu = h.iteration > 0 ? h.old_dt : 0.0;
-      for (long long i = 0; i < N; ++i)
-        for (int a = 0; a < 3; ++a) o[3 * i + a] = h.iteration > 0 ? x0h[a * N + i] + vhh[a * N + i] * dtu : x0h[a * N + i];
-      return MHY_OK;
-    }
+    case MHY_FIELD_NODE_COORD: src = c->x0; vec = true; n = N; break;   // x0 + dt * v_half, MahycoModule.cc:899-901
     default: return fail(MHY_ERR_ARG, "unknown field");
   }
   const size_t need = (size_t)n * (vec ? 3 : 1) * sizeof(double);
   if (bytes < need) return fail(MHY_ERR_ARG, "destination too small");
-  MHY_CUDA(cudaStreamSynchronize(c->stream));
-  if (!vec) {
-    MHY_CUDA(cudaMemcpy(dst, src, need, cudaMemcpyDeviceToHost));
-  } else {
-    std::vector<double> soa(3 * n);
-    MHY_CUDA(cudaMemcpy(soa.data(), src, need, cudaMemcpyDeviceToHost));
-    double* o = static_cast<double*>(dst);
-    for (long long i = 0; i < n; ++i)
-      for (int a = 0; a < 3; ++a) o[3 * i + a] = soa[a * n + i];
+  if (vec) {
+    // xyz interleaving on the device, into the dual remap variables (5N
+    // doubles), which hold nothing between entry-point calls
+    const bool coord = field == MHY_FIELD_NODE_COORD;
+    k_aos3<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, src, coord ? c->vh : nullptr, c->S, c->ud[0]);
+    MHY_CUDA(cudaGetLastError());
+    src = c->ud[0];
   }
+  MHY_CUDA(cudaMemcpyAsync(dst, src, need, cudaMemcpyDeviceToHost, c->stream));
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
   return MHY_OK;
 }
 

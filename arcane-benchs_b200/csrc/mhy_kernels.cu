@@ -107,6 +107,19 @@ __global__ void k_soa3(long long n, const double* __restrict__ aos, double* __re
   soa[i] = aos[3 * i]; soa[n + i] = aos[3 * i + 1]; soa[2 * n + i] = aos[3 * i + 2];
 }
 
+// Three planes (3 x n) -> xyz-interleaved (n x 3); with vh, the Lagrangian
+// node coordinates of the last cycle, x0 + old_dt * v_half (MahycoModule.cc:
+// 899-901), or x0 before the first cycle.
+__global__ void k_aos3(long long n, const double* __restrict__ soa, const double* __restrict__ vh,
+                       const Scalars* __restrict__ S, double* __restrict__ aos) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool lag = vh != nullptr && S->iteration > 0;
+  const double dtu = lag ? S->old_dt : 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) aos[3 * i + a] = lag ? soa[a * n + i] + vh[a * n + i] * dtu : soa[a * n + i];
+}
+
 // Maximum node coordinate per axis, from -1 as PrepareFaceGroup starts it
 // (MahycoAnnexe.cc:189-199): per-block maxima, then one block over them.
 // The maximum does not depend on the order in which it is taken.

@@ -163,6 +163,7 @@ __global__ void k_init_state(Dims dm, Phys ph, const double* vol, double* rho, c
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
 __global__ void k_to_f32(long long n, const double* src, float* dst);
 __global__ void k_soa3(long long n, const double* aos, double* soa);
+__global__ void k_aos3(long long n, const double* soa, const double* vh, const Scalars* S, double* aos);
 __global__ void k_max3_partial(long long n, const double* x, double* part);
 __global__ void k_face_groups(Dims dm, const double* x0, const double* part, int nparts, double thr, unsigned* grp);
 __global__ void k_bc_mask(long long n, const unsigned* grp, int nbc, const int* surf, uint16_t* mask);

@@ -62,6 +62,20 @@ def test_sedov_jittered_bitwise():
     assert_bitwise(o, g, dto, dtg)
 
 
+def test_node_coordinates_bitwise():
+    """MHY_FIELD_NODE_COORD: the initial coordinates before the first cycle,
+    then the Lagrangian ones of the last cycle (x0 + dt v_half,
+    MahycoModule.cc:899-901), interleaved on the device."""
+    case = gen.sedov(n=12, jitter=0.01, seed=5, cycles=15)
+    o, g = mhy_oracle.Oracle(case), Context(case)
+    assert np.array_equal(o.field("node_coord"), g.field("node_coord"))
+    assert np.array_equal(g.field("node_coord").reshape(-1, 3), case.coords)
+    o.step(15)
+    g.step(15)
+    assert np.array_equal(o.field("node_coord"), g.field("node_coord"))
+    assert np.array_equal(o.field("velocity"), g.field("velocity"))
+
+
 @pytest.mark.parametrize("lim", [1, 2])
 def test_limiters_bitwise(lim):
     case = gen.sedov(n=12, jitter=0.01, seed=5, cycles=40)
