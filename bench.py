@@ -293,7 +293,8 @@ def run_reference_batched(args, threads):
 def run_ours_batched(args):
     """The batched form: 64 independent uneven instances in one set of
     persistent launches per cycle, per-instance dt on the device.  With N GPUs
-    the instance list is split round-robin (strong scaling: the job is fixed)."""
+    the instance list is split by cell count (replicas.partition; strong
+    scaling: the job is fixed)."""
     import numpy as np
     import torch
     import mhy_b200
@@ -309,7 +310,7 @@ def run_ours_batched(args):
     all_cases = gen.batched()
     for c in all_cases:
         c.options.precision = 0 if args.precision == "fp64" else 1
-    mine = [c for i, c in enumerate(all_cases) if i % world == rank]
+    mine = [all_cases[i] for i in replicas.partition([c.ncells for c in all_cases], world, rank)]
     cells = sum(c.ncells for c in mine)
     b = mhy_b200.Batch(mine, device=local)
     stream = torch.cuda.ExternalStream(b.stream(), device=dev)
