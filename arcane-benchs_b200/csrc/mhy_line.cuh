@@ -44,12 +44,17 @@ constexpr int kTileArr = kLineWarps * kTileLd;   // doubles per staged array
 // by thread (x = tid % W, p = tid / W) hit 33 x + p, whose 8-byte bank pairs
 // (x + p) mod 16 take every pair twice per warp, and line reads run along p.
 // Every W keeps 64 registers a thread: 32 / W resident blocks of 32 W threads.
+// A node sweep's cell tile [2][W + 1][cld] is filled with the W + 1 columns
+// fastest (coalesced global loads): element (q, xx, p) at ((q (W + 1) + xx)
+// cld + p); cld = 41 for W = 8 and 33 otherwise put every warp's 32 stores on
+// 16 distinct 8-byte bank pairs twice, the minimum of two wavefronts (a row
+// of 32 put the 9 columns of W = 8 on the same pairs: 9 wavefronts).
 template <int W> struct TileGeom {
   static_assert(W == 8 || W == 16 || W == 32, "lines per block");
   static constexpr int ld = W == 8 ? kTileLd : 33;
   static constexpr int arr = W * ld;                 // doubles per staged array
   static constexpr int minb = 32 / W;                // resident blocks at 64 registers
-  static constexpr int cld = W == 8 ? 32 : 33;       // row length of a node sweep's cell tile
+  static constexpr int cld = W == 8 ? 41 : 33;       // row length of a node sweep's cell tile
 };
 
 // remapVariables "moy" kernel for a single-environment cell and the PerfectGas
