@@ -103,6 +103,36 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
   out[5] = cc;
 }
 
+// The mixed form's end of the remap for one environment: the moy kernel above
+// with its volume and mass fractions, which are 1 for a single environment,
+// folded in (rho = U1 / V, e = U2 / U1, q = U3 / V in FP64), and the
+// PerfectGas EOS evaluated in FP32 (the StiffenedGas EOS, whose p + g pinf
+// cancels, stays in FP64).
+__device__ __forceinline__ void finalize_cell_mixed(const Phys& ph, const Scalars* S, double vol, const double u[4],
+                                                    double out[6]) {
+  const double U1 = u[1], U2 = u[2], U3 = u[3];
+  if (U1 == 0.) atomicOr(&const_cast<Scalars*>(S)->status, MHY_STATUS_ZERO_MASS);
+  const double unsurvol = 1. / vol;
+  const double de = U1 * unsurvol;
+  double e = U1 != 0. ? U2 / U1 : 0.;
+  double r = de;
+  if (r < 0. || e < 0.) { e = 0.; r = 0.; }
+  double pr, cc;
+  if (ph.eos == 0) {
+    const float g = (float)ph.gamma, rf = (float)r, pf = (g - 1.f) * rf * (float)e;
+    pr = pf;
+    cc = sqrtf(g * pf / rf);
+  } else {
+    eos_pc(ph.eos, ph.gamma, ph.pinf, r, e, pr, cc);
+  }
+  out[0] = r;
+  out[1] = e;
+  out[2] = U3 * unsurvol;
+  out[3] = vol * de;
+  out[4] = pr;
+  out[5] = cc;
+}
+
 // Phi = U / sum of the environment volumes = U / U0 for one environment
 // (RemapADIService.cc:962-970, PrepareRemap.cc:394-398); Phi0 = U0/U0 = 1.
 template <typename R>
@@ -409,7 +439,8 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
     for (int v = 0; v < 4; ++v) out[v] = u[v];
     out[4] = dpm;
   } else {
-    finalize_cell(ph, S, in.vol, u, out);
+    if constexpr (sizeof(R) == 4) finalize_cell_mixed(ph, S, in.vol, u, out);
+    else finalize_cell(ph, S, in.vol, u, out);
     out[6] = dpm;
   }
 }
