@@ -106,3 +106,15 @@ def test_pente_borne_refused_for_several_environments_and_batches():
     cases = gen.batched(count=2, seed=3, side_lo=8, side_hi=10, cycles=1)
     cases[1].options.pente_borne = 1
     assert code_of(lambda: Batch(cases)) == ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("opts", [
+    dict(schema_csts=1),
+    dict(eos=(1,), limit_tension=(0.5,)),
+    dict(schema_csts=1, with_newton=0, projection_limiteur_id=1),
+], ids=["csts", "stiffened", "csts_superbee"])
+def test_pente_borne_with_other_options_bitwise(opts):
+    """Pente-borne beside the schema-csts time scheme and the StiffenedGas EOS."""
+    o = gen.Options(pente_borne=1, pente_borne_debar_fix=1, **opts)
+    compare(gen.sod(cycles=120, options=o), 120, 30)
+    compare(gen.sedov(n=14, cycles=40, options=gen.Options(pente_borne=1, pente_borne_debar_fix=2, **opts)), 40, 20)
