@@ -168,6 +168,10 @@ int mhy_step(mhy_ctx* ctx, int ncycles);
  * the device raised the matching status bit. */
 int mhy_synchronize(mhy_ctx* ctx);
 
+/* Copy one field to host memory (pinned memory copies at full bus speed):
+ * ncells or nnodes doubles, or nnodes x 3 interleaved for the velocity and
+ * the node coordinates (interleaved on the device, then one copy).  Waits
+ * for the work recorded so far; MHY_ERR_ARG when bytes is too small. */
 int mhy_get_field(mhy_ctx* ctx, int field, void* dst, size_t bytes);
 /* Per-environment cell values (Arcane's environment views, e.g. the
  * EnvCellVariableRealRef fields of Mahyco.axl read through an IMeshEnvironment):
