@@ -24,6 +24,12 @@ from mhy_b200 import gen  # noqa: E402
 CASES = {
     "sod_small": lambda: gen.sod(nx=24, ny=4, nz=3, jitter=0.01, seed=4, cycles=40),
     "two_material_small": lambda: gen.two_material(16, 8, 8, cycles=30, seed=7),
+    # option paths: pente-borne (debar fix 1, superBee); order 3 with a
+    # generalised limiter, Newton energy update and a stiffened gas
+    "sod_pente_borne_small": lambda: gen.sod(nx=24, ny=4, nz=3, jitter=0.01, seed=4, cycles=40, options=gen.Options(
+        pente_borne=1, pente_borne_debar_fix=1, projection_limiteur_id=1)),
+    "sedov_order3_options_small": lambda: gen.sedov(n=10, jitter=0.01, seed=9, cycles=25, options=gen.Options(
+        ordre_projection=3, projection_limiteur_id=5, with_newton=1, eos=(1,), limit_tension=(1.0e-3,))),
 }
 
 
@@ -51,6 +57,7 @@ def run(name):
 
 
 if __name__ == "__main__":
-    for name in CASES:
+    # python tests/golden/make_golden.py [name ...]: all fixtures, or the named ones
+    for name in (sys.argv[1:] or CASES):
         np.savez_compressed(HERE / f"{name}.npz", **run(name))
         print("wrote", HERE / f"{name}.npz")

@@ -128,7 +128,8 @@ def test_deterministic_rerun():
         assert a.field(f).tobytes() == b.field(f).tobytes()
 
 
-@pytest.mark.parametrize("name", ["sod_small", "two_material_small"])
+@pytest.mark.parametrize("name", ["sod_small", "two_material_small", "sod_pente_borne_small",
+                                  "sedov_order3_options_small"])
 def test_golden_fixtures_on_gpu(name):
     """The device path reproduces the committed golden fixtures bit for bit."""
     import pathlib

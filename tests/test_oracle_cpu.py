@@ -230,7 +230,8 @@ def test_project_cube_root_is_correctly_rounded():
     assert off <= 3
 
 
-@pytest.mark.parametrize("name", ["sod_small", "two_material_small"])
+@pytest.mark.parametrize("name", ["sod_small", "two_material_small", "sod_pente_borne_small",
+                                  "sedov_order3_options_small"])
 def test_golden_fixtures(name):
     """The oracle reproduces the committed fixtures (made by tests/golden/make_golden.py) bit for bit."""
     import make_golden
