@@ -37,6 +37,20 @@ int fail(int code, const std::string& msg) {
 constexpr int kThreads = 256;
 inline unsigned blocks(long long n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
+// Makes a context's (or batch's) device current for the duration of an entry
+// point and gives the caller back its own current device afterwards, so a
+// context may be driven from a thread whose current device is another GPU.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    int cur = 0;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~DeviceScope() { if (prev >= 0) cudaSetDevice(prev); }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
 enum Phase {
   PH_SAVE = 0, PH_VELOCITY, PH_BC, PH_POSITION, PH_GEOMETRY, PH_DENSITY, PH_VISCOSITY, PH_ENERGY,
   PH_REMAP, PH_DELTA_T
@@ -341,6 +355,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
 
 int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
   if (!c || !st || !st->fracvol || !st->density || !st->pressure || !st->velocity) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   const long long C = c->dm.C, N = c->dm.N;
   const int K = c->K;
   if (K == 1) {
@@ -431,6 +446,7 @@ extern "C" {
 int mhy_hydro_start_init(mhy_ctx* c) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
   if (!c->state_set) return fail(MHY_ERR_STATE, "mhy_set_state must come first");
+  DeviceScope on_dev(c->device);
   const Dims& dm = c->dm;
   cudaStream_t s = c->stream;
   const int rc = init_geometry(c);
@@ -562,6 +578,7 @@ int mhy_remap(mhy_ctx* c) {
 }
 int mhy_compute_delta_t(mhy_ctx* c) {
   int rc = check_phase(c, PH_DELTA_T); if (rc) return rc;
+  DeviceScope on_dev(c->device);
   if (c->pend == 7) {                                // a whole cycle recorded: one graph launch
     rc = cycle_graph(c, c->pend_sens);
     if (rc != MHY_OK) return rc;
@@ -577,6 +594,7 @@ int mhy_compute_delta_t(mhy_ctx* c) {
 int mhy_step(mhy_ctx* c, int ncycles) {
   int rc = check_phase(c, PH_SAVE); if (rc) return rc;
   if (ncycles < 0) return fail(MHY_ERR_ARG, "ncycles < 0");
+  DeviceScope on_dev(c->device);
   for (int it = 0; it < ncycles; ++it) {
     const int s = c->sens;
     rc = cycle_graph(c, s);
@@ -589,6 +607,7 @@ int mhy_step(mhy_ctx* c, int ncycles) {
 
 int mhy_synchronize(mhy_ctx* c) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   Scalars h{};
@@ -658,6 +677,7 @@ extern "C" {
 
 void mhy_batch_destroy(mhy_batch* b) {
   if (!b) return;
+  DeviceScope on_dev(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (int s = 0; s < 3; ++s) if (b->graph[s]) cudaGraphExecDestroy(b->graph[s]);
   for (int k = 0; k < BK_COUNT; ++k) if (b->d_work[k]) cudaFree(b->d_work[k]);
@@ -725,6 +745,7 @@ int mhy_batch_set_state(mhy_batch* b, int i, const mhy_state* st) {
 
 int mhy_batch_hydro_start_init(mhy_batch* b) {
   if (!b) return fail(MHY_ERR_ARG, "null batch");
+  DeviceScope on_dev(b->device);
   std::vector<CycleArgs> d;
   for (mhy_ctx* c : b->inst) {
     const int rc = mhy_hydro_start_init(c);
@@ -740,6 +761,7 @@ int mhy_batch_step(mhy_batch* b, int ncycles) {
   if (!b) return fail(MHY_ERR_ARG, "null batch");
   if (!b->initialized) return fail(MHY_ERR_STATE, "mhy_batch_hydro_start_init must come first");
   if (ncycles < 0) return fail(MHY_ERR_ARG, "ncycles < 0");
+  DeviceScope on_dev(b->device);
   for (int it = 0; it < ncycles; ++it) {
     const int s = b->sens;
     if (!b->graph[s]) {
@@ -763,6 +785,7 @@ int mhy_batch_step(mhy_batch* b, int ncycles) {
 
 int mhy_batch_synchronize(mhy_batch* b) {
   if (!b) return fail(MHY_ERR_ARG, "null batch");
+  DeviceScope on_dev(b->device);
   MHY_CUDA(cudaStreamSynchronize(b->stream));
   for (mhy_ctx* c : b->inst) {
     const int rc = mhy_synchronize(c);
@@ -864,11 +887,23 @@ int apply_tuning(mhy_ctx* c, const mhy_tuning& t) {
   return MHY_OK;
 }
 
-// Cache key: the precision, the number of environments and the sorted mesh sizes.
+// Cache key: the precision, the number of environments, the options that
+// change which kernels a cycle launches or what they cost (schema-csts adds
+// kernels and sweeps on the Lagrangian coordinates; Newton, the EOS kinds,
+// the order, the limiter and the length mode change the work per item) and
+// the sorted mesh sizes (with each instance's own options in a batch).
 std::string tune_key(const std::vector<mhy_ctx*>& inst, const char* kind) {
+  auto opts = [](const mhy_ctx* c) {
+    std::string s = "c" + std::to_string(c->ph.csts) + "n" + std::to_string(c->ph.with_newton) + "o" +
+                    std::to_string(c->ph.ordre_projection) + "l" + std::to_string(c->ph.limiteur_id) + "L" +
+                    std::to_string(c->ph.lc_mode) + "e";
+    for (int k = 0; k < c->K; ++k) s += std::to_string(c->env.eos[k]);
+    return s;
+  };
   std::vector<std::string> sz;
   for (const mhy_ctx* c : inst)
-    sz.push_back(std::to_string(c->dm.nx) + "x" + std::to_string(c->dm.ny) + "x" + std::to_string(c->dm.nz));
+    sz.push_back(std::to_string(c->dm.nx) + "x" + std::to_string(c->dm.ny) + "x" + std::to_string(c->dm.nz) + "/" +
+                 opts(c));
   std::sort(sz.begin(), sz.end());
   std::string key = std::string(kind) + ":p" + std::to_string(inst[0]->ph.precision) + ":k" +
                     std::to_string(inst[0]->K);
@@ -998,6 +1033,7 @@ int mhy_get_tuning(mhy_ctx* c, mhy_tuning* out) {
 
 int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
   if (!c || !t) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   mhy_tuning u = *t;
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) { u.order[k] = 0; u.occupancy_pct[k] = 100; }
@@ -1015,6 +1051,7 @@ int mhy_set_tuning(mhy_ctx* c, const mhy_tuning* t) {
 
 int mhy_autotune(mhy_ctx* c, int cycles, mhy_tuning* out) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "autotune runs between cycles");
@@ -1095,6 +1132,7 @@ int mhy_batch_set_tuning(mhy_batch* b, const mhy_tuning* t) {
   u.order[BK_DT_MIN] = u.order[BK_LCELLS];
   u.order[BK_DT_FINISH] = 0;
   u.occupancy_pct[BK_DT_FINISH] = 100;
+  DeviceScope on_dev(b->device);
   int rc = check_tuning(u);
   if (rc == MHY_OK) rc = apply_tuning(b, u);
   if (rc == MHY_OK) b->tuning = u;
@@ -1105,6 +1143,7 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
   if (!b) return fail(MHY_ERR_ARG, "null batch");
   if (!b->initialized) return fail(MHY_ERR_STATE, "mhy_batch_hydro_start_init must come first");
   if (cycles < 1 || cycles > 20) return fail(MHY_ERR_ARG, "cycles must be 1..20");
+  DeviceScope on_dev(b->device);
   const std::string key = tune_key(b->inst, "batch");
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1119,7 +1158,6 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
       return MHY_OK;
     }
   }
-  MHY_CUDA(cudaSetDevice(b->device));
   MHY_CUDA(cudaStreamSynchronize(b->stream));
   Snapshot snap;
   int rc = snap.save(b->inst, b->stream);
@@ -1188,6 +1226,7 @@ void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr
 
 int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   const long long C = c->dm.C, N = c->dm.N;
   const double* src = nullptr;
@@ -1236,7 +1275,31 @@ struct CkptHeader {
   double dt, old_dt, time;
   int64_t iteration;
   uint32_t status, pad;
+  uint64_t options_hash;   // options_hash() of the context that saved the dump
 };
+constexpr int32_t kCkptVersion = 2;
+
+// FNV-1a hash of every option that changes the computed state (all of
+// mhy_options but deltat-init, whose effect the dump's dt replaces): a dump
+// only loads into a context that will continue with the same physics.
+uint64_t options_hash(const mhy_options& o) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  auto add = [&](const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 0x100000001b3ull; }
+  };
+  auto d = [&](double x) { add(&x, sizeof(x)); };
+  auto i = [&](int32_t x) { add(&x, sizeof(x)); };
+  d(o.cfl); d(o.threshold); d(o.deltat_min); d(o.deltat_max); d(o.final_time);
+  i(o.longueur_caracteristique); i(o.pseudo_centree); i(o.ordre_projection); i(o.projection_limiteur_id);
+  i(o.nb_bc);
+  for (int b = 0; b < o.nb_bc && b < MHY_MAX_BC; ++b) { i(o.bc[b].surface); i(o.bc[b].type); d(o.bc[b].value); }
+  i(o.nb_env);
+  for (int k = 0; k < o.nb_env && k < MHY_MAX_ENV; ++k) { d(o.adiabatic_cst[k]); i(o.eos[k]); d(o.limit_tension[k]); }
+  i(o.precision); i(o.with_newton); i(o.schema_csts); i(o.projection_pente_borne); i(o.pente_borne_debar_fix);
+  i(o.pente_borne_mixte); i(o.limiteur_pure_id);
+  return h;
+}
 struct CkptField {
   char name[40];
   int32_t dtype;        // 0 double, 1 float, 2 uint32
@@ -1288,6 +1351,7 @@ extern "C" {
 
 int mhy_checkpoint_size(mhy_ctx* c, size_t* bytes) {
   if (!c || !bytes) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   std::vector<int64_t> off;
   *bytes = ckpt_layout(ckpt_fields(c), off);
@@ -1296,6 +1360,7 @@ int mhy_checkpoint_size(mhy_ctx* c, size_t* bytes) {
 
 int mhy_checkpoint_save(mhy_ctx* c, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   if (!c->initialized) return fail(MHY_ERR_STATE, "mhy_hydro_start_init must come first");
   if (c->phase != PH_SAVE) return fail(MHY_ERR_ORDER, "a restart dump is taken between cycles");
@@ -1310,8 +1375,9 @@ int mhy_checkpoint_save(mhy_ctx* c, void* dst, size_t bytes) {
   std::memset(base, 0, sizeof(CkptHeader) + f.size() * sizeof(CkptField));
   CkptHeader hd{};
   std::memcpy(hd.magic, kCkptMagic, 8);
-  hd.version = 1; hd.nx = c->dm.nx; hd.ny = c->dm.ny; hd.nz = c->dm.nz; hd.nenv = c->K;
+  hd.version = kCkptVersion; hd.nx = c->dm.nx; hd.ny = c->dm.ny; hd.nz = c->dm.nz; hd.nenv = c->K;
   hd.precision = c->ph.precision; hd.nfields = (int32_t)f.size(); hd.sens = c->sens;
+  hd.options_hash = options_hash(c->opt);
   hd.dt = h.dt; hd.old_dt = h.old_dt; hd.time = h.time; hd.iteration = h.iteration; hd.status = h.status;
   std::memcpy(base, &hd, sizeof(hd));
   for (size_t i = 0; i < f.size(); ++i) {
@@ -1326,15 +1392,19 @@ int mhy_checkpoint_save(mhy_ctx* c, void* dst, size_t bytes) {
 
 int mhy_checkpoint_load(mhy_ctx* c, const void* src, size_t bytes) {
   if (!c || !src) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   if (bytes < sizeof(CkptHeader)) return fail(MHY_ERR_ARG, "not a restart dump");
   const char* base = static_cast<const char*>(src);
   CkptHeader hd;
   std::memcpy(&hd, base, sizeof(hd));
-  if (std::memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != 1) return fail(MHY_ERR_ARG, "not a restart dump");
+  if (std::memcmp(hd.magic, kCkptMagic, 8) != 0 || hd.version != kCkptVersion)
+    return fail(MHY_ERR_ARG, "not a restart dump");
   if (hd.nx != c->dm.nx || hd.ny != c->dm.ny || hd.nz != c->dm.nz || hd.nenv != c->K ||
       hd.precision != c->ph.precision)
     return fail(MHY_ERR_ARG, "restart dump of another mesh, environment count or precision");
+  if (hd.options_hash != options_hash(c->opt))
+    return fail(MHY_ERR_ARG, "restart dump taken with other options (EOS, gamma, limiter, order, schemes, BCs, ...)");
   if (hd.sens < 0 || hd.sens > 2) return fail(MHY_ERR_ARG, "corrupt restart dump");
   const std::vector<CkField> f = ckpt_fields(c);
   if (hd.nfields != (int32_t)f.size() || bytes < sizeof(CkptHeader) + f.size() * sizeof(CkptField))
@@ -1365,6 +1435,7 @@ int mhy_checkpoint_load(mhy_ctx* c, const void* src, size_t bytes) {
 
 int mhy_get_env_mask(mhy_ctx* c, uint32_t* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   const long long C = c->dm.C;
   if (bytes < (size_t)C * sizeof(uint32_t)) return fail(MHY_ERR_ARG, "destination too small");
@@ -1379,6 +1450,7 @@ int mhy_get_env_mask(mhy_ctx* c, uint32_t* dst, size_t bytes) {
 
 int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
   if (!c || !dst) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   if (env < 0 || env >= c->K) return fail(MHY_ERR_ARG, "environment index out of range");
   const long long C = c->dm.C;
@@ -1419,6 +1491,7 @@ int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
 
 int mhy_get_dt(mhy_ctx* c, double* dt, double* dt_old) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   Scalars h{};
   MHY_CUDA(cudaStreamSynchronize(c->stream));
@@ -1430,6 +1503,7 @@ int mhy_get_dt(mhy_ctx* c, double* dt, double* dt_old) {
 
 int mhy_get_time(mhy_ctx* c, double* time, int64_t* iteration) {
   if (!c) return fail(MHY_ERR_ARG, "null context");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   Scalars h{};
   MHY_CUDA(cudaStreamSynchronize(c->stream));
@@ -1441,6 +1515,7 @@ int mhy_get_time(mhy_ctx* c, double* time, int64_t* iteration) {
 
 int mhy_get_status(mhy_ctx* c, uint32_t* flags) {
   if (!c || !flags) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   Scalars h{};
   MHY_CUDA(cudaStreamSynchronize(c->stream));
@@ -1459,6 +1534,7 @@ int mhy_get_sizes(mhy_ctx* c, int64_t* ncells, int64_t* nnodes, int64_t* nfaces)
 
 int mhy_get_totals(mhy_ctx* c, double* out) {
   if (!c || !out) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
   MHY_FLUSH(c);
   if (!c->initialized) return fail(MHY_ERR_ORDER, "mhy_hydro_start_init has not run");
   double* part = c->setup;                       // 6 x kTotalsBlocks partials, then the 3 totals
@@ -1473,6 +1549,7 @@ int mhy_get_totals(mhy_ctx* c, double* out) {
 
 void* mhy_get_stream(mhy_ctx* c) {
   if (!c) return nullptr;
+  DeviceScope on_dev(c->device);
   flush(c);                                        // work the caller enqueues follows the entry points
   return (void*)c->stream;
 }
@@ -1481,6 +1558,7 @@ int mhy_kernels_per_cycle(mhy_ctx* c) { return c ? c->kernels_per_cycle : 0; }
 
 void mhy_destroy(mhy_ctx* c) {
   if (!c) return;
+  DeviceScope on_dev(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int s = 0; s < 3; ++s) if (c->graph[s]) cudaGraphExecDestroy(c->graph[s]);
   for (void* p_ : c->allocs) cudaFree(p_);

@@ -25,8 +25,18 @@
 //    streams, or different host threads on one device) race on the scratch and
 //    must be serialised by the caller;
 //  * the first call on a device looks up the scratch's device address with
-//    cudaGetSymbolAddress (once per device, with that device current); make
-//    that first call before any stream capture.
+//    cudaGetSymbolAddress (with that device current); make that first call
+//    before any stream capture.  The address is kept per device together with
+//    the identity of the device's current CUDA context, and looked up again
+//    when that context has changed (after cudaDeviceReset, for instance), so
+//    the first call after such a reset must also come before any capture;
+//  * a cell whose L / (c + max |v|) is NaN or negative (an inverted cell, a NaN
+//    field) is not skipped: the call then writes out[0] = NaN and out[1] = 0,
+//    a time step below any positive deltat-min, so a caller that checks the
+//    new dt against deltat-min stops as the reference does (MahycoModule.cc:
+//    2152-2159).  The context's own reduction raises MHY_STATUS_NAN_DT for the
+//    same cells.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,12 +51,49 @@ constexpr int kNoAllocThreads = 256;
 constexpr int kNoAllocCellsPerThread = 64;
 constexpr long long kNoAllocMaxCells = (long long)kNoAllocBlocks * kNoAllocThreads * kNoAllocCellsPerThread;
 constexpr unsigned long long kDblMaxBits = 0x7fefffffffffffffull;
+// A block's partial minimum is the bit pattern of a non-negative double (bit
+// 63 clear); bit 63 set records that the block met an invalid cell.
+constexpr unsigned long long kInvalidBit = 0x8000000000000000ull;
 
 static __device__ __align__(256) unsigned long long g_dt_scratch[kNoAllocBlocks];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
-unsigned long long* g_scratch_addr[kMaxDevices] = {nullptr};
+struct ScratchAddr {
+  unsigned long long* addr = nullptr;
+  unsigned long long ctx_id = 0;   // CUDA context the address belongs to (0: unknown)
+};
+ScratchAddr g_scratch[kMaxDevices];
+
+// Identity of the calling thread's current CUDA context (cuCtxGetId through
+// the runtime's driver entry points, so the library does not link libcuda);
+// 0 when there is none or the driver cannot say.
+unsigned long long current_ctx_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {             // under g_mutex
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f1);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f2);
+    cudaGetLastError();
+    looked_up = true;
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 __device__ __forceinline__ unsigned long long block_min(unsigned long long best, unsigned long long* wmin) {
   for (int o = 16; o > 0; o >>= 1) {
@@ -68,11 +115,16 @@ __device__ __forceinline__ unsigned long long block_min(unsigned long long best,
 
 // First pass: dx_sound = L / (c + max over the cell's nodes of |v|), as in
 // computeHydroDeltaT (mahyco/src/MahycoModule.cc:2047-2060); one partial
-// minimum per block (bit patterns of non-negative doubles order like integers).
+// minimum per block (bit patterns of non-negative doubles order like
+// integers), with kInvalidBit set when the block met a NaN or negative value.
 __global__ void k_dt_partial_noalloc(Dims dm, const double* __restrict__ L, const double* __restrict__ cs,
                                      const double* __restrict__ v, unsigned long long* __restrict__ scratch) {
   __shared__ unsigned long long wmin[32];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
   unsigned long long best = kDblMaxBits;
+  bool invalid = false;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < dm.C;
        c += (long long)gridDim.x * blockDim.x) {
     int i, j, k; dm.cijk(c, i, j, k);
@@ -85,21 +137,40 @@ __global__ void k_dt_partial_noalloc(Dims dm, const double* __restrict__ L, cons
     if (dx_sound >= 0.) {
       unsigned long long b = (unsigned long long)__double_as_longlong(dx_sound);
       best = b < best ? b : best;
+    } else {
+      invalid = true;                               // NaN or negative
     }
   }
-  best = block_min(best, wmin);
-  if (threadIdx.x == 0) scratch[blockIdx.x] = best;
+  if (invalid) bad = 1;                             // benign race: every writer stores 1
+  best = block_min(best, wmin);                     // its barrier also orders the writes to `bad`
+  if (threadIdx.x == 0) scratch[blockIdx.x] = best | (bad ? kInvalidBit : 0ull);
 }
 
 // Second pass: minimum of the partial minima, then the new dt of
-// computeDeltaT (MahycoModule.cc:2144-2150): min(cfl * min, 1.05 * dt_old, deltat_max).
+// computeDeltaT (MahycoModule.cc:2144-2150): min(cfl * min, 1.05 * dt_old, deltat_max);
+// NaN and 0 when any block met an invalid cell.
 __global__ void k_dt_final_noalloc(const unsigned long long* __restrict__ scratch, int nparts, double cfl,
                                    double dt_old, double deltat_max, double* __restrict__ out) {
   __shared__ unsigned long long wmin[32];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
   unsigned long long best = kDblMaxBits;
-  for (int t = threadIdx.x; t < nparts; t += blockDim.x) best = scratch[t] < best ? scratch[t] : best;
+  bool invalid = false;
+  for (int t = threadIdx.x; t < nparts; t += blockDim.x) {
+    const unsigned long long s = scratch[t];
+    if (s & kInvalidBit) invalid = true;
+    const unsigned long long b = s & ~kInvalidBit;
+    best = b < best ? b : best;
+  }
+  if (invalid) bad = 1;
   best = block_min(best, wmin);
   if (threadIdx.x == 0) {
+    if (bad) {
+      out[0] = __longlong_as_double(0x7ff8000000000000ll);   // quiet NaN: no valid minimum
+      out[1] = 0.;
+      return;
+    }
     const double minimum_aux = __longlong_as_double((long long)best);
     double new_dt = cfl * minimum_aux;
     new_dt = amin(new_dt, 1.05 * dt_old);
@@ -127,12 +198,20 @@ extern "C" int mhy_compute_hydro_dt_noalloc(int32_t nx, int32_t ny, int32_t nz, 
   unsigned long long* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_addr[dev]) {
+    ScratchAddr& sa = g_scratch[dev];
+    const unsigned long long id = current_ctx_id();
+    if (!sa.addr || id == 0 || id != sa.ctx_id) {
+      // set-up of this device (or of its new context): the scratch's device address
       void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_dt_scratch) != cudaSuccess || !p) return MHY_ERR_CUDA;
-      g_scratch_addr[dev] = static_cast<unsigned long long*>(p);
+      if (cudaGetSymbolAddress(&p, g_dt_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        sa = ScratchAddr{};
+        return MHY_ERR_CUDA;
+      }
+      sa.addr = static_cast<unsigned long long*>(p);
+      sa.ctx_id = current_ctx_id();                 // the lookup has made the context current
     }
-    scratch = g_scratch_addr[dev];
+    scratch = sa.addr;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   long long want = (dm.C + kNoAllocThreads - 1) / kNoAllocThreads;

@@ -15,6 +15,16 @@ cycles driven entry point by entry point with dt read back to the host every
 cycle (the Arcane time loop reads it), then the final density, energy and
 velocity read back.  N > 1 GPUs run independent replicas (weak scaling; the
 path has no data exchange between independent meshes).
+
+Beside the timed number, the default line carries `parity` (a fresh context
+stepped cycle by cycle against the CPU oracle with the C library's pow, over
+the same cycles as the timed run when they are at most --parity-cycles:
+relative L-inf of density, energy and velocity, dt-sequence difference, and
+whether the timed run's fields equal that context's bit for bit),
+`cpu_baseline` (the same oracle run's wall time on all host cores, plus one
+cycle on one thread, with the CPU model) and `forms` (the mixed-precision
+Sedov mesh and the 64-instance batched sweep in FP64 and mixed, same cycles,
+with their ratios to this line and the mixed forms' errors).
 """
 from __future__ import annotations
 
@@ -69,14 +79,52 @@ def parse():
                     help="set lines per block of the cell y, cell z, node y, node z sweeps (e.g. 16,16,8,8) instead "
                          "of autotuning (profiling runs: timings under a profiler mislead the autotuner)")
     ap.add_argument("--cpu-sample-cycles", type=int, default=5)
+    ap.add_argument("--parity-cycles", type=int, default=60,
+                    help="cycles of the parity check against the libm-pow oracle (capped at warmup + steps; "
+                         "0 = no parity check)")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the mixed-precision and batched figures of the default line")
     return ap.parse_args()
 
 
-# DRAM bytes (read + write) of one whole cycle, summed over its kernels, from
-# one ncu capture of the 128^3 Sedov cycle (profiles/dram_traffic_sedov128_cycle.md).
-# DRAM bytes of one cycle from ncu (dram__bytes_read.sum + dram__bytes_write.sum over the 10 kernels of the
-# fourth cycle, cell y/z sweeps at 16 lines per block as the autotuner picks them)
-TRAFFIC_PER_CYCLE = {("sedov", 128, "fp64"): 3465343744.0, ("sedov", 128, "mixed"): 2912002560.0}
+# DRAM bytes (read + write) of one whole cycle, summed over its kernels
+# (dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of the
+# 128^3 Sedov cycle), with the digest of the kernel sources they were measured
+# on: after any change to those sources the figure is reported as stale (null).
+TRAFFIC_PER_CYCLE = {("sedov", 128, "fp64"): (3465343744.0, None), ("sedov", 128, "mixed"): (2912002560.0, None)}
+KERNEL_SOURCES = ("mhy_kernels.cuh", "mhy_device.cuh", "mhy_pow_third.h", "mhy_line.cuh", "mhy_lagrange.cuh",
+                  "mhy_kernels.cu", "mhy_cycle.cu", "mhy_multi.cu")
+
+
+def kernel_sources_digest():
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update((ROOT / "arcane-benchs_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def cycle_traffic(key):
+    """(traffic bytes or None, note)."""
+    entry = TRAFFIC_PER_CYCLE.get(key)
+    if entry is None:
+        return None, "no ncu capture of this workload"
+    traffic, digest = entry
+    if digest != kernel_sources_digest():
+        return None, "stale: the kernel sources changed since the ncu capture"
+    return traffic, f"ncu capture on kernel sources {digest}"
+
+
+def cpu_info():
+    model = None
+    try:
+        for line in pathlib.Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
 
 
 def measured_peak():
@@ -136,8 +184,23 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def single_thread(o, case):
+    """One more cycle of an oracle on one thread (the oracle's thread count is
+    process-wide, so it is restored afterwards)."""
+    import mhy_oracle
+    threads = os.cpu_count() or 1
+    mhy_oracle.lib().orc_set_threads(1)
+    t0 = time.perf_counter()
+    o.step(1)
+    el = time.perf_counter() - t0
+    mhy_oracle.lib().orc_set_threads(threads)
+    return {"value": case.ncells / el, "unit": METRIC, "cores": 1, "cycles": 1,
+            "sample": "one cycle after the all-core sample, 1 OpenMP thread"}
+
+
 def cpu_baseline(case, cycles, wname):
-    """The oracle (CPU restatement of the reference algorithm) on this host, all cores."""
+    """The oracle (CPU restatement of the reference algorithm) on this host:
+    all cores, then one thread."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import mhy_oracle
     threads = os.cpu_count() or 1
@@ -146,10 +209,70 @@ def cpu_baseline(case, cycles, wname):
     t0 = time.perf_counter()
     o.step(cycles)
     dt = time.perf_counter() - t0
+    one = single_thread(o, case)
     o.close()
     return {"value": case.ncells * cycles / dt, "unit": METRIC, "cores": threads, "kind": "port",
             "sample": f"{wname} (same mesh and state), cycles 2..{cycles + 1} after init, "
-                      f"OpenMP {threads} threads, oracle built -O3 -ffp-contract=off"}
+                      f"OpenMP {threads} threads, oracle built -O3 -ffp-contract=off",
+            "single_thread": one, **cpu_info()}
+
+
+def oracle_leg(case, wname, cycles, device, timed=None, want_cpu=True):
+    """Parity and CPU baseline from one run of the oracle with the C library's
+    pow (the reference's V^(1/3.), MahycoModule.cc:1259) on all host cores.
+
+    Parity: a fresh FP64 context on the GPU, stepped one cycle at a time with
+    its dt read back each cycle, against the oracle over `cycles` cycles from
+    the same initial state: relative L-inf of density, specific internal energy
+    and node velocity, and the largest relative difference of the dt sequence.
+    When `timed` (the timed run's final fields, after the same number of
+    cycles) is given, the timed run is also compared with that context bit for
+    bit.  CPU baseline: the oracle's own wall time for cycles 2..cycles, then
+    one cycle on one thread."""
+    import numpy as np
+    import mhy_b200
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import mhy_oracle
+    threads = os.cpu_count() or 1
+    g = mhy_b200.Context(case, device=device)
+    dtg = [g.dt()[0]]
+    for _ in range(cycles):
+        g.step(1)
+        dtg.append(g.dt()[0])
+    g.synchronize()
+    gf = {f: g.field(f) for f in ("density", "internal_energy", "velocity")}
+    g.close()
+    o = mhy_oracle.Oracle(case, pow_mode="libm", threads=threads)
+    dto = [o.scalars()["dt"]]
+    o.step(1)                                          # first cycle (page faults, thread start) not timed
+    dto.append(o.scalars()["dt"])
+    t0 = time.perf_counter()
+    for _ in range(cycles - 1):
+        o.step(1)
+        dto.append(o.scalars()["dt"])
+    el = time.perf_counter() - t0
+
+    def rel_linf(a, b):
+        s = float(np.max(np.abs(b)))
+        return float(np.max(np.abs(a - b))) / (s if s > 0 else 1.0)
+
+    dto, dtg = np.array(dto), np.array(dtg)
+    errs = {f"{f}_rel_linf": rel_linf(gf[f], o.field(f)) for f in gf}
+    dt_err = float(np.max(np.abs(dtg - dto) / dto))
+    parity = {"cycles": cycles, **errs, "dt_sequence_max_rel": dt_err,
+              "bar": {"fields_rel_linf": 1e-10, "dt_rel": 1e-12},
+              "within_bar": bool(max(errs.values()) <= 1e-10 and dt_err <= 1e-12),
+              "reference": f"CPU oracle with libm pow, OpenMP {threads} threads; GPU context stepped cycle by cycle"}
+    if timed is not None:
+        parity["timed_run_bitwise_equal"] = bool(all(np.array_equal(timed[f], gf[f]) for f in gf))
+    cpu = None
+    if want_cpu and cycles >= 2:
+        cpu = {"value": case.ncells * (cycles - 1) / el, "unit": METRIC, "cores": threads, "kind": "port",
+               "sample": f"{wname} (same mesh and state), cycles 2..{cycles} of the parity run, "
+                         f"OpenMP {threads} threads, oracle built -O3 -ffp-contract=off",
+               "single_thread": single_thread(o, case), **cpu_info()}
+    o.close()
+    return parity, cpu
 
 
 def run_reference(args):
@@ -180,7 +303,8 @@ def run_reference(args):
             "steps": k, "warmup": max(1, args.warmup), "ms_per_step": el / k * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": wname, "cells": case.ncells, "nodes": case.nnodes},
-            "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample,
+                             **cpu_info()},
             "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -443,6 +567,7 @@ def run_ours(args):
     accuracy = None
     if args.precision == "mixed":
         accuracy = mixed_accuracy([case], [ctx.field("density")], args.warmup + args.steps, local, totals=tot1)
+    timed_fields = {f: ctx.field(f) for f in ("density", "internal_energy", "velocity")}
     ctx.close()
 
     # end to end through the per-entry-point C ABI, host buffers in pinned memory
@@ -477,24 +602,37 @@ def run_ours(args):
         e2e = {"value": e2e_value, "unit": METRIC,
                "h2d_bytes_per_step": round(h2d, 1), "d2h_bytes_per_step": round(d2h, 1),
                "path": "mhy_create+mhy_set_state+mhy_hydro_start_init, per-cycle entry points + mhy_get_dt, "
-                       "mhy_get_field x3; wall clock, max over ranks"}
+                       "mhy_get_field x3; wall clock, max over ranks",
+               "tuning": "the autotuner's in-process cache for this mesh size (filled by the device-timed run "
+                         "above); a first-time caller pays the trials once"
+                         + (f", {tuning['cycle_ms_default'] * 3 * (tuning.get('trials') or 0):.1f} ms of "
+                            "device time here" if tuning and 'cycle_ms_default' in tuning else "")}
 
     mixed_fraction = float(((case.fracvol > 0).sum(0) > 1).mean()) if case.nenv > 1 else 0.0
     b_alg = bytes_model.bytes_per_cell_cycle(case.ncells, case.nnodes, case.nenv, mixed_fraction)
     peak, peak_kind = measured_peak()
     per_gpu_cells_per_s = case.ncells * args.steps / (ms / 1e3)
     achieved = b_alg * per_gpu_cells_per_s / 1e9
+    traffic, traffic_note = cycle_traffic((args.workload, args.n, args.precision))
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
-                "traffic": TRAFFIC_PER_CYCLE.get((args.workload, args.n, args.precision)),
+                "traffic": traffic, "traffic_note": traffic_note,
                 "algorithmic_bytes_per_launch": round(b_alg * case.ncells, 1),
                 "kernel": f"one cycle graph ({kpc} kernels, launched as one unit), algorithmic bytes "
                           f"{b_alg:.1f} B/cell-cycle x {case.ncells} cells; traffic = DRAM bytes of one cycle (ncu)",
                 "peak_kind": peak_kind}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu, parity = None, None
+    total_cycles = args.warmup + args.steps
+    pcycles = min(args.parity_cycles, total_cycles)
+    if rank == 0 and world == 1 and args.precision == "fp64" and pcycles > 0:
+        parity, cpu = oracle_leg(case, wname, pcycles, local, timed_fields if pcycles == total_cycles else None,
+                                 want_cpu=not args.no_cpu_baseline)
+    if cpu is None and rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, args.cpu_sample_cycles, wname)
+    forms = None
+    if (rank == 0 and world == 1 and not args.no_forms and args.workload == "sedov" and args.precision == "fp64"):
+        forms = measure_forms(args, local, value, timed_fields["density"], tot1[0])
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -508,12 +646,102 @@ def run_ours(args):
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": kpc * args.steps, "clocks": clk.summary(), "device_status": status,
                 "conservation": cons}
+        if parity:
+            line["parity"] = parity
+        if forms:
+            line["forms"] = forms
         if accuracy:
             line["accuracy"] = accuracy
             line["dtype"] = "f32 remap evaluation / f64 state"
         print(json.dumps(line), flush=True)
     replicas.finish()
     return 0
+
+
+def timed_cycles(obj, args, device):
+    """Warm-up, then args.steps cycles timed with CUDA events on the object's
+    stream (a Context or a Batch); returns ms."""
+    import torch
+    stream = torch.cuda.ExternalStream(obj.stream(), device=torch.device("cuda", device))
+    obj.step(args.warmup)
+    obj.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    obj.step(args.steps)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    obj.synchronize()
+    return start.elapsed_time(stop)
+
+
+def measure_forms(args, device, plain_value, plain_density, plain_totals):
+    """The two production forms beside the plain FP64 Sedov line, over the
+    same warm-up and timed cycles: the mixed-precision Sedov mesh, and the
+    64-instance batched sweep (32^3..96^3, one persistent launch per kernel
+    per cycle) in FP64 and mixed.  Each gives its cell-cycles/s and its ratio
+    to the plain line; the mixed forms add the density L1 error against the
+    FP64 path on the same inputs (that path equals the oracle bit for bit) and
+    the relative differences of total mass and total energy."""
+    import math
+    import numpy as np
+    import mhy_b200
+    from mhy_b200 import gen
+    cycles = args.warmup + args.steps
+
+    def l1(a_list, r_list):
+        num = math.fsum(float(np.abs(a - r).sum()) for a, r in zip(a_list, r_list))
+        den = math.fsum(float(np.abs(r).sum()) for r in r_list)
+        return num / den
+
+    def rel(a, r):
+        return (a - r) / r
+
+    out = {"cycles_timed": args.steps, "cycles_total": cycles, "plain_fp64_value": plain_value}
+    # mixed-precision Sedov
+    case = gen.sedov(n=args.n)
+    case.options.precision = 1
+    ctx = mhy_b200.Context(case, device=device)
+    apply_tuning(ctx, args)
+    ms = timed_cycles(ctx, args, device)
+    val = case.ncells * args.steps / (ms / 1e3)
+    tm = ctx.totals()
+    out["mixed_sedov"] = {"workload": f"sedov-{args.n}^3-jitter1%-mixed", "value": val, "ms_per_step": ms / args.steps,
+                          "vs_plain_fp64": val / plain_value,
+                          "density_l1_rel_vs_fp64": l1([ctx.field("density")], [plain_density]),
+                          "mass_rel_vs_fp64": rel(tm["mass"], plain_totals["mass"]),
+                          "total_energy_rel_vs_fp64": rel(tm["total_energy"], plain_totals["total_energy"]),
+                          "device_status": ctx.status()}
+    ctx.close()
+    # batched sweep, FP64 then mixed
+    res = {}
+    for prec in (0, 1):
+        cases = gen.batched()
+        for c in cases:
+            c.options.precision = prec
+        b = mhy_b200.Batch(cases, device=device)
+        apply_tuning(b, args)
+        ms = timed_cycles(b, args, device)
+        cells = sum(c.ncells for c in cases)
+        res[prec] = {"value": cells * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "density": [b.field(i, "density") for i in range(len(cases))],
+                     "totals": [b.totals(i) for i in range(len(cases))],
+                     "status": max(b.status(i) for i in range(len(cases)))}
+        b.close()
+    for prec, name in ((0, "batched_fp64"), (1, "batched_mixed")):
+        r = res[prec]
+        out[name] = {"workload": f"batched-64-sod-sedov-32..96^3-{'fp64' if prec == 0 else 'mixed'}",
+                     "value": r["value"], "ms_per_step": r["ms_per_step"], "vs_plain_fp64": r["value"] / plain_value,
+                     "device_status": r["status"]}
+    f64, mx = res[0], res[1]
+    out["batched_mixed"]["vs_batched_fp64"] = mx["value"] / f64["value"]
+    out["batched_mixed"]["density_l1_rel_vs_fp64"] = l1(mx["density"], f64["density"])
+    for key, q in (("mass_rel_vs_fp64", "mass"), ("total_energy_rel_vs_fp64", "total_energy")):
+        a = math.fsum(t[q] for t in mx["totals"])
+        r = math.fsum(t[q] for t in f64["totals"])
+        out["batched_mixed"][key] = rel(a, r)
+    out["target"] = "mixed batched >= 1.6x the plain FP64 path at density L1 <= 1e-5"
+    return out
 
 
 def main():

@@ -286,12 +286,18 @@ void mhy_batch_destroy(mhy_batch* b);
  * characteristic length L and sound speed cs per cell, node velocity v as
  * three planes (x[N], y[N], z[N]).  Output (device pointer, 2 doubles):
  * out[0] = min over cells of L/(cs + max |v| over the cell's nodes),
- * out[1] = min(cfl*out[0], 1.05*dt_old, deltat_max).  Work is queued on
- * `stream` (a cudaStream_t, NULL for the default stream); nothing is allocated.
- * Meshes above 134217728 cells are rejected with MHY_ERR_ARG.  All calls on a
- * device share the scratch: calls that overlap on the GPU race and must be
- * serialised by the caller.  The first call on a device resolves the scratch
- * address; make it before any stream capture. */
+ * out[1] = min(cfl*out[0], 1.05*dt_old, deltat_max).  When any cell's
+ * L/(cs + max |v|) is NaN or negative (an inverted cell, a NaN field), the
+ * call writes out[0] = NaN and out[1] = 0: a dt below any positive deltat_min,
+ * so a caller that checks the new dt against deltat_min stops the run as the
+ * reference does (the context's reduction raises MHY_STATUS_NAN_DT instead).
+ * Work is queued on `stream` (a cudaStream_t, NULL for the default stream);
+ * nothing is allocated.  Meshes above 134217728 cells are rejected with
+ * MHY_ERR_ARG.  All calls on a device share the scratch: calls that overlap
+ * on the GPU race and must be serialised by the caller.  The first call on a
+ * device, and the first call after the device's context was reset
+ * (cudaDeviceReset), resolve the scratch address; make them before any
+ * stream capture. */
 int mhy_compute_hydro_dt_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* L, const double* cs,
                                  const double* v, double cfl, double dt_old, double deltat_max,
                                  double* out, void* stream);

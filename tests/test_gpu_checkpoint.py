@@ -49,3 +49,30 @@ def test_dump_of_another_mesh_is_rejected():
         Context.from_checkpoint(gen.sod(nx=22, ny=4, nz=4, cycles=5), blob)
     with pytest.raises(MhyError):
         Context.from_checkpoint(gen.sod(nx=20, ny=4, nz=4, cycles=5), b"garbage" * 10)
+
+
+@pytest.mark.parametrize("change", ["limiter", "gamma", "newton", "eos", "cfl"])
+def test_dump_with_other_physics_options_is_rejected(change):
+    """The dump records a hash of the options that change the computed state;
+    a context with the same mesh but other physics refuses it."""
+    case = gen.sod(nx=20, ny=4, nz=4, cycles=5)
+    a = Context(case)
+    a.step(2)
+    blob = a.save_checkpoint()
+    other = gen.sod(nx=20, ny=4, nz=4, cycles=5)
+    if change == "limiter":
+        other.options.projection_limiteur_id = 1
+    elif change == "gamma":
+        other.gamma = np.array([1.5])
+    elif change == "newton":
+        other.options.with_newton = 1
+    elif change == "eos":
+        other.options.eos = (1,)
+    else:
+        other.options.cfl = 0.25
+    with pytest.raises(MhyError):
+        Context.from_checkpoint(other, blob)
+    same = gen.sod(nx=20, ny=4, nz=4, cycles=5)
+    same.options.deltat_init = 2e-5                     # replaced by the dump's dt: accepted
+    b = Context.from_checkpoint(same, blob)
+    assert b.dt() == a.dt()
