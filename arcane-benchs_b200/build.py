@@ -16,7 +16,7 @@ HERE = pathlib.Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB_DIR = HERE / "lib"
 LIB = LIB_DIR / "libmhy_b200.so"
-SOURCES = ["mhy_kernels.cu", "mhy_cycle.cu", "mhy_multi.cu", "mhy_capi.cu", "mhy_noalloc.cu"]
+SOURCES = ["mhy_kernels.cu", "mhy_cycle.cu", "mhy_multi.cu", "mhy_capi.cu", "mhy_csr.cu", "mhy_noalloc.cu"]
 HEADERS = ["mhy_kernels.cuh", "mhy_device.cuh", "mhy_pow_third.h", "mhy_line.cuh", "mhy_lagrange.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -78,6 +78,11 @@ struct mhy_ctx {
   double *L = nullptr, *Ve = nullptr, *dpf = nullptr, *cqs = nullptr, *ofn = nullptr, *xc = nullptr;
   float* cqs32 = nullptr;
   double *vnb = nullptr, *vf = nullptr, *xl = nullptr, *pf = nullptr;   // schema-csts
+  double *mfc = nullptr, *ecn = nullptr;   // conservation-energie-totale: cell mass fraction, node term
+  // explicit connectivity (mhy_create_csr): the structured id of each of the
+  // caller's cells and nodes, on the host and in HBM; empty for mhy_create
+  std::vector<int32_t> cell_index, node_index;
+  int32_t *d_cell_index = nullptr, *d_node_index = nullptr;
   double *U[2] = {nullptr, nullptr};
   // environments (K > 1)
   int K = 1;
@@ -136,6 +141,7 @@ struct mhy_ctx {
     a.K = K; a.env = env; a.Vlag = Vlag;
     for (int k = 0; k < BK_COUNT; ++k) a.lines[k] = lines[k];
     a.vnb = vnb; a.vf = vf; a.xl = xl; a.pf = pf;
+    a.st.mf = mfc; a.ecn = ecn;
     return a;
   }
 };
@@ -220,6 +226,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   for (int b = 0; b < opt->nb_bc; ++b)
     if (opt->bc[b].surface < 0 || opt->bc[b].surface > 5 || opt->bc[b].type < 0 || opt->bc[b].type > 2)
       return fail(MHY_ERR_ARG, "bad boundary condition");
+  if (opt->conservation_energie_totale != 0 && opt->conservation_energie_totale != 1)
+    return fail(MHY_ERR_ARG, "conservation_energie_totale must be 0 or 1");
+  if (opt->conservation_energie_totale && (opt->nb_env != 1 || opt->precision != 0))
+    return fail(MHY_ERR_UNSUPPORTED, "conservation-energie-totale: one environment in FP64 on the device");
 
   mhy_ctx* c = new mhy_ctx();
   for (int k = 0; k < MHY_TUNE_SLOTS; ++k) {
@@ -264,6 +274,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   ph.pb_debar = opt->pente_borne_debar_fix;
   ph.pb_lim_y0 = opt->pente_borne_mixte ? opt->limiteur_pure_id : opt->projection_limiteur_id;
   ph.pb_first = 0;
+  ph.cons_ec = opt->conservation_energie_totale;
   c->bct.nb = opt->nb_bc;
   for (int b = 0; b < opt->nb_bc; ++b) { c->bct.type[b] = opt->bc[b].type; c->bct.value[b] = opt->bc[b].value; }
 
@@ -286,6 +297,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     if (rc == MHY_OK) rc = c->alloc(&c->pf, (size_t)C);
   }
   A_(&c->U[0], NV * C); A_(&c->U[1], NV * C);
+  if (opt->conservation_energie_totale) { A_(&c->mfc, C); A_(&c->ecn, N); }
   if (K > 1) {
     EnvState& ev = c->env;
     A_(&ev.f, K * C); A_(&ev.x, K * C); A_(&ev.rho, K * C); A_(&ev.e, K * C); A_(&ev.p, K * C);
@@ -348,7 +360,46 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv
-                               : kKernelsPerCycle + (opt->schema_csts ? 2 : 0) + (opt->ordre_projection == 3 ? 3 : 0);
+                               : kKernelsPerCycle + (opt->schema_csts ? 2 : 0) + (opt->ordre_projection == 3 ? 3 : 0) +
+                                     (opt->conservation_energie_totale ? 1 : 0);
+  *out = c;
+  return MHY_OK;
+}
+
+int mhy_create_csr(const mhy_csr_mesh* mesh, const mhy_options* opt, int device, mhy_ctx** out) {
+  if (!mesh || !opt || !out || !mesh->cell_node_offsets || !mesh->cell_nodes || !mesh->node_coords)
+    return fail(MHY_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (mesh->ncells < 8 || mesh->nnodes < 27) return fail(MHY_ERR_ARG, "need at least 2 cells per direction");
+  std::vector<int32_t> ci((size_t)mesh->ncells), ni((size_t)mesh->nnodes);
+  int32_t dims[3] = {0, 0, 0};
+  int rc = mhy_csr_structure(mesh->ncells, mesh->nnodes, mesh->cell_node_offsets, mesh->cell_nodes, dims, ci.data(),
+                             ni.data());
+  if (rc != MHY_OK)
+    return fail(rc, rc == MHY_ERR_ARG ? "bad connectivity arrays (offsets, node ids or sizes)"
+                                      : "connectivity is not one logically Cartesian block of hexahedra with the "
+                                        "SN_trigo local node order (CartConnectivityCellNode.h:83-94)");
+  std::vector<double> xs((size_t)3 * mesh->nnodes);
+  for (int64_t u = 0; u < mesh->nnodes; ++u)
+    for (int a = 0; a < 3; ++a) xs[3 * (size_t)ni[u] + a] = mesh->node_coords[3 * u + a];
+  const mhy_mesh_desc md{dims[0], dims[1], dims[2], xs.data()};
+  mhy_ctx* c = nullptr;
+  rc = mhy_create(&md, opt, device, &c);
+  if (rc != MHY_OK) return rc;
+  DeviceScope on_dev(c->device);
+  const size_t bc = ci.size() * sizeof(int32_t), bn = ni.size() * sizeof(int32_t);
+  void* d = nullptr;
+  cudaError_t err = cudaMalloc(&d, bc + bn + 256);
+  if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
+  c->allocs.push_back(d);
+  c->alloc_bytes.push_back(bc + bn + 256);
+  c->d_cell_index = static_cast<int32_t*>(d);
+  c->d_node_index = reinterpret_cast<int32_t*>(static_cast<char*>(d) + ((bc + 255) & ~size_t(255)));
+  err = cudaMemcpy(c->d_cell_index, ci.data(), bc, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaMemcpy(c->d_node_index, ni.data(), bn, cudaMemcpyHostToDevice);
+  if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
+  c->cell_index = std::move(ci);
+  c->node_index = std::move(ni);
   *out = c;
   return MHY_OK;
 }
@@ -358,6 +409,21 @@ int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
   DeviceScope on_dev(c->device);
   const long long C = c->dm.C, N = c->dm.N;
   const int K = c->K;
+  std::vector<double> pfv, pde, ppr, pve;
+  mhy_state perm{};
+  if (!c->cell_index.empty()) {
+    // the caller's numbering -> the structured one
+    pfv.resize((size_t)K * C); pde.resize((size_t)K * C); ppr.resize((size_t)K * C); pve.resize((size_t)3 * N);
+    for (int k = 0; k < K; ++k)
+      for (long long u = 0; u < C; ++u) {
+        const size_t d = (size_t)k * C + c->cell_index[u], o = (size_t)k * C + u;
+        pfv[d] = st->fracvol[o]; pde[d] = st->density[o]; ppr[d] = st->pressure[o];
+      }
+    for (long long u = 0; u < N; ++u)
+      for (int a = 0; a < 3; ++a) pve[3 * (size_t)c->node_index[u] + a] = st->velocity[3 * u + a];
+    perm = mhy_state{pfv.data(), pde.data(), ppr.data(), pve.data()};
+    st = &perm;
+  }
   if (K == 1) {
     for (long long i = 0; i < C; ++i)
       if (!(st->fracvol[i] > 0.)) return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
@@ -476,6 +542,7 @@ int launch_remap_(mhy_ctx* c, int sens, KernelMarks* m = nullptr) {
   if (c->K == 1) {
     if (c->ph.csts) launch_csts_forward(c->args(), c->stream);   // PrepareRemap.cc:456, then the face velocities
     launch_remap(c->args(), sens, c->stream, m);
+    if (c->ph.cons_ec) launch_cons_ec(c->args(), c->stream);   // after the last node sweep, before dt
   } else {
     launch_remap_env(c->args(), sens, c->stream, m);
   }
@@ -698,6 +765,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters are not batched");
     if (opts[i].projection_pente_borne || opts[i].pente_borne_mixte)
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: pente-borne is not batched");
+    if (opts[i].conservation_energie_totale)
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: conservation-energie-totale is not batched");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();
@@ -1256,6 +1325,13 @@ int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {
     MHY_CUDA(cudaGetLastError());
     src = c->ud[0];
   }
+  if (c->d_cell_index) {
+    // into the caller's numbering, in the other dual remap buffer (5N doubles)
+    const int32_t* idx = n == N ? c->d_node_index : c->d_cell_index;
+    k_gather_index<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, vec ? 3 : 1, idx, src, c->ud[1]);
+    MHY_CUDA(cudaGetLastError());
+    src = c->ud[1];
+  }
   MHY_CUDA(cudaMemcpyAsync(dst, src, need, cudaMemcpyDeviceToHost, c->stream));
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   return MHY_OK;
@@ -1297,7 +1373,7 @@ uint64_t options_hash(const mhy_options& o) {
   i(o.nb_env);
   for (int k = 0; k < o.nb_env && k < MHY_MAX_ENV; ++k) { d(o.adiabatic_cst[k]); i(o.eos[k]); d(o.limit_tension[k]); }
   i(o.precision); i(o.with_newton); i(o.schema_csts); i(o.projection_pente_borne); i(o.pente_borne_debar_fix);
-  i(o.pente_borne_mixte); i(o.limiteur_pure_id);
+  i(o.pente_borne_mixte); i(o.limiteur_pure_id); i(o.conservation_energie_totale);
   return h;
 }
 struct CkptField {
@@ -1445,6 +1521,10 @@ int mhy_get_env_mask(mhy_ctx* c, uint32_t* dst, size_t bytes) {
     return MHY_OK;
   }
   MHY_CUDA(cudaMemcpy(dst, c->env.mask, C * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (!c->cell_index.empty()) {
+    const std::vector<uint32_t> t(dst, dst + C);
+    for (long long u = 0; u < C; ++u) dst[u] = t[c->cell_index[u]];
+  }
   return MHY_OK;
 }
 
@@ -1469,12 +1549,18 @@ int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
   }
   MHY_CUDA(cudaStreamSynchronize(c->stream));
   double* o = static_cast<double*>(dst);
+  auto to_caller = [&]() {                         // the structured numbering -> the caller's
+    if (c->cell_index.empty()) return;
+    const std::vector<double> t(o, o + C);
+    for (long long u = 0; u < C; ++u) o[u] = t[c->cell_index[u]];
+  };
   if (c->K == 1) {
     if (field == MHY_ENV_FRACVOL || field == MHY_ENV_MASS_FRACTION) {
       for (long long i = 0; i < C; ++i) o[i] = 1.;
       return MHY_OK;
     }
     MHY_CUDA(cudaMemcpy(o, glob, C * sizeof(double), cudaMemcpyDeviceToHost));
+    to_caller();
     return MHY_OK;
   }
   std::vector<uint32_t> mask(C);
@@ -1486,6 +1572,7 @@ int mhy_get_env_field(mhy_ctx* c, int field, int env, void* dst, size_t bytes) {
     const uint32_t m = mask[i];
     o[i] = !(m >> env & 1) ? 0. : (__builtin_popcount(m) == 1 ? g[i] : pt[i]);
   }
+  to_caller();
   return MHY_OK;
 }
 

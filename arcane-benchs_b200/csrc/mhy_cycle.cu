@@ -191,6 +191,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   } else {
     st.rho[c] = out[0]; st.e[c] = out[1]; st.q[c] = out[2]; st.mass[c] = out[3]; st.p[c] = out[4]; st.cs[c] = out[5];
     dpf[c] = out[6];
+    if (st.mf) st.mf[c] = out[7];
   }
 }
 
@@ -307,6 +308,7 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
   } else {
     st.rho[sc] = r[0]; st.e[sc] = r[kTileArr]; st.q[sc] = r[2 * kTileArr]; st.mass[sc] = r[3 * kTileArr];
     st.p[sc] = r[4 * kTileArr]; st.cs[sc] = r[5 * kTileArr]; dpf[sc] = r[6 * kTileArr];
+    if (st.mf) st.mf[sc] = r[7 * kTileArr];
   }
 }
 
@@ -562,6 +564,37 @@ static void remap_impl(const CycleArgs& a0, int sens, cudaStream_t s, KernelMark
     mark(m, BK_NODES_X + d, s);
     prev |= 1 << d;
   }
+}
+
+// conservation-energie-totale for one environment (RemapADIFinal.cc:751-773,
+// then the EOS that follows the remap, PrepareRemap.cc:553-558): the
+// 0.25 (ec_proj - ec_reconst) terms of the cell's 8 nodes (written by the
+// last node sweep) summed in cell-node order from 0, floored at 0 as
+// std::max(0., delta) does, times the cell's mass fraction, added to e; p and
+// c again from the new e.
+__global__ void __launch_bounds__(128) k_cons_ec(Dims dm, Phys ph, const double* __restrict__ ecn,
+    const double* __restrict__ mf, const double* __restrict__ rho, double* __restrict__ e, double* __restrict__ p,
+    double* __restrict__ cs, int linear) {
+  int i, j, k;
+  if (!block_item(dm.nx, dm.ny, dm.nz, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, i, j, k)) return;
+  const long long c = dm.cid(i, j, k);
+  double delta_ec = 0.;
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    delta_ec += ecn[dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2])];
+  delta_ec = smax(0., delta_ec);
+  const double en = e[c] + mf[c] * delta_ec;
+  double pr, cc;
+  eos_pc(ph.eos, ph.gamma, ph.pinf, rho[c], en, pr, cc);
+  e[c] = en;
+  p[c] = pr;
+  cs[c] = cc;
+}
+
+void launch_cons_ec(const CycleArgs& a, cudaStream_t s) {
+  int linear;
+  const dim3 nbc = cell_grid(a.dm, linear);
+  k_cons_ec<<<nbc, 128, 0, s>>>(a.dm, a.ph, a.ecn, a.st.mf, a.st.rho, a.st.e, a.st.p, a.st.cs, linear);
 }
 
 void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {

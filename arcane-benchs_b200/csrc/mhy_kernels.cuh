@@ -35,6 +35,7 @@ struct Phys {
   // (0: computeFluxPP, 1: computeFluxPPPure), its debar fix, the limiter of its
   // reconstruction (computeY0), and whether the sweep is the first of the cycle
   int pb, pb_pure, pb_debar, pb_lim_y0, pb_first;
+  int cons_ec;          // conservation-energie-totale (RemapADI.axl:151; one environment, FP64)
 };
 
 struct BCTable {
@@ -61,6 +62,8 @@ struct FaceData {
 struct CellState {
   double *rho, *e, *q, *p, *cs, *mass;
   const double* Ve;
+  double* mf;           // conservation-energie-totale: the cell's mass fraction out of the last
+                        // cell sweep (0 where the remap zeroed the cell); null otherwise
 };
 
 // Environments (materials) of a mesh with K > 1 of them.  A cell that
@@ -99,6 +102,8 @@ struct CycleArgs {
   int lines[8];         // lines per block of each sweep (indexed like BatchKernel; y/z sweeps of K = 1: 8, 16, 32)
   double *vnb, *vf, *xl;  // schema-csts: backward v_n, forward v, Lagrangian node coordinates (3N each)
   double* pf;             // schema-csts: p + q of the forward step (C)
+  double* ecn;            // conservation-energie-totale: each node's kinetic-energy term out of the
+                          // last node sweep (N); null otherwise
 };
 
 void launch_lagrange_nodes(const CycleArgs& a, cudaStream_t s);
@@ -107,6 +112,7 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s);
 struct KernelMarks;
 void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 void launch_delta_t(const CycleArgs& a, cudaStream_t s);
+void launch_cons_ec(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycle = 10;
 // meshes with 2..kMaxEnvDevice environments (mhy_multi.cu)
 constexpr int kMaxEnvDevice = 4;
@@ -163,6 +169,7 @@ __global__ void k_init_state(Dims dm, Phys ph, const double* vol, double* rho, c
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
 __global__ void k_to_f32(long long n, const double* src, float* dst);
 __global__ void k_soa3(long long n, const double* aos, double* soa);
+__global__ void k_gather_index(long long n, int comps, const int32_t* idx, const double* src, double* out);
 __global__ void k_aos3(long long n, const double* soa, const double* vh, const Scalars* S, double* aos);
 __global__ void k_max3_partial(long long n, const double* x, double* part);
 __global__ void k_face_groups(Dims dm, const double* x0, const double* part, int nparts, double thr, unsigned* grp);

@@ -59,9 +59,10 @@ template <int W> struct TileGeom {
 
 // remapVariables "moy" kernel for a single-environment cell and the PerfectGas
 // EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
-// PrepareRemap.cc:553-559).  out = rho, e, q, mass, p, c.
+// PrepareRemap.cc:553-559).  out = rho, e, q, mass, p, c, -, mass fraction
+// (0 when the cell was zeroed; conservation-energie-totale scales by it).
 __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, double vol, const double u[4],
-                                              double out[6]) {
+                                              double out[8]) {
   const double thr = ph.threshold;
   const double U0 = u[0], U1 = u[1], U2 = u[2], U3 = u[3];
   const double volt = 0. + U0, masset = 0. + U1;
@@ -92,7 +93,8 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
   const double pv = U3 * unsurvol;
   const double pseudo = 0. + fvol * pv;
   double r = de;
-  if (r < 0. || energie < 0.) { energie = 0.; r = 0.; }
+  out[7] = mf;
+  if (r < 0. || energie < 0.) { energie = 0.; r = 0.; out[7] = 0.; }   // RemapADIFinal.cc:611-626
   double pr, cc;
   eos_pc(ph.eos, ph.gamma, ph.pinf, r, energie, pr, cc);
   out[0] = r;
@@ -109,14 +111,15 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
 // PerfectGas EOS evaluated in FP32 (the StiffenedGas EOS, whose p + g pinf
 // cancels, stays in FP64).
 __device__ __forceinline__ void finalize_cell_mixed(const Phys& ph, const Scalars* S, double vol, const double u[4],
-                                                    double out[6]) {
+                                                    double out[8]) {
   const double U1 = u[1], U2 = u[2], U3 = u[3];
   if (U1 == 0.) atomicOr(&const_cast<Scalars*>(S)->status, MHY_STATUS_ZERO_MASS);
   const double unsurvol = 1. / vol;
   const double de = U1 * unsurvol;
   double e = U1 != 0. ? U2 / U1 : 0.;
   double r = de;
-  if (r < 0. || e < 0.) { e = 0.; r = 0.; }
+  out[7] = 1.;
+  if (r < 0. || e < 0.) { e = 0.; r = 0.; out[7] = 0.; }
   double pr, cc;
   if (ph.eos == 0) {
     const float g = (float)ph.gamma, rf = (float)r, pf = (g - 1.f) * rf * (float)e;
@@ -310,7 +313,7 @@ struct CellIn {
   double h;                    // G limiters: cell width along d (RemapADIService.cc:225-258)
   double pb[3];                // pente-borne: rho and e (first sweep only) and the q of the remap's start
 };
-constexpr int kCellOutLast = 7;   // rho, e, q, mass, p, c, dual mass flux
+constexpr int kCellOutLast = 8;   // rho, e, q, mass, p, c, dual mass flux, mass fraction
 constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
 
 // One line step of computeGradPhiFace, computeGradPhiCell, the upwind face
@@ -509,7 +512,8 @@ struct NodeIn {
   double x2[2];    // G limiters, halo lanes 1 and 30: the coordinates along d two nodes back / ahead,
                    // which lie outside the warp's segment
 };
-constexpr int kNodeOut = 5;   // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| on the last sweep
+constexpr int kNodeOut = 5;       // U_dual[0..4], or v.x, v.y, v.z, node mass, |v| on the last sweep
+constexpr int kNodeOutLast = 6;   // the last sweep adds the node's conservation-energie-totale term
 
 // One line step of computeDualUremap and computeDualGradPhi_LimC
 // (DualPhaseRemap.cc:22-523, 700-778), then remapVariables for the node
@@ -595,13 +599,20 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
   } else {
     const double m = ud[3];
     D3 u;
+    double rm = 0.;
     if (m != 0.) {
-      const double rm = 1.0 / m;
+      rm = 1.0 / m;
       u = d3(qdiv(ud[0], m, rm), qdiv(ud[1], m, rm), qdiv(ud[2], m, rm));
     } else {
       u = d3(in.vh[0], in.vh[1], in.vh[2]);
     }
     out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = .125 * in.msum; out[4] = norm2(u);
+    // conservation-energie-totale (RemapADIFinal.cc:757-764): this node's
+    // share 0.25 (ec_proj - ec_reconst) of the kinetic energy the remap lost,
+    // ec_proj = U_dual[4] / U_dual[3], ec_reconst = 0.5 |v|^2; nothing for a
+    // node of zero mass
+    if (ph.cons_ec)
+      out[5] = m != 0. ? 0.25 * (qdiv(ud[4], m, rm) - 0.5 * (u.x * u.x + u.y * u.y + u.z * u.z)) : 0.;
   }
 }
 
@@ -628,7 +639,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
-    int bx_, int by_, int bz_) {
+    int bx_, int by_, int bz_, double* __restrict__ ecn = nullptr) {
   const int lane = threadIdx.x & 31;
   const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
   if (j > dm.ny) return;                               // whole warp leaves together
@@ -694,7 +705,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
       in.msum = sm;
     }
   }
-  double out[kNodeOut];
+  double out[LAST ? kNodeOutLast : kNodeOut];
   node_line<0, FIRST, LAST, R, GL>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
                                    m + 2 <= nx);
   if (!upd) return;
@@ -704,6 +715,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
     for (int c = 0; c < 5; ++c) udout[c * N + n] = out[c];
   } else {
     vout[n] = out[0]; vout[N + n] = out[1]; vout[2 * N + n] = out[2]; nm_out[n] = out[3]; vnorm[n] = out[4];
+    if (ecn) ecn[n] = out[5];
   }
 }
 
@@ -712,8 +724,8 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_cyc_sweep_n
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm, double* __restrict__ ecn) {
+  k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z, ecn);
 }
 
 // Node sweep along y (D = 1) or z (D = 2), staged through shared memory.
@@ -737,7 +749,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
     double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
-    int bx_, int by_, int bz_) {
+    int bx_, int by_, int bz_, double* __restrict__ ecn = nullptr) {
   using TS = NodeTileSize<D, FIRST, LAST, K, W>;
   constexpr int NA = TS::NA, CT = TS::CT;
   constexpr int CLd = TileGeom<W>::cld;               // row length of a cell tile
@@ -842,14 +854,14 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   R G[3] = {0, 0, 0};
   const int n = valid ? node_id(i, m) : 0;
   if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
-  double out[kNodeOut];
+  double out[LAST ? kNodeOutLast : kNodeOut];
   node_line<D, FIRST, LAST, R, GL>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
                                    m + 2 <= nn - 1);
   if (upd) {
     if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
     // each lane overwrites only the tile column it read itself
 #pragma unroll
-    for (int c = 0; c < kNodeOut; ++c) row[c * kTileArr] = out[c];
+    for (int c = 0; c < (LAST ? kNodeOutLast : kNodeOut); ++c) row[c * kTileArr] = out[c];
   }
   __syncthreads();
   if (!(s_valid && sp >= 2 && sp < 2 + kLineUpd)) return;
@@ -860,6 +872,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   } else {
     vout[sn] = r[0]; vout[N + sn] = r[kTileArr]; vout[2 * N + sn] = r[2 * kTileArr];
     nm_out[sn] = r[3 * kTileArr]; vnorm[sn] = r[4 * kTileArr];
+    if (ecn) ecn[sn] = r[5 * kTileArr];
   }
 }
 
@@ -868,8 +881,8 @@ __global__ void __launch_bounds__(32 * W, TileGeom<W>::minb) k_cyc_sweep_nodes_t
     Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
     const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
     const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm) {
-  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z);
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm, double* __restrict__ ecn) {
+  k_cyc_sweep_nodes_t_body<D, FIRST, LAST, K, R, W, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, udout, dpf, Gd, mass, vout, nm_out, vnorm, blockIdx.x, blockIdx.y, blockIdx.z, ecn);
 }
 
 // ------------------------------------------------------------------------
@@ -887,7 +900,7 @@ static void sweep_nodes_launch_w(const CycleArgs& a, int prev, const double* udi
   auto kern = k_cyc_sweep_nodes_t<D, FIRST, LAST, K, R, W, GL>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout, a.dpf, a.Gd, a.st.mass, a.v,
-                               a.nm, a.vnorm);
+                               a.nm, a.vnorm, a.ecn);
 }
 
 template <int D, bool FIRST, bool LAST, int K, typename R>
@@ -901,10 +914,10 @@ static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin,
     const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
     if (gl)
       k_cyc_sweep_nodes_x<FIRST, LAST, K, R, true><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin,
-                                                                udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+                                                                udout, a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, a.ecn);
     else
       k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout,
-                                                       a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm);
+                                                       a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, a.ecn);
   } else {
     if constexpr (K == 1 && sizeof(R) == 8) {
       if (gl) { sweep_nodes_launch_w<D, FIRST, LAST, K, R, kLineWarps, true>(a, prev, udin, udout, s); return; }

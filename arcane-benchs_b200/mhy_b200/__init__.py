@@ -38,7 +38,8 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_batch_get_status", "mhy_batch_size", "mhy_batch_kernels_per_cycle", "mhy_batch_get_stream",
             "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load",
             "mhy_get_totals", "mhy_batch_get_totals", "mhy_autotune", "mhy_set_tuning", "mhy_get_tuning",
-            "mhy_batch_autotune", "mhy_batch_set_tuning", "mhy_batch_get_tuning"]
+            "mhy_batch_autotune", "mhy_batch_set_tuning", "mhy_batch_get_tuning", "mhy_create_csr",
+            "mhy_csr_structure"]
 MHY_TUNE_SLOTS = 10
 TUNE_SLOTS = ("lagrange_nodes", "lagrange_cells", "cells_x", "cells_y", "cells_z", "nodes_x", "nodes_y", "nodes_z",
               "dt_min", "dt_finish")
@@ -90,11 +91,17 @@ class COptions(ctypes.Structure):
                 ("with_newton", ctypes.c_int32), ("schema_csts", ctypes.c_int32),
                 ("projection_pente_borne", ctypes.c_int32), ("pente_borne_debar_fix", ctypes.c_int32),
                 ("pente_borne_mixte", ctypes.c_int32), ("limiteur_pure_id", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 1)]
+                ("conservation_energie_totale", ctypes.c_int32)]
 
 
 class CMesh(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("node_coords", ctypes.POINTER(ctypes.c_double))]
+
+
+class CCsrMesh(ctypes.Structure):
+    _fields_ = [("ncells", ctypes.c_int64), ("nnodes", ctypes.c_int64),
+                ("cell_node_offsets", ctypes.POINTER(ctypes.c_int64)), ("cell_nodes", ctypes.POINTER(ctypes.c_int64)),
                 ("node_coords", ctypes.POINTER(ctypes.c_double))]
 
 
@@ -167,6 +174,11 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.mhy_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
     L.mhy_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    L.mhy_csr_structure.argtypes = [ctypes.c_int64, ctypes.c_int64, i64p, i64p, i32p, i32p, i32p]
+    L.mhy_csr_structure.restype = ctypes.c_int
+    L.mhy_create_csr.argtypes = [ctypes.POINTER(CCsrMesh), ctypes.POINTER(COptions), ctypes.c_int, ctypes.POINTER(vp)]
+    L.mhy_create_csr.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -179,6 +191,23 @@ def _check(rc):
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def csr_structure(cell_nodes: np.ndarray, nnodes: int):
+    """mhy_csr_structure: (dims, cell_index, node_index) of a logically
+    Cartesian hexahedral block given as cell -> node connectivity
+    (ncells x 8, SN_trigo local order, any numbering).  Host only."""
+    cn = np.ascontiguousarray(cell_nodes, dtype=np.int64).reshape(-1)
+    ncells = cn.size // 8
+    off = np.arange(0, 8 * ncells + 1, 8, dtype=np.int64)
+    dims = np.zeros(3, dtype=np.int32)
+    ci = np.zeros(ncells, dtype=np.int32)
+    ni = np.zeros(int(nnodes), dtype=np.int32)
+    i32 = ctypes.POINTER(ctypes.c_int32)
+    i64 = ctypes.POINTER(ctypes.c_int64)
+    _check(load().mhy_csr_structure(ncells, int(nnodes), off.ctypes.data_as(i64), cn.ctypes.data_as(i64),
+                                    dims.ctypes.data_as(i32), ci.ctypes.data_as(i32), ni.ctypes.data_as(i32)))
+    return tuple(int(d) for d in dims), ci, ni
 
 
 def make_options(opts, gammas) -> COptions:
@@ -204,6 +233,7 @@ def make_options(opts, gammas) -> COptions:
     o.pente_borne_debar_fix = int(getattr(opts, "pente_borne_debar_fix", 0))
     o.pente_borne_mixte = int(getattr(opts, "pente_borne_mixte", 0))
     o.limiteur_pure_id = int(getattr(opts, "limiteur_pure_id", 0))
+    o.conservation_energie_totale = int(getattr(opts, "conservation_energie_totale", 0))
     for k, kind in enumerate(getattr(opts, "eos", ()) or ()):
         o.eos[k] = int(kind)
     for k, v in enumerate(getattr(opts, "limit_tension", ()) or ()):
@@ -310,6 +340,31 @@ class Context:
         buf = ctypes.create_string_buffer(n.value)
         _check(L.mhy_checkpoint_save(self.h, buf, n.value))
         return buf.raw
+
+    @classmethod
+    def from_csr(cls, case, cell_nodes, node_coords, fracvol, density, pressure, velocity, device: int = -1):
+        """mhy_create_csr: a context on explicit connectivity in the caller's
+        numbering (cell_nodes: ncells x 8 node ids, SN_trigo order), with the
+        initial state in the same numbering; case gives the options and gases.
+        Fields come back in the caller's numbering."""
+        self = cls.__new__(cls)
+        L = load()
+        self.case = case
+        cn = np.ascontiguousarray(cell_nodes, dtype=np.int64).reshape(-1)
+        off = np.arange(0, cn.size + 1, 8, dtype=np.int64)
+        self._coords = np.ascontiguousarray(node_coords, dtype=np.float64)
+        i64 = ctypes.POINTER(ctypes.c_int64)
+        mesh = CCsrMesh(cn.size // 8, self._coords.shape[0], off.ctypes.data_as(i64), cn.ctypes.data_as(i64),
+                        _dp(self._coords))
+        opt = make_options(case.options, case.gamma)
+        h = ctypes.c_void_p()
+        _check(L.mhy_create_csr(ctypes.byref(mesh), ctypes.byref(opt), device, ctypes.byref(h)))
+        self.h = h
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fracvol, density, pressure, velocity)]
+        st = CState(*[_dp(a) for a in arrs])
+        _check(L.mhy_set_state(self.h, ctypes.byref(st)))
+        _check(L.mhy_hydro_start_init(self.h))
+        return self
 
     @classmethod
     def from_checkpoint(cls, case, blob: bytes, device: int = -1):

@@ -74,6 +74,7 @@ class Options:
     pente_borne_debar_fix: int = 0          # projection-pente-borne-debar-fix: 0, 1 or 2 (RemapADI.axl:171)
     pente_borne_mixte: int = 0              # projection-pente-borne-mixte (RemapADI.axl:155)
     limiteur_pure_id: int = 0               # projection-limiteur-pure-id (RemapADI.axl:163)
+    conservation_energie_totale: int = 0    # conservation-energie-totale (RemapADI.axl:151)
 
 
 @dataclasses.dataclass

@@ -97,7 +97,12 @@ typedef struct mhy_options {
                                         (computeFluxPPPure) and limiter apply; one environment, precision 0 */
   int32_t limiteur_pure_id;          /* 0..7: projection-limiteur-pure-id (RemapADI.axl:163), the reconstruction's
                                         limiter in pure neighbourhoods, and the gradient's when it is 1 */
-  int32_t reserved[1];
+  int32_t conservation_energie_totale; /* 0; 1: conservation-energie-totale (RemapADI.axl:151;
+                                        RemapADIFinal.cc:751-773): after the remap each cell's specific
+                                        internal energy gains max(0, sum over its 8 nodes of
+                                        0.25 (U_dual[4]/U_dual[3] - 0.5 |v|^2)) times its mass fraction,
+                                        with U_dual[4] = 0.5 m |v| as the reference builds it; one
+                                        environment, precision 0, not batched */
 } mhy_options;
 
 /* Structured hexahedral mesh: (nx+1)(ny+1)(nz+1) nodes, node (i,j,k) at
@@ -106,6 +111,30 @@ typedef struct mhy_mesh_desc {
   int32_t nx, ny, nz;
   const double* node_coords;
 } mhy_mesh_desc;
+
+/* Explicit connectivity, in the caller's own numbering of cells and nodes:
+ * cell c has the 8 nodes cell_nodes[cell_node_offsets[c] .. +8) in the
+ * SN_trigo local order of Arcane's Cartesian cells
+ * (cartesian/CartConnectivityCellNode.h:83-94), offsets every 8 from 0;
+ * node coordinates xyz interleaved.  This is the cell -> node table the
+ * reference reads from Arcane (accenv/AccEnvDefaultService.cc:240-268 builds
+ * its node -> cell counterpart from it). */
+typedef struct mhy_csr_mesh {
+  int64_t ncells, nnodes;
+  const int64_t* cell_node_offsets;   /* ncells + 1 */
+  const int64_t* cell_nodes;          /* 8 * ncells node ids */
+  const double* node_coords;          /* nnodes x 3 */
+} mhy_csr_mesh;
+
+/* Recognises a logically Cartesian block of hexahedra in explicit
+ * connectivity (any numbering, every cell in the SN_trigo local order):
+ * dims = cells along x, y, z; cell_index[c] / node_index[n] = the structured
+ * id (i + nx (j + ny k), nodes with nx+1, ny+1) of the caller's cell c / node
+ * n.  Host only, no GPU needed.  MHY_ERR_UNSUPPORTED when the connectivity is
+ * not one full box of cells with consistently ordered nodes, MHY_ERR_ARG on
+ * bad arrays. */
+int mhy_csr_structure(int64_t ncells, int64_t nnodes, const int64_t* cell_node_offsets, const int64_t* cell_nodes,
+                      int32_t dims[3], int32_t* cell_index, int32_t* node_index);
 
 /* Initial state, the role of the test-case service initVar + the EOS initEOS
  * (casTest/IInitialisations.h:32-50, eos/IEquationOfState.h): per environment
@@ -135,6 +164,16 @@ void mhy_options_default(mhy_options* opt);
  * the mesh/connectivity part of AccEnvDefaultService::initMesh,
  * accenv/AccEnvDefaultService.cc:274-302). device < 0: current device. */
 int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mhy_ctx** out);
+
+/* The same from explicit connectivity (the mesh part of
+ * AccEnvDefaultService::initMesh, accenv/AccEnvDefaultService.cc:240-302,
+ * from Arcane's item lists): the block is recognised with mhy_csr_structure
+ * and the two numbering maps are kept in device memory.  Every cell and node
+ * array the context exchanges with the caller (mhy_set_state, mhy_get_field,
+ * mhy_get_env_field, mhy_get_env_mask) is then in the caller's numbering; the
+ * kernels run on the structured layout.  Results equal those of mhy_create on
+ * the same block bit for bit. */
+int mhy_create_csr(const mhy_csr_mesh* mesh, const mhy_options* opt, int device, mhy_ctx** out);
 
 /* Initial state (casModel()->initVar, MahycoModule.cc:104). */
 int mhy_set_state(mhy_ctx* ctx, const mhy_state* st);

@@ -96,6 +96,7 @@ struct Oracle {
   // RemapADI.axl:155-173: projection-pente-borne, -debar-fix (0, 1, 2),
   // projection-pente-borne-mixte, projection-limiteur-pure-id
   int pente_borne = 0, pb_debar_fix = 0, pb_mixte = 0, limiteur_pure_id = 0;
+  int conservation_energie_totale = 0;   // RemapADI.axl:151
   std::vector<double> gamma;
   std::vector<int> eos;             // per environment: 0 PerfectGas, 1 StiffenedGas
   std::vector<double> pinf;         // StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
@@ -1504,6 +1505,33 @@ struct Oracle {
       if (nbEnv(c) == 1) continue;
       for (int k = 0; k < K; ++k) if (env_mask[c] >> k & 1) cell_volume.p[k][c] = fracvol.p[k][c] * cell_volume.g[c];
     }
+    // conservation-energie-totale (RemapADI.axl:151), F:751-773: the kinetic
+    // energy the dual remap carried (U_dual[4] / U_dual[3]) minus the kinetic
+    // energy of the remapped velocity, 0.25 per node over the cell's 8 nodes in
+    // cell-node order (only nodes of non-zero mass), floored at 0, goes into
+    // the specific internal energy: e_k += x_k delta on every environment cell
+    // and, in a mixed cell, the mean e += delta.  U_dual[4] is 0.5 m |v|
+    // (PrepareRemap.cc:421), not 0.5 m |v|^2; the reference's quirk is kept.
+    if (conservation_energie_totale) {
+#pragma omp parallel for schedule(static)
+      for (long c = 0; c < C; ++c) {
+        long cn[8];
+        cell_nodes(c, cn);
+        double delta_ec = 0.;
+        for (int a = 0; a < 8; ++a) {
+          const double* Ud = &u_dual[(size_t)cn[a] * nvars];
+          if (Ud[3] != 0.) {
+            const double ec_proj = Ud[4] / Ud[3];
+            const R3 v = velocity[cn[a]];
+            const double ec_reconst = 0.5 * (v.x * v.x + v.y * v.y + v.z * v.z);   // squareNormL2
+            delta_ec += 0.25 * (ec_proj - ec_reconst);
+          }
+        }
+        delta_ec = smax(0., delta_ec);                                  // std::max(0., delta_ec)
+        for (int k = 0; k < K; ++k) if (env_mask[c] >> k & 1) mv(internal_energy, k, c) += mv(mass_fraction, k, c) * delta_ec;
+        if (nbEnv(c) != 1) internal_energy.g[c] += delta_ec;
+      }
+    }
   }
   std::vector<uint32_t> prev_mask_scratch;
   bool env_mask_prev_bit(long c, int k) const { return !prev_mask_scratch.empty() && (prev_mask_scratch[c] >> k & 1); }
@@ -1695,6 +1723,13 @@ void orc_step(void* h, int ncycles) {
 }
 
 void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
+
+// Options beyond orc_create's list, by name; 0 when known, -1 otherwise.
+int orc_set_option(void* h, const char* name, int value) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (std::strcmp(name, "conservation_energie_totale") == 0) { o->conservation_energie_totale = value; return 0; }
+  return -1;
+}
 
 void orc_set_threads(int n) { omp_set_num_threads(n); }
 

@@ -53,6 +53,8 @@ def lib():
         L.orc_get_field.restype = ctypes.c_int
         L.orc_pow_third.argtypes = [ctypes.c_double, ctypes.c_int]
         L.orc_pow_third.restype = ctypes.c_double
+        L.orc_set_option.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
+        L.orc_set_option.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -98,6 +100,9 @@ class Oracle:
                               int(getattr(o, "with_newton", 0)), int(getattr(o, "schema_csts", 0)),
                               int(getattr(o, "pente_borne", 0)), int(getattr(o, "pente_borne_debar_fix", 0)),
                               int(getattr(o, "pente_borne_mixte", 0)), int(getattr(o, "limiteur_pure_id", 0)))
+        if int(getattr(o, "conservation_energie_totale", 0)):
+            if L.orc_set_option(self.h, b"conservation_energie_totale", 1) != 0:
+                raise RuntimeError("oracle: unknown option")
         fv = np.ascontiguousarray(case.fracvol, dtype=np.float64)
         de = np.ascontiguousarray(case.density, dtype=np.float64)
         pr = np.ascontiguousarray(case.pressure, dtype=np.float64)
