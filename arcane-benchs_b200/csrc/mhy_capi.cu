@@ -248,6 +248,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   dm.Fx = (long long)(dm.nx + 1) * dm.ny * dm.nz;
   dm.Fy = (long long)dm.nx * (dm.ny + 1) * dm.nz;
   dm.F = dm.Fx + dm.Fy + (long long)dm.nx * dm.ny * (dm.nz + 1);
+  dm.dt_k0 = 0; dm.dt_k1 = dm.nz;
   Phys& ph = c->ph;
   ph.gamma = opt->adiabatic_cst[0];
   c->K = opt->nb_env;
@@ -1642,6 +1643,116 @@ void* mhy_get_stream(mhy_ctx* c) {
 }
 
 int mhy_kernels_per_cycle(mhy_ctx* c) { return c ? c->kernels_per_cycle : 0; }
+
+// ---- slabs: one mesh split along z over several contexts ----------------------
+int mhy_set_dt_reduction(mhy_ctx* c, int32_t k_lo, int32_t k_hi, int32_t external) {
+  if (!c) return fail(MHY_ERR_ARG, "null context");
+  if (k_lo < 0 || k_hi > c->dm.nz || k_lo >= k_hi || (external != 0 && external != 1))
+    return fail(MHY_ERR_ARG, "need 0 <= k_lo < k_hi <= nz and external 0 or 1");
+  DeviceScope on_dev(c->device);
+  MHY_FLUSH(c);
+  c->dm.dt_k0 = k_lo;
+  c->dm.dt_k1 = k_hi;
+  c->ph.ext_dt = external;
+  for (int s = 0; s < 3; ++s)
+    if (c->graph[s]) { cudaGraphExecDestroy(c->graph[s]); c->graph[s] = nullptr; }
+  return MHY_OK;
+}
+
+int mhy_dt_local_min(mhy_ctx* c, void* dev_min_bits) {
+  if (!c || !dev_min_bits) return fail(MHY_ERR_ARG, "null argument");
+  if (!c->ph.ext_dt) return fail(MHY_ERR_STATE, "mhy_set_dt_reduction(..., external = 1) must come first");
+  DeviceScope on_dev(c->device);
+  MHY_FLUSH(c);
+  MHY_CUDA(cudaMemcpyAsync(dev_min_bits, &c->S->min_bits, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                           c->stream));
+  return MHY_OK;
+}
+
+int mhy_dt_finish(mhy_ctx* c, const void* dev_min_bits) {
+  if (!c || !dev_min_bits) return fail(MHY_ERR_ARG, "null argument");
+  if (!c->ph.ext_dt) return fail(MHY_ERR_STATE, "mhy_set_dt_reduction(..., external = 1) must come first");
+  DeviceScope on_dev(c->device);
+  MHY_FLUSH(c);
+  k_dt_finish_ext<<<1, 1, 0, c->stream>>>(c->S, c->ph, static_cast<const unsigned long long*>(dev_min_bits));
+  MHY_CUDA(cudaGetLastError());
+  return MHY_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The persistent state of layers [lo, hi) of cells and [nlo, nhi) of nodes, as
+// (device pointer, bytes) pieces in a fixed order: every restart-dump field,
+// each component plane's slice of those layers (contiguous, k is outermost).
+int halo_pieces(mhy_ctx* c, int lo, int hi, int nlo, int nhi, std::vector<std::pair<char*, size_t>>& out) {
+  const Dims& dm = c->dm;
+  if (c->K != 1) return fail(MHY_ERR_UNSUPPORTED, "slabs: one environment");
+  if (lo < 0 || hi > dm.nz || lo > hi || nlo < 0 || nhi > dm.nz + 1 || nlo > nhi)
+    return fail(MHY_ERR_ARG, "layer range outside the mesh");
+  const long long cl = (long long)dm.nx * dm.ny, nl = (long long)(dm.nx + 1) * (dm.ny + 1);
+  out.clear();
+  for (const CkField& f : ckpt_fields(c)) {
+    const size_t el = ckpt_elem(f.dtype);
+    const bool cell = std::strcmp(f.name, "Velocity") != 0 && std::strcmp(f.name, "NodeMass") != 0 &&
+                      std::strcmp(f.name, "DualGradPhi") != 0;   // the node fields of ckpt_fields
+    const long long items = cell ? dm.C : dm.N, comps = f.count / items, per = cell ? cl : nl;
+    const int a = cell ? lo : nlo, b = cell ? hi : nhi;
+    for (long long q = 0; q < comps; ++q)
+      out.emplace_back(static_cast<char*>(f.dev) + ((size_t)q * items + (size_t)a * per) * el, (size_t)(b - a) * per * el);
+  }
+  return MHY_OK;
+}
+
+int halo_copy(mhy_ctx* c, int lo, int hi, int nlo, int nhi, char* buf, size_t bytes, bool pack) {
+  std::vector<std::pair<char*, size_t>> pc;
+  int rc = halo_pieces(c, lo, hi, nlo, nhi, pc);
+  if (rc != MHY_OK) return rc;
+  size_t need = 0;
+  for (auto& x : pc) need += x.second;
+  if (bytes < need) return fail(MHY_ERR_ARG, "halo buffer too small (mhy_halo_bytes)");
+  size_t off = 0;
+  for (auto& x : pc) {
+    if (x.second)
+      MHY_CUDA(cudaMemcpyAsync(pack ? buf + off : x.first, pack ? x.first : buf + off, x.second,
+                               cudaMemcpyDeviceToDevice, c->stream));
+    off += x.second;
+  }
+  return MHY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhy_halo_bytes(mhy_ctx* c, int32_t cell_layers, int32_t node_layers, size_t* bytes) {
+  if (!c || !bytes) return fail(MHY_ERR_ARG, "null argument");
+  std::vector<std::pair<char*, size_t>> pc;
+  const int rc = halo_pieces(c, 0, cell_layers, 0, node_layers, pc);
+  if (rc != MHY_OK) return rc;
+  size_t need = 0;
+  for (auto& x : pc) need += x.second;
+  *bytes = need;
+  return MHY_OK;
+}
+
+int mhy_halo_pack(mhy_ctx* c, int32_t cell_lo, int32_t cell_hi, int32_t node_lo, int32_t node_hi, void* dev_dst,
+                  size_t bytes) {
+  if (!c || !dev_dst) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
+  MHY_FLUSH(c);
+  return halo_copy(c, cell_lo, cell_hi, node_lo, node_hi, static_cast<char*>(dev_dst), bytes, true);
+}
+
+int mhy_halo_unpack(mhy_ctx* c, int32_t cell_lo, int32_t cell_hi, int32_t node_lo, int32_t node_hi,
+                    const void* dev_src, size_t bytes) {
+  if (!c || !dev_src) return fail(MHY_ERR_ARG, "null argument");
+  DeviceScope on_dev(c->device);
+  MHY_FLUSH(c);
+  return halo_copy(c, cell_lo, cell_hi, node_lo, node_hi, const_cast<char*>(static_cast<const char*>(dev_src)), bytes,
+                   false);
+}
 
 void mhy_destroy(mhy_ctx* c) {
   if (!c) return;

@@ -614,7 +614,7 @@ void launch_delta_t(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
   k_dt_min<<<nbc, 128, 0, s>>>(a.dm, a.S, a.L, a.st.cs, a.vnorm, linear);
-  k_dt_finish<<<1, 1, 0, s>>>(a.S, a.ph);
+  if (!a.ph.ext_dt) k_dt_finish<<<1, 1, 0, s>>>(a.S, a.ph);
 }
 
 // ------------------------------------------------------------------------

@@ -240,6 +240,8 @@ __device__ __forceinline__ void compute_cqs(const D3 x[8], const D3 fc[6], D3 ou
 struct Dims {
   int nx, ny, nz;          // cells per direction
   long long C, N, F, Fx, Fy;
+  int dt_k0, dt_k1;        // cell layers k the dt reduction covers: [0, nz) unless the mesh is a slab
+                           // with ghost layers (mhy_set_dt_reduction)
   __device__ __forceinline__ long long cid(int i, int j, int k) const { return i + (long long)nx * (j + (long long)ny * k); }
   __device__ __forceinline__ long long nid(int i, int j, int k) const { return i + (long long)(nx + 1) * (j + (long long)(ny + 1) * k); }
   __host__ __device__ __forceinline__ int ncd(int d) const { return d == 0 ? nx : (d == 1 ? ny : nz); }

@@ -276,4 +276,11 @@ __global__ void k_dt_min(Dims dm, Scalars* __restrict__ S, const double* __restr
 
 __global__ void k_dt_finish(Scalars* S, Phys ph) { dt_finish_body(S, ph); }
 
+// The dt of a slab decomposition: the minimum over all ranks' owned cells
+// (combined by the caller) replaces the local one, then computeDeltaT as usual.
+__global__ void k_dt_finish_ext(Scalars* S, Phys ph, const unsigned long long* __restrict__ min_bits) {
+  S->min_bits = *min_bits;
+  dt_finish_body(S, ph);
+}
+
 }  // namespace mhy

@@ -36,6 +36,8 @@ struct Phys {
   // reconstruction (computeY0), and whether the sweep is the first of the cycle
   int pb, pb_pure, pb_debar, pb_lim_y0, pb_first;
   int cons_ec;          // conservation-energie-totale (RemapADI.axl:151; one environment, FP64)
+  int ext_dt;           // slabs: the cycle ends with the local dt minimum; the caller combines the
+                        // ranks' minima and finishes the dt (mhy_dt_finish)
 };
 
 struct BCTable {
@@ -177,6 +179,7 @@ __global__ void k_bc_mask(long long n, const unsigned* grp, int nbc, const int* 
 __global__ void k_dt_min(Dims dm, Scalars* S, const double* L, const double* cs, const double* vnorm, int linear);
 dim3 cell_grid(const Dims& dm, int& linear);
 __global__ void k_dt_finish(Scalars* S, Phys ph);
+__global__ void k_dt_finish_ext(Scalars* S, Phys ph, const unsigned long long* min_bits);
 
 // computeHydroDeltaT (MahycoModule.cc:2047-2061): min over cells of
 // L / (c + max |v|) (|v| per node precomputed), warp shuffle + block
@@ -187,7 +190,7 @@ __device__ __forceinline__ void dt_min_body(Dims dm, Scalars* __restrict__ S, co
                                             int bx_, int by_, int bz_) {
   __shared__ unsigned long long wmin[32];
   int i, j, k;
-  const bool has = block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k);
+  const bool has = block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k) && k >= dm.dt_k0 && k < dm.dt_k1;
   unsigned long long best = 0x7fefffffffffffffull;  // DBL_MAX
   if (has) {
     const long long c = dm.cid(i, j, k);

@@ -39,7 +39,8 @@ EXPORTED = ["mhy_options_default", "mhy_create", "mhy_set_state", "mhy_hydro_sta
             "mhy_batch_destroy", "mhy_checkpoint_size", "mhy_checkpoint_save", "mhy_checkpoint_load",
             "mhy_get_totals", "mhy_batch_get_totals", "mhy_autotune", "mhy_set_tuning", "mhy_get_tuning",
             "mhy_batch_autotune", "mhy_batch_set_tuning", "mhy_batch_get_tuning", "mhy_create_csr",
-            "mhy_csr_structure"]
+            "mhy_csr_structure", "mhy_set_dt_reduction", "mhy_dt_local_min", "mhy_dt_finish", "mhy_halo_bytes",
+            "mhy_halo_pack", "mhy_halo_unpack"]
 MHY_TUNE_SLOTS = 10
 TUNE_SLOTS = ("lagrange_nodes", "lagrange_cells", "cells_x", "cells_y", "cells_z", "nodes_x", "nodes_y", "nodes_z",
               "dt_min", "dt_finish")
@@ -179,6 +180,12 @@ def load(path: pathlib.Path | str | None = None):
     L.mhy_csr_structure.restype = ctypes.c_int
     L.mhy_create_csr.argtypes = [ctypes.POINTER(CCsrMesh), ctypes.POINTER(COptions), ctypes.c_int, ctypes.POINTER(vp)]
     L.mhy_create_csr.restype = ctypes.c_int
+    L.mhy_set_dt_reduction.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    L.mhy_dt_local_min.argtypes = [vp, vp]
+    L.mhy_dt_finish.argtypes = [vp, vp]
+    L.mhy_halo_bytes.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t)]
+    L.mhy_halo_pack.argtypes = [vp] + [ctypes.c_int32] * 4 + [vp, ctypes.c_size_t]
+    L.mhy_halo_unpack.argtypes = [vp] + [ctypes.c_int32] * 4 + [vp, ctypes.c_size_t]
     _lib = L
     return L
 
@@ -388,6 +395,28 @@ class Context:
         _check(load().mhy_get_env_field(self.h, ENV_FIELDS[name], int(k), out.ctypes.data_as(ctypes.c_void_p),
                                         out.nbytes))
         return out
+
+    # slabs: dt over owned cell layers, combined and finished by the caller;
+    # the ghost layers' state moved through device buffers (data pointers)
+    def set_dt_reduction(self, k_lo: int, k_hi: int, external: bool = True):
+        _check(load().mhy_set_dt_reduction(self.h, int(k_lo), int(k_hi), int(external)))
+
+    def dt_local_min(self, dev_ptr: int):
+        _check(load().mhy_dt_local_min(self.h, ctypes.c_void_p(dev_ptr)))
+
+    def dt_finish(self, dev_ptr: int):
+        _check(load().mhy_dt_finish(self.h, ctypes.c_void_p(dev_ptr)))
+
+    def halo_bytes(self, cell_layers: int, node_layers: int) -> int:
+        n = ctypes.c_size_t()
+        _check(load().mhy_halo_bytes(self.h, int(cell_layers), int(node_layers), ctypes.byref(n)))
+        return n.value
+
+    def halo_pack(self, clo, chi, nlo, nhi, dev_ptr: int, nbytes: int):
+        _check(load().mhy_halo_pack(self.h, clo, chi, nlo, nhi, ctypes.c_void_p(dev_ptr), nbytes))
+
+    def halo_unpack(self, clo, chi, nlo, nhi, dev_ptr: int, nbytes: int):
+        _check(load().mhy_halo_unpack(self.h, clo, chi, nlo, nhi, ctypes.c_void_p(dev_ptr), nbytes))
 
     def env_mask(self) -> np.ndarray:
         out = np.empty(self.case.ncells, dtype=np.uint32)

@@ -14,7 +14,9 @@ buffers (pinned), mhy_create + mhy_set_state + mhy_hydro_start_init, then K
 cycles driven entry point by entry point with dt read back to the host every
 cycle (the Arcane time loop reads it), then the final density, energy and
 velocity read back.  N > 1 GPUs run independent replicas (weak scaling; the
-path has no data exchange between independent meshes).
+path has no data exchange between independent meshes); with --slabs the one
+mesh is split along z over the N GPUs instead (strong scaling: ghost layers,
+one NCCL dt all-reduce and one halo exchange per cycle).
 
 Beside the timed number, the default line carries `parity` (a fresh context
 stepped cycle by cycle against the CPU oracle with the C library's pow, over
@@ -82,6 +84,9 @@ def parse():
     ap.add_argument("--parity-cycles", type=int, default=60,
                     help="cycles of the parity check against the libm-pow oracle (capped at warmup + steps; "
                          "0 = no parity check)")
+    ap.add_argument("--slabs", action="store_true",
+                    help="split the one mesh along z over the N GPUs (ghost layers, one dt all-reduce and one "
+                         "halo exchange per cycle over NCCL; strong scaling) instead of N independent replicas")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the mixed-precision and batched figures of the default line")
     return ap.parse_args()
@@ -744,10 +749,73 @@ def measure_forms(args, device, plain_value, plain_density, plain_totals):
     return out
 
 
+def run_ours_slabs(args):
+    """--slabs: the workload's mesh split along z over the N GPUs
+    (mhy_b200/slabs.py).  Each rank advances its slab plus ghost layers; per
+    cycle one NCCL all-reduce (min) of the dt bit patterns and one halo
+    exchange (send/recv of the neighbours' boundary layers), both ordered on
+    the context's stream.  value = the whole mesh's cell-cycles/s (owned cells
+    only; the ghost layers' recomputation is overhead), max time over ranks."""
+    import torch
+    from mhy_b200 import bytes_model, replicas, slabs
+
+    world, rank, local = replicas.ranks()
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        replicas.init("nccl", device=dev)
+    case, wname = make_case(args)
+    lay = slabs.layout(case.nz, world)
+    rk = slabs.SlabRank(case, lay, rank, lambda c: slabs.GpuEngine(c, local))
+    ctx = rk.eng.ctx
+    tuning = apply_tuning(ctx, args)
+    kpc = ctx.kernels_per_cycle() + 1                     # + the dt finish from the combined minimum
+    slabs.run_distributed(rk, args.warmup)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        replicas.barrier()
+        torch.cuda.synchronize()
+        start.record(rk.eng.stream)
+        slabs.run_distributed(rk, args.steps)
+        stop.record(rk.eng.stream)
+        torch.cuda.synchronize()
+        replicas.barrier()
+    owned_cells = rk.s.own * case.nx * case.ny
+    ms, value = replicas.aggregate(owned_cells, args.steps, start.elapsed_time(stop), dev)
+    status = ctx.status()
+    b_alg = bytes_model.bytes_per_cell_cycle(case.ncells, case.nnodes)
+    peak, peak_kind = measured_peak()
+    achieved = b_alg * value / 1e9 / world
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 remap evaluation / f64 state",
+                "data": "synthetic",
+                "config": {"workload": f"{wname}-slabs{world}", "cells": case.ncells, "nodes": case.nnodes,
+                           "parallelism": f"z-slabs over {world} GPUs, {slabs.GHOST} ghost layers a side",
+                           "slab_layers": [s.own for s in lay],
+                           "l2": "working set > 126 MB L2 (no flush needed)", "tuning": tuning},
+                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                             "kernel": "one slab cycle per GPU (graph) + dt finish; algorithmic bytes of the owned "
+                                       f"cells, {b_alg:.1f} B/cell-cycle"},
+                "cpu_baseline": None, "e2e": None, "gpu_launches": kpc * args.steps, "clocks": clk.summary(),
+                "device_status": status}
+        print(json.dumps(line), flush=True)
+    rk.eng.close()
+    replicas.finish()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.slabs:
+        return run_ours_slabs(args)
     if args.workload == "batched":
         return run_ours_batched(args)
     return run_ours(args)

@@ -257,6 +257,37 @@ int mhy_checkpoint_size(mhy_ctx* ctx, size_t* bytes);
 int mhy_checkpoint_save(mhy_ctx* ctx, void* dst, size_t bytes);
 int mhy_checkpoint_load(mhy_ctx* ctx, const void* src, size_t bytes);
 
+/* ---- slabs: one mesh split along z over several contexts (GPUs) ----
+ * The reference splits its mesh into MPI subdomains with ghost layers
+ * (MahycoModule.cc:62-75) and reduces dt over all of them once a cycle
+ * (ReducerMin, MahycoModule.cc:2067).  Here each rank holds a context on its
+ * own z-slab plus `ghost` layers of the neighbours' cells and nodes on each
+ * inner side, deeper than one cycle's dependency reach along z (at most 5
+ * layers: Lagrange 1, cell sweep 2, node sweep and its mass fluxes 2), so the
+ * owned layers of every rank come out of a cycle exactly as in the unsplit
+ * run.  A cycle is: mhy_step(ctx, 1) (ending with the dt minimum over the
+ * owned cell layers only), mhy_dt_local_min, a minimum over the ranks done by
+ * the caller (e.g. an NCCL all-reduce on the 64-bit pattern: non-negative
+ * doubles order like unsigned integers), mhy_dt_finish, then the ghost
+ * layers refreshed from the neighbours with mhy_halo_pack / mhy_halo_unpack
+ * (every restart-dump field, contiguous per component and layer range; the
+ * caller moves the buffers, e.g. with NCCL send/recv).  One environment. */
+/* dt reduced over cell layers [k_lo, k_hi) of this context; external = 1:
+ * the cycle stops after the local minimum (mhy_dt_local_min / mhy_dt_finish). */
+int mhy_set_dt_reduction(mhy_ctx* ctx, int32_t k_lo, int32_t k_hi, int32_t external);
+/* copies the local minimum (uint64 bit pattern) to device memory, on the context's stream */
+int mhy_dt_local_min(mhy_ctx* ctx, void* dev_min_bits);
+/* the new dt from the combined minimum (device uint64), on the context's stream */
+int mhy_dt_finish(mhy_ctx* ctx, const void* dev_min_bits);
+/* bytes of the state of `cell_layers` cell layers and `node_layers` node layers */
+int mhy_halo_bytes(mhy_ctx* ctx, int32_t cell_layers, int32_t node_layers, size_t* bytes);
+/* state of cell layers [cell_lo, cell_hi) and node layers [node_lo, node_hi) to / from a
+ * device buffer, on the context's stream */
+int mhy_halo_pack(mhy_ctx* ctx, int32_t cell_lo, int32_t cell_hi, int32_t node_lo, int32_t node_hi, void* dev_dst,
+                  size_t bytes);
+int mhy_halo_unpack(mhy_ctx* ctx, int32_t cell_lo, int32_t cell_hi, int32_t node_lo, int32_t node_hi,
+                    const void* dev_src, size_t bytes);
+
 /* ---- batches: many independent single-environment meshes on one GPU ----
  * No counterpart in the reference (one Arcane process runs one mesh): a batch
  * advances n instances of uneven sizes, options and initial states together,

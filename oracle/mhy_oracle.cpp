@@ -97,6 +97,10 @@ struct Oracle {
   // projection-pente-borne-mixte, projection-limiteur-pure-id
   int pente_borne = 0, pb_debar_fix = 0, pb_mixte = 0, limiteur_pure_id = 0;
   int conservation_energie_totale = 0;   // RemapADI.axl:151
+  // slabs: the dt minimum over cell layers [dt_k0, dt_k1) only; with ext_dt
+  // the cycle stops at the local minimum and orc_dt_finish completes it
+  int dt_k0 = 0, dt_k1 = -1, ext_dt = 0;
+  double local_min = 0.;
   std::vector<double> gamma;
   std::vector<int> eos;             // per environment: 0 PerfectGas, 1 StiffenedGas
   std::vector<double> pinf;         // StiffenedGas limit-tension (StiffenedGasEOS.axl:104)
@@ -1609,15 +1613,15 @@ struct Oracle {
     computePressionMoyenne();
   }
 
-  void computeDeltaT() {  // M:2076-2191 -> computeHydroDeltaT M:2027-2071
-    global_old_deltat = global_deltat;
-    old_deltat = global_old_deltat;
+  // computeHydroDeltaT M:2027-2071 over the cells of layers [dt_k0, dt_k1)
+  double hydroDeltaTMin() {
     double minimum_aux = std::numeric_limits<double>::max();
+    const long c0 = (long)dt_k0 * nx * ny, c1 = dt_k1 < 0 ? C : (long)dt_k1 * nx * ny;
 #pragma omp parallel
     {
       double lmin = std::numeric_limits<double>::max();
 #pragma omp for schedule(static)
-      for (long c = 0; c < C; ++c) {
+      for (long c = c0; c < c1; ++c) {
         long cn[8]; cell_nodes(c, cn);
         double vmax = 0.;
         for (int a = 0; a < 8; ++a) vmax = amax(normL2(velocity[cn[a]]), vmax);
@@ -1627,6 +1631,14 @@ struct Oracle {
 #pragma omp critical
       minimum_aux = amin(minimum_aux, lmin);
     }
+    return minimum_aux;
+  }
+
+  void computeDeltaT() { finishDeltaT(hydroDeltaTMin()); }   // M:2076-2191
+
+  void finishDeltaT(double minimum_aux) {
+    global_old_deltat = global_deltat;
+    old_deltat = global_old_deltat;
     double new_dt = cfl * minimum_aux;
     new_dt = amin(new_dt, 1.05 * global_old_deltat);
     new_dt = amin(new_dt, deltat_max);
@@ -1646,8 +1658,23 @@ struct Oracle {
     updateEnergyAndPressure();
     remap();
     global_time += global_deltat;
+    if (ext_dt) { local_min = hydroDeltaTMin(); return; }       // orc_dt_finish completes the cycle
     computeDeltaT();
     ++iteration;
+  }
+
+  // slabs: the state a cycle starts from (K = 1) for cell layers [clo, chi)
+  // and node layers [nlo, nhi), field by field; pack (to buf) or unpack
+  template <class F>
+  void halo_fields(int clo, int chi, int nlo, int nhi, F&& f) {
+    const long cl = (long)nx * ny, nl = (long)NX * NY;
+    const long c0 = clo * cl, c1 = chi * cl, n0 = nlo * nl, n1 = nhi * nl;
+    MatVar* cv[] = {&density, &internal_energy, &pressure, &sound_speed, &pseudo_viscosity, &cell_mass};
+    for (MatVar* v : cv) for (long c = c0; c < c1; ++c) f(v->g[c]);
+    for (long c = c0; c < c1; ++c) for (int a = 0; a < 8; ++a) { f(cqs[8 * c + a].x); f(cqs[8 * c + a].y); f(cqs[8 * c + a].z); }
+    for (long n = n0; n < n1; ++n) { f(velocity[n].x); f(velocity[n].y); f(velocity[n].z); }
+    for (long n = n0; n < n1; ++n) f(node_mass[n]);
+    for (long n = n0; n < n1; ++n) for (int v = 0; v < nvars; ++v) f(dual_grad_phi[(size_t)n * nvars + v]);
   }
 };
 
@@ -1723,6 +1750,39 @@ void orc_step(void* h, int ncycles) {
 }
 
 void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
+
+// Slabs (one environment): dt over cell layers [k_lo, k_hi), external finish.
+int orc_set_dt_reduction(void* h, int k_lo, int k_hi, int external) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (o->K != 1 || k_lo < 0 || k_hi > o->nz || k_lo >= k_hi) return -1;
+  o->dt_k0 = k_lo; o->dt_k1 = k_hi; o->ext_dt = external;
+  return 0;
+}
+double orc_dt_local_min(void* h) { return static_cast<Oracle*>(h)->local_min; }
+void orc_dt_finish(void* h, double minimum) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->finishDeltaT(minimum);
+  ++o->iteration;
+}
+long orc_halo_count(void* h, int cell_layers, int node_layers) {
+  long n = 0;
+  static_cast<Oracle*>(h)->halo_fields(0, cell_layers, 0, node_layers, [&](double&) { ++n; });
+  return n;
+}
+int orc_halo_pack(void* h, int clo, int chi, int nlo, int nhi, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (clo < 0 || chi > o->nz || clo > chi || nlo < 0 || nhi > o->nz + 1 || nlo > nhi) return -1;
+  long i = 0;
+  o->halo_fields(clo, chi, nlo, nhi, [&](double& v) { out[i++] = v; });
+  return 0;
+}
+int orc_halo_unpack(void* h, int clo, int chi, int nlo, int nhi, const double* in) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (clo < 0 || chi > o->nz || clo > chi || nlo < 0 || nhi > o->nz + 1 || nlo > nhi) return -1;
+  long i = 0;
+  o->halo_fields(clo, chi, nlo, nhi, [&](double& v) { v = in[i++]; });
+  return 0;
+}
 
 // Options beyond orc_create's list, by name; 0 when known, -1 otherwise.
 int orc_set_option(void* h, const char* name, int value) {

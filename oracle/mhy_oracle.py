@@ -55,6 +55,16 @@ def lib():
         L.orc_pow_third.restype = ctypes.c_double
         L.orc_set_option.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         L.orc_set_option.restype = ctypes.c_int
+        L.orc_set_dt_reduction.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 3
+        L.orc_set_dt_reduction.restype = ctypes.c_int
+        L.orc_dt_local_min.argtypes = [ctypes.c_void_p]
+        L.orc_dt_local_min.restype = ctypes.c_double
+        L.orc_dt_finish.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.orc_halo_count.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.orc_halo_count.restype = ctypes.c_long
+        for name in ("orc_halo_pack", "orc_halo_unpack"):
+            getattr(L, name).argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 4 + [dp]
+            getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -143,6 +153,31 @@ class Oracle:
         if lib().orc_get_field(self.h, 50, _dp(out)) != 0:
             raise KeyError("env_mask")
         return out.astype(np.uint32)
+
+    # slabs (one environment): dt over owned cell layers, combined outside
+    def set_dt_reduction(self, k_lo: int, k_hi: int, external: bool = True):
+        if lib().orc_set_dt_reduction(self.h, int(k_lo), int(k_hi), int(external)) != 0:
+            raise ValueError("bad dt layer range")
+
+    def dt_local_min(self) -> float:
+        return lib().orc_dt_local_min(self.h)
+
+    def dt_finish(self, minimum: float):
+        lib().orc_dt_finish(self.h, float(minimum))
+
+    def halo_count(self, cell_layers: int, node_layers: int) -> int:
+        return int(lib().orc_halo_count(self.h, int(cell_layers), int(node_layers)))
+
+    def halo_pack(self, clo, chi, nlo, nhi) -> np.ndarray:
+        out = np.empty(self.halo_count(chi - clo, nhi - nlo))
+        if lib().orc_halo_pack(self.h, clo, chi, nlo, nhi, _dp(out)) != 0:
+            raise ValueError("bad layer range")
+        return out
+
+    def halo_unpack(self, clo, chi, nlo, nhi, buf: np.ndarray):
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        if buf.size != self.halo_count(chi - clo, nhi - nlo) or lib().orc_halo_unpack(self.h, clo, chi, nlo, nhi, _dp(buf)) != 0:
+            raise ValueError("bad layer range or buffer")
 
     def close(self):
         if self.h:
