@@ -351,10 +351,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       err = cudaMemcpyAsync(surf, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream);
       k_bc_mask<<<(unsigned)nb, 256, 0, c->stream>>>(N, grp, opt->nb_bc, surf, c->bcmask);
       if (err == cudaSuccess) err = cudaGetLastError();
-      if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
     }
     if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   }
+  // one wait at the end: the caller's coordinates may be pinned memory it frees on return
   Scalars s0{};
   s0.dt = opt->deltat_init; s0.old_dt = 0.; s0.time = 0.; s0.inv_dt = 1.0 / opt->deltat_init; s0.min_bits = 0x7fefffffffffffffull;
   err = cudaMemcpyAsync(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream);
@@ -426,10 +426,18 @@ int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
     st = &perm;
   }
   if (K == 1) {
-    for (long long i = 0; i < C; ++i)
-      if (!(st->fracvol[i] > 0.)) return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
+    // the copies run while the host checks the volume fractions; a refused
+    // state leaves the context without a state (state_set stays false)
     MHY_CUDA(cudaMemcpyAsync(c->rho, st->density, C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     MHY_CUDA(cudaMemcpyAsync(c->p, st->pressure, C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    MHY_CUDA(cudaMemcpyAsync(c->ud[0], st->velocity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    bool ok = true;
+    for (long long i = 0; i < C; ++i) ok &= st->fracvol[i] > 0.;
+    if (!ok) {
+      cudaStreamSynchronize(c->stream);               // the caller may free its buffers on return
+      c->state_set = false;
+      return fail(MHY_ERR_UNSUPPORTED, "single-environment context: every cell needs fracvol > 0");
+    }
   } else {
     // Environments from the volume fractions and the initial per-environment
     // state, as HydroStartInit sets them up on the host (MahycoModule.cc:48-127
@@ -473,7 +481,8 @@ int mhy_set_state(mhy_ctx* c, const mhy_state* st) {
     MHY_CUDA(cudaMemcpyAsync(ev.p, pk.data(), (size_t)K * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   }
   // interleaved velocity staged in ud[0] (unused until the first cycle), then planes
-  MHY_CUDA(cudaMemcpyAsync(c->ud[0], st->velocity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (K > 1)
+    MHY_CUDA(cudaMemcpyAsync(c->ud[0], st->velocity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   k_soa3<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(N, c->ud[0], c->v);
   MHY_CUDA(cudaGetLastError());
   MHY_CUDA(cudaStreamSynchronize(c->stream));
@@ -491,18 +500,10 @@ namespace {
 int init_geometry(mhy_ctx* c) {
   const Dims& dm = c->dm;
   cudaStream_t s = c->stream;
-  double *xc0 = nullptr, *xf0 = nullptr;          // temporaries: initial cell and face centres
-  MHY_CUDA(cudaMalloc(&xc0, 3 * dm.C * sizeof(double)));
-  cudaError_t err = cudaMalloc(&xf0, 3 * dm.F * sizeof(double));
-  if (err != cudaSuccess) { cudaFree(xc0); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
-  k_init_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, xc0, c->cqs, c->Ve, c->L, c->ph.lc_mode);
-  k_init_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->x0, c->n0, xf0);
-  k_init_outer_normals<<<blocks(dm.C), kThreads, 0, s>>>(dm, xc0, xf0, c->ofn);
-  err = cudaGetLastError();
-  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-  cudaFree(xc0);
-  cudaFree(xf0);
-  if (err != cudaSuccess) return fail(MHY_ERR_CUDA, cudaGetErrorString(err));
+  k_init_cells<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, nullptr, c->cqs, c->Ve, c->L, c->ph.lc_mode);
+  k_init_faces<<<blocks(dm.F), kThreads, 0, s>>>(dm, c->x0, c->n0, nullptr);
+  k_init_outer_normals<<<blocks(dm.C), kThreads, 0, s>>>(dm, c->x0, c->ofn);
+  MHY_CUDA(cudaGetLastError());
   return MHY_OK;
 }
 
@@ -1486,9 +1487,11 @@ int mhy_checkpoint_load(mhy_ctx* c, const void* src, size_t bytes) {
   const std::vector<CkField> f = ckpt_fields(c);
   if (hd.nfields != (int32_t)f.size() || bytes < sizeof(CkptHeader) + f.size() * sizeof(CkptField))
     return fail(MHY_ERR_ARG, "restart dump field list does not match this context");
-  // geometry of t = 0 from the mesh, then the dumped state over it
+  // geometry of t = 0 from the mesh, then the dumped state over it (the
+  // copies below are synchronous on another stream: wait for the geometry)
   const int rc = init_geometry(c);
   if (rc != MHY_OK) return rc;
+  MHY_CUDA(cudaStreamSynchronize(c->stream));
   for (size_t i = 0; i < f.size(); ++i) {
     CkptField r;
     std::memcpy(&r, base + sizeof(CkptHeader) + i * sizeof(CkptField), sizeof(r));

@@ -23,7 +23,7 @@ __global__ void k_init_cells(Dims dm, const double* __restrict__ x0, double* __r
   D3 s = d3(0., 0., 0.);
   for (int a = 0; a < 8; ++a) s = s + x[a];
   D3 cc = 0.125 * s;
-  xc0[c] = cc.x; xc0[dm.C + c] = cc.y; xc0[2 * dm.C + c] = cc.z;
+  if (xc0) { xc0[c] = cc.x; xc0[dm.C + c] = cc.y; xc0[2 * dm.C + c] = cc.z; }
   D3 fc[6], q[8];
   face_centres(x, fc);
   compute_cqs(x, fc, q);
@@ -59,6 +59,7 @@ __global__ void k_init_faces(Dims dm, const double* __restrict__ x0, double* __r
   nn.z = v1.x * v2.y - v1.y * v2.x;
   double nr = norm2(nn);
   n0[f] = nn.x / nr; n0[dm.F + f] = nn.y / nr; n0[2 * dm.F + f] = nn.z / nr;
+  if (!xf0) return;
   D3 s = d3(0., 0., 0.);
   for (int a = 0; a < 4; ++a) s = s + 0.25 * x[a];
   xf0[f] = s.x; xf0[dm.F + f] = s.y; xf0[2 * dm.F + f] = s.z;
@@ -66,20 +67,27 @@ __global__ void k_init_faces(Dims dm, const double* __restrict__ x0, double* __r
 
 // Outer face normals (axis component only, the one the remap uses),
 // MahycoModule.cc:1041-1048.  ofn[lf*C + c], local faces z-,x-,y-,z+,x+,y+.
-__global__ void k_init_outer_normals(Dims dm, const double* __restrict__ xc0, const double* __restrict__ xf0,
-                                     double* __restrict__ ofn) {
+// The initial cell and face centres are recomputed here from the node
+// coordinates with the operations of k_init_cells and k_init_faces (the same
+// bits), so the set-up needs no temporary arrays.
+__global__ void k_init_outer_normals(Dims dm, const double* __restrict__ x0, double* __restrict__ ofn) {
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= dm.C) return;
   int i, j, k; dm.cijk(c, i, j, k);
-  const long long cf[6] = {dm.fid(2, i, j, k), dm.fid(0, i, j, k), dm.fid(1, i, j, k),
-                           dm.fid(2, i, j, k + 1), dm.fid(0, i + 1, j, k), dm.fid(1, i, j + 1, k)};
-  const int ax[6] = {2, 0, 1, 2, 0, 1};
-  D3 cc = d3(xc0[c], xc0[dm.C + c], xc0[2 * dm.C + c]);
+  D3 s = d3(0., 0., 0.);
+  for (int a = 0; a < 8; ++a) {
+    const long long n = dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2]);
+    s = s + d3(x0[n], x0[dm.N + n], x0[2 * dm.N + n]);
+  }
+  const D3 cc = 0.125 * s;
+  const int fd[6][4] = {{2, i, j, k}, {0, i, j, k}, {1, i, j, k}, {2, i, j, k + 1}, {0, i + 1, j, k}, {1, i, j + 1, k}};
   for (int a = 0; a < 6; ++a) {
-    long long f = cf[a];
-    D3 dv = d3(xf0[f], xf0[dm.F + f], xf0[2 * dm.F + f]) - cc;
-    double nr = norm2(dv);
-    ofn[a * dm.C + c] = comp(dv, ax[a]) / nr;
+    long long fn[4]; face_node_ids(dm, fd[a][0], fd[a][1], fd[a][2], fd[a][3], fn);
+    D3 xf = d3(0., 0., 0.);
+    for (int b = 0; b < 4; ++b) xf = xf + 0.25 * d3(x0[fn[b]], x0[dm.N + fn[b]], x0[2 * dm.N + fn[b]]);
+    const D3 dv = xf - cc;
+    const double nr = norm2(dv);
+    ofn[a * dm.C + c] = comp(dv, fd[a][0]) / nr;
   }
 }
 

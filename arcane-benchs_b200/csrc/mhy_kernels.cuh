@@ -159,7 +159,7 @@ constexpr int kKernelsPerCycleBatch = 10;
 
 __global__ void k_init_cells(Dims dm, const double* x0, double* xc0, double* cqs, double* vol, double* L, int lc_mode);
 __global__ void k_init_faces(Dims dm, const double* x0, double* n0, double* xf0);
-__global__ void k_init_outer_normals(Dims dm, const double* xc0, const double* xf0, double* ofn);
+__global__ void k_init_outer_normals(Dims dm, const double* x0, double* ofn);
 constexpr int kTotalsThreads = 256;
 constexpr int kTotalsBlocks = 148;   // one per SM; partials: 6 doubles per block
 __global__ void k_totals_partial(Dims dm, const double* mass, const double* e, const double* nm, const double* v,
