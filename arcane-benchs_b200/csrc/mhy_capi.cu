@@ -199,8 +199,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection 3: one environment in FP64 on the device");
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 7)
     return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0..7 (TypesMahyco.h:65-74)");
-  if (opt->projection_limiteur_id >= 3 && (opt->nb_env != 1 || opt->precision != 0))
-    return fail(MHY_ERR_UNSUPPORTED, "the generalised (G) limiters: one environment in FP64 on the device");
+  if (opt->projection_limiteur_id >= 3 && opt->precision != 0)
+    return fail(MHY_ERR_UNSUPPORTED, "the generalised (G) limiters: FP64 on the device");
   if (opt->projection_limiteur_id >= 3 && (mesh->nx < 3 || mesh->ny < 3 || mesh->nz < 3))
     return fail(MHY_ERR_UNSUPPORTED, "the generalised (G) limiters need 3 cells or more along every direction");
   if (opt->nb_bc < 0 || opt->nb_bc > MHY_MAX_BC) return fail(MHY_ERR_ARG, "nb_bc out of range");

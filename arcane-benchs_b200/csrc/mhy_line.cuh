@@ -908,8 +908,8 @@ static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin,
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + 1 + kLineUpd - 1) / kLineUpd;
   const int T = 32 * kLineWarps;
-  // the generalised limiters (one environment, FP64) have their own kernels
-  const bool gl = K == 1 && sizeof(R) == 8 && a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
+  // the generalised limiters (FP64) have their own kernels
+  const bool gl = sizeof(R) == 8 && a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3;
   if constexpr (D == 0) {
     const dim3 g(nseg, (dm.ny + 1 + kLineWarps - 1) / kLineWarps, dm.nz + 1);
     if (gl)
@@ -919,7 +919,7 @@ static void sweep_nodes_launch(const CycleArgs& a, int prev, const double* udin,
       k_cyc_sweep_nodes_x<FIRST, LAST, K, R><<<g, T, 0, s>>>(dm, a.S, a.ph, prev, a.x0, a.xl, a.vh, a.nm, udin, udout,
                                                        a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, a.ecn);
   } else {
-    if constexpr (K == 1 && sizeof(R) == 8) {
+    if constexpr (sizeof(R) == 8) {
       if (gl) { sweep_nodes_launch_w<D, FIRST, LAST, K, R, kLineWarps, true>(a, prev, udin, udout, s); return; }
     }
     // lines per block of this sweep (the tuning; K > 1 meshes keep 8)

@@ -38,12 +38,16 @@ struct CellInK {
   double db, df, u, A, n[3];   // low face of the cell along d (inner faces only)
   double ob, of;               // outward-normal component along d of the back and front faces
   double den;                  // divisor of Phi on the first sweep: the Lagrangian volume
+  double h;                    // G limiters: the cell's width along d (RemapADIService.cc:225-258)
 };
 
 // One line step of the remap of a K-environment cell (RemapADIService.cc:91-271,
 // 447-517, 658-720, 883-1040).  out = the 3K+1 updated components, then the
-// K dual mass fluxes.
-template <int K, bool FIRST, typename R>
+// K dual mass fluxes.  GL: the generalised limiters for uneven widths
+// (RemapADIService.cc:319-437 -> UtilesRemap.cc:295-330), every component
+// limited alike; at the ends of the line the back or front cell is the cell
+// itself.
+template <int K, bool FIRST, typename R, bool GL = false>
 __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
                                               bool upd, const CellInK<K>& in, double* out) {
   constexpr int NV = 3 * K + 1;
@@ -71,12 +75,22 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
                           : 0.;
   const R dxR = (R)dx, rdx = inner ? Ar<R>::rcp(dxR) : R(0);
   R G[NV], Pp[NV];
+  R h0 = R(0), hm = R(0), hp = R(0);
+  if constexpr (GL) {
+    const double hb = __shfl_up_sync(full, in.h, 1), hn = __shfl_down_sync(full, in.h, 1);
+    h0 = (R)in.h; hm = (R)(inner ? hb : in.h); hp = (R)(infr ? hn : in.h);
+  }
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     Pp[v] = __shfl_up_sync(full, P[v], 1);
     const R g = inner ? Ar<R>::div(P[v] - Pp[v], dxR, rdx) : R(0);
     const R gr = __shfl_down_sync(full, g, 1);
-    G[v] = limited_one<R>(lim, g, gr);
+    if constexpr (GL) {
+      const R Pn = __shfl_down_sync(full, P[v], 1);
+      G[v] = flux_limiter_g<R>(lim, gr, g, P[v], infr ? Pn : P[v], inner ? Pp[v] : P[v], h0, hp, hm);
+    } else {
+      G[v] = limited_one<R>(lim, g, gr);
+    }
   }
   const bool back = in.u * dx > 0.0;
   const R dot_xf = (R)(back ? in.db : in.df);
@@ -108,7 +122,7 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
 }
 
 // K-environment cell sweep along x (lanes along the rows).
-template <int K, bool FIRST, typename R>
+template <int K, bool FIRST, typename R, bool GL = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -129,12 +143,13 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
 #pragma unroll
   for (int v = 0; v < NV; ++v) in.U[v] = 0.;
   in.xc[0] = in.xc[1] = in.xc[2] = 0.;
-  in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = 0.; in.den = 0.;
+  in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = 0.; in.den = 0.; in.h = 0.;
   if (valid) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) in.U[v] = Uin[v * C + c];
     in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
     if (FIRST) in.den = Vlag[c];
+    if constexpr (GL) in.h = fd.h[c];
   }
   if (inner) {
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
@@ -142,7 +157,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
   }
   if (upd) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }
   double out[NV + K];
-  cell_line_env<K, FIRST, R>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R, GL>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (!upd) return;
 #pragma unroll
   for (int v = 0; v < NV; ++v) Uout[v * C + c] = out[v];
@@ -157,7 +172,7 @@ template <int K, bool FIRST>
 __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
 
 // W: lines per block (8 or 16, the tuning; the register budget stays 128).
-template <int K, int D, bool FIRST, typename R, int W = kLineWarps>
+template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false>
 __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_sweep_cells_t(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -214,10 +229,15 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
   in.n[0] = row[AN * kTileArr]; in.n[1] = row[(AN + 1) * kTileArr]; in.n[2] = row[(AN + 2) * kTileArr];
   in.ob = row[AO * kTileArr]; in.of = row[(AO + 1) * kTileArr];
   in.den = FIRST ? row[AD * kTileArr] : 0.;
+  in.h = 0.;
+  if (GL && valid) {                                   // own width only: read directly
+    const int ci = i0 + w;
+    in.h = fd.h[D * C + (D == 1 ? ci + dm.nx * (s + dm.ny * o) : ci + dm.nx * (o + dm.ny * s))];
+  }
   constexpr int NO = NV + K;
   static_assert(NO <= NA, "outputs reuse the staged rows");
   double out[NO];
-  cell_line_env<K, FIRST, R>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R, GL>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (upd) {
 #pragma unroll
     for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];
@@ -446,13 +466,16 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-template <int K, int D, bool FIRST, typename R, int W>
+// the generalised limiters (FP64): the cell sweeps' GL kernels
+static bool env_gl(const CycleArgs& a) { return a.ph.ordre_projection > 1 && a.ph.lim_cell >= 3; }
+
+template <int K, int D, bool FIRST, typename R, int W, bool GL = false>
 static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
   const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<W>::arr * sizeof(double);
-  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W>;
+  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W, GL>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
 }
@@ -460,6 +483,9 @@ static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uo
 // lines per block of this sweep: the tuning's (8 or 16)
 template <int K, int D, bool FIRST, typename R>
 static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
+  if constexpr (sizeof(R) == 8) {
+    if (env_gl(a)) { env_cells_staged_w<K, D, FIRST, R, kLineWarps, true>(a, Uin, Uout, s); return; }
+  }
   if (a.lines[BK_CELLS_X + D] == 16) env_cells_staged_w<K, D, FIRST, R, 16>(a, Uin, Uout, s);
   else env_cells_staged_w<K, D, FIRST, R, kLineWarps>(a, Uin, Uout, s);
 }
@@ -470,8 +496,10 @@ static void env_cells(const CycleArgs& a, int d, const double* Uin, double* Uout
   if (d == 0) {
     const int nseg = (dm.nx + kLineUpd - 1) / kLineUpd;
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
-    k_env_sweep_cells_x<K, FIRST, R><<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin,
-                                                                   Uout, a.dpf, a.Vlag);
+    auto kern = k_env_sweep_cells_x<K, FIRST, R>;
+    if constexpr (sizeof(R) == 8)
+      if (env_gl(a)) kern = k_env_sweep_cells_x<K, FIRST, R, true>;
+    kern<<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
   } else if (d == 1) {
     env_cells_staged<K, 1, FIRST, R>(a, Uin, Uout, s);
   } else {
@@ -510,6 +538,12 @@ static void set_env_attributes_r() {
   cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  if constexpr (sizeof(R) == 8) {
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, true, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  }
 }
 
 template <int K>
@@ -518,23 +552,27 @@ static void set_env_attributes() {
   set_env_attributes_r<K, float>();
 }
 
+template <int K, typename R>
+static void lagrange_cells_env(const CycleArgs& a, const dim3 nbc, int linear, cudaStream_t s) {
+  auto kern = k_cyc_lagrange_cells<K, R>;
+  if constexpr (sizeof(R) == 8)
+    if (a.fd.h) kern = k_cyc_lagrange_cells<K, R, true>;   // cell widths: the generalised limiters
+  kern<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs, a.st.mass,
+                           a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, linear);
+}
+
 void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
-#define MHY_LAG_ENV(KK, RR)                                                                                     \
-  k_cyc_lagrange_cells<KK, RR><<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e,     \
-                                                       a.st.q, a.st.p, a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L,  \
-                                                       a.U[0], a.xc, a.fd, a.env, a.Vlag, linear)
   if (a.ph.precision) {
-    if (a.K == 2) MHY_LAG_ENV(2, float);
-    else if (a.K == 3) MHY_LAG_ENV(3, float);
-    else MHY_LAG_ENV(4, float);
+    if (a.K == 2) lagrange_cells_env<2, float>(a, nbc, linear, s);
+    else if (a.K == 3) lagrange_cells_env<3, float>(a, nbc, linear, s);
+    else lagrange_cells_env<4, float>(a, nbc, linear, s);
   } else {
-    if (a.K == 2) MHY_LAG_ENV(2, double);
-    else if (a.K == 3) MHY_LAG_ENV(3, double);
-    else MHY_LAG_ENV(4, double);
+    if (a.K == 2) lagrange_cells_env<2, double>(a, nbc, linear, s);
+    else if (a.K == 3) lagrange_cells_env<3, double>(a, nbc, linear, s);
+    else lagrange_cells_env<4, double>(a, nbc, linear, s);
   }
-#undef MHY_LAG_ENV
 }
 
 void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {

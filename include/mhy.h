@@ -69,7 +69,8 @@ typedef struct mhy_options {
   int32_t ordre_projection;          /* 2 (1, 2, and 3 for one environment in FP64: Remap-ordre-3.cc) */
   int32_t projection_limiteur_id;    /* 0 minmod, 1 superBee, 2 vanLeer; the generalised limiters for uneven
                                         widths 3 minmodG, 4 superBeeG, 5 vanLeerG, 6 arithmeticG, 7 ultrabeeG
-                                        (UtilesRemap.cc:127-175; one environment, FP64, >= 3 cells a direction) */
+                                        (UtilesRemap.cc:127-175; FP64, one to four environments, >= 3 cells a
+                                        direction) */
   int32_t nb_bc;
   mhy_bc bc[MHY_MAX_BC];             /* default: walls on the six planes */
   int32_t nb_env;                    /* number of environments (one ideal gas each; 1..4 on the device) */
