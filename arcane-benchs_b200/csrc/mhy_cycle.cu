@@ -138,15 +138,18 @@ __global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __re
 
 
 // Cell sweep along x: lanes run along the rows, loads and stores as they are.
-template <bool LAST, typename R, bool O3 = false, bool GL = false, bool PB = false>
-__device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
-    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
-    double* __restrict__ dpf, CellState st,
-    int bx_, int by_, int bz_) {
+// cells_x_line is one lane's loads and line step.  The body runs it with
+// speculative FP64 quotients (not in the pente-borne form, whose quotients
+// stay exact); in a warp where any lane's were out of range it recomputes
+// the segment exactly out of line (cells_x_line_exact reloads the inputs, so
+// that none of them stays live across the common path), then stores.
+template <bool LAST, typename R, bool O3, bool GL, bool PB, bool SP>
+__device__ __forceinline__ void cells_x_line(const Dims& dm, const Scalars* __restrict__ S, const Phys& ph,
+    const FaceData& fd, const double* __restrict__ n0, const double* __restrict__ xcs, const double* __restrict__ ofn,
+    const double* __restrict__ Uin, const double* __restrict__ Ve, int bx_, int by_, int bz_, double* out,
+    unsigned* oor) {
   const int lane = threadIdx.x & 31;
   const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
-  if (j >= dm.ny) return;                              // whole warp leaves together
   const int nd = dm.nx, C = (int)dm.C, F = (int)dm.F;
   const int s = bx_ * kLineUpd - 2 + lane;      // position of this lane's cell along x
   const bool valid = s >= 0 && s < nd;
@@ -179,10 +182,46 @@ __device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars*
   }
   if (upd) {
     in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c];
-    if (LAST) in.vol = st.Ve[c];
+    if (LAST) in.vol = Ve[c];
   }
-  double out[LAST ? kCellOutLast : kCellOutMid];
-  cell_line<LAST, R, O3, GL, PB>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  cell_line<LAST, R, O3, GL, PB, SP>(ph, S->dt, S, valid, inner, infr, upd, in, out, oor);
+}
+
+template <bool LAST, typename R, bool O3, bool GL, bool PB>
+__device__ __noinline__ LineOut<LAST ? kCellOutLast : kCellOutMid> cells_x_line_exact(Dims dm, const Scalars* S,
+    Phys ph, FaceData fd, const double* n0, const double* xcs, const double* ofn, const double* Uin, const double* Ve,
+    int bx_, int by_, int bz_) {
+  LineOut<LAST ? kCellOutLast : kCellOutMid> o;
+  cells_x_line<LAST, R, O3, GL, PB, false>(dm, S, ph, fd, n0, xcs, ofn, Uin, Ve, bx_, by_, bz_, o.v, nullptr);
+  return o;
+}
+
+template <bool LAST, typename R, bool O3 = false, bool GL = false, bool PB = false>
+__device__ __forceinline__ void k_cyc_sweep_cells_x_body(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, FaceData fd, const double* __restrict__ n0, const double* __restrict__ xcs,
+    const double* __restrict__ ofn, const double* __restrict__ Uin, double* __restrict__ Uout,
+    double* __restrict__ dpf, CellState st,
+    int bx_, int by_, int bz_) {
+  constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
+  const int lane = threadIdx.x & 31;
+  const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
+  if (j >= dm.ny) return;                              // whole warp leaves together
+  double out[NO];
+  if constexpr (sizeof(R) == 8 && !PB) {
+    unsigned oor = 0u;
+    cells_x_line<LAST, R, O3, GL, PB, true>(dm, S, ph, fd, n0, xcs, ofn, Uin, st.Ve, bx_, by_, bz_, out, &oor);
+    if (__any_sync(0xffffffffu, oor != 0u)) {
+      const auto o = cells_x_line_exact<LAST, R, O3, GL, PB>(dm, S, ph, fd, n0, xcs, ofn, Uin, st.Ve, bx_, by_, bz_);
+#pragma unroll
+      for (int a = 0; a < NO; ++a) out[a] = o.v[a];
+    }
+  } else {
+    cells_x_line<LAST, R, O3, GL, PB, false>(dm, S, ph, fd, n0, xcs, ofn, Uin, st.Ve, bx_, by_, bz_, out, nullptr);
+  }
+  const int nd = dm.nx, C = (int)dm.C;
+  const int s = bx_ * kLineUpd - 2 + lane;
+  const bool upd = s >= 0 && s < nd && lane >= 2 && lane < 2 + kLineUpd;
+  const int c = s + dm.nx * (j + dm.ny * k);
   if (!upd) return;
   if (!LAST) {
 #pragma unroll
@@ -213,6 +252,59 @@ struct CellTileSize {
   static constexpr int NA = NB + (O3 ? 4 : 0);        // + the order-3 face values
   static constexpr size_t bytes = (size_t)NA * TileGeom<W>::arr * sizeof(double);
 };
+
+// One lane's line step of a cell y/z sweep, from the staged tile (each warp
+// reads only its own tile row, which no other warp writes).
+template <int D, bool LAST, typename R, int W, bool O3, bool GL, bool PB, bool SP>
+__device__ __forceinline__ void cells_t_line(const Dims& dm, const Scalars* __restrict__ S, const Phys& ph,
+    const FaceData& fd, int bx_, int by_, int bz_, double* out, unsigned* oor) {
+  constexpr int NB = CellTileSize<LAST, W, O3>::NB;
+  constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
+  extern __shared__ double smem_dyn[];
+  const double* tile = smem_dyn;                      // [NA][W][ld]
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = bx_ * W, seg0 = by_ * kLineUpd - 2, o = bz_;
+  const int nd = dm.ncd(D), C = (int)dm.C;
+  // line w, position lane
+  const int s = seg0 + lane;
+  const bool line_ok = i0 + w < dm.nx;
+  const bool valid = line_ok && s >= 0 && s < nd;
+  const bool inner = line_ok && s >= 1 && s <= nd - 1;
+  const bool infr = s + 1 <= nd - 1;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  const double* row = tile + w * kTileLd + lane;
+  CellIn in;
+  in.U[0] = row[0]; in.U[1] = row[kTileArr]; in.U[2] = row[2 * kTileArr]; in.U[3] = row[3 * kTileArr];
+  in.xc[0] = row[4 * kTileArr]; in.xc[1] = row[5 * kTileArr]; in.xc[2] = row[6 * kTileArr];
+  in.db = row[7 * kTileArr]; in.df = row[8 * kTileArr]; in.u = row[9 * kTileArr]; in.A = row[10 * kTileArr];
+  in.n[0] = row[11 * kTileArr]; in.n[1] = row[12 * kTileArr]; in.n[2] = row[13 * kTileArr];
+  in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
+  in.vol = LAST ? row[(NB - 1) * kTileArr] : 0.;
+  in.h = 0.;
+  in.pb[0] = in.pb[1] = in.pb[2] = 0.;
+  if ((GL || PB) && valid) {
+    const int i = i0 + w;
+    const int c = D == 1 ? i + dm.nx * (s + dm.ny * o) : i + dm.nx * (o + dm.ny * s);
+    in.h = fd.h[D * C + c];
+    if constexpr (PB) {
+      if (ph.pb_first) { in.pb[0] = fd.pbphi[c]; in.pb[1] = fd.pbphi[C + c]; }
+      in.pb[2] = fd.pbphi[2 * C + c];
+    }
+  }
+  if constexpr (O3) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) in.pf3[a] = row[(NB + a) * kTileArr];
+  }
+  cell_line<LAST, R, O3, GL, PB, SP>(ph, S->dt, S, valid, inner, infr, upd, in, out, oor);
+}
+
+template <int D, bool LAST, typename R, int W, bool O3, bool GL, bool PB>
+__device__ __noinline__ LineOut<LAST ? kCellOutLast : kCellOutMid> cells_t_line_exact(Dims dm, const Scalars* S,
+    Phys ph, FaceData fd, int bx_, int by_, int bz_) {
+  LineOut<LAST ? kCellOutLast : kCellOutMid> o;
+  cells_t_line<D, LAST, R, W, O3, GL, PB, false>(dm, S, ph, fd, bx_, by_, bz_, o.v, nullptr);
+  return o;
+}
 
 template <int D, bool LAST, typename R, int W, bool O3 = false, bool GL = false, bool PB = false>
 __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars* __restrict__ S,
@@ -260,39 +352,22 @@ __device__ __forceinline__ void k_cyc_sweep_cells_t_body(Dims dm, const Scalars*
     for (int a = 0; a < NA; ++a) tile[a * kTileArr + sx * kTileLd + sp] = v[a];
   }
   __syncthreads();
-  // line w, position lane
-  const int s = seg0 + lane;
-  const bool line_ok = i0 + w < dm.nx;
-  const bool valid = line_ok && s >= 0 && s < nd;
-  const bool inner = line_ok && s >= 1 && s <= nd - 1;
-  const bool infr = s + 1 <= nd - 1;
-  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
-  double* row = tile + w * kTileLd + lane;
-  CellIn in;
-  in.U[0] = row[0]; in.U[1] = row[kTileArr]; in.U[2] = row[2 * kTileArr]; in.U[3] = row[3 * kTileArr];
-  in.xc[0] = row[4 * kTileArr]; in.xc[1] = row[5 * kTileArr]; in.xc[2] = row[6 * kTileArr];
-  in.db = row[7 * kTileArr]; in.df = row[8 * kTileArr]; in.u = row[9 * kTileArr]; in.A = row[10 * kTileArr];
-  in.n[0] = row[11 * kTileArr]; in.n[1] = row[12 * kTileArr]; in.n[2] = row[13 * kTileArr];
-  in.ob = row[14 * kTileArr]; in.of = row[15 * kTileArr];
-  in.vol = LAST ? row[(NB - 1) * kTileArr] : 0.;
-  in.h = 0.;
-  in.pb[0] = in.pb[1] = in.pb[2] = 0.;
-  if ((GL || PB) && valid) {
-    const int i = i0 + w;
-    const int c = D == 1 ? i + dm.nx * (s + dm.ny * o) : i + dm.nx * (o + dm.ny * s);
-    in.h = fd.h[D * C + c];
-    if constexpr (PB) {
-      if (ph.pb_first) { in.pb[0] = fd.pbphi[c]; in.pb[1] = fd.pbphi[C + c]; }
-      in.pb[2] = fd.pbphi[2 * C + c];
-    }
-  }
-  if constexpr (O3) {
-#pragma unroll
-    for (int a = 0; a < 4; ++a) in.pf3[a] = row[(NB + a) * kTileArr];
-  }
   constexpr int NO = LAST ? kCellOutLast : kCellOutMid;
   double out[NO];
-  cell_line<LAST, R, O3, GL, PB>(ph, S->dt, S, valid, inner, infr, upd, in, out);
+  if constexpr (sizeof(R) == 8 && !PB) {
+    unsigned oor = 0u;
+    cells_t_line<D, LAST, R, W, O3, GL, PB, true>(dm, S, ph, fd, bx_, by_, bz_, out, &oor);
+    if (__any_sync(0xffffffffu, oor != 0u)) {
+      const auto o2 = cells_t_line_exact<D, LAST, R, W, O3, GL, PB>(dm, S, ph, fd, bx_, by_, bz_);
+#pragma unroll
+      for (int a = 0; a < NO; ++a) out[a] = o2.v[a];
+    }
+  } else {
+    cells_t_line<D, LAST, R, W, O3, GL, PB, false>(dm, S, ph, fd, bx_, by_, bz_, out, nullptr);
+  }
+  const int s = seg0 + lane;
+  const bool upd = i0 + w < dm.nx && s >= 0 && s < nd && lane >= 2 && lane < 2 + kLineUpd;
+  double* row = tile + w * kTileLd + lane;
   // each lane overwrites only the tile column it read itself
   if (upd) {
 #pragma unroll

@@ -61,8 +61,9 @@ template <int W> struct TileGeom {
 // EOS (RemapADIFinal.cc:446-643, PerfectGasEOSService.cc:92-106, with
 // PrepareRemap.cc:553-559).  out = rho, e, q, mass, p, c, -, mass fraction
 // (0 when the cell was zeroed; conservation-energie-totale scales by it).
+template <bool SP = false>
 __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, double vol, const double u[4],
-                                              double out[8]) {
+                                              double out[8], unsigned* oor = nullptr) {
   const double thr = ph.threshold;
   const double U0 = u[0], U1 = u[1], U2 = u[2], U3 = u[3];
   const double volt = 0. + U0, masset = 0. + U1;
@@ -88,7 +89,7 @@ __device__ __forceinline__ void finalize_cell(const Phys& ph, const Scalars* S, 
   const double density_nplus1 = 0. + fvol * de;
   const double cm = vol * density_nplus1;
   double ee = 0.;
-  if (fvol > thr && U1 != 0.) ee = qdiv(U2, U1, 1. / masset);   // masset = 0 + U1 = U1
+  if (fvol > thr && U1 != 0.) ee = dv<double, SP>(U2, U1, 1. / masset, oor);   // masset = 0 + U1 = U1
   double energie = 0. + mf * ee;
   const double pv = U3 * unsurvol;
   const double pseudo = 0. + fvol * pv;
@@ -138,20 +139,23 @@ __device__ __forceinline__ void finalize_cell_mixed(const Phys& ph, const Scalar
 
 // Phi = U / sum of the environment volumes = U / U0 for one environment
 // (RemapADIService.cc:962-970, PrepareRemap.cc:394-398); Phi0 = U0/U0 = 1.
-template <typename R>
-__device__ __forceinline__ void phi_of(const double U[4], R P[4]) {
+template <typename R, bool SP = false>
+__device__ __forceinline__ void phi_of(const double U[4], R P[4], unsigned* oor = nullptr) {
   const R U0 = (R)U[0], r = Ar<R>::rcp(U0);
   P[0] = 1;
-  P[1] = Ar<R>::div((R)U[1], U0, r); P[2] = Ar<R>::div((R)U[2], U0, r); P[3] = Ar<R>::div((R)U[3], U0, r);
+  P[1] = dv<R, SP>((R)U[1], U0, r, oor); P[2] = dv<R, SP>((R)U[2], U0, r, oor); P[3] = dv<R, SP>((R)U[3], U0, r, oor);
 }
 
 // Face gradients (R:174-177) of variables 1..3; variable 0 is zero.
-template <typename R>
-__device__ __forceinline__ void face_grad(bool inner, R dx, const R Pn[4], const R Pp[4], R g[4]) {
+template <typename R, bool SP = false>
+__device__ __forceinline__ void face_grad(bool inner, R dx, const R Pn[4], const R Pp[4], R g[4], unsigned* oor = nullptr) {
   g[0] = 0;
   const R r = inner ? Ar<R>::rcp(dx) : R(0);
+  unsigned fo = 0u;
 #pragma unroll
-  for (int v = 1; v < 4; ++v) g[v] = inner ? Ar<R>::div(Pn[v] - Pp[v], dx, r) : R(0);
+  for (int v = 1; v < 4; ++v) g[v] = inner ? dv<R, SP>(Pn[v] - Pp[v], dx, r, &fo) : R(0);
+  // lane 0's back neighbour is itself (0 / 0): its gradient reaches no updated cell
+  if constexpr (SP) { if ((threadIdx.x & 31) != 0) *oor |= fo; }
 }
 
 // Limited cell gradient from the back and front face gradients (R:497-506):
@@ -324,9 +328,9 @@ constexpr int kCellOutMid = 5;    // U0..U3, dual mass flux
 // PrepareRemap.cc:201-212 (first sweep) or RemapADIService.cc:805-834, the
 // general gradient (R:319-378), face values from the fluxes leaving the two
 // cells (R:380-431, 574-578) and fluxes o*A*Phi_f (R:770-774).
-template <bool LAST, typename R = double, bool O3 = false, bool GL = false, bool PB = false>
+template <bool LAST, typename R = double, bool O3 = false, bool GL = false, bool PB = false, bool SP = false>
 __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scalars* S, bool valid, bool inner,
-                                          bool infr, bool upd, const CellIn& in, double* out) {
+                                          bool infr, bool upd, const CellIn& in, double* out, unsigned* oor = nullptr) {
   const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
   R P[4] = {0, 0, 0, 0};
@@ -342,7 +346,7 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
       P[3] = in.pb[2];
     }
   } else {
-    if (valid) phi_of<R>(in.U, P);
+    if (valid) phi_of<R, SP>(in.U, P, oor);
   }
   const unsigned full = 0xffffffffu;
   const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
@@ -359,7 +363,7 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
 #pragma unroll
     for (int v = 0; v < 4; ++v) g[v] = inner ? Ar<R>::div(P[v] - Pp[v], (R)dx, r) : R(0);
   } else {
-    face_grad<R>(inner, (R)dx, P, Pp, g);
+    face_grad<R, SP>(inner, (R)dx, P, Pp, g, oor);
   }
 #pragma unroll
   for (int v = 0; v < 4; ++v) gr[v] = __shfl_down_sync(full, g[v], 1);
@@ -443,7 +447,7 @@ __device__ __forceinline__ void cell_line(const Phys& ph, double dt, const Scala
     out[4] = dpm;
   } else {
     if constexpr (sizeof(R) == 4) finalize_cell_mixed(ph, S, in.vol, u, out);
-    else finalize_cell(ph, S, in.vol, u, out);
+    else finalize_cell<SP>(ph, S, in.vol, u, out, oor);
     out[6] = dpm;
   }
 }
@@ -522,10 +526,10 @@ constexpr int kNodeOutLast = 6;   // the last sweep adds the node's conservation
 // start of a sweep is PrepareRemap.cc:411-433 on the first sweep or for nodes
 // not yet updated this cycle, else U_dual / m.  G holds the node's stale
 // gradient on entry and its gradient on return.
-template <int D, bool FIRST, bool LAST, typename R = double, bool GL = false>
+template <int D, bool FIRST, bool LAST, typename R = double, bool GL = false, bool SP = false>
 __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid, bool inner, bool updated,
                                           bool upd, const NodeIn& in, R G[3], double* out, bool xabs = false,
-                                          bool bb_ok = true, bool ff_ok = true) {
+                                          bool bb_ok = true, bool ff_ok = true, unsigned* oor = nullptr) {
   const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.limiteur_id : -1;
   const bool grad_on = ph.ordre_projection > 1;
@@ -543,8 +547,8 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
       for (int c = 0; c < 5; ++c) ud[c] = in.ud[c];
       if (updated) {
         const R m = (R)ud[3], rm = Ar<R>::rcp(m);
-        P[0] = Ar<R>::div((R)ud[0], m, rm); P[1] = Ar<R>::div((R)ud[1], m, rm);
-        P[2] = Ar<R>::div((R)ud[2], m, rm); P[3] = Ar<R>::div((R)ud[4], m, rm);
+        P[0] = dv<R, SP>((R)ud[0], m, rm, oor); P[1] = dv<R, SP>((R)ud[1], m, rm, oor);
+        P[2] = dv<R, SP>((R)ud[2], m, rm, oor); P[3] = dv<R, SP>((R)ud[4], m, rm, oor);
       } else {
         P[0] = (R)u.x; P[1] = (R)u.y; P[2] = (R)u.z; P[3] = (R)(0.5 * norm2(u));
       }
@@ -560,8 +564,15 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
     // front difference quotient of this node = back difference quotient of the next
     const R hf = (R)(xp - x), rf = Ar<R>::rcp(hf);
     R gf[3], gb[3];
+    // speculative quotients count only where they are used: a valid node
+    // whose next node is valid and in this warp (the last lane divides by 0)
+    unsigned gfo = 0u;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) gf[c] = Ar<R>::div(Pp[c] - P[c], hf, rf);
+    for (int c = 0; c < 3; ++c) gf[c] = dv<R, SP>(Pp[c] - P[c], hf, rf, &gfo);
+    if constexpr (SP) {
+      const int next_valid = __shfl_down_sync(full, valid ? 1 : 0, 1);   // every lane takes part
+      if (valid && (threadIdx.x & 31) < 31 && next_valid != 0) *oor |= gfo;
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) gb[c] = __shfl_up_sync(full, gf[c], 1);
     if constexpr (GL) {
@@ -602,7 +613,7 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
     double rm = 0.;
     if (m != 0.) {
       rm = 1.0 / m;
-      u = d3(qdiv(ud[0], m, rm), qdiv(ud[1], m, rm), qdiv(ud[2], m, rm));
+      u = d3(dv<double, SP>(ud[0], m, rm, oor), dv<double, SP>(ud[1], m, rm, oor), dv<double, SP>(ud[2], m, rm, oor));
     } else {
       u = d3(in.vh[0], in.vh[1], in.vh[2]);
     }
@@ -612,9 +623,13 @@ __device__ __forceinline__ void node_line(const Phys& ph, double dt, bool valid,
     // ec_proj = U_dual[4] / U_dual[3], ec_reconst = 0.5 |v|^2; nothing for a
     // node of zero mass
     if (ph.cons_ec)
-      out[5] = m != 0. ? 0.25 * (qdiv(ud[4], m, rm) - 0.5 * (u.x * u.x + u.y * u.y + u.z * u.z)) : 0.;
+      out[5] = m != 0. ? 0.25 * (dv<double, SP>(ud[4], m, rm, oor) - 0.5 * (u.x * u.x + u.y * u.y + u.z * u.z)) : 0.;
   }
 }
+
+// Outputs of one lane's line step, as the sweeps' exact recomputations return them.
+template <int NO> struct LineOut { double v[NO]; };
+struct NodeLineOut { double v[kNodeOutLast]; double g[3]; };
 
 // inner along an earlier direction of this cycle: Phi_dual = U_dual / m there
 __device__ __forceinline__ bool node_updated(const Dims& dm, int D, int prev_inner, const int idx[3]) {
@@ -632,17 +647,19 @@ __device__ __forceinline__ bool node_on_plane(const Dims& dm, int D, const int i
          (D != 2 && (idx[2] == 0 || idx[2] == dm.nz));
 }
 
-// Node sweep along x: lanes run along the rows of nodes.
-template <bool FIRST, bool LAST, int K, typename R, bool GL = false>
-__device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars* __restrict__ S,
-    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
-    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
-    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
-    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
-    int bx_, int by_, int bz_, double* __restrict__ ecn = nullptr) {
+// Node sweep along x: lanes run along the rows of nodes.  nodes_x_line is one
+// lane's loads and line step.  The body runs it with speculative FP64
+// quotients; in a warp where any lane's were out of range it recomputes the
+// segment exactly out of line (nodes_x_line_exact reloads the inputs, so
+// that none of them stays live across the common path), then stores.
+template <bool FIRST, bool LAST, int K, typename R, bool GL, bool SP>
+__device__ __forceinline__ void nodes_x_line(const Dims& dm, const Scalars* __restrict__ S, const Phys& ph,
+    int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, const double* __restrict__ dpf,
+    const double* __restrict__ Gd, const double* __restrict__ mass, int bx_, int by_, int bz_, R G[3], double* out,
+    unsigned* oor) {
   const int lane = threadIdx.x & 31;
   const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
-  if (j > dm.ny) return;                               // whole warp leaves together
   const int nx = dm.nx, ny = dm.ny, nz = dm.nz, N = (int)dm.N;
   const int m = bx_ * kLineUpd - 2 + lane;      // position of this lane's node along x
   const bool valid = m >= 0 && m <= nx;
@@ -656,7 +673,7 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
   in.vh[0] = in.vh[1] = in.vh[2] = 0.; in.x0d = 0.; in.nm = 0.;
   in.ud[0] = in.ud[1] = in.ud[2] = in.ud[3] = in.ud[4] = 0.; in.ffm = 0.; in.msum = 0.;
   in.x2[0] = in.x2[1] = 0.;
-  R G[3] = {0, 0, 0};
+  G[0] = G[1] = G[2] = R(0);
   if (GL && valid && (lane == 1 || lane == 30)) {
     const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
     if (q >= 0 && q <= nx) {
@@ -705,9 +722,56 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars*
       in.msum = sm;
     }
   }
+  node_line<0, FIRST, LAST, R, GL, SP>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
+                                       m + 2 <= nx, oor);
+}
+
+template <bool FIRST, bool LAST, int K, typename R, bool GL>
+__device__ __noinline__ NodeLineOut nodes_x_line_exact(Dims dm, const Scalars* S, Phys ph, int prev_inner,
+    const double* x0, const double* xl, const double* vh, const double* nm_in, const double* udin, const double* dpf,
+    const double* Gd, const double* mass, int bx_, int by_, int bz_) {
+  NodeLineOut o;
+  R G[3];
+  nodes_x_line<FIRST, LAST, K, R, GL, false>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, dpf, Gd, mass, bx_, by_,
+                                             bz_, G, o.v, nullptr);
+  o.g[0] = (double)G[0]; o.g[1] = (double)G[1]; o.g[2] = (double)G[2];
+  return o;
+}
+
+template <bool FIRST, bool LAST, int K, typename R, bool GL = false>
+__device__ __forceinline__ void k_cyc_sweep_nodes_x_body(Dims dm, const Scalars* __restrict__ S,
+    Phys ph, int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
+    const double* __restrict__ nm_in, const double* __restrict__ udin, double* __restrict__ udout,
+    const double* __restrict__ dpf, double* __restrict__ Gd, const double* __restrict__ mass,
+    double* __restrict__ vout, double* __restrict__ nm_out, double* __restrict__ vnorm,
+    int bx_, int by_, int bz_, double* __restrict__ ecn = nullptr) {
+  const int lane = threadIdx.x & 31;
+  const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
+  if (j > dm.ny) return;                               // whole warp leaves together
+  R G[3];
   double out[LAST ? kNodeOutLast : kNodeOut];
-  node_line<0, FIRST, LAST, R, GL>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
-                                   m + 2 <= nx);
+  if constexpr (sizeof(R) == 8) {
+    unsigned oor = 0u;
+    nodes_x_line<FIRST, LAST, K, R, GL, true>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, dpf, Gd, mass, bx_, by_,
+                                              bz_, G, out, &oor);
+    if (__any_sync(0xffffffffu, oor != 0u)) {
+      const NodeLineOut o = nodes_x_line_exact<FIRST, LAST, K, R, GL>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin,
+                                                                      dpf, Gd, mass, bx_, by_, bz_);
+#pragma unroll
+      for (int c = 0; c < (LAST ? kNodeOutLast : kNodeOut); ++c) out[c] = o.v[c];
+      G[0] = o.g[0]; G[1] = o.g[1]; G[2] = o.g[2];
+    }
+  } else {
+    nodes_x_line<FIRST, LAST, K, R, GL, false>(dm, S, ph, prev_inner, x0, xl, vh, nm_in, udin, dpf, Gd, mass, bx_, by_,
+                                               bz_, G, out, nullptr);
+  }
+  const int nx = dm.nx, ny = dm.ny, N = (int)dm.N;
+  const int m = bx_ * kLineUpd - 2 + lane;
+  const bool upd = m >= 0 && m <= nx && lane >= 2 && lane < 2 + kLineUpd;
+  const bool inner = m >= 1 && m <= nx - 1;
+  const bool grad_on = ph.ordre_projection > 1;
+  const int idx[3] = {m, j, k};
+  const int n = m + (nx + 1) * (j + (ny + 1) * k);
   if (!upd) return;
   if (inner && grad_on && node_on_plane(dm, 0, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
   if (!LAST) {
@@ -742,6 +806,100 @@ struct NodeTileSize {
   static constexpr int CT = 2 * (W + 1) * TileGeom<W>::cld;  // elements of one cell tile
   static constexpr size_t bytes = (size_t)(NA * TileGeom<W>::arr + NT * CT) * sizeof(double);
 };
+
+// One lane's line step of a node y/z sweep, from the staged tiles (each warp
+// reads only its own tile row and the cell tiles, which no warp writes
+// before the stores at the end of the body).
+template <int D, bool FIRST, bool LAST, int K, typename R, int W, bool GL, bool SP>
+__device__ __forceinline__ void nodes_t_line(const Dims& dm, const Scalars* __restrict__ S, const Phys& ph,
+    int prev_inner, const double* __restrict__ x0, const double* __restrict__ xl, const double* __restrict__ vh,
+    const double* __restrict__ Gd, int bx_, int by_, int bz_, R G[3], double* out, unsigned* oor) {
+  using TS = NodeTileSize<D, FIRST, LAST, K, W>;
+  constexpr int NA = TS::NA, CT = TS::CT;
+  constexpr int CLd = TileGeom<W>::cld;               // row length of a cell tile
+  constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
+  extern __shared__ double smem_dyn[];
+  const double* tile = smem_dyn;                      // [NA][W][ld]
+  const double* ctile = smem_dyn + NA * kTileArr;     // [NT][2][W + 1][cld]
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = bx_ * W, seg0 = by_ * kLineUpd - 2, o = bz_;
+  const int nx = dm.nx, ny = dm.ny, N = (int)dm.N;
+  const int nn = dm.ncd(D) + 1;                       // nodes along D
+  auto node_id = [&](int i, int m) { return D == 1 ? i + (nx + 1) * (m + (ny + 1) * o) : i + (nx + 1) * (o + (ny + 1) * m); };
+  const int m = seg0 + lane;
+  const int i = i0 + w;
+  const bool valid = i <= nx && m >= 0 && m < nn;
+  const bool inner = i <= nx && m >= 1 && m <= nn - 2;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  int idx[3];
+  idx[0] = i; idx[D] = m; idx[3 - D] = o;               // D = 1: (i, m, o); D = 2: (i, o, m)
+  const bool updated = node_updated(dm, D, prev_inner, idx);
+  const bool grad_on = ph.ordre_projection > 1;
+  const double* row = tile + w * kTileLd + lane;
+  NodeIn in;
+  in.vh[0] = row[0]; in.vh[1] = row[kTileArr]; in.vh[2] = row[2 * kTileArr]; in.x0d = row[3 * kTileArr];
+  in.nm = FIRST ? row[4 * kTileArr] : 0.;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) in.ud[c] = FIRST ? 0. : row[(4 + c) * kTileArr];
+  // cells in front of the node along D have index m along D; transverse
+  // (x - 1, x) = columns (w, w + 1) and (o - 1, o) = tile rows (0, 1)
+  const double* cr = ctile + w * CLd + lane;
+  constexpr int QS = (W + 1) * CLd;                   // stride between the two tile rows
+  // DualPhaseRemap.cc:299-340 order: s1 over d1 = (D+1)%3, s2 over d2 = (D+2)%3,
+  // environments innermost.  D = 1: s1 over z (q), s2 over x; D = 2: s1 over
+  // x, s2 over y (q).  Tile offsets of the cells (q, dx): q * QS + dx * CLd.
+  constexpr int o1 = D == 1 ? CLd : QS, o2 = D == 1 ? QS : CLd;
+  double f = 0.;
+#pragma unroll
+  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT];
+#pragma unroll
+  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT + o1];
+#pragma unroll
+  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT + o2];
+#pragma unroll
+  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT + QS + CLd];
+  in.ffm = (valid && m < nn - 1) ? f : 0.;
+  in.msum = 0.;
+  if (LAST) {
+    const double* mr = cr + K * CT;
+    const double a00 = mr[0], a01 = mr[CLd], a10 = mr[QS], a11 = mr[QS + CLd];   // cells at index m along D
+    const unsigned full = 0xffffffffu;
+    const double b00 = __shfl_up_sync(full, a00, 1), b01 = __shfl_up_sync(full, a01, 1),
+                 b10 = __shfl_up_sync(full, a10, 1), b11 = __shfl_up_sync(full, a11, 1);   // index m - 1
+    // increasing cell id: z outer, y, x inner
+    double sm = 0.;
+    if (D == 1) {   // (x, y=m-1|m, z=o-1|o): q = z
+      sm += b00; sm += b01; sm += a00; sm += a01; sm += b10; sm += b11; sm += a10; sm += a11;
+    } else {        // (x, y=o-1|o, z=m-1|m): q = y
+      sm += b00; sm += b01; sm += b10; sm += b11; sm += a00; sm += a01; sm += a10; sm += a11;
+    }
+    in.msum = sm;
+  }
+  in.x2[0] = in.x2[1] = 0.;
+  if (GL && valid && (lane == 1 || lane == 30)) {
+    const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
+    if (q >= 0 && q < nn) {
+      const int nq = node_id(i, q);
+      in.x2[lane == 1 ? 0 : 1] = xl ? xl[D * N + nq] : x0[D * N + nq] + vh[D * N + nq] * S->dt;
+    }
+  }
+  G[0] = G[1] = G[2] = R(0);
+  const int n = valid ? node_id(i, m) : 0;
+  if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
+  node_line<D, FIRST, LAST, R, GL, SP>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
+                                       m + 2 <= nn - 1, oor);
+}
+
+template <int D, bool FIRST, bool LAST, int K, typename R, int W, bool GL>
+__device__ __noinline__ NodeLineOut nodes_t_line_exact(Dims dm, const Scalars* S, Phys ph, int prev_inner,
+    const double* x0, const double* xl, const double* vh, const double* Gd, int bx_, int by_, int bz_) {
+  NodeLineOut o;
+  R G[3];
+  nodes_t_line<D, FIRST, LAST, K, R, W, GL, false>(dm, S, ph, prev_inner, x0, xl, vh, Gd, bx_, by_, bz_, G, o.v,
+                                                   nullptr);
+  o.g[0] = (double)G[0]; o.g[1] = (double)G[1]; o.g[2] = (double)G[2];
+  return o;
+}
 
 template <int D, bool FIRST, bool LAST, int K, typename R, int W = kLineWarps, bool GL = false>
 __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars* __restrict__ S,
@@ -794,6 +952,22 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
     }
   }
   __syncthreads();
+  R G[3];
+  double out[LAST ? kNodeOutLast : kNodeOut];
+  if constexpr (sizeof(R) == 8) {
+    unsigned oor = 0u;
+    nodes_t_line<D, FIRST, LAST, K, R, W, GL, true>(dm, S, ph, prev_inner, x0, xl, vh, Gd, bx_, by_, bz_, G, out, &oor);
+    if (__any_sync(0xffffffffu, oor != 0u)) {
+      const NodeLineOut o2 = nodes_t_line_exact<D, FIRST, LAST, K, R, W, GL>(dm, S, ph, prev_inner, x0, xl, vh, Gd,
+                                                                             bx_, by_, bz_);
+#pragma unroll
+      for (int c = 0; c < (LAST ? kNodeOutLast : kNodeOut); ++c) out[c] = o2.v[c];
+      G[0] = o2.g[0]; G[1] = o2.g[1]; G[2] = o2.g[2];
+    }
+  } else {
+    nodes_t_line<D, FIRST, LAST, K, R, W, GL, false>(dm, S, ph, prev_inner, x0, xl, vh, Gd, bx_, by_, bz_, G, out,
+                                                     nullptr);
+  }
   const int m = seg0 + lane;
   const int i = i0 + w;
   const bool valid = i <= nx && m >= 0 && m < nn;
@@ -801,62 +975,9 @@ __device__ __forceinline__ void k_cyc_sweep_nodes_t_body(Dims dm, const Scalars*
   const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
   int idx[3];
   idx[0] = i; idx[D] = m; idx[3 - D] = o;               // D = 1: (i, m, o); D = 2: (i, o, m)
-  const bool updated = node_updated(dm, D, prev_inner, idx);
   const bool grad_on = ph.ordre_projection > 1;
   double* row = tile + w * kTileLd + lane;
-  NodeIn in;
-  in.vh[0] = row[0]; in.vh[1] = row[kTileArr]; in.vh[2] = row[2 * kTileArr]; in.x0d = row[3 * kTileArr];
-  in.nm = FIRST ? row[4 * kTileArr] : 0.;
-#pragma unroll
-  for (int c = 0; c < 5; ++c) in.ud[c] = FIRST ? 0. : row[(4 + c) * kTileArr];
-  // cells in front of the node along D have index m along D; transverse
-  // (x - 1, x) = columns (w, w + 1) and (o - 1, o) = tile rows (0, 1)
-  const double* cr = ctile + w * CLd + lane;
-  constexpr int QS = (W + 1) * CLd;                   // stride between the two tile rows
-  // DualPhaseRemap.cc:299-340 order: s1 over d1 = (D+1)%3, s2 over d2 = (D+2)%3,
-  // environments innermost.  D = 1: s1 over z (q), s2 over x; D = 2: s1 over
-  // x, s2 over y (q).  Tile offsets of the cells (q, dx): q * QS + dx * CLd.
-  constexpr int o1 = D == 1 ? CLd : QS, o2 = D == 1 ? QS : CLd;
-  double f = 0.;
-#pragma unroll
-  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT];
-#pragma unroll
-  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT + o1];
-#pragma unroll
-  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT + o2];
-#pragma unroll
-  for (int e = 0; e < K; ++e) f += 0.25 * cr[e * CT + QS + CLd];
-  in.ffm = (valid && m < nn - 1) ? f : 0.;
-  in.msum = 0.;
-  if (LAST) {
-    const double* mr = cr + K * CT;
-    const double a00 = mr[0], a01 = mr[CLd], a10 = mr[QS], a11 = mr[QS + CLd];   // cells at index m along D
-    const unsigned full = 0xffffffffu;
-    const double b00 = __shfl_up_sync(full, a00, 1), b01 = __shfl_up_sync(full, a01, 1),
-                 b10 = __shfl_up_sync(full, a10, 1), b11 = __shfl_up_sync(full, a11, 1);   // index m - 1
-    // increasing cell id: z outer, y, x inner
-    double sm = 0.;
-    if (D == 1) {   // (x, y=m-1|m, z=o-1|o): q = z
-      sm += b00; sm += b01; sm += a00; sm += a01; sm += b10; sm += b11; sm += a10; sm += a11;
-    } else {        // (x, y=o-1|o, z=m-1|m): q = y
-      sm += b00; sm += b01; sm += b10; sm += b11; sm += a00; sm += a01; sm += a10; sm += a11;
-    }
-    in.msum = sm;
-  }
-  in.x2[0] = in.x2[1] = 0.;
-  if (GL && valid && (lane == 1 || lane == 30)) {
-    const int q = lane == 1 ? m - 2 : m + 2;           // the node two back (lane 1) or ahead (lane 30)
-    if (q >= 0 && q < nn) {
-      const int nq = node_id(i, q);
-      in.x2[lane == 1 ? 0 : 1] = xl ? xl[D * N + nq] : x0[D * N + nq] + vh[D * N + nq] * S->dt;
-    }
-  }
-  R G[3] = {0, 0, 0};
   const int n = valid ? node_id(i, m) : 0;
-  if (valid && !(inner && grad_on)) { G[0] = (R)Gd[n]; G[1] = (R)Gd[N + n]; G[2] = (R)Gd[2 * N + n]; }
-  double out[LAST ? kNodeOutLast : kNodeOut];
-  node_line<D, FIRST, LAST, R, GL>(ph, S->dt, valid, inner, updated, upd, in, G, out, xl != nullptr, m >= 2,
-                                   m + 2 <= nn - 1);
   if (upd) {
     if (inner && grad_on && node_on_plane(dm, D, idx)) { Gd[n] = (double)G[0]; Gd[N + n] = (double)G[1]; Gd[2 * N + n] = (double)G[2]; }
     // each lane overwrites only the tile column it read itself

@@ -62,6 +62,23 @@ def test_sedov_jittered_bitwise():
     assert_bitwise(o, g, dto, dtg)
 
 
+def test_tiny_values_take_the_exact_quotients():
+    """The sweeps divide with a fast corrected quotient that flags operands
+    outside 2^-960 <= |.| < 2^960; a warp with a flagged lane recomputes its
+    segment with exact quotients.  An ambient energy of 1e-300 (cell energies
+    m e near 1e-304) and node velocities down to 1e-165 (kinetic energies in
+    the subnormals) flag lanes in every sweep direction: bitwise vs the oracle."""
+    case = gen.sedov(n=16, jitter=0.01, seed=5, e_amb=1.0e-300, cycles=30)
+    rng = np.random.default_rng(7)
+    n = case.velocity.shape[0]
+    case.velocity = rng.uniform(-1.0, 1.0, size=(n, 3)) * 10.0 ** rng.uniform(-165.0, -145.0, size=(n, 1))
+    tiny = 2.0 ** -960
+    assert (0.5 * np.sum(case.velocity ** 2, axis=1) < tiny).mean() > 0.5
+    assert (case.pressure[0] < tiny).mean() > 0.9
+    o, g, dto, dtg = run_both(case, 30)
+    assert_bitwise(o, g, dto, dtg)
+
+
 def test_node_coordinates_bitwise():
     """MHY_FIELD_NODE_COORD: the initial coordinates before the first cycle,
     then the Lagrangian ones of the last cycle (x0 + dt v_half,
