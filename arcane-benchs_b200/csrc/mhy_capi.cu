@@ -195,8 +195,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (opt->with_newton != 0 && opt->with_newton != 1) return fail(MHY_ERR_ARG, "with_newton must be 0 or 1");
   if (opt->ordre_projection < 1 || opt->ordre_projection > 3)
     return fail(MHY_ERR_UNSUPPORTED, "ordre-projection must be 1, 2 or 3");
-  if (opt->ordre_projection == 3 && (opt->nb_env != 1 || opt->precision != 0))
-    return fail(MHY_ERR_UNSUPPORTED, "ordre-projection 3: one environment in FP64 on the device");
+  if (opt->ordre_projection == 3 && opt->precision != 0)
+    return fail(MHY_ERR_UNSUPPORTED, "ordre-projection 3: FP64 on the device");
   if (opt->projection_limiteur_id < 0 || opt->projection_limiteur_id > 7)
     return fail(MHY_ERR_UNSUPPORTED, "projection-limiteur-id must be 0..7 (TypesMahyco.h:65-74)");
   if (opt->projection_limiteur_id >= 3 && opt->precision != 0)
@@ -315,7 +315,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     if (opt->ordre_projection == 3 || opt->projection_limiteur_id >= 3 || opt->projection_pente_borne)
       A_(&c->fd.h, 3 * C);                                                                      // cell widths
     if (opt->projection_pente_borne) A_(&c->fd.pbphi, 3 * C);
-    if (opt->ordre_projection == 3) A_(&c->fd.phi3, 4 * std::max(nf[0], std::max(nf[1], nf[2])));
+    if (opt->ordre_projection == 3)   // face values of the current sweep: 4 (one environment) or 3K+1 components
+      A_(&c->fd.phi3, (K == 1 ? 4 : 3 * K + 1) * std::max(nf[0], std::max(nf[1], nf[2])));
   }
   if (rc == MHY_OK) rc = c->alloc(&c->bcmask, (size_t)N);
   if (rc == MHY_OK) rc = c->alloc(&c->S, 1);
@@ -360,7 +361,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   err = cudaMemcpyAsync(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv
+  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv + (opt->ordre_projection == 3 ? 3 : 0)
                                : kKernelsPerCycle + (opt->schema_csts ? 2 : 0) + (opt->ordre_projection == 3 ? 3 : 0) +
                                      (opt->conservation_energie_totale ? 1 : 0);
   *out = c;

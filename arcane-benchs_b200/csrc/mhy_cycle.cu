@@ -540,48 +540,6 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
 // Remap-ordre-3.cc:7-131) for one environment: Phi of the six cells around
 // each inner face (clamped at the ends of the line) from the sweep's input U,
 // the cell widths h along D and u_f dt; written to fd.phi3 [4][F_D].
-__device__ __forceinline__ double o3_grad(double hm, double h0, double hp, double ym, double y0, double yp) {
-  return h0 / (hm + h0 + hp) * ((2. * hm + h0) / (h0 + hp) * (yp - y0) + (h0 + 2. * hp) / (hm + h0) * (y0 - ym));
-}
-__device__ __forceinline__ double o3_ystar(double hmm, double hm, double hp, double hpp, double ymm, double ym,
-                                           double yp, double ypp, double gradm, double gradp) {
-  const double tmp1 = (2. * hp * hm) / (hm + hp) * ((hmm + hm) / (2. * hm + hp) - (hpp + hp) / (2. * hp + hm)) * (yp - ym);
-  const double tmp2 = -hm * (hmm + hm) / (2. * hm + hp) * gradp + hp * (hp + hpp) / (hm + 2. * hp) * gradm;
-  return ym + hm / (hm + hp) * (yp - ym) + 1. / (hmm + hm + hp + hpp) * (tmp1 + tmp2);
-}
-__device__ __forceinline__ double o3_flux(const double y[6], const double h[6], double vdt) {
-  const double ymmm = y[0], ymm = y[1], ym = y[2], yp = y[3], ypp = y[4], yppp = y[5];
-  const double hmmm = h[0], hmm = h[1], hm = h[2], hp = h[3], hpp = h[4], hppp = h[5];
-  const double gradmm = o3_grad(hmmm, hmm, hm, ymmm, ymm, ym);
-  const double gradm = o3_grad(hmm, hm, hp, ymm, ym, yp);
-  const double gradp = o3_grad(hm, hp, hpp, ym, yp, ypp);
-  const double gradpp = o3_grad(hp, hpp, hppp, yp, ypp, yppp);
-  const double ystarm = o3_ystar(hmmm, hmm, hm, hp, ymmm, ymm, ym, yp, gradmm, gradm);
-  const double ystar = o3_ystar(hmm, hm, hp, hpp, ymm, ym, yp, ypp, gradm, gradp);
-  const double ystarp = o3_ystar(hm, hp, hpp, hppp, ym, yp, ypp, yppp, gradp, gradpp);
-  const double ym_m = ystarm, ym_p = ystar, yp_m = ystar, yp_p = ystarp;
-  const double grad_m = ym_p - ym_m, grad_p = yp_p - yp_m;
-  const double ym6 = 6. * (ym - 0.5 * (ym_m + ym_p));
-  const double yp6 = 6. * (yp - 0.5 * (yp_m + yp_p));
-  double flux;
-  if (vdt > 0.) { const double x = vdt, dx = hm; flux = ym_p - 0.5 * x / dx * (grad_m - (1. - 2. / 3. * x / dx) * ym6); }
-  else if (vdt < 0.) { const double x = -vdt, dx = hp; flux = yp_m + 0.5 * x / dx * (grad_p - (1. - 2. / 3. * x / dx) * yp6); }
-  else return 0.;
-  const double num = vdt / hm, nup = vdt / hp;
-  const double ym_ym = ym + (1. - num) / num * (ym - ymm);
-  const double yp_ym = yp - (1. + nup) / nup * (yp - ypp);
-  const double i10 = amin(ym, yp), i11 = amax(ym, yp);
-  double i20, i21;
-  if (vdt >= 0.) { i20 = amin(ym, ym_ym); i21 = amax(ym, ym_ym); }
-  else { i20 = amin(yp, yp_ym); i21 = amax(yp, yp_ym); }
-  double l0, l1;
-  if ((i11 < i20) || (i21 < i10)) { l0 = 0.; l1 = 0.; }
-  else { l0 = amax(i10, i20); l1 = amin(i11, i21); }
-  if (flux < l0) flux = l0;
-  if (flux > l1) flux = l1;
-  return flux;
-}
-
 template <int D>
 __global__ void __launch_bounds__(128) k_o3_faces(Dims dm, const Scalars* __restrict__ S,
     const double* __restrict__ Uin, FaceData fd) {

@@ -39,17 +39,18 @@ struct CellInK {
   double ob, of;               // outward-normal component along d of the back and front faces
   double den;                  // divisor of Phi on the first sweep: the Lagrangian volume
   double h;                    // G limiters: the cell's width along d (RemapADIService.cc:225-258)
+  double pf3[3 * K + 1];       // order 3: Phi of the low face from k_o3_faces_env (inner faces only)
 };
 
-// One line step of the remap of a K-environment cell (RemapADIService.cc:91-271,
-// 447-517, 658-720, 883-1040).  out = the 3K+1 updated components, then the
-// K dual mass fluxes.  GL: the generalised limiters for uneven widths
+// Face values of a K-environment line at orders 1 and 2
+// (RemapADIService.cc:91-271, 447-517, 658-720): Pf of this lane's low face
+// and Pfn of its high face.  GL: the generalised limiters for uneven widths
 // (RemapADIService.cc:319-437 -> UtilesRemap.cc:295-330), every component
 // limited alike; at the ends of the line the back or front cell is the cell
 // itself.
-template <int K, bool FIRST, typename R, bool GL = false>
-__device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
-                                              bool upd, const CellInK<K>& in, double* out) {
+template <int K, bool FIRST, typename R, bool GL>
+__device__ __forceinline__ void face_values_env(const Phys& ph, bool valid, bool inner, bool infr,
+                                                const CellInK<K>& in, R Pf[3 * K + 1], R Pfn[3 * K + 1]) {
   constexpr int NV = 3 * K + 1;
   const R order2 = (R)(ph.ordre_projection - 1);
   const int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
@@ -94,12 +95,33 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
   }
   const bool back = in.u * dx > 0.0;
   const R dot_xf = (R)(back ? in.db : in.df);
-  R Pf[NV], Pfn[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     const R Gp = __shfl_up_sync(full, G[v], 1);
     Pf[v] = inner ? (back ? (Pp[v] + order2 * dot_xf * Gp) : (P[v] + order2 * dot_xf * G[v])) : R(0);
     Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
+  }
+}
+
+// One line step of the remap of a K-environment cell (RemapADIService.cc:91-271,
+// 447-517, 658-720, 883-1040).  out = the 3K+1 updated components, then the
+// K dual mass fluxes.  O3: the face values of order 3 (R:583-641), computed
+// per face beforehand by k_o3_faces_env; no gradient is formed.
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false>
+__device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
+                                              bool upd, const CellInK<K>& in, double* out) {
+  constexpr int NV = 3 * K + 1;
+  const unsigned full = 0xffffffffu;
+  R Pf[NV], Pfn[NV];
+  if constexpr (O3) {
+    static_assert(sizeof(R) == 8, "order 3 is FP64");
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      Pf[v] = inner ? in.pf3[v] : 0.;
+      Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
+    }
+  } else {
+    face_values_env<K, FIRST, R, GL>(ph, valid, inner, infr, in, Pf, Pfn);
   }
   const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
   if (!upd) return;
@@ -122,7 +144,7 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
 }
 
 // K-environment cell sweep along x (lanes along the rows).
-template <int K, bool FIRST, typename R, bool GL = false>
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -155,9 +177,14 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
     in.n[0] = n0[t]; in.n[1] = n0[F + t]; in.n[2] = n0[2 * F + t];
   }
+  if constexpr (O3) {
+    const int Fd = (int)dm.Fx;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in.pf3[v] = inner ? fd.phi3[v * Fd + t] : 0.;
+  }
   if (upd) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }
   double out[NV + K];
-  cell_line_env<K, FIRST, R, GL>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R, GL, O3>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (!upd) return;
 #pragma unroll
   for (int v = 0; v < NV; ++v) Uout[v * C + c] = out[v];
@@ -172,7 +199,7 @@ template <int K, bool FIRST>
 __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
 
 // W: lines per block (8 or 16, the tuning; the register budget stays 128).
-template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false>
+template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false, bool O3 = false>
 __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_sweep_cells_t(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -234,10 +261,18 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
     const int ci = i0 + w;
     in.h = fd.h[D * C + (D == 1 ? ci + dm.nx * (s + dm.ny * o) : ci + dm.nx * (o + dm.ny * s))];
   }
+  if constexpr (O3) {
+    // face values in the line layout of k_o3_faces_env: position along D
+    // fastest, so the lanes' reads are contiguous
+    const int Fd = (int)(D == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
+    const int q = s + (nd + 1) * (i0 + w + dm.nx * o);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in.pf3[v] = inner ? fd.phi3[v * Fd + q] : 0.;
+  }
   constexpr int NO = NV + K;
   static_assert(NO <= NA, "outputs reuse the staged rows");
   double out[NO];
-  cell_line_env<K, FIRST, R, GL>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R, GL, O3>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (upd) {
 #pragma unroll
     for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];
@@ -249,6 +284,92 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
   for (int v = 0; v < NV; ++v) Uout[v * C + sc] = r[v * kTileArr];
 #pragma unroll
   for (int e = 0; e < K; ++e) dpf[e * C + sc] = r[(NV + e) * kTileArr];
+}
+
+// Order-3 face values of direction D for K environments
+// (RemapADIService.cc:583-641, Remap-ordre-3.cc:7-131), one thread per face.
+// Phi of the six cells around an inner face (clamped at the ends of the
+// line) as the sweeps form it (U over the Lagrangian volume on the first
+// sweep, over the sum of the environment volumes afterwards), o3_flux per
+// component; then, unless the two cells are pure cells of one environment,
+// each environment's density and energy face values are rescaled by the
+// upwind cell's ratios (R:623-641).  A cell is mixed when more than one
+// environment has Phi_k > 0, else pure in the last such environment
+// (R:972-988 after every sweep, RemapADIFinal.cc:495-507 after the remap):
+// that is a function of the Phi the sweep starts from, except before the
+// run's first remap, where both indicators are still zero (every face
+// counts as pure).  Faces are written in line order: the position along D
+// fastest, then x, then the remaining axis (for D = 0 the usual face order).
+template <int D, int K, bool FIRST>
+__global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ Uin, FaceData fd, const double* __restrict__ Vlag) {
+  constexpr int NV = 3 * K + 1;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long Fd = dm.nfd(D);
+  if (t >= Fd) return;
+  const int n = dm.ncd(D);
+  const int id = (int)(t % (n + 1));
+  const long long line = t / (n + 1);
+  if (id <= 0 || id >= n) return;                     // boundary faces carry no flux
+  int i, j, k;
+  if (D == 0) { i = id; j = (int)(line % dm.ny); k = (int)(line / dm.ny); }
+  else if (D == 1) { i = (int)(line % dm.nx); j = id; k = (int)(line / dm.nx); }
+  else { i = (int)(line % dm.nx); j = (int)(line / dm.nx); k = id; }
+  int pos[6];
+  pos[2] = id - 1; pos[1] = pos[2] > 0 ? pos[2] - 1 : pos[2]; pos[0] = pos[1] > 0 ? pos[1] - 1 : pos[1];
+  pos[3] = id; pos[4] = pos[3] + 1 < n ? pos[3] + 1 : pos[3]; pos[5] = pos[4] + 1 < n ? pos[4] + 1 : pos[4];
+  const long long C = dm.C;
+  long long cc[6];
+  double den[6], rden[6], h[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    cc[a] = D == 0 ? dm.cid(pos[a], j, k) : (D == 1 ? dm.cid(i, pos[a], k) : dm.cid(i, j, pos[a]));
+    if (FIRST) den[a] = Vlag[cc[a]];
+    else {
+      double sv = 0.;
+#pragma unroll
+      for (int e = 0; e < K; ++e) sv += Uin[e * C + cc[a]];
+      den[a] = sv;
+    }
+    rden[a] = 1.0 / den[a];
+    h[a] = fd.h[D * C + cc[a]];
+  }
+  const long long tf = dm.fid(D, i, j, k) - (D == 0 ? 0 : (D == 1 ? dm.Fx : dm.Fx + dm.Fy));
+  const double vdt = fd.u[D][tf] * S->dt;
+  double pf[NV];
+  double pb[NV], pn[NV];                              // Phi of the two cells of the face
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double y[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) y[a] = qdiv(Uin[v * C + cc[a]], den[a], rden[a]);
+    pb[v] = y[2]; pn[v] = y[3];
+    pf[v] = o3_flux(y, h, vdt);
+  }
+  bool pure = true;
+  if (!(FIRST && S->iteration == 0)) {
+    int nb = 0, eb = -1, nf = 0, ef = -1;
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      if (pb[e] > 0.) { ++nb; eb = e; }
+      if (pn[e] > 0.) { ++nf; ef = e; }
+    }
+    pure = nb <= 1 && nf <= 1 && eb == ef;
+  }
+  if (!pure) {
+#pragma unroll
+    for (int e = 0; e < K; ++e) {
+      if (vdt > 0. && pb[e] != 0. && pb[K + e] != 0.) {
+        pf[K + e] = (pb[K + e] / pb[e]) * pf[e];
+        pf[2 * K + e] = (pb[2 * K + e] / pb[K + e]) * pf[K + e];
+      } else if (vdt < 0. && pn[e] != 0. && pn[K + e] != 0.) {
+        pf[K + e] = (pn[K + e] / pn[e]) * pf[e];
+        pf[2 * K + e] = (pn[2 * K + e] / pn[K + e]) * pf[K + e];
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) fd.phi3[v * Fd + t] = pf[v];
 }
 
 // ---- end of the remap, per cell ----------------------------------------
@@ -469,13 +590,16 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
 // the generalised limiters (FP64): the cell sweeps' GL kernels
 static bool env_gl(const CycleArgs& a) { return a.ph.ordre_projection > 1 && a.ph.lim_cell >= 3; }
 
-template <int K, int D, bool FIRST, typename R, int W, bool GL = false>
+// order 3 (FP64): the sweeps read the face values of k_o3_faces_env
+static bool env_o3(const CycleArgs& a) { return a.ph.ordre_projection == 3; }
+
+template <int K, int D, bool FIRST, typename R, int W, bool GL = false, bool O3 = false>
 static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
   const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<W>::arr * sizeof(double);
-  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W, GL>;
+  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W, GL, O3>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
 }
@@ -484,6 +608,7 @@ static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uo
 template <int K, int D, bool FIRST, typename R>
 static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   if constexpr (sizeof(R) == 8) {
+    if (env_o3(a)) { env_cells_staged_w<K, D, FIRST, R, kLineWarps, false, true>(a, Uin, Uout, s); return; }
     if (env_gl(a)) { env_cells_staged_w<K, D, FIRST, R, kLineWarps, true>(a, Uin, Uout, s); return; }
   }
   if (a.lines[BK_CELLS_X + D] == 16) env_cells_staged_w<K, D, FIRST, R, 16>(a, Uin, Uout, s);
@@ -497,8 +622,10 @@ static void env_cells(const CycleArgs& a, int d, const double* Uin, double* Uout
     const int nseg = (dm.nx + kLineUpd - 1) / kLineUpd;
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
     auto kern = k_env_sweep_cells_x<K, FIRST, R>;
-    if constexpr (sizeof(R) == 8)
-      if (env_gl(a)) kern = k_env_sweep_cells_x<K, FIRST, R, true>;
+    if constexpr (sizeof(R) == 8) {
+      if (env_o3(a)) kern = k_env_sweep_cells_x<K, FIRST, R, false, true>;
+      else if (env_gl(a)) kern = k_env_sweep_cells_x<K, FIRST, R, true>;
+    }
     kern<<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
   } else if (d == 1) {
     env_cells_staged<K, 1, FIRST, R>(a, Uin, Uout, s);
@@ -518,6 +645,13 @@ static void remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks*
     double* uout = a.U[(it + 1) & 1];
     const double* udin = a.ud[(it + 1) & 1];
     double* udout = a.ud[it & 1];
+    if (sizeof(R) == 8 && env_o3(a)) {
+      const long long Fd = d == 0 ? a.dm.Fx : (d == 1 ? a.dm.Fy : a.dm.F - a.dm.Fx - a.dm.Fy);
+      const unsigned nb = (unsigned)((Fd + 127) / 128);
+      auto kern = first ? (d == 0 ? k_o3_faces_env<0, K, true> : (d == 1 ? k_o3_faces_env<1, K, true> : k_o3_faces_env<2, K, true>))
+                        : (d == 0 ? k_o3_faces_env<0, K, false> : (d == 1 ? k_o3_faces_env<1, K, false> : k_o3_faces_env<2, K, false>));
+      kern<<<nb, 128, 0, s>>>(a.dm, a.S, uin, a.fd, a.Vlag);
+    }
     if (first) env_cells<K, true, R>(a, d, uin, uout, s);
     else env_cells<K, false, R>(a, d, uin, uout, s);
     if (last) {
@@ -543,6 +677,10 @@ static void set_env_attributes_r() {
     cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
     cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
     cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R, kLineWarps, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, true, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   }
 }
 
@@ -556,7 +694,7 @@ template <int K, typename R>
 static void lagrange_cells_env(const CycleArgs& a, const dim3 nbc, int linear, cudaStream_t s) {
   auto kern = k_cyc_lagrange_cells<K, R>;
   if constexpr (sizeof(R) == 8)
-    if (a.fd.h) kern = k_cyc_lagrange_cells<K, R, true>;   // cell widths: the generalised limiters
+    if (a.fd.h) kern = k_cyc_lagrange_cells<K, R, true>;   // cell widths: order 3 and the generalised limiters
   kern<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs, a.st.mass,
                            a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, linear);
 }

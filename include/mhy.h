@@ -66,7 +66,7 @@ typedef struct mhy_options {
   double final_time;                 /* 0.2 */
   int32_t longueur_caracteristique;  /* 0 "racine-cubique-volume", 1 "faces-opposees" */
   int32_t pseudo_centree;            /* 0 */
-  int32_t ordre_projection;          /* 2 (1, 2, and 3 for one environment in FP64: Remap-ordre-3.cc) */
+  int32_t ordre_projection;          /* 2 (1, 2, and 3 in FP64 for one to four environments: Remap-ordre-3.cc) */
   int32_t projection_limiteur_id;    /* 0 minmod, 1 superBee, 2 vanLeer; the generalised limiters for uneven
                                         widths 3 minmodG, 4 superBeeG, 5 vanLeerG, 6 arithmeticG, 7 ultrabeeG
                                         (UtilesRemap.cc:127-175; FP64, one to four environments, >= 3 cells a

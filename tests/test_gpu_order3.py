@@ -61,9 +61,34 @@ def test_order3_entry_points_match_graph():
     assert a.kernels_per_cycle() == 13
 
 
+@pytest.mark.parametrize("limiter", [0, 2])
+def test_order3_two_gases_bitwise(limiter):
+    """Several environments: the face values of each component, then the
+    density and energy rescaling on faces whose cells are not pure cells of
+    one environment (R:623-641); the first sweep of the run sees every face
+    as pure (the mixed/pure indicators start at zero)."""
+    opts = gen.Options(ordre_projection=3, projection_limiteur_id=limiter)
+    compare(gen.two_material(32, 16, 16, cycles=50, seed=9, options=opts), 50, 10)
+
+
+def test_order3_three_gases_bitwise():
+    compare(gen.three_material(cycles=40, options=gen.Options(ordre_projection=3)), 40, 10)
+
+
+def test_order3_two_gases_entry_points_match_graph():
+    case = gen.two_material(20, 10, 10, cycles=12, seed=4, options=gen.Options(ordre_projection=3))
+    a, b = Context(case), Context(case)
+    for _ in range(12):
+        a.cycle_by_entry_points()
+    b.step(12)
+    for f in ("density", "internal_energy", "velocity"):
+        assert np.array_equal(a.field(f), b.field(f)), f
+    assert a.kernels_per_cycle() == 14
+
+
 def test_order3_unsupported_forms_are_refused():
     with pytest.raises(MhyError):
-        Context(gen.two_material(16, 8, 8, cycles=5, options=gen.Options(ordre_projection=3)))
+        Context(gen.two_material(16, 8, 8, cycles=5, options=gen.Options(ordre_projection=3, precision=1)))
     with pytest.raises(MhyError):
         Context(gen.sod(cycles=5, options=gen.Options(ordre_projection=3, precision=1)))
     cases = gen.batched(count=2, seed=5, side_lo=8, side_hi=10, cycles=5)
