@@ -219,8 +219,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     return fail(MHY_ERR_ARG, "pente_borne_debar_fix must be 0, 1 or 2");
   if (opt->limiteur_pure_id < 0 || opt->limiteur_pure_id > 7)
     return fail(MHY_ERR_ARG, "limiteur_pure_id must be 0..7 (TypesMahyco.h:65-74)");
-  if ((opt->projection_pente_borne || opt->pente_borne_mixte) && (opt->nb_env != 1 || opt->precision != 0))
-    return fail(MHY_ERR_UNSUPPORTED, "pente-borne: one environment in FP64 on the device");
+  if ((opt->projection_pente_borne || opt->pente_borne_mixte) && opt->precision != 0)
+    return fail(MHY_ERR_UNSUPPORTED, "pente-borne: FP64 on the device");
   if (opt->projection_pente_borne && opt->ordre_projection != 2)
     return fail(MHY_ERR_UNSUPPORTED, "pente-borne: ordre-projection 2 on the device");
   for (int b = 0; b < opt->nb_bc; ++b)
@@ -274,6 +274,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   ph.pb_pure = opt->pente_borne_mixte;
   ph.pb_debar = opt->pente_borne_debar_fix;
   ph.pb_lim_y0 = opt->pente_borne_mixte ? opt->limiteur_pure_id : opt->projection_limiteur_id;
+  ph.pb_mixte = opt->pente_borne_mixte;
+  ph.lim_pure = opt->limiteur_pure_id;
   ph.pb_first = 0;
   ph.cons_ec = opt->conservation_energie_totale;
   c->bct.nb = opt->nb_bc;
@@ -314,7 +316,9 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     }
     if (opt->ordre_projection == 3 || opt->projection_limiteur_id >= 3 || opt->projection_pente_borne)
       A_(&c->fd.h, 3 * C);                                                                      // cell widths
-    if (opt->projection_pente_borne) A_(&c->fd.pbphi, 3 * C);
+    if (opt->projection_pente_borne) A_(&c->fd.pbphi, (K == 1 ? 3 : 3 * K + 1) * C);
+    if (K > 1 && (opt->ordre_projection == 3 || opt->pente_borne_mixte) && rc == MHY_OK)
+      rc = c->alloc(&c->fd.est, (size_t)C);                                                   // mixed/pure indicators
     if (opt->ordre_projection == 3)   // face values of the current sweep: 4 (one environment) or 3K+1 components
       A_(&c->fd.phi3, (K == 1 ? 4 : 3 * K + 1) * std::max(nf[0], std::max(nf[1], nf[2])));
   }
@@ -340,6 +344,10 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       k_soa3<<<(unsigned)nb, 256, 0, c->stream>>>(N, c->ud[0], c->x0);
       // dual gradients of nodes never inner so far read 0 (the reference's variables start at zero)
       cudaMemsetAsync(c->Gd, 0, 3 * N * sizeof(double), c->stream);
+      // several environments: pente-borne Phi of environments absent so far read 0, and both
+      // mixed/pure indicators start at zero (code 1), as the reference's variables do
+      if (K > 1 && c->fd.pbphi) cudaMemsetAsync(c->fd.pbphi, 0, (size_t)(3 * K + 1) * C * sizeof(double), c->stream);
+      if (c->fd.est) k_fill_u32<<<(unsigned)((C + 255) / 256), 256, 0, c->stream>>>(C, c->fd.est, 1u);
       k_max3_partial<<<nparts, 256, 0, c->stream>>>(N, c->x0, c->setup);
       unsigned* grp = reinterpret_cast<unsigned*>(c->vh);
       cudaMemsetAsync(grp, 0, N * sizeof(unsigned), c->stream);
@@ -1407,6 +1415,8 @@ std::vector<CkField> ckpt_fields(mhy_ctx* c) {
     f.push_back({"Pressure.env", ev.p, 0, K * C}); f.push_back({"SoundSpeed.env", ev.cs, 0, K * C});
     f.push_back({"PseudoViscosity.env", ev.q, 0, K * C}); f.push_back({"CellMass.env", ev.m, 0, K * C});
     f.push_back({"FracVol", ev.fg, 0, C}); f.push_back({"MassFraction", ev.xg, 0, C});
+    if (c->fd.est) f.push_back({"EstMixtePure", c->fd.est, 2, C});
+    if (c->fd.pbphi) f.push_back({"PenteBornePhi", c->fd.pbphi, 0, (3 * K + 1) * C});
   }
   return f;
 }

@@ -109,6 +109,11 @@ __global__ void k_init_state(Dims dm, Phys ph, const double* __restrict__ vol, d
 // ------------------------------------------------------------ set-up ----
 
 // xyz-interleaved (n x 3) -> three planes (3 x n).
+__global__ void k_fill_u32(long long n, uint32_t* __restrict__ a, uint32_t value) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = value;
+}
+
 __global__ void k_soa3(long long n, const double* __restrict__ aos, double* __restrict__ soa) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;

@@ -38,6 +38,9 @@ struct Phys {
   int cons_ec;          // conservation-energie-totale (RemapADI.axl:151; one environment, FP64)
   int ext_dt;           // slabs: the cycle ends with the local dt minimum; the caller combines the
                         // ranks' minima and finishes the dt (mhy_dt_finish)
+  // several environments: projection-pente-borne-mixte and projection-limiteur-pure-id, applied
+  // cell by cell where the neighbourhood is pure (RemapADIService.cc:364-375, UtilesRemap.cc:406-409)
+  int pb_mixte, lim_pure;
 };
 
 struct BCTable {
@@ -57,7 +60,15 @@ struct FaceData {
   double* h;      // order 3: cell widths along each direction, 3 planes of C (RemapADIService.cc:225-258)
   double* phi3;   // order 3: face values of the current sweep, [4][faces of its direction]
   double* pbphi;  // pente-borne: rho, e and q after the Lagrange step, 3 planes of C (Phi of the first
-                  // sweep, PrepareRemap.cc:201-212; q stays the Phi of q in every sweep)
+                  // sweep, PrepareRemap.cc:201-212; q stays the Phi of q in every sweep).  Several
+                  // environments: the 3K+1 planes of Phi for the first sweep (volume fraction, density,
+                  // internal energy of each environment, then q); an environment absent from a cell
+                  // keeps the Phi of the previous remap's last sweep (PrepareRemap.cc:201-212 sets only
+                  // the cell's environments), zero before the first remap
+  uint32_t* est;  // several environments with order 3 or projection-pente-borne-mixte: each cell's
+                  // mixed/pure indicator after the last remap (m_est_mixte, m_est_pure,
+                  // RemapADIFinal.cc:495-507) as 255 (mixed) or 1 + the pure environment (0: none);
+                  // 1 (both indicators zero) before the first remap
 };
 
 // Persistent cell state (global values of a single-environment mesh).
@@ -171,6 +182,7 @@ __global__ void k_init_state(Dims dm, Phys ph, const double* vol, double* rho, c
 __global__ void k_node_mass(Dims dm, const double* mass, double* nm);
 __global__ void k_to_f32(long long n, const double* src, float* dst);
 __global__ void k_soa3(long long n, const double* aos, double* soa);
+__global__ void k_fill_u32(long long n, uint32_t* a, uint32_t value);
 __global__ void k_gather_index(long long n, int comps, const int32_t* idx, const double* src, double* out);
 __global__ void k_aos3(long long n, const double* soa, const double* vh, const Scalars* S, double* aos);
 __global__ void k_max3_partial(long long n, const double* x, double* part);

@@ -178,13 +178,17 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
 // V q] as planes; V is kept in Vlag, the divisor of Phi on the first sweep.
 // The global density m/V is stored for every cell: the remap keeps it in a
 // mixed cell whose fractions leave one environment only (RemapADIFinal.cc:561-562).
+// pbphi (pente-borne): Phi of the first sweep for the cell's environments,
+// volume fraction, density and internal energy after this step, and q of
+// the last of them (PrepareRemap.cc:201-212); the other environments' planes
+// are left as they are.
 template <int K>
 __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalars* S, const EnvState& env, int c,
                                                     int C, double V, double Lc, double* __restrict__ rho,
                                                     const double* __restrict__ e, const double* __restrict__ q,
                                                     const double* __restrict__ p, const double* __restrict__ cs,
                                                     const double* __restrict__ mass, double* __restrict__ U,
-                                                    double* __restrict__ Vlag) {
+                                                    double* __restrict__ Vlag, double* __restrict__ pbphi) {
   constexpr int NV = 3 * K + 1;
   const double inv_deltat = S->inv_dt;
   const double rn = rho[c];
@@ -209,6 +213,10 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
     for (int k = 0; k < K; ++k)
       if (k == ke) { u[k] = V; u[K + k] = V * nd; u[2 * K + k] = V * nd * en; }
     u[3 * K] = V * qn;
+    if (pbphi) {
+      pbphi[ke * C + c] = env.fg[c]; pbphi[(K + ke) * C + c] = nd; pbphi[(2 * K + ke) * C + c] = en;
+      pbphi[3 * K * C + c] = qn;
+    }
   } else {
     const double csc = cs[c];
 #pragma unroll
@@ -228,6 +236,9 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
       u[K + k] = vk * rk;
       u[2 * K + k] = vk * rk * ek;
       u[3 * K] = vk * qk;                                        // the last environment wins (P:318-330)
+      if (pbphi) {
+        pbphi[o] = env.f[o]; pbphi[K * C + o] = rk; pbphi[2 * K * C + o] = ek; pbphi[3 * K * C + c] = qk;
+      }
     }
   }
 #pragma unroll
@@ -396,7 +407,7 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     U[3 * C + c] = V * qn;
     if (fd.pbphi) { fd.pbphi[c] = nd; fd.pbphi[C + c] = en; fd.pbphi[2 * C + c] = qn; }
   } else {
-    lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag);
+    lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag, fd.pbphi);
   }
   if constexpr (F32) face_data<float>(dm, i, j, k, xr, F3{0.f, 0.f, 0.f}, n0, vh, fd);
   else face_data<double, HC>(dm, i, j, k, x, xc, n0, vh, fd);

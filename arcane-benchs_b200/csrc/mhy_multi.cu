@@ -40,35 +40,23 @@ struct CellInK {
   double den;                  // divisor of Phi on the first sweep: the Lagrangian volume
   double h;                    // G limiters: the cell's width along d (RemapADIService.cc:225-258)
   double pf3[3 * K + 1];       // order 3: Phi of the low face from k_o3_faces_env (inner faces only)
+  double pbP[3 * K + 1];       // pente-borne, first sweep: Phi of the cell (FaceData::pbphi)
+  double pbq;                  // pente-borne: Phi of q, q at the start of the remap
+  uint32_t est;                // first sweep with projection-pente-borne-mixte: the cell's FaceData::est
 };
 
 // Face values of a K-environment line at orders 1 and 2
 // (RemapADIService.cc:91-271, 447-517, 658-720): Pf of this lane's low face
-// and Pfn of its high face.  GL: the generalised limiters for uneven widths
-// (RemapADIService.cc:319-437 -> UtilesRemap.cc:295-330), every component
-// limited alike; at the ends of the line the back or front cell is the cell
-// itself.
-template <int K, bool FIRST, typename R, bool GL>
-__device__ __forceinline__ void face_values_env(const Phys& ph, bool valid, bool inner, bool infr,
-                                                const CellInK<K>& in, R Pf[3 * K + 1], R Pfn[3 * K + 1]) {
+// and Pfn of its high face, from the lanes' Phi.  lim: this cell's limiter
+// (-1 at order 1).  GL: the cell widths are at hand, and limiters 3..7 take
+// the generalised form for uneven widths (RemapADIService.cc:319-437 ->
+// UtilesRemap.cc:295-330), every component limited alike; at the ends of
+// the line the back or front cell is the cell itself.
+template <int K, typename R, bool GL>
+__device__ __forceinline__ void face_values_env(const Phys& ph, int lim, bool inner, bool infr, const CellInK<K>& in,
+                                                const R P[3 * K + 1], R Pf[3 * K + 1], R Pfn[3 * K + 1]) {
   constexpr int NV = 3 * K + 1;
   const R order2 = (R)(ph.ordre_projection - 1);
-  const int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
-  R P[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) P[v] = 0;
-  if (valid) {
-    double den;
-    if (FIRST) den = in.den;
-    else {
-      den = 0.;
-#pragma unroll
-      for (int k = 0; k < K; ++k) den += in.U[k];
-    }
-    const R dR = (R)den, r = Ar<R>::rcp(dR);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) P[v] = Ar<R>::div((R)in.U[v], dR, r);
-  }
   const unsigned full = 0xffffffffu;
   const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
                xpz = __shfl_up_sync(full, in.xc[2], 1);
@@ -88,7 +76,8 @@ __device__ __forceinline__ void face_values_env(const Phys& ph, bool valid, bool
     const R gr = __shfl_down_sync(full, g, 1);
     if constexpr (GL) {
       const R Pn = __shfl_down_sync(full, P[v], 1);
-      G[v] = flux_limiter_g<R>(lim, gr, g, P[v], infr ? Pn : P[v], inner ? Pp[v] : P[v], h0, hp, hm);
+      G[v] = lim < 3 ? limited_one<R>(lim, g, gr)
+                     : flux_limiter_g<R>(lim, gr, g, P[v], infr ? Pn : P[v], inner ? Pp[v] : P[v], h0, hp, hm);
     } else {
       G[v] = limited_one<R>(lim, g, gr);
     }
@@ -103,11 +92,71 @@ __device__ __forceinline__ void face_values_env(const Phys& ph, bool valid, bool
   }
 }
 
+// Mixed/pure indicator of a cell from its Phi (RemapADIService.cc:972-988):
+// 255 when more than one environment has Phi_k > 0, else 1 + the last such
+// environment (0: none), the coding of FaceData::est.
+template <int K, typename R>
+__device__ __forceinline__ uint32_t est_code(const R* P) {
+  int n = 0, e = -1;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (P[k] > R(0)) { ++n; e = k; }
+  return n > 1 ? 255u : (uint32_t)(e + 1);
+}
+
+// pente-borne fluxes of the 3K+1 components leaving a K-environment cell
+// through one face (UtilesRemap.cc:406-627 computeFluxPP, :628-823
+// computeFluxPPPure): the integral of each component's reconstruction, then
+// the debar fix over the environments (the mass flux is left alone where the
+// neighbourhood is pure).
+template <int K>
+__device__ __forceinline__ void pb_fluxes_env(const Phys& ph, int type, double ppv, int lim_y0, bool pure,
+                                              const double* P, const double* Pn, const double* Pp, double h0,
+                                              double hp, double hm, const double* G, double* F) {
+  constexpr int NV = 3 * K + 1;
+  const double thr = ph.threshold;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) F[v] = pb_flux_var(type, lim_y0, thr, ppv, P[v], Pn[v], Pp[v], h0, hp, hm, G[v]);
+  if (ph.pb_debar == 1) {
+    double svol = 0.;
+#pragma unroll
+    for (int m = 0; m < K; ++m) svol += F[m];
+    if (fabs(svol) > thr) {
+#pragma unroll
+      for (int m = 0; m < K; ++m) {
+        if (!pure) F[K + m] = (F[K + m] / svol) * F[m];
+        F[2 * K + m] = (F[2 * K + m] / svol) * F[K + m];
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) F[v] = 0.;
+    }
+  } else if (ph.pb_debar == 2) {
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+      if (!pure) F[K + m] = P[K + m] * F[m];
+      F[2 * K + m] = P[2 * K + m] * F[K + m];
+    }
+  }
+  if (ppv == 0.) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) F[v] = 0.;
+  }
+}
+
 // One line step of the remap of a K-environment cell (RemapADIService.cc:91-271,
 // 447-517, 658-720, 883-1040).  out = the 3K+1 updated components, then the
 // K dual mass fluxes.  O3: the face values of order 3 (R:583-641), computed
-// per face beforehand by k_o3_faces_env; no gradient is formed.
-template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false>
+// per face beforehand by k_o3_faces_env; no gradient is formed.  PB:
+// projection-pente-borne (FP64): Phi of PrepareRemap.cc:201-212 (first
+// sweep) or R:805-834, the general gradient (R:319-378) and the fluxes of
+// pb_fluxes_env, face values from the fluxes leaving the two cells
+// (R:380-431, 574-578) and fluxes o*A*Phi_f (R:770-774).  With
+// projection-pente-borne-mixte the limiter of the gradient and of the
+// reconstruction, and the debar fix, follow the cell's neighbourhood
+// (R:364-375): pure when the cell and its back and front neighbours (the
+// cell itself at the ends of the line) are pure cells of one environment.
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
 __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
                                               bool upd, const CellInK<K>& in, double* out) {
   constexpr int NV = 3 * K + 1;
@@ -121,13 +170,88 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
       Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
     }
   } else {
-    face_values_env<K, FIRST, R, GL>(ph, valid, inner, infr, in, Pf, Pfn);
+    R P[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) P[v] = 0;
+    if (valid) {
+      if constexpr (PB) {
+        if (FIRST) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) P[v] = in.pbP[v];
+        } else {
+          double sv = 0.;
+#pragma unroll
+          for (int k = 0; k < K; ++k) sv += in.U[k];
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            P[k] = in.U[k] / sv;
+            P[K + k] = in.U[k] != 0. ? in.U[K + k] / in.U[k] : 0.;
+            P[2 * K + k] = in.U[K + k] != 0. ? in.U[2 * K + k] / in.U[K + k] : 0.;
+          }
+          P[3 * K] = in.pbq;
+        }
+      } else {
+        double den;
+        if (FIRST) den = in.den;
+        else {
+          den = 0.;
+#pragma unroll
+          for (int k = 0; k < K; ++k) den += in.U[k];
+        }
+        const R dR = (R)den, r = Ar<R>::rcp(dR);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) P[v] = Ar<R>::div((R)in.U[v], dR, r);
+      }
+    }
+    int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
+    bool pure = false;
+    if (ph.pb_mixte) {
+      const uint32_t code = FIRST ? in.est : est_code<K>(P);
+      const uint32_t cb = __shfl_up_sync(full, code, 1), cf = __shfl_down_sync(full, code, 1);
+      pure = code != 255u && code == (inner ? cb : code) && code == (infr ? cf : code);
+      if (ph.ordre_projection > 1) lim = (ph.lim_pure == 1 && pure) ? ph.lim_pure : ph.limiteur_id;
+    }
+    if constexpr (PB) {
+      static_assert(sizeof(R) == 8, "pente-borne is FP64");
+      const double xpx = __shfl_up_sync(full, in.xc[0], 1), xpy = __shfl_up_sync(full, in.xc[1], 1),
+                   xpz = __shfl_up_sync(full, in.xc[2], 1);
+      const double dx =
+          inner ? dot(d3(in.xc[0], in.xc[1], in.xc[2]) - d3(xpx, xpy, xpz), d3(in.n[0], in.n[1], in.n[2])) : 0.;
+      const double rdx = inner ? 1.0 / dx : 0.;
+      const double hb = __shfl_up_sync(full, in.h, 1), hn = __shfl_down_sync(full, in.h, 1);
+      const double h0 = in.h, hm = inner ? hb : in.h, hp = infr ? hn : in.h;
+      double Pne[NV], Ppe[NV], G[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double Pp = __shfl_up_sync(full, P[v], 1), Pn = __shfl_down_sync(full, P[v], 1);
+        Pne[v] = infr ? Pn : P[v]; Ppe[v] = inner ? Pp : P[v];
+        const double g = inner ? qdiv(P[v] - Pp, dx, rdx) : 0.;
+        const double gr = __shfl_down_sync(full, g, 1);
+        G[v] = lim < 3 ? limited_one<double>(lim, g, gr)
+                       : flux_limiter_g<double>(lim, gr, g, P[v], Pne[v], Ppe[v], h0, hp, hm);
+      }
+      const double un = __shfl_down_sync(full, in.u, 1);
+      const double ob = in.ob * in.u, of = in.of * un;             // outward velocities of the two faces
+      const int lim_y0 = pure ? ph.lim_pure : ph.limiteur_id;
+      double ar[NV], av[NV];
+      pb_fluxes_env<K>(ph, 0, 0.5 * (ob + fabs(ob)) * dt, lim_y0, pure, P, Pne, Ppe, h0, hp, hm, G, ar);
+      pb_fluxes_env<K>(ph, 1, 0.5 * (of + fabs(of)) * dt, lim_y0, pure, P, Pne, Ppe, h0, hp, hm, G, av);
+      // back face: what leaves the previous cell forwards minus what leaves this one backwards
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double avp = __shfl_up_sync(full, av[v], 1);
+        Pf[v] = inner ? avp - ar[v] : 0.;
+        Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
+      }
+    } else {
+      face_values_env<K, R, GL>(ph, lim, inner, infr, in, P, Pf, Pfn);
+    }
   }
   const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
   if (!upd) return;
   // flux sums in FP64 in every precision (each face flux is one rounded value)
-  const double cb = inner ? in.ob * in.u * in.A * dt : 0.;
-  const double cf = infr ? in.of * un * An * dt : 0.;
+  const double cb = inner ? (PB ? in.ob * in.A : in.ob * in.u * in.A * dt) : 0.;
+  const double cf = infr ? (PB ? in.of * An : in.of * un * An * dt) : 0.;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     double flux_face = 0., dp = 0.;
@@ -143,8 +267,24 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
   }
 }
 
+// Inputs of a K-environment cell that its own index gives: the cell width
+// (GL, PB), the pente-borne Phi and the first sweep's mixed/pure indicator.
+template <int K, bool FIRST, bool GL, bool PB>
+__device__ __forceinline__ void env_cell_extras(const Phys& ph, const FaceData& fd, int C, int c, int D,
+                                                CellInK<K>& in) {
+  if constexpr (GL || PB) in.h = fd.h[D * C + c];
+  if constexpr (PB) {
+    if (FIRST) {
+#pragma unroll
+      for (int v = 0; v < 3 * K + 1; ++v) in.pbP[v] = fd.pbphi[v * C + c];
+    }
+    in.pbq = fd.pbphi[3 * K * C + c];
+  }
+  if (FIRST && ph.pb_mixte) in.est = fd.est[c];
+}
+
 // K-environment cell sweep along x (lanes along the rows).
-template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false>
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -166,12 +306,16 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
   for (int v = 0; v < NV; ++v) in.U[v] = 0.;
   in.xc[0] = in.xc[1] = in.xc[2] = 0.;
   in.db = in.df = in.u = in.A = 0.; in.n[0] = in.n[1] = in.n[2] = 0.; in.ob = in.of = 0.; in.den = 0.; in.h = 0.;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) in.pbP[v] = 0.;
+  in.pbq = 0.; in.est = 0u;
   if (valid) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) in.U[v] = Uin[v * C + c];
     in.xc[0] = xcs[c]; in.xc[1] = xcs[C + c]; in.xc[2] = xcs[2 * C + c];
     if (FIRST) in.den = Vlag[c];
-    if constexpr (GL) in.h = fd.h[c];
+    env_cell_extras<K, FIRST, GL, PB>(ph, fd, C, c, 0, in);
+    if (PB) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }   // every lane's two faces take part
   }
   if (inner) {
     in.db = fd.db[0][t]; in.df = fd.df[0][t]; in.u = fd.u[0][t]; in.A = fd.A[0][t];
@@ -184,7 +328,7 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
   }
   if (upd) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }
   double out[NV + K];
-  cell_line_env<K, FIRST, R, GL, O3>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R, GL, O3, PB>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (!upd) return;
 #pragma unroll
   for (int v = 0; v < NV; ++v) Uout[v * C + c] = out[v];
@@ -199,7 +343,7 @@ template <int K, bool FIRST>
 __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
 
 // W: lines per block (8 or 16, the tuning; the register budget stays 128).
-template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false, bool O3 = false>
+template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false, bool O3 = false, bool PB = false>
 __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_sweep_cells_t(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
@@ -256,10 +400,13 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
   in.n[0] = row[AN * kTileArr]; in.n[1] = row[(AN + 1) * kTileArr]; in.n[2] = row[(AN + 2) * kTileArr];
   in.ob = row[AO * kTileArr]; in.of = row[(AO + 1) * kTileArr];
   in.den = FIRST ? row[AD * kTileArr] : 0.;
-  in.h = 0.;
-  if (GL && valid) {                                   // own width only: read directly
+  in.h = 0.; in.pbq = 0.; in.est = 0u;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) in.pbP[v] = 0.;
+  if (valid) {                                         // the cell's own extras: read directly
     const int ci = i0 + w;
-    in.h = fd.h[D * C + (D == 1 ? ci + dm.nx * (s + dm.ny * o) : ci + dm.nx * (o + dm.ny * s))];
+    env_cell_extras<K, FIRST, GL, PB>(ph, fd, C, D == 1 ? ci + dm.nx * (s + dm.ny * o) : ci + dm.nx * (o + dm.ny * s),
+                                      D, in);
   }
   if constexpr (O3) {
     // face values in the line layout of k_o3_faces_env: position along D
@@ -272,7 +419,7 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
   constexpr int NO = NV + K;
   static_assert(NO <= NA, "outputs reuse the staged rows");
   double out[NO];
-  cell_line_env<K, FIRST, R, GL, O3>(ph, S->dt, valid, inner, infr, upd, in, out);
+  cell_line_env<K, FIRST, R, GL, O3, PB>(ph, S->dt, valid, inner, infr, upd, in, out);
   if (upd) {
 #pragma unroll
     for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];
@@ -296,10 +443,11 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
 // upwind cell's ratios (R:623-641).  A cell is mixed when more than one
 // environment has Phi_k > 0, else pure in the last such environment
 // (R:972-988 after every sweep, RemapADIFinal.cc:495-507 after the remap):
-// that is a function of the Phi the sweep starts from, except before the
-// run's first remap, where both indicators are still zero (every face
-// counts as pure).  Faces are written in line order: the position along D
-// fastest, then x, then the remaining axis (for D = 0 the usual face order).
+// within a remap that is a function of the Phi the sweep starts from; the
+// first sweep reads the indicator the previous remap left (FaceData::est;
+// before the run's first remap both indicators are zero, every face pure).
+// Faces are written in line order: the position along D fastest, then x,
+// then the remaining axis (for D = 0 the usual face order).
 template <int D, int K, bool FIRST>
 __global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __restrict__ S,
     const double* __restrict__ Uin, FaceData fd, const double* __restrict__ Vlag) {
@@ -346,16 +494,9 @@ __global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __
     pb[v] = y[2]; pn[v] = y[3];
     pf[v] = o3_flux(y, h, vdt);
   }
-  bool pure = true;
-  if (!(FIRST && S->iteration == 0)) {
-    int nb = 0, eb = -1, nf = 0, ef = -1;
-#pragma unroll
-    for (int e = 0; e < K; ++e) {
-      if (pb[e] > 0.) { ++nb; eb = e; }
-      if (pn[e] > 0.) { ++nf; ef = e; }
-    }
-    pure = nb <= 1 && nf <= 1 && eb == ef;
-  }
+  const uint32_t codeb = FIRST ? fd.est[cc[2]] : est_code<K>(pb);
+  const uint32_t codef = FIRST ? fd.est[cc[3]] : est_code<K>(pn);
+  const bool pure = codeb != 255u && codeb == codef;
   if (!pure) {
 #pragma unroll
     for (int e = 0; e < K; ++e) {
@@ -381,10 +522,14 @@ __global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __
 // and the partial slots as Arcane's material modifier moves them; of those
 // only the mass fraction can outlive this kernel (it is kept when the cell's
 // mass is exactly zero), so only it is moved.
+// fd.est: the cell's mixed/pure indicator of RemapADIFinal.cc:495-507.
+// fd.pbphi (pente-borne): the Phi of this last sweep for every environment
+// (RemapADIService.cc:805-834); the next Lagrange step overwrites the cell's
+// environments, and the others keep these values into the next remap.
 template <int K>
 __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __restrict__ S, Phys ph,
                                                             EnvState env, const double* __restrict__ U,
-                                                            CellState st) {
+                                                            CellState st, FaceData fd) {
   constexpr int NV = 3 * K + 1;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int C = (int)dm.C;
@@ -392,6 +537,17 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
   double u[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u[v] = U[v * C + c];
+  if (fd.pbphi) {
+    double sv = 0.;
+#pragma unroll
+    for (int k = 0; k < K; ++k) sv += u[k];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      fd.pbphi[k * C + c] = u[k] / sv;
+      fd.pbphi[(K + k) * C + c] = u[k] != 0. ? u[K + k] / u[k] : 0.;
+      fd.pbphi[(2 * K + k) * C + c] = u[K + k] != 0. ? u[2 * K + k] / u[K + k] : 0.;
+    }
+  }
   const double vol = st.Ve[c];
   const double thr = ph.threshold;
   uint32_t mask = env.mask[c];
@@ -446,15 +602,16 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
     somme_frac += fvol;
   }
   const double unsursomme_frac = 1. / somme_frac;
-  int matcell = 0;
+  int matcell = 0, imatpure = -1;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     if (!(mask >> k & 1)) continue;
     const double fvol = f[k] * unsursomme_frac;
-    if (fvol > 0.) matcell++;
+    if (fvol > 0.) { matcell++; imatpure = k; }
     f[k] = fvol;
   }
   const bool est_mixte = matcell > 1;
+  if (fd.est) fd.est[c] = est_mixte ? 255u : (uint32_t)(imatpure + 1);
 #pragma unroll
   for (int k = 0; k < K; ++k)
     if (mask >> k & 1) x[k] = pure ? env.xg[c] : env.x[k * C + c];
@@ -587,19 +744,22 @@ __global__ void k_env_init_state(Dims dm, EnvState env, CellState st) {
 
 // ------------------------------------------------------------------------
 // Host-side launchers.
-// the generalised limiters (FP64): the cell sweeps' GL kernels
-static bool env_gl(const CycleArgs& a) { return a.ph.ordre_projection > 1 && a.ph.lim_cell >= 3; }
+// the generalised limiters (FP64): the cell sweeps' GL kernels (with
+// projection-pente-borne-mixte some cells may take the pure limiter instead)
+static bool env_gl(const CycleArgs& a) { return a.ph.ordre_projection > 1 && a.ph.limiteur_id >= 3; }
+// projection-pente-borne (FP64): the PB kernels, which read the cell widths themselves
+static bool env_pb(const CycleArgs& a) { return a.ph.pb != 0; }
 
 // order 3 (FP64): the sweeps read the face values of k_o3_faces_env
 static bool env_o3(const CycleArgs& a) { return a.ph.ordre_projection == 3; }
 
-template <int K, int D, bool FIRST, typename R, int W, bool GL = false, bool O3 = false>
+template <int K, int D, bool FIRST, typename R, int W, bool GL = false, bool O3 = false, bool PB = false>
 static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   const Dims& dm = a.dm;
   const int nseg = (dm.ncd(D) + kLineUpd - 1) / kLineUpd;
   const dim3 g((dm.nx + W - 1) / W, nseg, D == 1 ? dm.nz : dm.ny);
   const size_t smem = (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<W>::arr * sizeof(double);
-  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W, GL, O3>;
+  auto kern = k_env_sweep_cells_t<K, D, FIRST, R, W, GL, O3, PB>;
   smem_opt_in((const void*)kern, smem);
   kern<<<g, 32 * W, smem, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
 }
@@ -608,6 +768,7 @@ static void env_cells_staged_w(const CycleArgs& a, const double* Uin, double* Uo
 template <int K, int D, bool FIRST, typename R>
 static void env_cells_staged(const CycleArgs& a, const double* Uin, double* Uout, cudaStream_t s) {
   if constexpr (sizeof(R) == 8) {
+    if (env_pb(a)) { env_cells_staged_w<K, D, FIRST, R, kLineWarps, false, false, true>(a, Uin, Uout, s); return; }
     if (env_o3(a)) { env_cells_staged_w<K, D, FIRST, R, kLineWarps, false, true>(a, Uin, Uout, s); return; }
     if (env_gl(a)) { env_cells_staged_w<K, D, FIRST, R, kLineWarps, true>(a, Uin, Uout, s); return; }
   }
@@ -623,7 +784,8 @@ static void env_cells(const CycleArgs& a, int d, const double* Uin, double* Uout
     const dim3 g(nseg, (dm.ny + kLineWarps - 1) / kLineWarps, dm.nz);
     auto kern = k_env_sweep_cells_x<K, FIRST, R>;
     if constexpr (sizeof(R) == 8) {
-      if (env_o3(a)) kern = k_env_sweep_cells_x<K, FIRST, R, false, true>;
+      if (env_pb(a)) kern = k_env_sweep_cells_x<K, FIRST, R, false, false, true>;
+      else if (env_o3(a)) kern = k_env_sweep_cells_x<K, FIRST, R, false, true>;
       else if (env_gl(a)) kern = k_env_sweep_cells_x<K, FIRST, R, true>;
     }
     kern<<<g, 32 * kLineWarps, 0, s>>>(dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, Uin, Uout, a.dpf, a.Vlag);
@@ -656,7 +818,7 @@ static void remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks*
     else env_cells<K, false, R>(a, d, uin, uout, s);
     if (last) {
       const unsigned nb = (unsigned)((a.dm.C + 255) / 256);
-      k_env_finalize_cells<K><<<nb, 256, 0, s>>>(a.dm, a.S, a.ph, a.env, uout, a.st);
+      k_env_finalize_cells<K><<<nb, 256, 0, s>>>(a.dm, a.S, a.ph, a.env, uout, a.st, a.fd);
     }
     mark(m, BK_CELLS_X + d, s);
     sweep_nodes<K, R>(a, d, first, last, prev, udin, udout, s);
@@ -681,6 +843,10 @@ static void set_env_attributes_r() {
     cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
     cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
     cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R, kLineWarps, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, true, R, kLineWarps, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, true, R, kLineWarps, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 1, false, R, kLineWarps, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(k_env_sweep_cells_t<K, 2, false, R, kLineWarps, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
   }
 }
 

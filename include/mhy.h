@@ -90,12 +90,13 @@ typedef struct mhy_options {
                                         PrepareRemap.cc:69-79, 456); one environment, precision 0 */
   int32_t projection_pente_borne;    /* 0; 1: the pente-borne remap (RemapADI.axl:167; RemapADIService.cc:319-437,
                                         530-581, 745-840; UtilesRemap.cc:73-93, 184-296, 406-823): fluxes
-                                        integrated from a three-piece reconstruction; one environment,
-                                        precision 0, ordre-projection 2 */
+                                        integrated from a three-piece reconstruction; precision 0,
+                                        ordre-projection 2, one to four environments */
   int32_t pente_borne_debar_fix;     /* 0, 1 or 2: projection-pente-borne-debar-fix (RemapADI.axl:171) */
-  int32_t pente_borne_mixte;         /* 0; 1: projection-pente-borne-mixte (RemapADI.axl:155): with one environment
-                                        every cell has a pure neighbourhood, so the pure-cell fluxes
-                                        (computeFluxPPPure) and limiter apply; one environment, precision 0 */
+  int32_t pente_borne_mixte;         /* 0; 1: projection-pente-borne-mixte (RemapADI.axl:155): where a cell and
+                                        its two neighbours along the sweep are pure cells of one environment
+                                        (with one environment: everywhere) the pure-cell fluxes
+                                        (computeFluxPPPure) and limiter apply; precision 0 */
   int32_t limiteur_pure_id;          /* 0..7: projection-limiteur-pure-id (RemapADI.axl:163), the reconstruction's
                                         limiter in pure neighbourhoods, and the gradient's when it is 1 */
   int32_t conservation_energie_totale; /* 0; 1: conservation-energie-totale (RemapADI.axl:151;

@@ -20,6 +20,7 @@ def _mixed(c):
 @pytest.mark.parametrize("make", [
     lambda: gen.sedov(n=14, jitter=0.01, seed=2, cycles=60),
     lambda: gen.two_material(24, 12, 12, cycles=60, seed=9),
+    lambda: gen.two_material(24, 12, 12, cycles=60, seed=9, options=gen.Options(ordre_projection=3)),
     lambda: _mixed(gen.sod(nx=40, ny=6, nz=5, jitter=0.01, seed=3, cycles=60)),
 ])
 def test_resume_equals_uninterrupted_run(make):

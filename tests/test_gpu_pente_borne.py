@@ -100,9 +100,75 @@ def test_unsupported_pente_borne_options_are_refused(opts, code):
     assert code_of(lambda: Context(gen.sod(cycles=1, options=gen.Options(**opts)))) == code
 
 
-def test_pente_borne_refused_for_several_environments_and_batches():
-    opts = gen.Options(pente_borne=1)
-    assert code_of(lambda: Context(gen.two_material(16, 8, 8, cycles=1, options=opts))) == ERR_UNSUPPORTED
+# Two gases (debar fix, projection-limiteur-id): the settings whose oracle run
+# keeps a sane dt for 40 cycles.  With debar fix 0 an environment's mass flux
+# lacks its volume fraction, and with pente-borne-mixte the pure cells keep
+# that raw mass flux while an environment absent from a cell keeps the Phi of
+# the previous remap (PrepareRemap.cc:201-212 sets only the cell's
+# environments): there the oracle's dt collapses within a few cycles (to
+# 1e-31 by cycle 2 for some settings), and the device follows it bit for bit.
+SANE_FORMS = [(1, 0), (1, 1), (1, 5), (2, 2), (2, 6)]
+# (debar fix, limiteur-pure-id, projection-limiteur-id) with pente-borne-mixte,
+# run with deltat-min 0 for 10 cycles, during which the fields stay finite
+MIXTE_FORMS = [(1, 1, 0), (1, 2, 5), (1, 4, 6), (2, 4, 2), (2, 1, 1), (0, 2, 1)]
+
+
+@pytest.mark.parametrize("debar,limiter", SANE_FORMS)
+def test_pente_borne_two_gases_bitwise(debar, limiter):
+    """Several environments: Phi of PrepareRemap.cc:201-212 for the cell's
+    environments (the others keep the last sweep's), every component's
+    reconstruction and the debar fix over the environments."""
+    opts = gen.Options(pente_borne=1, pente_borne_debar_fix=debar, projection_limiteur_id=limiter)
+    compare(gen.two_material(32, 16, 16, cycles=40, seed=9, options=opts), 40, 10)
+
+
+@pytest.mark.parametrize("debar,pure_id,limiter", MIXTE_FORMS)
+def test_pente_borne_mixte_two_gases_bitwise(debar, pure_id, limiter):
+    """pente-borne-mixte with two gases: the pure-neighbourhood choice cell
+    by cell (limiters of the gradient and of the reconstruction, the mass
+    flux left out of the debar fix), from the mixed/pure indicators of the
+    previous remap on the first sweep and of the sweep's Phi afterwards."""
+    opts = gen.Options(pente_borne=1, pente_borne_debar_fix=debar, pente_borne_mixte=1, limiteur_pure_id=pure_id,
+                       projection_limiteur_id=limiter, deltat_min=0.0)
+    compare(gen.two_material(32, 16, 16, cycles=10, seed=9, options=opts), 10, 2)
+
+
+def test_pente_borne_debar0_two_gases_collapse_bitwise():
+    """Debar fix 0 with two gases: the dt collapses (1e-17 at cycle 2) on both sides alike."""
+    opts = gen.Options(pente_borne=1, pente_borne_debar_fix=0, deltat_min=0.0)
+    compare(gen.two_material(32, 16, 16, cycles=4, seed=9, options=opts), 4, 2)
+
+
+@pytest.mark.parametrize("debar", [1, 2])
+def test_pente_borne_three_gases_bitwise(debar):
+    compare(gen.three_material(cycles=30, options=gen.Options(pente_borne=1, pente_borne_debar_fix=debar)), 30, 10)
+
+
+@pytest.mark.parametrize("limiter", [2, 5])
+def test_pure_limiter_switch_two_gases_bitwise(limiter):
+    """projection-pente-borne-mixte alone with two gases: superBee on the
+    cells whose neighbourhood is pure, projection-limiteur-id elsewhere."""
+    opts = gen.Options(pente_borne_mixte=1, limiteur_pure_id=1, projection_limiteur_id=limiter)
+    compare(gen.two_material(32, 16, 16, cycles=40, seed=9, options=opts), 40, 20)
+
+
+def test_pente_borne_two_gases_restart_dump():
+    """The pente-borne Phi of absent environments and the mixed/pure
+    indicators travel in the restart dump."""
+    opts = gen.Options(pente_borne=1, pente_borne_debar_fix=1, pente_borne_mixte=1, limiteur_pure_id=2,
+                       projection_limiteur_id=5, deltat_min=0.0)
+    case = gen.two_material(32, 16, 16, cycles=10, seed=9, options=opts)
+    a = Context(case)
+    a.step(5)
+    blob = a.save_checkpoint()
+    b = Context.from_checkpoint(case, blob)
+    a.step(5)
+    b.step(5)
+    for f in FIELDS:
+        assert np.array_equal(a.field(f), b.field(f)), f
+
+
+def test_pente_borne_refused_for_batches():
     cases = gen.batched(count=2, seed=3, side_lo=8, side_hi=10, cycles=1)
     cases[1].options.pente_borne = 1
     assert code_of(lambda: Batch(cases)) == ERR_UNSUPPORTED
