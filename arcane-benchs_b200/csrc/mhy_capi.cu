@@ -228,8 +228,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
       return fail(MHY_ERR_ARG, "bad boundary condition");
   if (opt->conservation_energie_totale != 0 && opt->conservation_energie_totale != 1)
     return fail(MHY_ERR_ARG, "conservation_energie_totale must be 0 or 1");
-  if (opt->conservation_energie_totale && (opt->nb_env != 1 || opt->precision != 0))
-    return fail(MHY_ERR_UNSUPPORTED, "conservation-energie-totale: one environment in FP64 on the device");
+  if (opt->conservation_energie_totale && opt->precision != 0)
+    return fail(MHY_ERR_UNSUPPORTED, "conservation-energie-totale: FP64 on the device");
 
   mhy_ctx* c = new mhy_ctx();
   for (int k = 0; k < MHY_TUNE_SLOTS; ++k) {
@@ -369,7 +369,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   err = cudaMemcpyAsync(c->S, &s0, sizeof(s0), cudaMemcpyHostToDevice, c->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
-  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv + (opt->ordre_projection == 3 ? 3 : 0)
+  c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv + (opt->ordre_projection == 3 ? 3 : 0) +
+                                     (opt->conservation_energie_totale ? 1 : 0)
                                : kKernelsPerCycle + (opt->schema_csts ? 2 : 0) + (opt->ordre_projection == 3 ? 3 : 0) +
                                      (opt->conservation_energie_totale ? 1 : 0);
   *out = c;
@@ -556,6 +557,7 @@ int launch_remap_(mhy_ctx* c, int sens, KernelMarks* m = nullptr) {
     if (c->ph.cons_ec) launch_cons_ec(c->args(), c->stream);   // after the last node sweep, before dt
   } else {
     launch_remap_env(c->args(), sens, c->stream, m);
+    if (c->ph.cons_ec) launch_cons_ec_env(c->args(), c->stream);   // after the last node sweep, before dt
   }
   return MHY_OK;
 }

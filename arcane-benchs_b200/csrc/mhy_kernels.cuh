@@ -126,6 +126,7 @@ struct KernelMarks;
 void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 void launch_delta_t(const CycleArgs& a, cudaStream_t s);
 void launch_cons_ec(const CycleArgs& a, cudaStream_t s);
+void launch_cons_ec_env(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycle = 10;
 // meshes with 2..kMaxEnvDevice environments (mhy_multi.cu)
 constexpr int kMaxEnvDevice = 4;

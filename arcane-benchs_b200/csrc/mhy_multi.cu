@@ -669,16 +669,19 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
     if (!(mask >> k & 1)) continue;
     if (r[k] < 0. || e[k] < 0.) { e[k] = 0.; r[k] = 0.; f[k] = 0.; x[k] = 0.; }
   }
+  // conservation-energie-totale: the energies change once the node terms are
+  // known (k_env_cons_ec, after the last node sweep), which then applies the EOS
+  const bool eos_now = !ph.cons_ec;
   double pk[K], ck[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     pk[k] = ck[k] = 0.;
-    if (!(mask >> k & 1)) continue;
+    if (!(mask >> k & 1) || !eos_now) continue;
     eos_pc(env.eos[k], env.gamma[k], env.pinf[k], r[k], e[k], pk[k], ck[k]);
   }
   if (pure) {
     st.rho[c] = r[ke]; st.e[c] = e[ke]; st.q[c] = q[ke]; st.mass[c] = m[ke];
-    st.p[c] = pk[ke]; st.cs[c] = ck[ke];
+    if (eos_now) { st.p[c] = pk[ke]; st.cs[c] = ck[ke]; }
     env.fg[c] = f[ke]; env.xg[c] = x[ke];
   } else {
     double pm = 0., cm = 1.e-20;
@@ -693,8 +696,61 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
     }
     if (est_mixte) st.rho[c] = density_nplus1;
     st.e[c] = energie_nplus1; st.q[c] = pseudo_nplus1; st.mass[c] = cell_mass;
-    st.p[c] = pm; st.cs[c] = cm;
+    if (eos_now) { st.p[c] = pm; st.cs[c] = cm; }
   }
+}
+
+// conservation-energie-totale with K environments (RemapADIFinal.cc:751-773,
+// then PerfectGasEOSService.cc:72-136 and MahycoModule.cc:1836-1915): the
+// kinetic energy the dual remap lost, summed over the cell's 8 nodes in
+// cell-node order (each node's 0.25 (U_dual[4]/U_dual[3] - 0.5 |v|^2) from
+// the last node sweep), floored at 0, added as x_k delta to every
+// environment's specific energy and as delta to a mixed cell's mean; then the
+// EOS of every environment and the mixed-cell pressure and sound speed.  A
+// pure cell's environment values are its global values.
+template <int K>
+__global__ void __launch_bounds__(128) k_env_cons_ec(Dims dm, Phys ph, EnvState env, CellState st,
+                                                     const double* __restrict__ ecn, int linear) {
+  int i, j, k;
+  if (!block_item(dm.nx, dm.ny, dm.nz, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, i, j, k)) return;
+  const int C = (int)dm.C;
+  const int c = (int)dm.cid(i, j, k);
+  double delta_ec = 0.;
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    delta_ec += ecn[dm.nid(i + kCellNodeOff[a][0], j + kCellNodeOff[a][1], k + kCellNodeOff[a][2])];
+  delta_ec = smax(0., delta_ec);
+  const uint32_t mask = env.mask[c];
+  if (__popc(mask) == 1) {
+    const int ke = __ffs(mask) - 1;
+    const double en = st.e[c] + env.xg[c] * delta_ec;
+    double pr, cc;
+    eos_pc(env.eos[ke], env.gamma[ke], env.pinf[ke], st.rho[c], en, pr, cc);
+    st.e[c] = en; st.p[c] = pr; st.cs[c] = cc;
+    return;
+  }
+  double pm = 0., cm = 1.e-20;
+#pragma unroll
+  for (int kk = 0; kk < K; ++kk) {
+    if (!(mask >> kk & 1)) continue;
+    const int o = kk * C + c;
+    const double ek = env.e[o] + env.x[o] * delta_ec;
+    double pr, cc;
+    eos_pc(env.eos[kk], env.gamma[kk], env.pinf[kk], env.rho[o], ek, pr, cc);
+    env.e[o] = ek; env.p[o] = pr; env.cs[o] = cc;
+    pm += env.f[o] * pr;
+    cm = amax(cc, cm);
+  }
+  st.e[c] += delta_ec;
+  st.p[c] = pm; st.cs[c] = cm;
+}
+
+void launch_cons_ec_env(const CycleArgs& a, cudaStream_t s) {
+  int linear;
+  const dim3 nbc = cell_grid(a.dm, linear);
+  if (a.K == 2) k_env_cons_ec<2><<<nbc, 128, 0, s>>>(a.dm, a.ph, a.env, a.st, a.ecn, linear);
+  else if (a.K == 3) k_env_cons_ec<3><<<nbc, 128, 0, s>>>(a.dm, a.ph, a.env, a.st, a.ecn, linear);
+  else k_env_cons_ec<4><<<nbc, 128, 0, s>>>(a.dm, a.ph, a.env, a.st, a.ecn, linear);
 }
 
 // Initial thermodynamic state of a K-environment mesh, after the initial

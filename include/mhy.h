@@ -103,8 +103,9 @@ typedef struct mhy_options {
                                         RemapADIFinal.cc:751-773): after the remap each cell's specific
                                         internal energy gains max(0, sum over its 8 nodes of
                                         0.25 (U_dual[4]/U_dual[3] - 0.5 |v|^2)) times its mass fraction,
-                                        with U_dual[4] = 0.5 m |v| as the reference builds it; one
-                                        environment, precision 0, not batched */
+                                        with U_dual[4] = 0.5 m |v| as the reference builds it (each
+                                        environment's energy gains x_k delta, a mixed cell's mean delta);
+                                        precision 0, not batched */
 } mhy_options;
 
 /* Structured hexahedral mesh: (nx+1)(ny+1)(nz+1) nodes, node (i,j,k) at

@@ -1,6 +1,7 @@
 """GPU: the conservation-energie-totale remap option (RemapADI.axl:151,
-RemapADIFinal.cc:751-773) for one environment in FP64, bit for bit against
-the oracle: Sod, jittered Sedov, with schema-csts, order 3 and a stiffened gas.
+RemapADIFinal.cc:751-773) in FP64, bit for bit against the oracle: Sod,
+jittered Sedov, with schema-csts, order 3 and a stiffened gas; two and three
+gases.
 
 After the remap each cell's specific internal energy gains max(0, sum over its
 8 nodes of 0.25 (U_dual[4] / U_dual[3] - 0.5 |v|^2)) times its mass fraction,
@@ -76,10 +77,27 @@ def test_cons_ec_with_other_options_bitwise(variant):
         assert np.array_equal(o.field(f), g.field(f)), f
 
 
+@pytest.mark.parametrize("make,cycles", [
+    (lambda: gen.two_material(32, 16, 16, cycles=60, seed=9), 60),
+    (lambda: gen.three_material(cycles=40), 40),
+    (lambda: gen.two_material(24, 12, 12, cycles=40, seed=3, options=gen.Options(ordre_projection=3)), 40),
+], ids=["two_gases", "three_gases", "two_gases_order3"])
+def test_cons_ec_several_environments_bitwise(make, cycles):
+    """Several environments: each environment's energy gains x_k delta, a
+    mixed cell's mean gains delta, then every environment's EOS and the
+    mixed-cell pressure and sound speed (RemapADIFinal.cc:751-773)."""
+    case = _ec(make())
+    o, g, dto, dtg = _run(case, cycles)
+    assert dto == dtg
+    for f in FIELDS:
+        assert np.array_equal(o.field(f), g.field(f)), f
+    for k in range(case.nenv):
+        for w in ("fracvol", "density", "internal_energy"):
+            assert np.array_equal(o.env_field(w, k), g.env_field(w, k)), (w, k)
+    assert g.kernels_per_cycle() == (15 if case.options.ordre_projection == 3 else 12)
+
+
 def test_cons_ec_refused_where_not_built():
-    two = _ec(gen.two_material(16, 8, 8, cycles=2))
-    with pytest.raises(MhyError):
-        Context(two)
     mixed = _ec(gen.sod(cycles=2))
     mixed.options.precision = 1
     with pytest.raises(MhyError):
