@@ -209,8 +209,8 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
     return fail(MHY_ERR_ARG, "cfl, deltat-init, deltat-max and final-time must be > 0, deltat-min and threshold >= 0");
   if (opt->precision < 0 || opt->precision > 1) return fail(MHY_ERR_ARG, "precision must be 0 (FP64) or 1 (mixed)");
   if (opt->schema_csts != 0 && opt->schema_csts != 1) return fail(MHY_ERR_ARG, "schema_csts must be 0 or 1");
-  if (opt->schema_csts && (opt->nb_env != 1 || opt->precision != 0))
-    return fail(MHY_ERR_UNSUPPORTED, "schema-csts: one environment in FP64 on the device");
+  if (opt->schema_csts && opt->precision != 0)
+    return fail(MHY_ERR_UNSUPPORTED, "schema-csts: FP64 on the device");
   if (opt->projection_pente_borne != 0 && opt->projection_pente_borne != 1)
     return fail(MHY_ERR_ARG, "projection_pente_borne must be 0 or 1");
   if (opt->pente_borne_mixte != 0 && opt->pente_borne_mixte != 1)
@@ -370,7 +370,7 @@ int mhy_create(const mhy_mesh_desc* mesh, const mhy_options* opt, int device, mh
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
   if (err != cudaSuccess) { mhy_destroy(c); return fail(MHY_ERR_CUDA, cudaGetErrorString(err)); }
   c->kernels_per_cycle = K > 1 ? kKernelsPerCycleEnv + (opt->ordre_projection == 3 ? 3 : 0) +
-                                     (opt->conservation_energie_totale ? 1 : 0)
+                                     (opt->conservation_energie_totale ? 1 : 0) + (opt->schema_csts ? 2 : 0)
                                : kKernelsPerCycle + (opt->schema_csts ? 2 : 0) + (opt->ordre_projection == 3 ? 3 : 0) +
                                      (opt->conservation_energie_totale ? 1 : 0);
   *out = c;
@@ -556,6 +556,7 @@ int launch_remap_(mhy_ctx* c, int sens, KernelMarks* m = nullptr) {
     launch_remap(c->args(), sens, c->stream, m);
     if (c->ph.cons_ec) launch_cons_ec(c->args(), c->stream);   // after the last node sweep, before dt
   } else {
+    if (c->ph.csts) launch_csts_forward(c->args(), c->stream);   // PrepareRemap.cc:456, then the face velocities
     launch_remap_env(c->args(), sens, c->stream, m);
     if (c->ph.cons_ec) launch_cons_ec_env(c->args(), c->stream);   // after the last node sweep, before dt
   }

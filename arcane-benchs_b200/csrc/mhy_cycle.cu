@@ -488,8 +488,8 @@ void launch_csts_forward(const CycleArgs& a, cudaStream_t s) {
   k_csts_face_u<<<(unsigned)((a.dm.F + 127) / 128), 128, 0, s>>>(a.dm, a.vf, a.vnb, a.n0, a.fd);
 }
 
-// The schema-csts form of the one-environment FP64 cell kernel.
-template <bool HC>
+// The schema-csts form of the FP64 cell kernel (K environments).
+template <int K, bool HC>
 __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells_csts(Dims dm,
     const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
@@ -498,8 +498,19 @@ __global__ void __launch_bounds__(128, 3) k_cyc_lagrange_cells_csts(Dims dm,
     double* __restrict__ cqs, double* __restrict__ L, double* __restrict__ U,
     double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag, int linear,
     const double* __restrict__ vnb, double* __restrict__ pf) {
-  k_cyc_lagrange_cells_body<1, double, true, HC>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, nullptr, L, U, xcs, fd,
+  k_cyc_lagrange_cells_body<K, double, true, HC>(dm, S, ph, x0, vh, n0, rho, e, q, p, cs, mass, cqs, nullptr, L, U, xcs, fd,
                                              env, Vlag, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, vnb, pf);
+}
+
+void launch_lagrange_cells_csts_env(const CycleArgs& a, cudaStream_t s) {
+  int linear;
+  const dim3 nbc = cell_grid(a.dm, linear);
+  const bool hc = a.fd.h != nullptr;
+  auto kern = a.K == 2 ? (hc ? k_cyc_lagrange_cells_csts<2, true> : k_cyc_lagrange_cells_csts<2, false>)
+            : a.K == 3 ? (hc ? k_cyc_lagrange_cells_csts<3, true> : k_cyc_lagrange_cells_csts<3, false>)
+                       : (hc ? k_cyc_lagrange_cells_csts<4, true> : k_cyc_lagrange_cells_csts<4, false>);
+  kern<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs, a.st.mass,
+                           a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, linear, a.vnb, a.pf);
 }
 
 // Cell kernels: rows of 128 cells when nx is a multiple of 128, else 128
@@ -515,7 +526,7 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
   const dim3 nbc = cell_grid(a.dm, linear);
   const bool hc = a.fd.h != nullptr;               // cell widths: order 3 or the generalised limiters
   if (a.ph.csts) {
-    auto kern = hc ? k_cyc_lagrange_cells_csts<true> : k_cyc_lagrange_cells_csts<false>;
+    auto kern = hc ? k_cyc_lagrange_cells_csts<1, true> : k_cyc_lagrange_cells_csts<1, false>;
     kern<<<nbc, 128, 0, s>>>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs, a.st.mass,
                              a.cqs, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, linear, a.vnb, a.pf);
   } else if (hc && !a.ph.precision) {

@@ -127,6 +127,7 @@ void launch_remap(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* mar
 void launch_delta_t(const CycleArgs& a, cudaStream_t s);
 void launch_cons_ec(const CycleArgs& a, cudaStream_t s);
 void launch_cons_ec_env(const CycleArgs& a, cudaStream_t s);
+void launch_lagrange_cells_csts_env(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycle = 10;
 // meshes with 2..kMaxEnvDevice environments (mhy_multi.cu)
 constexpr int kMaxEnvDevice = 4;

@@ -168,6 +168,46 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
   }
 }
 
+// schema-csts energy of one environment of a cell (MahycoModule.cc:1776-1810,
+// updateEnergyAndPressureforGP; or by Newton on f, :1552-1613 with
+// MahycoModule.h:433-445, the first iteration always run as in newton_eint).
+// cn1, cn, cdn, con: the corner-vector sums v.cqs dt, v.cqs_n dt,
+// (v - v_n).cqs_n (dt - dt_old), v_n.cqs_n dt_old.  The n-1 pseudo-viscosity
+// is zero: the remap resets the n-level fields (PrepareRemap.cc:485-550)
+// before saveValuesAtN copies them into it.  pf gets the pressure that
+// updateVelocityForward reads: p_n, or the last Newton EOS value; the
+// kernel stores it plus this cycle's pseudo-viscosity.  g, eos, pinf: the
+// environment's adiabatic constant, EOS and limit tension.
+__device__ __forceinline__ double csts_eint(const Phys& ph, double g, int eos, double pinf, double cn1, double cn,
+                                            double cdn, double con, double e0, double r, double m, double pn,
+                                            double qn, double q, double& pf) {
+  const double qnm1 = 0.;
+  if (!ph.with_newton) {
+    const double denom = 1 + 0.5 * (g - 1.0) * r * cn1 / m;
+    const double numer = e0 - (0.5 * (pn + qn) * cn / m) - (0.5 * q * cn1 / m) + (0.25 * (pn + qn) * cdn / m) -
+                         (0.5 * (qn - qnm1) * con / m);
+    pf = pn;
+    return numer / denom;
+  }
+  const double cdon = 0., epsilon = ph.threshold, itermax = 50;
+  const double en = e0;
+  double e = en, pp, dpde;
+  int i = 0;
+  do {
+    if (eos == 1) pp = ((g - 1.) * r * e) - (g * pinf);
+    else pp = (g - 1.) * r * e;
+    dpde = (g - 1.) * r;
+    const double fe = e - en + 0.5 * (pp + q) * cn1 / m + 0.5 * (pn + qn) * cn / m - 0.25 * (pn + qn) * cdn / m +
+                      0.5 * (q - qnm1) * cdon / m;
+    const double enew = e - fe / (1. + 0.5 * dpde * cn1 / m);
+    e = enew;
+    i++;
+  } while (i < itermax && fabs(e - en + 0.5 * (pp + q) * cn1 / m + 0.5 * (pn + qn) * cn / m -
+                                0.25 * (pn + qn) * cdn / m + 0.5 * (q - qnm1) * cdon / m) >= epsilon);
+  pf = pp;
+  return e;
+}
+
 // Lagrange thermodynamics of a mesh with K > 1 environments, then the remap
 // variables (MahycoModule.cc:1331-1426 updateDensity, :454-578
 // computeArtificialViscosity, :1659-1770 updateEnergyAndPressureforGP,
@@ -181,14 +221,19 @@ __device__ __forceinline__ void face_data(const Dims& dm, int i, int j, int k, c
 // pbphi (pente-borne): Phi of the first sweep for the cell's environments,
 // volume fraction, density and internal energy after this step, and q of
 // the last of them (PrepareRemap.cc:201-212); the other environments' planes
-// are left as they are.
-template <int K>
+// are left as they are.  CSTS: each environment's energy by csts_eint from
+// the cell's corner-vector sums cssum (cn1, cn, cdn, con), and pf = the
+// global p + q the forward step reads (MahycoModule.cc:792-831): a pure
+// cell's p_n or Newton pressure plus its q, a mixed cell's mean p_n plus
+// sum_k f_k q_k (MahycoModule.cc:454-578).
+template <int K, bool CSTS = false>
 __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalars* S, const EnvState& env, int c,
                                                     int C, double V, double Lc, double* __restrict__ rho,
                                                     const double* __restrict__ e, const double* __restrict__ q,
                                                     const double* __restrict__ p, const double* __restrict__ cs,
                                                     const double* __restrict__ mass, double* __restrict__ U,
-                                                    double* __restrict__ Vlag, double* __restrict__ pbphi) {
+                                                    double* __restrict__ Vlag, double* __restrict__ pbphi,
+                                                    const double* cssum = nullptr, double* __restrict__ pf = nullptr) {
   constexpr int NV = 3 * K + 1;
   const double inv_deltat = S->inv_dt;
   const double rn = rho[c];
@@ -207,8 +252,16 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
     const double g = env.gamma[ke];
     double qn = 0.;
     if (du < 0.0) qn = itau * (-0.5 * Lc * cs[c] * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-    const double en = energy_update(ph.with_newton != 0, pc, env.eos[ke], g, env.pinf[ke], ph.threshold, q[c], qn, ind,
-                                    irn, nd, p[c], e[c]);
+    double en;
+    if constexpr (CSTS) {
+      double pforward;
+      en = csts_eint(ph, g, env.eos[ke], env.pinf[ke], cssum[0], cssum[1], cssum[2], cssum[3], e[c], nd, mass[c],
+                     p[c], q[c], qn, pforward);
+      pf[c] = pforward + qn;
+    } else {
+      en = energy_update(ph.with_newton != 0, pc, env.eos[ke], g, env.pinf[ke], ph.threshold, q[c], qn, ind, irn, nd,
+                         p[c], e[c]);
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k == ke) { u[k] = V; u[K + k] = V * nd; u[2 * K + k] = V * nd * en; }
@@ -219,6 +272,7 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
     }
   } else {
     const double csc = cs[c];
+    double qg = 0.;                                              // the mixed cell's pseudo-viscosity sum_k f_k q_k
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (!(mk >> k & 1)) continue;
@@ -230,8 +284,16 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
       const double g = env.gamma[k];
       double qk = 0.;
       if (du < 0.0) qk = 1. / tauk * (-0.5 * Lc * csc * du + (g + 1) / 2.0 * Lc * Lc * du * du);
-      const double ek = energy_update(ph.with_newton != 0, pc, env.eos[k], g, env.pinf[k], ph.threshold, env.q[o], qk,
-                                      irk, irnk, rk, env.p[o], env.e[o]);
+      double ek;
+      if constexpr (CSTS) {
+        double pk_unused;
+        ek = csts_eint(ph, g, env.eos[k], env.pinf[k], cssum[0], cssum[1], cssum[2], cssum[3], env.e[o], rk, env.m[o],
+                       env.p[o], env.q[o], qk, pk_unused);
+        qg += qk * env.f[o];
+      } else {
+        ek = energy_update(ph.with_newton != 0, pc, env.eos[k], g, env.pinf[k], ph.threshold, env.q[o], qk, irk, irnk,
+                           rk, env.p[o], env.e[o]);
+      }
       u[k] = vk;
       u[K + k] = vk * rk;
       u[2 * K + k] = vk * rk * ek;
@@ -240,6 +302,7 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
         pbphi[o] = env.f[o]; pbphi[K * C + o] = rk; pbphi[2 * K * C + o] = ek; pbphi[3 * K * C + c] = qk;
       }
     }
+    if constexpr (CSTS) pf[c] = p[c] + qg;                      // the mean p_n: no EOS runs before the forward step
   }
 #pragma unroll
   for (int v = 0; v < NV; ++v) U[v * C + c] = u[v];
@@ -247,46 +310,9 @@ __device__ __forceinline__ void lagrange_thermo_env(const Phys& ph, const Scalar
   rho[c] = nd;
 }
 
-// schema-csts energy of a one-environment cell (MahycoModule.cc:1776-1810,
-// updateEnergyAndPressureforGP; or by Newton on f, :1552-1613 with
-// MahycoModule.h:433-445, the first iteration always run as in newton_eint).
-// cn1, cn, cdn, con: the corner-vector sums v.cqs dt, v.cqs_n dt,
-// (v - v_n).cqs_n (dt - dt_old), v_n.cqs_n dt_old.  The n-1 pseudo-viscosity
-// is zero: the remap resets the n-level fields (PrepareRemap.cc:485-550)
-// before saveValuesAtN copies them into it.  pf gets the pressure that
-// updateVelocityForward reads: p_n, or the last Newton EOS value; the
-// kernel stores it plus this cycle's pseudo-viscosity.
-__device__ __forceinline__ double csts_eint(const Phys& ph, double cn1, double cn, double cdn, double con, double e0,
-                                            double r, double m, double pn, double qn, double q, double& pf) {
-  const double g = ph.gamma, qnm1 = 0.;
-  if (!ph.with_newton) {
-    const double denom = 1 + 0.5 * (g - 1.0) * r * cn1 / m;
-    const double numer = e0 - (0.5 * (pn + qn) * cn / m) - (0.5 * q * cn1 / m) + (0.25 * (pn + qn) * cdn / m) -
-                         (0.5 * (qn - qnm1) * con / m);
-    pf = pn;
-    return numer / denom;
-  }
-  const double cdon = 0., epsilon = ph.threshold, itermax = 50;
-  const double en = e0;
-  double e = en, pp, dpde;
-  int i = 0;
-  do {
-    if (ph.eos == 1) pp = ((g - 1.) * r * e) - (g * ph.pinf);
-    else pp = (g - 1.) * r * e;
-    dpde = (g - 1.) * r;
-    const double fe = e - en + 0.5 * (pp + q) * cn1 / m + 0.5 * (pn + qn) * cn / m - 0.25 * (pn + qn) * cdn / m +
-                      0.5 * (q - qnm1) * cdon / m;
-    const double enew = e - fe / (1. + 0.5 * dpde * cn1 / m);
-    e = enew;
-    i++;
-  } while (i < itermax && fabs(e - en + 0.5 * (pp + q) * cn1 / m + 0.5 * (pn + qn) * cn / m -
-                                0.25 * (pn + qn) * cdn / m + 0.5 * (q - qnm1) * cdon / m) >= epsilon);
-  pf = pp;
-  return e;
-}
 
-// CSTS (schema-csts, one environment, FP64 only): vnb = the backward node
-// velocity of this cycle, pf = the pressure for the forward step.
+// CSTS (schema-csts, FP64 only): vnb = the backward node velocity of this
+// cycle, pf = the pressure plus pseudo-viscosity of the forward step.
 template <int K, typename R, bool CSTS = false, bool HC = false>
 __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars* __restrict__ S, Phys ph,
     const double* __restrict__ x0, const double* __restrict__ vh, const double* __restrict__ n0,
@@ -295,7 +321,7 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     double* __restrict__ cqs, float* __restrict__ cqs32, double* __restrict__ L, double* __restrict__ U,
     double* __restrict__ xcs, FaceData fd, EnvState env, double* __restrict__ Vlag,
     int bx_, int by_, int bz_, const double* __restrict__ vnb = nullptr, double* __restrict__ pf = nullptr) {
-  static_assert(!CSTS || (K == 1 && sizeof(R) == 8), "schema-csts: one environment, FP64");
+  static_assert(!CSTS || sizeof(R) == 8, "schema-csts: FP64");
   int i, j, k;
   if (!block_item(dm.nx, dm.ny, dm.nz, bx_, by_, bz_, i, j, k)) return;
   const long long c = dm.cid(i, j, k);
@@ -395,7 +421,8 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     double en;
     if constexpr (CSTS) {
       double pforward;
-      en = csts_eint(ph, cs_cn1, cs_cn, cs_cdn, cs_con, e[c], nd, mass[c], p[c], q[c], qn, pforward);
+      en = csts_eint(ph, g, ph.eos, ph.pinf, cs_cn1, cs_cn, cs_cdn, cs_con, e[c], nd, mass[c], p[c], q[c], qn,
+                     pforward);
       pf[c] = pforward + qn;                                    // the forward force's p + q (q: this cycle's)
     } else {
       en = energy_update(ph.with_newton != 0, ph.pseudo_centree != 0, ph.eos, g, ph.pinf, ph.threshold, q[c], qn, ind,
@@ -407,7 +434,9 @@ __device__ __forceinline__ void k_cyc_lagrange_cells_body(Dims dm, const Scalars
     U[3 * C + c] = V * qn;
     if (fd.pbphi) { fd.pbphi[c] = nd; fd.pbphi[C + c] = en; fd.pbphi[2 * C + c] = qn; }
   } else {
-    lagrange_thermo_env<K>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag, fd.pbphi);
+    const double cssum[4] = {cs_cn1, cs_cn, cs_cdn, cs_con};
+    lagrange_thermo_env<K, CSTS>(ph, S, env, (int)c, (int)C, V, Lc, rho, e, q, p, cs, mass, U, Vlag, fd.pbphi, cssum,
+                                 pf);
   }
   if constexpr (F32) face_data<float>(dm, i, j, k, xr, F3{0.f, 0.f, 0.f}, n0, vh, fd);
   else face_data<double, HC>(dm, i, j, k, x, xc, n0, vh, fd);

@@ -922,6 +922,7 @@ static void lagrange_cells_env(const CycleArgs& a, const dim3 nbc, int linear, c
 }
 
 void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
+  if (a.ph.csts) { launch_lagrange_cells_csts_env(a, s); return; }
   int linear;
   const dim3 nbc = cell_grid(a.dm, linear);
   if (a.ph.precision) {
@@ -935,7 +936,11 @@ void launch_lagrange_cells_env(const CycleArgs& a, cudaStream_t s) {
   }
 }
 
-void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks* m) {
+void launch_remap_env(const CycleArgs& a0, int sens, cudaStream_t s, KernelMarks* m) {
+  // schema-csts: the remap starts from the forward velocity (U_dual,
+  // Phi_dual, PrepareRemap.cc:411-433) on the Lagrangian coordinates
+  CycleArgs a = a0;
+  if (a.ph.csts) a.vh = a.vf;
   if (a.ph.precision) {
     if (a.K == 2) remap_env<2, float>(a, sens, s, m);
     else if (a.K == 3) remap_env<3, float>(a, sens, s, m);

@@ -87,7 +87,7 @@ typedef struct mhy_options {
   int32_t schema_csts;               /* 0; 1: the CSTS time scheme (Mahyco.axl:238): velocity taken back to n-1/2
                                         before the Lagrange step and forward to n+1 before the remap, energy from
                                         the corner vectors of n and n+1 (MahycoModule.cc:693-831, 1776-1810,
-                                        PrepareRemap.cc:69-79, 456); one environment, precision 0 */
+                                        PrepareRemap.cc:69-79, 456); precision 0 */
   int32_t projection_pente_borne;    /* 0; 1: the pente-borne remap (RemapADI.axl:167; RemapADIService.cc:319-437,
                                         530-581, 745-840; UtilesRemap.cc:73-93, 184-296, 406-823): fluxes
                                         integrated from a three-piece reconstruction; precision 0,
