@@ -772,7 +772,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   if (!meshes || !opts || !out || n <= 0) return fail(MHY_ERR_ARG, "null argument or empty batch");
   *out = nullptr;
   for (int i = 0; i < n; ++i) {
-    if (opts[i].nb_env != 1) return fail(MHY_ERR_UNSUPPORTED, "batched instances must have one environment");
+    if (opts[i].nb_env != opts[0].nb_env)
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances share one number of environments");
     if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
     if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
     if (opts[i].projection_limiteur_id >= 3)
@@ -810,6 +811,7 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   b->plan.descs = b->d_descs;
   b->plan.ninst = n;
   b->plan.precision = opts[0].precision;
+  b->plan.K = opts[0].nb_env;
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
     b->plan.occ_pct[k] = 100;
     b->tuning.occupancy_pct[k] = 100;
@@ -914,6 +916,14 @@ constexpr int kNP = sizeof(kTunePcts) / sizeof(kTunePcts[0]);
 constexpr int kNL = sizeof(kLineOptions) / sizeof(kLineOptions[0]);
 inline bool line_slot(int k) {
   return k == BK_CELLS_Y || k == BK_CELLS_Z || k == BK_NODES_Y || k == BK_NODES_Z;
+}
+
+// The line counts a batch's sweeps are built for: any on one environment; with
+// several, 8 or 16 on the cell y/z sweeps and 8 on the node y/z sweeps.
+bool batch_tunable_lines(const mhy_batch* b, int k, int w) {
+  if (!line_slot(k)) return w == kLineWarps;
+  if (b->plan.K > 1) return w == kLineWarps || ((k == BK_CELLS_Y || k == BK_CELLS_Z) && w == 16);
+  return true;
 }
 
 // The line counts a context's sweeps are built for: 8, 16 or 32 on the y/z
@@ -1217,6 +1227,10 @@ int mhy_batch_set_tuning(mhy_batch* b, const mhy_tuning* t) {
   u.occupancy_pct[BK_DT_FINISH] = 100;
   DeviceScope on_dev(b->device);
   int rc = check_tuning(u);
+  for (int k = 0; k < BK_TUNE_SLOTS && rc == MHY_OK; ++k)
+    if (!batch_tunable_lines(b, k, u.lines_per_block[k]))
+      rc = fail(MHY_ERR_ARG, "lines_per_block: 8 or 16 on the cell y/z sweeps and 8 on the node y/z sweeps of a batch "
+                             "with several environments");
   if (rc == MHY_OK) rc = apply_tuning(b, u);
   if (rc == MHY_OK) b->tuning = u;
   return rc;
@@ -1255,7 +1269,7 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
         mhy_tuning t = default_tuning();
         for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
           if (k != BK_DT_FINISH) { t.order[k] = o; t.occupancy_pct[k] = kTunePcts[q]; }
-          if (line_slot(k)) t.lines_per_block[k] = kLineOptions[l];
+          if (line_slot(k)) t.lines_per_block[k] = batch_tunable_lines(b, k, kLineOptions[l]) ? kLineOptions[l] : kLineWarps;
         }
         tr.push_back(t);
       }
@@ -1304,7 +1318,9 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
   if (out) *out = best;
   return MHY_OK;
 }
-int mhy_batch_kernels_per_cycle(mhy_batch* b) { return b ? kKernelsPerCycleBatch : 0; }
+int mhy_batch_kernels_per_cycle(mhy_batch* b) {
+  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) : 0;   // several environments: the end-of-remap kernel
+}
 void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 int mhy_get_field(mhy_ctx* c, int field, void* dst, size_t bytes) {

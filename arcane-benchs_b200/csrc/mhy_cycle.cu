@@ -801,6 +801,10 @@ static int persistent_blocks(Kern kernel, int threads, size_t smem, int nwork, i
   return nwork < g ? (nwork > 0 ? nwork : 1) : g;
 }
 
+int persistent_grid(const void* kernel, int threads, size_t smem, int nwork, int pct) {
+  return persistent_blocks(kernel, threads, smem, nwork, pct);
+}
+
 void mark(KernelMarks* m, int kind, cudaStream_t s) {
   if (!m || m->n >= KernelMarks::kMax) return;
   cudaEventRecord(m->ev[m->n], s);
@@ -870,14 +874,27 @@ static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s, Kern
   else bat_nodes_d<DD, false, false, R>(P, it, prev, s, m);
 }
 
-void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
-  if (P.precision) {
+void launch_bat_lagrange_nodes(const BatchPlan& P, cudaStream_t s, KernelMarks* m) {
+  if (P.precision)
     launch_persistent(k_bat_lagrange_nodes<float>, 128, 0, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
-    launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  } else {
+  else
     launch_persistent(k_bat_lagrange_nodes<double>, 128, 0, P, BK_LNODES, BK_LNODES, s, m, P.descs, P.work[BK_LNODES], P.nwork[BK_LNODES]);
+}
+
+void launch_bat_dt(const BatchPlan& P, cudaStream_t s, KernelMarks* m) {
+  // the dt reduction walks the cell tiles of the Lagrange cell kernel
+  launch_persistent(k_bat_dt_min, 128, 0, P, BK_LCELLS, BK_DT_MIN, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  k_bat_dt_finish<<<(P.ninst + 127) / 128, 128, 0, s>>>(P.descs, P.ninst);
+  mark(m, BK_DT_FINISH, s);
+}
+
+void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
+  if (P.K > 1) { launch_batch_cycle_env(P, sens, s, m); return; }
+  launch_bat_lagrange_nodes(P, s, m);
+  if (P.precision)
+    launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  else
     launch_persistent(k_bat_lagrange_cells<double>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  }
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
@@ -892,10 +909,7 @@ void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMark
     }
     prev |= 1 << d;
   }
-  // the dt reduction walks the cell tiles of the Lagrange cell kernel
-  launch_persistent(k_bat_dt_min, 128, 0, P, BK_LCELLS, BK_DT_MIN, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  k_bat_dt_finish<<<(P.ninst + 127) / 128, 128, 0, s>>>(P.descs, P.ninst);
-  mark(m, BK_DT_FINISH, s);
+  launch_bat_dt(P, s, m);
 }
 
 }  // namespace mhy

@@ -155,6 +155,7 @@ struct BatchPlan {
   int precision;                // all instances share it
   int occ_pct[BK_TUNE_SLOTS];   // persistent grid of each slot: % of the resident-block capacity
   int lines[BK_COUNT];          // lines per block of the y/z sweeps (8, 16, 32); the work shapes follow it
+  int K;                        // environments of every instance
 };
 // Events recorded after each launch of a cycle (autotuning), with the tuning
 // slot of each launch.
@@ -167,6 +168,13 @@ struct KernelMarks {
 void batch_work_shape(const Dims& dm, int kind, int lines, int& gx, int& gy, int& gz);
 // Records an event after a launch (autotuning): slot `kind` of the marks.
 void mark(KernelMarks* m, int kind, cudaStream_t s);
+// Batched cycle helpers: the resident-block grid of a persistent kernel, the
+// Lagrange node kernel and the dt reduction of a batch (any K), and the
+// batched cycle of instances with K > 1 environments.
+int persistent_grid(const void* kernel, int threads, size_t smem, int nwork, int pct);
+void launch_bat_lagrange_nodes(const BatchPlan& P, cudaStream_t s, KernelMarks* m);
+void launch_bat_dt(const BatchPlan& P, cudaStream_t s, KernelMarks* m);
+void launch_batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m);
 void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 constexpr int kKernelsPerCycleBatch = 10;
 

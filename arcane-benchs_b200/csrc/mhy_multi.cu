@@ -285,16 +285,16 @@ __device__ __forceinline__ void env_cell_extras(const Phys& ph, const FaceData& 
 
 // K-environment cell sweep along x (lanes along the rows).
 template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
-__global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
+__device__ __forceinline__ void env_sweep_cells_x_body(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
-    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag, int bx_, int by_, int bz_) {
   constexpr int NV = 3 * K + 1;
   const int lane = threadIdx.x & 31;
-  const int j = blockIdx.y * kLineWarps + (threadIdx.x >> 5), k = blockIdx.z;
+  const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
   if (j >= dm.ny) return;                              // whole warp leaves together
   const int nd = dm.nx, C = (int)dm.C, F = (int)dm.F;
-  const int s = blockIdx.x * kLineUpd - 2 + lane;
+  const int s = bx_ * kLineUpd - 2 + lane;
   const bool valid = s >= 0 && s < nd;
   const bool inner = s >= 1 && s <= nd - 1;
   const bool infr = s + 1 <= nd - 1;
@@ -336,6 +336,15 @@ __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_ce
   for (int e = 0; e < K; ++e) dpf[e * C + c] = out[NV + e];
 }
 
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
+__global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_env_sweep_cells_x(Dims dm,
+    const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
+    const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
+  env_sweep_cells_x_body<K, FIRST, R, GL, O3, PB>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, Vlag, blockIdx.x,
+                                                 blockIdx.y, blockIdx.z);
+}
+
 // K-environment cell sweep along y (D = 1) or z (D = 2), staged through
 // shared memory exactly as the single-environment one (dynamic shared
 // memory: NA * kTileArr doubles).
@@ -344,17 +353,17 @@ __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 +
 
 // W: lines per block (8 or 16, the tuning; the register budget stays 128).
 template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false, bool O3 = false, bool PB = false>
-__global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_sweep_cells_t(Dims dm,
+__device__ __forceinline__ void env_sweep_cells_t_body(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
     const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
-    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag, int bx_, int by_, int bz_) {
   constexpr int NV = 3 * K + 1;
   constexpr int NA = env_cells_staged_arrays<K, FIRST>();
   constexpr int AX = NV, AF = NV + 3, AN = NV + 7, AO = NV + 10, AD = NV + 12;   // array offsets
   constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
   extern __shared__ double tile[];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int i0 = blockIdx.x * W, seg0 = blockIdx.y * kLineUpd - 2, o = blockIdx.z;
+  const int i0 = bx_ * W, seg0 = by_ * kLineUpd - 2, o = bz_;
   const int nd = dm.ncd(D), C = (int)dm.C, F = (int)dm.F;
   const int foff = D == 1 ? (int)dm.Fx : (int)(dm.Fx + dm.Fy);
   const int lb = D == 1 ? 2 : 0, lf = D == 1 ? 5 : 3;
@@ -431,6 +440,15 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
   for (int v = 0; v < NV; ++v) Uout[v * C + sc] = r[v * kTileArr];
 #pragma unroll
   for (int e = 0; e < K; ++e) dpf[e * C + sc] = r[(NV + e) * kTileArr];
+}
+
+template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false, bool O3 = false, bool PB = false>
+__global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_sweep_cells_t(Dims dm,
+    const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
+    const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag) {
+  env_sweep_cells_t_body<K, D, FIRST, R, W, GL, O3, PB>(dm, S, ph, fd, n0, xcs, ofn, Uin, Uout, dpf, Vlag, blockIdx.x,
+                                                       blockIdx.y, blockIdx.z);
 }
 
 // Order-3 face values of direction D for K environments
@@ -527,13 +545,11 @@ __global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __
 // (RemapADIService.cc:805-834); the next Lagrange step overwrites the cell's
 // environments, and the others keep these values into the next remap.
 template <int K>
-__global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __restrict__ S, Phys ph,
-                                                            EnvState env, const double* __restrict__ U,
-                                                            CellState st, FaceData fd) {
+__device__ __forceinline__ void env_finalize_cell(const Dims& dm, Scalars* __restrict__ S, const Phys& ph,
+                                                  const EnvState& env, const double* __restrict__ U,
+                                                  const CellState& st, const FaceData& fd, int c) {
   constexpr int NV = 3 * K + 1;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int C = (int)dm.C;
-  if (c >= C) return;
   double u[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u[v] = U[v * C + c];
@@ -698,6 +714,15 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
     st.e[c] = energie_nplus1; st.q[c] = pseudo_nplus1; st.mass[c] = cell_mass;
     if (eos_now) { st.p[c] = pm; st.cs[c] = cm; }
   }
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __restrict__ S, Phys ph,
+                                                            EnvState env, const double* __restrict__ U,
+                                                            CellState st, FaceData fd) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (int)dm.C) return;
+  env_finalize_cell<K>(dm, S, ph, env, U, st, fd, c);
 }
 
 // conservation-energie-totale with K environments (RemapADIFinal.cc:751-773,
@@ -949,6 +974,166 @@ void launch_remap_env(const CycleArgs& a0, int sens, cudaStream_t s, KernelMarks
     if (a.K == 2) remap_env<2, double>(a, sens, s, m);
     else if (a.K == 3) remap_env<3, double>(a, sens, s, m);
     else remap_env<4, double>(a, sens, s, m);
+  }
+}
+
+// ------------------------------------------------------------------------
+// Batched cycle of instances with K environments each: the same bodies as the
+// single-context kernels, driven by the batch's work tables over persistent
+// grids (as the one-environment batch in mhy_cycle.cu).  The cell y/z sweeps
+// take 8 or 16 lines per block, the node y/z sweeps 8, as in one context.
+
+template <int K, typename R>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_env_lagrange_cells(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    k_cyc_lagrange_cells_body<K, R>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
+                                    a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
+  }
+}
+
+template <int K, bool FIRST, typename R>
+__global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_bat_env_cells_x(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    env_sweep_cells_x_body<K, FIRST, R>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+                                        a.dpf, a.Vlag, t.y, t.z, t.w);
+  }
+}
+
+template <int K, int DD, bool FIRST, typename R, int LW>
+__global__ void __launch_bounds__(32 * LW, kEnvMinBlocks * kLineWarps / LW) k_bat_env_cells_t(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    __syncthreads();                                   // the previous item's tile reads are done
+    env_sweep_cells_t_body<K, DD, FIRST, R, LW>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                a.U[(it + 1) & 1], a.dpf, a.Vlag, t.y, t.z, t.w);
+  }
+}
+
+// the end of the remap, per cell, over the Lagrange cell kernel's tiles; the
+// last cell sweep (it = 2) wrote U[1]
+template <int K>
+__global__ void __launch_bounds__(128) k_bat_env_finalize(const CycleArgs* __restrict__ D, const int4* __restrict__ W,
+                                                          int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    int i, j, k;
+    if (block_item(a.dm.nx, a.dm.ny, a.dm.nz, t.y, t.z, t.w, i, j, k))
+      env_finalize_cell<K>(a.dm, a.S, a.ph, a.env, a.U[1], a.st, a.fd, (int)a.dm.cid(i, j, k));
+  }
+}
+
+template <bool FIRST, bool LAST, int K, typename R>
+__global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_env_nodes_x(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm, a.ud[(it + 1) & 1],
+                                             a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
+  }
+}
+
+template <int DD, bool FIRST, bool LAST, int K, typename R>
+__global__ void __launch_bounds__(32 * kLineWarps, TileGeom<kLineWarps>::minb) k_bat_env_nodes_t(
+    const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    __syncthreads();
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, K, R, kLineWarps>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
+                                                                a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd,
+                                                                a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
+  }
+}
+
+template <class Kern, class... Args>
+static void bat_env_launch(Kern kernel, int threads, size_t smem, const BatchPlan& P, int kind, int tk, cudaStream_t s,
+                           KernelMarks* m, Args... args) {
+  const int nwork = P.nwork[kind];
+  smem_opt_in((const void*)kernel, smem);
+  if (nwork > 0)
+    kernel<<<persistent_grid((const void*)kernel, threads, smem, nwork, P.occ_pct[tk]), threads, smem, s>>>(args...);
+  mark(m, tk, s);
+}
+
+template <int K, int DD, bool FIRST, typename R>
+static void bat_env_cells(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
+  const int kind = BK_CELLS_X + DD;
+  if constexpr (DD == 0) {
+    bat_env_launch(k_bat_env_cells_x<K, FIRST, R>, 32 * kLineWarps, 0, P, kind, kind, s, nullptr, P.descs,
+                   P.work[kind], P.nwork[kind], it);
+  } else if (P.lines[kind] == 16) {
+    bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, 16>, 32 * 16,
+                   (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<16>::arr * sizeof(double), P, kind, kind, s,
+                   nullptr, P.descs, P.work[kind], P.nwork[kind], it);
+  } else {
+    bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, kLineWarps>, 32 * kLineWarps,
+                   (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<kLineWarps>::arr * sizeof(double), P, kind,
+                   kind, s, nullptr, P.descs, P.work[kind], P.nwork[kind], it);
+  }
+}
+
+template <int K, int DD, bool FIRST, bool LAST, typename R>
+static void bat_env_nodes(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
+  const int kind = BK_NODES_X + DD;
+  if constexpr (DD == 0)
+    bat_env_launch(k_bat_env_nodes_x<FIRST, LAST, K, R>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
+                   P.work[kind], P.nwork[kind], it, prev);
+  else
+    bat_env_launch(k_bat_env_nodes_t<DD, FIRST, LAST, K, R>, 32 * kLineWarps,
+                   NodeTileSize<DD, FIRST, LAST, K, kLineWarps>::bytes, P, kind, kind, s, m, P.descs, P.work[kind],
+                   P.nwork[kind], it, prev);
+}
+
+template <int K, int DD, typename R>
+static void bat_env_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
+  const bool first = it == 0, last = it == 2;
+  if (first) bat_env_cells<K, DD, true, R>(P, it, s, m);
+  else bat_env_cells<K, DD, false, R>(P, it, s, m);
+  if (last)   // the end of the remap per cell, between the last cell and node sweeps
+    bat_env_launch(k_bat_env_finalize<K>, 128, 0, P, BK_LCELLS, BK_CELLS_X + DD, s, nullptr, P.descs,
+                   P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  else
+    mark(m, BK_CELLS_X + DD, s);
+  if (first) bat_env_nodes<K, DD, true, false, R>(P, it, prev, s, m);
+  else if (last) bat_env_nodes<K, DD, false, true, R>(P, it, prev, s, m);
+  else bat_env_nodes<K, DD, false, false, R>(P, it, prev, s, m);
+}
+
+template <int K, typename R>
+static void batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
+  launch_bat_lagrange_nodes(P, s, m);
+  bat_env_launch(k_bat_env_lagrange_cells<K, R>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS],
+                 P.nwork[BK_LCELLS]);
+  int prev = 0;
+  for (int it = 0; it < 3; ++it) {
+    const int d = (it + sens) % 3;
+    if (d == 0) bat_env_sweep<K, 0, R>(P, it, prev, s, m);
+    else if (d == 1) bat_env_sweep<K, 1, R>(P, it, prev, s, m);
+    else bat_env_sweep<K, 2, R>(P, it, prev, s, m);
+    prev |= 1 << d;
+  }
+  launch_bat_dt(P, s, m);
+}
+
+void launch_batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
+  if (P.precision) {
+    if (P.K == 2) batch_cycle_env<2, float>(P, sens, s, m);
+    else if (P.K == 3) batch_cycle_env<3, float>(P, sens, s, m);
+    else batch_cycle_env<4, float>(P, sens, s, m);
+  } else {
+    if (P.K == 2) batch_cycle_env<2, double>(P, sens, s, m);
+    else if (P.K == 3) batch_cycle_env<3, double>(P, sens, s, m);
+    else batch_cycle_env<4, double>(P, sens, s, m);
   }
 }
 

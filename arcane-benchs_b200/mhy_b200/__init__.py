@@ -436,7 +436,8 @@ class Context:
 
 
 class Batch:
-    """Many independent single-environment meshes advanced together on one GPU (mhy_batch)."""
+    """Many independent meshes advanced together on one GPU (mhy_batch); every
+    instance has the same number of environments."""
 
     def __init__(self, cases, device: int = -1, init: bool = True):
         L = load()

@@ -1,6 +1,6 @@
-"""GPU: the batched cycle (many uneven single-gas meshes in one set of
-persistent launches, per-instance dt on the device) gives every instance the
-bits of its own single-mesh run and of the oracle."""
+"""GPU: the batched cycle (many uneven meshes in one set of persistent
+launches, per-instance dt on the device; one, two or three gases) gives every
+instance the bits of its own single-mesh run and of the oracle."""
 import numpy as np
 import pytest
 
@@ -59,3 +59,53 @@ def test_batch_chunked_steps_equal_single_steps():
     for i in range(len(cases)):
         for f in FIELDS:
             assert np.array_equal(a.field(i, f), b.field(i, f)), (i, f)
+
+
+def two_gas_batch(precision=0):
+    cases = []
+    for i, (nx, ny, nz) in enumerate([(16, 8, 8), (20, 10, 10), (12, 12, 6), (24, 8, 8)]):
+        c = gen.two_material(nx, ny, nz, cycles=30, seed=40 + i)
+        c.options.deltat_init = 1.0e-5 * (1 + i)
+        c.options.precision = precision
+        cases.append(c)
+    cases[1].options.projection_limiteur_id = 1                 # per-instance options
+    return cases
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_two_gases_matches_single_contexts(precision):
+    """Instances with two environments each: the K-environment Lagrange
+    kernel, cell sweeps, end-of-remap kernel and node sweeps over the batch's
+    work tables give every instance the bits of its own context (and, in
+    FP64, of the oracle)."""
+    cases = two_gas_batch(precision)
+    b = Batch(cases)
+    b.step(30)
+    b.synchronize()
+    assert b.kernels_per_cycle() == 11
+    for i, c in enumerate(cases):
+        g = Context(c)
+        g.step(30)
+        assert b.dt(i) == g.dt(), i
+        for f in FIELDS:
+            assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
+        if precision == 0:
+            o = mhy_oracle.Oracle(c)
+            o.step(30)
+            for f in FIELDS:
+                assert np.array_equal(b.field(i, f), o.field(f)), (i, f, "oracle")
+        assert b.status(i) == 0
+
+
+def test_batch_three_gases_autotuned_matches_single_contexts():
+    cases = [gen.three_material(nx=24, ny=8, nz=8, cycles=20), gen.three_material(nx=32, ny=12, nz=8, cycles=20)]
+    b = Batch(cases)
+    t = b.autotune(2)
+    for k, w in enumerate(t.lines_per_block):
+        assert w in ((8, 16) if k in (3, 4) else (8,)), (k, w)
+    b.step(20)
+    for i, c in enumerate(cases):
+        g = Context(c)
+        g.step(20)
+        for f in FIELDS:
+            assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
