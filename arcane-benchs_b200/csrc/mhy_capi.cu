@@ -1721,7 +1721,6 @@ namespace {
 // each component plane's slice of those layers (contiguous, k is outermost).
 int halo_pieces(mhy_ctx* c, int lo, int hi, int nlo, int nhi, std::vector<std::pair<char*, size_t>>& out) {
   const Dims& dm = c->dm;
-  if (c->K != 1) return fail(MHY_ERR_UNSUPPORTED, "slabs: one environment");
   if (lo < 0 || hi > dm.nz || lo > hi || nlo < 0 || nhi > dm.nz + 1 || nlo > nhi)
     return fail(MHY_ERR_ARG, "layer range outside the mesh");
   const long long cl = (long long)dm.nx * dm.ny, nl = (long long)(dm.nx + 1) * (dm.ny + 1);

@@ -183,8 +183,6 @@ class SlabRank:
     """Rank r of a split of `case`: its slab, local case and engine."""
 
     def __init__(self, case, slabs, r, make_engine):
-        if case.nenv != 1:
-            raise ValueError("slabs: one environment")
         self.slabs, self.r, self.s = slabs, r, slabs[r]
         self.local = sub_case(case, self.s)
         self.eng = make_engine(self.local)

@@ -274,7 +274,8 @@ int mhy_checkpoint_load(mhy_ctx* ctx, const void* src, size_t bytes);
  * doubles order like unsigned integers), mhy_dt_finish, then the ghost
  * layers refreshed from the neighbours with mhy_halo_pack / mhy_halo_unpack
  * (every restart-dump field, contiguous per component and layer range; the
- * caller moves the buffers, e.g. with NCCL send/recv).  One environment. */
+ * caller moves the buffers, e.g. with NCCL send/recv).  Any number of
+ * environments: the restart state holds every environment plane. */
 /* dt reduced over cell layers [k_lo, k_hi) of this context; external = 1:
  * the cycle stops after the local minimum (mhy_dt_local_min / mhy_dt_finish). */
 int mhy_set_dt_reduction(mhy_ctx* ctx, int32_t k_lo, int32_t k_hi, int32_t external);

@@ -1663,8 +1663,8 @@ struct Oracle {
     ++iteration;
   }
 
-  // slabs: the state a cycle starts from (K = 1) for cell layers [clo, chi)
-  // and node layers [nlo, nhi), field by field; pack (to buf) or unpack
+  // slabs: the state a cycle starts from for cell layers [clo, chi) and
+  // node layers [nlo, nhi), field by field; pack (to buf) or unpack
   template <class F>
   void halo_fields(int clo, int chi, int nlo, int nhi, F&& f) {
     const long cl = (long)nx * ny, nl = (long)NX * NY;
@@ -1675,6 +1675,29 @@ struct Oracle {
     for (long n = n0; n < n1; ++n) { f(velocity[n].x); f(velocity[n].y); f(velocity[n].z); }
     for (long n = n0; n < n1; ++n) f(node_mass[n]);
     for (long n = n0; n < n1; ++n) for (int v = 0; v < nvars; ++v) f(dual_grad_phi[(size_t)n * nvars + v]);
+    if (K > 1) {
+      // several environments: membership, every environment's values, the
+      // global fractions, the mixed/pure indicators and Phi (the pente-borne
+      // Phi of absent environments outlives a cycle); integers travel as
+      // doubles, exactly
+      for (long c = c0; c < c1; ++c) {
+        double m = (double)env_mask[c], e = (double)env_id[c];
+        f(m); f(e);
+        env_mask[c] = (uint32_t)m; env_id[c] = (int)e;
+      }
+      MatVar* ev[] = {&fracvol, &mass_fraction, &density, &internal_energy, &pressure, &sound_speed,
+                      &pseudo_viscosity, &cell_mass};
+      for (MatVar* v : ev) {
+        if (v == &fracvol || v == &mass_fraction) for (long c = c0; c < c1; ++c) f(v->g[c]);
+        for (int k = 0; k < K; ++k) for (long c = c0; c < c1; ++c) f(v->p[k][c]);
+      }
+      for (long c = c0; c < c1; ++c) {
+        double m = (double)est_mixte[c], e = (double)est_pure[c];
+        f(m); f(e);
+        est_mixte[c] = (int)m; est_pure[c] = (int)e;
+      }
+      for (long c = c0; c < c1; ++c) for (int v = 0; v < nvars; ++v) f(phi_lag[(size_t)c * nvars + v]);
+    }
   }
 };
 
@@ -1754,7 +1777,7 @@ void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
 // Slabs (one environment): dt over cell layers [k_lo, k_hi), external finish.
 int orc_set_dt_reduction(void* h, int k_lo, int k_hi, int external) {
   Oracle* o = static_cast<Oracle*>(h);
-  if (o->K != 1 || k_lo < 0 || k_hi > o->nz || k_lo >= k_hi) return -1;
+  if (k_lo < 0 || k_hi > o->nz || k_lo >= k_hi) return -1;
   o->dt_k0 = k_lo; o->dt_k1 = k_hi; o->ext_dt = external;
   return 0;
 }

@@ -44,6 +44,28 @@ def test_gpu_slabs_mixed_precision():
     _compare(case, 2, 12)
 
 
+@pytest.mark.parametrize("opts", [{}, dict(ordre_projection=3), dict(pente_borne=1, pente_borne_debar_fix=1)],
+                         ids=["two_gases", "two_gases_order3", "two_gases_pente_borne"])
+def test_gpu_slabs_two_gases(opts):
+    """Several environments: the halo carries every environment plane of the
+    restart state (membership, fractions, values, indicators, Phi)."""
+    case = gen.two_material(10, 6, 24, lx=0.5, ly=0.3, lz=1.2, seed=55, cycles=1, options=gen.Options(**opts))
+    lay = slabs.layout(case.nz, 2)
+    ranks = [slabs.SlabRank(case, lay, r, lambda c: slabs.GpuEngine(c, 0)) for r in range(2)]
+    slabs.run_local(ranks, 9)
+    g = Context(case)
+    g.step(9)
+    for f in FIELDS:
+        got = np.concatenate([rk.owned_field(f) for rk in ranks])
+        assert np.array_equal(got, g.field(f)), f
+    for k in range(case.nenv):
+        for w in ("fracvol", "density", "internal_energy"):
+            got = np.concatenate([slabs.owned(rk.s, rk.local, rk.eng.ctx.env_field(w, k), False) for rk in ranks])
+            assert np.array_equal(got, g.env_field(w, k)), (w, k)
+    for rk in ranks:
+        rk.eng.close()
+
+
 def test_halo_ranges_are_checked():
     g = Context(gen.sedov(n=8, cycles=1))
     with pytest.raises(MhyError):

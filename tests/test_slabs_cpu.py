@@ -56,6 +56,24 @@ def test_slabs_equal_the_unsplit_run(world):
     _check(case, ranks, _reference(case, cycles))
 
 
+@pytest.mark.parametrize("world,opts", [
+    (2, {}),
+    (3, {}),
+    (2, dict(ordre_projection=3)),
+    (2, dict(pente_borne=1, pente_borne_debar_fix=1)),
+    (2, dict(conservation_energie_totale=1, projection_limiteur_id=5)),
+], ids=["two", "three_ranks", "order3", "pente_borne", "cons_ec_g_limiter"])
+def test_two_gas_slabs_equal_the_unsplit_run(world, opts):
+    """Several environments: the ghost layers also carry the membership,
+    every environment's values, the mixed/pure indicators and Phi."""
+    case = gen.two_material(10, 6, 30 if world == 3 else 24, lx=0.5, ly=0.3, lz=1.2, seed=55, cycles=1,
+                            options=gen.Options(**opts))
+    cycles = 9
+    ranks = _split(case, world)
+    slabs.run_local(ranks, cycles)
+    _check(case, ranks, _reference(case, cycles))
+
+
 def test_ghost_depth_three_is_enough_and_two_is_not():
     """One cycle reaches at most 5 layers along z (the default depth); on this
     deck 3 ghost layers keep the split exact and 2 do not (the edge of the
