@@ -52,9 +52,10 @@ struct CellInK {
 // the generalised form for uneven widths (RemapADIService.cc:319-437 ->
 // UtilesRemap.cc:295-330), every component limited alike; at the ends of
 // the line the back or front cell is the cell itself.
-template <int K, typename R, bool GL>
+template <int K, typename R, bool GL, bool SP = false>
 __device__ __forceinline__ void face_values_env(const Phys& ph, int lim, bool inner, bool infr, const CellInK<K>& in,
-                                                const R P[3 * K + 1], R Pf[3 * K + 1], R Pfn[3 * K + 1]) {
+                                                const R P[3 * K + 1], R Pf[3 * K + 1], R Pfn[3 * K + 1],
+                                                unsigned* oor = nullptr) {
   constexpr int NV = 3 * K + 1;
   const R order2 = (R)(ph.ordre_projection - 1);
   const unsigned full = 0xffffffffu;
@@ -69,10 +70,11 @@ __device__ __forceinline__ void face_values_env(const Phys& ph, int lim, bool in
     const double hb = __shfl_up_sync(full, in.h, 1), hn = __shfl_down_sync(full, in.h, 1);
     h0 = (R)in.h; hm = (R)(inner ? hb : in.h); hp = (R)(infr ? hn : in.h);
   }
+  unsigned fo = 0u;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     Pp[v] = __shfl_up_sync(full, P[v], 1);
-    const R g = inner ? Ar<R>::div(P[v] - Pp[v], dxR, rdx) : R(0);
+    const R g = inner ? dv<R, SP>(P[v] - Pp[v], dxR, rdx, &fo) : R(0);
     const R gr = __shfl_down_sync(full, g, 1);
     if constexpr (GL) {
       const R Pn = __shfl_down_sync(full, P[v], 1);
@@ -82,6 +84,8 @@ __device__ __forceinline__ void face_values_env(const Phys& ph, int lim, bool in
       G[v] = limited_one<R>(lim, g, gr);
     }
   }
+  // lane 0's back neighbour is itself (0 / 0): its gradient reaches no updated cell
+  if constexpr (SP) { if ((threadIdx.x & 31) != 0) *oor |= fo; }
   const bool back = in.u * dx > 0.0;
   const R dot_xf = (R)(back ? in.db : in.df);
 #pragma unroll
@@ -156,9 +160,9 @@ __device__ __forceinline__ void pb_fluxes_env(const Phys& ph, int type, double p
 // reconstruction, and the debar fix, follow the cell's neighbourhood
 // (R:364-375): pure when the cell and its back and front neighbours (the
 // cell itself at the ends of the line) are pure cells of one environment.
-template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false, bool SP = false>
 __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool valid, bool inner, bool infr,
-                                              bool upd, const CellInK<K>& in, double* out) {
+                                              bool upd, const CellInK<K>& in, double* out, unsigned* oor = nullptr) {
   constexpr int NV = 3 * K + 1;
   const unsigned full = 0xffffffffu;
   R Pf[NV], Pfn[NV];
@@ -200,7 +204,7 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
         }
         const R dR = (R)den, r = Ar<R>::rcp(dR);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) P[v] = Ar<R>::div((R)in.U[v], dR, r);
+        for (int v = 0; v < NV; ++v) P[v] = dv<R, SP>((R)in.U[v], dR, r, oor);
       }
     }
     int lim = ph.ordre_projection > 1 ? ph.lim_cell : -1;
@@ -244,7 +248,7 @@ __device__ __forceinline__ void cell_line_env(const Phys& ph, double dt, bool va
         Pfn[v] = __shfl_down_sync(full, Pf[v], 1);
       }
     } else {
-      face_values_env<K, R, GL>(ph, lim, inner, infr, in, P, Pf, Pfn);
+      face_values_env<K, R, GL, SP>(ph, lim, inner, infr, in, P, Pf, Pfn, oor);
     }
   }
   const double un = __shfl_down_sync(full, in.u, 1), An = __shfl_down_sync(full, in.A, 1);
@@ -284,15 +288,18 @@ __device__ __forceinline__ void env_cell_extras(const Phys& ph, const FaceData& 
 }
 
 // K-environment cell sweep along x (lanes along the rows).
-template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
-__device__ __forceinline__ void env_sweep_cells_x_body(Dims dm,
-    const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
-    const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
-    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag, int bx_, int by_, int bz_) {
+// One lane's inputs and line step of the K-environment x sweep; the body
+// below runs it with speculative FP64 quotients and, in a warp where any
+// lane's were out of range, recomputes the segment exactly out of line
+// (env_x_line_exact reloads the inputs), then stores.
+template <int K, bool FIRST, typename R, bool GL, bool O3, bool PB, bool SP>
+__device__ __forceinline__ void env_x_line(const Dims& dm, const Scalars* __restrict__ S, const Phys& ph,
+    const FaceData& fd, const double* __restrict__ n0, const double* __restrict__ xcs, const double* __restrict__ ofn,
+    const double* __restrict__ Uin, const double* __restrict__ Vlag, int bx_, int by_, int bz_, double* out,
+    unsigned* oor) {
   constexpr int NV = 3 * K + 1;
   const int lane = threadIdx.x & 31;
   const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
-  if (j >= dm.ny) return;                              // whole warp leaves together
   const int nd = dm.nx, C = (int)dm.C, F = (int)dm.F;
   const int s = bx_ * kLineUpd - 2 + lane;
   const bool valid = s >= 0 && s < nd;
@@ -327,8 +334,43 @@ __device__ __forceinline__ void env_sweep_cells_x_body(Dims dm,
     for (int v = 0; v < NV; ++v) in.pf3[v] = inner ? fd.phi3[v * Fd + t] : 0.;
   }
   if (upd) { in.ob = ofn[1 * C + c]; in.of = ofn[4 * C + c]; }
+  cell_line_env<K, FIRST, R, GL, O3, PB, SP>(ph, S->dt, valid, inner, infr, upd, in, out, oor);
+}
+
+template <int K, bool FIRST, typename R, bool GL, bool O3, bool PB>
+__device__ __noinline__ LineOut<4 * K + 1> env_x_line_exact(Dims dm, const Scalars* S, Phys ph, FaceData fd,
+    const double* n0, const double* xcs, const double* ofn, const double* Uin, const double* Vlag, int bx_, int by_,
+    int bz_) {
+  LineOut<4 * K + 1> o;
+  env_x_line<K, FIRST, R, GL, O3, PB, false>(dm, S, ph, fd, n0, xcs, ofn, Uin, Vlag, bx_, by_, bz_, o.v, nullptr);
+  return o;
+}
+
+template <int K, bool FIRST, typename R, bool GL = false, bool O3 = false, bool PB = false>
+__device__ __forceinline__ void env_sweep_cells_x_body(Dims dm,
+    const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
+    const double* __restrict__ xcs, const double* __restrict__ ofn, const double* __restrict__ Uin,
+    double* __restrict__ Uout, double* __restrict__ dpf, const double* __restrict__ Vlag, int bx_, int by_, int bz_) {
+  constexpr int NV = 3 * K + 1;
+  const int lane = threadIdx.x & 31;
+  const int j = by_ * kLineWarps + (threadIdx.x >> 5), k = bz_;
+  if (j >= dm.ny) return;                              // whole warp leaves together
   double out[NV + K];
-  cell_line_env<K, FIRST, R, GL, O3, PB>(ph, S->dt, valid, inner, infr, upd, in, out);
+  if constexpr (sizeof(R) == 8 && !PB && !O3) {
+    unsigned oor = 0u;
+    env_x_line<K, FIRST, R, GL, O3, PB, true>(dm, S, ph, fd, n0, xcs, ofn, Uin, Vlag, bx_, by_, bz_, out, &oor);
+    if (__any_sync(0xffffffffu, oor != 0u)) {
+      const auto o = env_x_line_exact<K, FIRST, R, GL, O3, PB>(dm, S, ph, fd, n0, xcs, ofn, Uin, Vlag, bx_, by_, bz_);
+#pragma unroll
+      for (int v = 0; v < NV + K; ++v) out[v] = o.v[v];
+    }
+  } else {
+    env_x_line<K, FIRST, R, GL, O3, PB, false>(dm, S, ph, fd, n0, xcs, ofn, Uin, Vlag, bx_, by_, bz_, out, nullptr);
+  }
+  const int nd = dm.nx, C = (int)dm.C;
+  const int s = bx_ * kLineUpd - 2 + lane;
+  const bool upd = s >= 0 && s < nd && lane >= 2 && lane < 2 + kLineUpd;
+  const int c = s + dm.nx * (j + dm.ny * k);
   if (!upd) return;
 #pragma unroll
   for (int v = 0; v < NV; ++v) Uout[v * C + c] = out[v];
@@ -352,6 +394,61 @@ template <int K, bool FIRST>
 __host__ __device__ constexpr int env_cells_staged_arrays() { return 3 * K + 1 + 12 + (FIRST ? 1 : 0); }
 
 // W: lines per block (8 or 16, the tuning; the register budget stays 128).
+// One lane's line step of the K-environment y/z sweep, from the staged tile
+// (each warp reads only its own tile row, which no other warp writes).
+template <int K, int D, bool FIRST, typename R, int W, bool GL, bool O3, bool PB, bool SP>
+__device__ __forceinline__ void env_t_line(const Dims& dm, const Scalars* __restrict__ S, const Phys& ph,
+    const FaceData& fd, int bx_, int by_, int bz_, double* out, unsigned* oor) {
+  constexpr int NV = 3 * K + 1;
+  constexpr int AX = NV, AF = NV + 3, AN = NV + 7, AO = NV + 10, AD = NV + 12;   // array offsets
+  constexpr int kTileArr = TileGeom<W>::arr, kTileLd = TileGeom<W>::ld;
+  extern __shared__ double tile[];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int i0 = bx_ * W, seg0 = by_ * kLineUpd - 2, o = bz_;
+  const int nd = dm.ncd(D), C = (int)dm.C;
+  const int s = seg0 + lane;
+  const bool line_ok = i0 + w < dm.nx;
+  const bool valid = line_ok && s >= 0 && s < nd;
+  const bool inner = line_ok && s >= 1 && s <= nd - 1;
+  const bool infr = s + 1 <= nd - 1;
+  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
+  const double* row = tile + w * kTileLd + lane;
+  CellInK<K> in;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) in.U[v] = row[v * kTileArr];
+  in.xc[0] = row[AX * kTileArr]; in.xc[1] = row[(AX + 1) * kTileArr]; in.xc[2] = row[(AX + 2) * kTileArr];
+  in.db = row[AF * kTileArr]; in.df = row[(AF + 1) * kTileArr]; in.u = row[(AF + 2) * kTileArr];
+  in.A = row[(AF + 3) * kTileArr];
+  in.n[0] = row[AN * kTileArr]; in.n[1] = row[(AN + 1) * kTileArr]; in.n[2] = row[(AN + 2) * kTileArr];
+  in.ob = row[AO * kTileArr]; in.of = row[(AO + 1) * kTileArr];
+  in.den = FIRST ? row[AD * kTileArr] : 0.;
+  in.h = 0.; in.pbq = 0.; in.est = 0u;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) in.pbP[v] = 0.;
+  if (valid) {                                         // the cell's own extras: read directly
+    const int ci = i0 + w;
+    env_cell_extras<K, FIRST, GL, PB>(ph, fd, C, D == 1 ? ci + dm.nx * (s + dm.ny * o) : ci + dm.nx * (o + dm.ny * s),
+                                      D, in);
+  }
+  if constexpr (O3) {
+    // face values in the line layout of k_o3_faces_env: position along D
+    // fastest, so the lanes' reads are contiguous
+    const int Fd = (int)(D == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
+    const int q = s + (nd + 1) * (i0 + w + dm.nx * o);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in.pf3[v] = inner ? fd.phi3[v * Fd + q] : 0.;
+  }
+  cell_line_env<K, FIRST, R, GL, O3, PB, SP>(ph, S->dt, valid, inner, infr, upd, in, out, oor);
+}
+
+template <int K, int D, bool FIRST, typename R, int W, bool GL, bool O3, bool PB>
+__device__ __noinline__ LineOut<4 * K + 1> env_t_line_exact(Dims dm, const Scalars* S, Phys ph, FaceData fd, int bx_,
+                                                            int by_, int bz_) {
+  LineOut<4 * K + 1> o;
+  env_t_line<K, D, FIRST, R, W, GL, O3, PB, false>(dm, S, ph, fd, bx_, by_, bz_, o.v, nullptr);
+  return o;
+}
+
 template <int K, int D, bool FIRST, typename R, int W = kLineWarps, bool GL = false, bool O3 = false, bool PB = false>
 __device__ __forceinline__ void env_sweep_cells_t_body(Dims dm,
     const Scalars* __restrict__ S, Phys ph, FaceData fd, const double* __restrict__ n0,
@@ -393,42 +490,23 @@ __device__ __forceinline__ void env_sweep_cells_t_body(Dims dm,
     if (FIRST) wr[AD * kTileArr] = s_valid ? Vlag[sc] : 0.;
   }
   __syncthreads();
-  const int s = seg0 + lane;
-  const bool line_ok = i0 + w < dm.nx;
-  const bool valid = line_ok && s >= 0 && s < nd;
-  const bool inner = line_ok && s >= 1 && s <= nd - 1;
-  const bool infr = s + 1 <= nd - 1;
-  const bool upd = valid && lane >= 2 && lane < 2 + kLineUpd;
-  double* row = tile + w * kTileLd + lane;
-  CellInK<K> in;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) in.U[v] = row[v * kTileArr];
-  in.xc[0] = row[AX * kTileArr]; in.xc[1] = row[(AX + 1) * kTileArr]; in.xc[2] = row[(AX + 2) * kTileArr];
-  in.db = row[AF * kTileArr]; in.df = row[(AF + 1) * kTileArr]; in.u = row[(AF + 2) * kTileArr];
-  in.A = row[(AF + 3) * kTileArr];
-  in.n[0] = row[AN * kTileArr]; in.n[1] = row[(AN + 1) * kTileArr]; in.n[2] = row[(AN + 2) * kTileArr];
-  in.ob = row[AO * kTileArr]; in.of = row[(AO + 1) * kTileArr];
-  in.den = FIRST ? row[AD * kTileArr] : 0.;
-  in.h = 0.; in.pbq = 0.; in.est = 0u;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) in.pbP[v] = 0.;
-  if (valid) {                                         // the cell's own extras: read directly
-    const int ci = i0 + w;
-    env_cell_extras<K, FIRST, GL, PB>(ph, fd, C, D == 1 ? ci + dm.nx * (s + dm.ny * o) : ci + dm.nx * (o + dm.ny * s),
-                                      D, in);
-  }
-  if constexpr (O3) {
-    // face values in the line layout of k_o3_faces_env: position along D
-    // fastest, so the lanes' reads are contiguous
-    const int Fd = (int)(D == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
-    const int q = s + (nd + 1) * (i0 + w + dm.nx * o);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) in.pf3[v] = inner ? fd.phi3[v * Fd + q] : 0.;
-  }
   constexpr int NO = NV + K;
   static_assert(NO <= NA, "outputs reuse the staged rows");
   double out[NO];
-  cell_line_env<K, FIRST, R, GL, O3, PB>(ph, S->dt, valid, inner, infr, upd, in, out);
+  if constexpr (sizeof(R) == 8 && !PB && !O3) {
+    unsigned oor = 0u;
+    env_t_line<K, D, FIRST, R, W, GL, O3, PB, true>(dm, S, ph, fd, bx_, by_, bz_, out, &oor);
+    if (__any_sync(0xffffffffu, oor != 0u)) {
+      const auto o2 = env_t_line_exact<K, D, FIRST, R, W, GL, O3, PB>(dm, S, ph, fd, bx_, by_, bz_);
+#pragma unroll
+      for (int v = 0; v < NO; ++v) out[v] = o2.v[v];
+    }
+  } else {
+    env_t_line<K, D, FIRST, R, W, GL, O3, PB, false>(dm, S, ph, fd, bx_, by_, bz_, out, nullptr);
+  }
+  const int s = seg0 + lane;
+  const bool upd = i0 + w < dm.nx && s >= 0 && s < nd && lane >= 2 && lane < 2 + kLineUpd;
+  double* row = tile + w * kTileLd + lane;
   if (upd) {
 #pragma unroll
     for (int a = 0; a < NO; ++a) row[a * kTileArr] = out[a];

@@ -45,6 +45,23 @@ def assert_env_bitwise(o, g, dto, dtg, K):
             assert np.array_equal(a, b), f"env {k} {f}: {int((a != b).sum())} cells differ"
 
 
+def test_two_material_tiny_values_take_the_exact_quotients():
+    """The K-environment sweeps divide with a fast corrected quotient that
+    flags operands outside 2^-960 <= |.| < 2^960; a warp with a flagged lane
+    recomputes its segment exactly.  Gas B's energies near 1e-300 and node
+    velocities down to 1e-165 flag lanes in every sweep: bitwise vs the oracle."""
+    case = gen.two_material(20, 10, 10, cycles=20, seed=12)
+    case.pressure = case.pressure.copy()
+    case.pressure[1] *= 1e-300
+    rng = np.random.default_rng(3)
+    n = case.velocity.shape[0]
+    case.velocity = rng.uniform(-1.0, 1.0, size=(n, 3)) * 10.0 ** rng.uniform(-165.0, -145.0, size=(n, 1))
+    o, g, dto, dtg = run_both(case, 20, chunk=5)
+    e = o.env_field("internal_energy", 1)
+    assert (np.abs(e[e > 0]) < 2.0 ** -960).mean() > 0.3        # still in the flagged range at the end
+    assert_env_bitwise(o, g, dto, dtg, 2)
+
+
 def test_two_material_bitwise():
     case = gen.two_material(32, 16, 16, cycles=120)
     o, g, dto, dtg = run_both(case, 120, chunk=10)
