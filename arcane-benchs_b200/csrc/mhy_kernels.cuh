@@ -237,7 +237,11 @@ __device__ __forceinline__ void dt_min_body(Dims dm, Scalars* __restrict__ S, co
       unsigned long long other = __shfl_down_sync(0xffffffffu, best, o);
       best = other < best ? other : best;
     }
-    if (threadIdx.x == 0) atomicMin(&S->min_bits, best);
+    // the running minimum only decreases, so a block whose minimum is not
+    // below a value read from it would leave it unchanged: skip that atomic
+    // (one block per 128 cells would otherwise queue ~16k atomics on one
+    // address per Sedov 128^3 cycle)
+    if (threadIdx.x == 0 && best < __ldcg(&S->min_bits)) atomicMin(&S->min_bits, best);
   }
 }
 
