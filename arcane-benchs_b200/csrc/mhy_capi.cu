@@ -776,12 +776,10 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
       return fail(MHY_ERR_UNSUPPORTED, "batched instances share one number of environments");
     if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
     if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
-    if (opts[i].projection_limiteur_id >= 3)
-      return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters are not batched");
+    if ((opts[i].projection_limiteur_id >= 3) != (opts[0].projection_limiteur_id >= 3))
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters (ids 3..7) in every instance or in none");
     if (opts[i].projection_pente_borne || opts[i].pente_borne_mixte)
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: pente-borne is not batched");
-    if (opts[i].conservation_energie_totale)
-      return fail(MHY_ERR_UNSUPPORTED, "batched instances: conservation-energie-totale is not batched");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();
@@ -812,6 +810,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   b->plan.ninst = n;
   b->plan.precision = opts[0].precision;
   b->plan.K = opts[0].nb_env;
+  b->plan.gl = opts[0].projection_limiteur_id >= 3;   // the same in every instance (checked above)
+  for (int i = 0; i < n; ++i) b->plan.cons_ec |= opts[i].conservation_energie_totale;
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
     b->plan.occ_pct[k] = 100;
     b->tuning.occupancy_pct[k] = 100;
@@ -919,9 +919,10 @@ inline bool line_slot(int k) {
 }
 
 // The line counts a batch's sweeps are built for: any on one environment; with
-// several, 8 or 16 on the cell y/z sweeps and 8 on the node y/z sweeps.
+// several, 8 or 16 on the cell y/z sweeps and 8 on the node y/z sweeps; 8
+// everywhere with the G limiters.
 bool batch_tunable_lines(const mhy_batch* b, int k, int w) {
-  if (!line_slot(k)) return w == kLineWarps;
+  if (!line_slot(k) || b->plan.gl) return w == kLineWarps;   // the G limiters' sweeps keep 8 lines
   if (b->plan.K > 1) return w == kLineWarps || ((k == BK_CELLS_Y || k == BK_CELLS_Z) && w == 16);
   return true;
 }
@@ -1319,7 +1320,8 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
   return MHY_OK;
 }
 int mhy_batch_kernels_per_cycle(mhy_batch* b) {
-  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) : 0;   // several environments: the end-of-remap kernel
+  // several environments: the end-of-remap kernel; conservation-energie-totale: its kernel
+  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) + (b->plan.cons_ec ? 1 : 0) : 0;
 }
 void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
 

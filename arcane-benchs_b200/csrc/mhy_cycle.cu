@@ -616,11 +616,9 @@ static void remap_impl(const CycleArgs& a0, int sens, cudaStream_t s, KernelMark
 // last node sweep) summed in cell-node order from 0, floored at 0 as
 // std::max(0., delta) does, times the cell's mass fraction, added to e; p and
 // c again from the new e.
-__global__ void __launch_bounds__(128) k_cons_ec(Dims dm, Phys ph, const double* __restrict__ ecn,
+__device__ __forceinline__ void cons_ec_cell(const Dims& dm, const Phys& ph, const double* __restrict__ ecn,
     const double* __restrict__ mf, const double* __restrict__ rho, double* __restrict__ e, double* __restrict__ p,
-    double* __restrict__ cs, int linear) {
-  int i, j, k;
-  if (!block_item(dm.nx, dm.ny, dm.nz, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, i, j, k)) return;
+    double* __restrict__ cs, int i, int j, int k) {
   const long long c = dm.cid(i, j, k);
   double delta_ec = 0.;
 #pragma unroll
@@ -633,6 +631,14 @@ __global__ void __launch_bounds__(128) k_cons_ec(Dims dm, Phys ph, const double*
   e[c] = en;
   p[c] = pr;
   cs[c] = cc;
+}
+
+__global__ void __launch_bounds__(128) k_cons_ec(Dims dm, Phys ph, const double* __restrict__ ecn,
+    const double* __restrict__ mf, const double* __restrict__ rho, double* __restrict__ e, double* __restrict__ p,
+    double* __restrict__ cs, int linear) {
+  int i, j, k;
+  if (!block_item(dm.nx, dm.ny, dm.nz, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, i, j, k)) return;
+  cons_ec_cell(dm, ph, ecn, mf, rho, e, p, cs, i, j, k);
 }
 
 void launch_cons_ec(const CycleArgs& a, cudaStream_t s) {
@@ -701,61 +707,63 @@ __global__ void __launch_bounds__(128) k_bat_lagrange_nodes(const CycleArgs* __r
   }
 }
 
-template <typename R>
+template <typename R, bool HC = false>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_lagrange_cells(const CycleArgs* __restrict__ D,
                                                                                    const int4* __restrict__ W, int nw) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_lagrange_cells_body<1, R>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
-                                    a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
+    k_cyc_lagrange_cells_body<1, R, false, HC>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
+                                               a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env,
+                                               a.Vlag, t.y, t.z, t.w);
   }
 }
 
-template <bool LAST, typename R>
+template <bool LAST, typename R, bool GL = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_cells_x_body<LAST, R>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1], a.dpf,
-                                   a.st, t.y, t.z, t.w);
+    k_cyc_sweep_cells_x_body<LAST, R, false, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                 a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
   }
 }
 
-template <int DD, bool LAST, typename R, int LW>
+template <int DD, bool LAST, typename R, int LW, bool GL = false>
 __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_cells_t_body<DD, LAST, R, LW>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
-                                           a.dpf, a.st, t.y, t.z, t.w);
+    k_cyc_sweep_cells_t_body<DD, LAST, R, LW, false, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                      a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
   }
 }
 
-template <bool FIRST, bool LAST, typename R>
+template <bool FIRST, bool LAST, typename R, bool GL = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_nodes_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm, a.ud[(it + 1) & 1],
-                                             a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
+                                                 a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm,
+                                                 a.vnorm, t.y, t.z, t.w, a.ecn);
   }
 }
 
-template <int DD, bool FIRST, bool LAST, typename R, int LW>
+template <int DD, bool FIRST, bool LAST, typename R, int LW, bool GL = false>
 __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_nodes_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm, a.ud[(it + 1) & 1],
-                                                     a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y,
-                                                     t.z, t.w);
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
+                                                         a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v,
+                                                         a.nm, a.vnorm, t.y, t.z, t.w, a.ecn);
   }
 }
 
@@ -766,6 +774,20 @@ __global__ void __launch_bounds__(128) k_bat_dt_min(const CycleArgs* __restrict_
     const CycleArgs& a = D[t.x];
     __syncthreads();
     dt_min_body(a.dm, a.S, a.L, a.st.cs, a.vnorm, t.y, t.z, t.w);
+  }
+}
+
+// conservation-energie-totale over the Lagrange cell kernel's tiles, for the
+// instances that have it
+__global__ void __launch_bounds__(128) k_bat_cons_ec(const CycleArgs* __restrict__ D, const int4* __restrict__ W,
+                                                     int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    if (!a.ph.cons_ec) continue;
+    int i, j, k;
+    if (block_item(a.dm.nx, a.dm.ny, a.dm.nz, t.y, t.z, t.w, i, j, k))
+      cons_ec_cell(a.dm, a.ph, a.ecn, a.st.mf, a.st.rho, a.st.e, a.st.p, a.st.cs, i, j, k);
   }
 }
 
@@ -822,56 +844,74 @@ static void launch_persistent(Kern kernel, int threads, size_t smem, const Batch
   mark(marks, tk, s);
 }
 
-template <int DD, bool LAST, typename R, int LW>
+template <int DD, bool LAST, typename R, int LW, bool GL>
 static void bat_cells_t(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
-  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW>, 32 * LW, CellTileSize<LAST, LW>::bytes, P, kind, kind, s, m,
+  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW, GL>, 32 * LW, CellTileSize<LAST, LW>::bytes, P, kind, kind, s, m,
                     P.descs, P.work[kind], P.nwork[kind], it);
 }
 
-template <int DD, bool LAST, typename R>
+template <int DD, bool LAST, typename R, bool GL>
 static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
   if constexpr (DD == 0) {
-    launch_persistent(k_bat_sweep_cells_x<LAST, R>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs, P.work[kind],
+    launch_persistent(k_bat_sweep_cells_x<LAST, R, GL>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs, P.work[kind],
                       P.nwork[kind], it);
   } else {
     const int w = P.lines[kind];
-    if (w == 32) bat_cells_t<DD, LAST, R, 32>(P, it, s, m);
-    else if (w == 16) bat_cells_t<DD, LAST, R, 16>(P, it, s, m);
-    else bat_cells_t<DD, LAST, R, 8>(P, it, s, m);
+    if (GL || w == 8) bat_cells_t<DD, LAST, R, 8, GL>(P, it, s, m);   // the G limiters keep 8 lines
+    else if (w == 32) bat_cells_t<DD, LAST, R, 32, false>(P, it, s, m);
+    else bat_cells_t<DD, LAST, R, 16, false>(P, it, s, m);
   }
 }
 
-template <int DD, bool FIRST, bool LAST, typename R, int LW>
+template <int DD, bool FIRST, bool LAST, typename R, int LW, bool GL>
 static void bat_nodes_t(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_NODES_X + DD;
-  launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R, LW>, 32 * LW, NodeTileSize<DD, FIRST, LAST, 1, LW>::bytes,
+  launch_persistent(k_bat_sweep_nodes_t<DD, FIRST, LAST, R, LW, GL>, 32 * LW, NodeTileSize<DD, FIRST, LAST, 1, LW>::bytes,
                     P, kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it, prev);
 }
 
-template <int DD, bool FIRST, bool LAST, typename R>
+template <int DD, bool FIRST, bool LAST, typename R, bool GL>
 static void bat_nodes_d(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_NODES_X + DD;
   if constexpr (DD == 0) {
-    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
+    launch_persistent(k_bat_sweep_nodes_x<FIRST, LAST, R, GL>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
                       P.work[kind], P.nwork[kind], it, prev);
   } else {
     const int w = P.lines[kind];
-    if (w == 32) bat_nodes_t<DD, FIRST, LAST, R, 32>(P, it, prev, s, m);
-    else if (w == 16) bat_nodes_t<DD, FIRST, LAST, R, 16>(P, it, prev, s, m);
-    else bat_nodes_t<DD, FIRST, LAST, R, 8>(P, it, prev, s, m);
+    if (GL || w == 8) bat_nodes_t<DD, FIRST, LAST, R, 8, GL>(P, it, prev, s, m);
+    else if (w == 32) bat_nodes_t<DD, FIRST, LAST, R, 32, false>(P, it, prev, s, m);
+    else bat_nodes_t<DD, FIRST, LAST, R, 16, false>(P, it, prev, s, m);
   }
 }
 
-template <int DD, typename R>
+template <int DD, typename R, bool GL>
 static void bat_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const bool first = it == 0, last = it == 2;
-  if (last) bat_cells_d<DD, true, R>(P, it, s, m);
-  else bat_cells_d<DD, false, R>(P, it, s, m);
-  if (first) bat_nodes_d<DD, true, false, R>(P, it, prev, s, m);
-  else if (last) bat_nodes_d<DD, false, true, R>(P, it, prev, s, m);
-  else bat_nodes_d<DD, false, false, R>(P, it, prev, s, m);
+  if (last) bat_cells_d<DD, true, R, GL>(P, it, s, m);
+  else bat_cells_d<DD, false, R, GL>(P, it, s, m);
+  if (first) bat_nodes_d<DD, true, false, R, GL>(P, it, prev, s, m);
+  else if (last) bat_nodes_d<DD, false, true, R, GL>(P, it, prev, s, m);
+  else bat_nodes_d<DD, false, false, R, GL>(P, it, prev, s, m);
+}
+
+template <typename R, bool GL>
+static void bat_sweeps(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
+  int prev = 0;
+  for (int it = 0; it < 3; ++it) {
+    const int d = (it + sens) % 3;
+    if (d == 0) bat_sweep<0, R, GL>(P, it, prev, s, m);
+    else if (d == 1) bat_sweep<1, R, GL>(P, it, prev, s, m);
+    else bat_sweep<2, R, GL>(P, it, prev, s, m);
+    prev |= 1 << d;
+  }
+}
+
+void launch_bat_cons_ec(const BatchPlan& P, cudaStream_t s) {
+  if (P.cons_ec)
+    launch_persistent(k_bat_cons_ec, 128, 0, P, BK_LCELLS, BK_LCELLS, s, nullptr, P.descs, P.work[BK_LCELLS],
+                      P.nwork[BK_LCELLS]);
 }
 
 void launch_bat_lagrange_nodes(const BatchPlan& P, cudaStream_t s, KernelMarks* m) {
@@ -893,22 +933,14 @@ void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMark
   launch_bat_lagrange_nodes(P, s, m);
   if (P.precision)
     launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  else if (P.gl)   // the G limiters: the cell widths too
+    launch_persistent(k_bat_lagrange_cells<double, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   else
     launch_persistent(k_bat_lagrange_cells<double>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  int prev = 0;
-  for (int it = 0; it < 3; ++it) {
-    const int d = (it + sens) % 3;
-    if (P.precision) {
-      if (d == 0) bat_sweep<0, float>(P, it, prev, s, m);
-      else if (d == 1) bat_sweep<1, float>(P, it, prev, s, m);
-      else bat_sweep<2, float>(P, it, prev, s, m);
-    } else {
-      if (d == 0) bat_sweep<0, double>(P, it, prev, s, m);
-      else if (d == 1) bat_sweep<1, double>(P, it, prev, s, m);
-      else bat_sweep<2, double>(P, it, prev, s, m);
-    }
-    prev |= 1 << d;
-  }
+  if (P.precision) bat_sweeps<float, false>(P, sens, s, m);
+  else if (P.gl) bat_sweeps<double, true>(P, sens, s, m);
+  else bat_sweeps<double, false>(P, sens, s, m);
+  launch_bat_cons_ec(P, s);
   launch_bat_dt(P, s, m);
 }
 

@@ -28,14 +28,14 @@ struct Phys {
   int eos;              // environment 0: 0 PerfectGas, 1 StiffenedGas
   double pinf;          // its limit-tension
   int with_newton;      // Lagrange energy update by Newton iterations
-  int csts;             // schema-csts time scheme (one environment, FP64)
+  int csts;             // schema-csts time scheme (FP64)
   int lim_cell;         // limiter of the cell gradients: limiteur_id, or the pure-cell limiter when
                         // projection-pente-borne-mixte and projection-limiteur-pure-id 1 (RemapADIService.cc:369-375)
-  // projection-pente-borne (one environment, FP64, order 2): the flux variant
+  // projection-pente-borne (FP64, order 2): the flux variant
   // (0: computeFluxPP, 1: computeFluxPPPure), its debar fix, the limiter of its
   // reconstruction (computeY0), and whether the sweep is the first of the cycle
   int pb, pb_pure, pb_debar, pb_lim_y0, pb_first;
-  int cons_ec;          // conservation-energie-totale (RemapADI.axl:151; one environment, FP64)
+  int cons_ec;          // conservation-energie-totale (RemapADI.axl:151; FP64)
   int ext_dt;           // slabs: the cycle ends with the local dt minimum; the caller combines the
                         // ranks' minima and finishes the dt (mhy_dt_finish)
   // several environments: projection-pente-borne-mixte and projection-limiteur-pure-id, applied
@@ -136,7 +136,7 @@ void launch_remap_env(const CycleArgs& a, int sens, cudaStream_t s, KernelMarks*
 void launch_init_env(const CycleArgs& a, cudaStream_t s);
 constexpr int kKernelsPerCycleEnv = 11;
 
-// Batched cycle of many independent single-environment meshes.  Each kernel
+// Batched cycle of many independent meshes (the same K in each).  Each kernel
 // type has a work table: one (instance, bx, by, bz) entry per block of the
 // instance's own grid; a persistent grid of resident blocks walks the table.
 // The arguments of instance i are descs[i] in device memory.
@@ -156,6 +156,8 @@ struct BatchPlan {
   int occ_pct[BK_TUNE_SLOTS];   // persistent grid of each slot: % of the resident-block capacity
   int lines[BK_COUNT];          // lines per block of the y/z sweeps (8, 16, 32); the work shapes follow it
   int K;                        // environments of every instance
+  int gl;                       // every instance takes the G limiters (FP64): the GL sweeps and cell widths
+  int cons_ec;                  // some instance has conservation-energie-totale
 };
 // Events recorded after each launch of a cycle (autotuning), with the tuning
 // slot of each launch.
@@ -175,6 +177,7 @@ int persistent_grid(const void* kernel, int threads, size_t smem, int nwork, int
 void launch_bat_lagrange_nodes(const BatchPlan& P, cudaStream_t s, KernelMarks* m);
 void launch_bat_dt(const BatchPlan& P, cudaStream_t s, KernelMarks* m);
 void launch_batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m);
+void launch_bat_cons_ec(const BatchPlan& P, cudaStream_t s);
 void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s, KernelMarks* marks = nullptr);
 constexpr int kKernelsPerCycleBatch = 10;
 

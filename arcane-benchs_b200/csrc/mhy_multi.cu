@@ -812,10 +812,8 @@ __global__ void __launch_bounds__(256) k_env_finalize_cells(Dims dm, Scalars* __
 // EOS of every environment and the mixed-cell pressure and sound speed.  A
 // pure cell's environment values are its global values.
 template <int K>
-__global__ void __launch_bounds__(128) k_env_cons_ec(Dims dm, Phys ph, EnvState env, CellState st,
-                                                     const double* __restrict__ ecn, int linear) {
-  int i, j, k;
-  if (!block_item(dm.nx, dm.ny, dm.nz, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, i, j, k)) return;
+__device__ __forceinline__ void env_cons_ec_cell(const Dims& dm, const EnvState& env, const CellState& st,
+                                                 const double* __restrict__ ecn, int i, int j, int k) {
   const int C = (int)dm.C;
   const int c = (int)dm.cid(i, j, k);
   double delta_ec = 0.;
@@ -846,6 +844,14 @@ __global__ void __launch_bounds__(128) k_env_cons_ec(Dims dm, Phys ph, EnvState 
   }
   st.e[c] += delta_ec;
   st.p[c] = pm; st.cs[c] = cm;
+}
+
+template <int K>
+__global__ void __launch_bounds__(128) k_env_cons_ec(Dims dm, Phys ph, EnvState env, CellState st,
+                                                     const double* __restrict__ ecn, int linear) {
+  int i, j, k;
+  if (!block_item(dm.nx, dm.ny, dm.nz, blockIdx.x, linear ? -1 : (int)blockIdx.y, blockIdx.z, i, j, k)) return;
+  env_cons_ec_cell<K>(dm, env, st, ecn, i, j, k);
 }
 
 void launch_cons_ec_env(const CycleArgs& a, cudaStream_t s) {
@@ -1061,36 +1067,36 @@ void launch_remap_env(const CycleArgs& a0, int sens, cudaStream_t s, KernelMarks
 // grids (as the one-environment batch in mhy_cycle.cu).  The cell y/z sweeps
 // take 8 or 16 lines per block, the node y/z sweeps 8, as in one context.
 
-template <int K, typename R>
+template <int K, typename R, bool HC>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_env_lagrange_cells(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_lagrange_cells_body<K, R>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
+    k_cyc_lagrange_cells_body<K, R, false, HC>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
                                     a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
   }
 }
 
-template <int K, bool FIRST, typename R>
+template <int K, bool FIRST, typename R, bool GL>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_bat_env_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    env_sweep_cells_x_body<K, FIRST, R>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+    env_sweep_cells_x_body<K, FIRST, R, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
                                         a.dpf, a.Vlag, t.y, t.z, t.w);
   }
 }
 
-template <int K, int DD, bool FIRST, typename R, int LW>
+template <int K, int DD, bool FIRST, typename R, int LW, bool GL>
 __global__ void __launch_bounds__(32 * LW, kEnvMinBlocks * kLineWarps / LW) k_bat_env_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();                                   // the previous item's tile reads are done
-    env_sweep_cells_t_body<K, DD, FIRST, R, LW>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+    env_sweep_cells_t_body<K, DD, FIRST, R, LW, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
                                                 a.U[(it + 1) & 1], a.dpf, a.Vlag, t.y, t.z, t.w);
   }
 }
@@ -1109,27 +1115,29 @@ __global__ void __launch_bounds__(128) k_bat_env_finalize(const CycleArgs* __res
   }
 }
 
-template <bool FIRST, bool LAST, int K, typename R>
+template <bool FIRST, bool LAST, int K, typename R, bool GL>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_env_nodes_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm, a.ud[(it + 1) & 1],
-                                             a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
+                                                 a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm,
+                                                 a.vnorm, t.y, t.z, t.w, a.ecn);
   }
 }
 
-template <int DD, bool FIRST, bool LAST, int K, typename R>
+template <int DD, bool FIRST, bool LAST, int K, typename R, bool GL>
 __global__ void __launch_bounds__(32 * kLineWarps, TileGeom<kLineWarps>::minb) k_bat_env_nodes_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it, int prev) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, K, R, kLineWarps>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
-                                                                a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd,
-                                                                a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z, t.w);
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, K, R, kLineWarps, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh,
+                                                                    a.nm, a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf,
+                                                                    a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z,
+                                                                    t.w, a.ecn);
   }
 }
 
@@ -1143,76 +1151,95 @@ static void bat_env_launch(Kern kernel, int threads, size_t smem, const BatchPla
   mark(m, tk, s);
 }
 
-template <int K, int DD, bool FIRST, typename R>
+template <int K, int DD, bool FIRST, typename R, bool GL>
 static void bat_env_cells(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
   if constexpr (DD == 0) {
-    bat_env_launch(k_bat_env_cells_x<K, FIRST, R>, 32 * kLineWarps, 0, P, kind, kind, s, nullptr, P.descs,
+    bat_env_launch(k_bat_env_cells_x<K, FIRST, R, GL>, 32 * kLineWarps, 0, P, kind, kind, s, nullptr, P.descs,
                    P.work[kind], P.nwork[kind], it);
-  } else if (P.lines[kind] == 16) {
-    bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, 16>, 32 * 16,
+  } else if (!GL && P.lines[kind] == 16) {
+    bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, 16, false>, 32 * 16,
                    (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<16>::arr * sizeof(double), P, kind, kind, s,
                    nullptr, P.descs, P.work[kind], P.nwork[kind], it);
   } else {
-    bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, kLineWarps>, 32 * kLineWarps,
+    bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, kLineWarps, GL>, 32 * kLineWarps,
                    (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<kLineWarps>::arr * sizeof(double), P, kind,
                    kind, s, nullptr, P.descs, P.work[kind], P.nwork[kind], it);
   }
 }
 
-template <int K, int DD, bool FIRST, bool LAST, typename R>
+template <int K, int DD, bool FIRST, bool LAST, typename R, bool GL>
 static void bat_env_nodes(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_NODES_X + DD;
   if constexpr (DD == 0)
-    bat_env_launch(k_bat_env_nodes_x<FIRST, LAST, K, R>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
+    bat_env_launch(k_bat_env_nodes_x<FIRST, LAST, K, R, GL>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
                    P.work[kind], P.nwork[kind], it, prev);
   else
-    bat_env_launch(k_bat_env_nodes_t<DD, FIRST, LAST, K, R>, 32 * kLineWarps,
+    bat_env_launch(k_bat_env_nodes_t<DD, FIRST, LAST, K, R, GL>, 32 * kLineWarps,
                    NodeTileSize<DD, FIRST, LAST, K, kLineWarps>::bytes, P, kind, kind, s, m, P.descs, P.work[kind],
                    P.nwork[kind], it, prev);
 }
 
-template <int K, int DD, typename R>
+template <int K, int DD, typename R, bool GL>
 static void bat_env_sweep(const BatchPlan& P, int it, int prev, cudaStream_t s, KernelMarks* m) {
   const bool first = it == 0, last = it == 2;
-  if (first) bat_env_cells<K, DD, true, R>(P, it, s, m);
-  else bat_env_cells<K, DD, false, R>(P, it, s, m);
+  if (first) bat_env_cells<K, DD, true, R, GL>(P, it, s, m);
+  else bat_env_cells<K, DD, false, R, GL>(P, it, s, m);
   if (last)   // the end of the remap per cell, between the last cell and node sweeps
     bat_env_launch(k_bat_env_finalize<K>, 128, 0, P, BK_LCELLS, BK_CELLS_X + DD, s, nullptr, P.descs,
                    P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   else
     mark(m, BK_CELLS_X + DD, s);
-  if (first) bat_env_nodes<K, DD, true, false, R>(P, it, prev, s, m);
-  else if (last) bat_env_nodes<K, DD, false, true, R>(P, it, prev, s, m);
-  else bat_env_nodes<K, DD, false, false, R>(P, it, prev, s, m);
+  if (first) bat_env_nodes<K, DD, true, false, R, GL>(P, it, prev, s, m);
+  else if (last) bat_env_nodes<K, DD, false, true, R, GL>(P, it, prev, s, m);
+  else bat_env_nodes<K, DD, false, false, R, GL>(P, it, prev, s, m);
 }
 
-template <int K, typename R>
+// conservation-energie-totale of the instances that have it, over the Lagrange
+// cell kernel's tiles, after the last node sweep
+template <int K>
+__global__ void __launch_bounds__(128) k_bat_env_cons_ec(const CycleArgs* __restrict__ D, const int4* __restrict__ W,
+                                                         int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    if (!a.ph.cons_ec) continue;
+    int i, j, k;
+    if (block_item(a.dm.nx, a.dm.ny, a.dm.nz, t.y, t.z, t.w, i, j, k))
+      env_cons_ec_cell<K>(a.dm, a.env, a.st, a.ecn, i, j, k);
+  }
+}
+
+template <int K, typename R, bool GL>
 static void batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
   launch_bat_lagrange_nodes(P, s, m);
-  bat_env_launch(k_bat_env_lagrange_cells<K, R>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS],
-                 P.nwork[BK_LCELLS]);
+  bat_env_launch(k_bat_env_lagrange_cells<K, R, GL>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs,
+                 P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;
-    if (d == 0) bat_env_sweep<K, 0, R>(P, it, prev, s, m);
-    else if (d == 1) bat_env_sweep<K, 1, R>(P, it, prev, s, m);
-    else bat_env_sweep<K, 2, R>(P, it, prev, s, m);
+    if (d == 0) bat_env_sweep<K, 0, R, GL>(P, it, prev, s, m);
+    else if (d == 1) bat_env_sweep<K, 1, R, GL>(P, it, prev, s, m);
+    else bat_env_sweep<K, 2, R, GL>(P, it, prev, s, m);
     prev |= 1 << d;
   }
+  if (P.cons_ec)
+    bat_env_launch(k_bat_env_cons_ec<K>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, nullptr, P.descs, P.work[BK_LCELLS],
+                   P.nwork[BK_LCELLS]);
   launch_bat_dt(P, s, m);
 }
 
+template <int K>
+static void batch_cycle_env_k(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
+  if (P.precision) batch_cycle_env<K, float, false>(P, sens, s, m);
+  else if (P.gl) batch_cycle_env<K, double, true>(P, sens, s, m);
+  else batch_cycle_env<K, double, false>(P, sens, s, m);
+}
+
 void launch_batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
-  if (P.precision) {
-    if (P.K == 2) batch_cycle_env<2, float>(P, sens, s, m);
-    else if (P.K == 3) batch_cycle_env<3, float>(P, sens, s, m);
-    else batch_cycle_env<4, float>(P, sens, s, m);
-  } else {
-    if (P.K == 2) batch_cycle_env<2, double>(P, sens, s, m);
-    else if (P.K == 3) batch_cycle_env<3, double>(P, sens, s, m);
-    else batch_cycle_env<4, double>(P, sens, s, m);
-  }
+  if (P.K == 2) batch_cycle_env_k<2>(P, sens, s, m);
+  else if (P.K == 3) batch_cycle_env_k<3>(P, sens, s, m);
+  else batch_cycle_env_k<4>(P, sens, s, m);
 }
 
 // Called once per context before any cycle (and so before any graph capture).

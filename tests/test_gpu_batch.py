@@ -109,3 +109,43 @@ def test_batch_three_gases_autotuned_matches_single_contexts():
         g.step(20)
         for f in FIELDS:
             assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
+
+
+def _same_as_single_contexts(cases, cycles, oracle=True):
+    b = Batch(cases)
+    b.step(cycles)
+    b.synchronize()
+    for i, c in enumerate(cases):
+        g = Context(c)
+        g.step(cycles)
+        assert b.dt(i) == g.dt(), i
+        for f in FIELDS:
+            assert np.array_equal(b.field(i, f), g.field(f)), (i, f)
+        if oracle:
+            o = mhy_oracle.Oracle(c)
+            o.step(cycles)
+            for f in FIELDS:
+                assert np.array_equal(b.field(i, f), o.field(f)), (i, f, "oracle")
+        assert b.status(i) == 0
+    return b
+
+
+def test_batch_g_limiters_and_total_energy_match_single_contexts():
+    """The G limiters in every instance (ids 3..7 per instance: the GL sweeps
+    and the cell widths), conservation-energie-totale in some instances only
+    (its kernel skips the others)."""
+    cases = gen.batched(count=5, seed=33, side_lo=8, side_hi=16, cycles=25)
+    for i, c in enumerate(cases):
+        c.options.projection_limiteur_id = 3 + i % 5
+        c.options.conservation_energie_totale = i % 2
+    b = _same_as_single_contexts(cases, 25)
+    assert b.kernels_per_cycle() == 11
+
+
+def test_batch_two_gases_g_limiter_total_energy():
+    cases = two_gas_batch()
+    for i, c in enumerate(cases):
+        c.options.projection_limiteur_id = 5 if i % 2 else 6
+        c.options.conservation_energie_totale = 1 if i < 2 else 0
+    b = _same_as_single_contexts(cases, 20)
+    assert b.kernels_per_cycle() == 12

@@ -102,5 +102,3 @@ def test_cons_ec_refused_where_not_built():
     mixed.options.precision = 1
     with pytest.raises(MhyError):
         Context(mixed)
-    with pytest.raises(MhyError):
-        Batch([_ec(gen.sod(nx=20, ny=4, nz=4, cycles=2))])
