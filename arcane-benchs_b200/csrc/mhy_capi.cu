@@ -778,8 +778,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
     if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
     if ((opts[i].projection_limiteur_id >= 3) != (opts[0].projection_limiteur_id >= 3))
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters (ids 3..7) in every instance or in none");
-    if (opts[i].projection_pente_borne || opts[i].pente_borne_mixte)
-      return fail(MHY_ERR_UNSUPPORTED, "batched instances: pente-borne is not batched");
+    if ((opts[i].projection_pente_borne != 0) != (opts[0].projection_pente_borne != 0))
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: pente-borne in every instance or in none");
     if (opts[i].precision != opts[0].precision) return fail(MHY_ERR_ARG, "batched instances share one precision");
   }
   mhy_batch* b = new mhy_batch();
@@ -811,6 +811,7 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   b->plan.precision = opts[0].precision;
   b->plan.K = opts[0].nb_env;
   b->plan.gl = opts[0].projection_limiteur_id >= 3;   // the same in every instance (checked above)
+  b->plan.pb = opts[0].projection_pente_borne != 0;
   for (int i = 0; i < n; ++i) b->plan.cons_ec |= opts[i].conservation_energie_totale;
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
     b->plan.occ_pct[k] = 100;
@@ -920,9 +921,9 @@ inline bool line_slot(int k) {
 
 // The line counts a batch's sweeps are built for: any on one environment; with
 // several, 8 or 16 on the cell y/z sweeps and 8 on the node y/z sweeps; 8
-// everywhere with the G limiters.
+// everywhere with the G limiters or pente-borne.
 bool batch_tunable_lines(const mhy_batch* b, int k, int w) {
-  if (!line_slot(k) || b->plan.gl) return w == kLineWarps;   // the G limiters' sweeps keep 8 lines
+  if (!line_slot(k) || b->plan.gl || b->plan.pb) return w == kLineWarps;   // these sweeps keep 8 lines
   if (b->plan.K > 1) return w == kLineWarps || ((k == BK_CELLS_Y || k == BK_CELLS_Z) && w == 16);
   return true;
 }

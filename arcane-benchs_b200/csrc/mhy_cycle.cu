@@ -719,26 +719,40 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_lagrange_ce
   }
 }
 
-template <bool LAST, typename R, bool GL = false>
+template <bool LAST, typename R, bool GL = false, bool PB = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_cells_x_body<LAST, R, false, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
-                                                 a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+    if constexpr (PB) {   // the first sweep of a remap takes Phi from the Lagrange phase
+      Phys ph = a.ph;
+      ph.pb_first = it == 0;
+      k_cyc_sweep_cells_x_body<LAST, R, false, GL, PB>(a.dm, a.S, ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                   a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+    } else {
+      k_cyc_sweep_cells_x_body<LAST, R, false, GL, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                   a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+    }
   }
 }
 
-template <int DD, bool LAST, typename R, int LW, bool GL = false>
+template <int DD, bool LAST, typename R, int LW, bool GL = false, bool PB = false>
 __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_cells_t_body<DD, LAST, R, LW, false, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
-                                                      a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+    if constexpr (PB) {
+      Phys ph = a.ph;
+      ph.pb_first = it == 0;
+      k_cyc_sweep_cells_t_body<DD, LAST, R, LW, false, GL, PB>(a.dm, a.S, ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                           a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+    } else {
+      k_cyc_sweep_cells_t_body<DD, LAST, R, LW, false, GL, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                           a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+    }
   }
 }
 
@@ -844,16 +858,26 @@ static void launch_persistent(Kern kernel, int threads, size_t smem, const Batch
   mark(marks, tk, s);
 }
 
-template <int DD, bool LAST, typename R, int LW, bool GL>
+template <int DD, bool LAST, typename R, int LW, bool GL, bool PB = false>
 static void bat_cells_t(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
-  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW, GL>, 32 * LW, CellTileSize<LAST, LW>::bytes, P, kind, kind, s, m,
+  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW, GL, PB>, 32 * LW, CellTileSize<LAST, LW>::bytes, P, kind, kind, s, m,
                     P.descs, P.work[kind], P.nwork[kind], it);
 }
 
 template <int DD, bool LAST, typename R, bool GL>
 static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
+  if constexpr (sizeof(R) == 8) {
+    if (P.pb) {   // pente-borne: its own cell sweeps (the widths too), 8 lines
+      if constexpr (DD == 0)
+        launch_persistent(k_bat_sweep_cells_x<LAST, R, false, true>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
+                          P.work[kind], P.nwork[kind], it);
+      else
+        bat_cells_t<DD, LAST, R, 8, false, true>(P, it, s, m);
+      return;
+    }
+  }
   if constexpr (DD == 0) {
     launch_persistent(k_bat_sweep_cells_x<LAST, R, GL>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs, P.work[kind],
                       P.nwork[kind], it);
@@ -933,7 +957,7 @@ void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMark
   launch_bat_lagrange_nodes(P, s, m);
   if (P.precision)
     launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  else if (P.gl)   // the G limiters: the cell widths too
+  else if (P.gl || P.pb)   // the G limiters, pente-borne: the cell widths too
     launch_persistent(k_bat_lagrange_cells<double, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   else
     launch_persistent(k_bat_lagrange_cells<double>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);

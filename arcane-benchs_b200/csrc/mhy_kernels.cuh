@@ -157,6 +157,7 @@ struct BatchPlan {
   int lines[BK_COUNT];          // lines per block of the y/z sweeps (8, 16, 32); the work shapes follow it
   int K;                        // environments of every instance
   int gl;                       // every instance takes the G limiters (FP64): the GL sweeps and cell widths
+  int pb;                       // every instance takes projection-pente-borne (FP64): the PB cell sweeps
   int cons_ec;                  // some instance has conservation-energie-totale
 };
 // Events recorded after each launch of a cycle (autotuning), with the tuning

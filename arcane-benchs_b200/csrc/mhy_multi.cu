@@ -1078,25 +1078,25 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_env_lagrang
   }
 }
 
-template <int K, bool FIRST, typename R, bool GL>
+template <int K, bool FIRST, typename R, bool GL, bool PB = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_bat_env_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    env_sweep_cells_x_body<K, FIRST, R, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+    env_sweep_cells_x_body<K, FIRST, R, GL, false, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
                                         a.dpf, a.Vlag, t.y, t.z, t.w);
   }
 }
 
-template <int K, int DD, bool FIRST, typename R, int LW, bool GL>
+template <int K, int DD, bool FIRST, typename R, int LW, bool GL, bool PB = false>
 __global__ void __launch_bounds__(32 * LW, kEnvMinBlocks * kLineWarps / LW) k_bat_env_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();                                   // the previous item's tile reads are done
-    env_sweep_cells_t_body<K, DD, FIRST, R, LW, GL>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+    env_sweep_cells_t_body<K, DD, FIRST, R, LW, GL, false, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
                                                 a.U[(it + 1) & 1], a.dpf, a.Vlag, t.y, t.z, t.w);
   }
 }
@@ -1154,6 +1154,18 @@ static void bat_env_launch(Kern kernel, int threads, size_t smem, const BatchPla
 template <int K, int DD, bool FIRST, typename R, bool GL>
 static void bat_env_cells(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
+  if constexpr (sizeof(R) == 8) {
+    if (P.pb) {   // pente-borne: its own cell sweeps, 8 lines
+      if constexpr (DD == 0)
+        bat_env_launch(k_bat_env_cells_x<K, FIRST, R, false, true>, 32 * kLineWarps, 0, P, kind, kind, s, nullptr,
+                       P.descs, P.work[kind], P.nwork[kind], it);
+      else
+        bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, kLineWarps, false, true>, 32 * kLineWarps,
+                       (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<kLineWarps>::arr * sizeof(double), P,
+                       kind, kind, s, nullptr, P.descs, P.work[kind], P.nwork[kind], it);
+      return;
+    }
+  }
   if constexpr (DD == 0) {
     bat_env_launch(k_bat_env_cells_x<K, FIRST, R, GL>, 32 * kLineWarps, 0, P, kind, kind, s, nullptr, P.descs,
                    P.work[kind], P.nwork[kind], it);
@@ -1210,10 +1222,10 @@ __global__ void __launch_bounds__(128) k_bat_env_cons_ec(const CycleArgs* __rest
   }
 }
 
-template <int K, typename R, bool GL>
+template <int K, typename R, bool GL, bool HC>
 static void batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
   launch_bat_lagrange_nodes(P, s, m);
-  bat_env_launch(k_bat_env_lagrange_cells<K, R, GL>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs,
+  bat_env_launch(k_bat_env_lagrange_cells<K, R, HC>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs,
                  P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
@@ -1231,9 +1243,11 @@ static void batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, Kernel
 
 template <int K>
 static void batch_cycle_env_k(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
-  if (P.precision) batch_cycle_env<K, float, false>(P, sens, s, m);
-  else if (P.gl) batch_cycle_env<K, double, true>(P, sens, s, m);
-  else batch_cycle_env<K, double, false>(P, sens, s, m);
+  // HC: the cell widths (the G limiters, pente-borne); GL: the G limiters' sweeps
+  if (P.precision) batch_cycle_env<K, float, false, false>(P, sens, s, m);
+  else if (P.gl) batch_cycle_env<K, double, true, true>(P, sens, s, m);
+  else if (P.pb) batch_cycle_env<K, double, false, true>(P, sens, s, m);
+  else batch_cycle_env<K, double, false, false>(P, sens, s, m);
 }
 
 void launch_batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {

@@ -168,7 +168,8 @@ def test_pente_borne_two_gases_restart_dump():
         assert np.array_equal(a.field(f), b.field(f)), f
 
 
-def test_pente_borne_refused_for_batches():
+def test_pente_borne_in_some_batch_instances_is_refused():
+    """A batch takes pente-borne in every instance or in none."""
     cases = gen.batched(count=2, seed=3, side_lo=8, side_hi=10, cycles=1)
     cases[1].options.pente_borne = 1
     assert code_of(lambda: Batch(cases)) == ERR_UNSUPPORTED
