@@ -707,6 +707,7 @@ struct mhy_batch {
   std::vector<mhy_ctx*> inst;
   CycleArgs* d_descs = nullptr;
   int4* d_work[BK_COUNT] = {};
+  int4* d_o3work[3] = {};                       // order 3: face work tables per direction
   int order[BK_COUNT] = {};                     // work-table order of each kind (mhy_tuning.order)
   BatchPlan plan{};
   int sens = 0;
@@ -762,6 +763,7 @@ void mhy_batch_destroy(mhy_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (int s = 0; s < 3; ++s) if (b->graph[s]) cudaGraphExecDestroy(b->graph[s]);
   for (int k = 0; k < BK_COUNT; ++k) if (b->d_work[k]) cudaFree(b->d_work[k]);
+  for (int d = 0; d < 3; ++d) if (b->d_o3work[d]) cudaFree(b->d_o3work[d]);
   if (b->d_descs) cudaFree(b->d_descs);
   for (mhy_ctx* c : b->inst) mhy_destroy(c);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -775,7 +777,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
     if (opts[i].nb_env != opts[0].nb_env)
       return fail(MHY_ERR_UNSUPPORTED, "batched instances share one number of environments");
     if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
-    if (opts[i].ordre_projection == 3) return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 is not batched");
+    if ((opts[i].ordre_projection == 3) != (opts[0].ordre_projection == 3))
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 in every instance or in none");
     if ((opts[i].projection_limiteur_id >= 3) != (opts[0].projection_limiteur_id >= 3))
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: the G limiters (ids 3..7) in every instance or in none");
     if ((opts[i].projection_pente_borne != 0) != (opts[0].projection_pente_borne != 0))
@@ -812,6 +815,23 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   b->plan.K = opts[0].nb_env;
   b->plan.gl = opts[0].projection_limiteur_id >= 3;   // the same in every instance (checked above)
   b->plan.pb = opts[0].projection_pente_borne != 0;
+  b->plan.o3 = opts[0].ordre_projection == 3;
+  if (b->plan.o3) {
+    // face work tables: (instance, chunk of 128 consecutive faces of direction d), instance-major
+    for (int d = 0; d < 3; ++d) {
+      std::vector<int4> w;
+      for (int i = 0; i < n; ++i) {
+        const Dims& dm = b->inst[i]->dm;
+        const long long Fd = d == 0 ? dm.Fx : (d == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
+        for (long long x = 0; x < (Fd + 127) / 128; ++x) w.push_back(make_int4(i, (int)x, 0, 0));
+      }
+      err = cudaMalloc(&b->d_o3work[d], w.size() * sizeof(int4));
+      if (err == cudaSuccess) err = cudaMemcpy(b->d_o3work[d], w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice);
+      if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
+      b->plan.o3work[d] = b->d_o3work[d];
+      b->plan.o3nwork[d] = (int)w.size();
+    }
+  }
   for (int i = 0; i < n; ++i) b->plan.cons_ec |= opts[i].conservation_energie_totale;
   for (int k = 0; k < BK_TUNE_SLOTS; ++k) {
     b->plan.occ_pct[k] = 100;
@@ -923,7 +943,7 @@ inline bool line_slot(int k) {
 // several, 8 or 16 on the cell y/z sweeps and 8 on the node y/z sweeps; 8
 // everywhere with the G limiters or pente-borne.
 bool batch_tunable_lines(const mhy_batch* b, int k, int w) {
-  if (!line_slot(k) || b->plan.gl || b->plan.pb) return w == kLineWarps;   // these sweeps keep 8 lines
+  if (!line_slot(k) || b->plan.gl || b->plan.pb || b->plan.o3) return w == kLineWarps;   // these sweeps keep 8 lines
   if (b->plan.K > 1) return w == kLineWarps || ((k == BK_CELLS_Y || k == BK_CELLS_Z) && w == 16);
   return true;
 }
@@ -1322,7 +1342,8 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
 }
 int mhy_batch_kernels_per_cycle(mhy_batch* b) {
   // several environments: the end-of-remap kernel; conservation-energie-totale: its kernel
-  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) + (b->plan.cons_ec ? 1 : 0) : 0;
+  // order 3: the face kernel of each direction
+  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) + (b->plan.cons_ec ? 1 : 0) + (b->plan.o3 ? 3 : 0) : 0;
 }
 void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
 

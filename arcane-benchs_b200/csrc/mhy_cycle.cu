@@ -552,9 +552,8 @@ void launch_lagrange_cells(const CycleArgs& a, cudaStream_t s) {
 // each inner face (clamped at the ends of the line) from the sweep's input U,
 // the cell widths h along D and u_f dt; written to fd.phi3 [4][F_D].
 template <int D>
-__global__ void __launch_bounds__(128) k_o3_faces(Dims dm, const Scalars* __restrict__ S,
-    const double* __restrict__ Uin, FaceData fd) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void o3_faces_item(const Dims& dm, const Scalars* __restrict__ S,
+    const double* __restrict__ Uin, const FaceData& fd, long long t) {
   const long long Fd = D == 0 ? dm.Fx : (D == 1 ? dm.Fy : dm.F - dm.Fx - dm.Fy);
   if (t >= Fd) return;
   int i, j, k; dm.fdijk(D, t, i, j, k);
@@ -579,6 +578,12 @@ __global__ void __launch_bounds__(128) k_o3_faces(Dims dm, const Scalars* __rest
   const double vdt = fd.u[D][t] * S->dt;
 #pragma unroll
   for (int v = 0; v < 4; ++v) fd.phi3[v * Fd + t] = o3_flux(y[v], h, vdt);
+}
+
+template <int D>
+__global__ void __launch_bounds__(128) k_o3_faces(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ Uin, FaceData fd) {
+  o3_faces_item<D>(dm, S, Uin, fd, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
 template <typename R>
@@ -719,7 +724,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_lagrange_ce
   }
 }
 
-template <bool LAST, typename R, bool GL = false, bool PB = false>
+template <bool LAST, typename R, bool GL = false, bool PB = false, bool O3 = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
@@ -728,16 +733,16 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_c
     if constexpr (PB) {   // the first sweep of a remap takes Phi from the Lagrange phase
       Phys ph = a.ph;
       ph.pb_first = it == 0;
-      k_cyc_sweep_cells_x_body<LAST, R, false, GL, PB>(a.dm, a.S, ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
-                                                   a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+      k_cyc_sweep_cells_x_body<LAST, R, O3, GL, PB>(a.dm, a.S, ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
     } else {
-      k_cyc_sweep_cells_x_body<LAST, R, false, GL, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
-                                                   a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+      k_cyc_sweep_cells_x_body<LAST, R, O3, GL, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
     }
   }
 }
 
-template <int DD, bool LAST, typename R, int LW, bool GL = false, bool PB = false>
+template <int DD, bool LAST, typename R, int LW, bool GL = false, bool PB = false, bool O3 = false>
 __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
@@ -747,12 +752,24 @@ __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_cells
     if constexpr (PB) {
       Phys ph = a.ph;
       ph.pb_first = it == 0;
-      k_cyc_sweep_cells_t_body<DD, LAST, R, LW, false, GL, PB>(a.dm, a.S, ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
-                                                           a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+      k_cyc_sweep_cells_t_body<DD, LAST, R, LW, O3, GL, PB>(a.dm, a.S, ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                        a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
     } else {
-      k_cyc_sweep_cells_t_body<DD, LAST, R, LW, false, GL, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
-                                                           a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
+      k_cyc_sweep_cells_t_body<DD, LAST, R, LW, O3, GL, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+                                                        a.U[(it + 1) & 1], a.dpf, a.st, t.y, t.z, t.w);
     }
+  }
+}
+
+// Order-3 face values of direction D over the face work table of D: items
+// (instance, chunk of 128 consecutive faces), the sweep's input U[it & 1].
+template <int D>
+__global__ void __launch_bounds__(128) k_bat_o3_faces(const CycleArgs* __restrict__ A, const int4* __restrict__ W,
+                                                      int nw, int it) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = A[t.x];
+    o3_faces_item<D>(a.dm, a.S, a.U[it & 1], a.fd, (long long)t.y * 128 + threadIdx.x);
   }
 }
 
@@ -858,17 +875,35 @@ static void launch_persistent(Kern kernel, int threads, size_t smem, const Batch
   mark(marks, tk, s);
 }
 
-template <int DD, bool LAST, typename R, int LW, bool GL, bool PB = false>
+template <int DD, bool LAST, typename R, int LW, bool GL, bool PB = false, bool O3 = false>
 static void bat_cells_t(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
-  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW, GL, PB>, 32 * LW, CellTileSize<LAST, LW>::bytes, P, kind, kind, s, m,
-                    P.descs, P.work[kind], P.nwork[kind], it);
+  launch_persistent(k_bat_sweep_cells_t<DD, LAST, R, LW, GL, PB, O3>, 32 * LW, CellTileSize<LAST, LW, O3>::bytes, P,
+                    kind, kind, s, m, P.descs, P.work[kind], P.nwork[kind], it);
+}
+
+// Order 3: the face values of direction DD from the sweep's input (no mark of
+// their own: their time counts towards the cell sweep's slot).
+template <int DD>
+static void launch_bat_o3_faces(const BatchPlan& P, int it, cudaStream_t s) {
+  auto kern = k_bat_o3_faces<DD>;
+  if (P.o3nwork[DD] > 0)
+    kern<<<persistent_blocks(kern, 128, 0, P.o3nwork[DD], 100), 128, 0, s>>>(P.descs, P.o3work[DD], P.o3nwork[DD], it);
 }
 
 template <int DD, bool LAST, typename R, bool GL>
 static void bat_cells_d(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
   if constexpr (sizeof(R) == 8) {
+    if (P.o3) {   // order 3: the face values first, then the O3 cell sweeps, 8 lines
+      launch_bat_o3_faces<DD>(P, it, s);
+      if constexpr (DD == 0)
+        launch_persistent(k_bat_sweep_cells_x<LAST, R, GL, false, true>, 32 * kLineWarps, 0, P, kind, kind, s, m,
+                          P.descs, P.work[kind], P.nwork[kind], it);
+      else
+        bat_cells_t<DD, LAST, R, 8, GL, false, true>(P, it, s, m);
+      return;
+    }
     if (P.pb) {   // pente-borne: its own cell sweeps (the widths too), 8 lines
       if constexpr (DD == 0)
         launch_persistent(k_bat_sweep_cells_x<LAST, R, false, true>, 32 * kLineWarps, 0, P, kind, kind, s, m, P.descs,
@@ -957,7 +992,7 @@ void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMark
   launch_bat_lagrange_nodes(P, s, m);
   if (P.precision)
     launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  else if (P.gl || P.pb)   // the G limiters, pente-borne: the cell widths too
+  else if (P.gl || P.pb || P.o3)   // the G limiters, pente-borne, order 3: the cell widths too
     launch_persistent(k_bat_lagrange_cells<double, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   else
     launch_persistent(k_bat_lagrange_cells<double>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);

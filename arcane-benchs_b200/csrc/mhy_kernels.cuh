@@ -158,6 +158,9 @@ struct BatchPlan {
   int K;                        // environments of every instance
   int gl;                       // every instance takes the G limiters (FP64): the GL sweeps and cell widths
   int pb;                       // every instance takes projection-pente-borne (FP64): the PB cell sweeps
+  int o3;                       // every instance takes order 3 (FP64): face values, then the O3 cell sweeps
+  const int4* o3work[3];        // order 3: face work tables (instance, chunk of 128 faces) per direction
+  int o3nwork[3];
   int cons_ec;                  // some instance has conservation-energie-totale
 };
 // Events recorded after each launch of a cycle (autotuning), with the tuning

@@ -545,10 +545,9 @@ __global__ void __launch_bounds__(32 * W, kEnvMinBlocks * kLineWarps / W) k_env_
 // Faces are written in line order: the position along D fastest, then x,
 // then the remaining axis (for D = 0 the usual face order).
 template <int D, int K, bool FIRST>
-__global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __restrict__ S,
-    const double* __restrict__ Uin, FaceData fd, const double* __restrict__ Vlag) {
+__device__ __forceinline__ void o3_faces_env_item(const Dims& dm, const Scalars* __restrict__ S,
+    const double* __restrict__ Uin, const FaceData& fd, const double* __restrict__ Vlag, long long t) {
   constexpr int NV = 3 * K + 1;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long Fd = dm.nfd(D);
   if (t >= Fd) return;
   const int n = dm.ncd(D);
@@ -607,6 +606,24 @@ __global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __
   }
 #pragma unroll
   for (int v = 0; v < NV; ++v) fd.phi3[v * Fd + t] = pf[v];
+}
+
+template <int D, int K, bool FIRST>
+__global__ void __launch_bounds__(128) k_o3_faces_env(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ Uin, FaceData fd, const double* __restrict__ Vlag) {
+  o3_faces_env_item<D, K, FIRST>(dm, S, Uin, fd, Vlag, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
+// The same over the face work table of D (instance, chunk of 128 faces), the
+// sweep's input U[it & 1].
+template <int D, int K, bool FIRST>
+__global__ void __launch_bounds__(128) k_bat_o3_faces_env(const CycleArgs* __restrict__ A, const int4* __restrict__ W,
+                                                          int nw, int it) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = A[t.x];
+    o3_faces_env_item<D, K, FIRST>(a.dm, a.S, a.U[it & 1], a.fd, a.Vlag, (long long)t.y * 128 + threadIdx.x);
+  }
 }
 
 // ---- end of the remap, per cell ----------------------------------------
@@ -1078,25 +1095,25 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_env_lagrang
   }
 }
 
-template <int K, bool FIRST, typename R, bool GL, bool PB = false>
+template <int K, bool FIRST, typename R, bool GL, bool PB = false, bool O3 = false>
 __global__ void __launch_bounds__(32 * kLineWarps, kEnvMinBlocks) k_bat_env_cells_x(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    env_sweep_cells_x_body<K, FIRST, R, GL, false, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
+    env_sweep_cells_x_body<K, FIRST, R, GL, O3, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1], a.U[(it + 1) & 1],
                                         a.dpf, a.Vlag, t.y, t.z, t.w);
   }
 }
 
-template <int K, int DD, bool FIRST, typename R, int LW, bool GL, bool PB = false>
+template <int K, int DD, bool FIRST, typename R, int LW, bool GL, bool PB = false, bool O3 = false>
 __global__ void __launch_bounds__(32 * LW, kEnvMinBlocks * kLineWarps / LW) k_bat_env_cells_t(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw, int it) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();                                   // the previous item's tile reads are done
-    env_sweep_cells_t_body<K, DD, FIRST, R, LW, GL, false, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
+    env_sweep_cells_t_body<K, DD, FIRST, R, LW, GL, O3, PB>(a.dm, a.S, a.ph, a.fd, a.n0, a.xc, a.ofn, a.U[it & 1],
                                                 a.U[(it + 1) & 1], a.dpf, a.Vlag, t.y, t.z, t.w);
   }
 }
@@ -1155,6 +1172,20 @@ template <int K, int DD, bool FIRST, typename R, bool GL>
 static void bat_env_cells(const BatchPlan& P, int it, cudaStream_t s, KernelMarks* m) {
   const int kind = BK_CELLS_X + DD;
   if constexpr (sizeof(R) == 8) {
+    if (P.o3) {   // order 3: the face values first, then the O3 cell sweeps (no gradient), 8 lines
+      auto fk = k_bat_o3_faces_env<DD, K, FIRST>;
+      if (P.o3nwork[DD] > 0)
+        fk<<<persistent_grid((const void*)fk, 128, 0, P.o3nwork[DD], 100), 128, 0, s>>>(P.descs, P.o3work[DD],
+                                                                                   P.o3nwork[DD], it);
+      if constexpr (DD == 0)
+        bat_env_launch(k_bat_env_cells_x<K, FIRST, R, false, false, true>, 32 * kLineWarps, 0, P, kind, kind, s,
+                       nullptr, P.descs, P.work[kind], P.nwork[kind], it);
+      else
+        bat_env_launch(k_bat_env_cells_t<K, DD, FIRST, R, kLineWarps, false, false, true>, 32 * kLineWarps,
+                       (size_t)env_cells_staged_arrays<K, FIRST>() * TileGeom<kLineWarps>::arr * sizeof(double), P,
+                       kind, kind, s, nullptr, P.descs, P.work[kind], P.nwork[kind], it);
+      return;
+    }
     if (P.pb) {   // pente-borne: its own cell sweeps, 8 lines
       if constexpr (DD == 0)
         bat_env_launch(k_bat_env_cells_x<K, FIRST, R, false, true>, 32 * kLineWarps, 0, P, kind, kind, s, nullptr,
@@ -1243,10 +1274,10 @@ static void batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, Kernel
 
 template <int K>
 static void batch_cycle_env_k(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
-  // HC: the cell widths (the G limiters, pente-borne); GL: the G limiters' sweeps
+  // HC: the cell widths (the G limiters, pente-borne, order 3); GL: the G limiters' sweeps
   if (P.precision) batch_cycle_env<K, float, false, false>(P, sens, s, m);
   else if (P.gl) batch_cycle_env<K, double, true, true>(P, sens, s, m);
-  else if (P.pb) batch_cycle_env<K, double, false, true>(P, sens, s, m);
+  else if (P.pb || P.o3) batch_cycle_env<K, double, false, true>(P, sens, s, m);
   else batch_cycle_env<K, double, false, false>(P, sens, s, m);
 }
 

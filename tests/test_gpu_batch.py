@@ -203,6 +203,45 @@ def test_batch_two_gases_pente_borne(mixte):
         assert [finite(b, i) for i in range(b.size())] == [True, False, True, False]
 
 
+def test_batch_order3_matches_single_contexts():
+    """Order 3 in every instance: the face kernel of each direction over the
+    face work table, then the O3 cell sweeps (limiters and total energy per
+    instance)."""
+    cases = gen.batched(count=5, seed=37, side_lo=8, side_hi=16, cycles=25)
+    for i, c in enumerate(cases):
+        c.options.ordre_projection = 3
+        c.options.projection_limiteur_id = (0, 1, 2, 1, 0)[i]
+        c.options.conservation_energie_totale = i % 2
+    b = _same_as_single_contexts(cases, 25)
+    assert b.kernels_per_cycle() == 14
+
+
+def test_batch_order3_g_limiters_match_single_contexts():
+    cases = gen.batched(count=4, seed=38, side_lo=8, side_hi=14, cycles=20)
+    for i, c in enumerate(cases):
+        c.options.ordre_projection = 3
+        c.options.projection_limiteur_id = 3 + i
+    _same_as_single_contexts(cases, 20)
+
+
+@pytest.mark.parametrize("limiter", [0, 5])
+def test_batch_two_gases_order3(limiter):
+    cases = two_gas_batch()
+    for c in cases:
+        c.options.ordre_projection = 3
+        c.options.projection_limiteur_id = limiter
+    b = _same_as_single_contexts(cases, 20)
+    assert b.kernels_per_cycle() == 14
+
+
+def test_batch_three_gases_order3():
+    cases = [gen.three_material(cycles=15), gen.three_material(cycles=15)]
+    cases[1].options.deltat_init = 2.0e-5
+    for c in cases:
+        c.options.ordre_projection = 3
+    _same_as_single_contexts(cases, 15)
+
+
 def test_batch_two_gases_pure_limiter_switch():
     cases = two_gas_batch()
     for c in cases:

@@ -92,6 +92,6 @@ def test_order3_unsupported_forms_are_refused():
     with pytest.raises(MhyError):
         Context(gen.sod(cycles=5, options=gen.Options(ordre_projection=3, precision=1)))
     cases = gen.batched(count=2, seed=5, side_lo=8, side_hi=10, cycles=5)
-    cases[0].options.ordre_projection = 3
+    cases[0].options.ordre_projection = 3        # a batch takes order 3 in every instance or in none
     with pytest.raises(MhyError):
         Batch(cases)
