@@ -708,6 +708,7 @@ struct mhy_batch {
   CycleArgs* d_descs = nullptr;
   int4* d_work[BK_COUNT] = {};
   int4* d_o3work[3] = {};                       // order 3: face work tables per direction
+  int4* d_fwork = nullptr;                      // schema-csts: face work table (all directions)
   int order[BK_COUNT] = {};                     // work-table order of each kind (mhy_tuning.order)
   BatchPlan plan{};
   int sens = 0;
@@ -764,6 +765,7 @@ void mhy_batch_destroy(mhy_batch* b) {
   for (int s = 0; s < 3; ++s) if (b->graph[s]) cudaGraphExecDestroy(b->graph[s]);
   for (int k = 0; k < BK_COUNT; ++k) if (b->d_work[k]) cudaFree(b->d_work[k]);
   for (int d = 0; d < 3; ++d) if (b->d_o3work[d]) cudaFree(b->d_o3work[d]);
+  if (b->d_fwork) cudaFree(b->d_fwork);
   if (b->d_descs) cudaFree(b->d_descs);
   for (mhy_ctx* c : b->inst) mhy_destroy(c);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -776,7 +778,8 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   for (int i = 0; i < n; ++i) {
     if (opts[i].nb_env != opts[0].nb_env)
       return fail(MHY_ERR_UNSUPPORTED, "batched instances share one number of environments");
-    if (opts[i].schema_csts) return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts is not batched");
+    if ((opts[i].schema_csts != 0) != (opts[0].schema_csts != 0))
+      return fail(MHY_ERR_UNSUPPORTED, "batched instances: schema-csts in every instance or in none");
     if ((opts[i].ordre_projection == 3) != (opts[0].ordre_projection == 3))
       return fail(MHY_ERR_UNSUPPORTED, "batched instances: order 3 in every instance or in none");
     if ((opts[i].projection_limiteur_id >= 3) != (opts[0].projection_limiteur_id >= 3))
@@ -816,6 +819,18 @@ int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts
   b->plan.gl = opts[0].projection_limiteur_id >= 3;   // the same in every instance (checked above)
   b->plan.pb = opts[0].projection_pente_borne != 0;
   b->plan.o3 = opts[0].ordre_projection == 3;
+  b->plan.csts = opts[0].schema_csts != 0;
+  if (b->plan.csts) {
+    // face work table: (instance, chunk of 128 consecutive faces of all directions), instance-major
+    std::vector<int4> w;
+    for (int i = 0; i < n; ++i)
+      for (long long x = 0; x < (b->inst[i]->dm.F + 127) / 128; ++x) w.push_back(make_int4(i, (int)x, 0, 0));
+    err = cudaMalloc(&b->d_fwork, w.size() * sizeof(int4));
+    if (err == cudaSuccess) err = cudaMemcpy(b->d_fwork, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) { mhy_batch_destroy(b); return fail(MHY_ERR_OOM, cudaGetErrorString(err)); }
+    b->plan.fwork = b->d_fwork;
+    b->plan.nfwork = (int)w.size();
+  }
   if (b->plan.o3) {
     // face work tables: (instance, chunk of 128 consecutive faces of direction d), instance-major
     for (int d = 0; d < 3; ++d) {
@@ -1342,8 +1357,10 @@ int mhy_batch_autotune(mhy_batch* b, int cycles, mhy_tuning* out) {
 }
 int mhy_batch_kernels_per_cycle(mhy_batch* b) {
   // several environments: the end-of-remap kernel; conservation-energie-totale: its kernel
-  // order 3: the face kernel of each direction
-  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) + (b->plan.cons_ec ? 1 : 0) + (b->plan.o3 ? 3 : 0) : 0;
+  // order 3: the face kernel of each direction; schema-csts: the forward step and the face velocities
+  return b ? kKernelsPerCycleBatch + (b->plan.K > 1 ? 1 : 0) + (b->plan.cons_ec ? 1 : 0) + (b->plan.o3 ? 3 : 0) +
+                 (b->plan.csts ? 2 : 0)
+           : 0;
 }
 void* mhy_batch_get_stream(mhy_batch* b) { return b ? (void*)b->stream : nullptr; }
 

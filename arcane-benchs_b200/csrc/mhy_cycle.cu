@@ -98,12 +98,12 @@ __global__ void __launch_bounds__(128) k_cyc_lagrange_nodes(Dims dm, const Scala
 // current pressure plus this cycle's pseudo-viscosity (pq, summed by the cell
 // kernel; no boundary condition); xl = the Lagrangian node coordinates
 // x0 + v_h dt, which the remap keeps.
-__global__ void __launch_bounds__(128) k_csts_forward(Dims dm, const Scalars* __restrict__ S,
+__device__ __forceinline__ void csts_forward_item(const Dims& dm, const Scalars* __restrict__ S,
     const double* __restrict__ pq, const double* __restrict__ cqs,
     const double* __restrict__ nm, const double* __restrict__ x0, const double* __restrict__ vh,
-    double* __restrict__ vf, double* __restrict__ xl) {
+    double* __restrict__ vf, double* __restrict__ xl, int bx_, int by_, int bz_) {
   int i, j, k;
-  if (!block_item(dm.nx + 1, dm.ny + 1, dm.nz + 1, blockIdx.x, -1, 0, i, j, k)) return;
+  if (!block_item(dm.nx + 1, dm.ny + 1, dm.nz + 1, bx_, by_, bz_, i, j, k)) return;
   const long long n = dm.nid(i, j, k), N = dm.N;
   const double dt = S->dt;
   const D3 F = node_force<double, true>(dm, i, j, k, pq, nullptr, cqs);
@@ -115,12 +115,18 @@ __global__ void __launch_bounds__(128) k_csts_forward(Dims dm, const Scalars* __
   for (int a = 0; a < 3; ++a) xl[a * N + n] = x0[a * N + n] + vh[a * N + n] * dt;
 }
 
+__global__ void __launch_bounds__(128) k_csts_forward(Dims dm, const Scalars* __restrict__ S,
+    const double* __restrict__ pq, const double* __restrict__ cqs,
+    const double* __restrict__ nm, const double* __restrict__ x0, const double* __restrict__ vh,
+    double* __restrict__ vf, double* __restrict__ xl) {
+  csts_forward_item(dm, S, pq, cqs, nm, x0, vh, vf, xl, blockIdx.x, -1, 0);
+}
+
 // schema-csts remap face velocities (PrepareRemap.cc:69-79): u_f =
 // (0.25 sum over the face nodes of 0.5 (v + v_n)) . n0, with v the forward
 // velocity and v_n the backward one, for every face of every direction.
-__global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __restrict__ vf,
-    const double* __restrict__ vnb, const double* __restrict__ n0, FaceData fd) {
-  const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void csts_face_u_item(const Dims& dm, const double* __restrict__ vf,
+    const double* __restrict__ vnb, const double* __restrict__ n0, const FaceData& fd, long long f) {
   if (f >= dm.F) return;
   int d; long long t;
   if (f < dm.Fx) { d = 0; t = f; } else if (f < dm.Fx + dm.Fy) { d = 1; t = f - dm.Fx; } else { d = 2; t = f - dm.Fx - dm.Fy; }
@@ -134,6 +140,11 @@ __global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __re
     vm = vm + 0.5 * (d3(vf[m], vf[N + m], vf[2 * N + m]) + d3(vnb[m], vnb[N + m], vnb[2 * N + m]));
   }
   fd.u[d][t] = dot(.25 * vm, d3(n0[f], n0[dm.F + f], n0[2 * dm.F + f]));
+}
+
+__global__ void __launch_bounds__(128) k_csts_face_u(Dims dm, const double* __restrict__ vf,
+    const double* __restrict__ vnb, const double* __restrict__ n0, FaceData fd) {
+  csts_face_u_item(dm, vf, vnb, n0, fd, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
 
@@ -706,21 +717,42 @@ __global__ void __launch_bounds__(128) k_bat_lagrange_nodes(const CycleArgs* __r
     if constexpr (sizeof(R) == 4)
       k_cyc_lagrange_nodes_body<float>(a.dm, a.S, a.st.p, a.st.q, a.cqs32, a.nm, a.v, a.bcmask, a.bct, a.vh, nullptr,
                                        t.y, t.z, t.w);
-    else
-      k_cyc_lagrange_nodes_body<double>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, nullptr,
+    else   // vnb: schema-csts (null otherwise)
+      k_cyc_lagrange_nodes_body<double>(a.dm, a.S, a.st.p, a.st.q, a.cqs, a.nm, a.v, a.bcmask, a.bct, a.vh, a.vnb,
                                         t.y, t.z, t.w);
   }
 }
 
-template <typename R, bool HC = false>
+template <typename R, bool HC = false, bool CSTS = false>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_lagrange_cells(const CycleArgs* __restrict__ D,
                                                                                    const int4* __restrict__ W, int nw) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_lagrange_cells_body<1, R, false, HC>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
-                                               a.st.cs, a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env,
-                                               a.Vlag, t.y, t.z, t.w);
+    k_cyc_lagrange_cells_body<1, R, CSTS, HC>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
+                                              a.st.cs, a.st.mass, a.cqs, CSTS ? nullptr : a.cqs32, a.L, a.U[0], a.xc,
+                                              a.fd, a.env, a.Vlag, t.y, t.z, t.w, a.vnb, a.pf);
+  }
+}
+
+// schema-csts of every instance: the forward velocity and the Lagrangian
+// coordinates over the node tiles, then the face velocities over the face
+// work table (instance, chunk of 128 faces of all directions)
+__global__ void __launch_bounds__(128) k_bat_csts_forward(const CycleArgs* __restrict__ D, const int4* __restrict__ W,
+                                                          int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    csts_forward_item(a.dm, a.S, a.pf, a.cqs, a.nm, a.x0, a.vh, a.vf, a.xl, t.y, t.z, t.w);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_bat_csts_face_u(const CycleArgs* __restrict__ D, const int4* __restrict__ W,
+                                                         int nw) {
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    const int4 t = W[w];
+    const CycleArgs& a = D[t.x];
+    csts_face_u_item(a.dm, a.vf, a.vnb, a.n0, a.fd, (long long)t.y * 128 + threadIdx.x);
   }
 }
 
@@ -779,7 +811,8 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_sweep_n
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
+    // schema-csts: the forward velocity on the Lagrangian coordinates (xl is null otherwise)
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, 1, R, GL>(a.dm, a.S, a.ph, prev, a.x0, a.xl, a.ph.csts ? a.vf : a.vh, a.nm,
                                                  a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm,
                                                  a.vnorm, t.y, t.z, t.w, a.ecn);
   }
@@ -792,9 +825,10 @@ __global__ void __launch_bounds__(32 * LW, TileGeom<LW>::minb) k_bat_sweep_nodes
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
-                                                         a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v,
-                                                         a.nm, a.vnorm, t.y, t.z, t.w, a.ecn);
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, 1, R, LW, GL>(a.dm, a.S, a.ph, prev, a.x0, a.xl,
+                                                         a.ph.csts ? a.vf : a.vh, a.nm, a.ud[(it + 1) & 1],
+                                                         a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm, a.vnorm,
+                                                         t.y, t.z, t.w, a.ecn);
   }
 }
 
@@ -987,15 +1021,30 @@ void launch_bat_dt(const BatchPlan& P, cudaStream_t s, KernelMarks* m) {
   mark(m, BK_DT_FINISH, s);
 }
 
+void launch_bat_csts_forward(const BatchPlan& P, cudaStream_t s) {
+  if (!P.csts) return;
+  launch_persistent(k_bat_csts_forward, 128, 0, P, BK_LNODES, BK_LNODES, s, nullptr, P.descs, P.work[BK_LNODES],
+                    P.nwork[BK_LNODES]);
+  if (P.nfwork > 0)
+    k_bat_csts_face_u<<<persistent_blocks(k_bat_csts_face_u, 128, 0, P.nfwork, 100), 128, 0, s>>>(P.descs, P.fwork,
+                                                                                                 P.nfwork);
+}
+
 void launch_batch_cycle(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
   if (P.K > 1) { launch_batch_cycle_env(P, sens, s, m); return; }
   launch_bat_lagrange_nodes(P, s, m);
+  const bool hc = P.gl || P.pb || P.o3;   // the G limiters, pente-borne, order 3: the cell widths too
   if (P.precision)
     launch_persistent(k_bat_lagrange_cells<float>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
-  else if (P.gl || P.pb || P.o3)   // the G limiters, pente-borne, order 3: the cell widths too
+  else if (P.csts && hc)
+    launch_persistent(k_bat_lagrange_cells<double, true, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  else if (P.csts)
+    launch_persistent(k_bat_lagrange_cells<double, false, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  else if (hc)
     launch_persistent(k_bat_lagrange_cells<double, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   else
     launch_persistent(k_bat_lagrange_cells<double>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs, P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  launch_bat_csts_forward(P, s);   // PrepareRemap.cc:456, then the face velocities
   if (P.precision) bat_sweeps<float, false>(P, sens, s, m);
   else if (P.gl) bat_sweeps<double, true>(P, sens, s, m);
   else bat_sweeps<double, false>(P, sens, s, m);

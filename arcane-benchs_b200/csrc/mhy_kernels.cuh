@@ -159,6 +159,9 @@ struct BatchPlan {
   int gl;                       // every instance takes the G limiters (FP64): the GL sweeps and cell widths
   int pb;                       // every instance takes projection-pente-borne (FP64): the PB cell sweeps
   int o3;                       // every instance takes order 3 (FP64): face values, then the O3 cell sweeps
+  int csts;                     // every instance takes schema-csts (FP64)
+  const int4* fwork;            // schema-csts: face work table (instance, chunk of 128 faces of all directions)
+  int nfwork;
   const int4* o3work[3];        // order 3: face work tables (instance, chunk of 128 faces) per direction
   int o3nwork[3];
   int cons_ec;                  // some instance has conservation-energie-totale
@@ -180,6 +183,7 @@ void mark(KernelMarks* m, int kind, cudaStream_t s);
 int persistent_grid(const void* kernel, int threads, size_t smem, int nwork, int pct);
 void launch_bat_lagrange_nodes(const BatchPlan& P, cudaStream_t s, KernelMarks* m);
 void launch_bat_dt(const BatchPlan& P, cudaStream_t s, KernelMarks* m);
+void launch_bat_csts_forward(const BatchPlan& P, cudaStream_t s);
 void launch_batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m);
 void launch_bat_cons_ec(const BatchPlan& P, cudaStream_t s);
 void launch_batch_cycle(const BatchPlan& plan, int sens, cudaStream_t s, KernelMarks* marks = nullptr);

@@ -1084,14 +1084,15 @@ void launch_remap_env(const CycleArgs& a0, int sens, cudaStream_t s, KernelMarks
 // grids (as the one-environment batch in mhy_cycle.cu).  The cell y/z sweeps
 // take 8 or 16 lines per block, the node y/z sweeps 8, as in one context.
 
-template <int K, typename R, bool HC>
+template <int K, typename R, bool HC, bool CSTS = false>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 5 : 3) k_bat_env_lagrange_cells(
     const CycleArgs* __restrict__ D, const int4* __restrict__ W, int nw) {
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_lagrange_cells_body<K, R, false, HC>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p, a.st.cs,
-                                    a.st.mass, a.cqs, a.cqs32, a.L, a.U[0], a.xc, a.fd, a.env, a.Vlag, t.y, t.z, t.w);
+    k_cyc_lagrange_cells_body<K, R, CSTS, HC>(a.dm, a.S, a.ph, a.x0, a.vh, a.n0, a.st.rho, a.st.e, a.st.q, a.st.p,
+                                              a.st.cs, a.st.mass, a.cqs, CSTS ? nullptr : a.cqs32, a.L, a.U[0], a.xc,
+                                              a.fd, a.env, a.Vlag, t.y, t.z, t.w, a.vnb, a.pf);
   }
 }
 
@@ -1138,7 +1139,8 @@ __global__ void __launch_bounds__(32 * kLineWarps, kLineMinBlocks) k_bat_env_nod
   for (int w = blockIdx.x; w < nw; w += gridDim.x) {
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
-    k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh, a.nm,
+    // schema-csts: the forward velocity on the Lagrangian coordinates (xl is null otherwise)
+    k_cyc_sweep_nodes_x_body<FIRST, LAST, K, R, GL>(a.dm, a.S, a.ph, prev, a.x0, a.xl, a.ph.csts ? a.vf : a.vh, a.nm,
                                                  a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf, a.Gd, a.st.mass, a.v, a.nm,
                                                  a.vnorm, t.y, t.z, t.w, a.ecn);
   }
@@ -1151,7 +1153,8 @@ __global__ void __launch_bounds__(32 * kLineWarps, TileGeom<kLineWarps>::minb) k
     const int4 t = W[w];
     const CycleArgs& a = D[t.x];
     __syncthreads();
-    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, K, R, kLineWarps, GL>(a.dm, a.S, a.ph, prev, a.x0, nullptr, a.vh,
+    k_cyc_sweep_nodes_t_body<DD, FIRST, LAST, K, R, kLineWarps, GL>(a.dm, a.S, a.ph, prev, a.x0, a.xl,
+                                                                    a.ph.csts ? a.vf : a.vh,
                                                                     a.nm, a.ud[(it + 1) & 1], a.ud[it & 1], a.dpf,
                                                                     a.Gd, a.st.mass, a.v, a.nm, a.vnorm, t.y, t.z,
                                                                     t.w, a.ecn);
@@ -1256,8 +1259,18 @@ __global__ void __launch_bounds__(128) k_bat_env_cons_ec(const CycleArgs* __rest
 template <int K, typename R, bool GL, bool HC>
 static void batch_cycle_env(const BatchPlan& P, int sens, cudaStream_t s, KernelMarks* m) {
   launch_bat_lagrange_nodes(P, s, m);
-  bat_env_launch(k_bat_env_lagrange_cells<K, R, HC>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs,
-                 P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+  bool done = false;
+  if constexpr (sizeof(R) == 8) {
+    if (P.csts) {   // schema-csts: the cell kernel's CSTS form, then the forward step and the face velocities
+      bat_env_launch(k_bat_env_lagrange_cells<K, R, HC, true>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs,
+                     P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
+      launch_bat_csts_forward(P, s);
+      done = true;
+    }
+  }
+  if (!done)
+    bat_env_launch(k_bat_env_lagrange_cells<K, R, HC>, 128, 0, P, BK_LCELLS, BK_LCELLS, s, m, P.descs,
+                   P.work[BK_LCELLS], P.nwork[BK_LCELLS]);
   int prev = 0;
   for (int it = 0; it < 3; ++it) {
     const int d = (it + sens) % 3;

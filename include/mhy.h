@@ -301,8 +301,8 @@ int mhy_halo_unpack(mhy_ctx* ctx, int32_t cell_lo, int32_t cell_hi, int32_t node
  * exactly as a context (mesh i, options i, state i) and its results equal a
  * context's bit for bit.  Every instance has the same nb_env (1..4) and the same
  * precision; the G limiters (projection_limiteur_id 3..7),
- * projection_pente_borne and ordre_projection 3 are in every instance or in
- * none; schema_csts is not batched (MHY_ERR_UNSUPPORTED). */
+ * projection_pente_borne, ordre_projection 3 and schema_csts are in every
+ * instance or in none (MHY_ERR_UNSUPPORTED otherwise). */
 typedef struct mhy_batch mhy_batch;
 int mhy_batch_create(int n, const mhy_mesh_desc* meshes, const mhy_options* opts, int device, mhy_batch** out);
 int mhy_batch_set_state(mhy_batch* b, int i, const mhy_state* st);

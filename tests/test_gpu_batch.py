@@ -242,6 +242,41 @@ def test_batch_three_gases_order3():
     _same_as_single_contexts(cases, 15)
 
 
+def test_batch_schema_csts_matches_single_contexts():
+    """schema-csts in every instance: the CSTS cell kernel, the forward step
+    over the node tiles and the face velocities over the face work table, the
+    node sweeps on the Lagrangian coordinates (Newton and limiters per
+    instance)."""
+    cases = gen.batched(count=5, seed=39, side_lo=8, side_hi=16, cycles=25)
+    for i, c in enumerate(cases):
+        c.options.schema_csts = 1
+        c.options.with_newton = i % 2
+        c.options.projection_limiteur_id = (0, 1, 2, 1, 0)[i]
+    b = _same_as_single_contexts(cases, 25)
+    assert b.kernels_per_cycle() == 12
+
+
+def test_batch_schema_csts_with_cell_widths():
+    """schema-csts beside the G limiters, pente-borne and order 3 (the cell
+    kernel's CSTS form with the cell widths)."""
+    for extra in (dict(projection_limiteur_id=5), dict(pente_borne=1, pente_borne_debar_fix=1),
+                  dict(ordre_projection=3)):
+        cases = gen.batched(count=3, seed=40, side_lo=8, side_hi=12, cycles=15)
+        for c in cases:
+            c.options.schema_csts = 1
+            for k, v in extra.items():
+                setattr(c.options, k, v)
+        _same_as_single_contexts(cases, 15)
+
+
+def test_batch_two_gases_schema_csts():
+    cases = two_gas_batch()
+    for c in cases:
+        c.options.schema_csts = 1
+    b = _same_as_single_contexts(cases, 12)
+    assert b.kernels_per_cycle() == 13
+
+
 def test_batch_two_gases_pure_limiter_switch():
     cases = two_gas_batch()
     for c in cases:

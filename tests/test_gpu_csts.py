@@ -106,6 +106,6 @@ def test_csts_unsupported_forms_are_refused():
     with pytest.raises(MhyError):
         Context(gen.sod(cycles=5, options=gen.Options(schema_csts=1, precision=1)))
     cases = gen.batched(count=2, seed=5, side_lo=8, side_hi=10, cycles=5)
-    cases[1].options.schema_csts = 1
+    cases[1].options.schema_csts = 1             # a batch takes schema-csts in every instance or in none
     with pytest.raises(MhyError):
         Batch(cases)
